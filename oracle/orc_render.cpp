@@ -1,0 +1,547 @@
+// ORACLE (test infrastructure only). The path tracer and the tile renderer restated from
+// engine/crates/rt-core/src/integrator/mod.rs:237-1891 and render.rs:79-497, plus the C entry
+// points the tests and the CPU baseline call through ctypes. Nothing in the product links this.
+#include <atomic>
+#include <cstdio>
+#include <memory>
+#include <mutex>
+#include <thread>
+
+#include "orc_scene.h"
+
+namespace orc {
+
+struct Prepared {  // integrator/mod.rs:237
+    Lights lights;
+    uint32_t background = 0;  // 0 environment, 1 colour, 2 transparent
+    Rgb background_color;
+    uint32_t floor_mode = 0;
+    float floor_z = 0;
+    Bsdf floor_bsdf;
+    uint32_t max_depth = 8;
+    float clamp_indirect = 0;
+    Material fallback;
+    std::vector<bool> has_medium;
+    std::vector<Rgb> media;  // per material: absorption per mm
+    struct Axes { bool on = false; Vec3 centre, axis, x_axis; };
+    std::vector<Axes> tangent_axes;
+
+    static Prepared make(const Scene& s);
+    float floor_t(const Ray& ray, bool camera_ray) const {
+        bool present = floor_mode == 1 || (floor_mode == 2 && camera_ray);
+        if (!present || ray.dir.z == 0.0f) return F_INF;
+        float t = (floor_z - ray.origin.z) / ray.dir.z;
+        return (t > ray.t_min && t < ray.t_max) ? t : F_INF;
+    }
+    const Material& material(const Scene& s, uint32_t inst) const {
+        if (inst < s.geometry.instances.size()) {
+            uint32_t id = s.geometry.instances[inst].material_id;
+            if (id < s.materials.size()) return s.materials[id];
+        }
+        return fallback;
+    }
+    Frame frame(bool has_inst, uint32_t inst, Vec3 point, Vec3 n) const {  // integrator/mod.rs:833
+        if (has_inst && inst < tangent_axes.size() && tangent_axes[inst].on) {
+            const Axes& a = tangent_axes[inst];
+            Vec3 cands[2] = {cross(a.axis, point - a.centre), a.x_axis};
+            for (Vec3 t : cands) {
+                t = t - n * dot(n, t);
+                if (length_squared(t) > 1.0e-12f) {
+                    Vec3 x = normalize(t);
+                    Frame f;
+                    f.x = x;
+                    f.y = cross(n, x);
+                    f.z = n;
+                    return f;
+                }
+            }
+        }
+        return Frame::from_normal(n);
+    }
+    void add(Rgb& sum, Rgb c, bool indirect) const {  // integrator/mod.rs:855
+        if (!(finite(c.r) && finite(c.g) && finite(c.b))) return;
+        float p = rmax(rmax(c.r, c.g), c.b);
+        if (indirect && clamp_indirect > 0.0f && p > clamp_indirect) sum = sum + c * (clamp_indirect / p);
+        else sum = sum + c;
+    }
+};
+
+Prepared Prepared::make(const Scene& s) {
+    Prepared p;
+    const Environment& env = s.environment;
+    p.background = env.background_mode == 1 || env.background_mode == 3 ? 1 : (env.background_mode == 2 ? 2 : 0);
+    p.background_color = Rgb(rmax(env.background_color.r, 0.0f), rmax(env.background_color.g, 0.0f), rmax(env.background_color.b, 0.0f));
+    p.floor_mode = s.floor.mode;
+    p.floor_z = s.floor.z;
+    p.floor_bsdf = Bsdf::lambert(s.floor.color);
+    p.max_depth = s.render.depth();
+    p.clamp_indirect = s.render.clamp_indirect;
+    for (const Material& m : s.materials) {
+        // medium_of (integrator/mod.rs:298)
+        bool clear = m.transmission > 0.0f && m.metallic < 1.0f && (m.flags & MATERIAL_FLAG_THIN) == 0;
+        bool on = false;
+        Rgb sigma;
+        if (clear && m.absorption_mm > 0.0f && !m.is_emissive()) {
+            auto f = [&](float c) { return -fln(rclamp(c, 1.0e-4f, 1.0f)) / m.absorption_mm; };
+            sigma = Rgb(f(m.base_color.r), f(m.base_color.g), f(m.base_color.b));
+            on = sigma.r > 0.0f || sigma.g > 0.0f || sigma.b > 0.0f;
+        }
+        p.has_medium.push_back(on);
+        p.media.push_back(sigma);
+    }
+    const Geometry& g = s.geometry;
+    for (size_t i = 0; i < g.instances.size(); ++i) {
+        Axes a;
+        const Instance& inst = g.instances[i];
+        if (inst.material_id < s.materials.size()) {
+            const Material& m = s.materials[inst.material_id];
+            if (!(m.anisotropy != m.anisotropy || m.anisotropy <= 0.0f || m.is_emissive()) && inst.mesh < g.meshes.size()) {
+                a.on = true;
+                a.centre = inst.transform.point(g.meshes[inst.mesh].bounds.centroid());
+                a.axis = normalize(inst.transform.vector(Vec3(0, 0, 1)));
+                a.x_axis = normalize(inst.transform.vector(Vec3(1, 0, 0)));
+            }
+        }
+        p.tangent_axes.push_back(a);
+    }
+    p.lights = Lights::make(s);
+    return p;
+}
+
+struct PathStats { uint64_t rays = 0; TraceStats trace; };
+
+// radiance_weighted (integrator/mod.rs:1140) for the scene features this subset reads.
+static void radiance(const Scene& scene, const Prepared& prep, const PixelSampler& sampler, Ray camera_ray, Rgb& out,
+                     float& alpha_out, PathStats& st) {
+    const Lights& lights = prep.lights;
+    Ray ray = camera_ray;
+    Rgb throughput = WHITE, sum = BLACK;
+    float alpha = 1.0f;
+    bool has_pdf = false;
+    float bsdf_pdf = 0.0f;
+    Selection sampled_at = lights.select_by_flux(camera_ray.origin);
+    uint32_t bounce = 0;
+    bool primary = true;
+    float offset = 0.0f;
+    bool in_medium = false;
+    Rgb sigma;
+    const Geometry& geo = scene.geometry;
+    for (;;) {
+        st.rays += 1;
+        RayHit hit;
+        bool got = geo.trace(ray, primary, hit, &st.trace);
+        float t_geometry = got ? hit.t : F_INF;
+        float t_floor = prep.floor_t(ray, primary);
+        float t_nearest = rmin(t_geometry, t_floor);
+        if (in_medium && finite(t_nearest)) {
+            Rgb bl(fexp(-sigma.r * t_nearest), fexp(-sigma.g * t_nearest), fexp(-sigma.b * t_nearest));
+            throughput = throughput * bl;
+        }
+        const float* sp = has_pdf ? &bsdf_pdf : nullptr;
+        Rgb crossed = lights.crossed_from(ray, t_nearest, sp, &sampled_at, offset);
+        prep.add(sum, throughput * crossed, bounce >= 2);
+        if (t_nearest == F_INF) {
+            if (primary && prep.background == 0) {
+                Rgb seen = lights.escaped(ray.dir, nullptr, nullptr);
+                float k = scene.camera.exterior;
+                sum = sum + throughput * (k == 1.0f ? seen : seen * k);
+            } else if (primary && prep.background == 1) {
+                sum = sum + throughput * prep.background_color;
+            } else if (primary && prep.background == 2) {
+                alpha = peak(crossed) > 0.0f ? 1.0f : 0.0f;
+            } else {
+                Rgb sky = lights.escaped(ray.dir, sp, &sampled_at);
+                prep.add(sum, throughput * sky, bounce >= 2);
+            }
+            break;
+        }
+        // The surface: the floor, or an instance with its shading point (bevel.rs:232).
+        Vec3 s_point, s_hit_point, s_normal, s_geometric;
+        bool s_inst = false, s_outside = true, s_front = true;
+        uint32_t inst = 0;
+        if (t_floor < t_geometry) {
+            Vec3 pp = ray.at(t_floor);
+            Vec3 point(pp.x, pp.y, prep.floor_z);
+            Vec3 n(0, 0, ray.dir.z < 0.0f ? 1.0f : -1.0f);
+            s_point = point; s_hit_point = point; s_normal = n; s_geometric = n;
+        } else {
+            Hit d;
+            if (!geo.hit_details(ray, hit, d)) break;
+            Vec3 ng = d.geometric_normal;
+            Vec3 normal = d.normal;
+            if (dot(normal, ng) < 0.0f) normal = -normal;
+            if (dot(normal, ray.dir) >= -1.0e-4f) normal = ng;
+            s_point = geo.terminator_point(d);
+            s_hit_point = d.point;
+            s_normal = normal;
+            s_geometric = ng;
+            s_inst = true;
+            inst = d.instance;
+            s_outside = d.outside;
+            s_front = d.front_face;
+        }
+        const Material* material = s_inst ? &prep.material(scene, inst) : nullptr;
+        if (material && material->is_emissive()) {
+            bool one_sided = (geo.instances[inst].flags & INSTANCE_ONE_SIDED) != 0;
+            if (s_front || !one_sided) {
+                // Emitters that are not mesh lights weigh 1 (light.rs:1541).
+                prep.add(sum, throughput * material->radiance() * 1.0f, bounce >= 2);
+            }
+            break;
+        }
+        if (bounce >= prep.max_depth) break;
+        Bsdf bsdf = material ? Bsdf::surface(*material, s_outside) : prep.floor_bsdf;
+        Frame frame = prep.frame(s_inst, inst, s_point, s_normal);
+        Vec3 wo = frame.to_local(-ray.dir);
+        Vec3 ng = s_geometric;
+        Vec3 origin = offset_origin(s_point, ng);
+        uint32_t dims = bounce_dim(bounce);
+
+        // Next-event estimation (integrator/mod.rs:1702).
+        Selection selection = lights.select(s_point);
+        float ul0, ul1;
+        sampler.get2(dims + OFFSET_LIGHT, ul0, ul1);
+        LightSample ls;
+        float usel = sampler.get1(dims + OFFSET_LIGHT_SELECT);
+        if (lights.sample_selected(selection, usel, ul0, ul1, ls)) {
+            Vec3 wi = frame.to_local(ls.wi);
+            Lobes lobes = ls.glossy ? Lobes::All : Lobes::Diffuse;
+            Rgb f = bsdf.eval(wo, wi, lobes);
+            if (peak(f) > 0.0f) {
+                Vec3 from = wi.z < 0.0f ? offset_origin(s_hit_point, -ng) : origin;
+                float distance = ls.distance;
+                bool arrives = true;
+                if (ls.shadow) {
+                    st.rays += 1;
+                    Ray sr(from, ls.wi);
+                    if (finite(distance)) sr.t_max = distance * (1.0f - 1.0e-4f);
+                    bool blocked = (prep.floor_mode == 1 && prep.floor_t(sr, false) < F_INF) || geo.occluded(sr, false, &st.trace);
+                    arrives = !blocked;
+                }
+                if (arrives) {
+                    float weight = (ls.delta || !ls.glossy) ? 1.0f : power_heuristic(ls.pdf, bsdf.pdf(wo, wi));
+                    Rgb c = throughput * f * ls.radiance * (std::fabs(wi.z) * weight / ls.pdf);
+                    prep.add(sum, c, bounce >= 1);
+                }
+            }
+        }
+        // The next direction.
+        float ub0, ub1;
+        sampler.get2(dims + OFFSET_BSDF, ub0, ub1);
+        BsdfSample bs;
+        if (!bsdf.sample(wo, ub0, ub1, bs)) break;
+        bool transmitted = bs.wi.z < 0.0f;
+        Vec3 wi = bs.straight ? ray.dir : normalize(frame.to_world(bs.wi));
+        if (transmitted) {
+            if (dot(wi, ng) >= 0.0f) break;
+        } else if (dot(wi, ng) <= 0.0f) {
+            break;
+        }
+        throughput = throughput * bs.weight;
+        if (bounce >= 2) {
+            float survive = rclamp(peak(throughput), 0.05f, 1.0f);
+            if (sampler.get1(dims + OFFSET_ROULETTE) >= survive) break;
+            throughput = throughput / survive;
+        }
+        float pk = peak(throughput);
+        if (!(pk > 0.0f && finite(pk))) break;
+        Vec3 next_origin = transmitted ? offset_origin(s_hit_point, -ng) : origin;
+        if (bs.straight) {
+            offset += dot(next_origin - ray.origin, ray.dir);
+        } else {
+            has_pdf = true;
+            bsdf_pdf = bs.pdf;
+            sampled_at = selection;
+            primary = false;
+            offset = 0.0f;
+            if (transmitted) {
+                if (s_outside && material && s_inst) {
+                    uint32_t mid = geo.instances[inst].material_id;
+                    in_medium = mid < prep.has_medium.size() && prep.has_medium[mid];
+                    if (in_medium) sigma = prep.media[mid];
+                } else {
+                    in_medium = false;
+                }
+            }
+        }
+        ray = Ray(next_origin, wi);
+        bounce += 1;
+    }
+    out = sum;
+    alpha_out = alpha;
+}
+
+static float filter_offset(uint32_t filter, float u) {  // pixel_filter.rs:103
+    if (filter == 1) return 0.5f;
+    if (filter == 2) return 0.5f + (u < 0.5f ? std::sqrt(2.0f * u) - 1.0f : 1.0f - std::sqrt(2.0f - 2.0f * u));
+    return u;
+}
+
+// camera_sample_weighted (render.rs:79) and the shade of render_tile_traced (render.rs:388).
+static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, uint32_t y, uint32_t index, Rgb& c,
+                        float& alpha, PathStats& st) {
+    uint32_t width = scene.render.width ? scene.render.width : 1, height = scene.render.height ? scene.render.height : 1;
+    float aspect = (float)width / (float)height;
+    PixelSampler sampler(scene.render.seed, x, y, index);
+    float du, dv;
+    sampler.get2(DIM_CAMERA, du, dv);
+    du = filter_offset(scene.render.pixel_filter, du);
+    dv = filter_offset(scene.render.pixel_filter, dv);
+    float u = ((float)x + du) / (float)width;
+    float v = ((float)y + dv) / (float)height;
+    float lx = 0.0f, ly = 0.0f;
+    if (scene.camera.lens_radius() > 0.0f) {
+        float a, b;
+        sampler.get2(DIM_LENS, a, b);
+        concentric_disk(a, b, lx, ly);
+    }
+    Ray ray = scene.camera.generate_ray(aspect, u, v, lx, ly);
+    radiance(scene, prep, sampler, ray, c, alpha, st);
+}
+
+struct Film {
+    uint32_t ox, oy, w, h;
+    std::vector<float> rgb, weight, alpha, lum2;
+    Film(uint32_t x, uint32_t y, uint32_t ww, uint32_t hh)
+        : ox(x), oy(y), w(ww), h(hh), rgb((size_t)ww * hh * 3), weight((size_t)ww * hh), alpha((size_t)ww * hh), lum2((size_t)ww * hh) {}
+    void splat(uint32_t x, uint32_t y, Rgb c, float a) {  // image.rs:82
+        if (x < ox || y < oy || x - ox >= w || y - oy >= h) return;
+        size_t i = (size_t)(y - oy) * w + (x - ox);
+        rgb[3 * i] += c.r;
+        rgb[3 * i + 1] += c.g;
+        rgb[3 * i + 2] += c.b;
+        weight[i] += 1.0f;
+        alpha[i] += a;
+        float l = c.luminance();
+        lum2[i] += l * l;
+    }
+};
+
+// render_tile_traced (render.rs:388) into `film`, one sample index, no edge pixels.
+static void render_tile(const Scene& scene, const Prepared& prep, uint32_t tx, uint32_t ty, uint32_t tw, uint32_t th,
+                        uint32_t index, Film& film, PathStats& st) {
+    uint32_t x_end = std::min<uint64_t>((uint64_t)tx + tw, scene.render.width);
+    uint32_t y_end = std::min<uint64_t>((uint64_t)ty + th, scene.render.height);
+    for (uint32_t y = ty; y < y_end; ++y)
+        for (uint32_t x = tx; x < x_end; ++x) {
+            Rgb c;
+            float a;
+            shade_pixel(scene, prep, x, y, index, c, a, st);
+            film.splat(x, y, c * WHITE, a);
+        }
+}
+
+struct Loaded {
+    Scene scene;
+    Prepared prep;
+};
+
+}  // namespace orc
+
+using namespace orc;
+
+namespace {
+std::mutex g_mu;
+std::vector<std::unique_ptr<Loaded>> g_scenes;
+std::string g_error;
+Loaded* get(uint32_t h) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (h == 0 || h > g_scenes.size()) return nullptr;
+    return g_scenes[h - 1].get();
+}
+}  // namespace
+
+extern "C" {
+
+// Loads an RSB scene; 0 on error (orc_error gives the message).
+uint32_t orc_scene_load(const uint8_t* bytes, uint32_t len) {
+    if (!bytes) return 0;
+    auto l = std::make_unique<Loaded>();
+    std::string err;
+    if (!read_rsb(bytes, len, l->scene, err)) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_error = err;
+        return 0;
+    }
+    l->prep = Prepared::make(l->scene);
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_error.clear();
+    for (size_t i = 0; i < g_scenes.size(); ++i)
+        if (!g_scenes[i]) { g_scenes[i] = std::move(l); return (uint32_t)i + 1; }
+    g_scenes.push_back(std::move(l));
+    return (uint32_t)g_scenes.size();
+}
+uint32_t orc_error(char* out, uint32_t cap) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    uint32_t n = (uint32_t)g_error.size();
+    if (out && cap) { uint32_t k = n < cap - 1 ? n : cap - 1; std::memcpy(out, g_error.data(), k); out[k] = 0; }
+    return n;
+}
+uint32_t orc_scene_free(uint32_t h) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (h == 0 || h > g_scenes.size() || !g_scenes[h - 1]) return 1;
+    g_scenes[h - 1].reset();
+    return 0;
+}
+// Scene facts: width, height, seed, max_depth, instance count, triangle count (instanced).
+uint32_t orc_scene_info(uint32_t h, uint32_t* out6) {
+    Loaded* l = get(h);
+    if (!l || !out6) return 1;
+    out6[0] = l->scene.render.width;
+    out6[1] = l->scene.render.height;
+    out6[2] = l->scene.render.seed;
+    out6[3] = l->prep.max_depth;
+    out6[4] = (uint32_t)l->scene.geometry.instances.size();
+    uint64_t tris = 0;
+    for (const Instance& in : l->scene.geometry.instances) tris += l->scene.geometry.meshes[in.mesh].triangle_count();
+    out6[5] = (uint32_t)tris;
+    return 0;
+}
+
+// Film accumulation over a region, samples [first, first + count) per pixel in order, tiles of
+// `tile` pixels claimed by `threads` workers (rt-cli/src/lib.rs:266-368). Outputs are the film's
+// sums: rgb (3 per pixel), weight, alpha, lum2. Returns the ray count; stats3 (may be null) gets
+// rays, inner-node visits, packet tests.
+uint64_t orc_render_film(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint32_t hgt, uint32_t first, uint32_t count,
+                         uint32_t tile, uint32_t threads, float* rgb, float* weight, float* alpha, float* lum2,
+                         uint64_t* stats3) {
+    Loaded* l = get(h);
+    if (!l || !rgb || w == 0 || hgt == 0) return 0;
+    if (tile == 0) tile = 32;
+    if (threads == 0) threads = 1;
+    std::vector<uint32_t> tiles;
+    for (uint32_t y = 0; y < hgt; y += tile)
+        for (uint32_t x = 0; x < w; x += tile) { tiles.push_back(x); tiles.push_back(y); }
+    std::atomic<size_t> next(0);
+    std::atomic<uint64_t> rays(0), nodes(0), packets(0);
+    auto worker = [&]() {
+        PathStats st;
+        for (;;) {
+            size_t t = next.fetch_add(1);
+            if (t >= tiles.size() / 2) break;
+            uint32_t tx = tiles[2 * t], ty = tiles[2 * t + 1];
+            uint32_t tw = std::min(tile, w - tx), th = std::min(tile, hgt - ty);
+            Film film(x0 + tx, y0 + ty, tw, th);
+            for (uint32_t s = 0; s < count; ++s) render_tile(l->scene, l->prep, x0 + tx, y0 + ty, tw, th, first + s, film, st);
+            for (uint32_t yy = 0; yy < th; ++yy)
+                for (uint32_t xx = 0; xx < tw; ++xx) {
+                    size_t i = (size_t)yy * tw + xx, o = (size_t)(ty + yy) * w + (tx + xx);
+                    for (int c = 0; c < 3; ++c) rgb[3 * o + c] += film.rgb[3 * i + c];
+                    if (weight) weight[o] += film.weight[i];
+                    if (alpha) alpha[o] += film.alpha[i];
+                    if (lum2) lum2[o] += film.lum2[i];
+                }
+        }
+        rays += st.rays;
+        nodes += st.trace.nodes;
+        packets += st.trace.packets;
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t i = 0; i < threads; ++i) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+    if (stats3) { stats3[0] = rays; stats3[1] = nodes; stats3[2] = packets; }
+    return rays;
+}
+
+// One sample of each pixel of a tile as `rt_render_tile` gives it: w*h*3 radiance (resolved
+// one-sample film), zero outside the image. Returns the ray count.
+uint64_t orc_render_tile(uint32_t h, uint32_t x, uint32_t y, uint32_t w, uint32_t hgt, uint32_t sample, float* out_rgb,
+                         float* out_alpha) {
+    Loaded* l = get(h);
+    if (!l || !out_rgb) return 0;
+    Film film(x, y, w, hgt);
+    PathStats st;
+    render_tile(l->scene, l->prep, x, y, w, hgt, sample, film, st);
+    for (size_t i = 0; i < (size_t)w * hgt; ++i) {
+        float wt = film.weight[i];
+        float inv = wt > 0.0f ? 1.0f / wt : 0.0f;
+        for (int c = 0; c < 3; ++c) out_rgb[3 * i + c] = wt > 0.0f ? film.rgb[3 * i + c] * inv : 0.0f;
+        if (out_alpha) out_alpha[i] = wt > 0.0f ? film.alpha[i] * inv : 0.0f;
+    }
+    return st.rays;
+}
+
+// Per-path radiance of explicit (pixel x, pixel y, sample) triples: out = r, g, b, alpha, rays.
+void orc_paths(uint32_t h, const uint32_t* xys, uint32_t n, float* out5) {
+    Loaded* l = get(h);
+    if (!l) return;
+    for (uint32_t i = 0; i < n; ++i) {
+        PathStats st;
+        Rgb c;
+        float a;
+        shade_pixel(l->scene, l->prep, xys[3 * i], xys[3 * i + 1], xys[3 * i + 2], c, a, st);
+        out5[5 * i] = c.r; out5[5 * i + 1] = c.g; out5[5 * i + 2] = c.b; out5[5 * i + 3] = a; out5[5 * i + 4] = (float)st.rays;
+    }
+}
+
+// Nearest hits of a ray batch (ray = ox oy oz dx dy dz tmin tmax); hits = instance, triangle,
+// t bits (0xffffffff instance: miss). `brute` uses every triangle instead of the BVH. stats2
+// (may be null) gets inner-node visits and packet tests summed over the batch.
+void orc_trace(uint32_t h, const float* rays, uint32_t n, uint32_t camera, uint32_t brute, uint32_t* hits, uint64_t* stats2) {
+    Loaded* l = get(h);
+    if (!l) return;
+    TraceStats st;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* r = rays + 8 * i;
+        Ray ray(Vec3(r[0], r[1], r[2]), Vec3(r[3], r[4], r[5]));
+        ray.t_min = r[6];
+        ray.t_max = r[7];
+        RayHit hit;
+        bool got = brute ? l->scene.geometry.trace_brute(ray, camera != 0, hit) : l->scene.geometry.trace(ray, camera != 0, hit, &st);
+        hits[3 * i] = got ? hit.instance : 0xffffffffu;
+        hits[3 * i + 1] = got ? hit.triangle : 0xffffffffu;
+        hits[3 * i + 2] = got ? fbits(hit.t) : 0u;
+    }
+    if (stats2) { stats2[0] = st.nodes; stats2[1] = st.packets; }
+}
+// Any-hit of a ray batch: occluded[i] = 1 when something lies in [tmin, tmax].
+void orc_occluded(uint32_t h, const float* rays, uint32_t n, uint8_t* occluded) {
+    Loaded* l = get(h);
+    if (!l) return;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* r = rays + 8 * i;
+        Ray ray(Vec3(r[0], r[1], r[2]), Vec3(r[3], r[4], r[5]));
+        ray.t_min = r[6];
+        ray.t_max = r[7];
+        occluded[i] = l->scene.geometry.occluded(ray, false) ? 1 : 0;
+    }
+}
+
+// The energy tables (u16 albedo[1024], schlick[1024], clear_in[17408], clear_out[17408];
+// f32 albedo_avg[32], schlick_avg[32]).
+void orc_energy_tables(uint16_t* u16s, float* f32s) {
+    const EnergyTables& t = energy_tables();
+    std::memcpy(u16s, t.albedo.data(), 1024 * 2);
+    std::memcpy(u16s + 1024, t.schlick.data(), 1024 * 2);
+    std::memcpy(u16s + 2048, t.clear_in.data(), 17408 * 2);
+    std::memcpy(u16s + 2048 + 17408, t.clear_out.data(), 17408 * 2);
+    std::memcpy(f32s, t.albedo_avg.data(), 32 * 4);
+    std::memcpy(f32s + 32, t.schlick_avg.data(), 32 * 4);
+}
+
+// Known-answer helpers: Pcg32, mix64, Sobol points, owen-scrambled sampler values, fmath.
+void orc_pcg32(uint64_t seed, uint64_t stream, uint32_t n, uint32_t* out) {
+    Pcg32 r = Pcg32::seeded(seed, stream);
+    for (uint32_t i = 0; i < n; ++i) out[i] = r.next_u32();
+}
+uint64_t orc_mix64(uint64_t z) { return mix64(z); }
+uint32_t orc_sobol(uint32_t dim, uint32_t index) { return sobol(dim, index); }
+float orc_sampler_get1(uint32_t seed, uint32_t x, uint32_t y, uint32_t index, uint32_t dim) {
+    return PixelSampler(seed, x, y, index).get1(dim);
+}
+void orc_fmath(uint32_t which, const float* in, uint32_t n, float* out) {
+    for (uint32_t i = 0; i < n; ++i) {
+        float x = in[i];
+        switch (which) {
+            case 0: out[i] = fsin(x); break;
+            case 1: out[i] = fcos(x); break;
+            case 2: out[i] = exp2(x); break;
+            case 3: out[i] = log2(x); break;
+            case 4: out[i] = fatan(x); break;
+            case 5: out[i] = facos(x); break;
+            default: out[i] = 0.0f;
+        }
+    }
+}
+
+}  // extern "C"

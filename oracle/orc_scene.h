@@ -1,0 +1,123 @@
+// ORACLE (test infrastructure only). Scene model, RSB subset reader, lights, environment ramp and
+// camera, restated from engine/crates/rt-core/src/{scene/mod.rs, scene/rsb.rs, light.rs,
+// environment.rs}.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "orc_bsdf.h"
+#include "orc_geometry.h"
+
+namespace orc {
+
+struct Camera {  // scene/mod.rs:91
+    Vec3 position{0, -1000, 0}, target{0, 0, 0}, up{0, 0, 1};
+    float focal_mm = 50, sensor_mm = 36, fstop = 0, focus_dist = 1000;
+    bool ortho = false;
+    float ortho_width = 1000;
+    uint32_t projection = 0;
+    float fov_x_deg = 360, fov_y_deg = 180, exterior = 1;
+    void basis(Vec3& forward, Vec3& right, Vec3& upv) const;
+    float lens_radius() const { return (fstop > 0.0f && focus_dist > 0.0f && !ortho) ? focal_mm / fstop * 0.5f : 0.0f; }
+    Ray generate_ray(float aspect, float u, float v, float lx, float ly) const;
+};
+enum class LightKind : uint32_t { Rect = 0, Disk = 1, Sun = 2, Point = 3, Spot = 4, Ies = 5 };
+constexpr uint32_t LIGHT_FLAG_GLOSSY = 1, LIGHT_FLAG_CAMERA = 2, LIGHT_FLAG_NO_SHADOW = 4;
+struct Light {
+    uint32_t kind = 0;
+    Vec3 position, direction{0, 0, -1}, up{0, 1, 0};
+    float size_x = 0, size_y = 0;
+    Rgb color = WHITE;
+    float power = 0, spread_deg = 180, angle_deg = 0;
+    uint32_t flags = 0;
+};
+struct Environment {  // scene/mod.rs:739
+    uint32_t kind = 0;
+    float floor = 0.1f, horizon = 0.3f, zenith = 0.6f, strength = 1.0f, rotation_deg = 0.0f;
+    Rgb background_color = Rgb::splat(0.05f);
+    uint32_t background_mode = 0;
+};
+struct Floor { uint32_t mode = 0; float z = 0; Rgb color = Rgb::splat(0.5f); };
+struct RenderSettings {  // scene/mod.rs:911
+    uint32_t width = 640, height = 360, max_samples = 64, seed = 0;
+    float max_seconds = 0, exposure_ev = 0;
+    uint32_t tonemap = 1, max_depth = 8;
+    float clamp_indirect = 0;
+    uint32_t passes = 0, denoise = 0, caustic_photons = 0;
+    float caustic_radius = 0, denoise_strength = 1;
+    uint32_t pixel_filter = 0, edge_supersample = 1, adaptive = 0;
+    float noise_threshold = 0;
+    uint32_t depth() const { return max_depth == 0 ? 8 : (max_depth < 1024 ? max_depth : 1024); }
+};
+struct Scene {
+    Camera camera;
+    std::vector<Material> materials;
+    Geometry geometry;
+    std::vector<Light> lights;
+    Environment environment;
+    Floor floor;
+    RenderSettings render;
+};
+// Parses the RSB subset (CAMR, MESH, MATL, LGHT, ENVR, FLOR, RNDR, INST; unknown tags skipped).
+// Sections of features outside the path tracer's core (LENS, BMAP, PATN, IMGS, PROG, FXAM,
+// SECT, GLAS, WET*, NEST, IESP) and scene values that need them are refused with a message.
+bool read_rsb(const uint8_t* bytes, size_t len, Scene& out, std::string& error);
+
+// ---- environment.rs: the dome / flat ramp ------------------------------------------------------
+struct Ramp {
+    float floor = 0, horizon = 0, zenith = 0, lower_mass = 0, total_mass = 0;
+    static Ramp make(float f, float h, float z, float strength);
+    float value(float z) const;
+    float pdf(Vec3 dir) const;
+    bool sample(float u0, float u1, Vec3& dir, float& pdf_out) const;
+    float mean_radiance() const { return 0.5f * total_mass; }
+    bool is_black() const { return total_mass <= 0.0f; }
+};
+
+// ---- light.rs ----------------------------------------------------------------------------------
+struct AreaLight {
+    bool rect;
+    float half_x, half_y, radius;
+    Vec3 centre;
+    Frame frame;
+    float area;
+    Rgb radiance;
+    float exponent;
+    bool glossy, camera, shadow;
+    uint32_t entry;
+    float base, bound;
+    Rgb radiance_at(float cos) const { return exponent == 0.0f ? radiance : radiance * powf_(cos, exponent); }
+    Vec3 sample_point(float u0, float u1) const;
+    bool intersect(const Ray& ray, float t_max, float& t, float& cos) const;
+    float weight(Vec3 x) const;
+};
+struct Selection { Vec3 point; float total = 0; bool by_flux = true; float weights[8] = {}; };
+struct LightSample { Vec3 wi; float distance; Rgb radiance; float pdf; bool delta, glossy, photon, shadow; };
+struct Lights {
+    std::vector<AreaLight> areas;
+    Ramp env;
+    bool env_is_entry = false;
+    uint32_t env_entry = 0;
+    float env_base = 0;
+    std::vector<int> entries;  // >= 0: area index; -1: environment
+    std::vector<float> cdf, flux_pmf;
+    bool per_point = false;
+
+    static Lights make(const Scene& scene);
+    float weight(size_t entry, Vec3 x) const;
+    Selection select(Vec3 x) const;
+    Selection select_by_flux(Vec3 x) const { Selection s; s.point = x; s.by_flux = true; return s; }
+    float weight_at(size_t entry, const Selection& s) const { return entry < 8 ? s.weights[entry] : weight(entry, s.point); }
+    float pmf(uint32_t entry, const Selection& from) const;
+    void pick_at(const Selection& s, float u, size_t& idx, float& rest, float& pmf_out) const;
+    bool sample_selected(const Selection& s, float u_select, float u0, float u1, LightSample& out) const;
+    Rgb crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, const Selection* from, float offset) const;
+    Rgb escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from) const;
+};
+inline float power_heuristic(float pa, float pb) {  // light.rs:129
+    if (!(pa > 0.0f)) return 0.0f;
+    float r = pb / pa;
+    return 1.0f / (1.0f + r * r);
+}
+
+}  // namespace orc
