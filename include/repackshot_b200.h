@@ -1,0 +1,115 @@
+/* repackshot_b200: the C ABI of the B200 path tracer, a drop-in for the progressive
+ * sample-and-accumulate render of the Repackshot engine.
+ *
+ * The reference's engine is Rust; its only C ABI is the hand-written one of the rt-wasm crate
+ * (engine/crates/rt-wasm/src/ffi.rs), which every host (the Web Worker pool, the parity tools)
+ * binds. The functions below keep its names (rt_ -> rtg_), argument meaning, ownership and
+ * status codes; the film and parity entry points have no wasm counterpart and replace the
+ * in-process Rust calls cited beside them.
+ *
+ * Threading: every call holds one library-wide lock, so calls serialise (the reference's
+ * registry sits behind a Mutex, rt-wasm/src/lib.rs:10-13). Work runs on a CUDA stream owned by
+ * the scene; every call returns after its work is complete unless stated otherwise.
+ */
+#ifndef REPACKSHOT_B200_H
+#define REPACKSHOT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTG_ABI_VERSION 1u
+
+/* Status codes: 0-5 as rt-wasm/src/lib.rs:37-53; 16 and up are this library's own. */
+#define RTG_STATUS_OK 0u
+#define RTG_STATUS_BAD_HANDLE 1u
+#define RTG_STATUS_BAD_TILE 2u      /* empty tile or more than RTG_MAX_TILE_PIXELS pixels */
+#define RTG_STATUS_NULL_POINTER 3u
+#define RTG_STATUS_BAD_SCENE 4u
+#define RTG_STATUS_CUDA_ERROR 16u   /* the message is in rtg_scene_error_* */
+#define RTG_STATUS_STACK_OVERFLOW 17u
+#define RTG_STATUS_BAD_FILM 18u
+
+/* Largest tile rtg_render_tile accepts: 2048 x 2048 (rt-wasm/src/lib.rs:56 MAX_TILE_PIXELS). */
+#define RTG_MAX_TILE_PIXELS (1ull << 22)
+
+/* rt_version (ffi.rs): the ABI version. */
+uint32_t rtg_version(void);
+
+/* rt_scene_load (ffi.rs:56-66, lib.rs:145): parses an RSB scene (copied; the caller keeps its
+ * bytes), builds its BVHs and uploads it. Returns a handle > 0, or 0 after recording the error
+ * (rtg_scene_error_len / _copy). Features outside the path tracer's core (textures, lens
+ * optics, particles, sky and HDRI maps, point/spot/sun lights, cut-outs, thin walls, media,
+ * bevels, the shadow catcher) are refused with a message that starts with "unsupported:". */
+uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len);
+
+/* rt_scene_error_len / rt_scene_error_copy (ffi.rs:90-110): the last error message, UTF-8,
+ * without terminator; empty after a successful load. */
+uint32_t rtg_scene_error_len(void);
+void rtg_scene_error_copy(uint8_t* out);
+
+/* rt_scene_free (ffi.rs:113-116): RTG_STATUS_OK or RTG_STATUS_BAD_HANDLE. */
+uint32_t rtg_scene_free(uint32_t handle);
+
+/* rt_render_tile (ffi.rs:118-157, lib.rs:701-710): sample `sample_index` of the pixel rectangle
+ * (x, y, w, h) into `out`, w*h*3 floats of linear RGB, row major; one sample, not accumulated;
+ * pixels outside the image are zero. */
+uint32_t rtg_render_tile(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index,
+                         float* out);
+
+/* rt_render_tile_rgba (ffi.rs:159-197, lib.rs:715): as rtg_render_tile with coverage, w*h*4
+ * floats of premultiplied RGBA. */
+uint32_t rtg_render_tile_rgba(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index,
+                              float* out);
+
+/* A film on the device: the reference's Film (rt-core/src/image.rs:14-93) over the image
+ * rectangle (x, y, w, h): per pixel the sums of RGB, sample count, coverage and squared
+ * luminance. Returns a film handle > 0, or 0 (error message as for loads). */
+uint32_t rtg_film_create(uint32_t scene, uint32_t x, uint32_t y, uint32_t w, uint32_t h);
+uint32_t rtg_film_free(uint32_t film);
+uint32_t rtg_film_clear(uint32_t film);
+
+/* render_tile_prepared (rt-core/src/render.rs:272-281) over a range of samples: for every
+ * pixel of the film inside the image, film += sample(first_sample) + ... +
+ * sample(first_sample + count - 1), added in sample order, as repeated calls of the reference
+ * accumulate. `rays` (may be null) receives the camera + extension + shadow rays cast. */
+uint32_t rtg_render_progressive(uint32_t scene, uint32_t film, uint32_t first_sample, uint32_t count, uint64_t* rays);
+
+/* Copies the film's sums to host memory (any pointer may be null): rgb 3*w*h floats, weight,
+ * alpha and lum2 w*h floats each. */
+uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2);
+
+/* The film's device arrays (valid until rtg_film_free), for callers that stay on the GPU. */
+uint32_t rtg_film_device(uint32_t film, float** rgb, float** weight, float** alpha, float** lum2);
+
+/* radiance_with (rt-core/src/integrator/mod.rs:1107) of explicit paths: for each (x, y,
+ * sample index) triple of `xys` (3*n u32), out5[5i..5i+5] = radiance r, g, b, alpha, 0. */
+uint32_t rtg_render_paths(uint32_t scene, const uint32_t* xys, uint32_t n, float* out5);
+
+/* Geometry::trace_class / occluded_class (rt-core/src/geometry/mod.rs:566-629) of a ray batch:
+ * rays 8*n floats (origin xyz, dir xyz, t_min, t_max). mode bit 0: camera class (instances
+ * hidden to the camera are skipped); bit 1: any hit. Nearest: out 3*n u32 = instance, triangle,
+ * t bits (instance 0xffffffff: miss). Any: out n u32 = 1 when blocked. */
+uint32_t rtg_trace_rays(uint32_t scene, const float* rays, uint32_t n, uint32_t mode, uint32_t* out);
+
+/* Facts of a loaded scene: width, height, max depth, instanced triangles, BVH nodes, leaf
+ * triangles, BVH build seconds, rays cast so far. */
+uint32_t rtg_scene_stats(uint32_t scene, double* out8);
+
+/* Largest number of paths one wave holds (default 4 Mi; memory is 160 bytes per path). */
+uint32_t rtg_set_path_capacity(uint32_t scene, uint32_t paths);
+
+/* Extend-kernel timing: when enabled, every extend launch is bracketed by CUDA events on the
+ * scene's stream. out4 = total extend milliseconds, extend launches, camera + extension rays,
+ * shadow rays, accumulated since the last reset (read before this call's reset). */
+uint32_t rtg_timing(uint32_t scene, uint32_t enable, uint32_t reset, double* out4);
+
+uint32_t rtg_synchronize(uint32_t scene);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* REPACKSHOT_B200_H */

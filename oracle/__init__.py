@@ -1,0 +1,144 @@
+"""ORACLE (test infrastructure only): ctypes binding of the C++ restatement of the Repackshot
+engine's path tracer (oracle/*.cpp, built by oracle/Makefile into oracle/_build/liborc.so).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use it, as the checker
+and the timed CPU reference; the product (repackshot_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liborc.so"
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = ctypes.CDLL(str(LIB))
+        v, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+        sig = {
+            "orc_scene_load": (u32, [ctypes.c_char_p, u32]),
+            "orc_error": (u32, [v, u32]),
+            "orc_scene_free": (u32, [u32]),
+            "orc_scene_info": (u32, [u32, v]),
+            "orc_render_film": (u64, [u32, u32, u32, u32, u32, u32, u32, u32, u32, v, v, v, v, v]),
+            "orc_render_tile": (u64, [u32, u32, u32, u32, u32, u32, v, v]),
+            "orc_paths": (None, [u32, v, u32, v]),
+            "orc_trace": (None, [u32, v, u32, u32, u32, v, v]),
+            "orc_occluded": (None, [u32, v, u32, v]),
+            "orc_energy_tables": (None, [v, v]),
+            "orc_pcg32": (None, [u64, u64, u32, v]),
+            "orc_mix64": (u64, [u64]),
+            "orc_sobol": (u32, [u32, u32]),
+            "orc_sampler_get1": (ctypes.c_float, [u32, u32, u32, u32, u32]),
+            "orc_fmath": (None, [u32, v, u32, v]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib().orc_error(buf, 1024)
+    return buf.value.decode()
+
+
+class OracleScene:
+    def __init__(self, rsb: bytes):
+        self.handle = lib().orc_scene_load(rsb, len(rsb))
+        if not self.handle:
+            raise ValueError(error())
+        info = np.zeros(6, np.uint32)
+        lib().orc_scene_info(self.handle, _p(info))
+        self.width, self.height, self.seed, self.max_depth, self.instances, self.triangles = map(int, info)
+
+    def close(self):
+        if self.handle:
+            lib().orc_scene_free(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render_film(self, first=0, count=1, x=0, y=0, w=None, h=None, tile=32, threads=1):
+        """Film sums of samples [first, first+count) over a rectangle: (rgb, weight, alpha, lum2,
+        stats=(rays, node visits, packet tests))."""
+        w = self.width if w is None else w
+        h = self.height if h is None else h
+        n = w * h
+        rgb, wt, al, l2 = (np.zeros(3 * n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32))
+        st = np.zeros(3, np.uint64)
+        lib().orc_render_film(self.handle, x, y, w, h, first, count, tile, threads, _p(rgb), _p(wt), _p(al), _p(l2), _p(st))
+        return rgb.reshape(h, w, 3), wt.reshape(h, w), al.reshape(h, w), l2.reshape(h, w), tuple(int(v) for v in st)
+
+    def render_tile(self, x, y, w, h, sample, rgba=False):
+        rgb = np.zeros(3 * w * h, np.float32)
+        al = np.zeros(w * h, np.float32)
+        lib().orc_render_tile(self.handle, x, y, w, h, sample, _p(rgb), _p(al))
+        if not rgba:
+            return rgb
+        return np.concatenate([rgb.reshape(-1, 3), al.reshape(-1, 1)], axis=1).reshape(-1)
+
+    def paths(self, xys):
+        xys = np.ascontiguousarray(xys, dtype=np.uint32).reshape(-1, 3)
+        out = np.zeros((len(xys), 5), np.float32)
+        lib().orc_paths(self.handle, _p(xys), len(xys), _p(out))
+        return out
+
+    def trace(self, rays, camera=False, brute=False):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        hits = np.zeros((len(rays), 3), np.uint32)
+        st = np.zeros(2, np.uint64)
+        lib().orc_trace(self.handle, _p(rays), len(rays), int(camera), int(brute), _p(hits), _p(st))
+        return hits, (int(st[0]), int(st[1]))
+
+    def occluded(self, rays):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        out = np.zeros(len(rays), np.uint8)
+        lib().orc_occluded(self.handle, _p(rays), len(rays), _p(out))
+        return out
+
+
+def energy_tables():
+    u16 = np.zeros(2048 + 2 * 17408, np.uint16)
+    f = np.zeros(64, np.float32)
+    lib().orc_energy_tables(_p(u16), _p(f))
+    return {"albedo": u16[:1024], "schlick": u16[1024:2048], "clear_in": u16[2048:2048 + 17408],
+            "clear_out": u16[2048 + 17408:], "albedo_avg": f[:32], "schlick_avg": f[32:]}
+
+
+def fnv1a(values) -> int:
+    h = 0x811C9DC5
+    for byte in np.ascontiguousarray(values, dtype="<f4").tobytes():
+        h = ((h ^ byte) * 0x01000193) & 0xFFFFFFFF
+    return h
+
+
+def resolve(rgb, weight):
+    """Film::resolve (image.rs:158): rgb * (1 / weight) in f32, black where weight is 0."""
+    w = np.asarray(weight, np.float32)
+    inv = np.where(w > 0, np.float32(1.0) / np.where(w > 0, w, np.float32(1.0)), np.float32(0.0)).astype(np.float32)
+    return (np.asarray(rgb, np.float32) * inv[..., None]).astype(np.float32)

@@ -1,0 +1,229 @@
+"""repackshot_b200: a B200-native (sm_100a) drop-in for the progressive sample-and-accumulate
+render of the Repackshot engine's path tracer.
+
+The native library ``librtg.so`` (built by ``repackshot_b200.build``) exports the C ABI declared
+in ``include/repackshot_b200.h``; this module binds it with ctypes and mirrors the Rust host API
+of the reference's rt-wasm crate (engine/crates/rt-wasm/src/lib.rs: ``scene_load``,
+``scene_free``, ``error_message``, ``render_tile``, ``render_tile_rgba``), with the same status
+codes, plus device films for progressive rendering.
+
+There is no CPU fallback: every call runs the CUDA kernels, and importing the binding without the
+built library (or without a GPU at call time) raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+STATUS_OK = 0
+STATUS_BAD_HANDLE = 1
+STATUS_BAD_TILE = 2
+STATUS_NULL_POINTER = 3
+STATUS_BAD_SCENE = 4
+STATUS_CUDA_ERROR = 16
+STATUS_STACK_OVERFLOW = 17
+STATUS_BAD_FILM = 18
+MAX_TILE_PIXELS = 1 << 22
+
+LIB_PATH = Path(__file__).resolve().parent / "librtg.so"
+_lib: Optional[ctypes.CDLL] = None
+
+_u32, _u64, _f = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
+# The ABI of include/repackshot_b200.h: name -> (restype, argtypes).
+ABI = {
+    "rtg_version": (_u32, []),
+    "rtg_scene_load": (_u32, [ctypes.c_char_p, _u32]),
+    "rtg_scene_error_len": (_u32, []),
+    "rtg_scene_error_copy": (None, [ctypes.c_void_p]),
+    "rtg_scene_free": (_u32, [_u32]),
+    "rtg_render_tile": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _f]),
+    "rtg_render_tile_rgba": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _f]),
+    "rtg_film_create": (_u32, [_u32, _u32, _u32, _u32, _u32]),
+    "rtg_film_free": (_u32, [_u32]),
+    "rtg_film_clear": (_u32, [_u32]),
+    "rtg_render_progressive": (_u32, [_u32, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
+    "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
+    "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
+    "rtg_render_paths": (_u32, [_u32, _f, _u32, _f]),
+    "rtg_trace_rays": (_u32, [_u32, _f, _u32, _u32, _f]),
+    "rtg_scene_stats": (_u32, [_u32, _f]),
+    "rtg_set_path_capacity": (_u32, [_u32, _u32]),
+    "rtg_timing": (_u32, [_u32, _u32, _u32, _f]),
+    "rtg_synchronize": (_u32, [_u32]),
+}
+
+
+class RtgError(RuntimeError):
+    """A non-zero status of the C ABI, with the library's last error message."""
+
+    def __init__(self, status: int, message: str = ""):
+        super().__init__(f"status {status}: {message}" if message else f"status {status}")
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded native library. Raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m repackshot_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in ABI.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def error_message() -> str:
+    """The last error (rt_scene_error_len / rt_scene_error_copy)."""
+    L = lib()
+    n = L.rtg_scene_error_len()
+    buf = ctypes.create_string_buffer(max(n, 1))
+    L.rtg_scene_error_copy(buf)
+    return buf.raw[:n].decode("utf-8", "replace")
+
+
+def _check(status: int):
+    if status != STATUS_OK:
+        raise RtgError(status, error_message() if status in (STATUS_CUDA_ERROR, STATUS_STACK_OVERFLOW) else "")
+
+
+def scene_load(rsb: bytes) -> int:
+    """rt_scene_load: a handle > 0, or 0 with ``error_message()`` set."""
+    return lib().rtg_scene_load(rsb, len(rsb))
+
+
+def scene_free(handle: int) -> int:
+    return lib().rtg_scene_free(handle)
+
+
+def render_tile(handle: int, x: int, y: int, w: int, h: int, sample_index: int, rgba: bool = False):
+    """rt_render_tile(_rgba): (status, w*h*3 or w*h*4 float32 array)."""
+    out = np.zeros(w * h * (4 if rgba else 3), np.float32) if 0 < w * h <= MAX_TILE_PIXELS else np.zeros(0, np.float32)
+    fn = lib().rtg_render_tile_rgba if rgba else lib().rtg_render_tile
+    status = fn(handle, x, y, w, h, sample_index, _ptr(out) if out.size else None)
+    return status, out
+
+
+class Scene:
+    """A loaded scene (owns its handle)."""
+
+    def __init__(self, rsb: bytes):
+        self.handle = scene_load(rsb)
+        if self.handle == 0:
+            raise RtgError(STATUS_BAD_SCENE, error_message())
+        st = np.zeros(8, np.float64)
+        _check(lib().rtg_scene_stats(self.handle, _ptr(st)))
+        self.width, self.height, self.max_depth = int(st[0]), int(st[1]), int(st[2])
+        self.triangles, self.nodes, self.leaf_triangles, self.build_seconds = int(st[3]), int(st[4]), int(st[5]), float(st[6])
+
+    def close(self):
+        if self.handle:
+            scene_free(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render_tile(self, x, y, w, h, sample_index, rgba=False) -> np.ndarray:
+        status, out = render_tile(self.handle, x, y, w, h, sample_index, rgba)
+        _check(status)
+        return out
+
+    def film(self, x=0, y=0, w=None, h=None) -> "Film":
+        return Film(self, x, y, self.width if w is None else w, self.height if h is None else h)
+
+    def render_paths(self, xys: np.ndarray) -> np.ndarray:
+        """Radiance of explicit (x, y, sample) paths: (n, 5) = r, g, b, alpha, 0."""
+        xys = np.ascontiguousarray(xys, dtype=np.uint32).reshape(-1, 3)
+        out = np.zeros((len(xys), 5), np.float32)
+        _check(lib().rtg_render_paths(self.handle, _ptr(xys), len(xys), _ptr(out)))
+        return out
+
+    def trace(self, rays: np.ndarray, camera=False, any_hit=False) -> np.ndarray:
+        """Nearest hits (n, 3) u32 = instance, triangle, t bits; or any-hit flags (n,)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = len(rays)
+        out = np.zeros(n if any_hit else 3 * n, np.uint32)
+        mode = (1 if camera else 0) | (2 if any_hit else 0)
+        _check(lib().rtg_trace_rays(self.handle, _ptr(rays), n, mode, _ptr(out)))
+        return out if any_hit else out.reshape(n, 3)
+
+    def set_path_capacity(self, paths: int):
+        _check(lib().rtg_set_path_capacity(self.handle, paths))
+
+    def timing(self, enable: bool, reset: bool = False):
+        """(extend ms, extend launches, camera+extension rays, shadow rays) since the last reset."""
+        out = np.zeros(4, np.float64)
+        _check(lib().rtg_timing(self.handle, int(enable), int(reset), _ptr(out)))
+        return float(out[0]), int(out[1]), int(out[2]), int(out[3])
+
+    def synchronize(self):
+        _check(lib().rtg_synchronize(self.handle))
+
+
+class Film:
+    """A device film over an image rectangle (rt-core Film): rgb, weight, alpha, lum2 sums."""
+
+    def __init__(self, scene: Scene, x: int, y: int, w: int, h: int):
+        self.scene, self.x, self.y, self.w, self.h = scene, x, y, w, h
+        self.handle = lib().rtg_film_create(scene.handle, x, y, w, h)
+        if self.handle == 0:
+            raise RtgError(STATUS_BAD_FILM, error_message())
+
+    def render(self, first: int, count: int) -> int:
+        """Accumulates samples [first, first + count); returns the rays cast."""
+        rays = _u64(0)
+        _check(lib().rtg_render_progressive(self.scene.handle, self.handle, first, count, ctypes.byref(rays)))
+        return int(rays.value)
+
+    def read(self, out=None):
+        """(rgb (h, w, 3), weight, alpha, lum2 (h, w)) copied to host."""
+        n = self.w * self.h
+        if out is None:
+            out = (np.zeros(3 * n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32))
+        _check(lib().rtg_film_read(self.handle, *[_ptr(a) for a in out]))
+        rgb, w, a, l2 = out
+        return rgb.reshape(self.h, self.w, 3), w.reshape(self.h, self.w), a.reshape(self.h, self.w), l2.reshape(self.h, self.w)
+
+    def resolve(self) -> np.ndarray:
+        """Film::resolve (image.rs:158): rgb * (1 / weight), black where no sample."""
+        rgb, w, _, _ = self.read()
+        inv = np.where(w > 0, np.float32(1.0) / np.where(w > 0, w, np.float32(1.0)), np.float32(0.0)).astype(np.float32)
+        return (rgb * inv[..., None]).astype(np.float32)
+
+    def clear(self):
+        _check(lib().rtg_film_clear(self.handle))
+
+    def close(self):
+        if self.handle:
+            lib().rtg_film_free(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def fnv1a(values: np.ndarray) -> int:
+    """FNV-1a over the little-endian bytes of float32 values (the reference's film hash)."""
+    b = np.ascontiguousarray(values, dtype="<f4").view(np.uint8)
+    h = 0x811C9DC5
+    for byte in b.tobytes():
+        h = ((h ^ byte) * 0x01000193) & 0xFFFFFFFF
+    return h

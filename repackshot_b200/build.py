@@ -1,0 +1,97 @@
+"""Build recipe of the native library: the energy-table generator, the sm_100a kernels and the
+C-ABI engine, linked into ``repackshot_b200/librtg.so`` (CUDA runtime linked statically, so the
+library carries no dependency on a Python package).
+
+Device code is compiled with ``-fmad=false -prec-div=true -prec-sqrt=true -ftz=false`` and host
+code with ``-ffp-contract=off``: every floating-point operation is one IEEE round-to-nearest
+step, as the Repackshot engine's arithmetic is.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+GEN = CSRC / "_gen"
+OBJ = PKG / "_build"
+LIB = PKG / "librtg.so"
+
+NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+CUDA_HOME = Path(NVCC).resolve().parent.parent
+CXX = os.environ.get("CXX", "g++")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+DEVICE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+                "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v"]
+HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-pthread", f"-I{CUDA_HOME}/include"]
+
+HOST_SOURCES = ["rtg_scene.cpp", "rtg_tables.cpp", "rtg_energy.cpp", "rtg_engine.cpp"]
+DEVICE_SOURCES = ["rtg_kernels.cu"]
+
+
+def _run(cmd, log=None):
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if log is not None:
+        log.write(" ".join(map(str, cmd)) + "\n" + res.stdout + res.stderr + "\n")
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(map(str, cmd))}")
+    return res
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Builds ``librtg.so`` if any source is newer; returns its path."""
+    GEN.mkdir(exist_ok=True)
+    OBJ.mkdir(exist_ok=True)
+    headers = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "repackshot_b200.h"]
+    log = open(OBJ / "build.log", "w")
+    # 1. energy tables (generated, then compiled in)
+    gen_exe = OBJ / "rtg_energy_gen"
+    inc = GEN / "rtg_energy_tables.inc"
+    gen_deps = [CSRC / "rtg_energy_gen.cpp"] + headers
+    if force or _stale(gen_exe, gen_deps):
+        _run([CXX, *HOST_FLAGS, "-O2", str(CSRC / "rtg_energy_gen.cpp"), "-o", str(gen_exe)], log)
+    if force or _stale(inc, [gen_exe]):
+        _run([str(gen_exe), str(inc)], log)
+    objs = []
+    for src in HOST_SOURCES:
+        o = OBJ / (src + ".o")
+        deps = [CSRC / src, inc] + headers
+        if force or _stale(o, deps):
+            _run([CXX, *HOST_FLAGS, "-c", str(CSRC / src), "-o", str(o)], log)
+        objs.append(o)
+    for src in DEVICE_SOURCES:
+        o = OBJ / (src + ".o")
+        deps = [CSRC / src] + headers
+        if force or _stale(o, deps):
+            _run([NVCC, *ARCH, *DEVICE_FLAGS, "-c", str(CSRC / src), "-o", str(o)], log)
+        objs.append(o)
+    if force or _stale(LIB, objs):
+        _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), *map(str, objs), "-lpthread"], log)
+    log.close()
+    if verbose:
+        sys.stdout.write((OBJ / "build.log").read_text())
+    return LIB
+
+
+def build_oracle() -> Path | None:
+    """Builds the oracle library (test infrastructure) with its Makefile; None without make."""
+    oracle = PKG.parent / "oracle"
+    if not (oracle / "Makefile").exists() or shutil.which("make") is None:
+        return None
+    _run(["make", "-s", "-C", str(oracle)])
+    return oracle / "_build" / "liborc.so"
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

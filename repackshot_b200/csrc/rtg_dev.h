@@ -1,0 +1,108 @@
+// Data layout in device memory shared by the host upload (rtg_scene.cpp) and the kernels
+// (rtg_kernels.cu). Everything here is plain data: no torch types, no host pointers.
+#pragma once
+#include <vector_types.h>
+
+#include <cstdint>
+
+#include "rtg_bsdf.cuh"
+
+namespace rtg {
+
+constexpr uint32_t NODE_EMPTY = 0xffffffffu;
+constexpr uint32_t NODE_LEAF = 1u << 31;
+// Leaf reference: NODE_LEAF | first << 4 | (count - 1), count in 1..16.
+RTG_HD uint32_t make_leaf(uint32_t first, uint32_t count) { return NODE_LEAF | (first << 4) | (count - 1); }
+
+// An 8-wide BVH node with child boxes quantised to 8 bits per plane (96 bytes, six 16-byte
+// loads). A child box decodes as p + q * 2^e per axis; the builder checks that every decoded box
+// (computed with the same IEEE operations as the kernels) contains the child's exact box, so the
+// slab test is conservative and the nearest hit stays the one brute force finds.
+struct alignas(16) QNode {
+    float px, py, pz;
+    uint8_t ex, ey, ez;   // biased exponents of the per-axis scales 2^(e-127)
+    uint8_t nchild;
+    uint8_t qlo[3][8];
+    uint8_t qhi[3][8];
+    uint32_t child[8];    // inner node index, leaf reference or NODE_EMPTY
+};
+static_assert(sizeof(QNode) == 96, "QNode must be 96 bytes");
+
+// A leaf triangle (48 bytes): corners in its BLAS's space; w lanes carry the triangle's index in
+// its mesh, its instance (0xffffffff: the BLAS instance's) and flags (bit 0 one-sided, bit 1
+// hidden to camera rays).
+struct alignas(16) TriRec {
+    float v0[3]; uint32_t tri;
+    float v1[3]; uint32_t inst;
+    float v2[3]; uint32_t flags;
+};
+
+// A TLAS leaf: one bottom-level tree placed in the world.
+struct alignas(16) BlasInst {
+    float to_local[12];   // world -> object rows (unused when identity)
+    uint32_t root;        // node index or leaf reference of the BLAS
+    uint32_t identity;    // the BLAS is in world space
+    uint32_t instance;    // instance id for BLAS records that carry 0xffffffff
+    uint32_t flags;       // bit 0 one-sided, bit 1 hidden to camera rays
+};
+
+// Per instance, what hit details and shading read.
+struct alignas(16) DevInstance {
+    float to_local[12];
+    float to_world[12];
+    uint32_t identity, active, material, mesh;
+    uint32_t flags, inside_out, has_normals, tri_base;  // tri_base: first global triangle of its mesh
+    uint32_t tangent_on, pad0, pad1, pad2;
+    float tan_centre[3], tan_axis[3], tan_x[3];
+    float pad3[3];
+};
+
+struct AreaLightDev {
+    float centre[3];
+    float fx[3], fy[3], fz[3];
+    float half_x, half_y, radius, area;
+    float radiance[3];
+    float exponent, base, bound;
+    uint32_t rect, glossy, camera, shadow, entry, pad;
+};
+constexpr int MAX_ENTRIES = 64;
+constexpr int MAX_AREAS = 63;
+
+struct LightsDev {
+    int n_areas, n_entries, per_point, env_is_entry;
+    uint32_t env_entry, pad0, pad1, pad2;
+    float env_floor, env_horizon, env_zenith, env_lower, env_total, env_base;
+    int entries[MAX_ENTRIES];  // >= 0 area index, -1 environment
+    float cdf[MAX_ENTRIES];
+    float flux_pmf[MAX_ENTRIES];
+    AreaLightDev areas[MAX_AREAS];
+};
+
+// Everything a launch needs besides the per-path buffers (constant memory).
+struct SceneDev {
+    // camera (basis precomputed on the host with the reference's operations)
+    float cam_pos[3], cam_fwd[3], cam_right[3], cam_up[3];
+    float focal_mm, sensor_mm, focus_dist, lens_radius, ortho_width, exterior;
+    uint32_t ortho;
+    // render settings
+    uint32_t width, height, seed, max_depth, pixel_filter;
+    float clamp_indirect;
+    uint32_t background;  // 0 environment, 1 colour, 2 transparent
+    float background_color[3];
+    uint32_t floor_mode;
+    float floor_z;
+    float floor_color[3];
+    // geometry
+    const QNode* nodes;
+    const TriRec* tris;
+    const BlasInst* blas;
+    const DevInstance* instances;
+    const float4* positions;  // xyz per vertex (global)
+    const float4* normals;    // xyz per vertex (global)
+    const uint4* tri_index;   // global vertex indices per global triangle
+    const DevMaterial* materials;
+    uint32_t tlas_root, n_instances, n_materials, stack_need;
+    EnergyTables energy;
+};
+
+}  // namespace rtg

@@ -1,0 +1,532 @@
+// The C-ABI drop-in: scene registry, device memory, tile and progressive renders, films, and the
+// parity entry points. Mirrors the hand-written ABI of the reference's rt-wasm
+// (engine/crates/rt-wasm/src/ffi.rs:28-197, rt-wasm/src/lib.rs:37-164, 562-730).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/repackshot_b200.h"
+#include "rtg_kernels.h"
+#include "rtg_scene.h"
+#include "rtg_tables.h"
+
+namespace rtg {
+namespace {
+
+#define RTG_CHECK(call)                                                          \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) { cuda_fail(e_, #call); return RTG_STATUS_CUDA_ERROR; } \
+    } while (0)
+
+std::mutex g_mu;  // every entry point holds it: calls serialise, as the reference's registry does
+std::string g_error;
+bool g_device_ready = false;
+void* g_energy_dev = nullptr;
+EnergyTables g_energy{};
+int g_sms = 148;
+
+void cuda_fail(cudaError_t e, const char* what) {
+    g_error = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ") in " + what;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+};
+
+struct Scene {
+    SceneDev S{};
+    LightsDev* d_lights = nullptr;
+    std::vector<DevBuf> bufs;
+    cudaStream_t stream = nullptr;
+    // path buffers
+    PathBuffers P{};
+    DevBuf path_mem;
+    uint32_t capacity = 0;
+    uint32_t max_capacity = 1u << 22;
+    // statistics
+    uint64_t rays = 0;
+    double build_seconds = 0;
+    uint64_t nodes = 0, tris = 0, instanced_triangles = 0;
+    uint32_t width = 0, height = 0, max_depth = 0;
+    // extend-kernel timing
+    bool timing = false;
+    WaveTiming* wt = nullptr;
+    double extend_ms = 0;
+    uint64_t extend_launches = 0;
+    uint64_t extend_rays = 0, shadow_rays = 0;
+    ~Scene() {
+        for (auto& b : bufs) b.release();
+        path_mem.release();
+        if (d_lights) cudaFree(d_lights);
+        if (wt) {
+            for (int i = 0; i < WaveTiming::MAX_EVENTS; ++i) cudaEventDestroy(wt->ev[i]);
+            delete wt;
+        }
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+struct Film {
+    uint32_t scene;
+    FilmDev dev{};
+    DevBuf mem;
+    ~Film() { mem.release(); }
+};
+std::vector<std::unique_ptr<Scene>> g_scenes;
+std::vector<std::unique_ptr<Film>> g_films;
+
+Scene* scene_of(uint32_t h) { return (h == 0 || h > g_scenes.size()) ? nullptr : g_scenes[h - 1].get(); }
+Film* film_of(uint32_t h) { return (h == 0 || h > g_films.size()) ? nullptr : g_films[h - 1].get(); }
+
+uint32_t device_init() {
+    if (g_device_ready) return RTG_STATUS_OK;
+    int dev = 0;
+    RTG_CHECK(cudaGetDevice(&dev));
+    RTG_CHECK(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
+    SobolTable sob;
+    build_sobol_table(sob);
+    RTG_CHECK(cudaDeviceSynchronize());
+    set_sobol(sob, 0);
+    RTG_CHECK(cudaGetLastError());
+    const EnergyData& E = energy_data();
+    size_t n16 = E.albedo.size() + E.schlick.size() + E.clear_in.size() + E.clear_out.size();
+    size_t bytes = n16 * 2 + 64 * 4;
+    RTG_CHECK(cudaMalloc(&g_energy_dev, bytes));
+    std::vector<uint8_t> host(bytes);
+    uint8_t* p = host.data();
+    auto put = [&](const void* src, size_t n) { std::memcpy(p, src, n); p += n; };
+    put(E.albedo.data(), E.albedo.size() * 2);
+    put(E.schlick.data(), E.schlick.size() * 2);
+    put(E.clear_in.data(), E.clear_in.size() * 2);
+    put(E.clear_out.data(), E.clear_out.size() * 2);
+    put(E.albedo_avg.data(), 32 * 4);
+    put(E.schlick_avg.data(), 32 * 4);
+    RTG_CHECK(cudaMemcpy(g_energy_dev, host.data(), bytes, cudaMemcpyHostToDevice));
+    const uint8_t* d = (const uint8_t*)g_energy_dev;
+    g_energy.albedo = (const uint16_t*)d;
+    g_energy.schlick = g_energy.albedo + E.albedo.size();
+    g_energy.clear_in = g_energy.schlick + E.schlick.size();
+    g_energy.clear_out = g_energy.clear_in + E.clear_in.size();
+    g_energy.albedo_avg = (const float*)(g_energy.clear_out + E.clear_out.size());
+    g_energy.schlick_avg = g_energy.albedo_avg + 32;
+    RTG_CHECK(cudaDeviceSynchronize());
+    g_device_ready = true;
+    return RTG_STATUS_OK;
+}
+
+template <class T>
+uint32_t upload(Scene& sc, const std::vector<T>& v, const T*& out) {
+    DevBuf b;
+    b.bytes = v.size() * sizeof(T);
+    if (b.bytes == 0) { out = nullptr; return RTG_STATUS_OK; }
+    RTG_CHECK(cudaMalloc(&b.p, b.bytes));
+    sc.bufs.push_back(b);
+    RTG_CHECK(cudaMemcpy(b.p, v.data(), b.bytes, cudaMemcpyHostToDevice));
+    out = (const T*)b.p;
+    return RTG_STATUS_OK;
+}
+
+uint32_t ensure_capacity(Scene& sc, uint32_t paths) {
+    if (paths <= sc.capacity) return RTG_STATUS_OK;
+    sc.path_mem.release();
+    size_t n = paths;
+    size_t bytes = n * (16 * 5 + 4 + 4 + 16 + 4 * 2 + 16 * 3) + 14 * 256 + 256;
+    RTG_CHECK(cudaMalloc(&sc.path_mem.p, bytes));
+    sc.path_mem.bytes = bytes;
+    uint8_t* p = (uint8_t*)sc.path_mem.p;
+    auto take = [&](size_t each) { uint8_t* r = p; p += ((n * each + 255) / 256) * 256; return r; };
+    // (sizes rounded to 256 bytes; `bytes` above leaves room for the rounding of 14 arrays)
+    sc.P.o = (float4*)take(16);
+    sc.P.d = (float4*)take(16);
+    sc.P.thr = (float4*)take(16);
+    sc.P.sum = (float4*)take(16);
+    sc.P.sel = (float4*)take(16);
+    sc.P.flags = (uint32_t*)take(4);
+    sc.P.medium = (uint32_t*)take(4);
+    sc.P.hit = (uint4*)take(16);
+    sc.P.queue[0] = (uint32_t*)take(4);
+    sc.P.queue[1] = (uint32_t*)take(4);
+    sc.P.sh_o = (float4*)take(16);
+    sc.P.sh_d = (float4*)take(16);
+    sc.P.sh_c = (float4*)take(16);
+    sc.P.counters = (uint32_t*)p;
+    p += 64;
+    sc.P.rays = (unsigned long long*)p;
+    p += 64;
+    if ((size_t)(p - (uint8_t*)sc.path_mem.p) > bytes) { g_error = "internal: path buffer layout"; return RTG_STATUS_CUDA_ERROR; }
+    sc.capacity = paths;
+    return RTG_STATUS_OK;
+}
+
+int grid_for(uint32_t n, int per_block) {
+    long g = ((long)n + per_block - 1) / per_block;
+    long cap = (long)g_sms * 16;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+// Runs one wave and (when timing) adds the extend-kernel time.
+uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film) {
+    WaveTiming* t = nullptr;
+    if (sc.timing) {
+        if (!sc.wt) {
+            sc.wt = new WaveTiming();
+            for (int i = 0; i < WaveTiming::MAX_EVENTS; ++i) RTG_CHECK(cudaEventCreate(&sc.wt->ev[i]));
+        }
+        sc.wt->ev_count = 0;
+        t = sc.wt;
+    }
+    launch_wave(sc.S, sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t);
+    RTG_CHECK(cudaGetLastError());
+    if (t) {
+        RTG_CHECK(cudaStreamSynchronize(sc.stream));
+        for (int i = 0; i + 1 < t->ev_count; i += 2) {
+            float ms = 0;
+            RTG_CHECK(cudaEventElapsedTime(&ms, t->ev[i], t->ev[i + 1]));
+            sc.extend_ms += ms;
+            sc.extend_launches += 1;
+        }
+    }
+    return RTG_STATUS_OK;
+}
+
+uint32_t finish(Scene& sc, uint64_t* rays_out) {
+    uint32_t counters[4];
+    unsigned long long rays[2] = {0, 0};
+    RTG_CHECK(cudaMemcpyAsync(counters, sc.P.counters, 16, cudaMemcpyDeviceToHost, sc.stream));
+    RTG_CHECK(cudaMemcpyAsync(rays, sc.P.rays, 16, cudaMemcpyDeviceToHost, sc.stream));
+    RTG_CHECK(cudaStreamSynchronize(sc.stream));
+    if (counters[3] & 1u) { g_error = "traversal stack overflow"; return RTG_STATUS_STACK_OVERFLOW; }
+    if (rays_out) *rays_out = rays[0] + rays[1];
+    sc.rays += rays[0] + rays[1];
+    sc.extend_rays += rays[0];
+    sc.shadow_rays += rays[1];
+    return RTG_STATUS_OK;
+}
+
+// Renders samples [first, first + count) of the image rectangle (x, y, w, h) (clipped to the
+// image) into `film`, every pixel's samples added in index order.
+uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t first, uint32_t count, const FilmDev& film,
+                       uint64_t* rays_out) {
+    uint64_t x_end = std::min<uint64_t>((uint64_t)x + w, sc.width), y_end = std::min<uint64_t>((uint64_t)y + h, sc.height);
+    if (rays_out) *rays_out = 0;
+    if (x >= x_end || y >= y_end || count == 0) return RTG_STATUS_OK;
+    uint32_t cw = (uint32_t)(x_end - x), ch = (uint32_t)(y_end - y);
+    uint64_t npix = (uint64_t)cw * ch;
+    // Rows per band so that one band of one sample fits the path capacity.
+    uint32_t band_rows = ch;
+    if (npix > sc.max_capacity) band_rows = std::max<uint32_t>(1, (uint32_t)(sc.max_capacity / cw));
+    uint64_t total_rays = 0;
+    for (uint32_t by = 0; by < ch; by += band_rows) {
+        uint32_t bh = std::min(band_rows, ch - by);
+        uint64_t bpix = (uint64_t)cw * bh;
+        uint32_t per_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(count, sc.max_capacity / bpix));
+        uint32_t need = (uint32_t)(bpix * per_wave);
+        uint32_t st = ensure_capacity(sc, need);
+        if (st) return st;
+        RTG_CHECK(cudaMemsetAsync(sc.P.counters, 0, 16, sc.stream));
+        RTG_CHECK(cudaMemsetAsync(sc.P.rays, 0, 16, sc.stream));
+        for (uint32_t s = 0; s < count; s += per_wave) {
+            uint32_t ns = std::min(per_wave, count - s);
+            WaveDesc wd{x, y + by, cw, bh, first + s, (uint32_t)(bpix * ns), nullptr};
+            st = run_wave(sc, wd, &film);
+            if (st) return st;
+        }
+        uint64_t r = 0;
+        st = finish(sc, &r);
+        if (st) return st;
+        total_rays += r;
+    }
+    if (rays_out) *rays_out = total_rays;
+    return RTG_STATUS_OK;
+}
+
+uint32_t make_film(uint32_t ox, uint32_t oy, uint32_t w, uint32_t h, Film& f) {
+    size_t n = (size_t)w * h;
+    f.mem.bytes = n * 6 * 4;
+    RTG_CHECK(cudaMalloc(&f.mem.p, f.mem.bytes));
+    RTG_CHECK(cudaMemset(f.mem.p, 0, f.mem.bytes));
+    float* p = (float*)f.mem.p;
+    f.dev = FilmDev{ox, oy, w, h, p, p + 3 * n, p + 4 * n, p + 5 * n};
+    return RTG_STATUS_OK;
+}
+
+uint32_t render_tile_impl(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample, float* out, bool rgba) {
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    uint64_t px = (uint64_t)w * h;
+    if (px == 0 || px > RTG_MAX_TILE_PIXELS) return RTG_STATUS_BAD_TILE;
+    if (!out) return RTG_STATUS_NULL_POINTER;
+    Film f;
+    f.scene = handle;
+    uint32_t st = make_film(x, y, w, h, f);
+    if (st) return st;
+    st = render_region(*sc, x, y, w, h, sample, 1, f.dev, nullptr);
+    if (st) return st;
+    std::vector<float> buf(px * 6);
+    RTG_CHECK(cudaMemcpyAsync(buf.data(), f.mem.p, px * 6 * 4, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    const float* rgb = buf.data();
+    const float* wt = rgb + 3 * px;
+    const float* al = rgb + 4 * px;
+    for (uint64_t i = 0; i < px; ++i) {
+        float inv = wt[i] > 0.0f ? 1.0f / wt[i] : 0.0f;
+        size_t o = rgba ? 4 * i : 3 * i;
+        for (int c = 0; c < 3; ++c) out[o + c] = wt[i] > 0.0f ? rgb[3 * i + c] * inv : 0.0f;
+        if (rgba) out[o + 3] = wt[i] > 0.0f ? al[i] * inv : 0.0f;
+    }
+    return RTG_STATUS_OK;
+}
+
+}  // namespace
+}  // namespace rtg
+
+using namespace rtg;
+
+extern "C" {
+
+uint32_t rtg_version(void) { return RTG_ABI_VERSION; }
+
+uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!bytes) { g_error = "null pointer"; return 0; }
+    if (device_init() != RTG_STATUS_OK) return 0;
+    HScene hs;
+    std::string err;
+    if (!parse_rsb(bytes, len, hs, err)) { g_error = err; return 0; }
+    Flat F;
+    if (!flatten_scene(hs, F, err)) { g_error = err; return 0; }
+    auto sc = std::make_unique<Scene>();
+    if (cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking) != cudaSuccess) { g_error = "cudaStreamCreate failed"; return 0; }
+    sc->S = F.scene;
+    std::vector<float4> pos(F.positions.size() / 4), nrm(F.normals.size() / 4);
+    std::memcpy(pos.data(), F.positions.data(), F.positions.size() * 4);
+    std::memcpy(nrm.data(), F.normals.data(), F.normals.size() * 4);
+    std::vector<uint4> ti(F.tri_index.size() / 4);
+    std::memcpy(ti.data(), F.tri_index.data(), F.tri_index.size() * 4);
+    if (upload(*sc, F.nodes, sc->S.nodes) || upload(*sc, F.tris, sc->S.tris) || upload(*sc, F.blas, sc->S.blas) ||
+        upload(*sc, F.instances, sc->S.instances) || upload(*sc, pos, sc->S.positions) || upload(*sc, nrm, sc->S.normals) ||
+        upload(*sc, ti, sc->S.tri_index) || upload(*sc, F.materials, sc->S.materials))
+        return 0;
+    if (cudaMalloc(&sc->d_lights, sizeof(LightsDev)) != cudaSuccess ||
+        cudaMemcpy(sc->d_lights, &F.lights, sizeof(LightsDev), cudaMemcpyHostToDevice) != cudaSuccess) {
+        g_error = "CUDA error uploading lights";
+        return 0;
+    }
+    sc->S.energy = g_energy;
+    sc->build_seconds = F.build_seconds;
+    sc->nodes = F.nodes.size();
+    sc->tris = F.tris.size();
+    sc->instanced_triangles = F.instanced_triangles;
+    sc->width = F.scene.width;
+    sc->height = F.scene.height;
+    sc->max_depth = F.scene.max_depth;
+    g_error.clear();
+    for (size_t i = 0; i < g_scenes.size(); ++i)
+        if (!g_scenes[i]) { g_scenes[i] = std::move(sc); return (uint32_t)i + 1; }
+    g_scenes.push_back(std::move(sc));
+    return (uint32_t)g_scenes.size();
+}
+
+uint32_t rtg_scene_error_len(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return (uint32_t)g_error.size();
+}
+void rtg_scene_error_copy(uint8_t* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (out) std::memcpy(out, g_error.data(), g_error.size());
+}
+
+uint32_t rtg_scene_free(uint32_t handle) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!scene_of(handle)) return RTG_STATUS_BAD_HANDLE;
+    cudaStreamSynchronize(g_scenes[handle - 1]->stream);
+    g_scenes[handle - 1].reset();
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_render_tile(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index, float* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return render_tile_impl(handle, x, y, w, h, sample_index, out, false);
+}
+uint32_t rtg_render_tile_rgba(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index, float* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return render_tile_impl(handle, x, y, w, h, sample_index, out, true);
+}
+
+uint32_t rtg_film_create(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!scene_of(handle)) { g_error = "bad scene handle"; return 0; }
+    if ((uint64_t)w * h == 0 || (uint64_t)w * h > (1ull << 28)) { g_error = "bad film size"; return 0; }
+    auto f = std::make_unique<Film>();
+    f->scene = handle;
+    if (make_film(x, y, w, h, *f) != RTG_STATUS_OK) return 0;
+    for (size_t i = 0; i < g_films.size(); ++i)
+        if (!g_films[i]) { g_films[i] = std::move(f); return (uint32_t)i + 1; }
+    g_films.push_back(std::move(f));
+    return (uint32_t)g_films.size();
+}
+uint32_t rtg_film_free(uint32_t film) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!film_of(film)) return RTG_STATUS_BAD_FILM;
+    cudaDeviceSynchronize();
+    g_films[film - 1].reset();
+    return RTG_STATUS_OK;
+}
+uint32_t rtg_film_clear(uint32_t film) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Film* f = film_of(film);
+    if (!f) return RTG_STATUS_BAD_FILM;
+    Scene* sc = scene_of(f->scene);
+    RTG_CHECK(cudaMemsetAsync(f->mem.p, 0, f->mem.bytes, sc ? sc->stream : 0));
+    if (sc) RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    return RTG_STATUS_OK;
+}
+uint32_t rtg_render_progressive(uint32_t handle, uint32_t film, uint32_t first_sample, uint32_t count, uint64_t* rays) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    Film* f = film_of(film);
+    if (!f || f->scene != handle) return RTG_STATUS_BAD_FILM;
+    return render_region(*sc, f->dev.ox, f->dev.oy, f->dev.w, f->dev.h, first_sample, count, f->dev, rays);
+}
+uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Film* f = film_of(film);
+    if (!f) return RTG_STATUS_BAD_FILM;
+    Scene* sc = scene_of(f->scene);
+    cudaStream_t s = sc ? sc->stream : 0;
+    size_t n = (size_t)f->dev.w * f->dev.h;
+    if (rgb) RTG_CHECK(cudaMemcpyAsync(rgb, f->dev.rgb, n * 12, cudaMemcpyDeviceToHost, s));
+    if (weight) RTG_CHECK(cudaMemcpyAsync(weight, f->dev.weight, n * 4, cudaMemcpyDeviceToHost, s));
+    if (alpha) RTG_CHECK(cudaMemcpyAsync(alpha, f->dev.alpha, n * 4, cudaMemcpyDeviceToHost, s));
+    if (lum2) RTG_CHECK(cudaMemcpyAsync(lum2, f->dev.lum2, n * 4, cudaMemcpyDeviceToHost, s));
+    RTG_CHECK(cudaStreamSynchronize(s));
+    return RTG_STATUS_OK;
+}
+uint32_t rtg_film_device(uint32_t film, float** rgb, float** weight, float** alpha, float** lum2) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Film* f = film_of(film);
+    if (!f) return RTG_STATUS_BAD_FILM;
+    if (rgb) *rgb = f->dev.rgb;
+    if (weight) *weight = f->dev.weight;
+    if (alpha) *alpha = f->dev.alpha;
+    if (lum2) *lum2 = f->dev.lum2;
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_render_paths(uint32_t handle, const uint32_t* xys, uint32_t n, float* out5) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (!xys || !out5) return RTG_STATUS_NULL_POINTER;
+    if (n == 0) return RTG_STATUS_OK;
+    uint32_t st = ensure_capacity(*sc, n);
+    if (st) return st;
+    uint32_t* d_xys = nullptr;
+    RTG_CHECK(cudaMalloc(&d_xys, (size_t)n * 12));
+    std::unique_ptr<uint32_t, void (*)(uint32_t*)> guard(d_xys, [](uint32_t* p) { cudaFree(p); });
+    RTG_CHECK(cudaMemcpyAsync(d_xys, xys, (size_t)n * 12, cudaMemcpyHostToDevice, sc->stream));
+    RTG_CHECK(cudaMemsetAsync(sc->P.counters, 0, 16, sc->stream));
+    RTG_CHECK(cudaMemsetAsync(sc->P.rays, 0, 16, sc->stream));
+    WaveDesc wd{0, 0, 1, 1, 0, n, d_xys};
+    st = run_wave(*sc, wd, nullptr);
+    if (st) return st;
+    std::vector<float4> sum(n), thr(n);
+    RTG_CHECK(cudaMemcpyAsync(sum.data(), sc->P.sum, (size_t)n * 16, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaMemcpyAsync(thr.data(), sc->P.thr, (size_t)n * 16, cudaMemcpyDeviceToHost, sc->stream));
+    st = finish(*sc, nullptr);
+    if (st) return st;
+    for (uint32_t i = 0; i < n; ++i) {
+        out5[5 * i] = sum[i].x;
+        out5[5 * i + 1] = sum[i].y;
+        out5[5 * i + 2] = sum[i].z;
+        out5[5 * i + 3] = thr[i].w;
+        out5[5 * i + 4] = 0.0f;
+    }
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_trace_rays(uint32_t handle, const float* rays, uint32_t n, uint32_t mode, uint32_t* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (!rays || !out) return RTG_STATUS_NULL_POINTER;
+    if (n == 0) return RTG_STATUS_OK;
+    uint32_t st = ensure_capacity(*sc, 1024);
+    if (st) return st;
+    size_t words = (mode & 2u) ? n : (size_t)n * 3;
+    void* mem = nullptr;
+    RTG_CHECK(cudaMalloc(&mem, (size_t)n * 32 + words * 4));
+    std::unique_ptr<void, void (*)(void*)> guard(mem, [](void* p) { cudaFree(p); });
+    float* d_rays = (float*)mem;
+    uint32_t* d_out = (uint32_t*)((uint8_t*)mem + (size_t)n * 32);
+    RTG_CHECK(cudaMemcpyAsync(d_rays, rays, (size_t)n * 32, cudaMemcpyHostToDevice, sc->stream));
+    RTG_CHECK(cudaMemsetAsync(sc->P.counters, 0, 16, sc->stream));
+    launch_trace_batch(sc->S, d_rays, n, mode, d_out, sc->P.counters, sc->stream, grid_for(n, 128));
+    RTG_CHECK(cudaGetLastError());
+    RTG_CHECK(cudaMemcpyAsync(out, d_out, words * 4, cudaMemcpyDeviceToHost, sc->stream));
+    uint32_t counters[4];
+    RTG_CHECK(cudaMemcpyAsync(counters, sc->P.counters, 16, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    if (counters[3] & 1u) { g_error = "traversal stack overflow"; return RTG_STATUS_STACK_OVERFLOW; }
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_scene_stats(uint32_t handle, double* out8) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (!out8) return RTG_STATUS_NULL_POINTER;
+    out8[0] = (double)sc->width;
+    out8[1] = (double)sc->height;
+    out8[2] = (double)sc->max_depth;
+    out8[3] = (double)sc->instanced_triangles;
+    out8[4] = (double)sc->nodes;
+    out8[5] = (double)sc->tris;
+    out8[6] = sc->build_seconds;
+    out8[7] = (double)sc->rays;
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_set_path_capacity(uint32_t handle, uint32_t paths) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (paths < 1024) paths = 1024;
+    sc->max_capacity = paths;
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_timing(uint32_t handle, uint32_t enable, uint32_t reset, double* out3) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (out3) {
+        out3[0] = sc->extend_ms;
+        out3[1] = (double)sc->extend_launches;
+        out3[2] = (double)sc->extend_rays;
+        out3[3] = (double)sc->shadow_rays;
+    }
+    if (reset) { sc->extend_ms = 0; sc->extend_launches = 0; sc->extend_rays = 0; sc->shadow_rays = 0; }
+    sc->timing = enable != 0;
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_synchronize(uint32_t handle) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    return RTG_STATUS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,56 @@
+// Launch interface of the wavefront kernels (rtg_kernels.cu), used by the C-ABI engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "rtg_dev.h"
+
+namespace rtg {
+
+// A wave of path slots: either the pixels of the rectangle (x0, y0, w, h) for the sample
+// indices first .. first + n / (w h) - 1 (slot = s * w * h + row-major pixel), or, when `xys` is
+// set, the explicit (x, y, sample index) triples of a device array.
+struct WaveDesc {
+    uint32_t x0, y0, w, h, first, n;
+    const uint32_t* xys;
+};
+
+// Structure-of-arrays path state of one wave (device pointers).
+struct PathBuffers {
+    float4* o;       // origin, w: distance since the last scattering vertex (straight events)
+    float4* d;       // direction, w: density of the BSDF sample that produced it
+    float4* thr;     // throughput, w: alpha
+    float4* sum;     // radiance
+    float4* sel;     // point of the light selection the MIS weights use
+    uint32_t* flags;
+    uint32_t* medium;
+    uint4* hit;
+    uint32_t* queue[2];
+    float4* sh_o;    // shadow rays: origin, w: t_max
+    float4* sh_d;
+    float4* sh_c;    // contribution, w: slot
+    uint32_t* counters;  // [0], [1] queue lengths, [2] shadow queue length, [3] error bits
+    unsigned long long* rays;
+};
+
+struct FilmDev {
+    uint32_t ox, oy, w, h;
+    float* rgb;
+    float* weight;
+    float* alpha;
+    float* lum2;
+};
+
+// CUDA events bracketing every extend launch of a wave (optional).
+struct WaveTiming {
+    static constexpr int MAX_EVENTS = 512;
+    cudaEvent_t ev[MAX_EVENTS];
+    int ev_count = 0;
+};
+
+void set_sobol(const SobolTable& t, cudaStream_t s);
+void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const FilmDev* film, cudaStream_t st,
+                 int grid, WaveTiming* timing);
+void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,
+                        cudaStream_t st, int grid);
+
+}  // namespace rtg

@@ -1,0 +1,89 @@
+// Host-side scene assembly of the drop-in: the RSB subset reader, the reference's binned-SAH
+// BVH builder (engine/crates/rt-core/src/geometry/bvh.rs:195-505) and its flattening into the
+// quantised 8-wide layout of rtg_dev.h, and the light preparation of Lights::new
+// (engine/crates/rt-core/src/light.rs:673-995).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "rtg_dev.h"
+
+namespace rtg {
+
+struct HMaterial {
+    uint32_t kind = 0;
+    float base[3] = {0.8f, 0.8f, 0.8f};
+    float metallic = 0, roughness = 0.5f, ior = 1.5f, transmission = 0, coat = 0, coat_roughness = 0;
+    float emission[3] = {0, 0, 0};
+    float emission_power = 0;
+    uint32_t flags = 0;
+    float opacity = 1, anisotropy = 0, absorption_mm = 0, bevel_mm = 0, scatter_mm = 0;
+    float scatter_color[3] = {1, 1, 1};
+    float scatter_g = 0, abbe = 0;
+};
+struct HLight {
+    uint32_t kind = 0;
+    V3 position{0, 0, 0}, direction{0, 0, -1}, up{0, 1, 0};
+    float size_x = 0, size_y = 0;
+    float color[3] = {1, 1, 1};
+    float power = 0, spread_deg = 180, angle_deg = 0;
+    uint32_t flags = 0;
+};
+struct HMesh {
+    std::vector<V3> positions, normals;  // normals empty: none
+    std::vector<uint32_t> indices;
+    uint32_t material_id = 0;
+    V3 bmin{0, 0, 0}, bmax{0, 0, 0};
+    bool empty_bounds = true, inside_out = false;
+    size_t triangles() const { return indices.size() / 3; }
+};
+struct HInstance {
+    uint32_t mesh = 0;
+    float rows[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+    uint32_t material_id = 0, flags = 0;
+};
+struct HScene {
+    V3 cam_position{0, -1000, 0}, cam_target{0, 0, 0}, cam_up{0, 0, 1};
+    float focal_mm = 50, sensor_mm = 36, fstop = 0, focus_dist = 1000, ortho_width = 1000;
+    uint32_t ortho = 0, projection = 0;
+    float fov_x = 360, fov_y = 180, exterior = 1;
+    std::vector<HMaterial> materials;
+    std::vector<HMesh> meshes;
+    std::vector<HInstance> instances;
+    std::vector<HLight> lights;
+    uint32_t env_kind = 0;
+    float env_floor = 0.1f, env_horizon = 0.3f, env_zenith = 0.6f, env_strength = 1, env_rotation = 0;
+    float background_color[3] = {0.05f, 0.05f, 0.05f};
+    uint32_t background_mode = 0;
+    uint32_t floor_mode = 0;
+    float floor_z = 0;
+    float floor_color[3] = {0.5f, 0.5f, 0.5f};
+    uint32_t width = 640, height = 360, max_samples = 64, seed = 0, tonemap = 1, max_depth = 8;
+    float max_seconds = 0, exposure_ev = 0, clamp_indirect = 0;
+    uint32_t pixel_filter = 0, edge_supersample = 1;
+};
+
+// Parses the RSB subset the path tracer reads. Returns false with `error` set (the reference's
+// wording for format errors, "unsupported: ..." for features outside this path).
+bool parse_rsb(const uint8_t* bytes, size_t len, HScene& out, std::string& error);
+
+// Flattened, device-ready arrays of a scene.
+struct Flat {
+    std::vector<QNode> nodes;
+    std::vector<TriRec> tris;
+    std::vector<BlasInst> blas;
+    std::vector<DevInstance> instances;
+    std::vector<float> positions, normals;  // 4 floats per vertex
+    std::vector<uint32_t> tri_index;        // 4 per triangle
+    std::vector<DevMaterial> materials;
+    LightsDev lights;
+    SceneDev scene;  // pointers left null
+    uint32_t tlas_root = NODE_EMPTY;
+    uint32_t stack_need = 0;
+    uint64_t instanced_triangles = 0;
+    double build_seconds = 0;
+};
+// Builds the BVHs and the device layout. Returns false with `error` when a limit is exceeded.
+bool flatten_scene(const HScene& s, Flat& out, std::string& error);
+
+}  // namespace rtg

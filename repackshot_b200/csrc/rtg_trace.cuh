@@ -1,0 +1,309 @@
+// Ray queries on the device: the watertight triangle test, the quantised 8-wide slab test and
+// the two-level closest-hit / any-hit traversal (engine/crates/rt-core/src/geometry/
+// triangle.rs:60-160, traverse.rs:47-802), and the hit details of geometry/mod.rs:682-808.
+//
+// The answer of a nearest-hit query is the smallest (t, instance, triangle) in lexicographic
+// order over every triangle the ray meets in [t_min, t_max], so it does not depend on the tree:
+// the flattened quantised BVH returns the bits the reference's BVH8 returns.
+#pragma once
+#include "rtg_dev.h"
+
+namespace rtg {
+
+constexpr int STACK_CAP = 96;
+constexpr uint32_t STACK_RETURN = 0xfffffffeu;
+#define RTG_ROBUST 1.00000047683715820312f  // 1 + 4 f32::EPSILON (Ize 2013)
+
+struct PRay {
+    float org[3], inv[3];
+    bool neg[3];
+    int kx, ky, kz;
+    float sx, sy, sz;
+    float tmin, tmax;
+};
+
+RTG_D PRay prepare_ray(V3 o, V3 d, float tmin, float tmax) {  // triangle.rs:60
+    PRay r;
+    float dd[3] = {d.x, d.y, d.z};
+    r.inv[0] = 1.0f / d.x;
+    r.inv[1] = 1.0f / d.y;
+    r.inv[2] = 1.0f / d.z;
+    float a0 = absf(d.x), a1 = absf(d.y), a2 = absf(d.z);
+    int kz = (a0 >= a1 && a0 >= a2) ? 0 : (a1 >= a2 ? 1 : 2);
+    int kx = (kz + 1) % 3, ky = (kz + 2) % 3;
+    if (dd[kz] < 0.0f) { int t = kx; kx = ky; ky = t; }
+    float sz = r.inv[kz];
+    r.org[0] = o.x; r.org[1] = o.y; r.org[2] = o.z;
+    r.neg[0] = signbitf(r.inv[0]);
+    r.neg[1] = signbitf(r.inv[1]);
+    r.neg[2] = signbitf(r.inv[2]);
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    r.sx = dd[kx] * sz;
+    r.sy = dd[ky] * sz;
+    r.sz = sz;
+    r.tmin = tmin;
+    r.tmax = rmin(tmax, F_MAX);
+    return r;
+}
+RTG_D float pick3(const float* v, int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
+
+// The scalar watertight test (triangle.rs:123), the reference's operations in its order.
+RTG_D bool watertight(const PRay& r, const float* v0, const float* v1, const float* v2, float tmax, bool cull_back,
+                      float& t, float& u, float& v, float& w, float& det) {
+    float ox = r.org[r.kx], oy = r.org[r.ky], oz = r.org[r.kz];
+    float a_x = pick3(v0, r.kx) - ox, a_y = pick3(v0, r.ky) - oy, a_z = pick3(v0, r.kz) - oz;
+    float b_x = pick3(v1, r.kx) - ox, b_y = pick3(v1, r.ky) - oy, b_z = pick3(v1, r.kz) - oz;
+    float c_x = pick3(v2, r.kx) - ox, c_y = pick3(v2, r.ky) - oy, c_z = pick3(v2, r.kz) - oz;
+    float ax = a_x - r.sx * a_z, ay = a_y - r.sy * a_z;
+    float bx = b_x - r.sx * b_z, by = b_y - r.sy * b_z;
+    float cx = c_x - r.sx * c_z, cy = c_y - r.sy * c_z;
+    u = cx * by - cy * bx;
+    v = ax * cy - ay * cx;
+    w = bx * ay - by * ax;
+    bool negative = u < 0.0f || v < 0.0f || w < 0.0f;
+    bool positive = u > 0.0f || v > 0.0f || w > 0.0f;
+    bool rejected = cull_back ? negative : (negative && positive);
+    det = u + v + w;
+    if (rejected || det == 0.0f) return false;
+    float az = r.sz * a_z, bz = r.sz * b_z, cz = r.sz * c_z;
+    t = (u * az + v * bz + w * cz) / det;
+    return t >= r.tmin && t <= tmax;
+}
+
+RTG_D float smax_(float a, float b) { return a > b ? a : b; }
+RTG_D float smin_(float a, float b) { return a < b ? a : b; }
+
+// Slab test of the eight children of a quantised node; returns the hit mask and entry distances.
+RTG_D uint32_t node_test(const QNode* __restrict__ node, const PRay& r, float tmax, float nr[8], uint32_t child[8]) {
+    const float4* q = reinterpret_cast<const float4*>(node);
+    float4 w0 = __ldg(q + 0), w1 = __ldg(q + 1), w2 = __ldg(q + 2), w3 = __ldg(q + 3), w4 = __ldg(q + 4), w5 = __ldg(q + 5);
+    float px = w0.x, py = w0.y, pz = w0.z;
+    uint32_t meta = __float_as_uint(w0.w);
+    float sx = __uint_as_float((meta & 0xffu) << 23);
+    float sy = __uint_as_float(((meta >> 8) & 0xffu) << 23);
+    float sz = __uint_as_float(((meta >> 16) & 0xffu) << 23);
+    // qlo x,y,z then qhi x,y,z: 8 bytes each = two words each.
+    uint32_t qw[12] = {__float_as_uint(w1.x), __float_as_uint(w1.y), __float_as_uint(w1.z), __float_as_uint(w1.w),
+                       __float_as_uint(w2.x), __float_as_uint(w2.y), __float_as_uint(w2.z), __float_as_uint(w2.w),
+                       __float_as_uint(w3.x), __float_as_uint(w3.y), __float_as_uint(w3.z), __float_as_uint(w3.w)};
+    child[0] = __float_as_uint(w4.x); child[1] = __float_as_uint(w4.y); child[2] = __float_as_uint(w4.z); child[3] = __float_as_uint(w4.w);
+    child[4] = __float_as_uint(w5.x); child[5] = __float_as_uint(w5.y); child[6] = __float_as_uint(w5.z); child[7] = __float_as_uint(w5.w);
+    uint32_t bits = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        int word = c >> 2, sh = (c & 3) * 8;
+        float lx = px + (float)((qw[0 + word] >> sh) & 0xffu) * sx;
+        float ly = py + (float)((qw[2 + word] >> sh) & 0xffu) * sy;
+        float lz = pz + (float)((qw[4 + word] >> sh) & 0xffu) * sz;
+        float hx = px + (float)((qw[6 + word] >> sh) & 0xffu) * sx;
+        float hy = py + (float)((qw[8 + word] >> sh) & 0xffu) * sy;
+        float hz = pz + (float)((qw[10 + word] >> sh) & 0xffu) * sz;
+        float tx0 = ((r.neg[0] ? hx : lx) - r.org[0]) * r.inv[0];
+        float ty0 = ((r.neg[1] ? hy : ly) - r.org[1]) * r.inv[1];
+        float tz0 = ((r.neg[2] ? hz : lz) - r.org[2]) * r.inv[2];
+        float tx1 = ((r.neg[0] ? lx : hx) - r.org[0]) * r.inv[0];
+        float ty1 = ((r.neg[1] ? ly : hy) - r.org[1]) * r.inv[1];
+        float tz1 = ((r.neg[2] ? lz : hz) - r.org[2]) * r.inv[2];
+        float n = smax_(tz0, smax_(ty0, smax_(tx0, r.tmin)));
+        float f = smin_(tz1, smin_(ty1, smin_(tx1, tmax))) * RTG_ROBUST;
+        nr[c] = n;
+        if (n <= f && child[c] != NODE_EMPTY) bits |= 1u << c;
+    }
+    return bits;
+}
+
+RTG_D uint64_t stack_key(float t, uint32_t ref) { return ((uint64_t)__float_as_uint(t) << 32) | (uint64_t)ref; }
+
+RTG_D V3 xf_point(const float* m, V3 p) {
+    return v3(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
+              m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]);
+}
+RTG_D V3 xf_vector(const float* m, V3 v) {
+    return v3(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z, m[8] * v.x + m[9] * v.y + m[10] * v.z);
+}
+RTG_D V3 xf_transpose(const float* m, V3 v) {
+    return v3(m[0] * v.x + m[4] * v.y + m[8] * v.z, m[1] * v.x + m[5] * v.y + m[9] * v.z, m[2] * v.x + m[6] * v.y + m[10] * v.z);
+}
+
+struct TraceResult { uint32_t inst, tri; float t; };
+
+// Two-level traversal. `any`: stop at the first hit in [t_min, t_max] (shadow rays; children in
+// slot order). Otherwise the nearest hit with the reference's tie-break, children nearest first.
+// Returns false on a miss; sets *err bit 0 (and misses) if the stack would overflow.
+template <bool ANY>
+RTG_D bool traverse(const SceneDev& S, V3 o, V3 d, float tmin, float tmax_in, bool camera, TraceResult& res,
+                    uint32_t* err, uint64_t* stack) {
+    if (!(vfinite(o) && vfinite(d) && !veq(d, v3(0, 0, 0)))) return false;
+    const PRay W = prepare_ray(o, d, tmin, tmax_in);
+    if (!(W.tmin <= W.tmax)) return false;
+    PRay R = W;
+    float best_t = W.tmax;
+    uint32_t best_i = 0xffffffffu, best_tri = 0xffffffffu;
+    uint32_t cur = S.tlas_root;
+    int sp = 0;
+    int level = 0;
+    uint32_t b_inst = 0xffffffffu, b_flags = 0;
+    for (;;) {
+        if ((cur & NODE_LEAF) == 0) {
+            float nr[8];
+            uint32_t child[8];
+            uint32_t bits = node_test(S.nodes + cur, R, best_t, nr, child);
+            if (bits) {
+                if ((bits & (bits - 1)) == 0) {
+                    cur = child[__ffs(bits) - 1];
+                    continue;
+                }
+                if (sp + 8 > STACK_CAP) { *err |= 1u; return false; }
+                if (ANY) {
+                    int first = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    while (bits) {
+                        int s = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        stack[sp++] = stack_key(nr[s], child[s]);
+                    }
+                    cur = child[first];
+                } else {
+                    uint64_t keys[8];
+                    int count = 0;
+                    while (bits) {
+                        int s = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        uint64_t key = stack_key(nr[s], child[s]);
+                        int j = count;
+                        while (j > 0 && keys[j - 1] < key) { keys[j] = keys[j - 1]; --j; }
+                        keys[j] = key;
+                        ++count;
+                    }
+                    for (int k = 0; k < count - 1; ++k) stack[sp++] = keys[k];
+                    cur = (uint32_t)keys[count - 1];
+                }
+                continue;
+            }
+        } else if (cur != NODE_EMPTY) {
+            uint32_t first = (cur & ~NODE_LEAF) >> 4, count = (cur & 15u) + 1;
+            if (level == 0) {
+                const BlasInst* bi = S.blas + first;
+                uint32_t flags = __ldg(&bi->flags);
+                if (!(camera && (flags & 2u))) {
+                    if (sp + 1 > STACK_CAP) { *err |= 1u; return false; }
+                    stack[sp++] = stack_key(0.0f, STACK_RETURN);
+                    if (__ldg(&bi->identity)) {
+                        R = W;
+                    } else {
+                        float m[12];
+#pragma unroll
+                        for (int k = 0; k < 12; ++k) m[k] = __ldg(&bi->to_local[k]);
+                        R = prepare_ray(xf_point(m, o), xf_vector(m, d), tmin, tmax_in);
+                    }
+                    b_inst = __ldg(&bi->instance);
+                    b_flags = flags;
+                    level = 1;
+                    cur = __ldg(&bi->root);
+                    continue;
+                }
+            } else {
+                for (uint32_t k = first; k < first + count; ++k) {
+                    const float4* tr = reinterpret_cast<const float4*>(S.tris + k);
+                    float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
+                    uint32_t flags = __float_as_uint(c.w) | b_flags;
+                    if (camera && (flags & 2u)) continue;
+                    float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+                    float t, uu, vv, ww, det;
+                    if (watertight(R, v0, v1, v2, ANY ? R.tmax : best_t, (flags & 1u) != 0, t, uu, vv, ww, det)) {
+                        uint32_t inst = __float_as_uint(b.w);
+                        if (inst == 0xffffffffu) inst = b_inst;
+                        uint32_t tri = __float_as_uint(a.w);
+                        if (ANY) { res.inst = inst; res.tri = tri; res.t = t; return true; }
+                        if (t < best_t || (t == best_t && (inst < best_i || (inst == best_i && tri < best_tri)))) {
+                            best_t = t; best_i = inst; best_tri = tri;
+                        }
+                    }
+                }
+            }
+        }
+        for (;;) {
+            if (sp == 0) {
+                if (ANY || best_i == 0xffffffffu) return false;
+                res.inst = best_i; res.tri = best_tri; res.t = best_t;
+                return true;
+            }
+            uint64_t e = stack[--sp];
+            uint32_t ref = (uint32_t)e;
+            if (ref == STACK_RETURN) { level = 0; R = W; continue; }
+            float t = __uint_as_float((uint32_t)(e >> 32));
+            if (t <= (ANY ? W.tmax : best_t) * RTG_ROBUST) { cur = ref; break; }
+        }
+    }
+}
+
+struct HitInfo {
+    V3 point, normal, geometric;
+    float bary[3];
+    bool front, outside;
+};
+
+// geometry/mod.rs:731 hit_details for an instance hit.
+RTG_D bool hit_details(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, uint32_t inst, uint32_t tri, HitInfo& h,
+                       const DevInstance*& I_out, uint4& idx_out) {
+    if (inst >= S.n_instances) return false;
+    const DevInstance* I = S.instances + inst;
+    I_out = I;
+    if (!I->active) return false;
+    uint4 idx = __ldg(S.tri_index + I->tri_base + tri);
+    idx_out = idx;
+    float4 q0 = __ldg(S.positions + idx.x), q1 = __ldg(S.positions + idx.y), q2 = __ldg(S.positions + idx.z);
+    V3 p0 = v3(q0.x, q0.y, q0.z), p1 = v3(q1.x, q1.y, q1.z), p2 = v3(q2.x, q2.y, q2.z);
+    bool identity = I->identity != 0;
+    PRay r = identity ? prepare_ray(o, d, tmin, tmax) : prepare_ray(xf_point(I->to_local, o), xf_vector(I->to_local, d), tmin, tmax);
+    float v0[3] = {p0.x, p0.y, p0.z}, v1[3] = {p1.x, p1.y, p1.z}, v2[3] = {p2.x, p2.y, p2.z};
+    float t, u, v, w, det;
+    if (watertight(r, v0, v1, v2, F_MAX, false, t, u, v, w, det)) {
+        h.bary[0] = u / det; h.bary[1] = v / det; h.bary[2] = w / det;
+    } else {
+        h.bary[0] = h.bary[1] = h.bary[2] = 1.0f / 3.0f;
+    }
+    V3 pl = p0 * h.bary[0] + p1 * h.bary[1] + p2 * h.bary[2];
+    V3 cr = cross(p1 - p0, p2 - p0);
+    V3 winding = normalize(identity ? cr : xf_transpose(I->to_local, cr));
+    V3 incoming = normalize(d);
+    V3 geometric = len2(winding) > 0.0f ? winding : -incoming;
+    h.front = dot(winding, d) < 0.0f;
+    V3 smooth = v3(0, 0, 0);
+    if (I->has_normals) {
+        float4 m0 = __ldg(S.normals + idx.x), m1 = __ldg(S.normals + idx.y), m2 = __ldg(S.normals + idx.z);
+        V3 s = v3(m0.x, m0.y, m0.z) * h.bary[0] + v3(m1.x, m1.y, m1.z) * h.bary[1] + v3(m2.x, m2.y, m2.z) * h.bary[2];
+        smooth = identity ? s : xf_transpose(I->to_local, s);
+    }
+    V3 normal = len2(smooth) > 1.0e-12f ? normalize(smooth) : geometric;
+    h.normal = dot(normal, d) > 0.0f ? -normal : normal;
+    h.geometric = dot(geometric, d) > 0.0f ? -geometric : geometric;
+    h.point = identity ? pl : xf_point(I->to_world, pl);
+    h.outside = h.front != (I->inside_out != 0);
+    return true;
+}
+
+// geometry/mod.rs:682 terminator_point (Hanika 2021).
+RTG_D V3 terminator_point(const SceneDev& S, const DevInstance* I, uint4 idx, const HitInfo& h) {
+    if (!I->has_normals) return h.point;
+    float4 q[3] = {__ldg(S.positions + idx.x), __ldg(S.positions + idx.y), __ldg(S.positions + idx.z)};
+    float4 m[3] = {__ldg(S.normals + idx.x), __ldg(S.normals + idx.y), __ldg(S.normals + idx.z)};
+    V3 c[3], n[3];
+    for (int k = 0; k < 3; ++k) { c[k] = v3(q[k].x, q[k].y, q[k].z); n[k] = v3(m[k].x, m[k].y, m[k].z); }
+    float b0 = h.bary[0], b1 = h.bary[1], b2 = h.bary[2];
+    V3 p = c[0] * b0 + c[1] * b1 + c[2] * b2;
+    V3 interp = n[0] * b0 + n[1] * b1 + n[2] * b2;
+    bool identity = I->identity != 0;
+    V3 wn = identity ? interp : xf_transpose(I->to_local, interp);
+    float side = dot(wn, h.geometric) < 0.0f ? -1.0f : 1.0f;
+    V3 lifted = p;
+    for (int k = 0; k < 3; ++k) {
+        V3 nn = normalize(n[k]) * side;
+        float below = dot(p - c[k], nn);
+        if (below < 0.0f) lifted = lifted - nn * (below * h.bary[k]);
+    }
+    if (!vfinite(lifted)) return h.point;
+    return identity ? lifted : xf_point(I->to_world, lifted);
+}
+
+}  // namespace rtg

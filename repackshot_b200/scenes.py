@@ -1,0 +1,423 @@
+"""Scene construction for the renders this package is measured on: an RSB writer (the format of
+engine/crates/rt-core/src/scene/rsb.rs:1-140), the reference's example scene
+(engine/crates/rt-core/src/example.rs:20-228) and the synthetic product scenes of the
+benchmark workloads.
+
+Geometry that the reference builds in f32 (the icosphere) is built here with the same f32
+operations, so the example's bytes are the reference's ``tests/fixtures/example.rsb``.
+
+Units follow the reference: millimetres, Z up. The benchmark workloads are described Y-up in
+metres; ``yup_m_to_mm`` maps (x, y, z) to 1000 * (x, -z, y).
+"""
+from __future__ import annotations
+
+import math
+import struct
+from dataclasses import dataclass, field
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+f32 = np.float32
+
+# ---- RSB writer ----------------------------------------------------------------------------------
+
+
+@dataclass
+class Material:
+    kind: int = 0
+    base_color: Tuple[float, float, float] = (0.8, 0.8, 0.8)
+    metallic: float = 0.0
+    roughness: float = 0.5
+    ior: float = 1.5
+    transmission: float = 0.0
+    coat: float = 0.0
+    coat_roughness: float = 0.0
+    emission: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    emission_power: float = 0.0
+    flags: int = 0
+    opacity: float = 1.0
+    anisotropy: float = 0.0
+    absorption_mm: float = 0.0
+    bevel_mm: float = 0.0
+    scatter_mm: float = 0.0
+    scatter_color: Tuple[float, float, float] = (1.0, 1.0, 1.0)
+    scatter_g: float = 0.0
+    abbe: float = 0.0
+
+
+@dataclass
+class Light:
+    kind: int = 0  # 0 rect, 1 disk
+    position: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    direction: Tuple[float, float, float] = (0.0, 0.0, -1.0)
+    up: Tuple[float, float, float] = (0.0, 1.0, 0.0)
+    size_x: float = 100.0
+    size_y: float = 100.0
+    color: Tuple[float, float, float] = (1.0, 1.0, 1.0)
+    power: float = 1.0
+    spread_deg: float = 180.0
+    angle_deg: float = 0.0
+    flags: int = 3  # glossy | camera
+
+
+@dataclass
+class Mesh:
+    positions: np.ndarray  # (n, 3) float32
+    normals: np.ndarray  # (n, 3) float32 (zeros: none)
+    indices: np.ndarray  # (m,) uint32
+    material_id: int = 0
+
+
+@dataclass
+class Instance:
+    mesh: int
+    rows: Sequence[float] = (1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0)
+    material_id: int = 0
+    flags: int = 0
+
+
+@dataclass
+class Scene:
+    camera_position: Tuple[float, float, float] = (0.0, -1000.0, 0.0)
+    camera_target: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    camera_up: Tuple[float, float, float] = (0.0, 0.0, 1.0)
+    focal_mm: float = 50.0
+    sensor_mm: float = 36.0
+    fstop: float = 0.0
+    focus_dist: float = 1000.0
+    ortho: int = 0
+    ortho_width: float = 1000.0
+    materials: List[Material] = field(default_factory=list)
+    meshes: List[Mesh] = field(default_factory=list)
+    instances: List[Instance] = field(default_factory=list)
+    lights: List[Light] = field(default_factory=list)
+    env_kind: int = 0
+    env_floor: float = 0.1
+    env_horizon: float = 0.3
+    env_zenith: float = 0.6
+    env_strength: float = 1.0
+    env_rotation: float = 0.0
+    background_color: Tuple[float, float, float] = (0.05, 0.05, 0.05)
+    background_mode: int = 0
+    floor_mode: int = 0
+    floor_z: float = 0.0
+    floor_color: Tuple[float, float, float] = (0.5, 0.5, 0.5)
+    width: int = 640
+    height: int = 360
+    max_samples: int = 64
+    seed: int = 0
+    max_seconds: float = 0.0
+    exposure_ev: float = 0.0
+    tonemap: int = 1
+    max_depth: int = 8
+    clamp_indirect: float = 0.0
+    pixel_filter: int = 0
+
+
+def _sec(tag: bytes, payload: bytes) -> bytes:
+    return tag + struct.pack("<I", len(payload)) + payload
+
+
+def _f(*v) -> bytes:
+    return struct.pack("<%df" % len(v), *[float(f32(x)) for x in v])
+
+
+def _u(*v) -> bytes:
+    return struct.pack("<%dI" % len(v), *v)
+
+
+def to_rsb(s: Scene) -> bytes:
+    """Serialises a scene as RSB version 1, sections in the reference writer's order (CAMR, MATL,
+    MESH, INST, LGHT, ENVR, FLOR, RNDR) and payload sizes (rsb.rs:1645-1990)."""
+    out = [b"RSB1", _u(0)]
+    out.append(_sec(b"CAMR", _f(*s.camera_position, *s.camera_target, *s.camera_up, s.focal_mm, s.sensor_mm, s.fstop,
+                                s.focus_dist) + _u(s.ortho) + _f(s.ortho_width)))
+    for m in s.materials:
+        out.append(_sec(b"MATL", _u(m.kind) + _f(*m.base_color, m.metallic, m.roughness, m.ior, m.transmission, m.coat,
+                                                 m.coat_roughness, *m.emission, m.emission_power) + _u(m.flags) +
+                        _f(m.opacity, m.anisotropy, m.absorption_mm, m.bevel_mm, m.scatter_mm, *m.scatter_color,
+                           m.scatter_g, m.abbe)))
+    for mesh in s.meshes:
+        p = np.ascontiguousarray(mesh.positions, dtype="<f4")
+        n = np.ascontiguousarray(mesh.normals, dtype="<f4")
+        i = np.ascontiguousarray(mesh.indices, dtype="<u4")
+        out.append(_sec(b"MESH", _u(len(p), len(i)) + p.tobytes() + n.tobytes() + i.tobytes() + _u(mesh.material_id)))
+    for inst in s.instances:
+        out.append(_sec(b"INST", _u(inst.mesh) + _f(*inst.rows) + _u(inst.material_id, inst.flags)))
+    for l in s.lights:
+        out.append(_sec(b"LGHT", _u(l.kind) + _f(*l.position, *l.direction, *l.up, l.size_x, l.size_y, *l.color, l.power,
+                                                 l.spread_deg, l.angle_deg) + _u(l.flags)))
+    out.append(_sec(b"ENVR", _u(s.env_kind) + _f(s.env_floor, s.env_horizon, s.env_zenith, s.env_strength, s.env_rotation,
+                                                 *s.background_color) + _u(s.background_mode) +
+                    _u(0xFFFFFFFF, 0xFFFFFFFF, 0) + _f(3.0, 0.0, 45.0, 0.0, 0.0, 1.0, 1.0) + _u(0)))
+    out.append(_sec(b"FLOR", _u(s.floor_mode) + _f(s.floor_z, *s.floor_color)))
+    out.append(_sec(b"RNDR", _u(s.width, s.height, s.max_samples, s.seed) + _f(s.max_seconds, s.exposure_ev) +
+                    _u(s.tonemap, s.max_depth) + _f(s.clamp_indirect) + _u(0, 0, 0) + _f(0.0, 1.0) +
+                    _u(s.pixel_filter, 1)))
+    return b"".join(out)
+
+
+# ---- f32 geometry helpers ----------------------------------------------------------------------
+
+
+def _normalize32(v):
+    x, y, z = f32(v[0]), f32(v[1]), f32(v[2])
+    ln = np.sqrt(f32(f32(f32(x * x) + f32(y * y)) + f32(z * z)))
+    if ln > 0 and np.isfinite(ln):
+        return (f32(x / ln), f32(y / ln), f32(z / ln))
+    return (x, y, z)
+
+
+def icosphere(center, radius: float, subdivisions: int, material_id: int = 0) -> Mesh:
+    """The reference's icosphere (example.rs:20) in f32: icosahedron, midpoint subdivision,
+    vertices pushed onto the sphere; normals are the unit radial directions."""
+    with np.errstate(all="ignore"):
+        t = f32(f32(1.0) + np.sqrt(f32(5.0))) / f32(2.0)
+        base = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+                (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+        dirs = [_normalize32(v) for v in base]
+        faces = [[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2], [10, 7, 6],
+                 [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10],
+                 [8, 6, 7], [9, 8, 1]]
+        for _ in range(subdivisions):
+            mids = {}
+
+            def midpoint(a, b):
+                key = (min(a, b), max(a, b))
+                if key not in mids:
+                    da, db = dirs[a], dirs[b]
+                    dirs.append(_normalize32((f32(da[0] + db[0]), f32(da[1] + db[1]), f32(da[2] + db[2]))))
+                    mids[key] = len(dirs) - 1
+                return mids[key]
+
+            nxt = []
+            for a, b, c in faces:
+                ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+                nxt += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
+            faces = nxt
+        d = np.array(dirs, dtype=np.float32)
+        pos = (np.asarray(center, dtype=np.float32)[None, :] + d * f32(radius)).astype(np.float32)
+    return Mesh(pos, d, np.array(faces, dtype=np.uint32).reshape(-1), material_id)
+
+
+def floor_quad(z: float, half: float, material_id: int) -> Mesh:
+    """example.rs:87: a quad at height z spanning [-half, half] on X and Y, facing up."""
+    p = np.array([(-half, -half, z), (half, -half, z), (half, half, z), (-half, half, z)], dtype=np.float32)
+    n = np.array([(0, 0, 1)] * 4, dtype=np.float32)
+    return Mesh(p, n, np.array([0, 1, 2, 0, 2, 3], dtype=np.uint32), material_id)
+
+
+def example_scene() -> Scene:
+    """The reference's example scene (example.rs:113): a 100 mm icosphere on a floor quad, a
+    half-size second instance, one 5 W rect light, the studio dome, an 85 mm camera at f/11."""
+    cam = (560.0, -900.0, 400.0)
+    target = (0.0, 0.0, 90.0)
+    light_pos = (250.0, -450.0, 650.0)
+    fd = np.float32(0)
+    dv = [f32(target[i]) - f32(cam[i]) for i in range(3)]
+    fd = np.sqrt(f32(f32(f32(dv[0] * dv[0]) + f32(dv[1] * dv[1])) + f32(dv[2] * dv[2])))
+    ld = _normalize32([f32(target[i]) - f32(light_pos[i]) for i in range(3)])
+    return Scene(
+        camera_position=cam, camera_target=target, camera_up=(0.0, 0.0, 1.0), focal_mm=85.0, sensor_mm=36.0,
+        fstop=11.0, focus_dist=float(fd), ortho=0, ortho_width=600.0,
+        materials=[Material(base_color=(0.92, 0.38, 0.22), roughness=0.35),
+                   Material(base_color=(0.3, 0.3, 0.32), roughness=0.8),
+                   Material(base_color=(0.2, 0.42, 0.85), roughness=0.25)],
+        meshes=[icosphere((0.0, 0.0, 100.0), 100.0, 2), floor_quad(0.0, 900.0, 1)],
+        instances=[Instance(0, material_id=0), Instance(1, material_id=1),
+                   Instance(0, rows=(0.5, 0, 0, -330.0, 0, 0.5, 0, 120.0, 0, 0, 0.5, 0), material_id=2)],
+        lights=[Light(kind=0, position=light_pos, direction=tuple(float(x) for x in ld), up=(0.0, 0.0, 1.0), size_x=400.0,
+                      size_y=400.0, power=5.0, flags=3)],
+        env_kind=0, env_floor=0.05, env_horizon=0.12, env_zenith=0.3, env_strength=1.0, background_color=(0.05, 0.05, 0.05),
+        width=512, height=384, max_samples=16, seed=1, tonemap=1, max_depth=8)
+
+
+# ---- benchmark workloads -----------------------------------------------------------------------------------
+
+
+def yup_m_to_mm(p):
+    """Y-up metres -> Z-up millimetres: (x, y, z) -> 1000 * (x, -z, y)."""
+    return (1000.0 * p[0], -1000.0 * p[2], 1000.0 * p[1])
+
+
+def focal_for_vfov(vfov_deg: float, width: int, height: int, sensor_mm: float = 36.0) -> float:
+    """Focal length giving a vertical field of view on a W x H image whose longer side spans
+    `sensor_mm` (scene/mod.rs:306-313)."""
+    sh = sensor_mm * min(1.0, height / width)
+    return (sh / 2.0) / math.tan(math.radians(vfov_deg) / 2.0)
+
+
+def rect_power(radiance: float, size_x_m: float, size_y_m: float) -> float:
+    """Flux in watts of a rect light of the given radiance (light.rs:731: L = P / (pi A))."""
+    return radiance * math.pi * size_x_m * size_y_m
+
+
+def cfg0_scene() -> Scene:
+    """Plain forward render, small: 256x256, 16 spp, depth 8, seed 1; pinhole 40 deg vertical FOV
+    at (0,1,4) looking at the origin; icosphere (subdivision 4, radius 1, centre (0,1,0)) on a
+    20x20 floor quad at y=0; GGX conductor F0 (0.95,0.64,0.54) alpha 0.3 on the sphere, Lambert
+    0.8 on the floor; one 2x2 rect light at y=4 of radiance 10; constant dome 0.1."""
+    w = h = 256
+    return Scene(
+        camera_position=yup_m_to_mm((0, 1, 4)), camera_target=(0.0, 0.0, 0.0), camera_up=(0.0, 0.0, 1.0),
+        focal_mm=focal_for_vfov(40.0, w, h), sensor_mm=36.0, fstop=0.0, focus_dist=1000.0,
+        materials=[Material(base_color=(0.95, 0.64, 0.54), metallic=1.0, roughness=math.sqrt(0.3)),
+                   Material(base_color=(0.8, 0.8, 0.8), metallic=0.0, roughness=1.0, ior=1.0)],
+        meshes=[icosphere(yup_m_to_mm((0, 1, 0)), 1000.0, 4, 0), floor_quad(0.0, 10000.0, 1)],
+        instances=[Instance(0, material_id=0), Instance(1, material_id=1)],
+        lights=[Light(kind=0, position=yup_m_to_mm((0, 4, 0)), direction=(0.0, 0.0, -1.0), up=(0.0, 1.0, 0.0),
+                      size_x=2000.0, size_y=2000.0, power=rect_power(10.0, 2.0, 2.0), flags=3)],
+        env_kind=1, env_floor=0.1, env_horizon=0.1, env_zenith=0.1, env_strength=1.0,
+        width=w, height=h, max_samples=16, seed=1, max_depth=8)
+
+
+def _value_noise3(p: np.ndarray, seed: int) -> np.ndarray:
+    """Trilinear value noise on the unit lattice, lattice values hashed from (seed, cell) with the
+    SplitMix64 finaliser; p (n, 3) float64 -> (n,) float64 in [-1, 1]."""
+    c = np.floor(p).astype(np.int64)
+    f = p - c
+    f = f * f * (3.0 - 2.0 * f)
+
+    def lattice(ix, iy, iz):
+        z = (ix.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15) ^ iy.astype(np.uint64) * np.uint64(0xC2B2AE3D27D4EB4F)
+             ^ iz.astype(np.uint64) * np.uint64(0x165667B19E3779F9) ^ np.uint64(seed) * np.uint64(0xD6E8FEB86659FD93))
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+        return (z >> np.uint64(40)).astype(np.float64) / float(1 << 24) * 2.0 - 1.0
+
+    out = 0.0
+    with np.errstate(over="ignore"):
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    wgt = (f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1]) * (f[:, 2] if dz else 1 - f[:, 2])
+                    out = out + wgt * lattice(c[:, 0] + dx, c[:, 1] + dy, c[:, 2] + dz)
+    return out
+
+
+def torus_knot(p: int = 2, q: int = 3, seg_u: int = 1024, seg_v: int = 512, radius: float = 1.0, tube: float = 0.12,
+               amplitude: float = 0.02, noise_seed: int = 7, noise_scale: float = 6.0):
+    """A (p, q) torus-knot tube of seg_u x seg_v quads (2 seg_u seg_v triangles), its surface
+    displaced along the tube's radial direction by amplitude * tube * noise (3-D value noise,
+    seeded). Returns positions (n, 3), normals (n, 3) float32 (Y-up, metres) and indices."""
+    u = np.arange(seg_u, dtype=np.float64) / seg_u * 2 * math.pi
+    v = np.arange(seg_v, dtype=np.float64) / seg_v * 2 * math.pi
+
+    def curve(t):
+        r = radius * (2 + np.cos(q * t)) / 3.0
+        return np.stack([r * np.cos(p * t), radius * -np.sin(q * t) / 3.0, r * np.sin(p * t)], axis=-1)
+
+    c = curve(u)
+    tangent = curve(u + 1e-4) - curve(u - 1e-4)
+    tangent /= np.linalg.norm(tangent, axis=1, keepdims=True)
+    ref = np.array([0.0, 1.0, 0.0])
+    n1 = np.cross(tangent, ref)
+    n1 /= np.linalg.norm(n1, axis=1, keepdims=True)
+    n2 = np.cross(tangent, n1)
+    cv, sv = np.cos(v), np.sin(v)
+    radial = n1[:, None, :] * cv[None, :, None] + n2[:, None, :] * sv[None, :, None]  # (U, V, 3)
+    base = c[:, None, :] + tube * radial
+    disp = _value_noise3(base.reshape(-1, 3) * noise_scale, noise_seed).reshape(seg_u, seg_v)
+    pos = c[:, None, :] + (tube * (1.0 + amplitude * disp))[:, :, None] * radial
+    # Normals: the tube's radial direction corrected by the displacement gradient (finite differences).
+    du = np.roll(pos, -1, axis=0) - np.roll(pos, 1, axis=0)
+    dv = np.roll(pos, -1, axis=1) - np.roll(pos, 1, axis=1)
+    nrm = np.cross(du, dv)
+    nrm /= np.linalg.norm(nrm, axis=2, keepdims=True)
+    nrm *= np.sign(np.sum(nrm * radial, axis=2, keepdims=True))
+    iu, iv = np.meshgrid(np.arange(seg_u), np.arange(seg_v), indexing="ij")
+    a = iu * seg_v + iv
+    b = ((iu + 1) % seg_u) * seg_v + iv
+    cc = ((iu + 1) % seg_u) * seg_v + (iv + 1) % seg_v
+    d = iu * seg_v + (iv + 1) % seg_v
+    tris = np.stack([np.stack([a, b, cc], -1), np.stack([a, cc, d], -1)], axis=2).reshape(-1, 3)
+    return pos.reshape(-1, 3).astype(np.float32), nrm.reshape(-1, 3).astype(np.float32), tris.astype(np.uint32)
+
+
+def product_materials(seed: int = 7):
+    """The 16-material table of the product scene, drawn from PCG32 (seed, stream 1): 6 GGX
+    conductors (alpha U(0.05, 0.5)), 4 dielectrics (ior 1.5, alpha U(0, 0.2)), 6 Lambert (albedo
+    U(0.1, 0.9))."""
+    rng = Pcg32(seed, 1)
+    f0s = [(0.95, 0.64, 0.54), (0.91, 0.92, 0.92), (1.0, 0.77, 0.34), (0.56, 0.57, 0.58), (0.97, 0.96, 0.91), (0.66, 0.62, 0.57)]
+    mats = []
+    for k in range(6):
+        alpha = 0.05 + 0.45 * rng.next_f32()
+        mats.append(Material(base_color=f0s[k], metallic=1.0, roughness=math.sqrt(alpha)))
+    for _ in range(4):
+        alpha = 0.2 * rng.next_f32()
+        mats.append(Material(kind=1, base_color=(1.0, 1.0, 1.0), transmission=1.0, ior=1.5, roughness=math.sqrt(alpha)))
+    for _ in range(6):
+        a = 0.1 + 0.8 * rng.next_f32()
+        mats.append(Material(base_color=(a, a, a), metallic=0.0, ior=1.0, roughness=1.0))
+    return mats
+
+
+def product_scene(width: int = 1920, height: int = 1080, spp: int = 64, depth: int = 12, seg_u: int = 1024,
+                  seg_v: int = 512, seed: int = 1, camera_angle_deg: float = 0.0, focal_mm: float = 50.0,
+                  rig: Sequence[Light] | None = None) -> Scene:
+    """The 1080p product scene: a displaced (2,3) torus knot of seg_u x seg_v quads (about 1 M
+    triangles at 1024 x 512) split round-robin by triangle id into 16 meshes, one per material
+    (materials are per instance in the reference), on a floor quad, lit by three rect softboxes
+    of radiance 5-20 and a gradient dome (floor 0.05, horizon 0.3, zenith 0.6)."""
+    pos, nrm, tris = torus_knot(seg_u=seg_u, seg_v=seg_v)
+    pos_mm = np.stack([pos[:, 0], -pos[:, 2], pos[:, 1]], axis=1) * np.float32(1000.0)
+    nrm_mm = np.stack([nrm[:, 0], -nrm[:, 2], nrm[:, 1]], axis=1)
+    lift = np.float32(-pos_mm[:, 2].min() + 20.0)
+    pos_mm[:, 2] += lift
+    mats = product_materials() + [Material(base_color=(0.6, 0.6, 0.6), ior=1.0, roughness=1.0)]
+    meshes, insts = [], []
+    for k in range(16):
+        sel = tris[k::16]
+        used, inv = np.unique(sel.reshape(-1), return_inverse=True)
+        meshes.append(Mesh(pos_mm[used].astype(np.float32), nrm_mm[used].astype(np.float32), inv.astype(np.uint32), k))
+        insts.append(Instance(k, material_id=k))
+    meshes.append(floor_quad(0.0, 20000.0, 16))
+    insts.append(Instance(16, material_id=16))
+    if rig is None:
+        rig = [
+            Light(0, (2500.0, -2500.0, 3000.0), tuple(_normalize_py((-2500.0, 2500.0, -2600.0))), (0.0, 0.0, 1.0), 1500.0,
+                  1500.0, (1.0, 1.0, 1.0), rect_power(20.0, 1.5, 1.5), flags=3),
+            Light(0, (-3000.0, -1500.0, 2000.0), tuple(_normalize_py((3000.0, 1500.0, -1600.0))), (0.0, 0.0, 1.0), 1200.0,
+                  2000.0, (1.0, 0.95, 0.9), rect_power(10.0, 1.2, 2.0), flags=3),
+            Light(0, (0.0, 3500.0, 2500.0), tuple(_normalize_py((0.0, -3500.0, -2100.0))), (0.0, 0.0, 1.0), 2500.0, 1000.0,
+                  (0.9, 0.95, 1.0), rect_power(5.0, 2.5, 1.0), flags=3),
+        ]
+    ang = math.radians(camera_angle_deg)
+    dist = 5200.0
+    cam = (dist * math.sin(ang), -dist * math.cos(ang), 1600.0)
+    target = (0.0, 0.0, 500.0)
+    return Scene(camera_position=cam, camera_target=target, camera_up=(0.0, 0.0, 1.0), focal_mm=focal_mm, sensor_mm=36.0,
+                 materials=mats, meshes=meshes, instances=insts, lights=list(rig), env_kind=0, env_floor=0.05,
+                 env_horizon=0.3, env_zenith=0.6, env_strength=1.0, width=width, height=height, max_samples=spp,
+                 seed=seed, max_depth=depth)
+
+
+def _normalize_py(v):
+    n = math.sqrt(sum(x * x for x in v))
+    return [x / n for x in v]
+
+
+class Pcg32:
+    """PCG-XSH-RR 64/32 (rng.rs:21), for seeded scene parameters."""
+
+    M = 6364136223846793005
+
+    def __init__(self, seed: int, stream: int):
+        self.state = 0
+        self.inc = ((stream << 1) | 1) & 0xFFFFFFFFFFFFFFFF
+        self.next_u32()
+        self.state = (self.state + seed) & 0xFFFFFFFFFFFFFFFF
+        self.next_u32()
+
+    def next_u32(self) -> int:
+        old = self.state
+        self.state = (old * self.M + self.inc) & 0xFFFFFFFFFFFFFFFF
+        xs = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        return ((xs >> rot) | (xs << ((32 - rot) & 31))) & 0xFFFFFFFF
+
+    def next_f32(self) -> float:
+        return float(np.float32(self.next_u32() >> 8) * np.float32(1.0 / 16777216.0))

@@ -1,0 +1,73 @@
+"""Writes tests/golden/reference_pins.json: the known answers the Repackshot reference pins for
+its path tracer, read from the reference's own source tree (run where it is checked out):
+
+* the FNV-1a film hashes of the example scene (engine/crates/rt-core/src/render.rs:1036-1065);
+* the PCG32 demo outputs and the mix64 value (engine/crates/rt-core/src/rng.rs:62-108);
+* the first Sobol points (engine/crates/rt-core/src/sampler.rs:403-430);
+* SHA-256 of the six energy tables (engine/crates/rt-core/src/bsdf/energy_table.rs), as the
+  little-endian bytes of their u16 values and f32 bit patterns;
+* SHA-256 of the example scene file (tests/fixtures/example.rsb).
+
+Usage: python tests/golden/make_golden.py [/path/to/reference]
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import re
+import struct
+import sys
+from pathlib import Path
+
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+CORE = REF / "engine" / "crates" / "rt-core" / "src"
+OUT = Path(__file__).resolve().parent / "reference_pins.json"
+
+
+def pinned(src: str, name: str) -> int:
+    m = re.search(r"const " + name + r": u32 = (0x[0-9a-f_]+);", src)
+    return int(m.group(1).replace("_", ""), 16)
+
+
+def main():
+    render = (CORE / "render.rs").read_text()
+    rng = (CORE / "rng.rs").read_text()
+    sampler = (CORE / "sampler.rs").read_text()
+    table = (CORE / "bsdf" / "energy_table.rs").read_text()
+    pins = {
+        "example_4spp": pinned(render, "PINNED_EXAMPLE_4SPP"),
+        "tile_centre_240_176_s3": pinned(render, "PINNED_CENTRE"),
+        "tile_small_sphere_48_144_s3": pinned(render, "PINNED_SMALL_SPHERE"),
+    }
+    block = rng[rng.index("fn matches_the_reference_implementation"):]
+    block = block[:block.index("]")]
+    pcg = [int(h.replace("_", ""), 16) for h in re.findall(r"0x[0-9a-f_]+", block)]
+    m = re.search(r"mix64\((0x[0-9A-F_]+)\), (0x[0-9A-F_]+)\)", rng)
+    sob = sampler[sampler.index("fn the_first_points_match_the_published_sequence"):]
+    sob = sob[sob.index("let expected"):sob.index("];")]
+    points = [[float(x) for x in row.split(",") if x.strip()] for row in re.findall(r"\[([0-9., ]+)\]", sob)]
+    tables = {}
+    for name in ["ALBEDO", "SCHLICK", "CLEAR_IN", "CLEAR_OUT", "ALBEDO_AVG", "SCHLICK_AVG"]:
+        mm = re.search(r"pub static " + name + r": \[(u16|f32); \d+\] = \[(.*?)\];", table, re.S)
+        vals = [v.strip() for v in mm.group(2).split(",") if v.strip()]
+        if mm.group(1) == "u16":
+            raw = struct.pack("<%dH" % len(vals), *[int(v) for v in vals])
+        else:
+            raw = struct.pack("<%df" % len(vals), *[float(v) for v in vals])
+        tables[name] = {"count": len(vals), "sha256": hashlib.sha256(raw).hexdigest()}
+    example = (REF / "tests" / "fixtures" / "example.rsb").read_bytes()
+    out = {
+        "source": "Repackshot reference tree (engine crate rt-core), read by tests/golden/make_golden.py",
+        "film_hashes": pins,
+        "pcg32_seed42_stream54": pcg,
+        "mix64": [int(m.group(1).replace("_", ""), 16), int(m.group(2).replace("_", ""), 16)],
+        "sobol_first_points_gray_order": points,
+        "energy_tables": tables,
+        "example_rsb": {"bytes": len(example), "sha256": hashlib.sha256(example).hexdigest()},
+    }
+    OUT.write_text(json.dumps(out, indent=1) + "\n")
+    print(OUT)
+
+
+if __name__ == "__main__":
+    main()
