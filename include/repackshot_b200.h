@@ -102,9 +102,14 @@ uint32_t rtg_scene_stats(uint32_t scene, double* out8);
 uint32_t rtg_set_path_capacity(uint32_t scene, uint32_t paths);
 
 /* Extend-kernel timing: when enabled, every extend launch is bracketed by CUDA events on the
- * scene's stream. out4 = total extend milliseconds, extend launches, camera + extension rays,
- * shadow rays, accumulated since the last reset (read before this call's reset). */
-uint32_t rtg_timing(uint32_t scene, uint32_t enable, uint32_t reset, double* out4);
+ * scene's stream. out5 = total extend milliseconds, extend launches, camera + extension rays,
+ * shadow rays, kernels launched, accumulated since the last reset (read before this call's
+ * reset). */
+uint32_t rtg_timing(uint32_t scene, uint32_t enable, uint32_t reset, double* out5);
+
+/* Runs the scene's work on `stream` (a cudaStream_t the caller owns and keeps alive until the
+ * scene is freed or another stream is set); null restores a stream of the scene's own. */
+uint32_t rtg_set_stream(uint32_t scene, void* stream);
 
 uint32_t rtg_synchronize(uint32_t scene);
 

@@ -39,6 +39,7 @@ def lib():
             "orc_trace": (None, [u32, v, u32, u32, u32, v, v]),
             "orc_occluded": (None, [u32, v, u32, v]),
             "orc_energy_tables": (None, [v, v]),
+            "orc_enable_merged_stats": (u32, [u32]),
             "orc_pcg32": (None, [u64, u64, u32, v]),
             "orc_mix64": (u64, [u64]),
             "orc_sobol": (u32, [u32, u32]),
@@ -85,14 +86,20 @@ class OracleScene:
 
     def render_film(self, first=0, count=1, x=0, y=0, w=None, h=None, tile=32, threads=1):
         """Film sums of samples [first, first+count) over a rectangle: (rgb, weight, alpha, lum2,
-        stats=(rays, node visits, packet tests))."""
+        stats=(rays, nearest queries, their node visits, packet tests, any-hit queries, their node
+        visits, packet tests, then the nearest and any-hit node visits and packet tests in the
+        merged single tree when enable_merged_stats() was called) with the reference's BVH8 layout."""
         w = self.width if w is None else w
         h = self.height if h is None else h
         n = w * h
         rgb, wt, al, l2 = (np.zeros(3 * n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32))
-        st = np.zeros(3, np.uint64)
+        st = np.zeros(11, np.uint64)
         lib().orc_render_film(self.handle, x, y, w, h, first, count, tile, threads, _p(rgb), _p(wt), _p(al), _p(l2), _p(st))
         return rgb.reshape(h, w, 3), wt.reshape(h, w), al.reshape(h, w), l2.reshape(h, w), tuple(int(v) for v in st)
+
+    def enable_merged_stats(self):
+        """Also count visits in one reference-layout BVH8 over all identity instances."""
+        lib().orc_enable_merged_stats(self.handle)
 
     def render_tile(self, x, y, w, h, sample, rgba=False):
         rgb = np.zeros(3 * w * h, np.float32)

@@ -108,7 +108,14 @@ Prepared Prepared::make(const Scene& s) {
     return p;
 }
 
-struct PathStats { uint64_t rays = 0; TraceStats trace; };
+// Ray counts and traversal statistics. `merged` (optional) is the scene's geometry with every
+// identity instance's triangles in one reference-layout BVH8: each query is traced there too,
+// only to count what a single tree of the reference's layout visits.
+struct PathStats {
+    uint64_t rays = 0, nearest = 0, any = 0;
+    TraceStats trace, shadow, merged_trace, merged_shadow;
+    const Geometry* merged = nullptr;
+};
 
 // radiance_weighted (integrator/mod.rs:1140) for the scene features this subset reads.
 static void radiance(const Scene& scene, const Prepared& prep, const PixelSampler& sampler, Ray camera_ray, Rgb& out,
@@ -129,7 +136,12 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
     for (;;) {
         st.rays += 1;
         RayHit hit;
+        st.nearest += 1;
         bool got = geo.trace(ray, primary, hit, &st.trace);
+        if (st.merged) {
+            RayHit unused;
+            st.merged->trace(ray, primary, unused, &st.merged_trace);
+        }
         float t_geometry = got ? hit.t : F_INF;
         float t_floor = prep.floor_t(ray, primary);
         float t_nearest = rmin(t_geometry, t_floor);
@@ -215,7 +227,8 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
                     st.rays += 1;
                     Ray sr(from, ls.wi);
                     if (finite(distance)) sr.t_max = distance * (1.0f - 1.0e-4f);
-                    bool blocked = (prep.floor_mode == 1 && prep.floor_t(sr, false) < F_INF) || geo.occluded(sr, false, &st.trace);
+                    bool blocked = (prep.floor_mode == 1 && prep.floor_t(sr, false) < F_INF) || (st.any += 1, geo.occluded(sr, false, &st.shadow));
+                    if (st.merged) st.merged->occluded(sr, false, &st.merged_shadow);
                     arrives = !blocked;
                 }
                 if (arrives) {
@@ -334,7 +347,34 @@ static void render_tile(const Scene& scene, const Prepared& prep, uint32_t tx, u
 struct Loaded {
     Scene scene;
     Prepared prep;
+    std::unique_ptr<Geometry> merged;  // statistics only (see PathStats)
 };
+
+// The scene's geometry with the triangles of all identity instances in one mesh (world space,
+// one reference-layout BVH8); transformed instances keep their own meshes and transforms.
+static void build_merged(const Geometry& g, Geometry& out) {
+    std::vector<Vec3> pos;
+    std::vector<uint32_t> idx;
+    std::vector<Mesh> meshes(1);
+    std::vector<Instance> insts(1);
+    for (size_t i = 0; i < g.instances.size(); ++i) {
+        const Instance& in = g.instances[i];
+        if (!g.prepared[i].active) continue;
+        const Mesh& m = g.meshes[in.mesh];
+        if (g.prepared[i].identity) {
+            uint32_t base = (uint32_t)pos.size();
+            pos.insert(pos.end(), m.positions.begin(), m.positions.end());
+            for (uint32_t k : m.indices) idx.push_back(base + k);
+        } else {
+            Instance copy = in;
+            copy.mesh = (uint32_t)meshes.size();
+            meshes.push_back(m);
+            insts.push_back(copy);
+        }
+    }
+    Mesh::make(meshes[0], pos, {}, idx, 0);
+    Geometry::make(out, std::move(meshes), std::move(insts));
+}
 
 }  // namespace orc
 
@@ -400,11 +440,13 @@ uint32_t orc_scene_info(uint32_t h, uint32_t* out6) {
 
 // Film accumulation over a region, samples [first, first + count) per pixel in order, tiles of
 // `tile` pixels claimed by `threads` workers (rt-cli/src/lib.rs:266-368). Outputs are the film's
-// sums: rgb (3 per pixel), weight, alpha, lum2. Returns the ray count; stats3 (may be null) gets
-// rays, inner-node visits, packet tests.
+// sums: rgb (3 per pixel), weight, alpha, lum2. Returns the ray count; stats7 (may be null) gets
+// rays; nearest-hit queries, their reference-BVH8 inner-node visits and packet tests; any-hit
+// queries, their node visits and packet tests; then (after orc_enable_merged_stats) the node
+// visits and packet tests of the same nearest and any-hit queries in the merged tree.
 uint64_t orc_render_film(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint32_t hgt, uint32_t first, uint32_t count,
                          uint32_t tile, uint32_t threads, float* rgb, float* weight, float* alpha, float* lum2,
-                         uint64_t* stats3) {
+                         uint64_t* stats11) {
     Loaded* l = get(h);
     if (!l || !rgb || w == 0 || hgt == 0) return 0;
     if (tile == 0) tile = 32;
@@ -413,9 +455,11 @@ uint64_t orc_render_film(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint3
     for (uint32_t y = 0; y < hgt; y += tile)
         for (uint32_t x = 0; x < w; x += tile) { tiles.push_back(x); tiles.push_back(y); }
     std::atomic<size_t> next(0);
-    std::atomic<uint64_t> rays(0), nodes(0), packets(0);
+    std::atomic<uint64_t> rays(0), nq(0), nodes(0), packets(0), aq(0), anodes(0), apackets(0);
+    std::atomic<uint64_t> mnodes(0), mpackets(0), manodes(0), mapackets(0);
     auto worker = [&]() {
         PathStats st;
+        st.merged = l->merged.get();
         for (;;) {
             size_t t = next.fetch_add(1);
             if (t >= tiles.size() / 2) break;
@@ -433,14 +477,37 @@ uint64_t orc_render_film(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint3
                 }
         }
         rays += st.rays;
+        nq += st.nearest;
         nodes += st.trace.nodes;
         packets += st.trace.packets;
+        aq += st.any;
+        anodes += st.shadow.nodes;
+        apackets += st.shadow.packets;
+        mnodes += st.merged_trace.nodes;
+        mpackets += st.merged_trace.packets;
+        manodes += st.merged_shadow.nodes;
+        mapackets += st.merged_shadow.packets;
     };
     std::vector<std::thread> pool;
     for (uint32_t i = 0; i < threads; ++i) pool.emplace_back(worker);
     for (auto& t : pool) t.join();
-    if (stats3) { stats3[0] = rays; stats3[1] = nodes; stats3[2] = packets; }
+    if (stats11) {
+        uint64_t v[11] = {rays, nq, nodes, packets, aq, anodes, apackets, mnodes, mpackets, manodes, mapackets};
+        std::memcpy(stats11, v, sizeof(v));
+    }
     return rays;
+}
+
+// Also counts every query's visits in a single reference-layout BVH8 over the identity
+// instances' triangles (stats11[7..10] of orc_render_film); builds that tree once.
+uint32_t orc_enable_merged_stats(uint32_t h) {
+    Loaded* l = get(h);
+    if (!l) return 1;
+    if (!l->merged) {
+        l->merged = std::make_unique<Geometry>();
+        build_merged(l->scene.geometry, *l->merged);
+    }
+    return 0;
 }
 
 // One sample of each pixel of a tile as `rt_render_tile` gives it: w*h*3 radiance (resolved

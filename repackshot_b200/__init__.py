@@ -53,6 +53,7 @@ ABI = {
     "rtg_scene_stats": (_u32, [_u32, _f]),
     "rtg_set_path_capacity": (_u32, [_u32, _u32]),
     "rtg_timing": (_u32, [_u32, _u32, _u32, _f]),
+    "rtg_set_stream": (_u32, [_u32, ctypes.c_void_p]),
     "rtg_synchronize": (_u32, [_u32]),
 }
 
@@ -166,10 +167,15 @@ class Scene:
         _check(lib().rtg_set_path_capacity(self.handle, paths))
 
     def timing(self, enable: bool, reset: bool = False):
-        """(extend ms, extend launches, camera+extension rays, shadow rays) since the last reset."""
-        out = np.zeros(4, np.float64)
+        """(extend ms, extend launches, camera+extension rays, shadow rays, kernels launched)
+        since the last reset."""
+        out = np.zeros(5, np.float64)
         _check(lib().rtg_timing(self.handle, int(enable), int(reset), _ptr(out)))
-        return float(out[0]), int(out[1]), int(out[2]), int(out[3])
+        return float(out[0]), int(out[1]), int(out[2]), int(out[3]), int(out[4])
+
+    def set_stream(self, stream_ptr: int | None):
+        """Runs this scene's work on a caller-owned cudaStream_t (e.g. torch's current stream)."""
+        _check(lib().rtg_set_stream(self.handle, stream_ptr))
 
     def synchronize(self):
         _check(lib().rtg_synchronize(self.handle))

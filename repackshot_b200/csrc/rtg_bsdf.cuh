@@ -406,7 +406,7 @@ RTG_HD Rgb eval_refraction(const EnergyTables& E, const Bsdf& b, V3 wo, V3 wi) {
     float attenuation = layer_passes(E, b.coat_layer, wo.z);
     return b.tint * (b.clear * attenuation * value);
 }
-RTG_HD Rgb bsdf_eval(const EnergyTables& E, const Bsdf& b, V3 wo, V3 wi, int lobes) {
+RTG_HD_NI Rgb bsdf_eval(const EnergyTables& E, const Bsdf& b, V3 wo, V3 wi, int lobes) {
     if (wo.z <= 0.0f) return splat(0.0f);
     if (wi.z <= 0.0f) {
         if (wi.z < 0.0f && lobes == LOBES_ALL && b.clear > 0.0f && !b.thin) return eval_refraction(E, b, wo, wi);
@@ -453,7 +453,7 @@ RTG_HD float refraction_pdf(const Bsdf& b, const LobeWeights& w, V3 wo, V3 wi) {
     float jacobian = b.eta * b.eta * (-ci) / (denom * denom);
     return w.clear * (1.0f - reflect_chance(b, wo.z, co)) * visible * jacobian;
 }
-RTG_HD float bsdf_pdf(const EnergyTables& E, const Bsdf& b, V3 wo, V3 wi) {
+RTG_HD_NI float bsdf_pdf(const EnergyTables& E, const Bsdf& b, V3 wo, V3 wi) {
     if (wo.z <= 0.0f) return 0.0f;
     if (wi.z <= 0.0f) {
         if (wi.z < 0.0f && b.clear > 0.0f && !b.thin) return refraction_pdf(b, lobe_weights(E, b, wo), wo, wi);
@@ -480,7 +480,7 @@ RTG_HD bool finish_refraction(const EnergyTables& E, const Bsdf& b, const LobeWe
     out.wi = wi; out.pdf = p; out.straight = false;
     return true;
 }
-RTG_HD bool bsdf_sample(const EnergyTables& E, const Bsdf& b, V3 wo, float u0, float u1, BsdfSample& out) {  // bsdf.rs:833
+RTG_HD_NI bool bsdf_sample(const EnergyTables& E, const Bsdf& b, V3 wo, float u0, float u1, BsdfSample& out) {  // bsdf.rs:833
     if (wo.z <= 0.0f) return false;
     LobeWeights w = lobe_weights(E, b, wo);
     V3 wi;

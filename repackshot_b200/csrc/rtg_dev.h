@@ -101,6 +101,9 @@ struct SceneDev {
     const float4* normals;    // xyz per vertex (global)
     const uint4* tri_index;   // global vertex indices per global triangle
     const DevMaterial* materials;
+    // Bsdf::surface of every material seen from outside (2 m) and from inside (2 m + 1), and the
+    // floor's Lambert lobe (2 n_materials): built once on the host, the same bits.
+    const Bsdf* bsdfs;
     uint32_t tlas_root, n_instances, n_materials, stack_need;
     EnergyTables energy;
 };

@@ -50,7 +50,7 @@ struct Scene {
     PathBuffers P{};
     DevBuf path_mem;
     uint32_t capacity = 0;
-    uint32_t max_capacity = 1u << 22;
+    uint32_t max_capacity = 1u << 24;  // 16 Mi paths (2.6 GB): waves of several samples amortise the path tail
     // statistics
     uint64_t rays = 0;
     double build_seconds = 0;
@@ -62,6 +62,8 @@ struct Scene {
     double extend_ms = 0;
     uint64_t extend_launches = 0;
     uint64_t extend_rays = 0, shadow_rays = 0;
+    uint64_t launches = 0;        // kernels launched since the last timing reset
+    bool own_stream = true;       // false after rtg_set_stream: the caller owns the stream
     ~Scene() {
         for (auto& b : bufs) b.release();
         path_mem.release();
@@ -70,7 +72,7 @@ struct Scene {
             for (int i = 0; i < WaveTiming::MAX_EVENTS; ++i) cudaEventDestroy(wt->ev[i]);
             delete wt;
         }
-        if (stream) cudaStreamDestroy(stream);
+        if (stream && own_stream) cudaStreamDestroy(stream);
     }
 };
 struct Film {
@@ -137,7 +139,7 @@ uint32_t ensure_capacity(Scene& sc, uint32_t paths) {
     if (paths <= sc.capacity) return RTG_STATUS_OK;
     sc.path_mem.release();
     size_t n = paths;
-    size_t bytes = n * (16 * 5 + 4 + 4 + 16 + 4 * 2 + 16 * 3) + 14 * 256 + 256;
+    size_t bytes = n * (16 * 5 + 4 + 4 + 16 + 4 * 4 + 16 * 3) + 16 * 256 + 256 + 512 * 4;
     RTG_CHECK(cudaMalloc(&sc.path_mem.p, bytes));
     sc.path_mem.bytes = bytes;
     uint8_t* p = (uint8_t*)sc.path_mem.p;
@@ -153,6 +155,10 @@ uint32_t ensure_capacity(Scene& sc, uint32_t paths) {
     sc.P.hit = (uint4*)take(16);
     sc.P.queue[0] = (uint32_t*)take(4);
     sc.P.queue[1] = (uint32_t*)take(4);
+    sc.P.sorted = (uint32_t*)take(4);
+    sc.P.key = (uint32_t*)take(4);
+    sc.P.bins = (uint32_t*)p;
+    p += 512 * 4;
     sc.P.sh_o = (float4*)take(16);
     sc.P.sh_d = (float4*)take(16);
     sc.P.sh_c = (float4*)take(16);
@@ -186,6 +192,7 @@ uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film) {
     }
     launch_wave(sc.S, sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t);
     RTG_CHECK(cudaGetLastError());
+    sc.launches += 2 + 6 * (uint64_t)(sc.S.max_depth + 1) - (film ? 0 : 1);
     if (t) {
         RTG_CHECK(cudaStreamSynchronize(sc.stream));
         for (int i = 0; i + 1 < t->ev_count; i += 2) {
@@ -314,7 +321,7 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     std::memcpy(ti.data(), F.tri_index.data(), F.tri_index.size() * 4);
     if (upload(*sc, F.nodes, sc->S.nodes) || upload(*sc, F.tris, sc->S.tris) || upload(*sc, F.blas, sc->S.blas) ||
         upload(*sc, F.instances, sc->S.instances) || upload(*sc, pos, sc->S.positions) || upload(*sc, nrm, sc->S.normals) ||
-        upload(*sc, ti, sc->S.tri_index) || upload(*sc, F.materials, sc->S.materials))
+        upload(*sc, ti, sc->S.tri_index) || upload(*sc, F.materials, sc->S.materials) || upload(*sc, F.bsdfs, sc->S.bsdfs))
         return 0;
     if (cudaMalloc(&sc->d_lights, sizeof(LightsDev)) != cudaSuccess ||
         cudaMemcpy(sc->d_lights, &F.lights, sizeof(LightsDev), cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -506,18 +513,41 @@ uint32_t rtg_set_path_capacity(uint32_t handle, uint32_t paths) {
     return RTG_STATUS_OK;
 }
 
-uint32_t rtg_timing(uint32_t handle, uint32_t enable, uint32_t reset, double* out3) {
+uint32_t rtg_timing(uint32_t handle, uint32_t enable, uint32_t reset, double* out5) {
     std::lock_guard<std::mutex> lk(g_mu);
     Scene* sc = scene_of(handle);
     if (!sc) return RTG_STATUS_BAD_HANDLE;
-    if (out3) {
-        out3[0] = sc->extend_ms;
-        out3[1] = (double)sc->extend_launches;
-        out3[2] = (double)sc->extend_rays;
-        out3[3] = (double)sc->shadow_rays;
+    if (out5) {
+        out5[0] = sc->extend_ms;
+        out5[1] = (double)sc->extend_launches;
+        out5[2] = (double)sc->extend_rays;
+        out5[3] = (double)sc->shadow_rays;
+        out5[4] = (double)sc->launches;
     }
-    if (reset) { sc->extend_ms = 0; sc->extend_launches = 0; sc->extend_rays = 0; sc->shadow_rays = 0; }
+    if (reset) {
+        sc->extend_ms = 0;
+        sc->extend_launches = 0;
+        sc->extend_rays = 0;
+        sc->shadow_rays = 0;
+        sc->launches = 0;
+    }
     sc->timing = enable != 0;
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_set_stream(uint32_t handle, void* stream) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    if (sc->own_stream) RTG_CHECK(cudaStreamDestroy(sc->stream));
+    if (stream) {
+        sc->stream = (cudaStream_t)stream;
+        sc->own_stream = false;
+    } else {
+        RTG_CHECK(cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking));
+        sc->own_stream = true;
+    }
     return RTG_STATUS_OK;
 }
 

@@ -52,11 +52,26 @@ __global__ void k_camera(SceneDev S, WaveDesc w, PathBuffers P) {
         P.flags[slot] = PF_PRIMARY;
         P.queue[0][slot] = slot;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        P.counters[0] = w.n;
-        P.counters[1] = 0;
-        P.counters[2] = 0;
+    if (blockIdx.x == 0) {
+        for (uint32_t k = threadIdx.x; k < 512; k += blockDim.x) P.bins[k] = 0;
+        if (threadIdx.x == 0) {
+            P.counters[0] = w.n;
+            P.counters[1] = 0;
+            P.counters[2] = 0;
+        }
     }
+}
+
+// Material key of a path's next vertex, for the material-sorted shade.
+__device__ __forceinline__ uint32_t material_key(const SceneDev& S, bool got, uint32_t inst) {
+    uint32_t k = got ? __ldg(&S.instances[inst].material) : S.n_materials;
+    return k < 255u ? k : 255u;
+}
+
+// Adds one to bins[key] for every active lane, one atomic per distinct key of the warp.
+__device__ __forceinline__ void warp_count(uint32_t* bins, uint32_t key) {
+    uint32_t mask = __match_any_sync(__activemask(), key);
+    if ((threadIdx.x & 31) == (uint32_t)(__ffs((int)mask) - 1)) atomicAdd(&bins[key], (uint32_t)__popc(mask));
 }
 
 // ---- extend: nearest hit of every active path ------------------------------------------------------------
@@ -71,8 +86,41 @@ __global__ void __launch_bounds__(128) k_extend(SceneDev S, PathBuffers P, int c
         TraceResult r;
         bool got = traverse<false>(S, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, f_inf(), primary, r, &err, stack);
         P.hit[slot] = got ? make_uint4(r.inst, r.tri, __float_as_uint(r.t), 1u) : make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+        uint32_t key = material_key(S, got, r.inst);
+        P.key[slot] = key;
+        warp_count(P.bins, key);
     }
     if (err) atomicOr(&P.counters[3], err);
+}
+
+// Exclusive prefix of the key histogram into the scatter cursors; clears the histogram.
+__global__ void k_scan(PathBuffers P) {
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int k = 0; k < 256; ++k) {
+            uint32_t c = P.bins[k];
+            P.bins[256 + k] = acc;
+            P.bins[k] = 0;
+            acc += c;
+        }
+    }
+}
+
+// The active queue reordered by material key (the order inside a key does not matter: every
+// path's result depends on its own slot only).
+__global__ void k_scatter(PathBuffers P, int cur) {
+    uint32_t n = *(volatile uint32_t*)&P.counters[cur];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t slot = P.queue[cur][i];
+        uint32_t key = P.key[slot];
+        uint32_t mask = __match_any_sync(__activemask(), key);
+        int leader = __ffs((int)mask) - 1;
+        uint32_t base = 0;
+        if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&P.bins[256 + key], (uint32_t)__popc(mask));
+        base = __shfl_sync(mask, base, leader);
+        uint32_t rank = __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
+        P.sorted[base + rank] = slot;
+    }
 }
 
 // ---- shade: one vertex of every active path ----------------------------------------------------------
@@ -82,7 +130,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneDev S, const LightsDev* __re
     uint32_t n = *(volatile uint32_t*)&P.counters[cur];
     uint32_t rays_local = 0, shadow_local = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t slot = P.queue[cur][i];
+        uint32_t slot = P.sorted[i];
         float4 o4 = P.o[slot], d4 = P.d[slot], thr4 = P.thr[slot], sum = P.sum[slot];
         uint32_t flags = P.flags[slot];
         uint4 hit = P.hit[slot];
@@ -162,8 +210,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneDev S, const LightsDev* __re
                 }
             }
             if (bounce >= S.max_depth) break;
-            Bsdf b = mat ? bsdf_surface(S.energy, *mat, s_outside)
-                         : bsdf_lambert(rgb(S.floor_color[0], S.floor_color[1], S.floor_color[2]));
+            const Bsdf& b = S.bsdfs[mat ? 2 * I->material + (s_outside ? 0 : 1) : 2 * S.n_materials];
             // Prepared::frame (integrator/mod.rs:833)
             Frame fr = frame_from_normal(s_normal);
             if (s_inst && I->tangent_on) {
@@ -362,6 +409,8 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
         } else {
             k_extend<<<g, 128, 0, st>>>(S, P, cur);
         }
+        k_scan<<<1, 32, 0, st>>>(P);
+        k_scatter<<<g, 256, 0, st>>>(P, cur);
         k_shade<<<g, 128, 0, st>>>(S, L, P, cur, bounce, w);
         k_shadow<<<g, 128, 0, st>>>(S, P);
         k_next_round<<<1, 1, 0, st>>>(P, cur);

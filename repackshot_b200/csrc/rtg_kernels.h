@@ -25,6 +25,9 @@ struct PathBuffers {
     uint32_t* medium;
     uint4* hit;
     uint32_t* queue[2];
+    uint32_t* sorted;    // the active queue ordered by material key (shade reads it)
+    uint32_t* key;       // per slot: material of the hit (n_materials: floor or miss)
+    uint32_t* bins;      // [0, 256) key histogram, [256, 512) scatter cursors
     float4* sh_o;    // shadow rays: origin, w: t_max
     float4* sh_d;
     float4* sh_c;    // contribution, w: slot

@@ -14,9 +14,15 @@
 #ifdef __CUDACC__
 #define RTG_HD __host__ __device__ __forceinline__
 #define RTG_D __device__ __forceinline__
+// Large functions called from several places of a kernel: kept out of line on the device so the
+// shade kernel's code stays small enough for the instruction cache.
+#define RTG_HD_NI __host__ __device__ __noinline__
+#define RTG_D_NI __device__ __noinline__
 #else
 #define RTG_HD inline
 #define RTG_D inline
+#define RTG_HD_NI inline
+#define RTG_D_NI inline
 #endif
 
 namespace rtg {

@@ -2,6 +2,8 @@
 // light preparation. See rtg_scene.h.
 #include "rtg_scene.h"
 
+#include "rtg_tables.h"
+
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -700,6 +702,18 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error) {
             d.has_medium = d.sigma[0] > 0.0f || d.sigma[1] > 0.0f || d.sigma[2] > 0.0f;
         }
         F.materials.push_back(d);
+    }
+    // Bsdf::surface_at (bsdf.rs:382) of every material, entering and leaving, and the floor's
+    // Bsdf::lambert: a BSDF depends on the material and the side only, so the kernels read it.
+    {
+        const EnergyData& ed = energy_data();
+        EnergyTables E{ed.albedo.data(), ed.schlick.data(), ed.clear_in.data(), ed.clear_out.data(), ed.albedo_avg.data(),
+                       ed.schlick_avg.data()};
+        for (const DevMaterial& d : F.materials) {
+            F.bsdfs.push_back(bsdf_surface(E, d, true));
+            F.bsdfs.push_back(bsdf_surface(E, d, false));
+        }
+        F.bsdfs.push_back(bsdf_lambert(rgb(s.floor_color[0], s.floor_color[1], s.floor_color[2])));
     }
     // Bottom level: one world-space tree over the triangles of every identity instance (the
     // nearest hit does not depend on the tree, so they can share one), one object-space tree per

@@ -76,6 +76,7 @@ struct Flat {
     std::vector<float> positions, normals;  // 4 floats per vertex
     std::vector<uint32_t> tri_index;        // 4 per triangle
     std::vector<DevMaterial> materials;
+    std::vector<Bsdf> bsdfs;  // 2 per material (entering, leaving), then the floor's
     LightsDev lights;
     SceneDev scene;  // pointers left null
     uint32_t tlas_root = NODE_EMPTY;

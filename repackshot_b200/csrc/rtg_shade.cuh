@@ -111,7 +111,7 @@ RTG_D float power_heuristic(float pa, float pb) {
 
 struct LightSample { V3 wi; float distance; Rgb radiance; float pdf; bool glossy, shadow; };
 
-RTG_D bool sample_light(const LightsDev& L, const Sel& s, float u_select, float u0, float u1, LightSample& out) {  // light.rs:1150
+RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, float u0, float u1, LightSample& out) {  // light.rs:1150
     int n = L.n_entries;
     if (n == 0) return false;
     int index = 0;
@@ -169,7 +169,7 @@ RTG_D bool sample_light(const LightsDev& L, const Sel& s, float u_select, float 
 }
 
 // Lights::crossed_from (light.rs:1350): area lights a ray crosses before t_max.
-RTG_D Rgb crossed_from(const LightsDev& L, V3 o, V3 d, float tmin, float tmax, bool has_pdf, float pdf, const Sel& from, float offset) {
+RTG_D_NI Rgb crossed_from(const LightsDev& L, V3 o, V3 d, float tmin, float tmax, bool has_pdf, float pdf, const Sel& from, float offset) {
     Rgb sum = splat(0.0f);
     for (int i = 0; i < L.n_areas; ++i) {
         const AreaLightDev& l = L.areas[i];

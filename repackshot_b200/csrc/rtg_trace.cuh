@@ -244,7 +244,7 @@ struct HitInfo {
 };
 
 // geometry/mod.rs:731 hit_details for an instance hit.
-RTG_D bool hit_details(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, uint32_t inst, uint32_t tri, HitInfo& h,
+RTG_D_NI bool hit_details(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, uint32_t inst, uint32_t tri, HitInfo& h,
                        const DevInstance*& I_out, uint4& idx_out) {
     if (inst >= S.n_instances) return false;
     const DevInstance* I = S.instances + inst;
@@ -284,7 +284,7 @@ RTG_D bool hit_details(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, ui
 }
 
 // geometry/mod.rs:682 terminator_point (Hanika 2021).
-RTG_D V3 terminator_point(const SceneDev& S, const DevInstance* I, uint4 idx, const HitInfo& h) {
+RTG_D_NI V3 terminator_point(const SceneDev& S, const DevInstance* I, uint4 idx, const HitInfo& h) {
     if (!I->has_normals) return h.point;
     float4 q[3] = {__ldg(S.positions + idx.x), __ldg(S.positions + idx.y), __ldg(S.positions + idx.z)};
     float4 m[3] = {__ldg(S.normals + idx.x), __ldg(S.normals + idx.y), __ldg(S.normals + idx.z)};
