@@ -17,7 +17,9 @@ RTG_HD uint32_t make_leaf(uint32_t first, uint32_t count) { return NODE_LEAF | (
 // An 8-wide BVH node with child boxes quantised to 8 bits per plane (96 bytes, six 16-byte
 // loads). A child box decodes as p + q * 2^e per axis; the builder checks that every decoded box
 // (computed with the same IEEE operations as the kernels) contains the child's exact box, so the
-// slab test is conservative and the nearest hit stays the one brute force finds.
+// slab test never drops a hit that the exact box keeps. A flat child at the node's lower corner
+// (a floor under the rest of the scene) decodes to its exact plane, so a ray starting within
+// t_min of it is culled exactly where the reference's box culls it.
 struct alignas(16) QNode {
     float px, py, pz;
     uint8_t ex, ey, ez;   // biased exponents of the per-axis scales 2^(e-127)

@@ -3,8 +3,12 @@
 // triangle.rs:60-160, traverse.rs:47-802), and the hit details of geometry/mod.rs:682-808.
 //
 // The answer of a nearest-hit query is the smallest (t, instance, triangle) in lexicographic
-// order over every triangle the ray meets in [t_min, t_max], so it does not depend on the tree:
-// the flattened quantised BVH returns the bits the reference's BVH8 returns.
+// order over the triangles the ray meets in [t_min, t_max] whose enclosing boxes pass the slab
+// test. The boxes are conservative except at t_min: a ray that starts within about 1e-3 of a
+// large axis-aligned quad can see its flat box end just before t_min while the triangle test
+// alone would accept the hit, and the reference drops that hit. The slab test below uses the
+// reference's operations in its order on boxes that decode to the same flat planes, so it drops
+// the same hits; a padded or FMA-contracted test would not.
 #pragma once
 #include "rtg_dev.h"
 

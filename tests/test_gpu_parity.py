@@ -11,7 +11,7 @@
 import numpy as np
 import pytest
 
-from rays import edge_rays, random_rays
+from rays import edge_rays, random_rays, surface_rays
 
 pytestmark = pytest.mark.gpu
 
@@ -45,6 +45,18 @@ def test_nearest_hits_are_bit_exact(rtg, oracle_lib, which, request):
         brute, _ = o.trace(rays[:2000], camera=camera, brute=True)
         assert np.array_equal(got, want)
         assert np.array_equal(got[:2000], brute)
+
+
+@pytest.mark.parametrize("which", ["example_rsb", "cfg0_rsb", "small_product_rsb"])
+def test_surface_rays_follow_the_reference_bvh(rtg, oracle_lib, which, request):
+    # Rays that start on or just under a surface: the reference's BVH culls some hits that the
+    # triangle test alone accepts, and the device traversal must cull the same ones.
+    g, o = scene_pair(rtg, oracle_lib, request.getfixturevalue(which))
+    rays = surface_rays(o, 20000, seed=21)
+    for camera in (False, True):
+        want, _ = o.trace(rays, camera=camera)
+        assert np.array_equal(g.trace(rays, camera=camera), want)
+    assert np.array_equal(g.trace(rays, any_hit=True).astype(np.uint8), o.occluded(rays))
 
 
 @pytest.mark.parametrize("which", ["example_rsb", "small_product_rsb"])
