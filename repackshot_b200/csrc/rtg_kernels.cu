@@ -12,6 +12,9 @@ namespace rtg {
 
 __constant__ SobolTable c_sobol;
 
+// Threads per block of the traversal kernels (the stride of their shared stacks).
+constexpr int TRACE_THREADS = 128;
+
 // Flags of a path slot.
 constexpr uint32_t PF_HAS_PDF = 1, PF_PRIMARY = 2, PF_MEDIUM = 4;
 
@@ -58,6 +61,8 @@ __global__ void k_camera(SceneDev S, WaveDesc w, PathBuffers P) {
             P.counters[0] = w.n;
             P.counters[1] = 0;
             P.counters[2] = 0;
+            P.counters[4] = 0;
+            P.counters[5] = 0;
         }
     }
 }
@@ -75,20 +80,57 @@ __device__ __forceinline__ void warp_count(uint32_t* bins, uint32_t key) {
 }
 
 // ---- extend: nearest hit of every active path ------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_extend(SceneDev S, PathBuffers P, int cur) {
-    uint64_t stack[STACK_CAP];
-    uint32_t n = *(volatile uint32_t*)&P.counters[cur];
-    uint32_t err = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t slot = P.queue[cur][i];
-        float4 o = P.o[slot], d = P.d[slot];
-        bool primary = (P.flags[slot] & PF_PRIMARY) != 0;
-        TraceResult r;
-        bool got = traverse<false>(S, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, f_inf(), primary, r, &err, stack);
-        P.hit[slot] = got ? make_uint4(r.inst, r.tri, __float_as_uint(r.t), 1u) : make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
-        uint32_t key = material_key(S, got, r.inst);
-        P.key[slot] = key;
-        warp_count(P.bins, key);
+// Persistent warps over the active queue: a lane whose ray has finished takes the next queue entry
+// (one atomic per warp on counters[4]) while the rest of the warp keeps traversing, so no lane idles
+// until the slowest ray of its warp is done.
+__global__ void __launch_bounds__(TRACE_THREADS) k_extend(SceneDev S, PathBuffers P, int cur) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const uint32_t n = *(volatile uint32_t*)&P.counters[cur];
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t err = 0, slot = 0;
+    bool busy = false, drained = false;
+    Trav T;
+    for (;;) {
+        if (!drained) {
+            const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
+            if (idle) {
+                const int leader = __ffs((int)idle) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(&P.counters[4], (uint32_t)__popc(idle));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + (uint32_t)__popc(idle) >= n) drained = true;
+                const uint32_t i = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+                if (!busy && i < n) {
+                    slot = P.queue[cur][i];
+                    const float4 o = P.o[slot], d = P.d[slot];
+                    const bool primary = (P.flags[slot] & PF_PRIMARY) != 0;
+                    busy = trav_init(S, T, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, f_inf(), primary);
+                    if (!busy) {
+                        P.hit[slot] = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+                        const uint32_t key = material_key(S, false, 0);
+                        P.key[slot] = key;
+                        warp_count(P.bins, key);
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy)) {
+            if (drained) break;
+            continue;
+        }
+        if (busy) {
+            bool got = false;
+            if (trav_step<false>(S, T, stack, &err, got)) {
+                busy = false;
+                P.hit[slot] = got ? make_uint4(T.best_i, T.best_tri, __float_as_uint(T.best_t), 1u)
+                                  : make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+                const uint32_t key = material_key(S, got, T.best_i);
+                P.key[slot] = key;
+                warp_count(P.bins, key);
+            }
+        }
     }
     if (err) atomicOr(&P.counters[3], err);
 }
@@ -323,29 +365,64 @@ __global__ void __launch_bounds__(128) k_shade(SceneDev S, const LightsDev* __re
 }
 
 // ---- shadow: any hit of every queued shadow ray; the unblocked add their light ----------------------------
-__global__ void __launch_bounds__(128) k_shadow(SceneDev S, PathBuffers P) {
-    uint64_t stack[STACK_CAP];
-    uint32_t n = *(volatile uint32_t*)&P.counters[2];
-    uint32_t err = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 o = P.sh_o[i], d = P.sh_d[i];
-        TraceResult r;
-        bool blocked = traverse<true>(S, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, o.w, false, r, &err, stack);
-        if (!blocked) {
-            float4 c = P.sh_c[i];
-            uint32_t slot = __float_as_uint(c.w);
-            float4 s = P.sum[slot];
-            s.x = s.x + c.x; s.y = s.y + c.y; s.z = s.z + c.z;
-            P.sum[slot] = s;
+// Persistent warps with lane refill, as k_extend (queue position counter: counters[5]).
+__device__ __forceinline__ void shadow_unblocked(const PathBuffers& P, uint32_t i) {
+    const float4 c = P.sh_c[i];
+    const uint32_t slot = __float_as_uint(c.w);
+    float4 s = P.sum[slot];
+    s.x = s.x + c.x; s.y = s.y + c.y; s.z = s.z + c.z;
+    P.sum[slot] = s;
+}
+
+__global__ void __launch_bounds__(TRACE_THREADS) k_shadow(SceneDev S, PathBuffers P) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const uint32_t n = *(volatile uint32_t*)&P.counters[2];
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t err = 0, ray = 0;
+    bool busy = false, drained = false;
+    Trav T;
+    for (;;) {
+        if (!drained) {
+            const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
+            if (idle) {
+                const int leader = __ffs((int)idle) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(&P.counters[5], (uint32_t)__popc(idle));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + (uint32_t)__popc(idle) >= n) drained = true;
+                const uint32_t i = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+                if (!busy && i < n) {
+                    ray = i;
+                    const float4 o = P.sh_o[i], d = P.sh_d[i];
+                    busy = trav_init(S, T, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, o.w, false);
+                    if (!busy) shadow_unblocked(P, i);
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy)) {
+            if (drained) break;
+            continue;
+        }
+        if (busy) {
+            bool blocked = false;
+            if (trav_step<true>(S, T, stack, &err, blocked)) {
+                busy = false;
+                if (!blocked) shadow_unblocked(P, ray);
+            }
         }
     }
     if (err) atomicOr(&P.counters[3], err);
 }
 
 __global__ void k_next_round(PathBuffers P, int cur) {
-    // The queue just consumed becomes the next round's output; the shadow queue empties.
+    // The queue just consumed becomes the next round's output; the shadow queue empties; the
+    // extend and shadow queue positions start again.
     P.counters[cur] = 0;
     P.counters[2] = 0;
+    P.counters[4] = 0;
+    P.counters[5] = 0;
 }
 
 // ---- accumulate: film += each pixel's samples in sample-index order (image.rs:82) -------------------------
@@ -373,9 +450,11 @@ __global__ void k_accumulate(WaveDesc w, PathBuffers P, FilmDev F) {
 }
 
 // ---- ray batches for the traversal parity harness ---------------------------------------------------
-__global__ void __launch_bounds__(128) k_trace_batch(SceneDev S, const float* __restrict__ rays, uint32_t n, uint32_t mode, uint32_t* out,
+__global__ void __launch_bounds__(TRACE_THREADS) k_trace_batch(SceneDev S, const float* __restrict__ rays, uint32_t n, uint32_t mode, uint32_t* out,
                                                      uint32_t* counters) {
-    uint64_t stack[STACK_CAP];
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
     uint32_t err = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float* r = rays + 8 * i;
@@ -396,23 +475,37 @@ __global__ void __launch_bounds__(128) k_trace_batch(SceneDev S, const float* __
 // ---- launchers ---------------------------------------------------------------------------------------
 void set_sobol(const SobolTable& t, cudaStream_t s) { cudaMemcpyToSymbolAsync(c_sobol, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s); }
 
+// Blocks of the persistent traversal kernels that fit on the device at once (their grid: more
+// blocks would only start after the queue has drained).
+static int resident_blocks(const void* kernel, int threads) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+        return 0;
+    return sms * per_sm;
+}
+
 void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const FilmDev* film, cudaStream_t st,
                  int grid, WaveTiming* timing) {
-    int g = grid;
+    static const int ext_resident = resident_blocks((const void*)k_extend, TRACE_THREADS);
+    static const int sh_resident = resident_blocks((const void*)k_shadow, TRACE_THREADS);
+    const int g = grid;
+    const int g_ext = ext_resident > 0 && ext_resident < g ? ext_resident : g;
+    const int g_sh = sh_resident > 0 && sh_resident < g ? sh_resident : g;
     k_camera<<<g, 256, 0, st>>>(S, w, P);
     int cur = 0;
     for (uint32_t bounce = 0; bounce <= S.max_depth; ++bounce) {
         if (timing && timing->ev_count + 2 <= WaveTiming::MAX_EVENTS) {
             cudaEventRecord(timing->ev[timing->ev_count++], st);
-            k_extend<<<g, 128, 0, st>>>(S, P, cur);
+            k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur);
             cudaEventRecord(timing->ev[timing->ev_count++], st);
         } else {
-            k_extend<<<g, 128, 0, st>>>(S, P, cur);
+            k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur);
         }
         k_scan<<<1, 32, 0, st>>>(P);
         k_scatter<<<g, 256, 0, st>>>(P, cur);
         k_shade<<<g, 128, 0, st>>>(S, L, P, cur, bounce, w);
-        k_shadow<<<g, 128, 0, st>>>(S, P);
+        k_shadow<<<g_sh, TRACE_THREADS, 0, st>>>(S, P);
         k_next_round<<<1, 1, 0, st>>>(P, cur);
         cur ^= 1;
     }
@@ -421,7 +514,7 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
 
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,
                         cudaStream_t st, int grid) {
-    k_trace_batch<<<grid, 128, 0, st>>>(S, rays, n, mode, out, counters);
+    k_trace_batch<<<grid, TRACE_THREADS, 0, st>>>(S, rays, n, mode, out, counters);
 }
 
 }  // namespace rtg

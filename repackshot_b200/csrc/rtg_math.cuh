@@ -15,9 +15,10 @@
 #define RTG_HD __host__ __device__ __forceinline__
 #define RTG_D __device__ __forceinline__
 // Large functions called from several places of a kernel: kept out of line on the device so the
-// shade kernel's code stays small enough for the instruction cache.
-#define RTG_HD_NI __host__ __device__ __noinline__
-#define RTG_D_NI __device__ __noinline__
+// shade kernel's code stays small enough for the instruction cache. Internal linkage, so that
+// several translation units can include them.
+#define RTG_HD_NI static __host__ __device__ __noinline__
+#define RTG_D_NI static __device__ __noinline__
 #else
 #define RTG_HD inline
 #define RTG_D inline
@@ -330,6 +331,7 @@ RTG_HD float pcg_f32(Pcg32& r) { return (float)(pcg_next(r) >> 8) * (1.0f / 1677
 template <class T>
 inline T __ldg(const T* p) { return *p; }
 inline int __ffs(int x) { return __builtin_ffs(x); }
+inline int __popc(uint32_t x) { return __builtin_popcount(x); }
 inline uint32_t __float_as_uint(float f) { return rtg::fbits(f); }
 inline float __uint_as_float(uint32_t u) { return rtg::bitsf(u); }
 #endif

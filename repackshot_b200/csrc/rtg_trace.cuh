@@ -131,114 +131,188 @@ RTG_D V3 xf_transpose(const float* m, V3 v) {
 
 struct TraceResult { uint32_t inst, tri; float t; };
 
-// Two-level traversal. `any`: stop at the first hit in [t_min, t_max] (shadow rays; children in
-// slot order). Otherwise the nearest hit with the reference's tie-break, children nearest first.
-// Returns false on a miss; sets *err bit 0 (and misses) if the stack would overflow.
-template <bool ANY>
-RTG_D bool traverse(const SceneDev& S, V3 o, V3 d, float tmin, float tmax_in, bool camera, TraceResult& res,
-                    uint32_t* err, uint64_t* stack) {
+// A traversal stack in one per-thread array.
+struct FlatStack {
+    uint64_t* p;
+    RTG_D void put(int k, uint64_t v) { p[k] = v; }
+    RTG_D uint64_t get(int k) const { return p[k]; }
+};
+
+// A traversal stack whose first SHORT_STACK entries sit in shared memory, interleaved by thread
+// (entry k of thread i at sm[k * stride + i]), and the deeper ones in a per-thread array. Almost
+// every ray stays within the shared part.
+constexpr int SHORT_STACK = 24;
+struct SplitStack {
+    uint64_t* sm;   // this thread's column of the shared block
+    uint64_t* deep; // STACK_CAP - SHORT_STACK entries
+    int stride;
+    RTG_D void put(int k, uint64_t v) {
+        if (k < SHORT_STACK) sm[k * stride] = v;
+        else deep[k - SHORT_STACK] = v;
+    }
+    RTG_D uint64_t get(int k) const { return k < SHORT_STACK ? sm[k * stride] : deep[k - SHORT_STACK]; }
+};
+
+// The traversal state of one ray, advanced one node or leaf per trav_step. A kernel can then give
+// a lane whose ray has finished a new ray while the rest of its warp keeps traversing.
+struct Trav {
+    PRay R;          // the ray in the space of the tree being walked (the world ray at level 0)
+    V3 o, d;         // the world ray, rebuilt into R on the way back from an instanced tree
+    float tmin, tmax;
+    float best_t;
+    uint32_t best_i, best_tri, cur, b_inst, b_flags;
+    int sp, level;
+    bool camera;
+};
+
+// Sets up a query. False when the ray can meet nothing (non-finite or zero direction, empty
+// interval): a miss.
+RTG_D bool trav_init(const SceneDev& S, Trav& T, V3 o, V3 d, float tmin, float tmax, bool camera) {
     if (!(vfinite(o) && vfinite(d) && !veq(d, v3(0, 0, 0)))) return false;
-    const PRay W = prepare_ray(o, d, tmin, tmax_in);
-    if (!(W.tmin <= W.tmax)) return false;
-    PRay R = W;
-    float best_t = W.tmax;
-    uint32_t best_i = 0xffffffffu, best_tri = 0xffffffffu;
-    uint32_t cur = S.tlas_root;
-    int sp = 0;
-    int level = 0;
-    uint32_t b_inst = 0xffffffffu, b_flags = 0;
-    for (;;) {
-        if ((cur & NODE_LEAF) == 0) {
-            float nr[8];
-            uint32_t child[8];
-            uint32_t bits = node_test(S.nodes + cur, R, best_t, nr, child);
-            if (bits) {
-                if ((bits & (bits - 1)) == 0) {
-                    cur = child[__ffs(bits) - 1];
-                    continue;
-                }
-                if (sp + 8 > STACK_CAP) { *err |= 1u; return false; }
-                if (ANY) {
-                    int first = __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    while (bits) {
-                        int s = __ffs(bits) - 1;
-                        bits &= bits - 1;
-                        stack[sp++] = stack_key(nr[s], child[s]);
-                    }
-                    cur = child[first];
-                } else {
-                    uint64_t keys[8];
-                    int count = 0;
-                    while (bits) {
-                        int s = __ffs(bits) - 1;
-                        bits &= bits - 1;
-                        uint64_t key = stack_key(nr[s], child[s]);
-                        int j = count;
-                        while (j > 0 && keys[j - 1] < key) { keys[j] = keys[j - 1]; --j; }
-                        keys[j] = key;
-                        ++count;
-                    }
-                    for (int k = 0; k < count - 1; ++k) stack[sp++] = keys[k];
-                    cur = (uint32_t)keys[count - 1];
-                }
-                continue;
-            }
-        } else if (cur != NODE_EMPTY) {
-            uint32_t first = (cur & ~NODE_LEAF) >> 4, count = (cur & 15u) + 1;
-            if (level == 0) {
-                const BlasInst* bi = S.blas + first;
-                uint32_t flags = __ldg(&bi->flags);
-                if (!(camera && (flags & 2u))) {
-                    if (sp + 1 > STACK_CAP) { *err |= 1u; return false; }
-                    stack[sp++] = stack_key(0.0f, STACK_RETURN);
-                    if (__ldg(&bi->identity)) {
-                        R = W;
-                    } else {
-                        float m[12];
+    T.R = prepare_ray(o, d, tmin, tmax);
+    if (!(T.R.tmin <= T.R.tmax)) return false;
+    T.o = o;
+    T.d = d;
+    T.tmin = T.R.tmin;
+    T.tmax = T.R.tmax;
+    T.best_t = T.R.tmax;
+    T.best_i = 0xffffffffu;
+    T.best_tri = 0xffffffffu;
+    T.cur = S.tlas_root;
+    T.b_inst = 0xffffffffu;
+    T.b_flags = 0;
+    T.sp = 0;
+    T.level = 0;
+    T.camera = camera;
+    return true;
+}
+
+// One step of the two-level traversal: the slab test of one node, or the triangles of one leaf,
+// then the next node (a child, or the nearest entry of the stack that is still in range).
+// `ANY`: stop at the first hit in [t_min, t_max] (shadow rays; children in slot order). Otherwise
+// the nearest hit with the reference's tie-break, children nearest first. Returns true when the
+// query is over; `hit` then says whether it found one (nearest: in T.best_*). A stack that would
+// overflow sets *err bit 0 and ends the query as a miss.
+template <bool ANY, class Stack>
+RTG_D bool trav_step(const SceneDev& S, Trav& T, Stack& stack, uint32_t* err, bool& hit) {
+    const uint32_t cur = T.cur;
+    if ((cur & NODE_LEAF) == 0) {
+        float nr[8];
+        uint32_t child[8];
+        const uint32_t bits = node_test(S.nodes + cur, T.R, T.best_t, nr, child);
+        // Every array index below is a constant after unrolling, so nr, child and key stay in
+        // registers.
+        if (bits) {
+            uint32_t next = 0;
+            if ((bits & (bits - 1)) == 0) {
 #pragma unroll
-                        for (int k = 0; k < 12; ++k) m[k] = __ldg(&bi->to_local[k]);
-                        R = prepare_ray(xf_point(m, o), xf_vector(m, d), tmin, tmax_in);
+                for (int c = 0; c < 8; ++c)
+                    if (bits == (1u << c)) next = child[c];
+                T.cur = next;
+                return false;
+            }
+            if (T.sp + 8 > STACK_CAP) { *err |= 1u; hit = false; return true; }
+            if (ANY) {
+                // Slot order: the lowest slot next, the others pushed lowest first.
+                const uint32_t first = bits & (0u - bits);
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    if ((bits >> c) & 1u) {
+                        if ((1u << c) == first) next = child[c];
+                        else stack.put(T.sp++, stack_key(nr[c], child[c]));
                     }
-                    b_inst = __ldg(&bi->instance);
-                    b_flags = flags;
-                    level = 1;
-                    cur = __ldg(&bi->root);
-                    continue;
                 }
             } else {
-                for (uint32_t k = first; k < first + count; ++k) {
-                    const float4* tr = reinterpret_cast<const float4*>(S.tris + k);
-                    float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
-                    uint32_t flags = __float_as_uint(c.w) | b_flags;
-                    if (camera && (flags & 2u)) continue;
-                    float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
-                    float t, uu, vv, ww, det;
-                    if (watertight(R, v0, v1, v2, ANY ? R.tmax : best_t, (flags & 1u) != 0, t, uu, vv, ww, det)) {
-                        uint32_t inst = __float_as_uint(b.w);
-                        if (inst == 0xffffffffu) inst = b_inst;
-                        uint32_t tri = __float_as_uint(a.w);
-                        if (ANY) { res.inst = inst; res.tri = tri; res.t = t; return true; }
-                        if (t < best_t || (t == best_t && (inst < best_i || (inst == best_i && tri < best_tri)))) {
-                            best_t = t; best_i = inst; best_tri = tri;
-                        }
+                // Nearest first: push the others farthest first (descending (t, ref) keys), so
+                // the nearest remaining child is popped next.
+                uint64_t key[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) key[c] = stack_key(nr[c], child[c]);
+                uint32_t live = bits;
+                for (int left = __popc(bits); left > 1; --left) {
+                    uint64_t top = 0;
+                    uint32_t pick = 0;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        if (((live >> c) & 1u) && (pick == 0 || key[c] > top)) { top = key[c]; pick = 1u << c; }
+                    stack.put(T.sp++, top);
+                    live &= ~pick;
+                }
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    if (live == (1u << c)) next = child[c];
+            }
+            T.cur = next;
+            return false;
+        }
+    } else if (cur != NODE_EMPTY) {
+        uint32_t first = (cur & ~NODE_LEAF) >> 4, count = (cur & 15u) + 1;
+        if (T.level == 0) {
+            const BlasInst* bi = S.blas + first;
+            uint32_t flags = __ldg(&bi->flags);
+            if (!(T.camera && (flags & 2u))) {
+                if (T.sp + 1 > STACK_CAP) { *err |= 1u; hit = false; return true; }
+                stack.put(T.sp++, stack_key(0.0f, STACK_RETURN));
+                if (!__ldg(&bi->identity)) {
+                    float m[12];
+#pragma unroll
+                    for (int k = 0; k < 12; ++k) m[k] = __ldg(&bi->to_local[k]);
+                    T.R = prepare_ray(xf_point(m, T.o), xf_vector(m, T.d), T.tmin, T.tmax);
+                }
+                T.b_inst = __ldg(&bi->instance);
+                T.b_flags = flags;
+                T.level = 1;
+                T.cur = __ldg(&bi->root);
+                return false;
+            }
+        } else {
+            for (uint32_t k = first; k < first + count; ++k) {
+                const float4* tr = reinterpret_cast<const float4*>(S.tris + k);
+                float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
+                uint32_t flags = __float_as_uint(c.w) | T.b_flags;
+                if (T.camera && (flags & 2u)) continue;
+                float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
+                float t, uu, vv, ww, det;
+                if (watertight(T.R, v0, v1, v2, ANY ? T.R.tmax : T.best_t, (flags & 1u) != 0, t, uu, vv, ww, det)) {
+                    if (ANY) { hit = true; return true; }
+                    uint32_t inst = __float_as_uint(b.w);
+                    if (inst == 0xffffffffu) inst = T.b_inst;
+                    uint32_t tri = __float_as_uint(a.w);
+                    if (t < T.best_t || (t == T.best_t && (inst < T.best_i || (inst == T.best_i && tri < T.best_tri)))) {
+                        T.best_t = t; T.best_i = inst; T.best_tri = tri;
                     }
                 }
             }
         }
-        for (;;) {
-            if (sp == 0) {
-                if (ANY || best_i == 0xffffffffu) return false;
-                res.inst = best_i; res.tri = best_tri; res.t = best_t;
-                return true;
-            }
-            uint64_t e = stack[--sp];
-            uint32_t ref = (uint32_t)e;
-            if (ref == STACK_RETURN) { level = 0; R = W; continue; }
-            float t = __uint_as_float((uint32_t)(e >> 32));
-            if (t <= (ANY ? W.tmax : best_t) * RTG_ROBUST) { cur = ref; break; }
-        }
     }
+    for (;;) {
+        if (T.sp == 0) {
+            hit = !ANY && T.best_i != 0xffffffffu;
+            return true;
+        }
+        uint64_t e = stack.get(--T.sp);
+        uint32_t ref = (uint32_t)e;
+        if (ref == STACK_RETURN) {
+            T.level = 0;
+            T.R = prepare_ray(T.o, T.d, T.tmin, T.tmax);
+            continue;
+        }
+        float t = __uint_as_float((uint32_t)(e >> 32));
+        if (t <= (ANY ? T.tmax : T.best_t) * RTG_ROBUST) { T.cur = ref; return false; }
+    }
+}
+
+// A whole query: false on a miss. Nearest-hit queries fill `res`.
+template <bool ANY, class Stack>
+RTG_D bool traverse(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, bool camera, TraceResult& res, uint32_t* err,
+                    Stack& stack) {
+    Trav T;
+    if (!trav_init(S, T, o, d, tmin, tmax, camera)) return false;
+    bool hit = false;
+    while (!trav_step<ANY>(S, T, stack, err, hit)) {
+    }
+    if (hit && !ANY) { res.inst = T.best_i; res.tri = T.best_tri; res.t = T.best_t; }
+    return hit;
 }
 
 struct HitInfo {
