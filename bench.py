@@ -41,6 +41,10 @@ WORKLOAD = ("1080p product scene: 1920x1080, 64 spp, max depth 12, seeded displa
 DATA = "synthetic (seeded procedural scene; no dataset)"
 FALLBACK_HBM_GBS = 6650.0
 BYTES_RAY_IO = 32 + 12  # ray in, hit out
+# DRAM bytes (read + write) per extend ray, from one full ncu capture of k_extend on this scene
+# (bounce 0 of a 4 Mi-path wave: 286 MB for 4,147,200 rays; profiles/k_extend_k_shadow_k_shade_
+# 1080p_product_4Mi_wave.md). Scaled to a launch by the rays it traces.
+DRAM_BYTES_PER_EXTEND_RAY = 69.0
 
 
 def peaks():
@@ -173,6 +177,7 @@ def run_ours(args, world, rank, local, dist):
     import torch
 
     import repackshot_b200 as rtg
+    from repackshot_b200 import shards
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     hbm_peak, peak_src = peaks()
@@ -188,7 +193,7 @@ def run_ours(args, world, rank, local, dist):
     scene.set_stream(stream.cuda_stream)
     film = scene.film()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    base = rank * SPP  # each rank its own sample range: a replica frame per rank
+    base, _ = shards.sample_range(rank, world, SPP)  # each rank its own sample range: a replica frame per rank
 
     def barrier():
         if dist is not None:
@@ -214,13 +219,7 @@ def run_ours(args, world, rank, local, dist):
     clk = clocks.stop() if clocks else None
     ext_ms, ext_launches, ext_rays, shadow_rays, launches = scene.timing(False)
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    local_ms = sum(step_ms)
-    if dist is not None:
-        t = torch.tensor([local_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    else:
-        total_ms = local_ms
+    total_ms = shards.max_over_ranks(sum(step_ms), dist)
     paths_step = WIDTH * HEIGHT * SPP
     value = world * args.steps * paths_step / (total_ms / 1e3) / 1e6
 
@@ -235,11 +234,7 @@ def run_ours(args, world, rank, local, dist):
         film.render(base, SPP)
         film.read(host)
     torch.cuda.synchronize(dev)
-    e2e_local = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_local], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_local = float(t.item())
+    e2e_local = shards.max_over_ranks(time.perf_counter() - t0, dist)
     e2e_value = world * e2e_steps * paths_step / e2e_local / 1e6
     img = film.resolve()
 
@@ -268,12 +263,15 @@ def run_ours(args, world, rank, local, dist):
         "dtype": "f32", "data": DATA,
         "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": DEPTH,
                    "triangles": scene.triangles, "paths_per_step_per_gpu": paths_step,
-                   "l2": "flushed between steps (512 MiB write); per-step working set (path state 640 MB) exceeds L2",
+                   "l2": "flushed between steps (512 MiB write); the per-step working set (2.8 GB of path state) exceeds L2",
                    "parallelism": f"replicas x{world}: each rank renders its own sample range of the frame",
                    "scene_gen_s": round(gen_s, 3), "scene_load_s": round(load_s, 3), "bvh_build_s": round(scene.build_seconds, 3)},
         "mrays_per_s": world * rays / (total_ms / 1e3) / 1e6 if rank == 0 else None,
         "roofline": {"kernel": "k_extend (nearest-hit traversal)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_src, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_src,
+                     "traffic": DRAM_BYTES_PER_EXTEND_RAY * ext_rays / max(ext_launches, 1),
+                     "traffic_note": "dram read + write bytes per extend launch: the ncu figure per ray (a 4 Mi-path "
+                                     "wave) times this run's mean rays per launch; the BVH is L2-resident",
                      "bytes_per_ray": b_ray, "bytes_per_ray_reference_two_level": b_ray_two_level,
                      "frac_reference_two_level": ext_rays * b_ray_two_level / (ext_ms / 1e3) / 1e9 / hbm_peak if ext_ms > 0 else None,
                      "extend_ms_per_launch": ext_ms / max(ext_launches, 1),
@@ -283,7 +281,7 @@ def run_ours(args, world, rank, local, dist):
                              "launch). Bytes per ray: 44 B ray I/O + 256 B per wide node + 160 B per 4-triangle packet of the "
                              "reference BVH8 layout, visits counted by the oracle on this workload's own paths in one reference-"
                              "layout BVH8 over all triangles; the reference's own two-level tree of 16 interleaved per-material "
-                             "instances visits ~10x more (bytes_per_ray_reference_two_level). traffic: see profiles/"},
+                             "instances visits ~10x more (bytes_per_ray_reference_two_level)."},
         "cpu_baseline": {"value": cpu_value, "unit": "Mpaths/s", "cores": threads, "kind": "port",
                          "sample": f"{len(bands)} bands of 8 rows x 1920 px spread over the frame at {spp_cpu} spp "
                                    "(C++ restatement of the reference, bit-exact with its pinned hashes)"},
