@@ -77,6 +77,37 @@ uint32_t rtg_film_clear(uint32_t film);
  * accumulate. `rays` (may be null) receives the camera + extension + shadow rays cast. */
 uint32_t rtg_render_progressive(uint32_t scene, uint32_t film, uint32_t first_sample, uint32_t count, uint64_t* rays);
 
+/* No counterpart in the reference. rtg_render_progressive without device allocation, for
+ * callers that cannot call cudaMalloc while they render: a host that has handed the device's
+ * memory to its own pool allocator, or a render server that must not meet an out-of-memory
+ * error in the middle of a frame. (The scene and the film are allocated when they are created,
+ * as before; only the per-wave path state differs.)
+ *
+ * The path state lives in one fixed array of RTG_NOALLOC_SCRATCH_BYTES (12 MiB) in the
+ * library's device code. Every GPU that loads the library holds that array until the process
+ * exits, whether or not this function is called. A wave holds at most RTG_NOALLOC_MAX_PATHS
+ * paths, so the film is rendered in bands of rows and waves of samples that fit; any film of a
+ * loadable scene (images are at most 16384 pixels wide) is accepted. A row wider than
+ * RTG_NOALLOC_MAX_PATHS pixels would not fit and is refused with RTG_STATUS_BAD_FILM and a
+ * message.
+ *
+ * The first call on each device does the set-up: it looks up the array's address on the
+ * current device (cudaGetSymbolAddress), which may load the library's device code there. Make
+ * that first call before any stream capture. Each call zeroes the array's queue counters
+ * itself before it renders; nothing else in the array has to start at zero.
+ *
+ * There is one array per device, shared by every call on that device. Calls through this
+ * library serialise on its lock and return after their work is complete, so they do not
+ * overlap; work of two calls that ran on the device at the same time would race on the array.
+ *
+ * Arguments, film result and status codes are those of rtg_render_progressive; the film's bits
+ * are the same. Extend-kernel timing (rtg_timing) counts its rays and launches but brackets no
+ * launch with events. */
+#define RTG_NOALLOC_SCRATCH_BYTES (12ull << 20)
+#define RTG_NOALLOC_MAX_PATHS 65536u
+uint32_t rtg_render_progressive_noalloc(uint32_t scene, uint32_t film, uint32_t first_sample, uint32_t count,
+                                        uint64_t* rays);
+
 /* Copies the film's sums to host memory (any pointer may be null): rgb 3*w*h floats, weight,
  * alpha and lum2 w*h floats each. */
 uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2);

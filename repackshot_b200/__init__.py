@@ -46,6 +46,7 @@ ABI = {
     "rtg_film_free": (_u32, [_u32]),
     "rtg_film_clear": (_u32, [_u32]),
     "rtg_render_progressive": (_u32, [_u32, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
+    "rtg_render_progressive_noalloc": (_u32, [_u32, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
     "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_render_paths": (_u32, [_u32, _f, _u32, _f]),
@@ -194,6 +195,13 @@ class Film:
         """Accumulates samples [first, first + count); returns the rays cast."""
         rays = _u64(0)
         _check(lib().rtg_render_progressive(self.scene.handle, self.handle, first, count, ctypes.byref(rays)))
+        return int(rays.value)
+
+    def render_noalloc(self, first: int, count: int) -> int:
+        """As ``render``, with the path state in the library's fixed device array
+        (rtg_render_progressive_noalloc): no device memory is allocated."""
+        rays = _u64(0)
+        _check(lib().rtg_render_progressive_noalloc(self.scene.handle, self.handle, first, count, ctypes.byref(rays)))
         return int(rays.value)
 
     def read(self, out=None):

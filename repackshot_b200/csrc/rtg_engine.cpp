@@ -12,6 +12,7 @@
 
 #include "../../include/repackshot_b200.h"
 #include "rtg_kernels.h"
+#include "rtg_noalloc.h"
 #include "rtg_scene.h"
 #include "rtg_tables.h"
 
@@ -404,6 +405,26 @@ uint32_t rtg_render_progressive(uint32_t handle, uint32_t film, uint32_t first_s
     Film* f = film_of(film);
     if (!f || f->scene != handle) return RTG_STATUS_BAD_FILM;
     return render_region(*sc, f->dev.ox, f->dev.oy, f->dev.w, f->dev.h, first_sample, count, f->dev, rays);
+}
+uint32_t rtg_render_progressive_noalloc(uint32_t handle, uint32_t film, uint32_t first_sample, uint32_t count,
+                                        uint64_t* rays) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    Film* f = film_of(film);
+    if (!f || f->scene != handle) return RTG_STATUS_BAD_FILM;
+    if (rays) *rays = 0;
+    NoallocJob job{&sc->S, sc->d_lights, f->dev, sc->width, sc->height, first_sample, count, sc->stream, g_sms};
+    NoallocResult res;
+    const char* why = "";
+    uint32_t st = noalloc_render(job, res, &why);
+    if (st) { g_error = why; return st; }
+    sc->launches += res.waves * (2 + 6 * (uint64_t)(sc->S.max_depth + 1));
+    sc->rays += res.extend_rays + res.shadow_rays;
+    sc->extend_rays += res.extend_rays;
+    sc->shadow_rays += res.shadow_rays;
+    if (rays) *rays = res.extend_rays + res.shadow_rays;
+    return RTG_STATUS_OK;
 }
 uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2) {
     std::lock_guard<std::mutex> lk(g_mu);
