@@ -306,12 +306,14 @@ uint32_t rtg_version(void) { return RTG_ABI_VERSION; }
 uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!bytes) { g_error = "null pointer"; return 0; }
-    if (device_init() != RTG_STATUS_OK) return 0;
+    // The scene is parsed, checked and flattened on the host before any device work, so a
+    // malformed or unsupported scene is refused the same way with or without a GPU.
     HScene hs;
     std::string err;
     if (!parse_rsb(bytes, len, hs, err)) { g_error = err; return 0; }
     Flat F;
     if (!flatten_scene(hs, F, err)) { g_error = err; return 0; }
+    if (device_init() != RTG_STATUS_OK) return 0;
     auto sc = std::make_unique<Scene>();
     if (cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking) != cudaSuccess) { g_error = "cudaStreamCreate failed"; return 0; }
     sc->S = F.scene;

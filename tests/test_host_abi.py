@@ -1,0 +1,104 @@
+"""The C-ABI library on the CPU: it loads, exports every function include/repackshot_b200.h
+declares (and the Python table binds exactly those), and its host-side logic answers the
+reference's way without a GPU: status codes for bad handles and null pointers
+(engine/crates/rt-wasm/src/lib.rs:37-53), parse errors and "unsupported:" refusals at load
+(rt_scene_load, ffi.rs:56-66), and a loud CUDA error, not a fallback, when no GPU is present.
+No test here launches a kernel.
+"""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "repackshot_b200.h"
+
+
+def header_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:uint32_t|void)\s+(rtg_\w+)\s*\(", text, flags=re.M)))
+
+
+def header_define(name):
+    """The value of an integer #define: a literal or a shift such as (1ull << 22)."""
+    m = re.search(rf"#define\s+{name}\s+([^/\n]+)", HEADER.read_text())
+    expr = re.sub(r"(?<=[0-9a-fA-F])(ull|ul|u)\b", "", m.group(1).strip())
+    assert re.fullmatch(r"[0-9a-fxA-FX()<\s]+", expr), expr
+    return int(eval(expr))
+
+
+@pytest.fixture(scope="module")
+def rtg():
+    import repackshot_b200 as rtg
+    from repackshot_b200 import build
+    build.build()  # no-op when the library is up to date
+    rtg.lib()
+    return rtg
+
+
+def test_header_declares_the_entry_points():
+    names = header_functions()
+    assert "rtg_scene_load" in names and "rtg_render_progressive" in names
+    assert len(names) >= 20
+
+
+def test_library_exports_every_declared_function(rtg):
+    L = ctypes.CDLL(str(rtg.LIB_PATH))
+    missing = [n for n in header_functions() if not hasattr(L, n)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_python_table_binds_exactly_the_header(rtg):
+    assert sorted(rtg.ABI) == header_functions()
+
+
+def test_version_and_constants(rtg):
+    assert rtg.lib().rtg_version() == header_define("RTG_ABI_VERSION")
+    assert rtg.MAX_TILE_PIXELS == header_define("RTG_MAX_TILE_PIXELS")
+    for name in ("OK", "BAD_HANDLE", "BAD_TILE", "NULL_POINTER", "BAD_SCENE", "CUDA_ERROR", "STACK_OVERFLOW", "BAD_FILM"):
+        assert getattr(rtg, "STATUS_" + name) == header_define("RTG_STATUS_" + name)
+
+
+def test_bad_handles_and_null_pointers(rtg):
+    L = rtg.lib()
+    out = (ctypes.c_float * 12)()
+    assert L.rtg_scene_free(0) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_scene_free(4096) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_render_tile(4096, 0, 0, 2, 2, 0, out) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_render_tile_rgba(4096, 0, 0, 1, 1, 0, out) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_film_free(4096) == rtg.STATUS_BAD_FILM
+    assert L.rtg_film_create(4096, 0, 0, 4, 4) == 0
+    assert L.rtg_render_progressive(4096, 1, 0, 1, None) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_scene_load(None, 0) == 0
+    assert rtg.error_message() == "null pointer"
+
+
+def test_malformed_scenes_are_refused_with_a_message(rtg, example_rsb):
+    assert rtg.scene_load(b"not a scene") == 0
+    assert rtg.error_message()
+    assert rtg.scene_load(example_rsb[: len(example_rsb) // 2]) == 0
+    assert rtg.error_message()
+
+
+@pytest.mark.parametrize("change, words", [
+    (lambda s: setattr(s, "env_kind", 2), "sky or HDRI"),
+    (lambda s: setattr(s.lights[0], "kind", 2), "light kind"),
+    (lambda s: setattr(s.materials[0], "bevel_mm", 1.0), "bevel"),
+    (lambda s: setattr(s.materials[0], "opacity", 0.5), "cut-out"),
+])
+def test_features_outside_the_path_are_refused(rtg, change, words):
+    from repackshot_b200 import scenes
+    s = scenes.cfg0_scene()
+    change(s)
+    assert rtg.scene_load(scenes.to_rsb(s)) == 0
+    msg = rtg.error_message()
+    assert msg.startswith("unsupported:") and words in msg
+
+
+def test_without_a_gpu_a_valid_scene_fails_loudly(rtg, cfg0_rsb):
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    assert rtg.scene_load(cfg0_rsb) == 0
+    assert "CUDA" in rtg.error_message()
