@@ -45,6 +45,16 @@ uint32_t rtg_version(void);
  * bevels, the shadow catcher) are refused with a message that starts with "unsupported:". */
 uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len);
 
+/* rt_scene_update (ffi.rs:68-88, rt-wasm/src/lib.rs:171-193, Scene::update_from_rsb
+ * rt-core/src/scene/rsb.rs:1630): replaces the loaded scene with new RSB bytes (copied). A file
+ * without MESH sections keeps the scene's meshes: its INST sections, or the implicit instances of
+ * the kept meshes, refer to them; when the instances' meshes, transforms and visibility flags are
+ * also unchanged, the device trees are kept and only the camera, image size, materials, lights and
+ * settings are uploaded again. Films keep their rectangles. RTG_STATUS_OK, RTG_STATUS_BAD_HANDLE,
+ * RTG_STATUS_NULL_POINTER, or RTG_STATUS_BAD_SCENE with the message in rtg_scene_error_*; on any
+ * error the scene is unchanged. */
+uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len);
+
 /* rt_scene_error_len / rt_scene_error_copy (ffi.rs:90-110): the last error message, UTF-8,
  * without terminator; empty after a successful load. */
 uint32_t rtg_scene_error_len(void);

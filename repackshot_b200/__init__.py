@@ -37,6 +37,7 @@ _u32, _u64, _f = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
 ABI = {
     "rtg_version": (_u32, []),
     "rtg_scene_load": (_u32, [ctypes.c_char_p, _u32]),
+    "rtg_scene_update": (_u32, [_u32, ctypes.c_char_p, _u32]),
     "rtg_scene_error_len": (_u32, []),
     "rtg_scene_error_copy": (None, [ctypes.c_void_p]),
     "rtg_scene_free": (_u32, [_u32]),
@@ -124,10 +125,21 @@ class Scene:
         self.handle = scene_load(rsb)
         if self.handle == 0:
             raise RtgError(STATUS_BAD_SCENE, error_message())
+        self._read_stats()
+
+    def _read_stats(self):
         st = np.zeros(8, np.float64)
         _check(lib().rtg_scene_stats(self.handle, _ptr(st)))
         self.width, self.height, self.max_depth = int(st[0]), int(st[1]), int(st[2])
         self.triangles, self.nodes, self.leaf_triangles, self.build_seconds = int(st[3]), int(st[4]), int(st[5]), float(st[6])
+
+    def update(self, rsb: bytes):
+        """rt_scene_update: replaces the scene; a file without MESH sections keeps the meshes (and,
+        with unchanged instances, the device trees). On error raises and the scene is unchanged."""
+        status = lib().rtg_scene_update(self.handle, rsb, len(rsb))
+        if status != STATUS_OK:
+            raise RtgError(status, error_message())
+        self._read_stats()
 
     def close(self):
         if self.handle:

@@ -42,10 +42,25 @@ struct DevBuf {
     void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
 };
 
+// Device buffers released together.
+struct BufSet {
+    std::vector<DevBuf> bufs;
+    LightsDev* lights = nullptr;
+    void release() {
+        for (auto& b : bufs) b.release();
+        bufs.clear();
+        if (lights) cudaFree(lights);
+        lights = nullptr;
+    }
+};
+
 struct Scene {
     SceneDev S{};
     LightsDev* d_lights = nullptr;
-    std::vector<DevBuf> bufs;
+    BufSet geometry;  // trees, leaf triangles, vertex arrays: kept by updates that keep the meshes
+    BufSet shading;   // instances, materials, BSDFs, lights: replaced by every update
+    std::vector<HMesh> meshes;  // the host meshes, for updates without MESH sections
+    std::string geom_key;
     cudaStream_t stream = nullptr;
     // path buffers
     PathBuffers P{};
@@ -66,9 +81,9 @@ struct Scene {
     uint64_t launches = 0;        // kernels launched since the last timing reset
     bool own_stream = true;       // false after rtg_set_stream: the caller owns the stream
     ~Scene() {
-        for (auto& b : bufs) b.release();
+        geometry.release();
+        shading.release();
         path_mem.release();
-        if (d_lights) cudaFree(d_lights);
         if (wt) {
             for (int i = 0; i < WaveTiming::MAX_EVENTS; ++i) cudaEventDestroy(wt->ev[i]);
             delete wt;
@@ -125,15 +140,51 @@ uint32_t device_init() {
 }
 
 template <class T>
-uint32_t upload(Scene& sc, const std::vector<T>& v, const T*& out) {
+uint32_t upload(BufSet& set, const std::vector<T>& v, const T*& out) {
     DevBuf b;
     b.bytes = v.size() * sizeof(T);
     if (b.bytes == 0) { out = nullptr; return RTG_STATUS_OK; }
     RTG_CHECK(cudaMalloc(&b.p, b.bytes));
-    sc.bufs.push_back(b);
+    set.bufs.push_back(b);
     RTG_CHECK(cudaMemcpy(b.p, v.data(), b.bytes, cudaMemcpyHostToDevice));
     out = (const T*)b.p;
     return RTG_STATUS_OK;
+}
+
+// Uploads the trees, leaf triangles and hit-detail arrays of `F` into `set`, pointers into `S`.
+uint32_t upload_geometry(const Flat& F, BufSet& set, SceneDev& S) {
+    std::vector<float4> pos(F.positions.size() / 4), nrm(F.normals.size() / 4);
+    std::memcpy(pos.data(), F.positions.data(), F.positions.size() * 4);
+    std::memcpy(nrm.data(), F.normals.data(), F.normals.size() * 4);
+    std::vector<uint4> ti(F.tri_index.size() / 4);
+    std::memcpy(ti.data(), F.tri_index.data(), F.tri_index.size() * 4);
+    uint32_t st;
+    if ((st = upload(set, F.nodes, S.nodes)) || (st = upload(set, F.tris, S.tris)) || (st = upload(set, F.blas, S.blas)) ||
+        (st = upload(set, pos, S.positions)) || (st = upload(set, nrm, S.normals)) || (st = upload(set, ti, S.tri_index)))
+        return st;
+    return RTG_STATUS_OK;
+}
+
+// Uploads instances, materials, BSDFs and lights of `F` into `set`, pointers into `S`.
+uint32_t upload_shading(const Flat& F, BufSet& set, SceneDev& S) {
+    uint32_t st;
+    if ((st = upload(set, F.instances, S.instances)) || (st = upload(set, F.materials, S.materials)) ||
+        (st = upload(set, F.bsdfs, S.bsdfs)))
+        return st;
+    RTG_CHECK(cudaMalloc(&set.lights, sizeof(LightsDev)));
+    RTG_CHECK(cudaMemcpy(set.lights, &F.lights, sizeof(LightsDev), cudaMemcpyHostToDevice));
+    return RTG_STATUS_OK;
+}
+
+// The scene constants of `F` with the device pointers and tree fields of `geom` and `shade`.
+SceneDev compose(const SceneDev& constants, const SceneDev& geom, const SceneDev& shade) {
+    SceneDev S = constants;
+    S.nodes = geom.nodes; S.tris = geom.tris; S.blas = geom.blas;
+    S.positions = geom.positions; S.normals = geom.normals; S.tri_index = geom.tri_index;
+    S.tlas_root = geom.tlas_root; S.stack_need = geom.stack_need;
+    S.instances = shade.instances; S.materials = shade.materials; S.bsdfs = shade.bsdfs;
+    S.energy = g_energy;
+    return S;
 }
 
 uint32_t ensure_capacity(Scene& sc, uint32_t paths) {
@@ -316,22 +367,12 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     if (device_init() != RTG_STATUS_OK) return 0;
     auto sc = std::make_unique<Scene>();
     if (cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking) != cudaSuccess) { g_error = "cudaStreamCreate failed"; return 0; }
-    sc->S = F.scene;
-    std::vector<float4> pos(F.positions.size() / 4), nrm(F.normals.size() / 4);
-    std::memcpy(pos.data(), F.positions.data(), F.positions.size() * 4);
-    std::memcpy(nrm.data(), F.normals.data(), F.normals.size() * 4);
-    std::vector<uint4> ti(F.tri_index.size() / 4);
-    std::memcpy(ti.data(), F.tri_index.data(), F.tri_index.size() * 4);
-    if (upload(*sc, F.nodes, sc->S.nodes) || upload(*sc, F.tris, sc->S.tris) || upload(*sc, F.blas, sc->S.blas) ||
-        upload(*sc, F.instances, sc->S.instances) || upload(*sc, pos, sc->S.positions) || upload(*sc, nrm, sc->S.normals) ||
-        upload(*sc, ti, sc->S.tri_index) || upload(*sc, F.materials, sc->S.materials) || upload(*sc, F.bsdfs, sc->S.bsdfs))
-        return 0;
-    if (cudaMalloc(&sc->d_lights, sizeof(LightsDev)) != cudaSuccess ||
-        cudaMemcpy(sc->d_lights, &F.lights, sizeof(LightsDev), cudaMemcpyHostToDevice) != cudaSuccess) {
-        g_error = "CUDA error uploading lights";
-        return 0;
-    }
-    sc->S.energy = g_energy;
+    SceneDev geom = F.scene, shade = F.scene;
+    if (upload_geometry(F, sc->geometry, geom) || upload_shading(F, sc->shading, shade)) return 0;
+    sc->S = compose(F.scene, geom, shade);
+    sc->d_lights = sc->shading.lights;
+    sc->meshes = std::move(hs.meshes);
+    sc->geom_key = geometry_key(hs);
     sc->build_seconds = F.build_seconds;
     sc->nodes = F.nodes.size();
     sc->tris = F.tris.size();
@@ -344,6 +385,56 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
         if (!g_scenes[i]) { g_scenes[i] = std::move(sc); return (uint32_t)i + 1; }
     g_scenes.push_back(std::move(sc));
     return (uint32_t)g_scenes.size();
+}
+
+uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (!bytes) { g_error = "rtg_scene_update: null pointer"; return RTG_STATUS_NULL_POINTER; }
+    HScene hs;
+    std::string err;
+    bool kept = false;
+    if (!parse_rsb(bytes, len, hs, err, &sc->meshes, &kept)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
+    std::string key = geometry_key(hs);
+    const bool same_geometry = kept && key == sc->geom_key;
+    Flat F;
+    if (!flatten_scene(hs, F, err, !same_geometry)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
+    // Everything new is uploaded first; the scene changes only once all of it is on the device.
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    BufSet geometry, shading;
+    SceneDev geom = sc->S, shade = F.scene;
+    uint32_t st = same_geometry ? RTG_STATUS_OK : upload_geometry(F, geometry, geom);
+    if (!st) st = upload_shading(F, shading, shade);
+    if (st) {
+        geometry.release();
+        shading.release();
+        return st;
+    }
+    if (same_geometry) {
+        geom.tlas_root = sc->S.tlas_root;
+        geom.stack_need = sc->S.stack_need;
+    } else {
+        geom.tlas_root = F.scene.tlas_root;
+        geom.stack_need = F.scene.stack_need;
+        sc->geometry.release();
+        sc->geometry = std::move(geometry);
+        sc->nodes = F.nodes.size();
+        sc->tris = F.tris.size();
+        sc->build_seconds = F.build_seconds;
+    }
+    sc->shading.release();
+    sc->shading = std::move(shading);
+    sc->S = compose(F.scene, geom, shade);
+    sc->d_lights = sc->shading.lights;
+    if (!kept) sc->meshes = std::move(hs.meshes);
+    sc->geom_key = std::move(key);
+    sc->instanced_triangles = F.instanced_triangles;
+    sc->width = F.scene.width;
+    sc->height = F.scene.height;
+    sc->max_depth = F.scene.max_depth;
+    g_error.clear();
+    return RTG_STATUS_OK;
 }
 
 uint32_t rtg_scene_error_len(void) {

@@ -73,8 +73,10 @@ const char* make_mesh(HMesh& m, std::vector<V3>&& p, std::vector<V3>&& nn, std::
 }
 }  // namespace
 
-bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error) {
+bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, const std::vector<HMesh>* kept, bool* used_kept) {
     s = HScene();
+    if (used_kept) *used_kept = false;
+    bool seen_mesh = false;
     if (len < 4 || std::memcmp(bytes, "RSB1", 4) != 0) { error = "not an RSB file (missing RSB1 magic)"; return false; }
     if (len < 8) { error = "RSB file is truncated in header"; return false; }
     uint32_t header_len;
@@ -111,6 +113,7 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error) 
             if (s.exterior < 0.0f) return r.invalid("exterior must not be negative");
             if (s.projection == 1 || s.projection == 2) { error = "unsupported: panoramic camera projection"; return false; }
         } else if (is("MESH")) {
+            seen_mesh = true;
             uint32_t vc, ic;
             if (!(r.u32(vc) && r.u32(ic))) return false;
             if (((uint64_t)vc * 6 + ic + 1) * 4 > r.remaining()) return r.too_short();
@@ -206,6 +209,10 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error) 
             for (const char* t : feature_tags)
                 if (is(t)) { error = std::string("unsupported: RSB section ") + t; return false; }
         }
+    }
+    if (!seen_mesh && kept) {
+        s.meshes = *kept;
+        if (used_kept) *used_kept = true;
     }
     size_t nm = s.materials.size();
     for (const HMesh& m : s.meshes)
@@ -611,7 +618,22 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
     return true;
 }
 
-bool flatten_scene(const HScene& s, Flat& F, std::string& error) {
+std::string geometry_key(const HScene& s) {
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    uint64_t nm = s.meshes.size(), ni = s.instances.size();
+    put(&nm, 8);
+    put(&ni, 8);
+    for (const HInstance& in : s.instances) {
+        uint32_t vis = in.flags & 5u;  // one-sided, hidden to the camera: stored in the leaves
+        put(&in.mesh, 4);
+        put(in.rows, sizeof(in.rows));
+        put(&vis, 4);
+    }
+    return k;
+}
+
+bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) {
     auto t0 = std::chrono::steady_clock::now();
     F = Flat();
     const size_t ni = s.instances.size();
@@ -624,25 +646,27 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error) {
         nv += (uint32_t)s.meshes[m].positions.size();
         nt += (uint32_t)s.meshes[m].triangles();
     }
-    F.positions.resize((size_t)nv * 4);
-    F.normals.assign((size_t)nv * 4, 0.0f);
-    F.tri_index.resize((size_t)nt * 4);
-    for (size_t m = 0; m < s.meshes.size(); ++m) {
-        const HMesh& M = s.meshes[m];
-        for (size_t v = 0; v < M.positions.size(); ++v) {
-            float* p = &F.positions[((size_t)vtx_base[m] + v) * 4];
-            p[0] = M.positions[v].x; p[1] = M.positions[v].y; p[2] = M.positions[v].z; p[3] = 0;
-            if (!M.normals.empty()) {
-                float* n = &F.normals[((size_t)vtx_base[m] + v) * 4];
-                n[0] = M.normals[v].x; n[1] = M.normals[v].y; n[2] = M.normals[v].z;
+    if (geometry) {
+        F.positions.resize((size_t)nv * 4);
+        F.normals.assign((size_t)nv * 4, 0.0f);
+        F.tri_index.resize((size_t)nt * 4);
+        for (size_t m = 0; m < s.meshes.size(); ++m) {
+            const HMesh& M = s.meshes[m];
+            for (size_t v = 0; v < M.positions.size(); ++v) {
+                float* p = &F.positions[((size_t)vtx_base[m] + v) * 4];
+                p[0] = M.positions[v].x; p[1] = M.positions[v].y; p[2] = M.positions[v].z; p[3] = 0;
+                if (!M.normals.empty()) {
+                    float* n = &F.normals[((size_t)vtx_base[m] + v) * 4];
+                    n[0] = M.normals[v].x; n[1] = M.normals[v].y; n[2] = M.normals[v].z;
+                }
             }
-        }
-        for (size_t t = 0; t < M.triangles(); ++t) {
-            uint32_t* ti = &F.tri_index[((size_t)tri_base[m] + t) * 4];
-            ti[0] = vtx_base[m] + M.indices[3 * t];
-            ti[1] = vtx_base[m] + M.indices[3 * t + 1];
-            ti[2] = vtx_base[m] + M.indices[3 * t + 2];
-            ti[3] = (uint32_t)m;
+            for (size_t t = 0; t < M.triangles(); ++t) {
+                uint32_t* ti = &F.tri_index[((size_t)tri_base[m] + t) * 4];
+                ti[0] = vtx_base[m] + M.indices[3 * t];
+                ti[1] = vtx_base[m] + M.indices[3 * t + 1];
+                ti[2] = vtx_base[m] + M.indices[3 * t + 2];
+                ti[3] = (uint32_t)m;
+            }
         }
     }
     // Instances.
@@ -715,133 +739,135 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error) {
         }
         F.bsdfs.push_back(bsdf_lambert(rgb(s.floor_color[0], s.floor_color[1], s.floor_color[2])));
     }
-    // Bottom level: one world-space tree over the triangles of every identity instance (the
-    // nearest hit does not depend on the tree, so they can share one), one object-space tree per
-    // mesh used by a transformed instance.
-    Flattener fl{F};
-    uint32_t blas_depth = 0;
-    std::vector<BlasInst> tlas_leaves;
-    std::vector<Box> tlas_boxes;
-    {
-        std::vector<std::pair<uint32_t, uint32_t>> prims;  // (instance, triangle)
-        for (size_t i = 0; i < ni; ++i)
-            if (live[i] && ident[i])
-                for (uint32_t t = 0; t < s.meshes[s.instances[i].mesh].triangles(); ++t) prims.push_back({(uint32_t)i, t});
-        if (!prims.empty()) {
-            std::vector<Box> boxes(prims.size());
-            std::vector<V3> cents(prims.size());
-            Box all;
-            for (size_t k = 0; k < prims.size(); ++k) {
-                const HMesh& M = s.meshes[s.instances[prims[k].first].mesh];
-                uint32_t t = prims[k].second;
-                Box b = Box().ext(M.positions[M.indices[3 * t]]).ext(M.positions[M.indices[3 * t + 1]]).ext(M.positions[M.indices[3 * t + 2]]);
-                boxes[k] = b;
-                cents[k] = b.centroid();
-                all = all.uni(b);
-            }
-            SahBuilder sb{boxes, cents, 4, 8, {}, {}};
-            sb.order.resize(prims.size());
-            for (size_t k = 0; k < prims.size(); ++k) sb.order[k] = (uint32_t)k;
-            sb.build(0, prims.size(), 0);
-            fl.bn = &sb.nodes;
-            fl.order = &sb.order;
-            fl.max_depth = 0;
-            fl.emit = [&](const uint32_t* p, uint32_t n) {
-                uint32_t first = (uint32_t)F.tris.size();
-                for (uint32_t k = 0; k < n; ++k) {
-                    uint32_t inst = prims[p[k]].first, t = prims[p[k]].second;
-                    const HMesh& M = s.meshes[s.instances[inst].mesh];
-                    TriRec r;
-                    const V3& a = M.positions[M.indices[3 * t]];
-                    const V3& b = M.positions[M.indices[3 * t + 1]];
-                    const V3& c = M.positions[M.indices[3 * t + 2]];
-                    r.v0[0] = a.x; r.v0[1] = a.y; r.v0[2] = a.z; r.tri = t;
-                    r.v1[0] = b.x; r.v1[1] = b.y; r.v1[2] = b.z; r.inst = inst;
-                    r.v2[0] = c.x; r.v2[1] = c.y; r.v2[2] = c.z;
-                    r.flags = (s.instances[inst].flags & 1u) | ((s.instances[inst].flags & 4u) ? 2u : 0u);
-                    F.tris.push_back(r);
+    if (geometry) {
+        // Bottom level: one world-space tree over the triangles of every identity instance (the
+        // nearest hit does not depend on the tree, so they can share one), one object-space tree per
+        // mesh used by a transformed instance.
+        Flattener fl{F};
+        uint32_t blas_depth = 0;
+        std::vector<BlasInst> tlas_leaves;
+        std::vector<Box> tlas_boxes;
+        {
+            std::vector<std::pair<uint32_t, uint32_t>> prims;  // (instance, triangle)
+            for (size_t i = 0; i < ni; ++i)
+                if (live[i] && ident[i])
+                    for (uint32_t t = 0; t < s.meshes[s.instances[i].mesh].triangles(); ++t) prims.push_back({(uint32_t)i, t});
+            if (!prims.empty()) {
+                std::vector<Box> boxes(prims.size());
+                std::vector<V3> cents(prims.size());
+                Box all;
+                for (size_t k = 0; k < prims.size(); ++k) {
+                    const HMesh& M = s.meshes[s.instances[prims[k].first].mesh];
+                    uint32_t t = prims[k].second;
+                    Box b = Box().ext(M.positions[M.indices[3 * t]]).ext(M.positions[M.indices[3 * t + 1]]).ext(M.positions[M.indices[3 * t + 2]]);
+                    boxes[k] = b;
+                    cents[k] = b.centroid();
+                    all = all.uni(b);
                 }
-                return make_leaf(first, n);
-            };
-            uint32_t root = fl.reference(0, 0);
-            blas_depth = std::max(blas_depth, fl.max_depth);
+                SahBuilder sb{boxes, cents, 4, 8, {}, {}};
+                sb.order.resize(prims.size());
+                for (size_t k = 0; k < prims.size(); ++k) sb.order[k] = (uint32_t)k;
+                sb.build(0, prims.size(), 0);
+                fl.bn = &sb.nodes;
+                fl.order = &sb.order;
+                fl.max_depth = 0;
+                fl.emit = [&](const uint32_t* p, uint32_t n) {
+                    uint32_t first = (uint32_t)F.tris.size();
+                    for (uint32_t k = 0; k < n; ++k) {
+                        uint32_t inst = prims[p[k]].first, t = prims[p[k]].second;
+                        const HMesh& M = s.meshes[s.instances[inst].mesh];
+                        TriRec r;
+                        const V3& a = M.positions[M.indices[3 * t]];
+                        const V3& b = M.positions[M.indices[3 * t + 1]];
+                        const V3& c = M.positions[M.indices[3 * t + 2]];
+                        r.v0[0] = a.x; r.v0[1] = a.y; r.v0[2] = a.z; r.tri = t;
+                        r.v1[0] = b.x; r.v1[1] = b.y; r.v1[2] = b.z; r.inst = inst;
+                        r.v2[0] = c.x; r.v2[1] = c.y; r.v2[2] = c.z;
+                        r.flags = (s.instances[inst].flags & 1u) | ((s.instances[inst].flags & 4u) ? 2u : 0u);
+                        F.tris.push_back(r);
+                    }
+                    return make_leaf(first, n);
+                };
+                uint32_t root = fl.reference(0, 0);
+                blas_depth = std::max(blas_depth, fl.max_depth);
+                BlasInst bi;
+                std::memset(&bi, 0, sizeof(bi));
+                bi.root = root;
+                bi.identity = 1;
+                bi.instance = 0xffffffffu;
+                tlas_leaves.push_back(bi);
+                tlas_boxes.push_back(all);
+            }
+        }
+        std::map<uint32_t, uint32_t> mesh_root;
+        for (size_t i = 0; i < ni; ++i) {
+            if (!live[i] || ident[i]) continue;
+            uint32_t m = s.instances[i].mesh;
+            if (!mesh_root.count(m)) {
+                const HMesh& M = s.meshes[m];
+                size_t n = M.triangles();
+                std::vector<Box> boxes(n);
+                std::vector<V3> cents(n);
+                for (size_t t = 0; t < n; ++t) {
+                    boxes[t] = Box().ext(M.positions[M.indices[3 * t]]).ext(M.positions[M.indices[3 * t + 1]]).ext(M.positions[M.indices[3 * t + 2]]);
+                    cents[t] = boxes[t].centroid();
+                }
+                SahBuilder sb{boxes, cents, 4, 8, {}, {}};
+                sb.order.resize(n);
+                for (size_t k = 0; k < n; ++k) sb.order[k] = (uint32_t)k;
+                sb.build(0, n, 0);
+                fl.bn = &sb.nodes;
+                fl.order = &sb.order;
+                fl.max_depth = 0;
+                fl.emit = [&](const uint32_t* p, uint32_t cnt) {
+                    uint32_t first = (uint32_t)F.tris.size();
+                    for (uint32_t k = 0; k < cnt; ++k) {
+                        uint32_t t = p[k];
+                        TriRec r;
+                        const V3& a = M.positions[M.indices[3 * t]];
+                        const V3& b = M.positions[M.indices[3 * t + 1]];
+                        const V3& c = M.positions[M.indices[3 * t + 2]];
+                        r.v0[0] = a.x; r.v0[1] = a.y; r.v0[2] = a.z; r.tri = t;
+                        r.v1[0] = b.x; r.v1[1] = b.y; r.v1[2] = b.z; r.inst = 0xffffffffu;
+                        r.v2[0] = c.x; r.v2[1] = c.y; r.v2[2] = c.z; r.flags = 0;
+                        F.tris.push_back(r);
+                    }
+                    return make_leaf(first, cnt);
+                };
+                mesh_root[m] = fl.reference(0, 0);
+                blas_depth = std::max(blas_depth, fl.max_depth);
+            }
             BlasInst bi;
             std::memset(&bi, 0, sizeof(bi));
-            bi.root = root;
-            bi.identity = 1;
-            bi.instance = 0xffffffffu;
+            std::memcpy(bi.to_local, &inv[i].r[0][0], 48);
+            bi.root = mesh_root[m];
+            bi.identity = 0;
+            bi.instance = (uint32_t)i;
+            bi.flags = (s.instances[i].flags & 1u) | ((s.instances[i].flags & 4u) ? 2u : 0u);
             tlas_leaves.push_back(bi);
-            tlas_boxes.push_back(all);
+            tlas_boxes.push_back(instance_box(s.meshes[m], xf[i]));
         }
-    }
-    std::map<uint32_t, uint32_t> mesh_root;
-    for (size_t i = 0; i < ni; ++i) {
-        if (!live[i] || ident[i]) continue;
-        uint32_t m = s.instances[i].mesh;
-        if (!mesh_root.count(m)) {
-            const HMesh& M = s.meshes[m];
-            size_t n = M.triangles();
-            std::vector<Box> boxes(n);
-            std::vector<V3> cents(n);
-            for (size_t t = 0; t < n; ++t) {
-                boxes[t] = Box().ext(M.positions[M.indices[3 * t]]).ext(M.positions[M.indices[3 * t + 1]]).ext(M.positions[M.indices[3 * t + 2]]);
-                cents[t] = boxes[t].centroid();
-            }
-            SahBuilder sb{boxes, cents, 4, 8, {}, {}};
-            sb.order.resize(n);
-            for (size_t k = 0; k < n; ++k) sb.order[k] = (uint32_t)k;
-            sb.build(0, n, 0);
+        // Top level over the placed trees (one per leaf).
+        F.blas = tlas_leaves;
+        uint32_t tlas_depth = 0;
+        if (!tlas_leaves.empty()) {
+            std::vector<V3> cents(tlas_boxes.size());
+            for (size_t k = 0; k < cents.size(); ++k) cents[k] = tlas_boxes[k].centroid();
+            SahBuilder sb{tlas_boxes, cents, 1, 1, {}, {}};
+            sb.order.resize(tlas_boxes.size());
+            for (size_t k = 0; k < tlas_boxes.size(); ++k) sb.order[k] = (uint32_t)k;
+            sb.build(0, tlas_boxes.size(), 0);
             fl.bn = &sb.nodes;
             fl.order = &sb.order;
             fl.max_depth = 0;
-            fl.emit = [&](const uint32_t* p, uint32_t cnt) {
-                uint32_t first = (uint32_t)F.tris.size();
-                for (uint32_t k = 0; k < cnt; ++k) {
-                    uint32_t t = p[k];
-                    TriRec r;
-                    const V3& a = M.positions[M.indices[3 * t]];
-                    const V3& b = M.positions[M.indices[3 * t + 1]];
-                    const V3& c = M.positions[M.indices[3 * t + 2]];
-                    r.v0[0] = a.x; r.v0[1] = a.y; r.v0[2] = a.z; r.tri = t;
-                    r.v1[0] = b.x; r.v1[1] = b.y; r.v1[2] = b.z; r.inst = 0xffffffffu;
-                    r.v2[0] = c.x; r.v2[1] = c.y; r.v2[2] = c.z; r.flags = 0;
-                    F.tris.push_back(r);
-                }
-                return make_leaf(first, cnt);
-            };
-            mesh_root[m] = fl.reference(0, 0);
-            blas_depth = std::max(blas_depth, fl.max_depth);
+            fl.emit = [&](const uint32_t* p, uint32_t) { return make_leaf(p[0], 1); };
+            F.tlas_root = fl.reference(0, 0);
+            tlas_depth = fl.max_depth;
         }
-        BlasInst bi;
-        std::memset(&bi, 0, sizeof(bi));
-        std::memcpy(bi.to_local, &inv[i].r[0][0], 48);
-        bi.root = mesh_root[m];
-        bi.identity = 0;
-        bi.instance = (uint32_t)i;
-        bi.flags = (s.instances[i].flags & 1u) | ((s.instances[i].flags & 4u) ? 2u : 0u);
-        tlas_leaves.push_back(bi);
-        tlas_boxes.push_back(instance_box(s.meshes[m], xf[i]));
+        F.stack_need = 7 * (tlas_depth + blas_depth) + 2;
+        if (F.stack_need > 96) { error = "unsupported: BVH too deep for the traversal stack"; return false; }
+        if (F.tris.size() >= (1u << 27) - 16) { error = "unsupported: more than 2^27 triangles"; return false; }
     }
-    // Top level over the placed trees (one per leaf).
-    F.blas = tlas_leaves;
-    uint32_t tlas_depth = 0;
-    if (!tlas_leaves.empty()) {
-        std::vector<V3> cents(tlas_boxes.size());
-        for (size_t k = 0; k < cents.size(); ++k) cents[k] = tlas_boxes[k].centroid();
-        SahBuilder sb{tlas_boxes, cents, 1, 1, {}, {}};
-        sb.order.resize(tlas_boxes.size());
-        for (size_t k = 0; k < tlas_boxes.size(); ++k) sb.order[k] = (uint32_t)k;
-        sb.build(0, tlas_boxes.size(), 0);
-        fl.bn = &sb.nodes;
-        fl.order = &sb.order;
-        fl.max_depth = 0;
-        fl.emit = [&](const uint32_t* p, uint32_t) { return make_leaf(p[0], 1); };
-        F.tlas_root = fl.reference(0, 0);
-        tlas_depth = fl.max_depth;
-    }
-    F.stack_need = 7 * (tlas_depth + blas_depth) + 2;
-    if (F.stack_need > 96) { error = "unsupported: BVH too deep for the traversal stack"; return false; }
-    if (F.tris.size() >= (1u << 27) - 16) { error = "unsupported: more than 2^27 triangles"; return false; }
     if (!prepare_lights(s, scene_box, F.lights, error)) return false;
 
     // Scene constants: camera basis (scene/mod.rs:158) and render settings.

@@ -64,8 +64,17 @@ struct HScene {
 };
 
 // Parses the RSB subset the path tracer reads. Returns false with `error` set (the reference's
-// wording for format errors, "unsupported: ..." for features outside this path).
-bool parse_rsb(const uint8_t* bytes, size_t len, HScene& out, std::string& error);
+// wording for format errors, "unsupported: ..." for features outside this path). With `kept`, a
+// file without MESH sections takes those meshes instead (Scene::update_from_rsb,
+// engine/crates/rt-core/src/scene/rsb.rs:1630): its INST sections, or the implicit instances of
+// the kept meshes, refer to them. `used_kept` (may be null) tells whether it did.
+bool parse_rsb(const uint8_t* bytes, size_t len, HScene& out, std::string& error, const std::vector<HMesh>* kept = nullptr,
+               bool* used_kept = nullptr);
+
+// What the device geometry (trees, leaf triangles, hit-detail arrays) of a scene depends on,
+// besides the meshes themselves: the instances' meshes, transforms and visibility flags. Two
+// scenes over the same meshes with equal keys have identical device geometry.
+std::string geometry_key(const HScene& s);
 
 // Flattened, device-ready arrays of a scene.
 struct Flat {
@@ -85,6 +94,9 @@ struct Flat {
     double build_seconds = 0;
 };
 // Builds the BVHs and the device layout. Returns false with `error` when a limit is exceeded.
-bool flatten_scene(const HScene& s, Flat& out, std::string& error);
+// Without `geometry`, only the shading part is built (instances, materials, BSDFs, lights, the
+// scene constants); nodes, triangles and vertex arrays stay empty and the tree fields of `scene`
+// (tlas_root, stack_need) are left for the caller to take from the geometry it keeps.
+bool flatten_scene(const HScene& s, Flat& out, std::string& error, bool geometry = true);
 
 }  // namespace rtg

@@ -127,9 +127,11 @@ def _u(*v) -> bytes:
     return struct.pack("<%dI" % len(v), *v)
 
 
-def to_rsb(s: Scene) -> bytes:
+def to_rsb(s: Scene, meshes: bool = True) -> bytes:
     """Serialises a scene as RSB version 1, sections in the reference writer's order (CAMR, MATL,
-    MESH, INST, LGHT, ENVR, FLOR, RNDR) and payload sizes (rsb.rs:1645-1990)."""
+    MESH, INST, LGHT, ENVR, FLOR, RNDR) and payload sizes (rsb.rs:1645-1990). Without ``meshes``
+    the MESH sections are left out: the file of a scene update that keeps the loaded geometry
+    (rt_scene_update)."""
     out = [b"RSB1", _u(0)]
     out.append(_sec(b"CAMR", _f(*s.camera_position, *s.camera_target, *s.camera_up, s.focal_mm, s.sensor_mm, s.fstop,
                                 s.focus_dist) + _u(s.ortho) + _f(s.ortho_width)))
@@ -138,7 +140,7 @@ def to_rsb(s: Scene) -> bytes:
                                                  m.coat_roughness, *m.emission, m.emission_power) + _u(m.flags) +
                         _f(m.opacity, m.anisotropy, m.absorption_mm, m.bevel_mm, m.scatter_mm, *m.scatter_color,
                            m.scatter_g, m.abbe)))
-    for mesh in s.meshes:
+    for mesh in (s.meshes if meshes else []):
         p = np.ascontiguousarray(mesh.positions, dtype="<f4")
         n = np.ascontiguousarray(mesh.normals, dtype="<f4")
         i = np.ascontiguousarray(mesh.indices, dtype="<u4")
