@@ -139,7 +139,10 @@ uint32_t rtg_trace_rays(uint32_t scene, const float* rays, uint32_t n, uint32_t 
  * triangles, BVH build seconds, rays cast so far. */
 uint32_t rtg_scene_stats(uint32_t scene, double* out8);
 
-/* Largest number of paths one wave holds (default 4 Mi; memory is 160 bytes per path). */
+/* Largest number of paths one wave holds (168 bytes of device memory per path, kept until the
+ * scene is freed). 0, the default, sizes each wave to every path of the call, bounded by half of
+ * the device memory then free: a call then runs as few waves as memory allows, and each wave's
+ * tail of long paths is paid once. */
 uint32_t rtg_set_path_capacity(uint32_t scene, uint32_t paths);
 
 /* Extend-kernel timing: when enabled, every extend launch is bracketed by CUDA events on the

@@ -66,7 +66,7 @@ struct Scene {
     PathBuffers P{};
     DevBuf path_mem;
     uint32_t capacity = 0;
-    uint32_t max_capacity = 1u << 24;  // 16 Mi paths (2.6 GB): waves of several samples amortise the path tail
+    uint32_t max_capacity = 0;  // paths per wave; 0: automatic (wave_limit)
     // statistics
     uint64_t rays = 0;
     double build_seconds = 0;
@@ -187,11 +187,32 @@ SceneDev compose(const SceneDev& constants, const SceneDev& geom, const SceneDev
     return S;
 }
 
+// Device bytes of one path slot: o, d, thr, sum, sel, hit, sh_o, sh_d, sh_c (16 each), flags,
+// medium, queue[0], queue[1], sorted, key (4 each).
+constexpr size_t PATH_BYTES = 9 * 16 + 6 * 4;
+constexpr uint64_t AUTO_MIN_PATHS = 1u << 20;
+constexpr uint64_t MAX_WAVE_PATHS = 0x7fffffffu;
+
+// Paths one wave of a call may hold: the limit set by rtg_set_path_capacity, or by default every
+// path the call renders, bounded by half of the device memory that is free (counting the scene's
+// own path buffers). Each wave ends with a tail of long paths that leaves the GPU part-idle, so
+// the fewer waves a call takes, the faster it runs: a 1080p frame at 64 spp is one wave of
+// 132.7 M paths (22 GB).
+uint64_t wave_limit(const Scene& sc, uint64_t call_paths) {
+    if (sc.max_capacity) return sc.max_capacity;
+    uint64_t by_memory = AUTO_MIN_PATHS;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+        by_memory = std::max<uint64_t>(AUTO_MIN_PATHS, (free_b + sc.path_mem.bytes) / 2 / PATH_BYTES);
+    return std::max<uint64_t>(1, std::min<uint64_t>(std::min(call_paths, by_memory), MAX_WAVE_PATHS));
+}
+
 uint32_t ensure_capacity(Scene& sc, uint32_t paths) {
     if (paths <= sc.capacity) return RTG_STATUS_OK;
     sc.path_mem.release();
+    sc.capacity = 0;
     size_t n = paths;
-    size_t bytes = n * (16 * 5 + 4 + 4 + 16 + 4 * 4 + 16 * 3) + 16 * 256 + 256 + 512 * 4;
+    size_t bytes = n * PATH_BYTES + 16 * 256 + 256 + 512 * 4;
     RTG_CHECK(cudaMalloc(&sc.path_mem.p, bytes));
     sc.path_mem.bytes = bytes;
     uint8_t* p = (uint8_t*)sc.path_mem.p;
@@ -280,14 +301,15 @@ uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h
     if (x >= x_end || y >= y_end || count == 0) return RTG_STATUS_OK;
     uint32_t cw = (uint32_t)(x_end - x), ch = (uint32_t)(y_end - y);
     uint64_t npix = (uint64_t)cw * ch;
-    // Rows per band so that one band of one sample fits the path capacity.
+    // Rows per band so that one band of one sample fits a wave.
+    const uint64_t cap = wave_limit(sc, npix * count);
     uint32_t band_rows = ch;
-    if (npix > sc.max_capacity) band_rows = std::max<uint32_t>(1, (uint32_t)(sc.max_capacity / cw));
+    if (npix > cap) band_rows = std::max<uint32_t>(1, (uint32_t)(cap / cw));
     uint64_t total_rays = 0;
     for (uint32_t by = 0; by < ch; by += band_rows) {
         uint32_t bh = std::min(band_rows, ch - by);
         uint64_t bpix = (uint64_t)cw * bh;
-        uint32_t per_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(count, sc.max_capacity / bpix));
+        uint32_t per_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(count, cap / bpix));
         uint32_t need = (uint32_t)(bpix * per_wave);
         uint32_t st = ensure_capacity(sc, need);
         if (st) return st;
@@ -622,7 +644,7 @@ uint32_t rtg_set_path_capacity(uint32_t handle, uint32_t paths) {
     std::lock_guard<std::mutex> lk(g_mu);
     Scene* sc = scene_of(handle);
     if (!sc) return RTG_STATUS_BAD_HANDLE;
-    if (paths < 1024) paths = 1024;
+    if (paths != 0 && paths < 1024) paths = 1024;
     sc->max_capacity = paths;
     return RTG_STATUS_OK;
 }
