@@ -118,6 +118,30 @@ uint32_t rtg_render_progressive(uint32_t scene, uint32_t film, uint32_t first_sa
 uint32_t rtg_render_progressive_noalloc(uint32_t scene, uint32_t film, uint32_t first_sample, uint32_t count,
                                         uint64_t* rays);
 
+/* The batched render queue (no reference counterpart; the reference's product runs its render
+ * queue one job after another, src/ui/render-queue.ts, over cameras x studios,
+ * src/core/render.ts:71). A queue renders many variants of one loaded scene -- other cameras,
+ * image sizes, materials, light rigs, seeds, sample ranges -- over the scene's geometry, packing
+ * the paths of all of them into as few waves as device memory allows instead of one call each.
+ * Every job's film gets the bits rtg_render_progressive gives after rtg_scene_update with the
+ * job's file.
+ *
+ * rtg_queue_create: a queue over scene `scene`; a handle > 0, or 0 (message as for loads).
+ * rtg_queue_add: a job: `bytes` is an RSB file without MESH sections whose instances match the
+ * scene's (the form rtg_scene_update takes for a change that keeps the geometry), samples
+ * [first_sample, first_sample + count). *film receives a new film over the job's whole image
+ * (free it with rtg_film_free). RTG_STATUS_BAD_SCENE (message) when the file is invalid or
+ * changes the geometry.
+ * rtg_queue_run: renders every job added since the last run, then forgets them (their films stay).
+ * flags: RTG_QUEUE_GRAPH captures the run's launches into one CUDA graph and launches that. `rays`
+ * (may be null) receives the camera + extension + shadow rays of all jobs.
+ * rtg_queue_free: forgets the queue and its pending jobs. */
+#define RTG_QUEUE_GRAPH 1u
+uint32_t rtg_queue_create(uint32_t scene);
+uint32_t rtg_queue_add(uint32_t queue, const uint8_t* bytes, uint32_t len, uint32_t first_sample, uint32_t count, uint32_t* film);
+uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays);
+uint32_t rtg_queue_free(uint32_t queue);
+
 /* Copies the film's sums to host memory (any pointer may be null): rgb 3*w*h floats, weight,
  * alpha and lum2 w*h floats each. */
 uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2);

@@ -28,6 +28,7 @@ STATUS_CUDA_ERROR = 16
 STATUS_STACK_OVERFLOW = 17
 STATUS_BAD_FILM = 18
 MAX_TILE_PIXELS = 1 << 22
+QUEUE_GRAPH = 1
 
 LIB_PATH = Path(__file__).resolve().parent / "librtg.so"
 _lib: Optional[ctypes.CDLL] = None
@@ -48,6 +49,10 @@ ABI = {
     "rtg_film_clear": (_u32, [_u32]),
     "rtg_render_progressive": (_u32, [_u32, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
     "rtg_render_progressive_noalloc": (_u32, [_u32, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
+    "rtg_queue_create": (_u32, [_u32]),
+    "rtg_queue_add": (_u32, [_u32, ctypes.c_char_p, _u32, _u32, _u32, ctypes.POINTER(_u32)]),
+    "rtg_queue_run": (_u32, [_u32, _u32, ctypes.POINTER(_u64)]),
+    "rtg_queue_free": (_u32, [_u32]),
     "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_render_paths": (_u32, [_u32, _f, _u32, _f]),
@@ -197,9 +202,9 @@ class Scene:
 class Film:
     """A device film over an image rectangle (rt-core Film): rgb, weight, alpha, lum2 sums."""
 
-    def __init__(self, scene: Scene, x: int, y: int, w: int, h: int):
+    def __init__(self, scene: Scene, x: int, y: int, w: int, h: int, handle: int = 0):
         self.scene, self.x, self.y, self.w, self.h = scene, x, y, w, h
-        self.handle = lib().rtg_film_create(scene.handle, x, y, w, h)
+        self.handle = handle or lib().rtg_film_create(scene.handle, x, y, w, h)
         if self.handle == 0:
             raise RtgError(STATUS_BAD_FILM, error_message())
 
@@ -237,6 +242,45 @@ class Film:
     def close(self):
         if self.handle:
             lib().rtg_film_free(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Queue:
+    """A batched render queue over a loaded scene (rtg_queue_*): jobs are variants of the scene
+    (RSB files without MESH sections) with sample ranges, rendered together by ``run``."""
+
+    def __init__(self, scene: Scene):
+        self.scene = scene
+        self.handle = lib().rtg_queue_create(scene.handle)
+        if self.handle == 0:
+            raise RtgError(STATUS_BAD_HANDLE, error_message())
+
+    def add(self, rsb: bytes, first: int, count: int, width: int, height: int) -> Film:
+        """Queues samples [first, first + count) of the variant ``rsb`` (whose image is width x
+        height); returns the film it will render into."""
+        film = _u32(0)
+        status = lib().rtg_queue_add(self.handle, rsb, len(rsb), first, count, ctypes.byref(film))
+        if status != STATUS_OK:
+            raise RtgError(status, error_message())
+        return Film(self.scene, 0, 0, width, height, handle=int(film.value))
+
+    def run(self, graph: bool = False) -> int:
+        """Renders every queued job; returns the rays cast."""
+        rays = _u64(0)
+        status = lib().rtg_queue_run(self.handle, QUEUE_GRAPH if graph else 0, ctypes.byref(rays))
+        if status != STATUS_OK:
+            raise RtgError(status, error_message())
+        return int(rays.value)
+
+    def close(self):
+        if self.handle:
+            lib().rtg_queue_free(self.handle)
             self.handle = 0
 
     def __del__(self):

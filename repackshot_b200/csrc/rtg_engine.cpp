@@ -3,6 +3,7 @@
 // (engine/crates/rt-wasm/src/ffi.rs:28-197, rt-wasm/src/lib.rs:37-164, 562-730).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -97,11 +98,32 @@ struct Film {
     DevBuf mem;
     ~Film() { mem.release(); }
 };
+// A job of a render queue: one variant of the queue's scene (its own camera, image, materials,
+// lights and settings over the scene's geometry), a sample range and the film it renders into.
+struct QueueJob {
+    BufSet shading;
+    SceneDev constants;  // F.scene of the job; geometry pointers are taken from the scene at run time
+    SceneDev shade;      // the job's instance, material and BSDF pointers
+    std::string geom_key;
+    uint32_t film = 0, first = 0, count = 0, width = 0, height = 0;
+};
+struct Queue {
+    uint32_t scene = 0;
+    std::vector<std::unique_ptr<QueueJob>> jobs;  // pending until the next run
+    DevBuf tables;                                // JobDev and SegDev arrays of a run
+    ~Queue() {
+        for (auto& j : jobs) j->shading.release();
+        tables.release();
+    }
+};
+
 std::vector<std::unique_ptr<Scene>> g_scenes;
 std::vector<std::unique_ptr<Film>> g_films;
+std::vector<std::unique_ptr<Queue>> g_queues;
 
 Scene* scene_of(uint32_t h) { return (h == 0 || h > g_scenes.size()) ? nullptr : g_scenes[h - 1].get(); }
 Film* film_of(uint32_t h) { return (h == 0 || h > g_films.size()) ? nullptr : g_films[h - 1].get(); }
+Queue* queue_of(uint32_t h) { return (h == 0 || h > g_queues.size()) ? nullptr : g_queues[h - 1].get(); }
 
 uint32_t device_init() {
     if (g_device_ready) return RTG_STATUS_OK;
@@ -253,7 +275,9 @@ int grid_for(uint32_t n, int per_block) {
 }
 
 // Runs one wave and (when timing) adds the extend-kernel time.
-uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film) {
+// `S` (default: the scene's) gives the launch its bounce count; batched waves pass the deepest job's.
+uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film, const SceneDev* S = nullptr) {
+    const SceneDev& Sw = S ? *S : sc.S;
     WaveTiming* t = nullptr;
     if (sc.timing) {
         if (!sc.wt) {
@@ -263,9 +287,9 @@ uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film) {
         sc.wt->ev_count = 0;
         t = sc.wt;
     }
-    launch_wave(sc.S, sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t);
+    launch_wave(Sw, sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t);
     RTG_CHECK(cudaGetLastError());
-    sc.launches += 2 + 6 * (uint64_t)(sc.S.max_depth + 1) - (film ? 0 : 1);
+    sc.launches += 2 + 6 * (uint64_t)(Sw.max_depth + 1) - ((film || w.segs) ? 0 : 1);
     if (t) {
         RTG_CHECK(cudaStreamSynchronize(sc.stream));
         for (int i = 0; i + 1 < t->ev_count; i += 2) {
@@ -340,6 +364,17 @@ uint32_t make_film(uint32_t ox, uint32_t oy, uint32_t w, uint32_t h, Film& f) {
     return RTG_STATUS_OK;
 }
 
+// Registers a new zeroed film over (x, y, w, h) of scene `handle`: its handle, or 0.
+uint32_t new_film(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h) {
+    auto f = std::make_unique<Film>();
+    f->scene = handle;
+    if (make_film(x, y, w, h, *f) != RTG_STATUS_OK) return 0;
+    for (size_t i = 0; i < g_films.size(); ++i)
+        if (!g_films[i]) { g_films[i] = std::move(f); return (uint32_t)i + 1; }
+    g_films.push_back(std::move(f));
+    return (uint32_t)g_films.size();
+}
+
 uint32_t render_tile_impl(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample, float* out, bool rgba) {
     Scene* sc = scene_of(handle);
     if (!sc) return RTG_STATUS_BAD_HANDLE;
@@ -393,8 +428,8 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     if (upload_geometry(F, sc->geometry, geom) || upload_shading(F, sc->shading, shade)) return 0;
     sc->S = compose(F.scene, geom, shade);
     sc->d_lights = sc->shading.lights;
-    sc->meshes = std::move(hs.meshes);
     sc->geom_key = geometry_key(hs);
+    sc->meshes = std::move(hs.meshes);
     sc->build_seconds = F.build_seconds;
     sc->nodes = F.nodes.size();
     sc->tris = F.tris.size();
@@ -489,13 +524,7 @@ uint32_t rtg_film_create(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, ui
     std::lock_guard<std::mutex> lk(g_mu);
     if (!scene_of(handle)) { g_error = "bad scene handle"; return 0; }
     if ((uint64_t)w * h == 0 || (uint64_t)w * h > (1ull << 28)) { g_error = "bad film size"; return 0; }
-    auto f = std::make_unique<Film>();
-    f->scene = handle;
-    if (make_film(x, y, w, h, *f) != RTG_STATUS_OK) return 0;
-    for (size_t i = 0; i < g_films.size(); ++i)
-        if (!g_films[i]) { g_films[i] = std::move(f); return (uint32_t)i + 1; }
-    g_films.push_back(std::move(f));
-    return (uint32_t)g_films.size();
+    return new_film(handle, x, y, w, h);
 }
 uint32_t rtg_film_free(uint32_t film) {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -541,6 +570,210 @@ uint32_t rtg_render_progressive_noalloc(uint32_t handle, uint32_t film, uint32_t
     if (rays) *rays = res.extend_rays + res.shadow_rays;
     return RTG_STATUS_OK;
 }
+uint32_t rtg_queue_create(uint32_t scene) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!scene_of(scene)) { g_error = "bad scene handle"; return 0; }
+    auto q = std::make_unique<Queue>();
+    q->scene = scene;
+    for (size_t i = 0; i < g_queues.size(); ++i)
+        if (!g_queues[i]) { g_queues[i] = std::move(q); return (uint32_t)i + 1; }
+    g_queues.push_back(std::move(q));
+    return (uint32_t)g_queues.size();
+}
+
+uint32_t rtg_queue_free(uint32_t queue) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!queue_of(queue)) return RTG_STATUS_BAD_HANDLE;
+    Scene* sc = scene_of(g_queues[queue - 1]->scene);
+    if (sc) cudaStreamSynchronize(sc->stream);
+    g_queues[queue - 1].reset();
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_queue_add(uint32_t queue, const uint8_t* bytes, uint32_t len, uint32_t first_sample, uint32_t count, uint32_t* film) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Queue* q = queue_of(queue);
+    Scene* sc = q ? scene_of(q->scene) : nullptr;
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (!bytes || !film) { g_error = "rtg_queue_add: null pointer"; return RTG_STATUS_NULL_POINTER; }
+    *film = 0;
+    HScene hs;
+    std::string err;
+    bool kept = false;
+    if (!parse_rsb(bytes, len, hs, err, &sc->meshes, &kept)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
+    std::string key = geometry_key(hs);
+    if (!kept || key != sc->geom_key) {
+        g_error = "a queue job keeps the scene's geometry: no MESH sections, the same instances";
+        return RTG_STATUS_BAD_SCENE;
+    }
+    Flat F;
+    if (!flatten_scene(hs, F, err, false)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
+    auto job = std::make_unique<QueueJob>();
+    job->constants = F.scene;
+    job->shade = F.scene;
+    uint32_t st = upload_shading(F, job->shading, job->shade);
+    if (st) { job->shading.release(); return st; }
+    job->geom_key = std::move(key);
+    job->first = first_sample;
+    job->count = count;
+    job->width = F.scene.width;
+    job->height = F.scene.height;
+    job->film = new_film(q->scene, 0, 0, job->width, job->height);
+    if (!job->film) { job->shading.release(); return RTG_STATUS_CUDA_ERROR; }
+    *film = job->film;
+    q->jobs.push_back(std::move(job));
+    g_error.clear();
+    return RTG_STATUS_OK;
+}
+
+namespace rtg {
+namespace {
+// Packs the queue's jobs into waves of at most `cap` paths. A job gives each wave one segment at
+// most (whole images over a run of samples, or a band of rows of one sample), so a pixel receives
+// its samples in index order: wave by wave, and within a wave from one segment only.
+void pack_waves(const std::vector<std::unique_ptr<QueueJob>>& jobs, uint64_t cap, std::vector<std::vector<SegDev>>& waves,
+                std::vector<uint64_t>& wave_paths) {
+    std::vector<SegDev> cur;
+    uint64_t used = 0;
+    auto flush = [&]() {
+        if (cur.empty()) return;
+        waves.push_back(cur);
+        wave_paths.push_back(used);
+        cur.clear();
+        used = 0;
+    };
+    for (uint32_t j = 0; j < jobs.size(); ++j) {
+        const QueueJob& J = *jobs[j];
+        const uint64_t W = J.width, H = J.height, npix = W * H;
+        uint32_t s = J.first, row = 0;
+        const uint32_t s_end = J.first + J.count;
+        while (s < s_end) {
+            uint64_t space = cap - used;
+            SegDev g{};
+            g.job = j;
+            g.w = (uint32_t)W;
+            if (row == 0 && space >= npix) {
+                uint64_t ns = std::min<uint64_t>(s_end - s, space / npix);
+                g.y0 = 0; g.h = (uint32_t)H; g.first = s; g.ns = (uint32_t)ns;
+                s += (uint32_t)ns;
+            } else if (space >= W) {
+                uint64_t rows = std::min<uint64_t>(H - row, space / W);
+                g.y0 = row; g.h = (uint32_t)rows; g.first = s; g.ns = 1;
+                row += (uint32_t)rows;
+                if (row == H) { row = 0; ++s; }
+            } else {
+                flush();
+                continue;
+            }
+            g.slot_begin = (uint32_t)used;
+            uint64_t seg_pix = (uint64_t)g.w * g.h;
+            g.pix_begin = cur.empty() ? 0 : cur.back().pix_begin + cur.back().w * cur.back().h;
+            cur.push_back(g);
+            used += seg_pix * g.ns;
+            if (s < s_end) flush();  // the job goes on: its next segment belongs to the next wave
+        }
+    }
+    flush();
+}
+}  // namespace
+}  // namespace rtg
+
+uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Queue* q = queue_of(queue);
+    Scene* sc = q ? scene_of(q->scene) : nullptr;
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (rays) *rays = 0;
+    // Jobs and their films as the device reads them; the geometry is the scene's as it is now.
+    std::vector<JobDev> jobs_h(q->jobs.size());
+    SceneDev Sw = sc->S;
+    uint64_t total = 0;
+    for (size_t j = 0; j < q->jobs.size(); ++j) {
+        QueueJob& J = *q->jobs[j];
+        Film* f = film_of(J.film);
+        if (!f) { g_error = "a queue job's film was freed"; return RTG_STATUS_BAD_FILM; }
+        if (J.geom_key != sc->geom_key) { g_error = "the scene's geometry changed after the job was added"; return RTG_STATUS_BAD_SCENE; }
+        jobs_h[j].S = compose(J.constants, sc->S, J.shade);
+        jobs_h[j].lights = J.shading.lights;
+        jobs_h[j].film = f->dev;
+        Sw.max_depth = std::max(Sw.max_depth, J.constants.max_depth);
+        total += (uint64_t)J.width * J.height * J.count;
+    }
+    if (total == 0) {
+        for (auto& j : q->jobs) j->shading.release();
+        q->jobs.clear();
+        return RTG_STATUS_OK;
+    }
+    uint64_t cap = wave_limit(*sc, total);
+    uint64_t widest = 0;
+    for (auto& j : q->jobs) widest = std::max<uint64_t>(widest, j->width);
+    cap = std::max(cap, widest);  // a wave holds at least one row of every job
+    std::vector<std::vector<SegDev>> waves;
+    std::vector<uint64_t> wave_paths;
+    pack_waves(q->jobs, cap, waves, wave_paths);
+    uint64_t max_wave = *std::max_element(wave_paths.begin(), wave_paths.end());
+    if (max_wave > MAX_WAVE_PATHS) { g_error = "a queue wave exceeds 2^31 paths"; return RTG_STATUS_BAD_SCENE; }
+    uint32_t st = ensure_capacity(*sc, (uint32_t)max_wave);
+    if (st) return st;
+    // One upload of the job table and every wave's segments.
+    size_t nseg = 0;
+    for (auto& w : waves) nseg += w.size();
+    size_t bytes = jobs_h.size() * sizeof(JobDev) + nseg * sizeof(SegDev);
+    if (q->tables.bytes < bytes) {
+        q->tables.release();
+        RTG_CHECK(cudaMalloc(&q->tables.p, bytes));
+        q->tables.bytes = bytes;
+    }
+    std::vector<uint8_t> host(bytes);
+    std::memcpy(host.data(), jobs_h.data(), jobs_h.size() * sizeof(JobDev));
+    size_t off = jobs_h.size() * sizeof(JobDev);
+    for (auto& w : waves) {
+        std::memcpy(host.data() + off, w.data(), w.size() * sizeof(SegDev));
+        off += w.size() * sizeof(SegDev);
+    }
+    RTG_CHECK(cudaMemcpyAsync(q->tables.p, host.data(), bytes, cudaMemcpyHostToDevice, sc->stream));
+    const JobDev* jobs_d = (const JobDev*)q->tables.p;
+    const SegDev* segs_d = (const SegDev*)((const uint8_t*)q->tables.p + jobs_h.size() * sizeof(JobDev));
+    // The waves: enqueued back to back, or captured into one CUDA graph and launched as one.
+    const bool graph = (flags & RTG_QUEUE_GRAPH) != 0;
+    const bool timing = sc->timing;
+    if (graph) {
+        sc->timing = false;
+        RTG_CHECK(cudaStreamSynchronize(sc->stream));
+        RTG_CHECK(cudaStreamBeginCapture(sc->stream, cudaStreamCaptureModeThreadLocal));
+    }
+    cudaError_t e = cudaMemsetAsync(sc->P.counters, 0, 16, sc->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sc->P.rays, 0, 16, sc->stream);
+    size_t seg_off = 0;
+    for (size_t k = 0; k < waves.size() && e == cudaSuccess && st == RTG_STATUS_OK; ++k) {
+        uint32_t npix = waves[k].back().pix_begin + waves[k].back().w * waves[k].back().h;
+        WaveDesc wd{0, 0, 0, 0, 0, (uint32_t)wave_paths[k], nullptr, segs_d + seg_off, jobs_d, (uint32_t)waves[k].size(), npix};
+        st = run_wave(*sc, wd, nullptr, &Sw);
+        seg_off += waves[k].size();
+    }
+    if (graph) {
+        sc->timing = timing;
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(sc->stream, &g);
+        if (e == cudaSuccess) e = ce;
+        cudaGraphExec_t exec = nullptr;
+        if (e == cudaSuccess && st == RTG_STATUS_OK) e = cudaGraphInstantiate(&exec, g, 0);
+        if (e == cudaSuccess && st == RTG_STATUS_OK) e = cudaGraphLaunch(exec, sc->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (g) cudaGraphDestroy(g);
+    }
+    if (e != cudaSuccess) { cuda_fail(e, "rtg_queue_run"); return RTG_STATUS_CUDA_ERROR; }
+    if (st) return st;
+    uint64_t r = 0;
+    st = finish(*sc, &r);
+    if (st) return st;
+    if (rays) *rays = r;
+    for (auto& j : q->jobs) j->shading.release();
+    q->jobs.clear();
+    return RTG_STATUS_OK;
+}
+
 uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2) {
     std::lock_guard<std::mutex> lk(g_mu);
     Film* f = film_of(film);

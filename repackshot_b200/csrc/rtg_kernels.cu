@@ -32,6 +32,28 @@ __device__ __forceinline__ void wave_slot(const WaveDesc& w, uint32_t slot, uint
     index = w.first + s;
 }
 
+// The segment of a batched wave that holds `slot`: the last with slot_begin <= slot.
+__device__ __forceinline__ uint32_t seg_of_slot(const WaveDesc& w, uint32_t slot) {
+    uint32_t lo = 0, hi = w.nseg;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&w.segs[mid].slot_begin) <= slot) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Job, pixel and sample index of a slot of a batched wave.
+__device__ __forceinline__ void batch_slot(const WaveDesc& w, uint32_t slot, uint32_t& job, uint32_t& x, uint32_t& y, uint32_t& index) {
+    const SegDev& g = w.segs[seg_of_slot(w, slot)];
+    uint32_t local = slot - g.slot_begin, npix = g.w * g.h;
+    uint32_t s = local / npix, rem = local - s * npix;
+    job = g.job;
+    y = g.y0 + rem / g.w;
+    x = rem % g.w;
+    index = g.first + s;
+}
+
 __device__ __forceinline__ void add_clamped(float4& sum, Rgb c, bool indirect, float clamp) {  // integrator/mod.rs:855
     if (!(finitef(c.r) && finitef(c.g) && finitef(c.b))) return;
     float p = rmax(rmax(c.r, c.g), c.b);
@@ -42,12 +64,20 @@ __device__ __forceinline__ void add_clamped(float4& sum, Rgb c, bool indirect, f
 }
 
 // ---- camera generation ---------------------------------------------------------------------------
+// BATCH: the slots belong to the jobs of a batched wave, each with its own camera.
+template <bool BATCH>
 __global__ void k_camera(SceneDev S, WaveDesc w, PathBuffers P) {
     for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n; slot += gridDim.x * blockDim.x) {
         uint32_t x, y, index;
-        wave_slot(w, slot, x, y, index);
         V3 o, d;
-        camera_ray(S, c_sobol, x, y, index, o, d);
+        if constexpr (BATCH) {
+            uint32_t job;
+            batch_slot(w, slot, job, x, y, index);
+            camera_ray(w.jobs[job].S, c_sobol, x, y, index, o, d);
+        } else {
+            wave_slot(w, slot, x, y, index);
+            camera_ray(S, c_sobol, x, y, index, o, d);
+        }
         P.o[slot] = make_float4(o.x, o.y, o.z, 0.0f);  // w: distance since the last scattering vertex
         P.d[slot] = make_float4(d.x, d.y, d.z, 0.0f);  // w: density of the BSDF sample
         P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);  // w: alpha
@@ -166,195 +196,213 @@ __global__ void k_scatter(PathBuffers P, int cur) {
 }
 
 // ---- shade: one vertex of every active path ----------------------------------------------------------
-__global__ void __launch_bounds__(128) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, uint32_t bounce,
-                                               WaveDesc w) {
-    const LightsDev& L = *Lg;
-    uint32_t n = *(volatile uint32_t*)&P.counters[cur];
-    uint32_t rays_local = 0, shadow_local = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t slot = P.sorted[i];
-        float4 o4 = P.o[slot], d4 = P.d[slot], thr4 = P.thr[slot], sum = P.sum[slot];
-        uint32_t flags = P.flags[slot];
-        uint4 hit = P.hit[slot];
-        V3 ro = v3(o4.x, o4.y, o4.z), rd = v3(d4.x, d4.y, d4.z);
-        float offset = o4.w, pdf = d4.w;
-        bool has_pdf = (flags & PF_HAS_PDF) != 0, primary = (flags & PF_PRIMARY) != 0;
-        Rgb thr = rgb(thr4.x, thr4.y, thr4.z);
-        float alpha = thr4.w;
-        rays_local += 1;
-        float t_geometry = hit.w ? __uint_as_float(hit.z) : f_inf();
-        // floor_t (integrator/mod.rs:493)
-        float t_floor = f_inf();
-        if ((S.floor_mode == 1) && rd.z != 0.0f) {
-            float t = (S.floor_z - ro.z) / rd.z;
-            if (t > 1.0e-3f && t < f_inf()) t_floor = t;
+// One vertex of the path in `slot` with the scene constants S and lights L; xyi(x, y, index) gives
+// the path's pixel and sample index (the sampler's key).
+template <class XYI>
+__device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L, const PathBuffers& P, uint32_t slot, int cur, uint32_t bounce,
+                                           XYI xyi, uint32_t& rays_local, uint32_t& shadow_local) {
+    float4 o4 = P.o[slot], d4 = P.d[slot], thr4 = P.thr[slot], sum = P.sum[slot];
+    uint32_t flags = P.flags[slot];
+    uint4 hit = P.hit[slot];
+    V3 ro = v3(o4.x, o4.y, o4.z), rd = v3(d4.x, d4.y, d4.z);
+    float offset = o4.w, pdf = d4.w;
+    bool has_pdf = (flags & PF_HAS_PDF) != 0, primary = (flags & PF_PRIMARY) != 0;
+    Rgb thr = rgb(thr4.x, thr4.y, thr4.z);
+    float alpha = thr4.w;
+    rays_local += 1;
+    float t_geometry = hit.w ? __uint_as_float(hit.z) : f_inf();
+    // floor_t (integrator/mod.rs:493)
+    float t_floor = f_inf();
+    if ((S.floor_mode == 1) && rd.z != 0.0f) {
+        float t = (S.floor_z - ro.z) / rd.z;
+        if (t > 1.0e-3f && t < f_inf()) t_floor = t;
+    }
+    float t_nearest = rmin(t_geometry, t_floor);
+    if ((flags & PF_MEDIUM) && finitef(t_nearest)) {
+        const DevMaterial& mm = S.materials[P.medium[slot]];
+        thr = thr * rgb(fexp(-mm.sigma[0] * t_nearest), fexp(-mm.sigma[1] * t_nearest), fexp(-mm.sigma[2] * t_nearest));
+    }
+    float4 sel4 = P.sel[slot];
+    Sel from;
+    from.p = v3(sel4.x, sel4.y, sel4.z);
+    from.by_flux = !(L.per_point && L.n_entries > 0);
+    from.total = 0.0f;
+    if (has_pdf && !from.by_flux) from = select_at(L, from.p);
+    Rgb crossed = crossed_from(L, ro, rd, 1.0e-3f, t_nearest, has_pdf, pdf, from, offset);
+    add_clamped(sum, thr * crossed, bounce >= 2, S.clamp_indirect);
+    bool alive = false;
+    do {
+        if (t_nearest == f_inf()) {
+            if (primary && S.background == 0) {
+                Rgb seen = escaped(L, rd, false, 0.0f, from);
+                Rgb c = thr * (S.exterior == 1.0f ? seen : seen * S.exterior);
+                sum.x = sum.x + c.r; sum.y = sum.y + c.g; sum.z = sum.z + c.b;
+            } else if (primary && S.background == 1) {
+                Rgb c = thr * rgb(S.background_color[0], S.background_color[1], S.background_color[2]);
+                sum.x = sum.x + c.r; sum.y = sum.y + c.g; sum.z = sum.z + c.b;
+            } else if (primary && S.background == 2) {
+                alpha = peak(crossed) > 0.0f ? 1.0f : 0.0f;
+            } else {
+                add_clamped(sum, thr * escaped(L, rd, has_pdf, pdf, from), bounce >= 2, S.clamp_indirect);
+            }
+            break;
         }
-        float t_nearest = rmin(t_geometry, t_floor);
-        if ((flags & PF_MEDIUM) && finitef(t_nearest)) {
-            const DevMaterial& mm = S.materials[P.medium[slot]];
-            thr = thr * rgb(fexp(-mm.sigma[0] * t_nearest), fexp(-mm.sigma[1] * t_nearest), fexp(-mm.sigma[2] * t_nearest));
-        }
-        float4 sel4 = P.sel[slot];
-        Sel from;
-        from.p = v3(sel4.x, sel4.y, sel4.z);
-        from.by_flux = !(L.per_point && L.n_entries > 0);
-        from.total = 0.0f;
-        if (has_pdf && !from.by_flux) from = select_at(L, from.p);
-        Rgb crossed = crossed_from(L, ro, rd, 1.0e-3f, t_nearest, has_pdf, pdf, from, offset);
-        add_clamped(sum, thr * crossed, bounce >= 2, S.clamp_indirect);
-        bool alive = false;
-        do {
-            if (t_nearest == f_inf()) {
-                if (primary && S.background == 0) {
-                    Rgb seen = escaped(L, rd, false, 0.0f, from);
-                    Rgb c = thr * (S.exterior == 1.0f ? seen : seen * S.exterior);
-                    sum.x = sum.x + c.r; sum.y = sum.y + c.g; sum.z = sum.z + c.b;
-                } else if (primary && S.background == 1) {
-                    Rgb c = thr * rgb(S.background_color[0], S.background_color[1], S.background_color[2]);
-                    sum.x = sum.x + c.r; sum.y = sum.y + c.g; sum.z = sum.z + c.b;
-                } else if (primary && S.background == 2) {
-                    alpha = peak(crossed) > 0.0f ? 1.0f : 0.0f;
-                } else {
-                    add_clamped(sum, thr * escaped(L, rd, has_pdf, pdf, from), bounce >= 2, S.clamp_indirect);
-                }
+        V3 s_point, s_hit, s_normal, s_geom;
+        bool s_inst = false, s_outside = true;
+        uint32_t inst = 0;
+        const DevInstance* I = nullptr;
+        const DevMaterial* mat = nullptr;
+        if (t_floor < t_geometry) {
+            V3 pp = ro + rd * t_floor;
+            V3 point = v3(pp.x, pp.y, S.floor_z);
+            V3 nn = v3(0.0f, 0.0f, rd.z < 0.0f ? 1.0f : -1.0f);
+            s_point = point; s_hit = point; s_normal = nn; s_geom = nn;
+        } else {
+            HitInfo h;
+            uint4 idx;
+            if (!hit_details(S, ro, rd, 1.0e-3f, f_inf(), hit.x, hit.y, h, I, idx)) break;
+            // bevel.rs:232 shading_point without a bevel
+            V3 ng = h.geometric, nrm = h.normal;
+            if (dot(nrm, ng) < 0.0f) nrm = -nrm;
+            if (dot(nrm, rd) >= -1.0e-4f) nrm = ng;
+            s_point = terminator_point(S, I, idx, h);
+            s_hit = h.point;
+            s_normal = nrm;
+            s_geom = ng;
+            s_inst = true;
+            inst = hit.x;
+            s_outside = h.outside;
+            mat = S.materials + I->material;
+            if (mat->kind == MATERIAL_EMISSIVE) {
+                if (h.front || !(I->flags & 1u))
+                    add_clamped(sum, thr * rgb(mat->emission[0], mat->emission[1], mat->emission[2]) * 1.0f, bounce >= 2, S.clamp_indirect);
                 break;
             }
-            V3 s_point, s_hit, s_normal, s_geom;
-            bool s_inst = false, s_outside = true;
-            uint32_t inst = 0;
-            const DevInstance* I = nullptr;
-            const DevMaterial* mat = nullptr;
-            if (t_floor < t_geometry) {
-                V3 pp = ro + rd * t_floor;
-                V3 point = v3(pp.x, pp.y, S.floor_z);
-                V3 nn = v3(0.0f, 0.0f, rd.z < 0.0f ? 1.0f : -1.0f);
-                s_point = point; s_hit = point; s_normal = nn; s_geom = nn;
-            } else {
-                HitInfo h;
-                uint4 idx;
-                if (!hit_details(S, ro, rd, 1.0e-3f, f_inf(), hit.x, hit.y, h, I, idx)) break;
-                // bevel.rs:232 shading_point without a bevel
-                V3 ng = h.geometric, nrm = h.normal;
-                if (dot(nrm, ng) < 0.0f) nrm = -nrm;
-                if (dot(nrm, rd) >= -1.0e-4f) nrm = ng;
-                s_point = terminator_point(S, I, idx, h);
-                s_hit = h.point;
-                s_normal = nrm;
-                s_geom = ng;
-                s_inst = true;
-                inst = hit.x;
-                s_outside = h.outside;
-                mat = S.materials + I->material;
-                if (mat->kind == MATERIAL_EMISSIVE) {
-                    if (h.front || !(I->flags & 1u))
-                        add_clamped(sum, thr * rgb(mat->emission[0], mat->emission[1], mat->emission[2]) * 1.0f, bounce >= 2, S.clamp_indirect);
+        }
+        if (bounce >= S.max_depth) break;
+        const Bsdf& b = S.bsdfs[mat ? 2 * I->material + (s_outside ? 0 : 1) : 2 * S.n_materials];
+        // Prepared::frame (integrator/mod.rs:833)
+        Frame fr = frame_from_normal(s_normal);
+        if (s_inst && I->tangent_on) {
+            V3 cands[2] = {cross(ld3(I->tan_axis), s_point - ld3(I->tan_centre)), ld3(I->tan_x)};
+            for (int k = 0; k < 2; ++k) {
+                V3 t = cands[k] - s_normal * dot(s_normal, cands[k]);
+                if (len2(t) > 1.0e-12f) {
+                    V3 xx = normalize(t);
+                    fr.x = xx; fr.y = cross(s_normal, xx); fr.z = s_normal;
                     break;
                 }
             }
-            if (bounce >= S.max_depth) break;
-            const Bsdf& b = S.bsdfs[mat ? 2 * I->material + (s_outside ? 0 : 1) : 2 * S.n_materials];
-            // Prepared::frame (integrator/mod.rs:833)
-            Frame fr = frame_from_normal(s_normal);
-            if (s_inst && I->tangent_on) {
-                V3 cands[2] = {cross(ld3(I->tan_axis), s_point - ld3(I->tan_centre)), ld3(I->tan_x)};
-                for (int k = 0; k < 2; ++k) {
-                    V3 t = cands[k] - s_normal * dot(s_normal, cands[k]);
-                    if (len2(t) > 1.0e-12f) {
-                        V3 xx = normalize(t);
-                        fr.x = xx; fr.y = cross(s_normal, xx); fr.z = s_normal;
-                        break;
+        }
+        V3 wo = to_local(fr, -rd);
+        V3 ng = s_geom;
+        V3 origin = offset_origin(s_point, ng);
+        uint32_t dims = bounce_dim(bounce);
+        uint32_t x, y, index;
+        xyi(x, y, index);
+        uint64_t key = pixel_key(S.seed, x, y);
+        // Next-event estimation: one light; the shadow ray goes to the shadow queue.
+        Sel selection = select_at(L, s_point);
+        LightSample ls;
+        if (sample_light(L, selection, sample1(c_sobol, key, index, dims + OFF_LIGHT_SELECT), sample1(c_sobol, key, index, dims + OFF_LIGHT),
+                         sample1(c_sobol, key, index, dims + OFF_LIGHT + 1), ls)) {
+            V3 wi = to_local(fr, ls.wi);
+            Rgb f = bsdf_eval(S.energy, b, wo, wi, ls.glossy ? LOBES_ALL : LOBES_DIFFUSE);
+            if (peak(f) > 0.0f) {
+                V3 from_p = wi.z < 0.0f ? offset_origin(s_hit, -ng) : origin;
+                float weight = !ls.glossy ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(S.energy, b, wo, wi));
+                Rgb c = thr * f * ls.radiance * (absf(wi.z) * weight / ls.pdf);
+                bool finite_c = finitef(c.r) && finitef(c.g) && finitef(c.b);
+                if (finite_c && bounce >= 1 && S.clamp_indirect > 0.0f) {
+                    float p = rmax(rmax(c.r, c.g), c.b);
+                    if (p > S.clamp_indirect) c = c * (S.clamp_indirect / p);
+                }
+                if (!ls.shadow) {
+                    if (finite_c) { sum.x = sum.x + c.r; sum.y = sum.y + c.g; sum.z = sum.z + c.b; }
+                } else {
+                    shadow_local += 1;
+                    float tmax = finitef(ls.distance) ? ls.distance * (1.0f - 1.0e-4f) : f_inf();
+                    bool floor_blocks = false;
+                    if (S.floor_mode == 1 && ls.wi.z != 0.0f) {
+                        float t = (S.floor_z - from_p.z) / ls.wi.z;
+                        floor_blocks = t > 1.0e-3f && t < tmax;
+                    }
+                    if (finite_c && !floor_blocks) {
+                        uint32_t k = atomicAdd(&P.counters[2], 1u);
+                        P.sh_o[k] = make_float4(from_p.x, from_p.y, from_p.z, tmax);
+                        P.sh_d[k] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, 0.0f);
+                        P.sh_c[k] = make_float4(c.r, c.g, c.b, __uint_as_float(slot));
                     }
                 }
             }
-            V3 wo = to_local(fr, -rd);
-            V3 ng = s_geom;
-            V3 origin = offset_origin(s_point, ng);
-            uint32_t dims = bounce_dim(bounce);
-            uint32_t x, y, index;
-            wave_slot(w, slot, x, y, index);
-            uint64_t key = pixel_key(S.seed, x, y);
-            // Next-event estimation: one light; the shadow ray goes to the shadow queue.
-            Sel selection = select_at(L, s_point);
-            LightSample ls;
-            if (sample_light(L, selection, sample1(c_sobol, key, index, dims + OFF_LIGHT_SELECT), sample1(c_sobol, key, index, dims + OFF_LIGHT),
-                             sample1(c_sobol, key, index, dims + OFF_LIGHT + 1), ls)) {
-                V3 wi = to_local(fr, ls.wi);
-                Rgb f = bsdf_eval(S.energy, b, wo, wi, ls.glossy ? LOBES_ALL : LOBES_DIFFUSE);
-                if (peak(f) > 0.0f) {
-                    V3 from_p = wi.z < 0.0f ? offset_origin(s_hit, -ng) : origin;
-                    float weight = !ls.glossy ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(S.energy, b, wo, wi));
-                    Rgb c = thr * f * ls.radiance * (absf(wi.z) * weight / ls.pdf);
-                    bool finite_c = finitef(c.r) && finitef(c.g) && finitef(c.b);
-                    if (finite_c && bounce >= 1 && S.clamp_indirect > 0.0f) {
-                        float p = rmax(rmax(c.r, c.g), c.b);
-                        if (p > S.clamp_indirect) c = c * (S.clamp_indirect / p);
-                    }
-                    if (!ls.shadow) {
-                        if (finite_c) { sum.x = sum.x + c.r; sum.y = sum.y + c.g; sum.z = sum.z + c.b; }
-                    } else {
-                        shadow_local += 1;
-                        float tmax = finitef(ls.distance) ? ls.distance * (1.0f - 1.0e-4f) : f_inf();
-                        bool floor_blocks = false;
-                        if (S.floor_mode == 1 && ls.wi.z != 0.0f) {
-                            float t = (S.floor_z - from_p.z) / ls.wi.z;
-                            floor_blocks = t > 1.0e-3f && t < tmax;
-                        }
-                        if (finite_c && !floor_blocks) {
-                            uint32_t k = atomicAdd(&P.counters[2], 1u);
-                            P.sh_o[k] = make_float4(from_p.x, from_p.y, from_p.z, tmax);
-                            P.sh_d[k] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, 0.0f);
-                            P.sh_c[k] = make_float4(c.r, c.g, c.b, __uint_as_float(slot));
-                        }
-                    }
-                }
-            }
-            // The next direction.
-            BsdfSample bs;
-            if (!bsdf_sample(S.energy, b, wo, sample1(c_sobol, key, index, dims + OFF_BSDF), sample1(c_sobol, key, index, dims + OFF_BSDF + 1), bs))
-                break;
-            bool transmitted = bs.wi.z < 0.0f;
-            V3 wi = bs.straight ? rd : normalize(to_world(fr, bs.wi));
+        }
+        // The next direction.
+        BsdfSample bs;
+        if (!bsdf_sample(S.energy, b, wo, sample1(c_sobol, key, index, dims + OFF_BSDF), sample1(c_sobol, key, index, dims + OFF_BSDF + 1), bs))
+            break;
+        bool transmitted = bs.wi.z < 0.0f;
+        V3 wi = bs.straight ? rd : normalize(to_world(fr, bs.wi));
+        if (transmitted) {
+            if (dot(wi, ng) >= 0.0f) break;
+        } else if (dot(wi, ng) <= 0.0f) {
+            break;
+        }
+        thr = thr * bs.weight;
+        if (bounce >= 2) {
+            float survive = rclamp(peak(thr), 0.05f, 1.0f);
+            if (sample1(c_sobol, key, index, dims + OFF_ROULETTE) >= survive) break;
+            thr = thr / survive;
+        }
+        float pk = peak(thr);
+        if (!(pk > 0.0f && finitef(pk))) break;
+        V3 next_origin = transmitted ? offset_origin(s_hit, -ng) : origin;
+        if (bs.straight) {
+            offset += dot(next_origin - ro, rd);
+        } else {
+            flags |= PF_HAS_PDF;
+            flags &= ~PF_PRIMARY;
+            pdf = bs.pdf;
+            P.sel[slot] = make_float4(s_point.x, s_point.y, s_point.z, 0.0f);
+            offset = 0.0f;
             if (transmitted) {
-                if (dot(wi, ng) >= 0.0f) break;
-            } else if (dot(wi, ng) <= 0.0f) {
-                break;
-            }
-            thr = thr * bs.weight;
-            if (bounce >= 2) {
-                float survive = rclamp(peak(thr), 0.05f, 1.0f);
-                if (sample1(c_sobol, key, index, dims + OFF_ROULETTE) >= survive) break;
-                thr = thr / survive;
-            }
-            float pk = peak(thr);
-            if (!(pk > 0.0f && finitef(pk))) break;
-            V3 next_origin = transmitted ? offset_origin(s_hit, -ng) : origin;
-            if (bs.straight) {
-                offset += dot(next_origin - ro, rd);
-            } else {
-                flags |= PF_HAS_PDF;
-                flags &= ~PF_PRIMARY;
-                pdf = bs.pdf;
-                P.sel[slot] = make_float4(s_point.x, s_point.y, s_point.z, 0.0f);
-                offset = 0.0f;
-                if (transmitted) {
-                    if (s_outside && mat && mat->has_medium) {
-                        flags |= PF_MEDIUM;
-                        P.medium[slot] = I->material;
-                    } else {
-                        flags &= ~PF_MEDIUM;
-                    }
+                if (s_outside && mat && mat->has_medium) {
+                    flags |= PF_MEDIUM;
+                    P.medium[slot] = I->material;
+                } else {
+                    flags &= ~PF_MEDIUM;
                 }
             }
-            P.o[slot] = make_float4(next_origin.x, next_origin.y, next_origin.z, offset);
-            P.d[slot] = make_float4(wi.x, wi.y, wi.z, pdf);
-            P.flags[slot] = flags;
-            alive = true;
-        } while (false);
-        P.thr[slot] = make_float4(thr.r, thr.g, thr.b, alpha);
-        P.sum[slot] = sum;
-        if (alive) {
-            uint32_t k = atomicAdd(&P.counters[cur ^ 1], 1u);
-            P.queue[cur ^ 1][k] = slot;
+        }
+        P.o[slot] = make_float4(next_origin.x, next_origin.y, next_origin.z, offset);
+        P.d[slot] = make_float4(wi.x, wi.y, wi.z, pdf);
+        P.flags[slot] = flags;
+        alive = true;
+    } while (false);
+    P.thr[slot] = make_float4(thr.r, thr.g, thr.b, alpha);
+    P.sum[slot] = sum;
+    if (alive) {
+        uint32_t k = atomicAdd(&P.counters[cur ^ 1], 1u);
+        P.queue[cur ^ 1][k] = slot;
+    }
+}
+
+// BATCH: the slots belong to the jobs of a batched wave, each with its own constants and lights.
+template <bool BATCH>
+__global__ void __launch_bounds__(128) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, uint32_t bounce,
+                                               WaveDesc w) {
+    uint32_t n = *(volatile uint32_t*)&P.counters[cur];
+    uint32_t rays_local = 0, shadow_local = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = P.sorted[i];
+        if constexpr (BATCH) {
+            uint32_t job, x, y, index;
+            batch_slot(w, slot, job, x, y, index);
+            const JobDev& J = w.jobs[job];
+            shade_slot(J.S, *J.lights, P, slot, cur, bounce,
+                       [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { xx = x; yy = y; ii = index; }, rays_local, shadow_local);
+        } else {
+            shade_slot(S, *Lg, P, slot, cur, bounce, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { wave_slot(w, slot, xx, yy, ii); },
+                       rays_local, shadow_local);
         }
     }
     // Ray counts: camera + extension rays in rays[0], shadow rays in rays[1]; one atomic per warp.
@@ -426,26 +474,47 @@ __global__ void k_next_round(PathBuffers P, int cur) {
 }
 
 // ---- accumulate: film += each pixel's samples in sample-index order (image.rs:82) -------------------------
+// Film pixel (x, y) += the ns samples in slots slot0, slot0 + stride, ..., in that order
+// (Film::splat_alpha, image.rs:82).
+__device__ __forceinline__ void accumulate_pixel(const FilmDev& F, uint32_t x, uint32_t y, const PathBuffers& P, uint32_t slot0, uint32_t stride,
+                                                 uint32_t ns) {
+    if (x < F.ox || y < F.oy || x - F.ox >= F.w || y - F.oy >= F.h) return;
+    size_t fi = (size_t)(y - F.oy) * F.w + (x - F.ox);
+    float r = F.rgb[3 * fi], g = F.rgb[3 * fi + 1], b = F.rgb[3 * fi + 2];
+    float wt = F.weight[fi], al = F.alpha[fi], l2 = F.lum2[fi];
+    for (uint32_t s = 0; s < ns; ++s) {
+        uint32_t slot = slot0 + s * stride;
+        float4 c = P.sum[slot];
+        r = r + c.x; g = g + c.y; b = b + c.z;
+        wt = wt + 1.0f;
+        al = al + P.thr[slot].w;
+        float l = luminance(rgb(c.x, c.y, c.z));
+        l2 = l2 + l * l;
+    }
+    F.rgb[3 * fi] = r; F.rgb[3 * fi + 1] = g; F.rgb[3 * fi + 2] = b;
+    F.weight[fi] = wt; F.alpha[fi] = al; F.lum2[fi] = l2;
+}
+
 __global__ void k_accumulate(WaveDesc w, PathBuffers P, FilmDev F) {
     uint32_t npix = w.w * w.h;
     uint32_t ns = w.n / npix;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-        uint32_t x = w.x0 + p % w.w, y = w.y0 + p / w.w;
-        if (x < F.ox || y < F.oy || x - F.ox >= F.w || y - F.oy >= F.h) continue;
-        size_t fi = (size_t)(y - F.oy) * F.w + (x - F.ox);
-        float r = F.rgb[3 * fi], g = F.rgb[3 * fi + 1], b = F.rgb[3 * fi + 2];
-        float wt = F.weight[fi], al = F.alpha[fi], l2 = F.lum2[fi];
-        for (uint32_t s = 0; s < ns; ++s) {
-            uint32_t slot = s * npix + p;
-            float4 c = P.sum[slot];
-            r = r + c.x; g = g + c.y; b = b + c.z;
-            wt = wt + 1.0f;
-            al = al + P.thr[slot].w;
-            float l = luminance(rgb(c.x, c.y, c.z));
-            l2 = l2 + l * l;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x)
+        accumulate_pixel(F, w.x0 + p % w.w, w.y0 + p / w.w, P, p, npix, ns);
+}
+
+// A batched wave: every pixel of every segment into its job's film. A job has at most one segment
+// per wave, so no pixel is added twice here, and waves run in sample order.
+__global__ void k_accumulate_jobs(WaveDesc w, PathBuffers P) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < w.npix; p += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = w.nseg;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(&w.segs[mid].pix_begin) <= p) lo = mid;
+            else hi = mid;
         }
-        F.rgb[3 * fi] = r; F.rgb[3 * fi + 1] = g; F.rgb[3 * fi + 2] = b;
-        F.weight[fi] = wt; F.alpha[fi] = al; F.lum2[fi] = l2;
+        const SegDev& g = w.segs[lo];
+        uint32_t local = p - g.pix_begin, npix = g.w * g.h;
+        accumulate_pixel(w.jobs[g.job].film, local % g.w, g.y0 + local / g.w, P, g.slot_begin + local, npix, g.ns);
     }
 }
 
@@ -492,7 +561,9 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
     const int g = grid;
     const int g_ext = ext_resident > 0 && ext_resident < g ? ext_resident : g;
     const int g_sh = sh_resident > 0 && sh_resident < g ? sh_resident : g;
-    k_camera<<<g, 256, 0, st>>>(S, w, P);
+    const bool batch = w.segs != nullptr;
+    if (batch) k_camera<true><<<g, 256, 0, st>>>(S, w, P);
+    else k_camera<false><<<g, 256, 0, st>>>(S, w, P);
     int cur = 0;
     for (uint32_t bounce = 0; bounce <= S.max_depth; ++bounce) {
         if (timing && timing->ev_count + 2 <= WaveTiming::MAX_EVENTS) {
@@ -504,12 +575,14 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
         }
         k_scan<<<1, 32, 0, st>>>(P);
         k_scatter<<<g, 256, 0, st>>>(P, cur);
-        k_shade<<<g, 128, 0, st>>>(S, L, P, cur, bounce, w);
+        if (batch) k_shade<true><<<g, 128, 0, st>>>(S, L, P, cur, bounce, w);
+        else k_shade<false><<<g, 128, 0, st>>>(S, L, P, cur, bounce, w);
         k_shadow<<<g_sh, TRACE_THREADS, 0, st>>>(S, P);
         k_next_round<<<1, 1, 0, st>>>(P, cur);
         cur ^= 1;
     }
-    if (film) k_accumulate<<<g, 256, 0, st>>>(w, P, *film);
+    if (batch) k_accumulate_jobs<<<g, 256, 0, st>>>(w, P);
+    else if (film) k_accumulate<<<g, 256, 0, st>>>(w, P, *film);
 }
 
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,

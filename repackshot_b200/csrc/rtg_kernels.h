@@ -6,12 +6,26 @@
 
 namespace rtg {
 
+struct JobDev;
+
+// A segment of a batched wave: samples [first, first + ns) of the full-width rows [y0, y0 + h) of
+// one job's image. Its slots start at slot_begin (sample-major, then row-major pixels); its pixels
+// start at pix_begin in the wave's accumulation order.
+struct SegDev {
+    uint32_t job, y0, w, h, first, ns, slot_begin, pix_begin;
+};
+
 // A wave of path slots: either the pixels of the rectangle (x0, y0, w, h) for the sample
 // indices first .. first + n / (w h) - 1 (slot = s * w * h + row-major pixel), or, when `xys` is
-// set, the explicit (x, y, sample index) triples of a device array.
+// set, the explicit (x, y, sample index) triples of a device array, or, when `segs` is set, the
+// segments of a batched wave (nseg of them, sorted by slot_begin; npix pixels in all), whose jobs
+// are `jobs`.
 struct WaveDesc {
     uint32_t x0, y0, w, h, first, n;
     const uint32_t* xys;
+    const SegDev* segs;
+    const JobDev* jobs;
+    uint32_t nseg, npix;
 };
 
 // Structure-of-arrays path state of one wave (device pointers).
@@ -41,6 +55,14 @@ struct FilmDev {
     float* weight;
     float* alpha;
     float* lum2;
+};
+
+// A job of the batched render queue: its scene constants (camera, image, settings, and its own
+// instances, materials and BSDFs; the tree pointers are the shared scene's), lights and film.
+struct JobDev {
+    SceneDev S;
+    const LightsDev* lights;
+    FilmDev film;
 };
 
 // CUDA events bracketing every extend launch of a wave (optional).

@@ -357,6 +357,72 @@ def product_materials(seed: int = 7):
     return mats
 
 
+_GEOMETRY_CACHE: dict = {}
+
+
+def _product_geometry(seg_u: int, seg_v: int):
+    """The product scene's 17 meshes (16 knot parts, one per material, and the floor) and their
+    instances; built once per size."""
+    key = (seg_u, seg_v)
+    if key not in _GEOMETRY_CACHE:
+        pos, nrm, tris = torus_knot(seg_u=seg_u, seg_v=seg_v)
+        pos_mm = np.stack([pos[:, 0], -pos[:, 2], pos[:, 1]], axis=1) * np.float32(1000.0)
+        nrm_mm = np.stack([nrm[:, 0], -nrm[:, 2], nrm[:, 1]], axis=1)
+        lift = np.float32(-pos_mm[:, 2].min() + 20.0)
+        pos_mm[:, 2] += lift
+        meshes, insts = [], []
+        for k in range(16):
+            sel = tris[k::16]
+            used, inv = np.unique(sel.reshape(-1), return_inverse=True)
+            meshes.append(Mesh(pos_mm[used].astype(np.float32), nrm_mm[used].astype(np.float32), inv.astype(np.uint32), k))
+            insts.append(Instance(k, material_id=k))
+        meshes.append(floor_quad(0.0, 20000.0, 16))
+        insts.append(Instance(16, material_id=16))
+        _GEOMETRY_CACHE[key] = (meshes, tuple(insts))
+    return _GEOMETRY_CACHE[key]
+
+
+JOB_RESOLUTIONS = ((256, 256), (512, 512), (1280, 720), (1920, 1080), (2048, 1152))
+JOB_SPP = (4, 16, 64, 256)
+
+
+def light_rig(rig: int) -> List[Light]:
+    """Light rig `rig` of the batched queue's workload: 1-4 rect softboxes (count, placement,
+    size and radiance 1-20 drawn from PCG32 seeded with the rig number), aimed at the knot."""
+    g = Pcg32(rig, 11)
+    n = 1 + (g.next_u32() % 4)
+    target = (0.0, 0.0, 500.0)
+    out = []
+    for _ in range(n):
+        az = 2.0 * math.pi * g.next_f32()
+        el = math.radians(20.0 + 45.0 * g.next_f32())
+        dist = 3000.0 + 2500.0 * g.next_f32()
+        pos = (dist * math.cos(el) * math.sin(az), -dist * math.cos(el) * math.cos(az), target[2] + dist * math.sin(el))
+        d = _normalize_py(tuple(t - p for t, p in zip(target, pos)))
+        sx, sy = 800.0 + 1700.0 * g.next_f32(), 800.0 + 1700.0 * g.next_f32()
+        radiance = 1.0 + 19.0 * g.next_f32()
+        out.append(Light(0, pos, tuple(d), (0.0, 0.0, 1.0), sx, sy, (1.0, 1.0, 1.0), rect_power(radiance, sx / 1000.0, sy / 1000.0),
+                         flags=3))
+    return out
+
+
+def product_jobs(n_jobs: int = 64, seg_u: int = 1024, seg_v: int = 512, spp_scale: float = 1.0) -> List[Scene]:
+    """The batched render queue's workload on the product geometry: job j uses camera j % 8 (orbit
+    angle 45 * (j % 8) degrees, focal length 35-135 mm) and light rig j // 8 (light_rig); its
+    resolution (from JOB_RESOLUTIONS), samples per pixel (from JOB_SPP, times spp_scale) and seed are
+    drawn from PCG32 seeded with the job id. Each job is a Scene whose max_samples is its spp."""
+    jobs = []
+    rigs = [light_rig(r) for r in range((n_jobs + 7) // 8)]
+    for j in range(n_jobs):
+        g = Pcg32(j, 7)
+        w, h = JOB_RESOLUTIONS[g.next_u32() % len(JOB_RESOLUTIONS)]
+        spp = max(1, int(round(JOB_SPP[g.next_u32() % len(JOB_SPP)] * spp_scale)))
+        cam = j % 8
+        jobs.append(product_scene(width=w, height=h, spp=spp, seg_u=seg_u, seg_v=seg_v, seed=1 + (g.next_u32() & 0xFFFF),
+                                  camera_angle_deg=45.0 * cam, focal_mm=35.0 + 100.0 * cam / 7.0, rig=rigs[j // 8]))
+    return jobs
+
+
 def product_scene(width: int = 1920, height: int = 1080, spp: int = 64, depth: int = 12, seg_u: int = 1024,
                   seg_v: int = 512, seed: int = 1, camera_angle_deg: float = 0.0, focal_mm: float = 50.0,
                   rig: Sequence[Light] | None = None) -> Scene:
@@ -364,20 +430,9 @@ def product_scene(width: int = 1920, height: int = 1080, spp: int = 64, depth: i
     triangles at 1024 x 512) split round-robin by triangle id into 16 meshes, one per material
     (materials are per instance in the reference), on a floor quad, lit by three rect softboxes
     of radiance 5-20 and a gradient dome (floor 0.05, horizon 0.3, zenith 0.6)."""
-    pos, nrm, tris = torus_knot(seg_u=seg_u, seg_v=seg_v)
-    pos_mm = np.stack([pos[:, 0], -pos[:, 2], pos[:, 1]], axis=1) * np.float32(1000.0)
-    nrm_mm = np.stack([nrm[:, 0], -nrm[:, 2], nrm[:, 1]], axis=1)
-    lift = np.float32(-pos_mm[:, 2].min() + 20.0)
-    pos_mm[:, 2] += lift
+    meshes, insts = _product_geometry(seg_u, seg_v)
+    insts = list(insts)
     mats = product_materials() + [Material(base_color=(0.6, 0.6, 0.6), ior=1.0, roughness=1.0)]
-    meshes, insts = [], []
-    for k in range(16):
-        sel = tris[k::16]
-        used, inv = np.unique(sel.reshape(-1), return_inverse=True)
-        meshes.append(Mesh(pos_mm[used].astype(np.float32), nrm_mm[used].astype(np.float32), inv.astype(np.uint32), k))
-        insts.append(Instance(k, material_id=k))
-    meshes.append(floor_quad(0.0, 20000.0, 16))
-    insts.append(Instance(16, material_id=16))
     if rig is None:
         rig = [
             Light(0, (2500.0, -2500.0, 3000.0), tuple(_normalize_py((-2500.0, 2500.0, -2600.0))), (0.0, 0.0, 1.0), 1500.0,

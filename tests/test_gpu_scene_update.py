@@ -32,8 +32,9 @@ def same(a, b):
 def check_update(rtg, base, changed):
     from repackshot_b200 import scenes
     s = rtg.Scene(scenes.to_rsb(base))
-    nodes = s.nodes
+    nodes, built = s.nodes, s.build_seconds
     s.update(scenes.to_rsb(changed, meshes=False))
+    s.kept_trees = s.build_seconds == built
     fresh = rtg.Scene(scenes.to_rsb(changed))
     assert (s.width, s.height) == (fresh.width, fresh.height)
     assert same(film_bits(s), film_bits(fresh))
@@ -50,6 +51,7 @@ def test_camera_lights_materials_and_size_keep_the_trees(rtg):
     changed.width, changed.height = 320, 200
     s, fresh, nodes = check_update(rtg, base, changed)
     assert s.nodes == nodes == fresh.nodes
+    assert s.kept_trees  # the device trees were not built again
 
 
 def test_new_instance_transforms_rebuild_over_the_kept_meshes(rtg):
