@@ -31,6 +31,7 @@ extern "C" {
 #define RTG_STATUS_CUDA_ERROR 16u   /* the message is in rtg_scene_error_* */
 #define RTG_STATUS_STACK_OVERFLOW 17u
 #define RTG_STATUS_BAD_FILM 18u
+#define RTG_STATUS_BAD_ARGUMENT 19u  /* a size or count the call cannot take; the message says which */
 
 /* Largest tile rtg_render_tile accepts: 2048 x 2048 (rt-wasm/src/lib.rs:56 MAX_TILE_PIXELS). */
 #define RTG_MAX_TILE_PIXELS (1ull << 22)
@@ -141,6 +142,28 @@ uint32_t rtg_queue_create(uint32_t scene);
 uint32_t rtg_queue_add(uint32_t queue, const uint8_t* bytes, uint32_t len, uint32_t first_sample, uint32_t count, uint32_t* film);
 uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays);
 uint32_t rtg_queue_free(uint32_t queue);
+
+/* The adjoint (no reference counterpart): gradients of an image loss with respect to the scene's
+ * parameters, by path replay backpropagation. rtg_adjoint_params gives the parameter counts:
+ * every material (4 parameters: base colour R, G, B and GGX alpha = roughness^2) and every scene
+ * light (1: its power).
+ *
+ * rtg_render_adjoint clears `film`, renders samples [first_sample, first_sample + count) into it
+ * (the forward pass: the same bits as rtg_render_progressive), and returns
+ *   *loss = mean over the film's pixels and channels of (I - target)^2, I = rgb / weight, `target`
+ *           w*h*3 floats of linear RGB over the film's rectangle (row major, host memory);
+ *   grads[0 .. 4 n_materials): per material d loss / d (base R, base G, base B, alpha);
+ *   grads[4 n_materials ..): per light d loss / d power  (n_grads = 4 n_materials + n_lights).
+ * The backward pass replays every path from its pixel and sample index (nothing of the paths is
+ * stored) and propagates the loss through them; sampling decisions are held fixed (detached), so
+ * the gradient is an unbiased estimate of the gradient of the expected loss. The film must lie
+ * inside the image; every path of the call is held in one wave (168 bytes each).
+ * `residual` (may be null) receives the sum over replayed paths of |radiance left after the
+ * replay| and of |radiance|: the first is 0 up to rounding when the replay retraced the forward
+ * paths. */
+uint32_t rtg_adjoint_params(uint32_t scene, uint32_t* n_materials, uint32_t* n_lights);
+uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, uint32_t first_sample, uint32_t count, float* loss,
+                            float* grads, uint32_t n_grads, float* residual);
 
 /* Copies the film's sums to host memory (any pointer may be null): rgb 3*w*h floats, weight,
  * alpha and lum2 w*h floats each. */

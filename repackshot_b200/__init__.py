@@ -27,6 +27,7 @@ STATUS_BAD_SCENE = 4
 STATUS_CUDA_ERROR = 16
 STATUS_STACK_OVERFLOW = 17
 STATUS_BAD_FILM = 18
+STATUS_BAD_ARGUMENT = 19
 MAX_TILE_PIXELS = 1 << 22
 QUEUE_GRAPH = 1
 
@@ -53,6 +54,8 @@ ABI = {
     "rtg_queue_add": (_u32, [_u32, ctypes.c_char_p, _u32, _u32, _u32, ctypes.POINTER(_u32)]),
     "rtg_queue_run": (_u32, [_u32, _u32, ctypes.POINTER(_u64)]),
     "rtg_queue_free": (_u32, [_u32]),
+    "rtg_adjoint_params": (_u32, [_u32, ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
+    "rtg_render_adjoint": (_u32, [_u32, _u32, _f, _u32, _u32, ctypes.POINTER(ctypes.c_float), _f, _u32, _f]),
     "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_render_paths": (_u32, [_u32, _f, _u32, _f]),
@@ -180,6 +183,26 @@ class Scene:
         mode = (1 if camera else 0) | (2 if any_hit else 0)
         _check(lib().rtg_trace_rays(self.handle, _ptr(rays), n, mode, _ptr(out)))
         return out if any_hit else out.reshape(n, 3)
+
+    def adjoint_params(self):
+        """(materials, lights): the adjoint's gradient has 4 entries per material, 1 per light."""
+        nm, nl = _u32(0), _u32(0)
+        _check(lib().rtg_adjoint_params(self.handle, ctypes.byref(nm), ctypes.byref(nl)))
+        return int(nm.value), int(nl.value)
+
+    def adjoint(self, film: "Film", target: np.ndarray, first: int, count: int):
+        """rtg_render_adjoint: (loss, gradients, residual). gradients: per material d/d base R, G,
+        B and d/d alpha, then per light d/d power."""
+        nm, nl = self.adjoint_params()
+        target = np.ascontiguousarray(target, dtype=np.float32).reshape(-1)
+        grads = np.zeros(4 * nm + nl, np.float32)
+        residual = np.zeros(2, np.float32)
+        loss = ctypes.c_float(0.0)
+        status = lib().rtg_render_adjoint(self.handle, film.handle, _ptr(target), first, count, ctypes.byref(loss), _ptr(grads),
+                                          len(grads), _ptr(residual))
+        if status != STATUS_OK:
+            raise RtgError(status, error_message())
+        return float(loss.value), grads, residual
 
     def set_path_capacity(self, paths: int):
         _check(lib().rtg_set_path_capacity(self.handle, paths))

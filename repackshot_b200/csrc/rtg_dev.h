@@ -65,7 +65,8 @@ struct AreaLightDev {
     float half_x, half_y, radius, area;
     float radiance[3];
     float exponent, base, bound;
-    uint32_t rect, glossy, camera, shadow, entry, pad;
+    uint32_t rect, glossy, camera, shadow, entry;
+    uint32_t source;  // index of the scene light it was built from
 };
 constexpr int MAX_ENTRIES = 64;
 constexpr int MAX_AREAS = 63;

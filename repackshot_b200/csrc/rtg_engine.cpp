@@ -62,6 +62,11 @@ struct Scene {
     BufSet shading;   // instances, materials, BSDFs, lights: replaced by every update
     std::vector<HMesh> meshes;  // the host meshes, for updates without MESH sections
     std::string geom_key;
+    // for the adjoint: materials as uploaded, each scene light's power, each area light's scene light
+    std::vector<DevMaterial> materials_h;
+    std::vector<float> light_power;
+    std::vector<uint32_t> area_source;
+    DevBuf adjoint_mem;
     cudaStream_t stream = nullptr;
     // path buffers
     PathBuffers P{};
@@ -85,6 +90,7 @@ struct Scene {
         geometry.release();
         shading.release();
         path_mem.release();
+        adjoint_mem.release();
         if (wt) {
             for (int i = 0; i < WaveTiming::MAX_EVENTS; ++i) cudaEventDestroy(wt->ev[i]);
             delete wt;
@@ -196,6 +202,16 @@ uint32_t upload_shading(const Flat& F, BufSet& set, SceneDev& S) {
     RTG_CHECK(cudaMalloc(&set.lights, sizeof(LightsDev)));
     RTG_CHECK(cudaMemcpy(set.lights, &F.lights, sizeof(LightsDev), cudaMemcpyHostToDevice));
     return RTG_STATUS_OK;
+}
+
+// Keeps what the adjoint needs on the host: the uploaded materials, the lights' powers and which
+// scene light each area light came from.
+void keep_shading(Scene& sc, const HScene& hs, const Flat& F) {
+    sc.materials_h = F.materials;
+    sc.light_power.clear();
+    for (const HLight& l : hs.lights) sc.light_power.push_back(l.power);
+    sc.area_source.clear();
+    for (int i = 0; i < F.lights.n_areas; ++i) sc.area_source.push_back(F.lights.areas[i].source);
 }
 
 // The scene constants of `F` with the device pointers and tree fields of `geom` and `shade`.
@@ -429,6 +445,7 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     sc->S = compose(F.scene, geom, shade);
     sc->d_lights = sc->shading.lights;
     sc->geom_key = geometry_key(hs);
+    keep_shading(*sc, hs, F);
     sc->meshes = std::move(hs.meshes);
     sc->build_seconds = F.build_seconds;
     sc->nodes = F.nodes.size();
@@ -484,6 +501,7 @@ uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
     sc->shading = std::move(shading);
     sc->S = compose(F.scene, geom, shade);
     sc->d_lights = sc->shading.lights;
+    keep_shading(*sc, hs, F);
     if (!kept) sc->meshes = std::move(hs.meshes);
     sc->geom_key = std::move(key);
     sc->instanced_triangles = F.instanced_triangles;
@@ -771,6 +789,118 @@ uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays) {
     if (rays) *rays = r;
     for (auto& j : q->jobs) j->shading.release();
     q->jobs.clear();
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_adjoint_params(uint32_t scene, uint32_t* n_materials, uint32_t* n_lights) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(scene);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (!n_materials || !n_lights) return RTG_STATUS_NULL_POINTER;
+    *n_materials = (uint32_t)sc->materials_h.size();
+    *n_lights = (uint32_t)sc->light_power.size();
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, uint32_t first_sample, uint32_t count, float* loss,
+                            float* grads, uint32_t n_grads, float* residual) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(scene);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    Film* f = film_of(film);
+    if (!f || f->scene != scene) return RTG_STATUS_BAD_FILM;
+    if (!target || !loss || !grads) { g_error = "rtg_render_adjoint: null pointer"; return RTG_STATUS_NULL_POINTER; }
+    const FilmDev& F = f->dev;
+    const uint32_t nm = (uint32_t)sc->materials_h.size(), na = (uint32_t)sc->area_source.size();
+    const uint32_t nl = (uint32_t)sc->light_power.size();
+    if (n_grads != 4 * nm + nl) {
+        g_error = "rtg_render_adjoint: grads holds 4 per material and 1 per light (" + std::to_string(4 * nm + nl) + " floats)";
+        return RTG_STATUS_BAD_ARGUMENT;
+    }
+    if ((uint64_t)F.ox + F.w > sc->width || (uint64_t)F.oy + F.h > sc->height) {
+        g_error = "rtg_render_adjoint: the film must lie inside the image";
+        return RTG_STATUS_BAD_FILM;
+    }
+    if (nm > 64 || count == 0) {
+        g_error = nm > 64 ? "rtg_render_adjoint: more than 64 materials" : "rtg_render_adjoint: no samples";
+        return RTG_STATUS_BAD_ARGUMENT;
+    }
+    const uint64_t npix = (uint64_t)F.w * F.h, paths = npix * count;
+    if (paths > MAX_WAVE_PATHS) { g_error = "rtg_render_adjoint: more than 2^31 paths in one call"; return RTG_STATUS_BAD_ARGUMENT; }
+    // BSDFs of every material and side at base +- h (all channels) and alpha +- h, built as the
+    // forward ones are (flatten_scene), for the replay's central differences.
+    const float h_albedo = 1.0e-3f, h_alpha = 1.0e-3f;
+    const EnergyData& ed = energy_data();
+    EnergyTables Eh{ed.albedo.data(), ed.schlick.data(), ed.clear_in.data(), ed.clear_out.data(), ed.albedo_avg.data(), ed.schlick_avg.data()};
+    std::vector<Bsdf> tab(4 * 2 * (size_t)nm);
+    for (uint32_t m = 0; m < nm; ++m) {
+        const DevMaterial& d0 = sc->materials_h[m];
+        float alpha = d0.roughness * d0.roughness;
+        for (int v = 0; v < 4; ++v) {
+            DevMaterial d = d0;
+            if (v < 2)
+                for (int c = 0; c < 3; ++c) d.base[c] = d0.base[c] + (v == 0 ? h_albedo : -h_albedo);
+            else
+                d.roughness = sqrt_(rmax(alpha + (v == 2 ? h_alpha : -h_alpha), 0.0f));
+            tab[(size_t)v * 2 * nm + 2 * m] = bsdf_surface(Eh, d, true);
+            tab[(size_t)v * 2 * nm + 2 * m + 1] = bsdf_surface(Eh, d, false);
+        }
+    }
+    // Work arrays: the BSDF tables, the target, the per-pixel path derivatives, the gradients,
+    // the residuals and the loss.
+    const uint32_t n_params = 4 * nm + na;
+    size_t off_tab = 0, off_target = off_tab + ((tab.size() * sizeof(Bsdf) + 255) / 256) * 256;
+    size_t off_dpath = off_target + ((npix * 12 + 255) / 256) * 256;
+    size_t off_grads = off_dpath + ((npix * 16 + 255) / 256) * 256;
+    size_t off_res = off_grads + ((n_params * 4 + 255) / 256) * 256;
+    size_t off_loss = off_res + 256;
+    size_t bytes = off_loss + 256;
+    if (sc->adjoint_mem.bytes < bytes) {
+        sc->adjoint_mem.release();
+        RTG_CHECK(cudaMalloc(&sc->adjoint_mem.p, bytes));
+        sc->adjoint_mem.bytes = bytes;
+    }
+    uint8_t* base = (uint8_t*)sc->adjoint_mem.p;
+    uint32_t st = ensure_capacity(*sc, (uint32_t)paths);
+    if (st) return st;
+    cudaStream_t s = sc->stream;
+    RTG_CHECK(cudaMemcpyAsync(base + off_tab, tab.data(), tab.size() * sizeof(Bsdf), cudaMemcpyHostToDevice, s));
+    RTG_CHECK(cudaMemcpyAsync(base + off_target, target, npix * 12, cudaMemcpyHostToDevice, s));
+    RTG_CHECK(cudaMemsetAsync(base + off_grads, 0, off_loss + 8 - off_grads, s));
+    // Forward: every path of the call in one wave, into the cleared film.
+    RTG_CHECK(cudaMemsetAsync(f->mem.p, 0, f->mem.bytes, s));
+    RTG_CHECK(cudaMemsetAsync(sc->P.counters, 0, 16, s));
+    RTG_CHECK(cudaMemsetAsync(sc->P.rays, 0, 16, s));
+    WaveDesc wd{F.ox, F.oy, F.w, F.h, first_sample, (uint32_t)paths, nullptr};
+    st = run_wave(*sc, wd, &F);
+    if (st) return st;
+    // Loss and path derivatives, then the replay.
+    launch_adjoint_delta(F, (const float*)(base + off_target), (float4*)(base + off_dpath), (double*)(base + off_loss), s, grid_for((uint32_t)npix, 256));
+    const Bsdf* t0 = (const Bsdf*)(base + off_tab);
+    AdjointDev A{t0, t0 + 2 * nm, t0 + 4 * nm, t0 + 6 * nm, 1.0f / (2.0f * h_albedo), 1.0f / (2.0f * h_alpha),
+                 (const float4*)(base + off_dpath), (float*)(base + off_grads), (float*)(base + off_res), nm, na};
+    launch_adjoint_replay(sc->S, sc->d_lights, wd, sc->P, A, s, grid_for((uint32_t)paths, 128));
+    RTG_CHECK(cudaGetLastError());
+    sc->launches += 2;
+    uint64_t rays = 0;
+    st = finish(*sc, &rays);
+    if (st) return st;
+    std::vector<float> g(n_params);
+    float res[2];
+    double lossd = 0.0;
+    RTG_CHECK(cudaMemcpy(g.data(), base + off_grads, n_params * 4, cudaMemcpyDeviceToHost));
+    RTG_CHECK(cudaMemcpy(res, base + off_res, 8, cudaMemcpyDeviceToHost));
+    RTG_CHECK(cudaMemcpy(&lossd, base + off_loss, 8, cudaMemcpyDeviceToHost));
+    *loss = (float)lossd;
+    for (uint32_t k = 0; k < 4 * nm; ++k) grads[k] = g[k];
+    // An area light's radiance is proportional to its power: d/d power = d/d scale / power.
+    for (uint32_t j = 0; j < nl; ++j) grads[4 * nm + j] = 0.0f;
+    for (uint32_t i = 0; i < na; ++i) {
+        uint32_t j = sc->area_source[i];
+        float p = sc->light_power[j];
+        if (p > 0.0f) grads[4 * nm + j] += g[4 * nm + i] / p;
+    }
+    if (residual) { residual[0] = res[0]; residual[1] = res[1]; }
     return RTG_STATUS_OK;
 }
 

@@ -541,6 +541,12 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_batch(SceneDev S, const
     if (err) atomicOr(&counters[3], err);
 }
 
+}  // namespace rtg
+
+#include "rtg_adjoint.cuh"
+
+namespace rtg {
+
 // ---- launchers ---------------------------------------------------------------------------------------
 void set_sobol(const SobolTable& t, cudaStream_t s) { cudaMemcpyToSymbolAsync(c_sobol, &t, sizeof(t), 0, cudaMemcpyHostToDevice, s); }
 
@@ -585,6 +591,13 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
     else if (film) k_accumulate<<<g, 256, 0, st>>>(w, P, *film);
 }
 
+void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, cudaStream_t st, int grid) {
+    k_adjoint_delta<<<grid, 256, 0, st>>>(F, target, dpath, loss);
+}
+void launch_adjoint_replay(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
+                           int grid) {
+    k_adjoint_replay<<<grid, TRACE_THREADS, 0, st>>>(S, L, P, w, A);
+}
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,
                         cudaStream_t st, int grid) {
     k_trace_batch<<<grid, TRACE_THREADS, 0, st>>>(S, rays, n, mode, out, counters);

@@ -65,6 +65,21 @@ struct JobDev {
     FilmDev film;
 };
 
+// What the adjoint replay (rtg_adjoint.cuh) reads besides the scene and the wave.
+struct AdjointDev {
+    // per material m and side s (0 outside, 1 inside), at [2 m + s]: BSDFs at base + h, base - h
+    // (every channel), alpha + h, alpha - h
+    const Bsdf* albedo_plus;
+    const Bsdf* albedo_minus;
+    const Bsdf* alpha_plus;
+    const Bsdf* alpha_minus;
+    float inv_2h_albedo, inv_2h_alpha;
+    const float4* dpath;  // per pixel of the wave's rectangle: d loss / d (one path's radiance)
+    float* grads;         // per material base R, G, B, alpha (4 n_materials), then per area light
+    float* residual;      // [0] sum of |L_rem| at the paths' ends, [1] sum of |L|
+    uint32_t n_materials, n_areas;
+};
+
 // CUDA events bracketing every extend launch of a wave (optional).
 struct WaveTiming {
     static constexpr int MAX_EVENTS = 512;
@@ -75,6 +90,11 @@ struct WaveTiming {
 void set_sobol(const SobolTable& t, cudaStream_t s);
 void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const FilmDev* film, cudaStream_t st,
                  int grid, WaveTiming* timing);
+// The adjoint: loss and per-pixel path derivatives of a film against a target (w*h*3 floats on
+// the device), then the replay of the wave that rendered it.
+void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, cudaStream_t st, int grid);
+void launch_adjoint_replay(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
+                           int grid);
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,
                         cudaStream_t st, int grid);
 

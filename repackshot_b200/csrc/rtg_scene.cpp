@@ -536,7 +536,8 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
         return facing / (d * d);
     };
     std::vector<float> weights;
-    for (const HLight& l : s.lights) {
+    for (size_t li = 0; li < s.lights.size(); ++li) {
+        const HLight& l = s.lights[li];
         float power = rmax(l.power, 0.0f);
         uint32_t entry = (uint32_t)L.n_entries;
         AreaLightDev a;
@@ -581,6 +582,7 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
         a.camera = (l.flags & 2u) != 0;
         a.shadow = (l.flags & 4u) == 0;
         a.entry = entry;
+        a.source = (uint32_t)li;
         a.base = luminance(rgb(a.radiance[0], a.radiance[1], a.radiance[2])) * a.area * 1.0e-6f;
         L.areas[L.n_areas++] = a;
     }

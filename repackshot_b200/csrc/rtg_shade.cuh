@@ -109,7 +109,7 @@ RTG_D float power_heuristic(float pa, float pb) {
     return 1.0f / (1.0f + r * r);
 }
 
-struct LightSample { V3 wi; float distance; Rgb radiance; float pdf; bool glossy, shadow; };
+struct LightSample { V3 wi; float distance; Rgb radiance; float pdf; bool glossy, shadow; int area; };  // area: -1 environment
 
 RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, float u0, float u1, LightSample& out) {  // light.rs:1150
     int n = L.n_entries;
@@ -136,6 +136,7 @@ RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, flo
     }
     if (!(pmf > 0.0f)) return false;
     int a = L.entries[index];
+    out.area = a;
     if (a >= 0) {
         const AreaLightDev& l = L.areas[a];
         float x, y;

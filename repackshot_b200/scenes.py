@@ -357,6 +357,53 @@ def product_materials(seed: int = 7):
     return mats
 
 
+def adjoint_scene(width: int = 512, height: int = 512, spp: int = 32, depth: int = 6, perturb_seed: int = 0,
+                  subdivisions: int = 4) -> Scene:
+    """The differentiable render's scene: the small scene's geometry (camera, icosphere of radius 1
+    on a 20 x 20 floor) with the icosphere split round-robin by triangle into 16 meshes carrying
+    the product scene's 16-material table, GGX alphas drawn U(0.05, 0.8), and three rect lights.
+    With perturb_seed > 0, every base colour, alpha and light power is scaled by U(0.8, 1.2)
+    drawn from PCG32 (perturb_seed, 3): the parameters of a target image. The floor (material 16)
+    is not a parameter."""
+    base = cfg0_scene()
+    sphere = icosphere(yup_m_to_mm((0, 1, 0)), 1000.0, subdivisions, 0)
+    tris = np.asarray(sphere.indices, np.uint32).reshape(-1, 3)
+    meshes, insts = [], []
+    for k in range(16):
+        sel = tris[k::16]
+        used, inv = np.unique(sel.reshape(-1), return_inverse=True)
+        meshes.append(Mesh(np.asarray(sphere.positions, np.float32)[used], np.asarray(sphere.normals, np.float32)[used],
+                           inv.astype(np.uint32), k))
+        insts.append(Instance(k, material_id=k))
+    meshes.append(floor_quad(0.0, 10000.0, 16))
+    insts.append(Instance(16, material_id=16))
+    rng = Pcg32(3, 5)
+    mats = []
+    for m in product_materials():
+        alpha = 0.05 + 0.75 * rng.next_f32()
+        mats.append(Material(kind=m.kind, base_color=m.base_color, metallic=m.metallic, transmission=m.transmission, ior=m.ior,
+                             roughness=math.sqrt(alpha)))
+    mats.append(Material(base_color=(0.8, 0.8, 0.8), metallic=0.0, ior=1.0, roughness=1.0))
+    lights = [base.lights[0],
+              Light(0, (3000.0, -2500.0, 2500.0), tuple(_normalize_py((-3000.0, 2500.0, -1500.0))), (0.0, 0.0, 1.0), 1500.0, 1500.0,
+                    (1.0, 0.9, 0.8), rect_power(6.0, 1.5, 1.5), flags=3),
+              Light(0, (-3000.0, 1000.0, 3000.0), tuple(_normalize_py((3000.0, -1000.0, -2000.0))), (0.0, 0.0, 1.0), 1000.0, 2000.0,
+                    (0.8, 0.9, 1.0), rect_power(8.0, 1.0, 2.0), flags=3)]
+    if perturb_seed:
+        g = Pcg32(perturb_seed, 3)
+        u = lambda: 0.8 + 0.4 * g.next_f32()
+        for k in range(16):
+            m = mats[k]
+            m.base_color = tuple(c * u() for c in m.base_color)
+            m.roughness = math.sqrt(min(m.roughness ** 2 * u(), 1.0))
+        for l in lights:
+            l.power *= u()
+    base.meshes, base.instances, base.materials, base.lights = meshes, insts, mats, lights
+    base.width, base.height, base.max_samples, base.max_depth = width, height, spp, depth
+    base.focal_mm = focal_for_vfov(40.0, width, height)
+    return base
+
+
 _GEOMETRY_CACHE: dict = {}
 
 
