@@ -854,7 +854,13 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     size_t off_grads = off_dpath + ((npix * 16 + 255) / 256) * 256;
     size_t off_res = off_grads + ((n_params * 4 + 255) / 256) * 256;
     size_t off_loss = off_res + 256;
-    size_t bytes = off_loss + 256;
+    // per path slot: radiance still to come, pending BSDF term (material, two float4); per shadow
+    // ray: material gradient, material and light ids
+    size_t off_rem = off_loss + 256;
+    auto span = [&](size_t each) { return ((paths * each + 255) / 256) * 256; };
+    size_t off_pend = off_rem + span(16), off_pa = off_pend + span(4), off_pr = off_pa + span(16);
+    size_t off_shg = off_pr + span(16), off_shi = off_shg + span(16);
+    size_t bytes = off_shi + span(4);
     if (sc->adjoint_mem.bytes < bytes) {
         sc->adjoint_mem.release();
         RTG_CHECK(cudaMalloc(&sc->adjoint_mem.p, bytes));
@@ -878,10 +884,12 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     launch_adjoint_delta(F, (const float*)(base + off_target), (float4*)(base + off_dpath), (double*)(base + off_loss), s, grid_for((uint32_t)npix, 256));
     const Bsdf* t0 = (const Bsdf*)(base + off_tab);
     AdjointDev A{t0, t0 + 2 * nm, t0 + 4 * nm, t0 + 6 * nm, 1.0f / (2.0f * h_albedo), 1.0f / (2.0f * h_alpha),
-                 (const float4*)(base + off_dpath), (float*)(base + off_grads), (float*)(base + off_res), nm, na};
-    launch_adjoint_replay(sc->S, sc->d_lights, wd, sc->P, A, s, grid_for((uint32_t)paths, 128));
+                 (const float4*)(base + off_dpath), (float*)(base + off_grads), (float*)(base + off_res), nm, na,
+                 (float4*)(base + off_rem), (uint32_t*)(base + off_pend), (float4*)(base + off_pa), (float4*)(base + off_pr),
+                 (float4*)(base + off_shg), (uint32_t*)(base + off_shi)};
+    launch_adjoint_wave(sc->S, sc->d_lights, wd, sc->P, A, s, grid_for((uint32_t)paths, 128));
     RTG_CHECK(cudaGetLastError());
-    sc->launches += 2;
+    sc->launches += 3 + 6 * (uint64_t)(sc->S.max_depth + 1);
     uint64_t rays = 0;
     st = finish(*sc, &rays);
     if (st) return st;

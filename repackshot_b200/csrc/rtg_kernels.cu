@@ -594,9 +594,25 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
 void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, cudaStream_t st, int grid) {
     k_adjoint_delta<<<grid, 256, 0, st>>>(F, target, dpath, loss);
 }
-void launch_adjoint_replay(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
-                           int grid) {
-    k_adjoint_replay<<<grid, TRACE_THREADS, 0, st>>>(S, L, P, w, A);
+void launch_adjoint_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
+                         int grid) {
+    static const int ext_resident = resident_blocks((const void*)k_extend, TRACE_THREADS);
+    static const int sh_resident = resident_blocks((const void*)k_shadow_adjoint, TRACE_THREADS);
+    const int g = grid;
+    const int g_ext = ext_resident > 0 && ext_resident < g ? ext_resident : g;
+    const int g_sh = sh_resident > 0 && sh_resident < g ? sh_resident : g;
+    k_adjoint_camera<<<g, 256, 0, st>>>(S, w, P, A);
+    int cur = 0;
+    for (uint32_t bounce = 0; bounce <= S.max_depth; ++bounce) {
+        k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur);
+        k_scan<<<1, 32, 0, st>>>(P);
+        k_scatter<<<g, 256, 0, st>>>(P, cur);
+        k_shade_adjoint<<<g, 128, 0, st>>>(S, L, P, cur, bounce, w, A);
+        k_shadow_adjoint<<<g_sh, TRACE_THREADS, 0, st>>>(S, P, w, A);
+        k_next_round<<<1, 1, 0, st>>>(P, cur);
+        cur ^= 1;
+    }
+    k_adjoint_residual<<<g, 256, 0, st>>>(w, P, A);
 }
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,
                         cudaStream_t st, int grid) {

@@ -76,9 +76,18 @@ struct AdjointDev {
     float inv_2h_albedo, inv_2h_alpha;
     const float4* dpath;  // per pixel of the wave's rectangle: d loss / d (one path's radiance)
     float* grads;         // per material base R, G, B, alpha (4 n_materials), then per area light
-    float* residual;      // [0] sum of |L_rem| at the paths' ends, [1] sum of |L|
+    float* residual;      // [0] sum of |radiance left| at the paths' ends, [1] sum of |radiance|
     uint32_t n_materials, n_areas;
+    // per path slot
+    float4* rem;          // the path's radiance still to come
+    uint32_t* pend;       // material of the BSDF sample taken at the last vertex, or ADJ_NONE
+    float4* pend_albedo;  // its d f / f over base colour, per channel
+    float4* pend_alpha;   // its d f / f over alpha, per channel
+    // per shadow ray
+    float4* sh_grad;      // the material gradient it adds when unblocked: base R, G, B, alpha
+    uint32_t* sh_ids;     // material + 1 (0: none) | (area light + 1) << 16 (0: environment)
 };
+constexpr uint32_t ADJ_NONE = 0xffffffffu;
 
 // CUDA events bracketing every extend launch of a wave (optional).
 struct WaveTiming {
@@ -91,10 +100,10 @@ void set_sobol(const SobolTable& t, cudaStream_t s);
 void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const FilmDev* film, cudaStream_t st,
                  int grid, WaveTiming* timing);
 // The adjoint: loss and per-pixel path derivatives of a film against a target (w*h*3 floats on
-// the device), then the replay of the wave that rendered it.
+// the device), then the backward wave: the replay of the wave that rendered the film.
 void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, cudaStream_t st, int grid);
-void launch_adjoint_replay(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
-                           int grid);
+void launch_adjoint_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
+                         int grid);
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,
                         cudaStream_t st, int grid);
 
