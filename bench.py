@@ -173,6 +173,98 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def batched_comparison(rtg, scene, spp_scale, dist, world):
+    """The metric's plain-vs-batched half: the 64 camera x light-rig jobs of uneven resolution and
+    spp on this scene's geometry, rendered back to back through the plain path (rtg_scene_update +
+    rtg_render_progressive per job) and as one batched queue (rtg_queue_*). Wall time around
+    synchronous calls, max over ranks; each rank renders the whole job set (replicas)."""
+    from repackshot_b200 import scenes, shards
+    jobs = scenes.product_jobs(spp_scale=spp_scale)
+    rsbs = [scenes.to_rsb(j, meshes=False) for j in jobs]
+    paths = sum(j.width * j.height * j.max_samples for j in jobs)
+    # warm-up of both paths on four small jobs
+    q = rtg.Queue(scene)
+    keep = [q.add(rsbs[k], 0, 1, jobs[k].width, jobs[k].height) for k in range(4)]
+    q.run()
+    for k in range(4):
+        scene.update(rsbs[k])
+        keep.append(scene.film())
+        keep[-1].render(0, 1)
+    del keep
+    scene.synchronize()
+    t0 = time.perf_counter()
+    films = []
+    for j, b in zip(jobs, rsbs):
+        scene.update(b)
+        f = scene.film()
+        f.render(0, j.max_samples)
+        films.append(f)
+    scene.synchronize()
+    t_plain = shards.max_over_ranks(time.perf_counter() - t0, dist)
+    plain_img = films[-1].resolve()
+    del films
+    q = rtg.Queue(scene)
+    t0 = time.perf_counter()
+    films = [q.add(b, 0, j.max_samples, j.width, j.height) for j, b in zip(jobs, rsbs)]
+    q.run()
+    t_batched = shards.max_over_ranks(time.perf_counter() - t0, dist)
+    same = bool(np.array_equal(films[-1].resolve(), plain_img))
+    return {"jobs": len(jobs), "paths_per_gpu": paths, "spp_scale": spp_scale,
+            "workload": "64 jobs on the product geometry: 8 orbit cameras (0-315 deg, 35-135 mm) x 8 light rigs (1-4 "
+                        "softboxes, radiance 1-20); per job a resolution from {256^2, 512^2, 1280x720, 1920x1080, "
+                        "2048x1152} and spp from {4, 16, 64, 256} x spp_scale, drawn from PCG32 seeded with the job id",
+            "plain_back_to_back_mpaths_s": world * paths / t_plain / 1e6, "batched_mpaths_s": world * paths / t_batched / 1e6,
+            "batched_over_plain": t_plain / t_batched, "plain_s": t_plain, "batched_s": t_batched,
+            "last_job_bits_equal": same}
+
+
+def adjoint_comparison(rtg, dist, world, iterations):
+    """The metric's adjoint half on the differentiable workload (the small scene's icosphere in 16
+    materials, 512 x 512, 32 spp, depth 6, three lights; the target rendered at 512 spp with every
+    parameter perturbed by U(0.8, 1.2), PCG32 seed 3): the forward render's time, one adjoint
+    iteration's (rtg_scene_update + rtg_render_adjoint + the Adam step), and a fit of `iterations`
+    steps. Wall time around synchronous calls, max over ranks."""
+    from repackshot_b200 import fit, scenes, shards
+    W = H = 512
+    SPP, DEPTH = 32, 6
+    base = scenes.adjoint_scene(W, H, SPP, DEPTH)
+    tgt = scenes.adjoint_scene(W, H, SPP, DEPTH, perturb_seed=3)
+    ts = rtg.Scene(scenes.to_rsb(tgt))
+    tf = ts.film()
+    tf.render(100_000, 512)
+    rgb, wt, _, _ = tf.read()
+    target = (rgb / wt[..., None]).astype(np.float32)
+    s = rtg.Scene(scenes.to_rsb(base))
+    f = s.film()
+    f.render(0, SPP)
+    fwd = []
+    for i in range(5):
+        f.clear()
+        s.synchronize()
+        t0 = time.perf_counter()
+        f.render(i * SPP, SPP)
+        s.synchronize()
+        fwd.append(time.perf_counter() - t0)
+    F = fit.Fit(s, base, target, SPP, lr=0.02)
+    F.step()  # warm-up (allocations)
+    t0 = time.perf_counter()
+    for _ in range(iterations):
+        F.step()
+    s.synchronize()
+    t_fit = shards.max_over_ranks(time.perf_counter() - t0, dist)
+    t_fwd = shards.max_over_ranks(statistics.median(fwd), dist)
+    want = np.array([l.power for l in tgt.lights])
+    return {"workload": "differentiable render: small-scene icosphere split into 16 instances with the product "
+                        "material table (16 base colours, 16 GGX alphas in 0.05-0.8), 3 rect lights, 512x512, 32 spp, "
+                        "depth 6; target at parameters perturbed by U(0.8, 1.2) (PCG32 seed 3), 512 spp",
+            "forward_ms": t_fwd * 1e3, "adjoint_ms_per_iter": t_fit / iterations * 1e3,
+            "adjoint_over_forward": (t_fit / iterations) / t_fwd, "iterations": iterations,
+            "loss_first": F.state.losses[0], "loss_last": F.state.losses[-1],
+            "light_power_error_first": float(np.abs(np.array([l.power for l in base.lights]) - want).sum()),
+            "light_power_error_last": float(np.abs(F.params()[2] - want).sum()),
+            "iteration": "rtg_scene_update (parameters) + rtg_render_adjoint (forward wave, loss, backward wave) + Adam step"}
+
+
 def run_ours(args, world, rank, local, dist):
     import torch
 
@@ -237,6 +329,8 @@ def run_ours(args, world, rank, local, dist):
     e2e_local = shards.max_over_ranks(time.perf_counter() - t0, dist)
     e2e_value = world * e2e_steps * paths_step / e2e_local / 1e6
     img = film.resolve()
+    batched = batched_comparison(rtg, scene, args.batched_spp_scale, dist, world)
+    adjoint = adjoint_comparison(rtg, dist, world, args.fit_iterations)
 
     if rank != 0:
         return
@@ -292,6 +386,8 @@ def run_ours(args, world, rank, local, dist):
         "gpu_launches": launches,
         "clocks": clk,
         "image_mean": float(img.mean()),
+        "batched": batched,
+        "adjoint": adjoint,
     }
     print(json.dumps(line), flush=True)
 
@@ -302,7 +398,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--capacity", type=int, default=0, help="paths per wave (default: the library's, 16 Mi)")
+    ap.add_argument("--capacity", type=int, default=0, help="paths per wave (default: the library's automatic size)")
+    ap.add_argument("--fit-iterations", type=int, default=200, help="adjoint fit iterations of the differentiable workload")
+    ap.add_argument("--batched-spp-scale", type=float, default=0.25,
+                    help="spp of the batched-queue comparison's 64 jobs, as a fraction of theirs (1: the full 6.5 G paths)")
     args = ap.parse_args()
     if args.impl == "reference":
         # The CPU reference runs on rank 0 alone; the other ranks have no work.

@@ -155,15 +155,21 @@ uint32_t rtg_queue_free(uint32_t queue);
  *   grads[0 .. 4 n_materials): per material d loss / d (base R, base G, base B, alpha);
  *   grads[4 n_materials ..): per light d loss / d power  (n_grads = 4 n_materials + n_lights).
  * The backward pass replays every path from its pixel and sample index (nothing of the paths is
- * stored) and propagates the loss through them; sampling decisions are held fixed (detached), so
- * the gradient is an unbiased estimate of the gradient of the expected loss. The film must lie
- * inside the image; every path of the call is held in one wave (168 bytes each).
+ * stored) and propagates the loss through them; sampling decisions are held fixed (detached).
+ * By default the samples are split into two halves and each half's paths take the loss's
+ * derivative from the other half's image, which makes the gradient an unbiased estimate of the
+ * gradient of the loss of the noise-free image (a residual and a derivative from the same paths
+ * carry correlated noise, a bias towards less noise, e.g. dimmer lights). With
+ * RTG_ADJOINT_CORRELATED every path uses the residual of the whole film: the derivative of this
+ * very estimate, as a same-seed finite difference measures it.
+ * The film must lie inside the image; every path of the call is held in one wave (168 bytes each).
  * `residual` (may be null) receives the sum over replayed paths of |radiance left after the
  * replay| and of |radiance|: the first is 0 up to rounding when the replay retraced the forward
  * paths. */
+#define RTG_ADJOINT_CORRELATED 1u
 uint32_t rtg_adjoint_params(uint32_t scene, uint32_t* n_materials, uint32_t* n_lights);
-uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, uint32_t first_sample, uint32_t count, float* loss,
-                            float* grads, uint32_t n_grads, float* residual);
+uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, uint32_t first_sample, uint32_t count, uint32_t flags,
+                            float* loss, float* grads, uint32_t n_grads, float* residual);
 
 /* Copies the film's sums to host memory (any pointer may be null): rgb 3*w*h floats, weight,
  * alpha and lum2 w*h floats each. */

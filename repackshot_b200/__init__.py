@@ -30,6 +30,7 @@ STATUS_BAD_FILM = 18
 STATUS_BAD_ARGUMENT = 19
 MAX_TILE_PIXELS = 1 << 22
 QUEUE_GRAPH = 1
+ADJOINT_CORRELATED = 1
 
 LIB_PATH = Path(__file__).resolve().parent / "librtg.so"
 _lib: Optional[ctypes.CDLL] = None
@@ -55,7 +56,7 @@ ABI = {
     "rtg_queue_run": (_u32, [_u32, _u32, ctypes.POINTER(_u64)]),
     "rtg_queue_free": (_u32, [_u32]),
     "rtg_adjoint_params": (_u32, [_u32, ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
-    "rtg_render_adjoint": (_u32, [_u32, _u32, _f, _u32, _u32, ctypes.POINTER(ctypes.c_float), _f, _u32, _f]),
+    "rtg_render_adjoint": (_u32, [_u32, _u32, _f, _u32, _u32, _u32, ctypes.POINTER(ctypes.c_float), _f, _u32, _f]),
     "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_render_paths": (_u32, [_u32, _f, _u32, _f]),
@@ -190,16 +191,17 @@ class Scene:
         _check(lib().rtg_adjoint_params(self.handle, ctypes.byref(nm), ctypes.byref(nl)))
         return int(nm.value), int(nl.value)
 
-    def adjoint(self, film: "Film", target: np.ndarray, first: int, count: int):
+    def adjoint(self, film: "Film", target: np.ndarray, first: int, count: int, correlated: bool = False):
         """rtg_render_adjoint: (loss, gradients, residual). gradients: per material d/d base R, G,
-        B and d/d alpha, then per light d/d power."""
+        B and d/d alpha, then per light d/d power. By default decorrelated by sample halves (an
+        unbiased gradient for fitting); `correlated` gives the derivative of this very estimate."""
         nm, nl = self.adjoint_params()
         target = np.ascontiguousarray(target, dtype=np.float32).reshape(-1)
         grads = np.zeros(4 * nm + nl, np.float32)
         residual = np.zeros(2, np.float32)
         loss = ctypes.c_float(0.0)
-        status = lib().rtg_render_adjoint(self.handle, film.handle, _ptr(target), first, count, ctypes.byref(loss), _ptr(grads),
-                                          len(grads), _ptr(residual))
+        status = lib().rtg_render_adjoint(self.handle, film.handle, _ptr(target), first, count, ADJOINT_CORRELATED if correlated else 0,
+                                          ctypes.byref(loss), _ptr(grads), len(grads), _ptr(residual))
         if status != STATUS_OK:
             raise RtgError(status, error_message())
         return float(loss.value), grads, residual

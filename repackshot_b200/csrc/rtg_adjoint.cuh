@@ -28,6 +28,13 @@ constexpr int MAX_ADJOINT_PARAMS = 4 * 64 + MAX_AREAS;
 
 __device__ __forceinline__ Rgb rgb_sub(Rgb a, Rgb b) { return rgb(a.r - b.r, a.g - b.g, a.b - b.b); }
 
+// The loss derivative a path uses: its pixel's, from the other half of the call's samples when the
+// call has two halves (samples before A.split and from A.split on).
+__device__ __forceinline__ size_t adj_dpath_index(const AdjointDev& A, const WaveDesc& w, uint32_t x, uint32_t y, uint32_t index) {
+    const size_t p = (size_t)(y - w.y0) * w.w + (x - w.x0);
+    return index >= A.split ? p + (size_t)w.w * w.h : p;
+}
+
 __device__ __forceinline__ void adj_add(float* g, uint32_t k, float v) {
     if (v != 0.0f && finitef(v)) atomicAdd(g + k, v);
 }
@@ -96,7 +103,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
     Rgb thr = rgb(thr4.x, thr4.y, thr4.z);
     uint32_t x, y, index;
     wave_slot(w, slot, x, y, index);
-    const float4 d4p = A.dpath[(size_t)(y - w.y0) * w.w + (x - w.x0)];
+    const float4 d4p = A.dpath[adj_dpath_index(A, w, x, y, index)];
     const Rgb dl = rgb(d4p.x, d4p.y, d4p.z);
     const float4 r4 = A.rem[slot];
     Rgb rem = rgb(r4.x, r4.y, r4.z);
@@ -374,7 +381,7 @@ __device__ __forceinline__ void adjoint_unblocked(const PathBuffers& P, const Ad
     A.rem[slot] = r;
     uint32_t x, y, index;
     wave_slot(w, slot, x, y, index);
-    const float4 d4p = A.dpath[(size_t)(y - w.y0) * w.w + (x - w.x0)];
+    const float4 d4p = A.dpath[adj_dpath_index(A, w, x, y, index)];
     const uint32_t ids = A.sh_ids[i], m1 = ids & 0xffffu, a1 = ids >> 16;
     if (a1) adj_add(g, 4 * A.n_materials + a1 - 1, d4p.x * c.x + d4p.y * c.y + d4p.z * c.z);
     if (m1) {
@@ -444,22 +451,43 @@ __global__ void k_adjoint_residual(WaveDesc w, PathBuffers P, AdjointDev A) {
     if ((threadIdx.x & 31) == 0) atomicAdd(A.residual, left);
 }
 
-// The loss L = mean over the film's pixels and channels of (I - T)^2, I = rgb / weight, and per
-// pixel dL/d(one path's radiance) = 2 (I - T) / (3 npix weight). Sums the loss in double.
-__global__ void k_adjoint_delta(FilmDev F, const float* __restrict__ target, float4* dpath, double* loss) {
+// The loss L = mean over the film's pixels and channels of (I - T)^2, I = rgb / weight (all the
+// call's samples), summed in double, and the per-pixel loss derivatives the backward wave uses.
+// An L2 gradient whose residual I - T and derivative dI/dtheta come from the same paths is biased
+// (their noise is correlated). So the call's `count` samples of each pixel (slots s * npix + p of
+// the wave, s < count) are split at h = count / 2 into halves A and B with means I_A, I_B, and
+//   dL/dtheta = 1/2 [ sum_p 2 (I_B - T) / (3 npix) dI_A/dtheta + sum_p 2 (I_A - T) / (3 npix) dI_B/dtheta ],
+// an unbiased estimate: a path of half A gets dpath[p] = (I_B - T) / (3 npix h), one of half B
+// dpath[npix + p] = (I_A - T) / (3 npix (count - h)). With one sample the halves coincide (the
+// correlated estimate 2 (I - T) / (3 npix)).
+__global__ void k_adjoint_delta(FilmDev F, const float* __restrict__ target, float4* dpath, double* loss, PathBuffers P, uint32_t count) {
     const uint32_t npix = F.w * F.h;
+    const uint32_t h = count / 2;  // count 1: one estimate from all samples (the correlated one)
     double local = 0.0;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
         float wt = F.weight[p];
         float inv = wt > 0.0f ? 1.0f / wt : 0.0f;
-        float d[3];
-        for (int c = 0; c < 3; ++c) {
-            float I = F.rgb[3 * p + c] * inv;
-            float e = I - target[3 * p + c];
-            local += (double)e * (double)e;
-            d[c] = wt > 0.0f ? 2.0f * e / (3.0f * (float)npix * wt) : 0.0f;
+        float sa[3] = {0.0f, 0.0f, 0.0f}, sb[3] = {0.0f, 0.0f, 0.0f};
+        for (uint32_t k = 0; k < count; ++k) {
+            float4 c = P.sum[(size_t)k * npix + p];
+            float* acc = k < h ? sa : sb;
+            acc[0] = acc[0] + c.x; acc[1] = acc[1] + c.y; acc[2] = acc[2] + c.z;
         }
-        dpath[p] = make_float4(d[0], d[1], d[2], 0.0f);
+        float da[3], db[3];
+        for (int c = 0; c < 3; ++c) {
+            float T = target[3 * p + c];
+            float e = F.rgb[3 * p + c] * inv - T;
+            local += (double)e * (double)e;
+            if (h == 0) {
+                da[c] = db[c] = wt > 0.0f ? 2.0f * e / (3.0f * (float)npix * wt) : 0.0f;
+            } else {
+                float ia = sa[c] / (float)h, ib = sb[c] / (float)(count - h);
+                da[c] = (ib - T) / (3.0f * (float)npix * (float)h);
+                db[c] = (ia - T) / (3.0f * (float)npix * (float)(count - h));
+            }
+        }
+        dpath[p] = make_float4(da[0], da[1], da[2], 0.0f);
+        dpath[npix + p] = make_float4(db[0], db[1], db[2], 0.0f);
     }
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(loss, local / (3.0 * (double)npix));

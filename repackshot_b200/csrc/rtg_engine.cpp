@@ -802,8 +802,8 @@ uint32_t rtg_adjoint_params(uint32_t scene, uint32_t* n_materials, uint32_t* n_l
     return RTG_STATUS_OK;
 }
 
-uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, uint32_t first_sample, uint32_t count, float* loss,
-                            float* grads, uint32_t n_grads, float* residual) {
+uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, uint32_t first_sample, uint32_t count, uint32_t flags,
+                            float* loss, float* grads, uint32_t n_grads, float* residual) {
     std::lock_guard<std::mutex> lk(g_mu);
     Scene* sc = scene_of(scene);
     if (!sc) return RTG_STATUS_BAD_HANDLE;
@@ -851,7 +851,7 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     const uint32_t n_params = 4 * nm + na;
     size_t off_tab = 0, off_target = off_tab + ((tab.size() * sizeof(Bsdf) + 255) / 256) * 256;
     size_t off_dpath = off_target + ((npix * 12 + 255) / 256) * 256;
-    size_t off_grads = off_dpath + ((npix * 16 + 255) / 256) * 256;
+    size_t off_grads = off_dpath + ((2 * npix * 16 + 255) / 256) * 256;
     size_t off_res = off_grads + ((n_params * 4 + 255) / 256) * 256;
     size_t off_loss = off_res + 256;
     // per path slot: radiance still to come, pending BSDF term (material, two float4); per shadow
@@ -881,10 +881,13 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     st = run_wave(*sc, wd, &F);
     if (st) return st;
     // Loss and path derivatives, then the replay.
-    launch_adjoint_delta(F, (const float*)(base + off_target), (float4*)(base + off_dpath), (double*)(base + off_loss), s, grid_for((uint32_t)npix, 256));
+    const bool halves = count >= 2 && !(flags & RTG_ADJOINT_CORRELATED);
+    launch_adjoint_delta(F, (const float*)(base + off_target), (float4*)(base + off_dpath), (double*)(base + off_loss), sc->P,
+                         halves ? count : 1, s, grid_for((uint32_t)npix, 256));
     const Bsdf* t0 = (const Bsdf*)(base + off_tab);
     AdjointDev A{t0, t0 + 2 * nm, t0 + 4 * nm, t0 + 6 * nm, 1.0f / (2.0f * h_albedo), 1.0f / (2.0f * h_alpha),
-                 (const float4*)(base + off_dpath), (float*)(base + off_grads), (float*)(base + off_res), nm, na,
+                 (const float4*)(base + off_dpath), halves ? first_sample + count / 2 : first_sample + count,
+                 (float*)(base + off_grads), (float*)(base + off_res), nm, na,
                  (float4*)(base + off_rem), (uint32_t*)(base + off_pend), (float4*)(base + off_pa), (float4*)(base + off_pr),
                  (float4*)(base + off_shg), (uint32_t*)(base + off_shi)};
     launch_adjoint_wave(sc->S, sc->d_lights, wd, sc->P, A, s, grid_for((uint32_t)paths, 128));

@@ -591,8 +591,9 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
     else if (film) k_accumulate<<<g, 256, 0, st>>>(w, P, *film);
 }
 
-void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, cudaStream_t st, int grid) {
-    k_adjoint_delta<<<grid, 256, 0, st>>>(F, target, dpath, loss);
+void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, const PathBuffers& P, uint32_t count, cudaStream_t st,
+                          int grid) {
+    k_adjoint_delta<<<grid, 256, 0, st>>>(F, target, dpath, loss, P, count);
 }
 void launch_adjoint_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
                          int grid) {

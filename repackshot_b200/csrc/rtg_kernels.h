@@ -74,7 +74,9 @@ struct AdjointDev {
     const Bsdf* alpha_plus;
     const Bsdf* alpha_minus;
     float inv_2h_albedo, inv_2h_alpha;
-    const float4* dpath;  // per pixel of the wave's rectangle: d loss / d (one path's radiance)
+    const float4* dpath;  // d loss / d (one path's radiance): per pixel of the wave's rectangle for
+                          // samples before `split`, then per pixel for samples from `split` on
+    uint32_t split;
     float* grads;         // per material base R, G, B, alpha (4 n_materials), then per area light
     float* residual;      // [0] sum of |radiance left| at the paths' ends, [1] sum of |radiance|
     uint32_t n_materials, n_areas;
@@ -101,7 +103,8 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
                  int grid, WaveTiming* timing);
 // The adjoint: loss and per-pixel path derivatives of a film against a target (w*h*3 floats on
 // the device), then the backward wave: the replay of the wave that rendered the film.
-void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, cudaStream_t st, int grid);
+void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, const PathBuffers& P, uint32_t count, cudaStream_t st,
+                          int grid);
 void launch_adjoint_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
                          int grid);
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,

@@ -3,8 +3,9 @@
 - Its forward pass renders the film rtg_render_progressive renders, bit for bit, and its loss is
   the host's f64 loss of that film against the target.
 - The replay retraces the forward paths: the radiance left after it is 0 up to rounding.
-- Its gradients match central finite differences of the loss (same sample indices, the parameter
-  changed through rtg_scene_update). The adjoint holds sampling fixed (detached sampling); a finite
+- Its gradients (the correlated estimate: the derivative of this very loss estimate) match
+  central finite differences of the loss (same sample indices, the parameter changed through
+  rtg_scene_update). The adjoint holds sampling fixed (detached sampling); a finite
   difference lets lobe choices, GGX sample directions and roulette decisions move with the
   parameter, so the two agree in expectation and differ by Monte Carlo noise that is small only
   where those decisions do not depend on the parameter. So, at depth 2 (no roulette) and 4096 spp:
@@ -57,7 +58,7 @@ def setup(rtg):
     target = image(tf).astype(np.float32)
     s = rtg.Scene(scenes.to_rsb(base))
     f = s.film()
-    loss, grads, residual = s.adjoint(f, target, 0, SPP)
+    loss, grads, residual = s.adjoint(f, target, 0, SPP, correlated=True)
     return s, base, target, loss, grads, residual, image(f)
 
 
@@ -131,7 +132,7 @@ def deep_setup(rtg):
     tf.render(100_000, 4096)
     target = image(tf).astype(np.float32)
     s = rtg.Scene(scenes.to_rsb(base))
-    _, grads, _ = s.adjoint(s.film(), target, 0, 4096)
+    _, grads, _ = s.adjoint(s.film(), target, 0, 4096, correlated=True)
     return s, base, target, grads
 
 
@@ -194,7 +195,7 @@ def test_gradients_against_the_cpu_oracle(rtg, oracle_lib):
     rgb, wt, _, _, _ = o.render_film(500, 128, threads=8)
     target = (rgb.astype(np.float64) / wt[..., None]).astype(np.float32)
     s = rtg.Scene(scenes.to_rsb(base))
-    _, grads, _ = s.adjoint(s.film(), target, 0, spp)
+    _, grads, _ = s.adjoint(s.film(), target, 0, spp, correlated=True)
 
     def oracle_fd(kind, index, dh):
         losses = []
@@ -213,3 +214,12 @@ def test_gradients_against_the_cpu_oracle(rtg, oracle_lib):
     fd = oracle_fd("albedo", (m, c), 0.02)
     print(f"lambert material {m} channel {c}: adjoint {g:.6g} oracle finite difference {fd:.6g}")
     assert abs(g - fd) <= 1e-2 * abs(fd)
+
+
+def test_decorrelated_gradient_agrees_with_the_correlated_one_at_high_spp(rtg, deep_setup):
+    # Both estimate the same gradient; at 4096 spp their difference (the noise covariance) is small.
+    s, base, target, grads = deep_setup
+    _, dec, _ = s.adjoint(s.film(), target, 0, 4096)
+    big = np.abs(grads) > 0.2 * np.abs(grads).max()
+    assert big.sum() >= 3
+    assert np.allclose(dec[big], grads[big], rtol=0.05)
