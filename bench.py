@@ -329,8 +329,9 @@ def run_ours(args, world, rank, local, dist):
     e2e_local = shards.max_over_ranks(time.perf_counter() - t0, dist)
     e2e_value = world * e2e_steps * paths_step / e2e_local / 1e6
     img = film.resolve()
-    batched = batched_comparison(rtg, scene, args.batched_spp_scale, dist, world)
-    adjoint = adjoint_comparison(rtg, dist, world, args.fit_iterations)
+    # The metric's other halves (0 leaves a section out, e.g. for a profiler's launch list).
+    batched = batched_comparison(rtg, scene, args.batched_spp_scale, dist, world) if args.batched_spp_scale > 0 else None
+    adjoint = adjoint_comparison(rtg, dist, world, args.fit_iterations) if args.fit_iterations > 0 else None
 
     if rank != 0:
         return
