@@ -175,6 +175,18 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
  * alpha and lum2 w*h floats each. */
 uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2);
 
+/* Film::to_srgb8_tonemapped / to_srgb16_tonemapped (rt-core/src/image.rs:186-214): the film
+ * resolved (rgb / weight, black where no sample), `ev` stops of exposure (2^ev), tone curve
+ * `tonemap` (the RNDR value: 0 linear, 1 ACES, 2 filmic, 3 AgX, 4 standard; any other ACES;
+ * color.rs:95-250), sRGB-encoded and quantised as the reference quantises (v * 255 + 0.5, or
+ * * 65535, truncated): `out` w*h*3 bytes or 16-bit words, row major. */
+uint32_t rtg_film_srgb8(uint32_t film, float ev, uint32_t tonemap, uint8_t* out);
+uint32_t rtg_film_srgb16(uint32_t film, float ev, uint32_t tonemap, uint16_t* out);
+
+/* The scene's output settings from its RNDR section: exposure in stops, tone curve, samples per
+ * pixel (any pointer may be null). */
+uint32_t rtg_scene_output(uint32_t scene, float* exposure_ev, uint32_t* tonemap, uint32_t* max_samples);
+
 /* The film's device arrays (valid until rtg_film_free), for callers that stay on the GPU. */
 uint32_t rtg_film_device(uint32_t film, float** rgb, float** weight, float** alpha, float** lum2);
 

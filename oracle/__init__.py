@@ -45,6 +45,9 @@ def lib():
             "orc_sobol": (u32, [u32, u32]),
             "orc_sampler_get1": (ctypes.c_float, [u32, u32, u32, u32, u32]),
             "orc_fmath": (None, [u32, v, u32, v]),
+            "orc_film_encode": (None, [v, v, u32, ctypes.c_float, u32, v, v]),
+            "orc_color": (None, [u32, v, u32, v]),
+            "orc_agx_identity": (None, [v]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -149,3 +152,28 @@ def resolve(rgb, weight):
     w = np.asarray(weight, np.float32)
     inv = np.where(w > 0, np.float32(1.0) / np.where(w > 0, w, np.float32(1.0)), np.float32(0.0)).astype(np.float32)
     return (np.asarray(rgb, np.float32) * inv[..., None]).astype(np.float32)
+
+
+def film_encode(rgb, weight, ev, tonemap):
+    """image.rs to_srgb8_tonemapped / to_srgb16_tonemapped of film sums: (u8 (n, 3), u16 (n, 3))."""
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1)
+    weight = np.ascontiguousarray(weight, np.float32).reshape(-1)
+    n = weight.size
+    out8 = np.zeros(3 * n, np.uint8)
+    out16 = np.zeros(3 * n, np.uint16)
+    lib().orc_film_encode(_p(rgb), _p(weight), n, ev, tonemap, _p(out8), _p(out16))
+    return out8.reshape(n, 3), out16.reshape(n, 3)
+
+
+def color(which, xs):
+    """orc_color: 0 exposure, 1 ACES, 2 sRGB encode, 3 + k Tonemap k on a grey (its green)."""
+    xs = np.ascontiguousarray(xs, np.float32)
+    out = np.zeros_like(xs)
+    lib().orc_color(which, _p(xs), xs.size, _p(out))
+    return out
+
+
+def agx_identity():
+    out = np.zeros(9, np.float32)
+    lib().orc_agx_identity(_p(out))
+    return out.reshape(3, 3)

@@ -57,6 +57,9 @@ ABI = {
     "rtg_queue_free": (_u32, [_u32]),
     "rtg_adjoint_params": (_u32, [_u32, ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "rtg_render_adjoint": (_u32, [_u32, _u32, _f, _u32, _u32, _u32, ctypes.POINTER(ctypes.c_float), _f, _u32, _f]),
+    "rtg_film_srgb8": (_u32, [_u32, ctypes.c_float, _u32, _f]),
+    "rtg_film_srgb16": (_u32, [_u32, ctypes.c_float, _u32, _f]),
+    "rtg_scene_output": (_u32, [_u32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_render_paths": (_u32, [_u32, _f, _u32, _f]),
@@ -206,6 +209,12 @@ class Scene:
             raise RtgError(status, error_message())
         return float(loss.value), grads, residual
 
+    def output(self):
+        """(exposure in stops, tone curve, samples per pixel) of the scene's RNDR section."""
+        ev, tm, spp = ctypes.c_float(0.0), _u32(0), _u32(0)
+        _check(lib().rtg_scene_output(self.handle, ctypes.byref(ev), ctypes.byref(tm), ctypes.byref(spp)))
+        return float(ev.value), int(tm.value), int(spp.value)
+
     def set_path_capacity(self, paths: int):
         _check(lib().rtg_set_path_capacity(self.handle, paths))
 
@@ -254,6 +263,17 @@ class Film:
         _check(lib().rtg_film_read(self.handle, *[_ptr(a) for a in out]))
         rgb, w, a, l2 = out
         return rgb.reshape(self.h, self.w, 3), w.reshape(self.h, self.w), a.reshape(self.h, self.w), l2.reshape(self.h, self.w)
+
+    def srgb(self, ev: float | None = None, tonemap: int | None = None, bits: int = 8) -> np.ndarray:
+        """Film::to_srgb8_tonemapped / to_srgb16_tonemapped: (h, w, 3) uint8 or uint16. Exposure and
+        tone curve default to the scene's RNDR settings."""
+        sev, stm, _ = self.scene.output()
+        ev = sev if ev is None else ev
+        tonemap = stm if tonemap is None else tonemap
+        out = np.zeros((self.h, self.w, 3), np.uint8 if bits == 8 else np.uint16)
+        fn = lib().rtg_film_srgb8 if bits == 8 else lib().rtg_film_srgb16
+        _check(fn(self.handle, ev, tonemap, _ptr(out)))
+        return out
 
     def resolve(self) -> np.ndarray:
         """Film::resolve (image.rs:158): rgb * (1 / weight), black where no sample."""

@@ -65,6 +65,8 @@ struct Scene {
     // for the adjoint: materials as uploaded, each scene light's power, each area light's scene light
     std::vector<DevMaterial> materials_h;
     std::vector<float> light_power;
+    float exposure_ev = 0.0f;  // RNDR's output settings
+    uint32_t tonemap = 1, max_samples = 0;
     std::vector<uint32_t> area_source;
     DevBuf adjoint_mem;
     cudaStream_t stream = nullptr;
@@ -102,7 +104,11 @@ struct Film {
     uint32_t scene;
     FilmDev dev{};
     DevBuf mem;
-    ~Film() { mem.release(); }
+    DevBuf encoded;  // the last 8- or 16-bit image, on its way to the host
+    ~Film() {
+        mem.release();
+        encoded.release();
+    }
 };
 // A job of a render queue: one variant of the queue's scene (its own camera, image, materials,
 // lights and settings over the scene's geometry), a sample range and the film it renders into.
@@ -208,6 +214,9 @@ uint32_t upload_shading(const Flat& F, BufSet& set, SceneDev& S) {
 // scene light each area light came from.
 void keep_shading(Scene& sc, const HScene& hs, const Flat& F) {
     sc.materials_h = F.materials;
+    sc.exposure_ev = hs.exposure_ev;
+    sc.tonemap = hs.tonemap;
+    sc.max_samples = hs.max_samples;
     sc.light_power.clear();
     for (const HLight& l : hs.lights) sc.light_power.push_back(l.power);
     sc.area_source.clear();
@@ -913,6 +922,48 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     }
     if (residual) { residual[0] = res[0]; residual[1] = res[1]; }
     return RTG_STATUS_OK;
+}
+
+uint32_t rtg_scene_output(uint32_t scene, float* exposure_ev, uint32_t* tonemap, uint32_t* max_samples) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(scene);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (exposure_ev) *exposure_ev = sc->exposure_ev;
+    if (tonemap) *tonemap = sc->tonemap;
+    if (max_samples) *max_samples = sc->max_samples;
+    return RTG_STATUS_OK;
+}
+
+namespace rtg {
+namespace {
+uint32_t film_encode(uint32_t film, float ev, uint32_t tonemap, uint32_t bits, void* out) {
+    Film* f = film_of(film);
+    if (!f) return RTG_STATUS_BAD_FILM;
+    if (!out) { g_error = "rtg_film_srgb: null pointer"; return RTG_STATUS_NULL_POINTER; }
+    Scene* sc = scene_of(f->scene);
+    cudaStream_t s = sc ? sc->stream : 0;
+    size_t bytes = (size_t)f->dev.w * f->dev.h * 3 * (bits / 8);
+    if (f->encoded.bytes < bytes) {
+        f->encoded.release();
+        RTG_CHECK(cudaMalloc(&f->encoded.p, bytes));
+        f->encoded.bytes = bytes;
+    }
+    launch_film_encode(f->dev, ev, tonemap, bits, f->encoded.p, s, grid_for(f->dev.w * f->dev.h, 256));
+    RTG_CHECK(cudaGetLastError());
+    RTG_CHECK(cudaMemcpyAsync(out, f->encoded.p, bytes, cudaMemcpyDeviceToHost, s));
+    RTG_CHECK(cudaStreamSynchronize(s));
+    return RTG_STATUS_OK;
+}
+}  // namespace
+}  // namespace rtg
+
+uint32_t rtg_film_srgb8(uint32_t film, float ev, uint32_t tonemap, uint8_t* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return film_encode(film, ev, tonemap, 8, out);
+}
+uint32_t rtg_film_srgb16(uint32_t film, float ev, uint32_t tonemap, uint16_t* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return film_encode(film, ev, tonemap, 16, out);
 }
 
 uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2) {

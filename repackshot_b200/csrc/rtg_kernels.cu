@@ -5,6 +5,7 @@
 // sample order (integrator/mod.rs:1140-1891, render.rs:388-497, image.rs:82-93).
 #include <cuda_runtime.h>
 
+#include "rtg_image.cuh"
 #include "rtg_kernels.h"
 #include "rtg_shade.cuh"
 
@@ -518,6 +519,25 @@ __global__ void k_accumulate_jobs(WaveDesc w, PathBuffers P) {
     }
 }
 
+// ---- film output (image.rs:186-214): resolve, exposure, tone curve, sRGB, 8 or 16 bits ----------------
+__global__ void k_film_encode(FilmDev F, float gain, uint32_t kind, AgxMatrices agx, uint32_t bits, void* out) {
+    const uint32_t n = F.w * F.h;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        float w = F.weight[p];
+        Rgb px = rgb(0.0f, 0.0f, 0.0f);
+        if (w > 0.0f) {
+            float inv = 1.0f / w;
+            px = rgb(F.rgb[3 * p] * inv, F.rgb[3 * p + 1] * inv, F.rgb[3 * p + 2] * inv);
+        }
+        Rgb m = tonemap_apply(kind, px * gain, agx);
+        float v[3] = {srgb_encode(m.r), srgb_encode(m.g), srgb_encode(m.b)};
+        for (int c = 0; c < 3; ++c) {
+            if (bits == 8) static_cast<uint8_t*>(out)[3 * p + c] = (uint8_t)saturate_cast(v[c] * 255.0f + 0.5f, 255.0f);
+            else static_cast<uint16_t*>(out)[3 * p + c] = (uint16_t)saturate_cast(v[c] * 65535.0f + 0.5f, 65535.0f);
+        }
+    }
+}
+
 // ---- ray batches for the traversal parity harness ---------------------------------------------------
 __global__ void __launch_bounds__(TRACE_THREADS) k_trace_batch(SceneDev S, const float* __restrict__ rays, uint32_t n, uint32_t mode, uint32_t* out,
                                                      uint32_t* counters) {
@@ -614,6 +634,9 @@ void launch_adjoint_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& 
         cur ^= 1;
     }
     k_adjoint_residual<<<g, 256, 0, st>>>(w, P, A);
+}
+void launch_film_encode(const FilmDev& F, float ev, uint32_t tonemap, uint32_t bits, void* out, cudaStream_t st, int grid) {
+    k_film_encode<<<grid, 256, 0, st>>>(F, fexp2(ev), tonemap, agx_matrices(), bits, out);
 }
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,
                         cudaStream_t st, int grid) {

@@ -107,6 +107,8 @@ void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, 
                           int grid);
 void launch_adjoint_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const AdjointDev& A, cudaStream_t st,
                          int grid);
+// Film::to_srgb8_tonemapped / to_srgb16_tonemapped into `out` (device, w*h*3 bytes or words).
+void launch_film_encode(const FilmDev& F, float ev, uint32_t tonemap, uint32_t bits, void* out, cudaStream_t st, int grid);
 void launch_trace_batch(const SceneDev& S, const float* rays, uint32_t n, uint32_t mode, uint32_t* out, uint32_t* counters,
                         cudaStream_t st, int grid);
 
