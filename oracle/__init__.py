@@ -48,6 +48,11 @@ def lib():
             "orc_film_encode": (None, [v, v, u32, ctypes.c_float, u32, v, v]),
             "orc_color": (None, [u32, v, u32, v]),
             "orc_agx_identity": (None, [v]),
+            "orc_light_count": (u32, [u32]),
+            "orc_light_flux_pmf": (ctypes.c_float, [u32, u32]),
+            "orc_light_sample": (u32, [u32, v, ctypes.c_float, ctypes.c_float, ctypes.c_float, v]),
+            "orc_light_sky": (None, [u32, v, v]),
+            "orc_light_crossed": (None, [u32, v, ctypes.c_float, v]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -124,6 +129,36 @@ class OracleScene:
         st = np.zeros(2, np.uint64)
         lib().orc_trace(self.handle, _p(rays), len(rays), int(camera), int(brute), _p(hits), _p(st))
         return hits, (int(st[0]), int(st[1]))
+
+    def light_count(self):
+        return int(lib().orc_light_count(self.handle))
+
+    def light_flux_pmf(self, entry):
+        """Probability of a selection entry under the static selection, by flux."""
+        return float(lib().orc_light_flux_pmf(self.handle, entry))
+
+    def light_sample(self, x, u_select, u):
+        """Lights::sample at x: (wi, distance, radiance, pdf, delta, shadow) or None."""
+        xs = np.asarray(x, np.float32)
+        out = np.zeros(10, np.float32)
+        if not lib().orc_light_sample(self.handle, _p(xs), float(u_select), float(u[0]), float(u[1]), _p(out)):
+            return None
+        return out[0:3].copy(), float(out[3]), out[4:7].copy(), float(out[7]), bool(out[8]), bool(out[9])
+
+    def light_sky(self, direction):
+        """The sky a camera ray sees along a unit direction (environment and sun discs)."""
+        d = np.asarray(direction, np.float32)
+        out = np.zeros(3, np.float32)
+        lib().orc_light_sky(self.handle, _p(d), _p(out))
+        return out
+
+    def light_crossed(self, origin, direction, t_max=float("inf"), bsdf_pdf=None, t_min=1.0e-3):
+        """Lights a ray crosses: seen by the camera (bsdf_pdf None) or MIS-weighted for a BSDF
+        sample of that density, with the selection at the ray's origin."""
+        r = np.array([*origin, *direction, t_min, t_max], np.float32)
+        out = np.zeros(3, np.float32)
+        lib().orc_light_crossed(self.handle, _p(r), -1.0 if bsdf_pdf is None else float(bsdf_pdf), _p(out))
+        return out
 
     def occluded(self, rays):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)

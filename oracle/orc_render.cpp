@@ -586,6 +586,49 @@ void orc_energy_tables(uint16_t* u16s, float* f32s) {
     std::memcpy(f32s + 32, t.schlick_avg.data(), 32 * 4);
 }
 
+// Known-answer helpers for the lights (light.rs tests): the number of selection entries and the
+// static (by flux) probability of one; a light
+// sample at x (Lights::sample: the selection at x, then sample_selected) into out10 = wi (3),
+// distance, radiance (3), pdf, delta, shadow, 1 when there is one; the sky a camera ray sees
+// along dir (Lights::escaped with no BSDF); the lights a ray (origin, dir, t_min, t_max) crosses,
+// seen by the camera (bsdf_pdf < 0) or by a BSDF sample of that density from the ray's origin.
+uint32_t orc_light_count(uint32_t h) {
+    Loaded* l = get(h);
+    return l ? (uint32_t)l->prep.lights.entries.size() : 0u;
+}
+float orc_light_flux_pmf(uint32_t h, uint32_t entry) {
+    Loaded* l = get(h);
+    if (!l || entry >= l->prep.lights.flux_pmf.size()) return 0.0f;
+    return l->prep.lights.flux_pmf[entry];
+}
+uint32_t orc_light_sample(uint32_t h, const float* x3, float u_select, float u0, float u1, float* out10) {
+    Loaded* l = get(h);
+    if (!l) return 0;
+    const Lights& L = l->prep.lights;
+    LightSample s;
+    if (!L.sample_selected(L.select(Vec3(x3[0], x3[1], x3[2])), u_select, u0, u1, s)) return 0;
+    float v[10] = {s.wi.x, s.wi.y, s.wi.z, s.distance, s.radiance.r, s.radiance.g, s.radiance.b, s.pdf,
+                   s.delta ? 1.0f : 0.0f, s.shadow ? 1.0f : 0.0f};
+    std::memcpy(out10, v, sizeof v);
+    return 1;
+}
+void orc_light_sky(uint32_t h, const float* dir3, float* out3) {
+    Loaded* l = get(h);
+    if (!l) return;
+    Rgb e = l->prep.lights.escaped(Vec3(dir3[0], dir3[1], dir3[2]), nullptr, nullptr);
+    out3[0] = e.r; out3[1] = e.g; out3[2] = e.b;
+}
+void orc_light_crossed(uint32_t h, const float* ray8, float bsdf_pdf, float* out3) {
+    Loaded* l = get(h);
+    if (!l) return;
+    const Lights& L = l->prep.lights;
+    Ray ray(Vec3(ray8[0], ray8[1], ray8[2]), Vec3(ray8[3], ray8[4], ray8[5]));
+    ray.t_min = ray8[6];
+    Selection at = L.select(ray.origin);
+    Rgb c = L.crossed_from(ray, ray8[7], bsdf_pdf < 0.0f ? nullptr : &bsdf_pdf, &at, 0.0f);
+    out3[0] = c.r; out3[1] = c.g; out3[2] = c.b;
+}
+
 // Known-answer helpers: Pcg32, mix64, Sobol points, owen-scrambled sampler values, fmath.
 void orc_pcg32(uint64_t seed, uint64_t stream, uint32_t n, uint32_t* out) {
     Pcg32 r = Pcg32::seeded(seed, stream);

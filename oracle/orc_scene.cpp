@@ -181,7 +181,7 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             if (!(r.vec3(l.position) && r.vec3(l.direction) && r.vec3(l.up) && r.f32(l.size_x) && r.f32(l.size_y) &&
                   r.rgb(l.color) && r.f32(l.power) && r.f32(l.spread_deg) && r.f32(l.angle_deg) && r.u32(l.flags)))
                 return false;
-            if (l.kind > 1) { error = "unsupported: light kind other than rect or disk"; return false; }
+            if (l.kind == 5) { error = "unsupported: IES light"; return false; }
             scene.lights.push_back(l);
         } else if (is("ENVR")) {
             if (dup(have_env)) return false;
@@ -378,6 +378,51 @@ static void pick(const std::vector<float>& cdf, float u, size_t& i, float& rest)
     rest = width > 0.0f ? rclamp((u - lo) / width, 0.0f, 0.99999994f) : 0.0f;
 }
 
+static Vec3 uniform_cone(float u0, float u1, float one_minus_cos_max) {  // warp.rs:38
+    float one_minus_cos = u0 * one_minus_cos_max;
+    float cos = 1.0f - one_minus_cos;
+    float sin = std::sqrt(rmax(one_minus_cos * (2.0f - one_minus_cos), 0.0f));
+    float sp, cp;
+    sin_cos(TAU * u1, sp, cp);
+    return Vec3(sin * cp, sin * sp, cos);
+}
+float SphereLight::mask(Vec3 x) const {  // light.rs:368
+    if (cos_outer < -1.0f) return 1.0f;
+    Vec3 d = x - centre;
+    float len2 = length_squared(d);
+    if (!(len2 > 0.0f)) return 0.0f;
+    float c = dot(d, axis) / std::sqrt(len2);
+    if (c <= cos_outer) return 0.0f;
+    if (c >= cos_inner) return 1.0f;
+    float t = (c - cos_outer) / (cos_inner - cos_outer);
+    return t * t * (3.0f - 2.0f * t);
+}
+bool SphereLight::cone(float dist2, float& omc) const {  // light.rs:398
+    float r2 = radius * radius;
+    if (!(dist2 - r2 > 0.0f)) return false;
+    float sin2 = r2 / dist2;
+    omc = sin2 / (1.0f + std::sqrt(rmax(1.0f - sin2, 0.0f)));
+    if (omc < 1.0e-7f) omc = 0.0f;  // POINT_CONE
+    return true;
+}
+bool SphereLight::intersect(const Ray& ray, float t_max, float& t) const {  // light.rs:409
+    if (!(radius > 0.0f)) return false;
+    Vec3 oc = ray.origin - centre;
+    float r2 = radius * radius;
+    if (length_squared(oc) <= r2) return false;
+    float b = dot(oc, ray.dir);
+    float disc = r2 - length_squared(oc - ray.dir * b);
+    if (disc < 0.0f) return false;
+    t = -b - std::sqrt(disc);
+    return t > ray.t_min && t < t_max;
+}
+float SphereLight::weight(Vec3 x) const {  // light.rs:430
+    float m = mask(x);
+    if (m <= 0.0f) return 0.0f;
+    float d2 = length_squared(x - centre) * 1.0e-6f;
+    return base * m / rmax(d2, near2);
+}
+
 Lights Lights::make(const Scene& scene) {  // light.rs:673
     Lights L;
     Aabb bounds = scene.geometry.bounds;
@@ -400,6 +445,68 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
         bool shadow = (light.flags & LIGHT_FLAG_NO_SHADOW) == 0;
         float power = rmax(light.power, 0.0f);
         uint32_t entry = (uint32_t)L.entries.size();
+        Rgb color(rmax(light.color.r, 0.0f), rmax(light.color.g, 0.0f), rmax(light.color.b, 0.0f));
+        if (light.kind == (uint32_t)LightKind::Sun) {  // light.rs:755
+            Vec3 to_sun = -normalize(light.direction);
+            if (length_squared(to_sun) < 0.5f) continue;
+            float half = rmin(0.5f * rmax(light.angle_deg, 0.0f) * DEG_TO_RAD, FRAC_PI_2);
+            Rgb irradiance = color * power;
+            if (!(irradiance.luminance() > 0.0f)) continue;
+            SunLight sun{};
+            sun.delta = half < 1.0e-5f;
+            float s = fsin(0.5f * half);
+            sun.one_minus_cos_max = 2.0f * s * s;
+            float sin_max = fsin(half);
+            sun.radiance = sun.delta ? irradiance : irradiance * (1.0f / (PI * sin_max * sin_max));
+            weights.push_back(PI * irradiance.luminance());
+            L.entries.push_back({LightRef::Sun, (uint32_t)L.suns.size()});
+            sun.frame = Frame::from_normal(to_sun);
+            sun.cos_max = 1.0f - sun.one_minus_cos_max;
+            sun.solid_angle = TAU * sun.one_minus_cos_max;
+            sun.glossy = glossy;
+            sun.camera = camera;
+            sun.shadow = shadow;
+            sun.entry = entry;
+            sun.base = irradiance.luminance();
+            L.suns.push_back(sun);
+            continue;
+        }
+        if (light.kind == (uint32_t)LightKind::Point || light.kind == (uint32_t)LightKind::Spot) {  // light.rs:780
+            SphereLight sp{};
+            sp.intensity = color * (power / (4.0f * PI));
+            float radius = 0.5f * std::fabs(light.size_x);
+            sp.radius = finite(radius) ? radius : 0.0f;
+            if (light.kind == (uint32_t)LightKind::Spot) {
+                Vec3 axis = normalize(light.direction);
+                if (length_squared(axis) < 0.5f) continue;
+                float half = 0.5f * rclamp(light.spread_deg, 1.0f, 180.0f) * DEG_TO_RAD;
+                float soft = rmax(light.angle_deg, 0.0f) * DEG_TO_RAD;
+                float inner = rmax(half - soft, 0.0f);
+                sp.axis = axis;
+                sp.cos_outer = fcos(half);
+                sp.cos_inner = fcos(inner);
+            } else {
+                sp.axis = Vec3(0, 0, -1);
+                sp.cos_outer = -2.0f;
+                sp.cos_inner = -2.0f;
+            }
+            float flux = color.luminance() * power;
+            if (!(flux > 0.0f)) continue;
+            float r_m = sp.radius * 1.0e-3f;
+            sp.radiance = sp.radius > 0.0f ? sp.intensity * (1.0f / (PI * r_m * r_m)) : BLACK;
+            sp.centre = light.position;
+            sp.glossy = glossy;
+            sp.camera = camera;
+            sp.shadow = shadow;
+            sp.entry = entry;
+            sp.base = sp.intensity.luminance();
+            sp.near2 = rmax(r_m * r_m, 1.0e-6f);  // MIN_DISTANCE2_M2
+            float toward = 0.05f + 0.95f * sp.mask(centre);
+            weights.push_back(flux * toward * reach(light.position, nullptr));
+            L.entries.push_back({LightRef::Sphere, (uint32_t)L.spheres.size()});
+            L.spheres.push_back(sp);
+            continue;
+        }
         AreaLight a{};
         a.rect = light.kind == 0;
         if (a.rect) {
@@ -414,13 +521,12 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
         }
         a.frame = light_frame(light.direction, light.up);
         if (!(a.area > 0.0f) || length_squared(a.frame.z) < 0.5f) continue;
-        Rgb color(rmax(light.color.r, 0.0f), rmax(light.color.g, 0.0f), rmax(light.color.b, 0.0f));
         a.radiance = color * (power / (PI * a.area * 1.0e-6f));
         a.exponent = spread_exponent(light.spread_deg);
         float flux = color.luminance() * power * 2.0f / (a.exponent + 2.0f);
         if (!(flux > 0.0f)) continue;
         weights.push_back(flux * reach(light.position, &a.frame.z));
-        L.entries.push_back((int)L.areas.size());
+        L.entries.push_back({LightRef::Area, (uint32_t)L.areas.size()});
         a.centre = light.position;
         a.glossy = glossy;
         a.camera = camera;
@@ -438,7 +544,7 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
         weights.push_back(4.0f * PI * PI * L.env.mean_radiance());
         L.env_is_entry = true;
         L.env_entry = (uint32_t)L.entries.size();
-        L.entries.push_back(-1);
+        L.entries.push_back({LightRef::Environment, 0});
     }
     L.cdf = build_cdf(weights);
     if (L.cdf.empty()) { L.entries.clear(); L.env_is_entry = false; }
@@ -447,9 +553,14 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
     return L;
 }
 
-float Lights::weight(size_t entry, Vec3 x) const {
-    int e = entries[entry];
-    return e >= 0 ? areas[e].weight(x) : env_base;
+float Lights::weight(size_t entry, Vec3 x) const {  // light.rs:1014
+    const LightRef& e = entries[entry];
+    switch (e.kind) {
+        case LightRef::Area: return areas[e.index].weight(x);
+        case LightRef::Sun: return suns[e.index].base;
+        case LightRef::Sphere: return spheres[e.index].weight(x);
+        default: return env_base;
+    }
 }
 Selection Lights::select(Vec3 x) const {  // light.rs:1026
     size_t n = entries.size();
@@ -504,9 +615,38 @@ bool Lights::sample_selected(const Selection& from, float u_select, float u0, fl
         pick_at(from, u_select, index, rest, pmf_v);
     }
     if (!(pmf_v > 0.0f)) return false;
-    int e = entries[index];
-    if (e >= 0) {
-        const AreaLight& light = areas[e];
+    const LightRef& e = entries[index];
+    if (e.kind == LightRef::Sun) {  // light.rs:1197
+        const SunLight& sun = suns[e.index];
+        if (sun.delta) {
+            out = {sun.frame.z, F_INF, sun.radiance, pmf_v, true, sun.glossy, sun.glossy, sun.shadow};
+        } else {
+            Vec3 local = uniform_cone(u0, u1, sun.one_minus_cos_max);
+            out = {normalize(sun.frame.to_world(local)), F_INF, sun.radiance, pmf_v / sun.solid_angle, false, sun.glossy,
+                   sun.glossy, sun.shadow};
+        }
+    } else if (e.kind == LightRef::Sphere) {  // light.rs:1224
+        const SphereLight& light = spheres[e.index];
+        float m = light.mask(x);
+        Vec3 d = light.centre - x;
+        float dist2 = length_squared(d);
+        if (!(m > 0.0f && dist2 > 0.0f)) return false;
+        float dist = std::sqrt(dist2);
+        Vec3 towards = d / dist;
+        float omc = 0.0f;
+        if (light.radius > 0.0f && !light.cone(dist2, omc)) return false;
+        if (omc == 0.0f) {
+            out = {towards, dist, light.intensity * (m / (dist2 * 1.0e-6f)), pmf_v, true, light.glossy, false, light.shadow};
+        } else {
+            Vec3 local = uniform_cone(u0, u1, omc);
+            Vec3 wi = normalize(Frame::from_normal(towards).to_world(local));
+            float b = dot(wi, d);
+            float r2 = light.radius * light.radius;
+            float near = b - std::sqrt(rmax(r2 - length_squared(d - wi * b), 0.0f));
+            out = {wi, rmax(near, 0.0f), light.radiance * m, pmf_v / (TAU * omc), false, light.glossy, false, light.shadow};
+        }
+    } else if (e.kind == LightRef::Area) {
+        const AreaLight& light = areas[e.index];
         Vec3 p = light.sample_point(u0, u1);
         Vec3 d = p - x;
         float dist2 = length_squared(d);
@@ -525,7 +665,7 @@ bool Lights::sample_selected(const Selection& from, float u_select, float u0, fl
     return out.pdf > 0.0f && finite(out.pdf) && out.radiance.luminance() > 0.0f;
 }
 Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, const Selection* from, float offset) const {
-    Rgb sum = BLACK;  // light.rs:1369 crossed_areas (no sphere lights in this subset)
+    Rgb sum = BLACK;  // light.rs:1354 crossed_areas, then light.rs:1387 crossed_spheres
     for (const AreaLight& light : areas) {
         bool visible = bsdf_pdf ? light.glossy : light.camera;
         if (!visible) continue;
@@ -539,13 +679,36 @@ Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, con
         }
         sum = sum + light.radiance_at(cos) * w;
     }
+    for (const SphereLight& light : spheres) {
+        bool visible = bsdf_pdf ? light.glossy : light.camera;
+        if (!visible) continue;
+        float t;
+        if (!light.intersect(ray, t_max, t)) continue;
+        Vec3 vertex = ray.origin - ray.dir * offset;
+        float m = light.mask(vertex);
+        if (!(m > 0.0f)) continue;
+        float w = 1.0f;
+        if (bsdf_pdf) {
+            float omc;
+            if (light.cone(length_squared(light.centre - vertex), omc) && omc > 0.0f)
+                w = power_heuristic(*bsdf_pdf, pmf(light.entry, *from) / (TAU * omc));
+            else
+                w = 0.0f;
+        }
+        sum = sum + light.radiance * (m * w);
+    }
     return sum;
 }
 Rgb Lights::escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from) const {  // light.rs:1502
-    Rgb e = Rgb::splat(env.value(dir.z));
-    if (!bsdf_pdf) return e;
-    if (!env_is_entry) return e;
-    return e * power_heuristic(*bsdf_pdf, pmf(env_entry, *from) * env.pdf(dir));
+    Rgb sum = Rgb::splat(env.value(dir.z));
+    if (bsdf_pdf && env_is_entry) sum = sum * power_heuristic(*bsdf_pdf, pmf(env_entry, *from) * env.pdf(dir));
+    for (const SunLight& sun : suns) {
+        bool visible = bsdf_pdf ? sun.glossy : sun.camera;
+        if (!(visible && sun.contains(dir))) continue;
+        float w = bsdf_pdf ? power_heuristic(*bsdf_pdf, pmf(sun.entry, *from) / sun.solid_angle) : 1.0f;
+        sum = sum + sun.radiance * w;
+    }
+    return sum;
 }
 
 }  // namespace orc

@@ -91,15 +91,44 @@ struct AreaLight {
     bool intersect(const Ray& ray, float t_max, float& t, float& cos) const;
     float weight(Vec3 x) const;
 };
+struct SunLight {  // light.rs:300
+    Frame frame;  // z points at the sun
+    float cos_max, one_minus_cos_max, solid_angle;
+    Rgb radiance;  // of the disc; for a delta sun, the irradiance
+    bool delta, glossy, camera, shadow;
+    uint32_t entry;
+    float base;
+    bool contains(Vec3 dir) const { return !delta && dot(dir, frame.z) >= cos_max; }
+};
+struct SphereLight {  // light.rs:330 (point lights and spots)
+    Vec3 centre;
+    float radius;
+    Rgb intensity, radiance;
+    Vec3 axis;
+    float cos_outer, cos_inner;  // cos_outer below -1: no mask
+    bool glossy, camera, shadow;
+    uint32_t entry;
+    float base, near2;
+    float mask(Vec3 x) const;
+    bool cone(float dist2, float& omc) const;
+    bool intersect(const Ray& ray, float t_max, float& t) const;
+    float weight(Vec3 x) const;
+};
 struct Selection { Vec3 point; float total = 0; bool by_flux = true; float weights[8] = {}; };
 struct LightSample { Vec3 wi; float distance; Rgb radiance; float pdf; bool delta, glossy, photon, shadow; };
+struct LightRef {  // light.rs:488
+    enum Kind : uint32_t { Area, Sun, Sphere, Environment } kind;
+    uint32_t index;
+};
 struct Lights {
     std::vector<AreaLight> areas;
+    std::vector<SunLight> suns;
+    std::vector<SphereLight> spheres;
     Ramp env;
     bool env_is_entry = false;
     uint32_t env_entry = 0;
     float env_base = 0;
-    std::vector<int> entries;  // >= 0: area index; -1: environment
+    std::vector<LightRef> entries;
     std::vector<float> cdf, flux_pmf;
     bool per_point = false;
 

@@ -23,7 +23,7 @@
 
 namespace rtg {
 
-constexpr int MAX_ADJOINT_PARAMS = 4 * 64 + MAX_AREAS;
+constexpr int MAX_ADJOINT_PARAMS = 4 * 64 + MAX_LIGHTS;
 
 
 __device__ __forceinline__ Rgb rgb_sub(Rgb a, Rgb b) { return rgb(a.r - b.r, a.g - b.g, a.b - b.b); }
@@ -92,6 +92,30 @@ __global__ void k_adjoint_camera(SceneDev S, WaveDesc w, PathBuffers P, AdjointD
 // One vertex of the backward wave: the forward's shading (shade_slot) step for step, taking every
 // radiance term it adds off the slot's radiance still to come and adding the gradients described
 // above. A shadow ray carries its contribution and its material gradient to k_shadow_adjoint.
+// The power gradients of the suns an escaping ray sees: each sun's light is proportional to
+// its power, so its share of the path's value is <dL, thr L_sun>.
+__device__ __noinline__ void adjoint_suns(const LightsDev& L, V3 dir, bool has_pdf, float pdf, const Sel& from, Rgb thr, Rgb dl,
+                                          float* g, uint32_t base_light) {
+    for (int i = L.n_areas; i < L.n_areas + (int)L.n_suns; ++i) {
+        Rgb term;
+        if (sun_seen(L, L.lights[i], dir, has_pdf, pdf, from, term)) adj_add(g, base_light + i, adj_dot(dl, thr * term));
+    }
+}
+
+// crossed plus the sphere lights a ray crosses, each adding <dL, thr L_sphere> to its power's
+// gradient.
+__device__ __noinline__ Rgb adjoint_spheres(const LightsDev& L, Rgb crossed, V3 ro, V3 rd, float t_nearest, bool has_pdf, float pdf,
+                                            const Sel& from, float offset, Rgb thr, Rgb dl, float* g, uint32_t base_light) {
+    const int first = L.n_areas + (int)L.n_suns;
+    for (int i = first; i < first + (int)L.n_spheres; ++i) {
+        Rgb term;
+        if (!sphere_crossed(L, L.lights[i], ro, rd, 1.0e-3f, t_nearest, has_pdf, pdf, from, offset, term)) continue;
+        crossed = crossed + term;
+        adj_add(g, base_light + i, adj_dot(dl, thr * term));
+    }
+    return crossed;
+}
+
 __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const LightsDev& L, const PathBuffers& P, const AdjointDev& A, float* g,
                                                    uint32_t slot, int cur, uint32_t bounce, const WaveDesc& w) {
     float4 o4 = P.o[slot], d4 = P.d[slot], thr4 = P.thr[slot];
@@ -148,7 +172,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
     // crossed_from, light by light, in its order
     Rgb crossed = splat(0.0f);
     for (int i = 0; i < L.n_areas; ++i) {
-        const AreaLightDev& l = L.areas[i];
+        const LightDev& l = L.lights[i];
         if (!(has_pdf ? l.glossy : l.camera)) continue;
         float t, cos;
         if (!area_intersect(l, ro, rd, 1.0e-3f, t_nearest, t, cos)) continue;
@@ -162,6 +186,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
         crossed = crossed + term;
         adj_add(g, base_light + i, adj_dot(dl, thr * term));
     }
+    if (L.n_spheres) crossed = adjoint_spheres(L, crossed, ro, rd, t_nearest, has_pdf, pdf, from, offset, thr, dl, g, base_light);
     {
         float4 c4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         add_clamped(c4, thr * crossed, bounce >= 2, S.clamp_indirect);
@@ -173,12 +198,14 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
             if (primary && S.background == 0) {
                 Rgb seen = escaped(L, rd, false, 0.0f, from);
                 rem = rgb_sub(rem, thr * (S.exterior == 1.0f ? seen : seen * S.exterior));
+                if (L.n_suns) adjoint_suns(L, rd, false, 0.0f, from, thr * S.exterior, dl, g, base_light);
             } else if (primary && S.background == 1) {
                 rem = rgb_sub(rem, thr * rgb(S.background_color[0], S.background_color[1], S.background_color[2]));
             } else if (!(primary && S.background == 2)) {
                 float4 c4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 add_clamped(c4, thr * escaped(L, rd, has_pdf, pdf, from), bounce >= 2, S.clamp_indirect);
                 rem = rgb_sub(rem, rgb(c4.x, c4.y, c4.z));
+                if (L.n_suns) adjoint_suns(L, rd, has_pdf, pdf, from, thr, dl, g, base_light);
             }
             break;
         }
@@ -243,7 +270,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
             Rgb f = bsdf_eval(S.energy, b, wo, wi, lobes);
             if (peak(f) > 0.0f) {
                 V3 from_p = wi.z < 0.0f ? offset_origin(s_hit, -ng) : origin;
-                float weight = !ls.glossy ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(S.energy, b, wo, wi));
+                float weight = (ls.delta || !ls.glossy) ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(S.energy, b, wo, wi));
                 float kscale = absf(wi.z) * weight / ls.pdf;
                 Rgb c = thr * f * ls.radiance * kscale;
                 bool finite_c = finitef(c.r) && finitef(c.g) && finitef(c.b);
@@ -270,7 +297,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
                 if (!ls.shadow) {
                     if (finite_c) {
                         rem = rgb_sub(rem, c);
-                        if (ls.area >= 0) adj_add(g, base_light + (uint32_t)ls.area, adj_dot(dl, c));
+                        if (ls.light >= 0) adj_add(g, base_light + (uint32_t)ls.light, adj_dot(dl, c));
                         if (mat) {
                             adj_add(g, 4 * m + 0, mg.x);
                             adj_add(g, 4 * m + 1, mg.y);
@@ -291,7 +318,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
                         P.sh_d[k] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, 0.0f);
                         P.sh_c[k] = make_float4(c.r, c.g, c.b, __uint_as_float(slot));
                         A.sh_grad[k] = mg;
-                        A.sh_ids[k] = (mat ? m + 1 : 0u) | ((uint32_t)(ls.area + 1) << 16);
+                        A.sh_ids[k] = (mat ? m + 1 : 0u) | ((uint32_t)(ls.light + 1) << 16);
                     }
                 }
             }
@@ -364,7 +391,7 @@ __global__ void __launch_bounds__(128, 8) k_shade_adjoint(SceneDev S, const Ligh
                                                        WaveDesc w, AdjointDev A) {
     __shared__ float s_grad[MAX_ADJOINT_PARAMS];
     AdjBlock blk{s_grad};
-    const uint32_t n_params = 4 * A.n_materials + A.n_areas;
+    const uint32_t n_params = 4 * A.n_materials + A.n_lights;
     blk.begin(n_params);
     uint32_t n = *(volatile uint32_t*)&P.counters[cur];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -401,7 +428,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow_adjoint(SceneDev S, Pa
     uint64_t deep[STACK_CAP - SHORT_STACK];
     SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
     AdjBlock blk{s_grad};
-    const uint32_t n_params = 4 * A.n_materials + A.n_areas;
+    const uint32_t n_params = 4 * A.n_materials + A.n_lights;
     blk.begin(n_params);
     const uint32_t n = *(volatile uint32_t*)&P.counters[2];
     const uint32_t lane = threadIdx.x & 31u;

@@ -59,26 +59,35 @@ struct alignas(16) DevInstance {
     float pad3[3];
 };
 
-struct AreaLightDev {
+// One light of the selection (light.rs:300-360): an area light (rect or disk), a sun, or a sphere
+// light (a point light or a spot; radius 0 is a point). Each kind reads its own fields.
+enum : uint32_t { LIGHT_AREA = 0, LIGHT_SUN = 1, LIGHT_SPHERE = 2 };
+struct LightDev {
     float centre[3];
+    // area: its frame; sun: a frame whose z points at the sun; sphere: fz is a spot's axis
     float fx[3], fy[3], fz[3];
     float half_x, half_y, radius, area;
-    float radiance[3];
+    float radiance[3];  // area, sun disc (a delta sun: its irradiance), sphere surface
     float exponent, base, bound;
-    uint32_t rect, glossy, camera, shadow, entry;
+    float cos_max, one_minus_cos_max, solid_angle;  // sun
+    float intensity[3];                             // sphere: W/sr
+    float cos_outer, cos_inner, near2;              // sphere: cos_outer below -1 means no mask
+    uint32_t kind, rect, delta;
+    uint32_t glossy, camera, shadow, entry;
     uint32_t source;  // index of the scene light it was built from
 };
 constexpr int MAX_ENTRIES = 64;
-constexpr int MAX_AREAS = 63;
+constexpr int MAX_LIGHTS = 63;
 
 struct LightsDev {
+    // lights[] holds the area lights, then the suns, then the sphere lights, each in scene order
     int n_areas, n_entries, per_point, env_is_entry;
-    uint32_t env_entry, pad0, pad1, pad2;
+    uint32_t env_entry, n_suns, n_spheres, n_lights;
     float env_floor, env_horizon, env_zenith, env_lower, env_total, env_base;
-    int entries[MAX_ENTRIES];  // >= 0 area index, -1 environment
+    int entries[MAX_ENTRIES];  // >= 0 index into lights[], -1 environment
     float cdf[MAX_ENTRIES];
     float flux_pmf[MAX_ENTRIES];
-    AreaLightDev areas[MAX_AREAS];
+    LightDev lights[MAX_LIGHTS];
 };
 
 // Everything a launch needs besides the per-path buffers (constant memory).

@@ -67,7 +67,7 @@ struct Scene {
     std::vector<float> light_power;
     float exposure_ev = 0.0f;  // RNDR's output settings
     uint32_t tonemap = 1, max_samples = 0;
-    std::vector<uint32_t> area_source;
+    std::vector<uint32_t> light_source;  // scene light of each prepared light (areas, suns, spheres)
     DevBuf adjoint_mem;
     cudaStream_t stream = nullptr;
     // path buffers
@@ -219,8 +219,8 @@ void keep_shading(Scene& sc, const HScene& hs, const Flat& F) {
     sc.max_samples = hs.max_samples;
     sc.light_power.clear();
     for (const HLight& l : hs.lights) sc.light_power.push_back(l.power);
-    sc.area_source.clear();
-    for (int i = 0; i < F.lights.n_areas; ++i) sc.area_source.push_back(F.lights.areas[i].source);
+    sc.light_source.clear();
+    for (uint32_t i = 0; i < F.lights.n_lights; ++i) sc.light_source.push_back(F.lights.lights[i].source);
 }
 
 // The scene constants of `F` with the device pointers and tree fields of `geom` and `shade`.
@@ -820,7 +820,7 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     if (!f || f->scene != scene) return RTG_STATUS_BAD_FILM;
     if (!target || !loss || !grads) { g_error = "rtg_render_adjoint: null pointer"; return RTG_STATUS_NULL_POINTER; }
     const FilmDev& F = f->dev;
-    const uint32_t nm = (uint32_t)sc->materials_h.size(), na = (uint32_t)sc->area_source.size();
+    const uint32_t nm = (uint32_t)sc->materials_h.size(), na = (uint32_t)sc->light_source.size();
     const uint32_t nl = (uint32_t)sc->light_power.size();
     if (n_grads != 4 * nm + nl) {
         g_error = "rtg_render_adjoint: grads holds 4 per material and 1 per light (" + std::to_string(4 * nm + nl) + " floats)";
@@ -913,10 +913,10 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     RTG_CHECK(cudaMemcpy(&lossd, base + off_loss, 8, cudaMemcpyDeviceToHost));
     *loss = (float)lossd;
     for (uint32_t k = 0; k < 4 * nm; ++k) grads[k] = g[k];
-    // An area light's radiance is proportional to its power: d/d power = d/d scale / power.
+    // Every light's radiance is proportional to its power: d/d power = d/d scale / power.
     for (uint32_t j = 0; j < nl; ++j) grads[4 * nm + j] = 0.0f;
     for (uint32_t i = 0; i < na; ++i) {
-        uint32_t j = sc->area_source[i];
+        uint32_t j = sc->light_source[i];
         float p = sc->light_power[j];
         if (p > 0.0f) grads[4 * nm + j] += g[4 * nm + i] / p;
     }

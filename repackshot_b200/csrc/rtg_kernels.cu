@@ -311,7 +311,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
             Rgb f = bsdf_eval(S.energy, b, wo, wi, ls.glossy ? LOBES_ALL : LOBES_DIFFUSE);
             if (peak(f) > 0.0f) {
                 V3 from_p = wi.z < 0.0f ? offset_origin(s_hit, -ng) : origin;
-                float weight = !ls.glossy ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(S.energy, b, wo, wi));
+                float weight = (ls.delta || !ls.glossy) ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(S.energy, b, wo, wi));
                 Rgb c = thr * f * ls.radiance * (absf(wi.z) * weight / ls.pdf);
                 bool finite_c = finitef(c.r) && finitef(c.g) && finitef(c.b);
                 if (finite_c && bounce >= 1 && S.clamp_indirect > 0.0f) {

@@ -77,9 +77,9 @@ struct AdjointDev {
     const float4* dpath;  // d loss / d (one path's radiance): per pixel of the wave's rectangle for
                           // samples before `split`, then per pixel for samples from `split` on
     uint32_t split;
-    float* grads;         // per material base R, G, B, alpha (4 n_materials), then per area light
+    float* grads;         // per material base R, G, B, alpha (4 n_materials), then per light
     float* residual;      // [0] sum of |radiance left| at the paths' ends, [1] sum of |radiance|
-    uint32_t n_materials, n_areas;
+    uint32_t n_materials, n_lights;
     // per path slot
     float4* rem;          // the path's radiance still to come
     uint32_t* pend;       // material of the BSDF sample taken at the last vertex, or ADJ_NONE
@@ -87,7 +87,7 @@ struct AdjointDev {
     float4* pend_alpha;   // its d f / f over alpha, per channel
     // per shadow ray
     float4* sh_grad;      // the material gradient it adds when unblocked: base R, G, B, alpha
-    uint32_t* sh_ids;     // material + 1 (0: none) | (area light + 1) << 16 (0: environment)
+    uint32_t* sh_ids;     // material + 1 (0: none) | (light + 1) << 16 (0: environment)
 };
 constexpr uint32_t ADJ_NONE = 0xffffffffu;
 

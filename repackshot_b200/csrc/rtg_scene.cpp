@@ -2,6 +2,8 @@
 // light preparation. See rtg_scene.h.
 #include "rtg_scene.h"
 
+#include "rtg_lights.cuh"
+
 #include "rtg_tables.h"
 
 #include <chrono>
@@ -166,7 +168,7 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (!(r.vec3(l.position) && r.vec3(l.direction) && r.vec3(l.up) && r.f32(l.size_x) && r.f32(l.size_y) && r.f3(l.color) &&
                   r.f32(l.power) && r.f32(l.spread_deg) && r.f32(l.angle_deg) && r.u32(l.flags)))
                 return false;
-            if (l.kind > 1) { error = "unsupported: light kind other than rect or disk"; return false; }
+            if (l.kind == 5) { error = "unsupported: IES light"; return false; }
             s.lights.push_back(l);
         } else if (is("ENVR")) {
             if (!once(seen_env)) return false;
@@ -535,57 +537,124 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
         d = rmax(d, radius_m);
         return facing / (d * d);
     };
+    // Each kind is collected in scene order; the selection entries keep the scene's order and
+    // point into lights[] once the kinds are laid out as areas, then suns, then spheres.
     std::vector<float> weights;
+    std::vector<LightDev> kinds[3];
+    std::vector<std::pair<uint32_t, uint32_t>> refs;  // (kind, index in its kind) per entry
+    auto put3 = [](float* d, V3 v) { d[0] = v.x; d[1] = v.y; d[2] = v.z; };
     for (size_t li = 0; li < s.lights.size(); ++li) {
         const HLight& l = s.lights[li];
         float power = rmax(l.power, 0.0f);
-        uint32_t entry = (uint32_t)L.n_entries;
-        AreaLightDev a;
-        std::memset(&a, 0, sizeof(a));
-        a.rect = l.kind == 0;
-        if (a.rect) {
-            a.half_x = 0.5f * absf(l.size_x);
-            a.half_y = 0.5f * absf(l.size_y);
-            a.area = 4.0f * a.half_x * a.half_y;
-            a.bound = sqrt_(a.half_x * a.half_x + a.half_y * a.half_y);
-        } else {
-            a.radius = 0.5f * absf(l.size_x);
-            a.area = PI * a.radius * a.radius;
-            a.bound = a.radius;
-        }
-        // light_frame (light.rs:245)
-        V3 z = normalize(l.direction);
-        V3 y = normalize(l.up - z * dot(z, l.up));
-        Frame f;
-        if (len2(y) < 0.5f) f = frame_from_normal(z);
-        else { f.x = cross(y, z); f.y = y; f.z = z; }
-        if (!(a.area > 0.0f) || len2(f.z) < 0.5f) continue;
+        uint32_t entry = (uint32_t)refs.size();
         float color[3] = {rmax(l.color[0], 0.0f), rmax(l.color[1], 0.0f), rmax(l.color[2], 0.0f)};
-        float k = power / (PI * a.area * 1.0e-6f);
-        a.radiance[0] = color[0] * k; a.radiance[1] = color[1] * k; a.radiance[2] = color[2] * k;
-        if (l.spread_deg >= 180.0f) a.exponent = 0.0f;
-        else {
-            float half = 0.5f * rmax(l.spread_deg, 1.0f) * (PI / 180.0f);
-            a.exponent = -1.0f / flog2(fcos(half));
-        }
         float lum = 0.2126f * color[0] + 0.7152f * color[1] + 0.0722f * color[2];
-        float flux = lum * power * 2.0f / (a.exponent + 2.0f);
-        if (!(flux > 0.0f)) continue;
-        if (L.n_areas >= MAX_AREAS) { error = "unsupported: more than 63 area lights"; return false; }
-        weights.push_back(flux * reach(l.position, &f.z));
-        L.entries[L.n_entries++] = L.n_areas;
-        a.centre[0] = l.position.x; a.centre[1] = l.position.y; a.centre[2] = l.position.z;
-        a.fx[0] = f.x.x; a.fx[1] = f.x.y; a.fx[2] = f.x.z;
-        a.fy[0] = f.y.x; a.fy[1] = f.y.y; a.fy[2] = f.y.z;
-        a.fz[0] = f.z.x; a.fz[1] = f.z.y; a.fz[2] = f.z.z;
+        LightDev a;
+        std::memset(&a, 0, sizeof(a));
         a.glossy = (l.flags & 1u) != 0;
         a.camera = (l.flags & 2u) != 0;
         a.shadow = (l.flags & 4u) == 0;
         a.entry = entry;
         a.source = (uint32_t)li;
-        a.base = luminance(rgb(a.radiance[0], a.radiance[1], a.radiance[2])) * a.area * 1.0e-6f;
-        L.areas[L.n_areas++] = a;
+        if (l.kind == 2) {  // sun (light.rs:755)
+            V3 to_sun = -normalize(l.direction);
+            if (len2(to_sun) < 0.5f) continue;
+            float half = rmin(0.5f * rmax(l.angle_deg, 0.0f) * (PI / 180.0f), FRAC_PI_2);
+            Rgb irr = rgb(color[0] * power, color[1] * power, color[2] * power);
+            if (!(luminance(irr) > 0.0f)) continue;
+            a.kind = LIGHT_SUN;
+            a.delta = half < 1.0e-5f;
+            float sh, ch;
+            sin_cos(0.5f * half, sh, ch);
+            a.one_minus_cos_max = 2.0f * sh * sh;
+            float sin_max, cos_half;
+            sin_cos(half, sin_max, cos_half);
+            Rgb rad = a.delta ? irr : irr * (1.0f / (PI * sin_max * sin_max));
+            a.radiance[0] = rad.r; a.radiance[1] = rad.g; a.radiance[2] = rad.b;
+            weights.push_back(PI * luminance(irr));
+            Frame f = frame_from_normal(to_sun);
+            put3(a.fx, f.x); put3(a.fy, f.y); put3(a.fz, f.z);
+            a.cos_max = 1.0f - a.one_minus_cos_max;
+            a.solid_angle = TAU * a.one_minus_cos_max;
+            a.base = luminance(irr);
+        } else if (l.kind == 3 || l.kind == 4) {  // point light or spot (light.rs:780)
+            a.kind = LIGHT_SPHERE;
+            float k = power / (4.0f * PI);
+            a.intensity[0] = color[0] * k; a.intensity[1] = color[1] * k; a.intensity[2] = color[2] * k;
+            float radius = 0.5f * absf(l.size_x);
+            a.radius = finitef(radius) ? radius : 0.0f;
+            V3 axis = v3(0.0f, 0.0f, -1.0f);
+            if (l.kind == 4) {
+                axis = normalize(l.direction);
+                if (len2(axis) < 0.5f) continue;
+                float half = 0.5f * rclamp(l.spread_deg, 1.0f, 180.0f) * (PI / 180.0f);
+                float soft = rmax(l.angle_deg, 0.0f) * (PI / 180.0f);
+                float inner = rmax(half - soft, 0.0f);
+                a.cos_outer = fcos(half);
+                a.cos_inner = fcos(inner);
+            } else {
+                a.cos_outer = -2.0f;
+                a.cos_inner = -2.0f;
+            }
+            put3(a.fz, axis);
+            float flux = lum * power;
+            if (!(flux > 0.0f)) continue;
+            float r_m = a.radius * 1.0e-3f;
+            if (a.radius > 0.0f) {
+                float kr = 1.0f / (PI * r_m * r_m);
+                a.radiance[0] = a.intensity[0] * kr; a.radiance[1] = a.intensity[1] * kr; a.radiance[2] = a.intensity[2] * kr;
+            }
+            put3(a.centre, l.position);
+            a.base = luminance(rgb(a.intensity[0], a.intensity[1], a.intensity[2]));
+            a.near2 = rmax(r_m * r_m, 1.0e-6f);
+            float toward = 0.05f + 0.95f * sphere_mask(a, centre);
+            weights.push_back(flux * toward * reach(l.position, nullptr));
+        } else {  // rect or disk
+            a.kind = LIGHT_AREA;
+            a.rect = l.kind == 0;
+            if (a.rect) {
+                a.half_x = 0.5f * absf(l.size_x);
+                a.half_y = 0.5f * absf(l.size_y);
+                a.area = 4.0f * a.half_x * a.half_y;
+                a.bound = sqrt_(a.half_x * a.half_x + a.half_y * a.half_y);
+            } else {
+                a.radius = 0.5f * absf(l.size_x);
+                a.area = PI * a.radius * a.radius;
+                a.bound = a.radius;
+            }
+            // light_frame (light.rs:245)
+            V3 z = normalize(l.direction);
+            V3 y = normalize(l.up - z * dot(z, l.up));
+            Frame f;
+            if (len2(y) < 0.5f) f = frame_from_normal(z);
+            else { f.x = cross(y, z); f.y = y; f.z = z; }
+            if (!(a.area > 0.0f) || len2(f.z) < 0.5f) continue;
+            float k = power / (PI * a.area * 1.0e-6f);
+            a.radiance[0] = color[0] * k; a.radiance[1] = color[1] * k; a.radiance[2] = color[2] * k;
+            if (l.spread_deg >= 180.0f) a.exponent = 0.0f;
+            else {
+                float half = 0.5f * rmax(l.spread_deg, 1.0f) * (PI / 180.0f);
+                a.exponent = -1.0f / flog2(fcos(half));
+            }
+            float flux = lum * power * 2.0f / (a.exponent + 2.0f);
+            if (!(flux > 0.0f)) continue;
+            weights.push_back(flux * reach(l.position, &f.z));
+            put3(a.centre, l.position);
+            put3(a.fx, f.x); put3(a.fy, f.y); put3(a.fz, f.z);
+            a.base = luminance(rgb(a.radiance[0], a.radiance[1], a.radiance[2])) * a.area * 1.0e-6f;
+        }
+        if (refs.size() >= (size_t)MAX_LIGHTS) { error = "unsupported: more than 63 lights"; return false; }
+        refs.push_back({a.kind, (uint32_t)kinds[a.kind].size()});
+        kinds[a.kind].push_back(a);
     }
+    uint32_t first[3] = {0, (uint32_t)kinds[0].size(), (uint32_t)(kinds[0].size() + kinds[1].size())};
+    for (int k = 0; k < 3; ++k)
+        for (size_t i = 0; i < kinds[k].size(); ++i) L.lights[first[k] + i] = kinds[k][i];
+    L.n_areas = (int)kinds[0].size();
+    L.n_suns = (uint32_t)kinds[1].size();
+    L.n_spheres = (uint32_t)kinds[2].size();
+    L.n_lights = (uint32_t)refs.size();
+    for (const auto& r : refs) L.entries[L.n_entries++] = (int)(first[r.first] + r.second);
     // environment.rs:333 ramp (flat: three equal stops)
     float strength = rmax(s.env_strength, 0.0f);
     float f0 = s.env_kind == 1 ? s.env_horizon : s.env_floor, z0 = s.env_kind == 1 ? s.env_horizon : s.env_zenith;

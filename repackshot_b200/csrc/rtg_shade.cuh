@@ -1,11 +1,10 @@
 // Lights, environment and camera on the device (engine/crates/rt-core/src/light.rs:120-1552,
 // environment.rs:275-441, scene/mod.rs:280-359, render.rs:79-97, pixel_filter.rs:103-130).
 #pragma once
+#include "rtg_lights.cuh"
 #include "rtg_trace.cuh"
 
 namespace rtg {
-
-RTG_D V3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
 
 // ---- environment ramp ---------------------------------------------------------------------------
 RTG_D float env_value(const LightsDev& L, float z) {
@@ -41,52 +40,16 @@ RTG_D bool env_sample(const LightsDev& L, float u0, float u1, V3& dir, float& pd
     return pdf > 0.0f;
 }
 
-// ---- area lights --------------------------------------------------------------------------------
-RTG_D float orientation_bound(V3 v, float d2, V3 axis, float bound) {  // light.rs:260 with θo = 0
-    if (d2 <= bound * bound) return 1.0f;
-    const float cos_o = 1.0f, sin_o = 0.0f;
-    float inv_d = 1.0f / sqrt_(d2);
-    float sin_u = bound * inv_d;
-    float cos_u = sqrt_(rmax(1.0f - sin_u * sin_u, 0.0f));
-    float cos_s = cos_o * cos_u - sin_o * sin_u;
-    float sin_s = sin_o * cos_u + cos_o * sin_u;
-    if (sin_s < 0.0f) return 1.0f;
-    float cos_t = dot(v, axis) * inv_d;
-    if (cos_t >= cos_s) return 1.0f;
-    float sin_t = sqrt_(rmax(1.0f - cos_t * cos_t, 0.0f));
-    return rmax(cos_t * cos_s + sin_t * sin_s, 0.0f);
-}
-RTG_D float area_weight(const AreaLightDev& a, V3 x) {
-    V3 v = x - ld3(a.centre);
-    float d2 = len2(v);
-    float o = orientation_bound(v, d2, ld3(a.fz), a.bound);
-    if (o <= 0.0f) return 0.0f;
-    return a.base * o / (rmax(d2, a.area) * 1.0e-6f);
-}
-RTG_D Rgb area_radiance(const AreaLightDev& a, float cos) {
-    Rgb r = rgb(a.radiance[0], a.radiance[1], a.radiance[2]);
-    return a.exponent == 0.0f ? r : r * fpow(cos, a.exponent);
-}
-RTG_D bool area_intersect(const AreaLightDev& a, V3 o, V3 d, float tmin, float tmax, float& t, float& cos) {
-    V3 n = ld3(a.fz);
-    float denom = dot(d, n);
-    if (denom >= 0.0f) return false;
-    t = dot(ld3(a.centre) - o, n) / denom;
-    if (!(t > tmin && t < tmax)) return false;
-    V3 q = (o + d * t) - ld3(a.centre);
-    float x = dot(q, ld3(a.fx)), y = dot(q, ld3(a.fy));
-    bool inside = a.rect ? (absf(x) <= a.half_x && absf(y) <= a.half_y) : (x * x + y * y <= a.radius * a.radius);
-    if (!inside) return false;
-    cos = -denom;
-    return true;
-}
-
 // The selection at a vertex (light.rs:495): its point, the sum of the weights there and whether
 // it is the static one. Weights are recomputed from the point with the same operations.
 struct Sel { V3 p; float total; bool by_flux; };
-RTG_D float entry_weight(const LightsDev& L, int e, V3 x) {
+RTG_D float entry_weight(const LightsDev& L, int e, V3 x) {  // light.rs:1014
     int a = L.entries[e];
-    return a >= 0 ? area_weight(L.areas[a], x) : L.env_base;
+    if (a < 0) return L.env_base;
+    const LightDev& l = L.lights[a];
+    if (l.kind == LIGHT_AREA) return area_weight(l, x);
+    if (l.kind == LIGHT_SUN) return l.base;
+    return sphere_weight(l, x);
 }
 RTG_D Sel select_at(const LightsDev& L, V3 x) {
     Sel s;
@@ -109,7 +72,8 @@ RTG_D float power_heuristic(float pa, float pb) {
     return 1.0f / (1.0f + r * r);
 }
 
-struct LightSample { V3 wi; float distance; Rgb radiance; float pdf; bool glossy, shadow; int area; };  // area: -1 environment
+// light: index into lights[], -1 the environment; delta: no other technique finds it
+struct LightSample { V3 wi; float distance; Rgb radiance; float pdf; bool glossy, shadow, delta; int light; };
 
 RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, float u0, float u1, LightSample& out) {  // light.rs:1150
     int n = L.n_entries;
@@ -136,9 +100,54 @@ RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, flo
     }
     if (!(pmf > 0.0f)) return false;
     int a = L.entries[index];
-    out.area = a;
-    if (a >= 0) {
-        const AreaLightDev& l = L.areas[a];
+    out.light = a;
+    out.delta = false;
+    if (a >= 0 && L.lights[a].kind == LIGHT_SUN) {  // light.rs:1197
+        const LightDev& l = L.lights[a];
+        out.distance = f_inf();
+        out.radiance = rgb(l.radiance[0], l.radiance[1], l.radiance[2]);
+        out.glossy = l.glossy != 0;
+        out.shadow = l.shadow != 0;
+        if (l.delta) {
+            out.wi = ld3(l.fz);
+            out.pdf = pmf;
+            out.delta = true;
+        } else {
+            Frame f;
+            f.x = ld3(l.fx); f.y = ld3(l.fy); f.z = ld3(l.fz);
+            out.wi = normalize(to_world(f, uniform_cone(u0, u1, l.one_minus_cos_max)));
+            out.pdf = pmf / l.solid_angle;
+        }
+    } else if (a >= 0 && L.lights[a].kind == LIGHT_SPHERE) {  // light.rs:1224
+        const LightDev& l = L.lights[a];
+        float m = sphere_mask(l, s.p);
+        V3 d = ld3(l.centre) - s.p;
+        float dist2 = len2(d);
+        if (!(m > 0.0f && dist2 > 0.0f)) return false;
+        float dist = sqrt_(dist2);
+        V3 towards = d / dist;
+        float omc = 0.0f;
+        if (l.radius > 0.0f && !sphere_cone(l, dist2, omc)) return false;
+        out.glossy = l.glossy != 0;
+        out.shadow = l.shadow != 0;
+        if (omc == 0.0f) {
+            out.wi = towards;
+            out.distance = dist;
+            out.radiance = rgb(l.intensity[0], l.intensity[1], l.intensity[2]) * (m / (dist2 * 1.0e-6f));
+            out.pdf = pmf;
+            out.delta = true;
+        } else {
+            V3 wi = normalize(to_world(frame_from_normal(towards), uniform_cone(u0, u1, omc)));
+            float b = dot(wi, d);
+            float r2 = l.radius * l.radius;
+            float near = b - sqrt_(rmax(r2 - len2(d - wi * b), 0.0f));
+            out.wi = wi;
+            out.distance = rmax(near, 0.0f);
+            out.radiance = rgb(l.radiance[0], l.radiance[1], l.radiance[2]) * m;
+            out.pdf = pmf / (TAU * omc);
+        }
+    } else if (a >= 0) {
+        const LightDev& l = L.lights[a];
         float x, y;
         if (l.rect) { x = (2.0f * u0 - 1.0f) * l.half_x; y = (2.0f * u1 - 1.0f) * l.half_y; }
         else { concentric_disk(u0, u1, x, y); x = x * l.radius; y = y * l.radius; }
@@ -169,11 +178,40 @@ RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, flo
     return out.pdf > 0.0f && finitef(out.pdf) && luminance(out.radiance) > 0.0f;
 }
 
-// Lights::crossed_from (light.rs:1350): area lights a ray crosses before t_max.
+// The light of one sphere a ray crosses before t_max (light.rs:1387), seen from the vertex the
+// ray left offset earlier; false when it adds nothing.
+RTG_D bool sphere_crossed(const LightsDev& L, const LightDev& l, V3 o, V3 d, float tmin, float tmax, bool has_pdf, float pdf,
+                          const Sel& from, float offset, Rgb& out) {
+    if (!(has_pdf ? l.glossy : l.camera)) return false;
+    float t;
+    if (!sphere_intersect(l, o, d, tmin, tmax, t)) return false;
+    V3 vertex = o - d * offset;
+    float m = sphere_mask(l, vertex);
+    if (!(m > 0.0f)) return false;
+    float w = 1.0f;
+    if (has_pdf) {
+        float omc;
+        if (sphere_cone(l, len2(ld3(l.centre) - vertex), omc) && omc > 0.0f)
+            w = power_heuristic(pdf, pmf_of(L, l.entry, from) / (TAU * omc));
+        else
+            w = 0.0f;
+    }
+    out = rgb(l.radiance[0], l.radiance[1], l.radiance[2]) * (m * w);
+    return true;
+}
+// The light of one sun an escaping ray sees (light.rs:1507); false when it adds nothing.
+RTG_D bool sun_seen(const LightsDev& L, const LightDev& l, V3 dir, bool has_pdf, float pdf, const Sel& from, Rgb& out) {
+    if (!((has_pdf ? l.glossy : l.camera) && sun_contains(l, dir))) return false;
+    float w = has_pdf ? power_heuristic(pdf, pmf_of(L, l.entry, from) / l.solid_angle) : 1.0f;
+    out = rgb(l.radiance[0], l.radiance[1], l.radiance[2]) * w;
+    return true;
+}
+
+// Lights::crossed_from (light.rs:1329): the area lights, then the spheres, a ray crosses before t_max.
 RTG_D_NI Rgb crossed_from(const LightsDev& L, V3 o, V3 d, float tmin, float tmax, bool has_pdf, float pdf, const Sel& from, float offset) {
     Rgb sum = splat(0.0f);
     for (int i = 0; i < L.n_areas; ++i) {
-        const AreaLightDev& l = L.areas[i];
+        const LightDev& l = L.lights[i];
         if (!(has_pdf ? l.glossy : l.camera)) continue;
         float t, cos;
         if (!area_intersect(l, o, d, tmin, tmax, t, cos)) continue;
@@ -185,13 +223,26 @@ RTG_D_NI Rgb crossed_from(const LightsDev& L, V3 o, V3 d, float tmin, float tmax
         }
         sum = sum + area_radiance(l, cos) * w;
     }
+    const int first_sphere = L.n_areas + (int)L.n_suns;
+    for (int i = first_sphere; i < first_sphere + (int)L.n_spheres; ++i) {
+        Rgb c;
+        if (sphere_crossed(L, L.lights[i], o, d, tmin, tmax, has_pdf, pdf, from, offset, c)) sum = sum + c;
+    }
     return sum;
 }
-// Lights::escaped (light.rs:1502) for the ramp environment.
+// sum plus the sun discs an escaping ray sees, in their order.
+RTG_D_NI Rgb add_suns(const LightsDev& L, Rgb sum, V3 dir, bool has_pdf, float pdf, const Sel& from) {
+    for (int i = L.n_areas; i < L.n_areas + (int)L.n_suns; ++i) {
+        Rgb c;
+        if (sun_seen(L, L.lights[i], dir, has_pdf, pdf, from, c)) sum = sum + c;
+    }
+    return sum;
+}
+// Lights::escaped (light.rs:1502): the ramp environment, then the sun discs.
 RTG_D Rgb escaped(const LightsDev& L, V3 dir, bool has_pdf, float pdf, const Sel& from) {
-    Rgb e = splat(env_value(L, dir.z));
-    if (!has_pdf || !L.env_is_entry) return e;
-    return e * power_heuristic(pdf, pmf_of(L, L.env_entry, from) * env_pdf(L, dir));
+    Rgb sum = splat(env_value(L, dir.z));
+    if (has_pdf && L.env_is_entry) sum = sum * power_heuristic(pdf, pmf_of(L, L.env_entry, from) * env_pdf(L, dir));
+    return L.n_suns ? add_suns(L, sum, dir, has_pdf, pdf, from) : sum;
 }
 
 // ---- camera (render.rs:79, scene/mod.rs:280) -------------------------------------------------------

@@ -48,7 +48,7 @@ class Material:
 
 @dataclass
 class Light:
-    kind: int = 0  # 0 rect, 1 disk
+    kind: int = 0  # 0 rect, 1 disk, 2 sun, 3 point (a sphere of diameter size_x), 4 spot
     position: Tuple[float, float, float] = (0.0, 0.0, 0.0)
     direction: Tuple[float, float, float] = (0.0, 0.0, -1.0)
     up: Tuple[float, float, float] = (0.0, 1.0, 0.0)
@@ -233,6 +233,38 @@ def example_scene() -> Scene:
                       size_y=400.0, power=5.0, flags=3)],
         env_kind=0, env_floor=0.05, env_horizon=0.12, env_zenith=0.3, env_strength=1.0, background_color=(0.05, 0.05, 0.05),
         width=512, height=384, max_samples=16, seed=1, tonemap=1, max_depth=8)
+
+
+LIGHT_SUN, LIGHT_POINT, LIGHT_SPOT = 2, 3, 4
+
+
+def sun_triangle_scene() -> Scene:
+    """render.rs:752-786: one Lambertian triangle (albedo 0.8, ior 1) facing a camera at y = -100
+    that looks along +Y, lit by a delta sun of irradiance pi shining along +Y, in a black world
+    with a black background colour; 16 x 16 pixels. Its centre pixel is albedo * E / pi = 0.8."""
+    tri = Mesh(np.array([(-10.0, 0.0, -10.0), (10.0, 0.0, -10.0), (0.0, 0.0, 10.0)], np.float32),
+               np.array([(0.0, -1.0, 0.0)] * 3, np.float32), np.array([0, 1, 2], np.uint32), 0)
+    return Scene(camera_position=(0.0, -100.0, 0.0), camera_target=(0.0, 0.0, 0.0), focal_mm=50.0, sensor_mm=36.0,
+                 materials=[Material(base_color=(0.8, 0.8, 0.8), ior=1.0)], meshes=[tri], instances=[Instance(0)],
+                 lights=[Light(kind=LIGHT_SUN, position=(0.0, 0.0, 1000.0), direction=(0.0, 1.0, 0.0), size_x=500.0,
+                               size_y=500.0, power=math.pi, angle_deg=0.0, flags=3)],
+                 env_strength=0.0, background_color=(0.0, 0.0, 0.0), background_mode=1, width=16, height=16)
+
+
+def light_kinds_scene(width: int = 256, height: int = 192) -> Scene:
+    """The example scene lit by every light kind of the path at once: its rect softbox, a sun with
+    a disc of 3 degrees, a point light, a sphere light of 60 mm and a spot with a soft edge, the
+    last two seen by the camera and in reflections, over a dim dome (2 + 5 selection entries)."""
+    s = example_scene()
+    s.width, s.height = width, height
+    s.lights.append(Light(kind=LIGHT_SUN, direction=(-0.3, 0.5, -0.81), power=2.0, angle_deg=3.0, flags=3))
+    s.lights.append(Light(kind=LIGHT_POINT, position=(-300.0, -250.0, 320.0), size_x=0.0, size_y=0.0, power=6.0,
+                          color=(1.0, 0.8, 0.6), flags=1))
+    s.lights.append(Light(kind=LIGHT_POINT, position=(200.0, 150.0, 260.0), size_x=60.0, size_y=60.0, power=4.0,
+                          color=(0.6, 0.8, 1.0), flags=3))
+    s.lights.append(Light(kind=LIGHT_SPOT, position=(-150.0, -500.0, 700.0), direction=(0.2, 0.6, -0.77),
+                          size_x=20.0, size_y=20.0, power=40.0, spread_deg=40.0, angle_deg=8.0, flags=3))
+    return s
 
 
 # ---- benchmark workloads -----------------------------------------------------------------------------------

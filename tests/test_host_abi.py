@@ -84,7 +84,7 @@ def test_malformed_scenes_are_refused_with_a_message(rtg, example_rsb):
 
 @pytest.mark.parametrize("change, words", [
     (lambda s: setattr(s, "env_kind", 2), "sky or HDRI"),
-    (lambda s: setattr(s.lights[0], "kind", 2), "light kind"),
+    (lambda s: setattr(s.lights[0], "kind", 5), "IES light"),
     (lambda s: setattr(s.materials[0], "bevel_mm", 1.0), "bevel"),
     (lambda s: setattr(s.materials[0], "opacity", 0.5), "cut-out"),
 ])
