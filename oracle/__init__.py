@@ -53,6 +53,8 @@ def lib():
             "orc_light_sample": (u32, [u32, v, ctypes.c_float, ctypes.c_float, ctypes.c_float, v]),
             "orc_light_sky": (None, [u32, v, v]),
             "orc_light_crossed": (None, [u32, v, ctypes.c_float, v]),
+            "orc_bitmap": (u32, [u32, u32, u32, ctypes.c_char_p, u32, v, v, u32, v, v]),
+            "orc_dist2d": (u32, [u32, u32, v, u32, v, v]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -165,6 +167,30 @@ class OracleScene:
         out = np.zeros(len(rays), np.uint8)
         lib().orc_occluded(self.handle, _p(rays), len(rays), _p(out))
         return out
+
+
+def bitmap(fmt, w, h, data, lookups=()):
+    """Bitmap::decode of a BMAP payload: (texels (h, w, 3), bilinear lookups (n, 3)) or raises
+    ValueError with the reason."""
+    wh = np.zeros(2, np.uint32)
+    uvw = np.asarray(lookups, np.float32).reshape(-1, 3)
+    out = np.zeros((len(uvw), 3), np.float32)
+    st = lib().orc_bitmap(fmt, w, h, bytes(data), len(data), _p(wh), None, len(uvw), _p(uvw), _p(out))
+    if st:
+        raise ValueError(error())
+    tex = np.zeros((int(wh[1]), int(wh[0]), 3), np.float32)
+    lib().orc_bitmap(fmt, w, h, bytes(data), len(data), _p(wh), _p(tex), 0, None, None)
+    return tex, out
+
+
+def dist2d(w, h, weights, samples):
+    """Distribution2D over w x h weights: (u, v, pdf, pdf at (u, v)) per sample, or None."""
+    wts = np.ascontiguousarray(weights, np.float32)
+    s = np.ascontiguousarray(samples, np.float32).reshape(-1, 2)
+    out = np.zeros((len(s), 4), np.float32)
+    if lib().orc_dist2d(w, h, _p(wts), len(s), _p(s), _p(out)):
+        return None
+    return out
 
 
 def energy_tables():

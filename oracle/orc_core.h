@@ -318,6 +318,10 @@ constexpr uint8_t LAYOUT[64] = {
 constexpr uint32_t DIM_CAMERA = 0, DIM_LENS = 2, DIM_FIRST_BOUNCE = 4, DIMS_PER_BOUNCE = 6;
 constexpr uint32_t OFFSET_LIGHT_SELECT = 0, OFFSET_LIGHT = 1, OFFSET_BSDF = 3, OFFSET_ROULETTE = 5;
 inline uint32_t bounce_dim(uint32_t b) { return DIM_FIRST_BOUNCE + b * DIMS_PER_BOUNCE; }
+// sampler.rs:127-135: the hashed dimension deciding whether the ray of vertex `bounce` passes its
+// `crossing`-th cut-out.
+constexpr uint32_t DIM_CUTOUT = 1u << 20;
+inline uint32_t cutout_dim(uint32_t bounce, uint32_t crossing) { return DIM_CUTOUT + bounce * 64 + (crossing < 63 ? crossing : 63); }
 
 // Joe & Kuo (2008) new-joe-kuo-6.21201, dimensions 2..64: degree s, coefficient a, m_1..m_s.
 struct JoeKuo { uint32_t s, a, m[9]; };

@@ -11,10 +11,20 @@
 
 namespace orc {
 
+struct PathStats;
+
 struct Prepared {  // integrator/mod.rs:237
     Lights lights;
-    uint32_t background = 0;  // 0 environment, 1 colour, 2 transparent
+    uint32_t background = 0;  // 0 environment, 1 colour, 2 transparent, 3 backplate
     Rgb background_color;
+    // The background image fitted to the frame (integrator/mod.rs:187).
+    const Image* plate = nullptr;
+    uint32_t plate_fit = 0;  // 0 fill, 1 fit, 2 stretch
+    float plate_rect[4] = {0.0f, 0.0f, 1.0f, 1.0f};
+    float frame_aspect = 1.0f, image_aspect = 1.0f;
+    // Per instance: shadow rays may pass it (a cut-out or a thin wall).
+    std::vector<uint8_t> passable;
+    bool any_passable = false;
     uint32_t floor_mode = 0;
     float floor_z = 0;
     Bsdf floor_bsdf;
@@ -58,6 +68,44 @@ struct Prepared {  // integrator/mod.rs:237
         }
         return Frame::from_normal(n);
     }
+    // Backplate::lookup (integrator/mod.rs:201): the image at screen position (su, sv), false
+    // outside a fitted image.
+    bool lookup(float su, float sv, Rgb& out) const {
+        float u = (su - plate_rect[0]) / (plate_rect[2] - plate_rect[0]);
+        float v = (sv - plate_rect[1]) / (plate_rect[3] - plate_rect[1]);
+        if (plate_fit != 2) {
+            bool fit = plate_fit == 1;
+            float k = frame_aspect / image_aspect;
+            if (image_aspect > frame_aspect) {
+                if (fit) v = 0.5f + (v - 0.5f) * (1.0f / k);
+                else u = 0.5f + (u - 0.5f) * k;
+            } else if (fit) {
+                u = 0.5f + (u - 0.5f) * k;
+            } else {
+                v = 0.5f + (v - 0.5f) * (image_aspect / frame_aspect);
+            }
+        }
+        if (plate_fit == 1 && !(u >= 0.0f && u <= 1.0f && v >= 0.0f && v <= 1.0f)) return false;
+        out = plate->bilinear(rclamp(u, 0.0f, 1.0f), rclamp(v, 0.0f, 1.0f), false);
+        return true;
+    }
+    Rgb backdrop(float su, float sv) const {  // integrator/mod.rs:867
+        Rgb c;
+        if (plate && background == 3 && lookup(su, sv, c)) return c;
+        return background_color;
+    }
+    // What a straight ray through the surface keeps, and where it goes on from: a cut-out lets
+    // 1 - opacity through, a thin wall its straight transmittance (integrator/mod.rs:581).
+    Rgb straight_through(const Scene& s, const Ray& r, uint32_t inst, const Hit& d, Vec3& origin) const {
+        const Material& m = material(s, inst);
+        float cos = dot(d.geometric_normal, r.dir);
+        float opacity = rclamp(m.opacity, 0.0f, 1.0f);
+        origin = offset_origin(d.point, -d.geometric_normal);
+        return Bsdf::surface(m, true).straight_transmittance(cos) * opacity + Rgb::splat(1.0f - opacity);
+    }
+    // Prepared::shadow (integrator/mod.rs:681) with Prepared::walk (integrator/mod.rs:629): false
+    // when the geometry or the visible floor blocks the ray, else what passes.
+    bool shadow(const Scene& s, const Ray& ray, Rgb& pass, PathStats& st) const;
     void add(Rgb& sum, Rgb c, bool indirect) const {  // integrator/mod.rs:855
         if (!(finite(c.r) && finite(c.g) && finite(c.b))) return;
         float p = rmax(rmax(c.r, c.g), c.b);
@@ -69,7 +117,16 @@ struct Prepared {  // integrator/mod.rs:237
 Prepared Prepared::make(const Scene& s) {
     Prepared p;
     const Environment& env = s.environment;
-    p.background = env.background_mode == 1 || env.background_mode == 3 ? 1 : (env.background_mode == 2 ? 2 : 0);
+    if (env.backplate_map != NO_BITMAP && env.backplate_map < s.bitmaps.size()) {
+        p.plate = &s.bitmaps[env.backplate_map];
+        uint32_t w = s.render.width ? s.render.width : 1, h = s.render.height ? s.render.height : 1;
+        const float* r = env.backplate_rect;
+        if (r[2] > r[0] && r[3] > r[1]) for (int k = 0; k < 4; ++k) p.plate_rect[k] = r[k];
+        p.plate_fit = env.backplate_fit;
+        p.frame_aspect = ((p.plate_rect[2] - p.plate_rect[0]) * (float)w) / ((p.plate_rect[3] - p.plate_rect[1]) * (float)h);
+        p.image_aspect = (float)p.plate->width / (float)p.plate->height;
+    }
+    p.background = env.background_mode == 1 ? 1 : env.background_mode == 2 ? 2 : env.background_mode == 3 ? (p.plate ? 3 : 1) : 0;
     p.background_color = Rgb(rmax(env.background_color.r, 0.0f), rmax(env.background_color.g, 0.0f), rmax(env.background_color.b, 0.0f));
     p.floor_mode = s.floor.mode;
     p.floor_z = s.floor.z;
@@ -90,6 +147,14 @@ Prepared Prepared::make(const Scene& s) {
         p.media.push_back(sigma);
     }
     const Geometry& g = s.geometry;
+    for (size_t i = 0; i < g.instances.size(); ++i) {  // integrator/mod.rs:371
+        const Material& m = p.material(s, (uint32_t)i);
+        bool thin = (m.flags & MATERIAL_FLAG_THIN) != 0;
+        bool pass = g.instances[i].material_id < s.materials.size() && !m.is_emissive() &&
+                    (m.opacity < 1.0f || (thin && m.transmission > 0.0f && (m.metallic < 1.0f || m.kind == MATERIAL_GLASS)));
+        p.passable.push_back(pass ? 1 : 0);
+        p.any_passable = p.any_passable || pass;
+    }
     for (size_t i = 0; i < g.instances.size(); ++i) {
         Axes a;
         const Instance& inst = g.instances[i];
@@ -117,9 +182,46 @@ struct PathStats {
     const Geometry* merged = nullptr;
 };
 
+bool Prepared::shadow(const Scene& s, const Ray& ray, Rgb& pass, PathStats& st) const {
+    const Geometry& geo = s.geometry;
+    if (!any_passable) {
+        bool blocked = (floor_mode == 1 && floor_t(ray, false) < F_INF) || (st.any += 1, geo.occluded(ray, false, &st.shadow));
+        if (st.merged) st.merged->occluded(ray, false, &st.merged_shadow);
+        pass = WHITE;
+        return !blocked;
+    }
+    // walk: through the cut-outs and thin walls up to the first surface that stops the ray
+    float floor = floor_mode == 1 ? floor_t(ray, false) : F_INF;
+    Rgb keep = WHITE;
+    Ray r = ray;
+    float travelled = 0.0f, blocker = F_INF;
+    bool done = false;
+    for (uint32_t k = 0; k < 32 && !done; ++k) {  // MAX_SHADOW_CROSSINGS
+        RayHit hit;
+        st.nearest += 1;
+        if (!geo.trace(r, false, hit, &st.trace)) { blocker = floor; done = true; break; }
+        float t = travelled + hit.t;
+        if (t >= floor) { blocker = floor; done = true; break; }
+        if (!(hit.instance < passable.size() && passable[hit.instance])) { blocker = t; done = true; break; }
+        Hit d;
+        if (!geo.hit_details(r, hit, d)) { blocker = t; done = true; break; }
+        Vec3 origin;
+        keep = keep * straight_through(s, r, hit.instance, d, origin);
+        if (rmax(rmax(keep.r, keep.g), keep.b) <= 0.0f) { keep = BLACK; blocker = t; done = true; break; }
+        travelled += dot(origin - r.origin, r.dir);
+        Ray next(origin, r.dir);
+        next.t_max = ray.t_max - travelled;
+        if (next.t_max != next.t_max || next.t_max <= next.t_min) { blocker = F_INF; done = true; break; }
+        r = next;
+    }
+    if (!done) { keep = BLACK; blocker = travelled; }
+    pass = keep;
+    return blocker == F_INF && peak(keep) > 0.0f;
+}
+
 // radiance_weighted (integrator/mod.rs:1140) for the scene features this subset reads.
-static void radiance(const Scene& scene, const Prepared& prep, const PixelSampler& sampler, Ray camera_ray, Rgb& out,
-                     float& alpha_out, PathStats& st) {
+static void radiance(const Scene& scene, const Prepared& prep, const PixelSampler& sampler, Ray camera_ray, float su, float sv,
+                     Rgb& out, float& alpha_out, PathStats& st) {
     const Lights& lights = prep.lights;
     Ray ray = camera_ray;
     Rgb throughput = WHITE, sum = BLACK;
@@ -131,6 +233,7 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
     bool primary = true;
     float offset = 0.0f;
     bool in_medium = false;
+    uint32_t cutouts = 0;
     Rgb sigma;
     const Geometry& geo = scene.geometry;
     for (;;) {
@@ -157,8 +260,8 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
                 Rgb seen = lights.escaped(ray.dir, nullptr, nullptr);
                 float k = scene.camera.exterior;
                 sum = sum + throughput * (k == 1.0f ? seen : seen * k);
-            } else if (primary && prep.background == 1) {
-                sum = sum + throughput * prep.background_color;
+            } else if (primary && (prep.background == 1 || prep.background == 3)) {
+                sum = sum + throughput * prep.backdrop(su, sv);
             } else if (primary && prep.background == 2) {
                 alpha = peak(crossed) > 0.0f ? 1.0f : 0.0f;
             } else {
@@ -201,6 +304,17 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
             }
             break;
         }
+        // A cut-out lets the ray through with probability 1 - opacity (integrator/mod.rs:1571).
+        if (material && material->opacity < 1.0f && cutouts < 64) {  // MAX_CUTOUTS
+            float u = sampler.get1(cutout_dim(bounce, cutouts));
+            cutouts += 1;
+            if (u >= rmax(material->opacity, 0.0f)) {
+                Vec3 o = offset_origin(s_hit_point, -s_geometric);
+                offset += dot(o - ray.origin, ray.dir);
+                ray = Ray(o, ray.dir);
+                continue;
+            }
+        }
         if (bounce >= prep.max_depth) break;
         Bsdf bsdf = material ? Bsdf::surface(*material, s_outside) : prep.floor_bsdf;
         Frame frame = prep.frame(s_inst, inst, s_point, s_normal);
@@ -223,17 +337,17 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
                 Vec3 from = wi.z < 0.0f ? offset_origin(s_hit_point, -ng) : origin;
                 float distance = ls.distance;
                 bool arrives = true;
+                Rgb pass = WHITE;
                 if (ls.shadow) {
                     st.rays += 1;
                     Ray sr(from, ls.wi);
                     if (finite(distance)) sr.t_max = distance * (1.0f - 1.0e-4f);
-                    bool blocked = (prep.floor_mode == 1 && prep.floor_t(sr, false) < F_INF) || (st.any += 1, geo.occluded(sr, false, &st.shadow));
-                    if (st.merged) st.merged->occluded(sr, false, &st.merged_shadow);
-                    arrives = !blocked;
+                    arrives = prep.shadow(scene, sr, pass, st);
                 }
                 if (arrives) {
                     float weight = (ls.delta || !ls.glossy) ? 1.0f : power_heuristic(ls.pdf, bsdf.pdf(wo, wi));
                     Rgb c = throughput * f * ls.radiance * (std::fabs(wi.z) * weight / ls.pdf);
+                    if (!(pass == WHITE)) c = c * pass;
                     prep.add(sum, c, bounce >= 1);
                 }
             }
@@ -309,7 +423,7 @@ static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, ui
         concentric_disk(a, b, lx, ly);
     }
     Ray ray = scene.camera.generate_ray(aspect, u, v, lx, ly);
-    radiance(scene, prep, sampler, ray, c, alpha, st);
+    radiance(scene, prep, sampler, ray, rclamp(u, 0.0f, 1.0f), rclamp(v, 0.0f, 1.0f), c, alpha, st);
 }
 
 struct Film {
@@ -627,6 +741,48 @@ void orc_light_crossed(uint32_t h, const float* ray8, float bsdf_pdf, float* out
     Selection at = L.select(ray.origin);
     Rgb c = L.crossed_from(ray, ray8[7], bsdf_pdf < 0.0f ? nullptr : &bsdf_pdf, &at, 0.0f);
     out3[0] = c.r; out3[1] = c.g; out3[2] = c.b;
+}
+
+// Known-answer helpers for the bitmaps (bitmap.rs, hdr.rs tests): decodes a BMAP payload; wh2 gets
+// its decoded size; texels (3 w h floats, may be null) its pixels; then n bilinear lookups at
+// uvw = (u, v, wrap) into out (3 floats each). 0 on success, 1 when it cannot be decoded (the
+// reason in orc_error), 2 for a format outside this path.
+uint32_t orc_bitmap(uint32_t format, uint32_t w, uint32_t h, const uint8_t* data, uint32_t len, uint32_t* wh2, float* texels,
+                    uint32_t n, const float* uvw, float* out) {
+    Image img;
+    std::string reason;
+    bool unsupported = false;
+    if (!decode_bitmap(format, w, h, data, len, img, reason, unsupported)) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_error = reason;
+        return unsupported ? 2u : 1u;
+    }
+    wh2[0] = img.width;
+    wh2[1] = img.height;
+    if (texels)
+        for (uint32_t y = 0; y < img.height; ++y)
+            for (uint32_t x = 0; x < img.width; ++x) {
+                Rgb c = img.texel(x, y);
+                float* o = texels + 3 * ((size_t)y * img.width + x);
+                o[0] = c.r; o[1] = c.g; o[2] = c.b;
+            }
+    for (uint32_t i = 0; i < n; ++i) {
+        Rgb c = img.bilinear(uvw[3 * i], uvw[3 * i + 1], uvw[3 * i + 2] != 0.0f);
+        out[3 * i] = c.r; out[3 * i + 1] = c.g; out[3 * i + 2] = c.b;
+    }
+    return 0;
+}
+// Distribution2D (bitmap.rs:330) over w x h weights: n samples at s (2 floats each) into out
+// (u, v, pdf, pdf(u, v) per sample). 1 when the weights are all zero.
+uint32_t orc_dist2d(uint32_t w, uint32_t h, const float* weights, uint32_t n, const float* s, float* out) {
+    Distribution2D d;
+    if (!Distribution2D::make(w, h, std::vector<float>(weights, weights + (size_t)w * h), d)) return 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        float u, v, p;
+        d.sample(s[2 * i], s[2 * i + 1], u, v, p);
+        out[4 * i] = u; out[4 * i + 1] = v; out[4 * i + 2] = p; out[4 * i + 3] = d.pdf(u, v);
+    }
+    return 0;
 }
 
 // Known-answer helpers: Pcg32, mix64, Sobol points, owen-scrambled sampler values, fmath.

@@ -191,10 +191,25 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             if (!(r.f32(e.floor) && r.f32(e.horizon) && r.f32(e.zenith) && r.f32(e.strength) && r.f32(e.rotation_deg) &&
                   r.rgb(e.background_color) && r.u32(e.background_mode)))
                 return false;
-            uint32_t hdri, plate;
-            if (!(r.opt_u32(hdri, 0xffffffffu) && r.opt_u32(plate, 0xffffffffu))) return false;
-            if (hdri != 0xffffffffu || plate != 0xffffffffu) return r.invalid("bitmap index does not refer to a BMAP section");
-            if (e.kind > 1) { error = "unsupported: sky or HDRI environment"; return false; }
+            if (!(r.opt_u32(e.hdri_map, NO_BITMAP) && r.opt_u32(e.backplate_map, NO_BITMAP) && r.opt_u32(e.backplate_fit, 0) &&
+                  r.opt_f32(e.sky_turbidity, 3.0f) && r.opt_f32(e.sun_azimuth_deg, 0.0f) && r.opt_f32(e.sun_elevation_deg, 45.0f) &&
+                  r.opt_f32(e.backplate_rect[0], 0.0f) && r.opt_f32(e.backplate_rect[1], 0.0f) && r.opt_f32(e.backplate_rect[2], 1.0f) &&
+                  r.opt_f32(e.backplate_rect[3], 1.0f) && r.opt_u32(e.sky_model, 0)))
+                return false;
+            if (e.kind == 2) { error = "unsupported: sky environment"; return false; }
+        } else if (is("BMAP")) {  // rsb.rs:1057
+            uint32_t format, w, h, n;
+            if (!(r.u32(format) && r.u32(w) && r.u32(h) && r.u32(n))) return false;
+            if ((size_t)n > r.remaining()) return r.too_short();
+            Image img;
+            std::string reason;
+            bool unsupported = false;
+            if (!decode_bitmap(format, w, h, r.data + r.pos, n, img, reason, unsupported)) {
+                if (unsupported) { error = reason; return false; }
+                return r.invalid(reason.c_str());
+            }
+            r.pos += n;
+            scene.bitmaps.push_back(std::move(img));
         } else if (is("FLOR")) {
             if (dup(have_floor)) return false;
             Floor& f = scene.floor;
@@ -221,12 +236,17 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             if (s.edge_supersample > 1) { error = "unsupported: edge supersampling"; return false; }
             if (s.pixel_filter == 3) { error = "unsupported: Blackman-Harris pixel filter"; return false; }
         } else {
-            static const char* feature_tags[] = {"LENS", "BMAP", "PATN", "IMGS", "PROG", "FXAM", "SECT", "GLAS",
+            static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "SECT", "GLAS",
                                                  "WETP", "WETF", "WTP2", "WETG", "NEST", "IESP"};
             for (const char* t : feature_tags)
                 if (is(t)) { error = std::string("unsupported: RSB section ") + t; return false; }
         }
     }
+    for (uint32_t map : {scene.environment.hdri_map, scene.environment.backplate_map})
+        if (map != NO_BITMAP && map >= scene.bitmaps.size()) {
+            error = "RSB section ENVR is invalid: bitmap index does not refer to a BMAP section";
+            return false;
+        }
     size_t nm = scene.materials.size();
     for (const Mesh& m : meshes)
         if (m.material_id >= nm) { error = "RSB section MESH is invalid: material_id does not refer to a MATL section"; return false; }
@@ -243,13 +263,7 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
     }
     // Material features outside this path (their branches of the reference integrator).
     for (const Material& m : scene.materials) {
-        bool thin = (m.flags & MATERIAL_FLAG_THIN) != 0;
         if (m.is_emissive() && (m.flags & MATERIAL_FLAG_LIGHT)) { error = "unsupported: emissive mesh lights"; return false; }
-        if (!m.is_emissive() && m.opacity < 1.0f) { error = "unsupported: cut-out (opacity) materials"; return false; }
-        if (!m.is_emissive() && thin && m.transmission > 0.0f && (m.metallic < 1.0f || m.kind == MATERIAL_GLASS)) {
-            error = "unsupported: thin-wall transmissive materials";
-            return false;
-        }
         if (m.scatter_mm > 0.0f && m.transmission > 0.0f) { error = "unsupported: scattering media"; return false; }
         if (m.abbe > 0.0f && m.transmission > 0.0f) { error = "unsupported: dispersive glass"; return false; }
         if (m.bevel_mm > 0.0f) { error = "unsupported: edge bevel"; return false; }
@@ -535,10 +549,7 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
         a.base = a.radiance.luminance() * a.area * 1.0e-6f;
         L.areas.push_back(a);
     }
-    const Environment& env = scene.environment;
-    float strength = rmax(env.strength, 0.0f);
-    L.env = env.kind == 1 ? Ramp::make(env.horizon, env.horizon, env.horizon, strength)
-                          : Ramp::make(env.floor, env.horizon, env.zenith, strength);
+    L.env = EnvLight::make(scene.environment, scene.bitmaps);
     L.env_base = PI * L.env.mean_radiance();
     if (!L.env.is_black()) {
         weights.push_back(4.0f * PI * PI * L.env.mean_radiance());
@@ -660,7 +671,7 @@ bool Lights::sample_selected(const Selection& from, float u_select, float u0, fl
         Vec3 wi;
         float p;
         if (!env.sample(u0, u1, wi, p)) return false;
-        out = {wi, F_INF, Rgb::splat(env.value(wi.z)), pmf_v * p, false, true, false, true};
+        out = {wi, F_INF, env.radiance(wi), pmf_v * p, false, true, false, true};
     }
     return out.pdf > 0.0f && finite(out.pdf) && out.radiance.luminance() > 0.0f;
 }
@@ -700,7 +711,7 @@ Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, con
     return sum;
 }
 Rgb Lights::escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from) const {  // light.rs:1502
-    Rgb sum = Rgb::splat(env.value(dir.z));
+    Rgb sum = env.radiance(dir);
     if (bsdf_pdf && env_is_entry) sum = sum * power_heuristic(*bsdf_pdf, pmf(env_entry, *from) * env.pdf(dir));
     for (const SunLight& sun : suns) {
         bool visible = bsdf_pdf ? sun.glossy : sun.camera;

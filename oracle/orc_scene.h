@@ -31,11 +31,40 @@ struct Light {
     float power = 0, spread_deg = 180, angle_deg = 0;
     uint32_t flags = 0;
 };
+constexpr uint32_t NO_BITMAP = 0xffffffffu;
 struct Environment {  // scene/mod.rs:739
-    uint32_t kind = 0;
+    uint32_t kind = 0;  // 0 studio, 1 flat, 2 sky, 3 HDRI
     float floor = 0.1f, horizon = 0.3f, zenith = 0.6f, strength = 1.0f, rotation_deg = 0.0f;
     Rgb background_color = Rgb::splat(0.05f);
-    uint32_t background_mode = 0;
+    uint32_t background_mode = 0;  // 0 environment, 1 colour, 2 transparent, 3 backplate
+    uint32_t hdri_map = NO_BITMAP, backplate_map = NO_BITMAP, backplate_fit = 0;  // fit: 0 fill, 1 fit, 2 stretch
+    float sky_turbidity = 3.0f, sun_azimuth_deg = 0.0f, sun_elevation_deg = 45.0f;
+    float backplate_rect[4] = {0.0f, 0.0f, 1.0f, 1.0f};
+    uint32_t sky_model = 0;
+};
+
+// ---- bitmap.rs, hdr.rs: decoded images ------------------------------------------------------------
+struct Image {  // bitmap.rs:90
+    uint32_t width = 0, height = 0;
+    bool srgb8 = false;           // sRGB bytes (3 per pixel), else linear floats (3 per pixel)
+    std::vector<uint8_t> bytes;
+    std::vector<float> linear;
+    Rgb texel(uint32_t x, uint32_t y) const;
+    Rgb bilinear(float u, float v, bool wrap_u) const;
+};
+// Bitmap::decode (bitmap.rs:236): formats 0 (sRGB RGB8), 1 (sRGB RGBA8), 2 (linear f32 RGB) and
+// 16 (a Radiance file). False with the reason on a bad size or file; OpenEXR (17) is refused.
+bool decode_bitmap(uint32_t format, uint32_t width, uint32_t height, const uint8_t* data, size_t len, Image& out,
+                   std::string& reason, bool& unsupported);
+const float* srgb_table();
+
+struct Distribution2D {  // bitmap.rs:330
+    size_t width = 0, height = 0;
+    std::vector<float> weights, conditional, marginal;
+    float mean = 0;
+    static bool make(size_t w, size_t h, std::vector<float> weights, Distribution2D& out);
+    void sample(float s0, float s1, float& u, float& v, float& pdf) const;
+    float pdf(float u, float v) const;
 };
 struct Floor { uint32_t mode = 0; float z = 0; Rgb color = Rgb::splat(0.5f); };
 struct RenderSettings {  // scene/mod.rs:911
@@ -51,6 +80,7 @@ struct RenderSettings {  // scene/mod.rs:911
 };
 struct Scene {
     Camera camera;
+    std::vector<Image> bitmaps;
     std::vector<Material> materials;
     Geometry geometry;
     std::vector<Light> lights;
@@ -72,6 +102,32 @@ struct Ramp {
     bool sample(float u0, float u1, Vec3& dir, float& pdf_out) const;
     float mean_radiance() const { return 0.5f * total_mass; }
     bool is_black() const { return total_mass <= 0.0f; }
+};
+
+// environment.rs:49-130: an equirectangular map (an HDRI), importance-sampled by its luminance
+struct EnvMap {
+    const Image* image = nullptr;
+    float scale = 0, rot_s = 0, rot_c = 1;
+    Distribution2D dist;
+    float mean_luminance = 0;
+    static bool make(const Image* image, float scale, float rotation_deg, EnvMap& out);
+    Vec3 to_image(Vec3 d) const { return Vec3(rot_c * d.x + rot_s * d.y, -rot_s * d.x + rot_c * d.y, d.z); }
+    Vec3 to_world(Vec3 d) const { return Vec3(rot_c * d.x - rot_s * d.y, rot_s * d.x + rot_c * d.y, d.z); }
+    Rgb radiance(Vec3 dir) const;
+    float pdf(Vec3 dir) const;
+    bool sample(float u0, float u1, Vec3& dir, float& pdf_out) const;
+};
+// environment.rs:333 EnvLight: the ramp or a map
+struct EnvLight {
+    bool is_map = false;
+    Ramp ramp;
+    EnvMap map;
+    static EnvLight make(const Environment& env, const std::vector<Image>& bitmaps);
+    Rgb radiance(Vec3 dir) const { return is_map ? map.radiance(dir) : Rgb::splat(ramp.value(dir.z)); }
+    float pdf(Vec3 dir) const { return is_map ? map.pdf(dir) : ramp.pdf(dir); }
+    bool sample(float u0, float u1, Vec3& dir, float& p) const { return is_map ? map.sample(u0, u1, dir, p) : ramp.sample(u0, u1, dir, p); }
+    float mean_radiance() const { return is_map ? map.mean_luminance : ramp.mean_radiance(); }
+    bool is_black() const { return is_map ? (map.mean_luminance != map.mean_luminance || map.mean_luminance <= 0.0f) : ramp.is_black(); }
 };
 
 // ---- light.rs ----------------------------------------------------------------------------------
@@ -124,7 +180,7 @@ struct Lights {
     std::vector<AreaLight> areas;
     std::vector<SunLight> suns;
     std::vector<SphereLight> spheres;
-    Ramp env;
+    EnvLight env;
     bool env_is_entry = false;
     uint32_t env_entry = 0;
     float env_base = 0;

@@ -62,6 +62,16 @@ class Light:
 
 
 @dataclass
+class Bitmap:
+    """A BMAP section: format 0 (sRGB RGB8), 1 (sRGB RGBA8), 2 (linear f32 RGB) or 16 (a
+    Radiance file, width and height 0), and its data bytes."""
+    format: int
+    width: int
+    height: int
+    data: bytes
+
+
+@dataclass
 class Mesh:
     positions: np.ndarray  # (n, 3) float32
     normals: np.ndarray  # (n, 3) float32 (zeros: none)
@@ -92,14 +102,23 @@ class Scene:
     meshes: List[Mesh] = field(default_factory=list)
     instances: List[Instance] = field(default_factory=list)
     lights: List[Light] = field(default_factory=list)
-    env_kind: int = 0
+    bitmaps: List[Bitmap] = field(default_factory=list)
+    env_kind: int = 0  # 0 studio, 1 flat, 2 sky, 3 HDRI
     env_floor: float = 0.1
     env_horizon: float = 0.3
     env_zenith: float = 0.6
     env_strength: float = 1.0
     env_rotation: float = 0.0
     background_color: Tuple[float, float, float] = (0.05, 0.05, 0.05)
-    background_mode: int = 0
+    background_mode: int = 0  # 0 environment, 1 colour, 2 transparent, 3 backplate
+    hdri_map: int = 0xFFFFFFFF
+    backplate_map: int = 0xFFFFFFFF
+    backplate_fit: int = 0  # 0 fill, 1 fit, 2 stretch
+    sky_turbidity: float = 3.0
+    sun_azimuth_deg: float = 0.0
+    sun_elevation_deg: float = 45.0
+    backplate_rect: Tuple[float, float, float, float] = (0.0, 0.0, 1.0, 1.0)
+    sky_model: int = 0
     floor_mode: int = 0
     floor_z: float = 0.0
     floor_color: Tuple[float, float, float] = (0.5, 0.5, 0.5)
@@ -131,7 +150,7 @@ def to_rsb(s: Scene, meshes: bool = True) -> bytes:
     """Serialises a scene as RSB version 1, sections in the reference writer's order (CAMR, MATL,
     MESH, INST, LGHT, ENVR, FLOR, RNDR) and payload sizes (rsb.rs:1645-1990). Without ``meshes``
     the MESH sections are left out: the file of a scene update that keeps the loaded geometry
-    (rt_scene_update)."""
+    (rt_scene_update). BMAP sections follow the lights, as the reference writes them."""
     out = [b"RSB1", _u(0)]
     out.append(_sec(b"CAMR", _f(*s.camera_position, *s.camera_target, *s.camera_up, s.focal_mm, s.sensor_mm, s.fstop,
                                 s.focus_dist) + _u(s.ortho) + _f(s.ortho_width)))
@@ -150,9 +169,12 @@ def to_rsb(s: Scene, meshes: bool = True) -> bytes:
     for l in s.lights:
         out.append(_sec(b"LGHT", _u(l.kind) + _f(*l.position, *l.direction, *l.up, l.size_x, l.size_y, *l.color, l.power,
                                                  l.spread_deg, l.angle_deg) + _u(l.flags)))
+    for b in s.bitmaps:
+        out.append(_sec(b"BMAP", _u(b.format, b.width, b.height, len(b.data)) + bytes(b.data) + bytes((4 - len(b.data) % 4) % 4)))
     out.append(_sec(b"ENVR", _u(s.env_kind) + _f(s.env_floor, s.env_horizon, s.env_zenith, s.env_strength, s.env_rotation,
                                                  *s.background_color) + _u(s.background_mode) +
-                    _u(0xFFFFFFFF, 0xFFFFFFFF, 0) + _f(3.0, 0.0, 45.0, 0.0, 0.0, 1.0, 1.0) + _u(0)))
+                    _u(s.hdri_map, s.backplate_map, s.backplate_fit) +
+                    _f(s.sky_turbidity, s.sun_azimuth_deg, s.sun_elevation_deg, *s.backplate_rect) + _u(s.sky_model)))
     out.append(_sec(b"FLOR", _u(s.floor_mode) + _f(s.floor_z, *s.floor_color)))
     out.append(_sec(b"RNDR", _u(s.width, s.height, s.max_samples, s.seed) + _f(s.max_seconds, s.exposure_ev) +
                     _u(s.tonemap, s.max_depth) + _f(s.clamp_indirect) + _u(0, 0, 0) + _f(0.0, 1.0) +
@@ -236,6 +258,96 @@ def example_scene() -> Scene:
 
 
 LIGHT_SUN, LIGHT_POINT, LIGHT_SPOT = 2, 3, 4
+MATERIAL_GLASS, MATERIAL_FLAG_THIN = 1, 2
+
+
+def _rgb_to_rgbe(c) -> bytes:
+    """hdr.rs:60 rgb_to_rgbe in f32: the shared exponent of the largest channel, mantissas truncated."""
+    clean = [f32(v) if (np.isfinite(v) and v > 0) else f32(0.0) for v in c]
+    m = max(max(clean[0], clean[1]), clean[2])
+    if m < f32(1.0e-32):
+        return bytes(4)
+    e = int((int(np.array(m, np.float32).view(np.uint32)) >> 23) & 0xFF) - 126
+    e = min(e, 127)
+    scale = f32(2.0) ** f32(8 - e) if -126 <= 8 - e <= 127 else f32(math.ldexp(1.0, 8 - e))
+    q = [min(int(f32(v * scale)), 255) for v in clean]
+    return bytes([q[0], q[1], q[2], e + 128])
+
+
+def _rle_channel(data: bytes) -> bytes:
+    """hdr.rs:261 encode_channel: runs of four or more as (128 + n, value), literals of up to 128."""
+    out = bytearray()
+    n, i = len(data), 0
+    while i < n:
+        run = 1
+        while i + run < n and run < 127 and data[i + run] == data[i]:
+            run += 1
+        if run >= 4:
+            out += bytes([128 + run, data[i]])
+            i += run
+            continue
+        start = i
+        while i < n and i - start < 128:
+            ahead = 1
+            while i + ahead < n and ahead < 4 and data[i + ahead] == data[i]:
+                ahead += 1
+            if ahead >= 4:
+                break
+            i += 1
+        out.append(i - start)
+        out += data[start:i]
+    return bytes(out)
+
+
+def hdr_encode(width: int, height: int, rgb) -> bytes:
+    """hdr.rs:295 encode: a Radiance file (-Y h +X w, the new run-length encoding where the width
+    allows it) of 3 w h linear floats, rows top to bottom."""
+    rgb = np.asarray(rgb, np.float32).reshape(height, width, 3)
+    out = bytearray(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {height} +X {width}\n".encode())
+    rle = 8 <= width <= 0x7FFF
+    for y in range(height):
+        px = [_rgb_to_rgbe(rgb[y, x]) for x in range(width)]
+        if not rle:
+            out += b"".join(px)
+            continue
+        out += bytes([2, 2, width >> 8, width & 0xFF])
+        for c in range(4):
+            out += _rle_channel(bytes(p[c] for p in px))
+    return bytes(out)
+
+
+def e5_scene() -> Scene:
+    """example.rs:232 e5_scene(false): the example at 160 x 120 and depth 12 with clear blue glass
+    (absorption 80 mm), a lacquered floor, brushed metal (anisotropy 0.8), a thin glass card and a
+    cut-out card (opacity 0.4), lit by its rect light and a 64 x 32 HDRI panorama (a grey gradient
+    with two bright panels, rotated 30 degrees) over a 16 x 8 background image."""
+    s = example_scene()
+    s.width, s.height, s.max_depth = 160, 120, 12
+    s.materials = [
+        Material(kind=MATERIAL_GLASS, base_color=(0.3, 0.5, 0.95), roughness=0.05, ior=1.5, transmission=1.0, absorption_mm=80.0),
+        Material(base_color=(0.3, 0.3, 0.32), roughness=0.6, coat=1.0, coat_roughness=0.05),
+        Material(base_color=(0.9, 0.85, 0.8), metallic=1.0, roughness=0.35, anisotropy=0.8),
+        Material(kind=MATERIAL_GLASS, base_color=(0.9, 0.6, 0.6), roughness=0.0, transmission=1.0, flags=MATERIAL_FLAG_THIN),
+        Material(base_color=(0.9, 0.9, 0.2), opacity=0.4),
+    ]
+    for x, material in ((150.0, 3), (-80.0, 4)):
+        p = np.array([(x - 60.0, -260.0, 0.0), (x + 60.0, -260.0, 0.0), (x + 60.0, -260.0, 160.0), (x - 60.0, -260.0, 160.0)], np.float32)
+        s.meshes.append(Mesh(p, np.zeros((4, 3), np.float32), np.array([0, 1, 2, 0, 2, 3], np.uint32), 0))
+        s.instances.append(Instance(len(s.meshes) - 1, material_id=material))
+    w, h = 64, 32
+    rgb = np.zeros((h, w, 3), np.float32)
+    for y in range(h):
+        up = f32(1.0) - f32(y) / f32(h)
+        for x in range(w):
+            panel = f32(8.0) if (20 <= x < 28 and 8 <= y < 14) else (f32(12.0) if (44 <= x < 47 and 6 <= y < 18) else f32(0.0))
+            rgb[y, x] = (f32(f32(0.05) + f32(0.2) * up) + panel, f32(f32(0.06) + f32(0.2) * up) + panel,
+                         f32(f32(0.08) + f32(0.25) * up) + panel)
+    plate = bytes(v for i in range(16 * 8) for v in ((i * 13) % 256, 120, 255 - (i * 7) % 256))
+    s.bitmaps = [Bitmap(16, 0, 0, hdr_encode(w, h, rgb)), Bitmap(0, 16, 8, plate)]
+    s.env_kind, s.hdri_map, s.backplate_map, s.background_mode = 3, 0, 1, 3
+    s.env_floor, s.env_horizon, s.env_zenith, s.env_strength, s.env_rotation = 0.1, 0.3, 0.6, 1.0, 30.0
+    s.background_color = (0.05, 0.05, 0.05)
+    return s
 
 
 def sun_triangle_scene() -> Scene:

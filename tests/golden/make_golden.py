@@ -6,7 +6,9 @@ its path tracer, read from the reference's own source tree (run where it is chec
 * the first Sobol points (engine/crates/rt-core/src/sampler.rs:403-430);
 * SHA-256 of the six energy tables (engine/crates/rt-core/src/bsdf/energy_table.rs), as the
   little-endian bytes of their u16 values and f32 bit patterns;
-* SHA-256 of the example scene file (tests/fixtures/example.rsb).
+* SHA-256 of the example scene file (tests/fixtures/example.rsb);
+* the FNV-1a film hash of the E5 scene with its HDRI (render.rs:1106) and SHA-256 of its file
+  (tests/fixtures/e5.rsb).
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -38,6 +40,7 @@ def main():
         "example_4spp": pinned(render, "PINNED_EXAMPLE_4SPP"),
         "tile_centre_240_176_s3": pinned(render, "PINNED_CENTRE"),
         "tile_small_sphere_48_144_s3": pinned(render, "PINNED_SMALL_SPHERE"),
+        "e5_hdri_4spp": pinned(render, "PINNED_E5_HDRI_4SPP"),
     }
     block = rng[rng.index("fn matches_the_reference_implementation"):]
     block = block[:block.index("]")]
@@ -56,6 +59,7 @@ def main():
             raw = struct.pack("<%df" % len(vals), *[float(v) for v in vals])
         tables[name] = {"count": len(vals), "sha256": hashlib.sha256(raw).hexdigest()}
     example = (REF / "tests" / "fixtures" / "example.rsb").read_bytes()
+    e5 = (REF / "tests" / "fixtures" / "e5.rsb").read_bytes()
     out = {
         "source": "Repackshot reference tree (engine crate rt-core), read by tests/golden/make_golden.py",
         "film_hashes": pins,
@@ -64,6 +68,7 @@ def main():
         "sobol_first_points_gray_order": points,
         "energy_tables": tables,
         "example_rsb": {"bytes": len(example), "sha256": hashlib.sha256(example).hexdigest()},
+        "e5_rsb": {"bytes": len(e5), "sha256": hashlib.sha256(e5).hexdigest()},
     }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(OUT)
