@@ -41,10 +41,11 @@ uint32_t rtg_version(void);
 
 /* rt_scene_load (ffi.rs:56-66, lib.rs:145): parses an RSB scene (copied; the caller keeps its
  * bytes), builds its BVHs and uploads it. Returns a handle > 0, or 0 after recording the error
- * (rtg_scene_error_len / _copy). Lights of kinds 0-4 (rect, disk, sun, point, spot) render;
- * features outside the path tracer's core (textures, lens optics, particles, sky and HDRI maps,
- * IES lights, cut-outs, thin walls, media, bevels, the shadow catcher) are refused with a
- * message that starts with "unsupported:". */
+ * (rtg_scene_error_len / _copy). Lights of kinds 0-4 (rect, disk, sun, point, spot), HDRI
+ * environments and background images (BMAP sections: 8-bit sRGB, linear f32, Radiance files),
+ * cut-outs and thin walls render; features outside the path tracer's core (textures, lens optics,
+ * particles, the sky model, OpenEXR bitmaps, IES lights, scattering media, bevels, the shadow
+ * catcher) are refused with a message that starts with "unsupported:". */
 uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len);
 
 /* rt_scene_update (ffi.rs:68-88, rt-wasm/src/lib.rs:171-193, Scene::update_from_rsb
@@ -52,7 +53,8 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len);
  * without MESH sections keeps the scene's meshes: its INST sections, or the implicit instances of
  * the kept meshes, refer to them; when the instances' meshes, transforms and visibility flags are
  * also unchanged, the device trees are kept and only the camera, image size, materials, lights and
- * settings are uploaded again. Films keep their rectangles. RTG_STATUS_OK, RTG_STATUS_BAD_HANDLE,
+ * settings are uploaded again. A file without BMAP sections keeps the scene's bitmaps, as the
+ * reference's update does. Films keep their rectangles. RTG_STATUS_OK, RTG_STATUS_BAD_HANDLE,
  * RTG_STATUS_NULL_POINTER, or RTG_STATUS_BAD_SCENE with the message in rtg_scene_error_*; on any
  * error the scene is unchanged. */
 uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len);
@@ -166,7 +168,8 @@ uint32_t rtg_queue_free(uint32_t queue);
  * The film must lie inside the image; every path of the call is held in one wave (168 bytes each).
  * `residual` (may be null) receives the sum over replayed paths of |radiance left after the
  * replay| and of |radiance|: the first is 0 up to rounding when the replay retraced the forward
- * paths. */
+ * paths. A scene with cut-outs or thin walls is refused (RTG_STATUS_BAD_SCENE): the replay does not
+ * walk shadow rays through them. */
 #define RTG_ADJOINT_CORRELATED 1u
 uint32_t rtg_adjoint_params(uint32_t scene, uint32_t* n_materials, uint32_t* n_lights);
 uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, uint32_t first_sample, uint32_t count, uint32_t flags,

@@ -1,0 +1,293 @@
+// Bitmaps of a scene on the host: decoding of the BMAP formats into linear RGB texels
+// (engine/crates/rt-core/src/bitmap.rs:100-300, hdr.rs:30-240) and the importance-sampling grid
+// of an environment map (environment.rs:60-95, bitmap.rs:312-372). The device reads the texels and
+// the grid's CDFs (rtg_shade.cuh).
+#include <cctype>
+#include <cmath>
+#include <cstring>
+
+#include "rtg_scene.h"
+
+namespace rtg {
+namespace {
+
+// The sRGB decoding of every byte value with the reference's powf (bitmap.rs:108).
+const float* srgb_to_linear() {
+    static float t[256];
+    static bool done = false;
+    if (!done) {
+        for (int i = 0; i < 256; ++i) {
+            float c = (float)i / 255.0f;
+            t[i] = c <= 0.04045f ? c / 12.92f : fpow((c + 0.055f) / 1.055f, 2.4f);
+        }
+        done = true;
+    }
+    return t;
+}
+
+// Cleans linear floats (non-finite and negative to 0) and halves the image (2 x 2 box, an odd
+// last row or column averaged with itself) until it is at most 4096 wide (bitmap.rs:182-216).
+void to_linear(uint32_t width, uint32_t height, std::vector<float> rgb, HImage& out) {
+    for (float& v : rgb)
+        if (!(finitef(v) && v > 0.0f)) v = 0.0f;
+    size_t w = width, h = height;
+    while (w > 4096) {
+        size_t nw = (w + 1) / 2, nh = (h + 1) / 2;
+        std::vector<float> half(3 * nw * nh);
+        for (size_t y = 0; y < nh; ++y) {
+            size_t ya = 2 * y, yb = std::min(2 * y + 1, h - 1);
+            for (size_t x = 0; x < nw; ++x) {
+                size_t xa = 2 * x, xb = std::min(2 * x + 1, w - 1);
+                for (int c = 0; c < 3; ++c) {
+                    float a = rgb[3 * (ya * w + xa) + c] + rgb[3 * (ya * w + xb) + c];
+                    float b = rgb[3 * (yb * w + xa) + c] + rgb[3 * (yb * w + xb) + c];
+                    half[3 * (y * nw + x) + c] = (a + b) * 0.25f;
+                }
+            }
+        }
+        rgb.swap(half);
+        w = nw;
+        h = nh;
+    }
+    out.width = (uint32_t)w;
+    out.height = (uint32_t)h;
+    out.texels = std::move(rgb);
+}
+
+// Radiance RGBE files (hdr.rs): a header ending in an empty line, "-Y h +X w" or "+Y h +X w",
+// then scanlines, flat (with old-style repeat markers) or in the newer per-channel run-length code.
+struct HdrReader {
+    const uint8_t* b;
+    size_t n, pos = 0;
+    bool line(size_t& start, size_t& end) {
+        size_t k = pos;
+        while (k < n && b[k] != '\n') ++k;
+        if (k >= n) return false;
+        start = pos;
+        end = k;
+        pos = k + 1;
+        return true;
+    }
+    bool scanline(std::vector<uint8_t>& row, size_t width) {
+        if (width >= 8 && width <= 0x7fff && pos + 4 <= n && b[pos] == 2 && b[pos + 1] == 2 && (b[pos + 2] & 0x80) == 0) {
+            if ((((size_t)b[pos + 2] << 8) | b[pos + 3]) != width) return false;
+            pos += 4;
+            for (int ch = 0; ch < 4; ++ch)
+                for (size_t x = 0; x < width;) {
+                    if (pos >= n) return false;
+                    size_t count = b[pos++];
+                    if (count > 128) {
+                        count -= 128;
+                        if (pos >= n || x + count > width) return false;
+                        const uint8_t value = b[pos++];
+                        for (size_t j = 0; j < count; ++j) row[4 * (x + j) + ch] = value;
+                    } else {
+                        if (count == 0 || x + count > width || pos + count > n) return false;
+                        for (size_t j = 0; j < count; ++j) row[4 * (x + j) + ch] = b[pos + j];
+                        pos += count;
+                    }
+                    x += count;
+                }
+            return true;
+        }
+        unsigned shift = 0;
+        for (size_t x = 0; x < width;) {
+            if (pos + 4 > n) return false;
+            const uint8_t* p = b + pos;
+            pos += 4;
+            if (p[0] == 1 && p[1] == 1 && p[2] == 1) {
+                size_t count = (size_t)p[3] << shift;
+                if (x == 0 || x + count > width) return false;
+                for (size_t j = 0; j < count; ++j) std::memcpy(&row[4 * (x + j)], &row[4 * (x - 1)], 4);
+                x += count;
+                shift += 8;
+            } else {
+                std::memcpy(&row[4 * x], p, 4);
+                x += 1;
+                shift = 0;
+            }
+        }
+        return true;
+    }
+};
+
+bool decode_hdr(const uint8_t* bytes, size_t n, uint32_t& width, uint32_t& height, std::vector<float>& rgb) {
+    auto starts = [&](const char* s) { size_t k = std::strlen(s); return n >= k && std::memcmp(bytes, s, k) == 0; };
+    if (!(starts("#?RADIANCE") || starts("#?RGBE"))) return false;
+    HdrReader r{bytes, n};
+    size_t a, z;
+    if (!r.line(a, z)) return false;
+    for (;;) {
+        if (!r.line(a, z)) return false;
+        if (a == z) break;
+        if (z - a >= 7 && std::memcmp(bytes + a, "FORMAT=", 7) == 0) {
+            size_t s = a + 7, e = z;
+            auto blank = [](uint8_t c) { return c == ' ' || c == '\t' || c == '\r' || c == '\f' || c == '\n'; };
+            while (s < e && blank(bytes[s])) ++s;
+            while (e > s && blank(bytes[e - 1])) --e;
+            if (!(e - s == 15 && std::memcmp(bytes + s, "32-bit_rle_rgbe", 15) == 0)) return false;
+        }
+    }
+    if (!r.line(a, z)) return false;
+    std::vector<std::string> words;
+    for (size_t i = a; i < z;) {
+        while (i < z && std::isspace(bytes[i])) ++i;
+        size_t j = i;
+        while (j < z && !std::isspace(bytes[j])) ++j;
+        if (j > i) words.emplace_back((const char*)bytes + i, j - i);
+        i = j;
+    }
+    if (words.size() != 4 || words[2] != "+X" || (words[0] != "-Y" && words[0] != "+Y")) return false;
+    const bool top_down = words[0] == "-Y";
+    auto number = [](const std::string& t, uint32_t& v) {
+        if (t.empty() || t.size() > 10) return false;
+        uint64_t x = 0;
+        for (char c : t) {
+            if (c < '0' || c > '9') return false;
+            x = 10 * x + (uint64_t)(c - '0');
+        }
+        if (x > 0xffffffffull) return false;
+        v = (uint32_t)x;
+        return true;
+    };
+    if (!number(words[1], height) || !number(words[3], width) || width == 0 || height == 0) return false;
+    if ((uint64_t)width * height > (1ull << 28)) return false;
+    rgb.assign(3 * (size_t)width * height, 0.0f);
+    std::vector<uint8_t> row(4 * (size_t)width);
+    for (size_t y = 0; y < height; ++y) {
+        if (!r.scanline(row, width)) return false;
+        float* out = rgb.data() + 3 * (top_down ? y : height - 1 - y) * (size_t)width;
+        for (size_t x = 0; x < width; ++x) {
+            const uint8_t* p = &row[4 * x];
+            if (p[3] == 0) continue;  // zero
+            // 2^(e - 136): the mantissa bytes scaled by the shared exponent (hdr.rs:40-56)
+            const int e = (int)p[3] - 136;
+            const float f = e >= -126 ? bitsf((uint32_t)(e + 127) << 23) : (e >= -149 ? bitsf(1u << (e + 149)) : 0.0f);
+            out[3 * x] = (float)p[0] * f;
+            out[3 * x + 1] = (float)p[1] * f;
+            out[3 * x + 2] = (float)p[2] * f;
+        }
+    }
+    return true;
+}
+
+// The bucket boundaries of a row of weights, normalised (the last exactly 1 when the row has
+// weight), and the row's sum.
+float cumulative(const float* w, size_t n, float* cdf) {
+    float acc = 0.0f;
+    for (size_t i = 0; i < n; ++i) {
+        acc += w[i];
+        cdf[i] = acc;
+    }
+    if (acc > 0.0f) {
+        for (size_t i = 0; i < n; ++i) cdf[i] /= acc;
+        cdf[n - 1] = 1.0f;
+    }
+    return acc;
+}
+
+}  // namespace
+
+bool decode_bitmap(uint32_t format, uint32_t width, uint32_t height, const uint8_t* data, size_t len, HImage& out, std::string& reason,
+                   bool& unsupported) {
+    unsupported = false;
+    const uint64_t px = (uint64_t)width * height;
+    auto raw = [&](uint64_t bytes_per_pixel) {
+        if (width == 0 || height == 0 || width > 65536 || height > 65536 || px > (1ull << 28) || px * bytes_per_pixel != len) {
+            reason = "bitmap size does not match its data";
+            return false;
+        }
+        return true;
+    };
+    const float* srgb = srgb_to_linear();
+    switch (format) {
+        case 0:
+        case 1: {  // 8-bit sRGB RGB or RGBA (alpha ignored)
+            const size_t stride = format == 0 ? 3 : 4;
+            if (!raw(stride)) return false;
+            out.width = width;
+            out.height = height;
+            out.texels.resize(3 * px);
+            for (size_t i = 0; i < px; ++i)
+                for (int c = 0; c < 3; ++c) out.texels[3 * i + c] = srgb[data[stride * i + c]];
+            return true;
+        }
+        case 2: {  // little-endian linear f32 RGB
+            if (!raw(12)) return false;
+            std::vector<float> rgb(3 * px);
+            std::memcpy(rgb.data(), data, len);
+            to_linear(width, height, std::move(rgb), out);
+            return true;
+        }
+        case 16: {  // a Radiance file
+            uint32_t w = 0, h = 0;
+            std::vector<float> rgb;
+            if (!decode_hdr(data, len, w, h, rgb)) {
+                reason = "unreadable Radiance HDR image";
+                return false;
+            }
+            if (!(width == 0 && height == 0) && !(width == w && height == h)) {
+                reason = "bitmap size does not match its data";
+                return false;
+            }
+            to_linear(w, h, std::move(rgb), out);
+            return true;
+        }
+        case 17:
+            unsupported = true;
+            reason = "unsupported: OpenEXR bitmap";
+            return false;
+        default:
+            reason = "unknown bitmap format";
+            return false;
+    }
+}
+
+bool build_env_map(const HImage& img, float scale, float rotation_deg, HEnvMap& out) {
+    const size_t w = img.width, h = img.height;
+    const size_t fx = std::max<size_t>((w + 511) / 512, 1), fy = std::max<size_t>((h + 255) / 256, 1);
+    const size_t gw = (w + fx - 1) / fx, gh = (h + fy - 1) / fy;
+    out.gw = (uint32_t)gw;
+    out.gh = (uint32_t)gh;
+    out.weights.assign(gw * gh, 0.0f);
+    float mean = 0.0f;
+    for (size_t gy = 0; gy < gh; ++gy) {
+        float s = 0.0f, cth;
+        sin_cos(PI * ((float)gy + 0.5f) / (float)gh, s, cth);
+        float row_sum = 0.0f;
+        for (size_t gx = 0; gx < gw; ++gx) {
+            float lum = 0.0f;
+            uint32_t count = 0;
+            for (size_t y = gy * fy; y < std::min((gy + 1) * fy, h); ++y)
+                for (size_t x = gx * fx; x < std::min((gx + 1) * fx, w); ++x) {
+                    const float* t = &img.texels[3 * (y * w + x)];
+                    lum += rmax(luminance(rgb(t[0], t[1], t[2])), 0.0f);
+                    count += 1;
+                }
+            lum = lum / (float)std::max(count, 1u);
+            out.weights[gy * gw + gx] = lum * s;
+            row_sum += lum * s;
+        }
+        mean += row_sum / (float)gw;
+    }
+    out.mean_luminance = scale * (mean / (float)gh) * (0.5f * PI);
+    // Distribution2D::new (bitmap.rs:343): per-row conditional CDFs, the marginal over rows.
+    out.conditional.assign(gw * gh, 0.0f);
+    std::vector<float> row_sums(gh);
+    for (size_t y = 0; y < gh; ++y) row_sums[y] = cumulative(&out.weights[y * gw], gw, &out.conditional[y * gw]);
+    out.marginal.assign(gh, 0.0f);
+    float acc = 0.0f;
+    for (size_t y = 0; y < gh; ++y) {
+        acc += row_sums[y];
+        out.marginal[y] = acc;
+    }
+    if (!(acc > 0.0f && finitef(acc))) return false;
+    for (float& m : out.marginal) m /= acc;
+    out.marginal[gh - 1] = 1.0f;
+    out.mean = acc / (float)(gw * gh);
+    out.scale = scale;
+    sin_cos(rotation_deg * (PI / 180.0f), out.rot_s, out.rot_c);
+    return true;
+}
+
+}  // namespace rtg

@@ -32,7 +32,7 @@ struct DevMaterial {
     float emission[3];  // radiance of an emitter (emission * emission_power, clamped at 0)
     float sigma[3];     // Beer–Lambert coefficients per mm inside a clear solid
     uint32_t has_medium;
-    uint32_t pad;
+    float opacity;  // below 1: a cut-out
 };
 constexpr uint32_t MATERIAL_GLASS = 1, MATERIAL_EMISSIVE = 2, MATERIAL_FLAG_THIN = 2;
 

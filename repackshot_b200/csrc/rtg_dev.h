@@ -54,7 +54,7 @@ struct alignas(16) DevInstance {
     float to_world[12];
     uint32_t identity, active, material, mesh;
     uint32_t flags, inside_out, has_normals, tri_base;  // tri_base: first global triangle of its mesh
-    uint32_t tangent_on, pad0, pad1, pad2;
+    uint32_t tangent_on, passable, pad1, pad2;  // passable: shadow rays cross it (cut-out or thin wall)
     float tan_centre[3], tan_axis[3], tan_x[3];
     float pad3[3];
 };
@@ -79,11 +79,27 @@ struct LightDev {
 constexpr int MAX_ENTRIES = 64;
 constexpr int MAX_LIGHTS = 63;
 
+// An equirectangular environment map (environment.rs:49): linear RGB texels, rows top to bottom,
+// importance-sampled by a piecewise-constant 2-D distribution over a grid of its cells
+// (bitmap.rs:330): per-row conditional CDFs, the marginal CDF over rows, the cell weights.
+struct EnvMapDev {
+    const float* texels;  // 3 per pixel
+    uint32_t width, height;
+    float scale, rot_s, rot_c;
+    const float* weights;      // gw * gh
+    const float* conditional;  // gw * gh
+    const float* marginal;     // gh
+    uint32_t gw, gh;
+    float mean;
+};
+
 struct LightsDev {
     // lights[] holds the area lights, then the suns, then the sphere lights, each in scene order
     int n_areas, n_entries, per_point, env_is_entry;
     uint32_t env_entry, n_suns, n_spheres, n_lights;
     float env_floor, env_horizon, env_zenith, env_lower, env_total, env_base;
+    uint32_t env_is_map;  // the environment is `env_map`, else the ramp above
+    EnvMapDev env_map;
     int entries[MAX_ENTRIES];  // >= 0 index into lights[], -1 environment
     float cdf[MAX_ENTRIES];
     float flux_pmf[MAX_ENTRIES];
@@ -99,8 +115,15 @@ struct SceneDev {
     // render settings
     uint32_t width, height, seed, max_depth, pixel_filter;
     float clamp_indirect;
-    uint32_t background;  // 0 environment, 1 colour, 2 transparent
+    uint32_t background;  // 0 environment, 1 colour, 2 transparent, 3 background image
     float background_color[3];
+    // The background image fitted to the frame (integrator/mod.rs:187): linear RGB texels.
+    const float* plate;
+    uint32_t plate_w, plate_h, plate_fit;  // fit: 0 fill, 1 fit, 2 stretch
+    float plate_rect[4], frame_aspect, image_aspect;
+    // Some instance lets shadow rays through (a cut-out or a thin wall); some material is a cut-out
+    // (paths then pass surfaces without a vertex, and waves run extra rounds).
+    uint32_t any_passable, any_cutout;
     uint32_t floor_mode;
     float floor_z;
     float floor_color[3];

@@ -61,6 +61,7 @@ struct Scene {
     BufSet geometry;  // trees, leaf triangles, vertex arrays: kept by updates that keep the meshes
     BufSet shading;   // instances, materials, BSDFs, lights: replaced by every update
     std::vector<HMesh> meshes;  // the host meshes, for updates without MESH sections
+    std::vector<HImage> bitmaps;  // the decoded bitmaps, for updates and jobs without BMAP sections
     std::string geom_key;
     // for the adjoint: materials as uploaded, each scene light's power, each area light's scene light
     std::vector<DevMaterial> materials_h;
@@ -199,14 +200,23 @@ uint32_t upload_geometry(const Flat& F, BufSet& set, SceneDev& S) {
     return RTG_STATUS_OK;
 }
 
-// Uploads instances, materials, BSDFs and lights of `F` into `set`, pointers into `S`.
+// Uploads instances, materials, BSDFs, lights, the environment map and the background image of
+// `F` into `set`, pointers into `S` and the uploaded lights.
 uint32_t upload_shading(const Flat& F, BufSet& set, SceneDev& S) {
     uint32_t st;
     if ((st = upload(set, F.instances, S.instances)) || (st = upload(set, F.materials, S.materials)) ||
         (st = upload(set, F.bsdfs, S.bsdfs)))
         return st;
+    LightsDev L = F.lights;
+    if (L.env_is_map && F.env_image) {
+        if ((st = upload(set, F.env_image->texels, L.env_map.texels)) || (st = upload(set, F.env_map.weights, L.env_map.weights)) ||
+            (st = upload(set, F.env_map.conditional, L.env_map.conditional)) || (st = upload(set, F.env_map.marginal, L.env_map.marginal)))
+            return st;
+    }
+    S.plate = nullptr;
+    if (F.plate && (st = upload(set, F.plate->texels, S.plate))) return st;
     RTG_CHECK(cudaMalloc(&set.lights, sizeof(LightsDev)));
-    RTG_CHECK(cudaMemcpy(set.lights, &F.lights, sizeof(LightsDev), cudaMemcpyHostToDevice));
+    RTG_CHECK(cudaMemcpy(set.lights, &L, sizeof(LightsDev), cudaMemcpyHostToDevice));
     return RTG_STATUS_OK;
 }
 
@@ -229,7 +239,7 @@ SceneDev compose(const SceneDev& constants, const SceneDev& geom, const SceneDev
     S.nodes = geom.nodes; S.tris = geom.tris; S.blas = geom.blas;
     S.positions = geom.positions; S.normals = geom.normals; S.tri_index = geom.tri_index;
     S.tlas_root = geom.tlas_root; S.stack_need = geom.stack_need;
-    S.instances = shade.instances; S.materials = shade.materials; S.bsdfs = shade.bsdfs;
+    S.instances = shade.instances; S.materials = shade.materials; S.bsdfs = shade.bsdfs; S.plate = shade.plate;
     S.energy = g_energy;
     return S;
 }
@@ -314,7 +324,7 @@ uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film, const Scene
     }
     launch_wave(Sw, sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t);
     RTG_CHECK(cudaGetLastError());
-    sc.launches += 2 + 6 * (uint64_t)(Sw.max_depth + 1) - ((film || w.segs) ? 0 : 1);
+    sc.launches += 2 + 6 * (uint64_t)wave_rounds(Sw) - ((film || w.segs) ? 0 : 1);
     if (t) {
         RTG_CHECK(cudaStreamSynchronize(sc.stream));
         for (int i = 0; i + 1 < t->ev_count; i += 2) {
@@ -456,6 +466,7 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     sc->geom_key = geometry_key(hs);
     keep_shading(*sc, hs, F);
     sc->meshes = std::move(hs.meshes);
+    sc->bitmaps = std::move(hs.bitmaps);
     sc->build_seconds = F.build_seconds;
     sc->nodes = F.nodes.size();
     sc->tris = F.tris.size();
@@ -478,7 +489,7 @@ uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
     HScene hs;
     std::string err;
     bool kept = false;
-    if (!parse_rsb(bytes, len, hs, err, &sc->meshes, &kept)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
+    if (!parse_rsb(bytes, len, hs, err, &sc->meshes, &kept, &sc->bitmaps)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
     std::string key = geometry_key(hs);
     const bool same_geometry = kept && key == sc->geom_key;
     Flat F;
@@ -512,6 +523,7 @@ uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
     sc->d_lights = sc->shading.lights;
     keep_shading(*sc, hs, F);
     if (!kept) sc->meshes = std::move(hs.meshes);
+    sc->bitmaps = std::move(hs.bitmaps);
     sc->geom_key = std::move(key);
     sc->instanced_triangles = F.instanced_triangles;
     sc->width = F.scene.width;
@@ -590,7 +602,7 @@ uint32_t rtg_render_progressive_noalloc(uint32_t handle, uint32_t film, uint32_t
     const char* why = "";
     uint32_t st = noalloc_render(job, res, &why);
     if (st) { g_error = why; return st; }
-    sc->launches += res.waves * (2 + 6 * (uint64_t)(sc->S.max_depth + 1));
+    sc->launches += res.waves * (2 + 6 * (uint64_t)wave_rounds(sc->S));
     sc->rays += res.extend_rays + res.shadow_rays;
     sc->extend_rays += res.extend_rays;
     sc->shadow_rays += res.shadow_rays;
@@ -627,7 +639,7 @@ uint32_t rtg_queue_add(uint32_t queue, const uint8_t* bytes, uint32_t len, uint3
     HScene hs;
     std::string err;
     bool kept = false;
-    if (!parse_rsb(bytes, len, hs, err, &sc->meshes, &kept)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
+    if (!parse_rsb(bytes, len, hs, err, &sc->meshes, &kept, &sc->bitmaps)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
     std::string key = geometry_key(hs);
     if (!kept || key != sc->geom_key) {
         g_error = "a queue job keeps the scene's geometry: no MESH sections, the same instances";
@@ -724,6 +736,8 @@ uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays) {
         jobs_h[j].lights = J.shading.lights;
         jobs_h[j].film = f->dev;
         Sw.max_depth = std::max(Sw.max_depth, J.constants.max_depth);
+        Sw.any_cutout |= J.constants.any_cutout;
+        Sw.any_passable |= J.constants.any_passable;
         total += (uint64_t)J.width * J.height * J.count;
     }
     if (total == 0) {
@@ -819,6 +833,10 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     Film* f = film_of(film);
     if (!f || f->scene != scene) return RTG_STATUS_BAD_FILM;
     if (!target || !loss || !grads) { g_error = "rtg_render_adjoint: null pointer"; return RTG_STATUS_NULL_POINTER; }
+    if (sc->S.any_passable) {
+        g_error = "rtg_render_adjoint: unsupported: cut-outs and thin walls (their shadow rays are not replayed)";
+        return RTG_STATUS_BAD_SCENE;
+    }
     const FilmDev& F = f->dev;
     const uint32_t nm = (uint32_t)sc->materials_h.size(), na = (uint32_t)sc->light_source.size();
     const uint32_t nl = (uint32_t)sc->light_power.size();

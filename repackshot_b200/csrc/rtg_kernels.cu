@@ -18,6 +18,13 @@ constexpr int TRACE_THREADS = 128;
 
 // Flags of a path slot.
 constexpr uint32_t PF_HAS_PDF = 1, PF_PRIMARY = 2, PF_MEDIUM = 4;
+// The path's flags also hold the cut-outs it passed (bits 8-14, at most MAX_CUTOUTS) and its vertex
+// count (bits 16-26): a cut-out pass is no vertex, so a path's bounce can fall behind the round.
+constexpr uint32_t PF_CUT_SHIFT = 8, PF_CUT_MASK = 0x7fu << 8, PF_BOUNCE_SHIFT = 16, PF_BOUNCE_MASK = 0x7ffu << 16;
+constexpr uint32_t MAX_CUTOUTS = 64;
+// sampler.rs:127-135: the hashed dimension deciding whether vertex `bounce`'s ray passes its
+// `crossing`-th cut-out.
+RTG_D uint32_t cutout_dim(uint32_t bounce, uint32_t crossing) { return (1u << 20) + bounce * 64u + (crossing < 63u ? crossing : 63u); }
 
 __device__ __forceinline__ void wave_slot(const WaveDesc& w, uint32_t slot, uint32_t& x, uint32_t& y, uint32_t& index) {
     if (w.xys) {
@@ -200,10 +207,11 @@ __global__ void k_scatter(PathBuffers P, int cur) {
 // One vertex of the path in `slot` with the scene constants S and lights L; xyi(x, y, index) gives
 // the path's pixel and sample index (the sampler's key).
 template <class XYI>
-__device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L, const PathBuffers& P, uint32_t slot, int cur, uint32_t bounce,
-                                           XYI xyi, uint32_t& rays_local, uint32_t& shadow_local) {
+__device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L, const PathBuffers& P, uint32_t slot, int cur, XYI xyi,
+                                           uint32_t& rays_local, uint32_t& shadow_local) {
     float4 o4 = P.o[slot], d4 = P.d[slot], thr4 = P.thr[slot], sum = P.sum[slot];
     uint32_t flags = P.flags[slot];
+    const uint32_t bounce = (flags & PF_BOUNCE_MASK) >> PF_BOUNCE_SHIFT;
     uint4 hit = P.hit[slot];
     V3 ro = v3(o4.x, o4.y, o4.z), rd = v3(d4.x, d4.y, d4.z);
     float offset = o4.w, pdf = d4.w;
@@ -238,8 +246,12 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
                 Rgb seen = escaped(L, rd, false, 0.0f, from);
                 Rgb c = thr * (S.exterior == 1.0f ? seen : seen * S.exterior);
                 sum.x = sum.x + c.r; sum.y = sum.y + c.g; sum.z = sum.z + c.b;
-            } else if (primary && S.background == 1) {
-                Rgb c = thr * rgb(S.background_color[0], S.background_color[1], S.background_color[2]);
+            } else if (primary && (S.background == 1 || S.background == 3)) {
+                uint32_t x, y, index;
+                xyi(x, y, index);
+                float su, sv;
+                screen_of(S, c_sobol, x, y, index, su, sv);
+                Rgb c = thr * backdrop(S, su, sv);
                 sum.x = sum.x + c.r; sum.y = sum.y + c.g; sum.z = sum.z + c.b;
             } else if (primary && S.background == 2) {
                 alpha = peak(crossed) > 0.0f ? 1.0f : 0.0f;
@@ -279,6 +291,24 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
                     add_clamped(sum, thr * rgb(mat->emission[0], mat->emission[1], mat->emission[2]) * 1.0f, bounce >= 2, S.clamp_indirect);
                 break;
             }
+            // A cut-out lets the ray through with probability 1 - opacity: no vertex, the same
+            // direction, density and selection; the path goes back to the extension queue
+            // (integrator/mod.rs:1571).
+            const uint32_t cut = (flags & PF_CUT_MASK) >> PF_CUT_SHIFT;
+            if (S.any_cutout && mat->opacity < 1.0f && cut < MAX_CUTOUTS) {
+                uint32_t x, y, index;
+                xyi(x, y, index);
+                const float u = sample1(c_sobol, pixel_key(S.seed, x, y), index, cutout_dim(bounce, cut));
+                flags = (flags & ~PF_CUT_MASK) | ((cut + 1u) << PF_CUT_SHIFT);
+                if (u >= rmax(mat->opacity, 0.0f)) {
+                    const V3 o2 = offset_origin(h.point, -ng);
+                    offset += dot(o2 - ro, rd);
+                    P.o[slot] = make_float4(o2.x, o2.y, o2.z, offset);
+                    P.flags[slot] = flags;
+                    alive = true;
+                    break;
+                }
+            }
         }
         if (bounce >= S.max_depth) break;
         const Bsdf& b = S.bsdfs[mat ? 2 * I->material + (s_outside ? 0 : 1) : 2 * S.n_materials];
@@ -314,7 +344,9 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
                 float weight = (ls.delta || !ls.glossy) ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(S.energy, b, wo, wi));
                 Rgb c = thr * f * ls.radiance * (absf(wi.z) * weight / ls.pdf);
                 bool finite_c = finitef(c.r) && finitef(c.g) && finitef(c.b);
-                if (finite_c && bounce >= 1 && S.clamp_indirect > 0.0f) {
+                // The clamp applies to what arrives: after the shadow walk when it may attenuate.
+                const bool walk = ls.shadow && S.any_passable;
+                if (finite_c && bounce >= 1 && S.clamp_indirect > 0.0f && !walk) {
                     float p = rmax(rmax(c.r, c.g), c.b);
                     if (p > S.clamp_indirect) c = c * (S.clamp_indirect / p);
                 }
@@ -331,7 +363,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
                     if (finite_c && !floor_blocks) {
                         uint32_t k = atomicAdd(&P.counters[2], 1u);
                         P.sh_o[k] = make_float4(from_p.x, from_p.y, from_p.z, tmax);
-                        P.sh_d[k] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, 0.0f);
+                        P.sh_d[k] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, bounce >= 1 ? 1.0f : 0.0f);  // w: indirect
                         P.sh_c[k] = make_float4(c.r, c.g, c.b, __uint_as_float(slot));
                     }
                 }
@@ -376,7 +408,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
         }
         P.o[slot] = make_float4(next_origin.x, next_origin.y, next_origin.z, offset);
         P.d[slot] = make_float4(wi.x, wi.y, wi.z, pdf);
-        P.flags[slot] = flags;
+        P.flags[slot] = (flags & ~PF_BOUNCE_MASK) | ((bounce + 1u) << PF_BOUNCE_SHIFT);
         alive = true;
     } while (false);
     P.thr[slot] = make_float4(thr.r, thr.g, thr.b, alpha);
@@ -392,8 +424,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
 // use on its own: the kernel waits on scattered hit-detail loads, and more warps hide them (1080p
 // frame: 369 -> 383 Mpaths/s; 5, 6 and 7 blocks measured 367, 379 and 372).
 template <bool BATCH>
-__global__ void __launch_bounds__(128, 8) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, uint32_t bounce,
-                                               WaveDesc w) {
+__global__ void __launch_bounds__(128, 8) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w) {
     uint32_t n = *(volatile uint32_t*)&P.counters[cur];
     uint32_t rays_local = 0, shadow_local = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -402,10 +433,10 @@ __global__ void __launch_bounds__(128, 8) k_shade(SceneDev S, const LightsDev* _
             uint32_t job, x, y, index;
             batch_slot(w, slot, job, x, y, index);
             const JobDev& J = w.jobs[job];
-            shade_slot(J.S, *J.lights, P, slot, cur, bounce,
-                       [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { xx = x; yy = y; ii = index; }, rays_local, shadow_local);
+            shade_slot(J.S, *J.lights, P, slot, cur, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { xx = x; yy = y; ii = index; },
+                       rays_local, shadow_local);
         } else {
-            shade_slot(S, *Lg, P, slot, cur, bounce, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { wave_slot(w, slot, xx, yy, ii); },
+            shade_slot(S, *Lg, P, slot, cur, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { wave_slot(w, slot, xx, yy, ii); },
                        rays_local, shadow_local);
         }
     }
@@ -464,6 +495,66 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow(SceneDev S, PathBuffer
                 if (!blocked) shadow_unblocked(P, ray);
             }
         }
+    }
+    if (err) atomicOr(&P.counters[3], err);
+}
+
+// ---- shadow walk: shadow rays through cut-outs and thin walls (integrator/mod.rs:629-690) ------------
+// Nearest hits along the ray: a passable surface multiplies what arrives by its straight
+// transmittance (a thin wall's) times its opacity plus 1 - opacity, and the ray goes on from just
+// behind it, up to 32 crossings; any other surface blocks it. One thread per ray: only scenes with
+// passable instances run it, instead of k_shadow. BATCH: each ray's job gives its materials.
+template <bool BATCH>
+__global__ void __launch_bounds__(TRACE_THREADS) k_shadow_walk(SceneDev S, PathBuffers P, WaveDesc w) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const uint32_t n = *(volatile uint32_t*)&P.counters[2];
+    uint32_t err = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o4 = P.sh_o[i], d4 = P.sh_d[i], c4 = P.sh_c[i];
+        const uint32_t slot = __float_as_uint(c4.w);
+        const SceneDev* Sp = &S;
+        if constexpr (BATCH) {
+            uint32_t job, x, y, index;
+            batch_slot(w, slot, job, x, y, index);
+            Sp = &w.jobs[job].S;
+        }
+        const SceneDev& J = *Sp;
+        const V3 d = v3(d4.x, d4.y, d4.z);
+        const float t_max = o4.w;
+        V3 o = v3(o4.x, o4.y, o4.z);
+        float tmax = t_max, travelled = 0.0f;
+        Rgb keep = splat(1.0f);
+        bool arrives = false;
+        for (uint32_t k = 0; k < 32; ++k) {  // MAX_SHADOW_CROSSINGS
+            TraceResult res;
+            if (!traverse<false>(J, o, d, 1.0e-3f, tmax, false, res, &err, stack)) { arrives = true; break; }
+            if (res.inst >= J.n_instances || !J.instances[res.inst].passable) break;
+            HitInfo h;
+            uint4 idx;
+            const DevInstance* I;
+            if (!hit_details(J, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, h, I, idx)) break;
+            const uint32_t m = I->material;
+            const float opacity = rclamp(J.materials[m].opacity, 0.0f, 1.0f);
+            keep = keep * (straight_transmittance(J.bsdfs[2 * m], dot(h.geometric, d)) * opacity + splat(1.0f - opacity));
+            if (rmax(rmax(keep.r, keep.g), keep.b) <= 0.0f) break;
+            const V3 origin = offset_origin(h.point, -h.geometric);
+            travelled += dot(origin - o, d);
+            const float next = t_max - travelled;
+            if (next != next || next <= 1.0e-3f) { arrives = true; break; }
+            o = origin;
+            tmax = next;
+        }
+        if (!(arrives && peak(keep) > 0.0f)) continue;
+        Rgb c = rgb(c4.x, c4.y, c4.z) * keep;
+        if (d4.w != 0.0f && J.clamp_indirect > 0.0f) {
+            const float p = rmax(rmax(c.r, c.g), c.b);
+            if (p > J.clamp_indirect) c = c * (J.clamp_indirect / p);
+        }
+        float4 s4 = P.sum[slot];
+        s4.x = s4.x + c.r; s4.y = s4.y + c.g; s4.z = s4.z + c.b;
+        P.sum[slot] = s4;
     }
     if (err) atomicOr(&P.counters[3], err);
 }
@@ -594,7 +685,8 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
     if (batch) k_camera<true><<<g, 256, 0, st>>>(S, w, P);
     else k_camera<false><<<g, 256, 0, st>>>(S, w, P);
     int cur = 0;
-    for (uint32_t bounce = 0; bounce <= S.max_depth; ++bounce) {
+    const uint32_t rounds = wave_rounds(S);
+    for (uint32_t round = 0; round < rounds; ++round) {
         if (timing && timing->ev_count + 2 <= WaveTiming::MAX_EVENTS) {
             cudaEventRecord(timing->ev[timing->ev_count++], st);
             k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur);
@@ -604,9 +696,11 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
         }
         k_scan<<<1, 32, 0, st>>>(P);
         k_scatter<<<g, 256, 0, st>>>(P, cur);
-        if (batch) k_shade<true><<<g, 128, 0, st>>>(S, L, P, cur, bounce, w);
-        else k_shade<false><<<g, 128, 0, st>>>(S, L, P, cur, bounce, w);
-        k_shadow<<<g_sh, TRACE_THREADS, 0, st>>>(S, P);
+        if (batch) k_shade<true><<<g, 128, 0, st>>>(S, L, P, cur, w);
+        else k_shade<false><<<g, 128, 0, st>>>(S, L, P, cur, w);
+        if (!S.any_passable) k_shadow<<<g_sh, TRACE_THREADS, 0, st>>>(S, P);
+        else if (batch) k_shadow_walk<true><<<g, TRACE_THREADS, 0, st>>>(S, P, w);
+        else k_shadow_walk<false><<<g, TRACE_THREADS, 0, st>>>(S, P, w);
         k_next_round<<<1, 1, 0, st>>>(P, cur);
         cur ^= 1;
     }

@@ -8,6 +8,10 @@ namespace rtg {
 
 struct JobDev;
 
+// Rounds of a wave: one per vertex up to the depth, plus, when a material is a cut-out, one per
+// cut-out a path may pass (at most 64; a pass is no vertex).
+inline uint32_t wave_rounds(const SceneDev& S) { return S.max_depth + 1u + (S.any_cutout ? 64u : 0u); }
+
 // A segment of a batched wave: samples [first, first + ns) of the full-width rows [y0, y0 + h) of
 // one job's image. Its slots start at slot_begin (sample-major, then row-major pixels); its pixels
 // start at pix_begin in the wave's accumulation order.

@@ -169,6 +169,46 @@ RTG_HD float fpow(float x, float y) {  // fmath.rs:174
     if (x == 1.0f) return 1.0f;
     return fexp2(y * flog2(x));
 }
+// atan(u) for |u| <= tan(pi/8): the Taylor series to u^17 (fmath.rs:191).
+RTG_HD float atan_taylor(float u) {
+    float u2 = u * u;
+    float p = 1.0f / 17.0f;
+    p = -p * u2 + 1.0f / 15.0f;
+    p = -p * u2 + 1.0f / 13.0f;
+    p = -p * u2 + 1.0f / 11.0f;
+    p = -p * u2 + 1.0f / 9.0f;
+    p = -p * u2 + 1.0f / 7.0f;
+    p = -p * u2 + 1.0f / 5.0f;
+    p = -p * u2 + 1.0f / 3.0f;
+    return u - u * u2 * p;
+}
+// Arctangent in [-pi/2, pi/2]: reduced to [0, 1] by atan(a) = pi/2 - atan(1/a), then below
+// tan(pi/8) by atan(t) = pi/4 + atan((t - 1)/(t + 1)) (fmath.rs:206).
+RTG_HD float fatan(float x) {
+    if (x != x) return x;
+    float a = absf(x);
+    bool flip = a > 1.0f;
+    float t = flip ? 1.0f / a : a;
+    float r = t > 0.41421357f ? FRAC_PI_4 + atan_taylor((t - 1.0f) / (t + 1.0f)) : atan_taylor(t);
+    if (flip) r = FRAC_PI_2 - r;
+    return x < 0.0f ? -r : r;
+}
+// Four-quadrant arctangent of y / x in [-pi, pi]; atan2(0, 0) = 0 (fmath.rs:227).
+RTG_HD float fatan2(float y, float x) {
+    if (x != x || y != y) return bitsf(0x7fc00000u);
+    if (x == 0.0f) return y > 0.0f ? FRAC_PI_2 : (y < 0.0f ? -FRAC_PI_2 : 0.0f);
+    if (absf(y) <= absf(x)) {
+        float r = fatan(y / x);
+        if (!(x < 0.0f)) return r;
+        return y < 0.0f ? r - PI : r + PI;
+    }
+    return y > 0.0f ? FRAC_PI_2 - fatan(x / y) : -FRAC_PI_2 - fatan(x / y);
+}
+// Arccosine in [0, pi] of x clamped to [-1, 1] (fmath.rs:253).
+RTG_HD float facos(float x) {
+    x = rclamp(x, -1.0f, 1.0f);
+    return fatan2(sqrt_((1.0f - x) * (1.0f + x)), x);
+}
 
 // ---- math.rs / color.rs ------------------------------------------------------------------------
 struct V3 { float x, y, z; };

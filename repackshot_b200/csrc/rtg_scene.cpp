@@ -75,7 +75,8 @@ const char* make_mesh(HMesh& m, std::vector<V3>&& p, std::vector<V3>&& nn, std::
 }
 }  // namespace
 
-bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, const std::vector<HMesh>* kept, bool* used_kept) {
+bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, const std::vector<HMesh>* kept, bool* used_kept,
+               const std::vector<HImage>* kept_bitmaps) {
     s = HScene();
     if (used_kept) *used_kept = false;
     bool seen_mesh = false;
@@ -177,10 +178,27 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (!(r.f32(s.env_floor) && r.f32(s.env_horizon) && r.f32(s.env_zenith) && r.f32(s.env_strength) && r.f32(s.env_rotation) &&
                   r.f3(s.background_color) && r.u32(s.background_mode)))
                 return false;
-            uint32_t hdri, plate;
-            if (!(r.ou32(hdri, 0xffffffffu) && r.ou32(plate, 0xffffffffu))) return false;
-            if (hdri != 0xffffffffu || plate != 0xffffffffu) return r.invalid("bitmap index does not refer to a BMAP section");
-            if (s.env_kind > 1) { error = "unsupported: sky or HDRI environment"; return false; }
+            float turbidity, azimuth, elevation;
+            uint32_t sky_model;
+            if (!(r.ou32(s.hdri_map, 0xffffffffu) && r.ou32(s.backplate_map, 0xffffffffu) && r.ou32(s.backplate_fit, 0) &&
+                  r.of32(turbidity, 3.0f) && r.of32(azimuth, 0.0f) && r.of32(elevation, 45.0f) && r.of32(s.backplate_rect[0], 0.0f) &&
+                  r.of32(s.backplate_rect[1], 0.0f) && r.of32(s.backplate_rect[2], 1.0f) && r.of32(s.backplate_rect[3], 1.0f) &&
+                  r.ou32(sky_model, 0)))
+                return false;
+            if (s.env_kind == 2) { error = "unsupported: sky environment"; return false; }
+        } else if (is("BMAP")) {  // rsb.rs:1057
+            uint32_t format, w, h, n;
+            if (!(r.u32(format) && r.u32(w) && r.u32(h) && r.u32(n))) return false;
+            if ((size_t)n > r.remaining()) return r.too_short();
+            HImage img;
+            std::string reason;
+            bool unsupported = false;
+            if (!decode_bitmap(format, w, h, r.d + r.pos, n, img, reason, unsupported)) {
+                if (unsupported) { error = reason; return false; }
+                return r.invalid(reason.c_str());
+            }
+            r.pos += n;
+            s.bitmaps.push_back(std::move(img));
         } else if (is("FLOR")) {
             if (!once(seen_floor)) return false;
             if (!(r.u32(s.floor_mode) && r.f32(s.floor_z) && r.f3(s.floor_color))) return false;
@@ -206,7 +224,7 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (s.edge_supersample > 1) { error = "unsupported: edge supersampling"; return false; }
             if (s.pixel_filter == 3) { error = "unsupported: Blackman-Harris pixel filter"; return false; }
         } else {
-            static const char* feature_tags[] = {"LENS", "BMAP", "PATN", "IMGS", "PROG", "FXAM", "SECT",
+            static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "SECT",
                                                  "GLAS", "WETP", "WETF", "WTP2", "WETG", "NEST", "IESP"};
             for (const char* t : feature_tags)
                 if (is(t)) { error = std::string("unsupported: RSB section ") + t; return false; }
@@ -216,6 +234,12 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
         s.meshes = *kept;
         if (used_kept) *used_kept = true;
     }
+    if (s.bitmaps.empty() && kept_bitmaps) s.bitmaps = *kept_bitmaps;
+    for (uint32_t map : {s.hdri_map, s.backplate_map})
+        if (map != 0xffffffffu && map >= s.bitmaps.size()) {
+            error = "RSB section ENVR is invalid: bitmap index does not refer to a BMAP section";
+            return false;
+        }
     size_t nm = s.materials.size();
     for (const HMesh& m : s.meshes)
         if (m.material_id >= nm) { error = "RSB section MESH is invalid: material_id does not refer to a MATL section"; return false; }
@@ -233,11 +257,6 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
     for (const HMaterial& m : s.materials) {
         bool emissive = m.kind == MATERIAL_EMISSIVE;
         if (emissive && (m.flags & 1u)) { error = "unsupported: emissive mesh lights"; return false; }
-        if (!emissive && m.opacity < 1.0f) { error = "unsupported: cut-out (opacity) materials"; return false; }
-        if (!emissive && (m.flags & MATERIAL_FLAG_THIN) && m.transmission > 0.0f && (m.metallic < 1.0f || m.kind == MATERIAL_GLASS)) {
-            error = "unsupported: thin-wall transmissive materials";
-            return false;
-        }
         if (m.scatter_mm > 0.0f && m.transmission > 0.0f) { error = "unsupported: scattering media"; return false; }
         if (m.abbe > 0.0f && m.transmission > 0.0f) { error = "unsupported: dispersive glass"; return false; }
         if (m.bevel_mm > 0.0f) { error = "unsupported: edge bevel"; return false; }
@@ -523,7 +542,7 @@ struct Flattener {
 }  // namespace
 
 // ---- light preparation (light.rs:245-995) ----------------------------------------------------------
-static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, std::string& error) {
+static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, Flat& F, std::string& error) {
     std::memset(&L, 0, sizeof(L));
     V3 centre;
     float radius;
@@ -655,18 +674,40 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
     L.n_spheres = (uint32_t)kinds[2].size();
     L.n_lights = (uint32_t)refs.size();
     for (const auto& r : refs) L.entries[L.n_entries++] = (int)(first[r.first] + r.second);
-    // environment.rs:333 ramp (flat: three equal stops)
+    // EnvLight::new (environment.rs:335): an HDRI with its bitmap is a map (black when it has no
+    // light), any other kind the ramp (flat: three equal stops; an HDRI without a bitmap: the dome).
     float strength = rmax(s.env_strength, 0.0f);
-    float f0 = s.env_kind == 1 ? s.env_horizon : s.env_floor, z0 = s.env_kind == 1 ? s.env_horizon : s.env_zenith;
+    float f0 = s.env_kind == 1 ? s.env_horizon : s.env_floor, h0 = s.env_horizon, z0 = s.env_kind == 1 ? s.env_horizon : s.env_zenith;
+    F.env_image = nullptr;
+    if (s.env_kind == 3 && s.hdri_map < s.bitmaps.size()) {
+        if (build_env_map(s.bitmaps[s.hdri_map], strength, s.env_rotation, F.env_map)) {
+            L.env_is_map = 1;
+            F.env_image = &s.bitmaps[s.hdri_map];
+        } else {
+            f0 = h0 = z0 = 0.0f;
+        }
+    }
     L.env_floor = rmax(f0 * strength, 0.0f);
-    L.env_horizon = rmax(s.env_horizon * strength, 0.0f);
+    L.env_horizon = rmax(h0 * strength, 0.0f);
     L.env_zenith = rmax(z0 * strength, 0.0f);
     L.env_lower = 0.5f * (L.env_floor + L.env_horizon);
     float upper = 0.5f * (L.env_horizon + L.env_zenith);
     L.env_total = L.env_lower + upper;
-    float mean = 0.5f * L.env_total;
+    const float mean = L.env_is_map ? F.env_map.mean_luminance : 0.5f * L.env_total;
+    const bool black = L.env_is_map ? (mean != mean || mean <= 0.0f) : L.env_total <= 0.0f;
+    if (L.env_is_map) {
+        const HEnvMap& m = F.env_map;
+        L.env_map.width = F.env_image->width;
+        L.env_map.height = F.env_image->height;
+        L.env_map.scale = m.scale;
+        L.env_map.rot_s = m.rot_s;
+        L.env_map.rot_c = m.rot_c;
+        L.env_map.gw = m.gw;
+        L.env_map.gh = m.gh;
+        L.env_map.mean = m.mean;
+    }
     L.env_base = PI * mean;
-    if (!(L.env_total <= 0.0f)) {
+    if (!black) {
         if (L.n_entries >= MAX_ENTRIES) { error = "unsupported: more than 64 lights"; return false; }
         weights.push_back(4.0f * PI * PI * mean);
         L.env_is_entry = 1;
@@ -764,8 +805,12 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
         d.inside_out = M.inside_out;
         d.has_normals = !M.normals.empty();
         d.tri_base = tri_base[in.mesh];
-        // Tangent axes of anisotropic materials (integrator/mod.rs:396).
         const HMaterial& mat = s.materials[in.material_id];
+        // Shadow rays cross cut-outs and thin walls (integrator/mod.rs:371).
+        const bool thin = (mat.flags & MATERIAL_FLAG_THIN) != 0;
+        d.passable = mat.kind != MATERIAL_EMISSIVE &&
+                     (mat.opacity < 1.0f || (thin && mat.transmission > 0.0f && (mat.metallic < 1.0f || mat.kind == MATERIAL_GLASS)));
+        // Tangent axes of anisotropic materials (integrator/mod.rs:396).
         if (!(mat.anisotropy != mat.anisotropy || mat.anisotropy <= 0.0f || mat.kind == MATERIAL_EMISSIVE)) {
             d.tangent_on = 1;
             V3 c = xf_point(xf[i], (v3(M.bmin.x, M.bmin.y, M.bmin.z) + M.bmax) * 0.5f);
@@ -788,6 +833,7 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
         for (int c = 0; c < 3; ++c) d.base[c] = m.base[c];
         d.metallic = m.metallic; d.roughness = m.roughness; d.ior = m.ior; d.transmission = m.transmission;
         d.coat = m.coat; d.coat_roughness = m.coat_roughness; d.anisotropy = m.anisotropy; d.absorption_mm = m.absorption_mm;
+        d.opacity = m.opacity;
         if (m.kind == MATERIAL_EMISSIVE)
             for (int c = 0; c < 3; ++c) d.emission[c] = rmax(m.emission[c] * m.emission_power, 0.0f);
         // medium_of (integrator/mod.rs:298)
@@ -939,7 +985,7 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
         if (F.stack_need > 96) { error = "unsupported: BVH too deep for the traversal stack"; return false; }
         if (F.tris.size() >= (1u << 27) - 16) { error = "unsupported: more than 2^27 triangles"; return false; }
     }
-    if (!prepare_lights(s, scene_box, F.lights, error)) return false;
+    if (!prepare_lights(s, scene_box, F.lights, F, error)) return false;
 
     // Scene constants: camera basis (scene/mod.rs:158) and render settings.
     SceneDev& S = F.scene;
@@ -963,8 +1009,27 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
     S.max_depth = s.max_depth == 0 ? 8 : (s.max_depth < 1024 ? s.max_depth : 1024);
     S.pixel_filter = s.pixel_filter;
     S.clamp_indirect = s.clamp_indirect;
-    S.background = (s.background_mode == 1 || s.background_mode == 3) ? 1 : (s.background_mode == 2 ? 2 : 0);
+    // The background image fitted to the frame (integrator/mod.rs:317); without one a background
+    // image shows the colour.
+    F.plate = s.backplate_map < s.bitmaps.size() ? &s.bitmaps[s.backplate_map] : nullptr;
+    if (F.plate) {
+        const float* r = s.backplate_rect;
+        const bool ok = r[2] > r[0] && r[3] > r[1];
+        for (int k = 0; k < 4; ++k) S.plate_rect[k] = ok ? r[k] : (k < 2 ? 0.0f : 1.0f);
+        const uint32_t w = s.width ? s.width : 1, h = s.height ? s.height : 1;
+        S.plate_w = F.plate->width;
+        S.plate_h = F.plate->height;
+        S.plate_fit = s.backplate_fit;
+        S.frame_aspect = ((S.plate_rect[2] - S.plate_rect[0]) * (float)w) / ((S.plate_rect[3] - S.plate_rect[1]) * (float)h);
+        S.image_aspect = (float)F.plate->width / (float)F.plate->height;
+    }
+    S.background = s.background_mode == 1 ? 1 : s.background_mode == 2 ? 2 : s.background_mode == 3 ? (F.plate ? 3 : 1) : 0;
     for (int c = 0; c < 3; ++c) S.background_color[c] = rmax(s.background_color[c], 0.0f);
+    for (const DevInstance& d : F.instances) S.any_passable |= d.passable;
+    for (const HInstance& in : s.instances) {
+        const HMaterial& m = s.materials[in.material_id];
+        if (m.kind != MATERIAL_EMISSIVE && m.opacity < 1.0f) S.any_cutout = 1;
+    }
     S.floor_mode = s.floor_mode;
     S.floor_z = s.floor_z;
     for (int c = 0; c < 3; ++c) S.floor_color[c] = s.floor_color[c];

@@ -42,6 +42,24 @@ struct HInstance {
     float rows[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
     uint32_t material_id = 0, flags = 0;
 };
+// A decoded bitmap: linear RGB texels (3 per pixel), rows top to bottom.
+struct HImage {
+    uint32_t width = 0, height = 0;
+    std::vector<float> texels;
+};
+// An environment map's sampling grid (rtg_bitmap.cpp): cell weights, per-row conditional CDFs,
+// the marginal CDF over rows, the mean weight, and the map's scale, rotation and mean luminance.
+struct HEnvMap {
+    uint32_t gw = 0, gh = 0;
+    std::vector<float> weights, conditional, marginal;
+    float mean = 0, scale = 0, rot_s = 0, rot_c = 1, mean_luminance = 0;
+};
+// Bitmap::decode (bitmap.rs:236): formats 0 and 1 (8-bit sRGB RGB, RGBA), 2 (linear f32 RGB) and
+// 16 (a Radiance file). False with the reason otherwise; `unsupported` for OpenEXR (17).
+bool decode_bitmap(uint32_t format, uint32_t width, uint32_t height, const uint8_t* data, size_t len, HImage& out, std::string& reason,
+                   bool& unsupported);
+// Map::new (environment.rs:60): false when the map has no light to sample.
+bool build_env_map(const HImage& img, float scale, float rotation_deg, HEnvMap& out);
 struct HScene {
     V3 cam_position{0, -1000, 0}, cam_target{0, 0, 0}, cam_up{0, 0, 1};
     float focal_mm = 50, sensor_mm = 36, fstop = 0, focus_dist = 1000, ortho_width = 1000;
@@ -51,10 +69,13 @@ struct HScene {
     std::vector<HMesh> meshes;
     std::vector<HInstance> instances;
     std::vector<HLight> lights;
-    uint32_t env_kind = 0;
+    std::vector<HImage> bitmaps;
+    uint32_t env_kind = 0;  // 0 studio, 1 flat, 2 sky, 3 HDRI
     float env_floor = 0.1f, env_horizon = 0.3f, env_zenith = 0.6f, env_strength = 1, env_rotation = 0;
     float background_color[3] = {0.05f, 0.05f, 0.05f};
-    uint32_t background_mode = 0;
+    uint32_t background_mode = 0;  // 0 environment, 1 colour, 2 transparent, 3 background image
+    uint32_t hdri_map = 0xffffffffu, backplate_map = 0xffffffffu, backplate_fit = 0;
+    float backplate_rect[4] = {0, 0, 1, 1};
     uint32_t floor_mode = 0;
     float floor_z = 0;
     float floor_color[3] = {0.5f, 0.5f, 0.5f};
@@ -67,9 +88,10 @@ struct HScene {
 // wording for format errors, "unsupported: ..." for features outside this path). With `kept`, a
 // file without MESH sections takes those meshes instead (Scene::update_from_rsb,
 // engine/crates/rt-core/src/scene/rsb.rs:1630): its INST sections, or the implicit instances of
-// the kept meshes, refer to them. `used_kept` (may be null) tells whether it did.
+// the kept meshes, refer to them. `used_kept` (may be null) tells whether it did. A file without
+// BMAP sections takes `kept_bitmaps` (when given) as its bitmaps, as the reference's update does.
 bool parse_rsb(const uint8_t* bytes, size_t len, HScene& out, std::string& error, const std::vector<HMesh>* kept = nullptr,
-               bool* used_kept = nullptr);
+               bool* used_kept = nullptr, const std::vector<HImage>* kept_bitmaps = nullptr);
 
 // What the device geometry (trees, leaf triangles, hit-detail arrays) of a scene depends on,
 // besides the meshes themselves: the instances' meshes, transforms and visibility flags. Two
@@ -78,6 +100,11 @@ std::string geometry_key(const HScene& s);
 
 // Flattened, device-ready arrays of a scene.
 struct Flat {
+    // the environment map's texels and sampling grid, the background image's texels (uploaded
+    // with the shading; the pointers in `lights` and `scene` are set on upload)
+    HEnvMap env_map;
+    const HImage* env_image = nullptr;
+    const HImage* plate = nullptr;
     std::vector<QNode> nodes;
     std::vector<TriRec> tris;
     std::vector<BlasInst> blas;

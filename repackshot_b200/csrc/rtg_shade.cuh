@@ -6,13 +6,105 @@
 
 namespace rtg {
 
+// ---- images (bitmap.rs:127-175) --------------------------------------------------------------------
+// f32 to u32 as Rust's `as` converts: NaN and negatives to 0, saturating above.
+RTG_D uint32_t sat_u32(float x) {
+    if (!(x > 0.0f)) return 0u;
+    if (x >= 4294967296.0f) return 0xffffffffu;
+    return (uint32_t)x;
+}
+RTG_D Rgb texel(const float* tex, uint32_t w, uint32_t h, uint32_t x, uint32_t y) {
+    x = x < w - 1 ? x : w - 1;
+    y = y < h - 1 ? y : h - 1;
+    const float* p = tex + 3 * ((size_t)y * w + x);
+    return rgb(p[0], p[1], p[2]);
+}
+// Bilinear lookup at (u, v), pixel centres at (i + 1/2) / n; wrap_u wraps the columns.
+RTG_D Rgb bilinear(const float* tex, uint32_t width, uint32_t height, float u, float v, bool wrap_u) {
+    float w = (float)width, h = (float)height;
+    float fx = u * w - 0.5f;
+    float fy = rclamp(v * h - 0.5f, 0.0f, h - 1.0f);
+    float x0f = floorf(fx), y0f = floorf(fy);
+    float tx = fx - x0f, ty = fy - y0f;
+    uint32_t x0, x1;
+    if (wrap_u) {
+        float r0 = fmodf(x0f, w), r1 = fmodf(x0f + 1.0f, w);
+        if (r0 < 0.0f) r0 = r0 + absf(w);
+        if (r1 < 0.0f) r1 = r1 + absf(w);
+        x0 = min(sat_u32(r0), width - 1);
+        x1 = min(sat_u32(r1), width - 1);
+    } else {
+        x0 = sat_u32(rclamp(x0f, 0.0f, w - 1.0f));
+        x1 = sat_u32(rclamp(x0f + 1.0f, 0.0f, w - 1.0f));
+    }
+    uint32_t y0 = sat_u32(y0f);
+    uint32_t y1 = y0 + 1 < height - 1 ? y0 + 1 : height - 1;
+    Rgb top = texel(tex, width, height, x0, y0) * (1.0f - tx) + texel(tex, width, height, x1, y0) * tx;
+    Rgb bottom = texel(tex, width, height, x0, y1) * (1.0f - tx) + texel(tex, width, height, x1, y1) * tx;
+    return top * (1.0f - ty) + bottom * ty;
+}
+
+// ---- environment map (environment.rs:40-130, bitmap.rs:312-408) -----------------------------------
+RTG_D void dir_to_uv(V3 d, float& u, float& v) {
+    float uu = 0.5f + fatan2(-d.y, d.x) * (0.5f * FRAC_1_PI);
+    u = uu - floorf(uu);
+    v = rclamp(facos(d.z) * FRAC_1_PI, 0.0f, 1.0f);
+}
+RTG_D V3 map_to_image(const EnvMapDev& m, V3 d) { return v3(m.rot_c * d.x + m.rot_s * d.y, -m.rot_s * d.x + m.rot_c * d.y, d.z); }
+RTG_D V3 map_to_world(const EnvMapDev& m, V3 d) { return v3(m.rot_c * d.x - m.rot_s * d.y, m.rot_s * d.x + m.rot_c * d.y, d.z); }
+RTG_D Rgb map_radiance(const EnvMapDev& m, V3 dir) {
+    float u, v;
+    dir_to_uv(map_to_image(m, dir), u, v);
+    return bilinear(m.texels, m.width, m.height, u, v, true) * m.scale;
+}
+// The bucket of a normalised CDF that holds u (the first entry above u), and u rescaled into it.
+RTG_D void cdf_search(const float* cdf, uint32_t n, float u, uint32_t& i, float& rest) {
+    uint32_t lo = 0, hi = n;  // partition point of cdf[k] <= u
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (cdf[mid] <= u) lo = mid + 1;
+        else hi = mid;
+    }
+    i = lo < n - 1 ? lo : n - 1;
+    float below = i == 0 ? 0.0f : cdf[i - 1];
+    float width = cdf[i] - below;
+    rest = width > 0.0f ? rclamp((u - below) / width, 0.0f, 0.99999994f) : 0.5f;
+}
+RTG_D float map_cell_pdf(const EnvMapDev& m, float u, float v) {
+    uint32_t x = min(sat_u32(u * (float)m.gw), m.gw - 1), y = min(sat_u32(v * (float)m.gh), m.gh - 1);
+    return m.weights[y * m.gw + x] / m.mean;
+}
+RTG_D float map_pdf(const EnvMapDev& m, V3 dir) {
+    V3 local = map_to_image(m, dir);
+    float sin_theta = sqrt_(rmax((1.0f - local.z) * (1.0f + local.z), 0.0f));
+    if (sin_theta <= 0.0f) return 0.0f;
+    float u, v;
+    dir_to_uv(local, u, v);
+    return map_cell_pdf(m, u, v) / (2.0f * PI * PI * sin_theta);
+}
+RTG_D bool map_sample(const EnvMapDev& m, float s0, float s1, V3& dir, float& pdf) {
+    uint32_t y, x;
+    float fy, fx;
+    cdf_search(m.marginal, m.gh, s1, y, fy);
+    cdf_search(m.conditional + (size_t)y * m.gw, m.gw, s0, x, fx);
+    float u = ((float)x + fx) / (float)m.gw, v = ((float)y + fy) / (float)m.gh;
+    float pdf_uv = m.weights[y * m.gw + x] / m.mean;
+    float st, ct, sp, cp;
+    sin_cos(PI * v, st, ct);
+    sin_cos(TAU * (u - 0.5f), sp, cp);
+    if (!(st > 0.0f && pdf_uv > 0.0f)) return false;
+    dir = normalize(map_to_world(m, v3(st * cp, -st * sp, ct)));
+    pdf = map_pdf(m, dir);
+    return pdf > 0.0f;
+}
+
 // ---- environment ramp ---------------------------------------------------------------------------
 RTG_D float env_value(const LightsDev& L, float z) {
     z = rclamp(z, -1.0f, 1.0f);
     if (z < 0.0f) return L.env_floor * -z + L.env_horizon * (1.0f + z);
     return L.env_horizon * (1.0f - z) + L.env_zenith * z;
 }
-RTG_D float env_pdf(const LightsDev& L, V3 dir) {
+RTG_D float ramp_pdf(const LightsDev& L, V3 dir) {
     if (L.env_total <= 0.0f) return 0.0f;
     return env_value(L, dir.z) / (TAU * L.env_total);
 }
@@ -21,7 +113,7 @@ RTG_D float invert_linear(float a, float b, float u) {
     float denom = a + sqrt_(rmax(a * a + 2.0f * (b - a) * c, 0.0f));
     return denom > 0.0f ? rclamp(2.0f * c / denom, 0.0f, 1.0f) : 0.0f;
 }
-RTG_D bool env_sample(const LightsDev& L, float u0, float u1, V3& dir, float& pdf) {
+RTG_D bool ramp_sample(const LightsDev& L, float u0, float u1, V3& dir, float& pdf) {
     if (L.env_total <= 0.0f) return false;
     float target = u0 * L.env_total;
     float z;
@@ -36,8 +128,38 @@ RTG_D bool env_sample(const LightsDev& L, float u0, float u1, V3& dir, float& pd
     float s, c;
     sin_cos(TAU * u1, s, c);
     dir = v3(r * c, r * s, z);
-    pdf = env_pdf(L, dir);
+    pdf = ramp_pdf(L, dir);
     return pdf > 0.0f;
+}
+// EnvLight (environment.rs:333): the map or the ramp.
+RTG_D Rgb env_radiance(const LightsDev& L, V3 dir) { return L.env_is_map ? map_radiance(L.env_map, dir) : splat(env_value(L, dir.z)); }
+RTG_D float env_pdf(const LightsDev& L, V3 dir) { return L.env_is_map ? map_pdf(L.env_map, dir) : ramp_pdf(L, dir); }
+RTG_D bool env_sample(const LightsDev& L, float u0, float u1, V3& dir, float& pdf) {
+    return L.env_is_map ? map_sample(L.env_map, u0, u1, dir, pdf) : ramp_sample(L, u0, u1, dir, pdf);
+}
+
+// ---- background image (integrator/mod.rs:199-232) -----------------------------------------------------
+// What a camera ray that escapes shows at screen position (su, sv): the fitted image, or the
+// background colour outside a fitted image.
+RTG_D Rgb backdrop(const SceneDev& S, float su, float sv) {
+    const Rgb colour = rgb(S.background_color[0], S.background_color[1], S.background_color[2]);
+    if (S.background != 3) return colour;
+    float u = (su - S.plate_rect[0]) / (S.plate_rect[2] - S.plate_rect[0]);
+    float v = (sv - S.plate_rect[1]) / (S.plate_rect[3] - S.plate_rect[1]);
+    if (S.plate_fit != 2) {
+        const bool fit = S.plate_fit == 1;
+        const float k = S.frame_aspect / S.image_aspect;
+        if (S.image_aspect > S.frame_aspect) {
+            if (fit) v = 0.5f + (v - 0.5f) * (1.0f / k);
+            else u = 0.5f + (u - 0.5f) * k;
+        } else if (fit) {
+            u = 0.5f + (u - 0.5f) * k;
+        } else {
+            v = 0.5f + (v - 0.5f) * (S.image_aspect / S.frame_aspect);
+        }
+    }
+    if (S.plate_fit == 1 && !(u >= 0.0f && u <= 1.0f && v >= 0.0f && v <= 1.0f)) return colour;
+    return bilinear(S.plate, S.plate_w, S.plate_h, rclamp(u, 0.0f, 1.0f), rclamp(v, 0.0f, 1.0f), false);
 }
 
 // The selection at a vertex (light.rs:495): its point, the sum of the weights there and whether
@@ -87,16 +209,16 @@ RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, flo
         pmf = pmf_of(L, (uint32_t)index, s);
     } else {
         if (!(s.total > 0.0f && finitef(s.total))) return false;
-        float acc = 0.0f, lo = 0.0f;
+        // pick_at (light.rs:1118): the first bucket whose end passes u_select (the point within
+        // it is not needed: every light kind here samples with its own two numbers)
+        float acc = 0.0f;
         int last = n - 1;
         for (int e = 0; e <= last; ++e) {
             float w = entry_weight(L, e, s.p);
             acc += w;
             float hi = e == last ? 1.0f : acc / s.total;
             if (hi > u_select || e == last) { index = e; pmf = w / s.total; break; }
-            lo = hi;
         }
-        (void)lo;
     }
     if (!(pmf > 0.0f)) return false;
     int a = L.entries[index];
@@ -170,7 +292,7 @@ RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, flo
         if (!env_sample(L, u0, u1, wi, p)) return false;
         out.wi = wi;
         out.distance = f_inf();
-        out.radiance = splat(env_value(L, wi.z));
+        out.radiance = env_radiance(L, wi);
         out.pdf = pmf * p;
         out.glossy = true;
         out.shadow = true;
@@ -240,7 +362,7 @@ RTG_D_NI Rgb add_suns(const LightsDev& L, Rgb sum, V3 dir, bool has_pdf, float p
 }
 // Lights::escaped (light.rs:1502): the ramp environment, then the sun discs.
 RTG_D Rgb escaped(const LightsDev& L, V3 dir, bool has_pdf, float pdf, const Sel& from) {
-    Rgb sum = splat(env_value(L, dir.z));
+    Rgb sum = env_radiance(L, dir);
     if (has_pdf && L.env_is_entry) sum = sum * power_heuristic(pdf, pmf_of(L, L.env_entry, from) * env_pdf(L, dir));
     return L.n_suns ? add_suns(L, sum, dir, has_pdf, pdf, from) : sum;
 }
@@ -250,6 +372,15 @@ RTG_D float filter_offset(uint32_t filter, float u) {
     if (filter == 1) return 0.5f;
     if (filter == 2) return 0.5f + (u < 0.5f ? sqrt_(2.0f * u) - 1.0f : 1.0f - sqrt_(2.0f - 2.0f * u));
     return u;
+}
+// The screen position (u, v) in [0, 1]^2 of a camera sample (render.rs:96).
+RTG_D void screen_of(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, float& su, float& sv) {
+    uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
+    uint64_t key = pixel_key(S.seed, x, y);
+    float du = filter_offset(S.pixel_filter, sample1(T, key, index, DIM_CAMERA));
+    float dv = filter_offset(S.pixel_filter, sample1(T, key, index, DIM_CAMERA + 1));
+    su = rclamp(((float)x + du) / (float)width, 0.0f, 1.0f);
+    sv = rclamp(((float)y + dv) / (float)height, 0.0f, 1.0f);
 }
 RTG_D void camera_ray(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, V3& o, V3& d) {
     uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
