@@ -418,10 +418,116 @@ bool EnvMap::sample(float u0, float u1, Vec3& dir, float& pdf_out) const {
     pdf_out = pdf(dir);
     return pdf_out > 0.0f;
 }
+// ---- sky.rs:200-348 the classic sky ----------------------------------------------------------------
+// The Perez coefficients A..E as (slope, intercept) in the turbidity for Y, x and y, and the zenith
+// chromaticity fits: Preetham et al. 1999, Appendix A.2.
+static const float PEREZ_TABLE[3][5][2] = {
+    {{0.1787f, -1.4630f}, {-0.3554f, 0.4275f}, {-0.0227f, 5.3251f}, {0.1206f, -2.5771f}, {-0.0670f, 0.3703f}},
+    {{-0.0193f, -0.2592f}, {-0.0665f, 0.0008f}, {-0.0004f, 0.2125f}, {-0.0641f, -0.8989f}, {-0.0033f, 0.0452f}},
+    {{-0.0167f, -0.2608f}, {-0.0950f, 0.0092f}, {-0.0079f, 0.2102f}, {-0.0441f, -1.6537f}, {-0.0109f, 0.0529f}},
+};
+static const float ZENITH_XC[3][4] = {{0.00166f, -0.00375f, 0.00209f, 0.0f}, {-0.02903f, 0.06377f, -0.03202f, 0.00394f},
+                                      {0.11693f, -0.21196f, 0.06052f, 0.25886f}};
+static const float ZENITH_YC[3][4] = {{0.00275f, -0.00610f, 0.00317f, 0.0f}, {-0.04214f, 0.08970f, -0.04153f, 0.00516f},
+                                      {0.15346f, -0.26756f, 0.06670f, 0.26688f}};
+static float sky_exp(float x) { return fexp(rclamp(x, -80.0f, 80.0f)); }
+static float perez(const float* c, float cos_theta, float gamma, float cos_gamma) {
+    return (1.0f + c[0] * sky_exp(c[1] / cos_theta)) * (1.0f + c[2] * sky_exp(c[3] * gamma) + c[4] * cos_gamma * cos_gamma);
+}
+static Rgb xyy_to_rgb(float x, float y, float lum) {  // sky.rs:341 (IEC 61966-2-1, D65)
+    float bx = x / y * lum;
+    float bz = (1.0f - x - y) / y * lum;
+    float r = 3.2404542f * bx - 1.5371385f * lum - 0.4985314f * bz;
+    float g = -0.969266f * bx + 1.8760108f * lum + 0.041556f * bz;
+    float b = 0.0556434f * bx - 0.2040259f * lum + 1.0572252f * bz;
+    return Rgb(rmax(r, 0.0f), rmax(g, 0.0f), rmax(b, 0.0f));
+}
+Preetham Preetham::make(float azimuth_deg, float elevation_deg, float turbidity) {
+    Preetham p;
+    float t = finite(turbidity) ? rclamp(turbidity, 1.7f, 10.0f) : 3.0f;
+    float elevation = finite(elevation_deg) ? rclamp(elevation_deg, 1.0f, 90.0f) : 45.0f;
+    float azimuth = finite(azimuth_deg) ? azimuth_deg : 0.0f;
+    float se, ce, sa, ca;
+    sin_cos(elevation * DEG_TO_RAD, se, ce);
+    sin_cos(azimuth * DEG_TO_RAD, sa, ca);
+    p.sun = Vec3(ce * ca, ce * sa, se);
+    float theta_s = (90.0f - elevation) * DEG_TO_RAD;
+    for (int q = 0; q < 3; ++q)
+        for (int k = 0; k < 5; ++k) p.coefficients[q][k] = PEREZ_TABLE[q][k][0] * t + PEREZ_TABLE[q][k][1];
+    float chi = (4.0f / 9.0f - t / 120.0f) * (PI - 2.0f * theta_s);
+    float sc, cc;
+    sin_cos(chi, sc, cc);
+    float y_z = (4.0453f * t - 4.9710f) * (sc / cc) - 0.2155f * t + 2.4192f;
+    float th[4] = {theta_s * theta_s * theta_s, theta_s * theta_s, theta_s, 1.0f};
+    auto poly = [&](const float (*m)[4]) {
+        float tt[3] = {t * t, t, 1.0f};
+        float sum = 0.0f;
+        for (int i = 0; i < 3; ++i) {
+            float r = 0.0f;
+            for (int j = 0; j < 4; ++j) r += m[i][j] * th[j];
+            sum += tt[i] * r;
+        }
+        return sum;
+    };
+    float zenith[3] = {rmax(y_z, 1.0e-3f), poly(ZENITH_XC), poly(ZENITH_YC)};
+    float cs = fcos(theta_s);
+    for (int q = 0; q < 3; ++q) p.zenith_over_perez[q] = zenith[q] / perez(p.coefficients[q], 1.0f, theta_s, cs);
+    return p;
+}
+Rgb Preetham::radiance(Vec3 dir) const {
+    if (dir.z <= 0.0f) return BLACK;
+    float cos_gamma = rclamp(dot(dir, sun), -1.0f, 1.0f);
+    float gamma = facos(cos_gamma);
+    float cos_theta = rmax(dir.z, 1.0e-3f);
+    float v[3];
+    for (int q = 0; q < 3; ++q) v[q] = zenith_over_perez[q] * perez(coefficients[q], cos_theta, gamma, cos_gamma);
+    return xyy_to_rgb(v[1], rmax(v[2], 1.0e-4f), rmax(v[0], 0.0f));
+}
+// environment.rs:207 tabulate_sky for the classic model (plain sums): the upper half from the
+// model, scaled so that a horizontal surface gets the dome's irradiance 2 pi (horizon / 6 +
+// zenith / 3) strength; the lower half the ground, floor * strength.
+Image sky_image(const Environment& env) {
+    Preetham sky = Preetham::make(env.sun_azimuth_deg, env.sun_elevation_deg, env.sky_turbidity);
+    const uint32_t w = 256, h = 128;
+    std::vector<float> rgb(3 * (size_t)w * h, 0.0f);
+    float irradiance = 0.0f;
+    const float cell = (PI / (float)h) * (TAU / (float)w);
+    for (uint32_t y = 0; y < h / 2; ++y) {
+        float v = ((float)y + 0.5f) / (float)h;
+        float row = 0.0f;
+        for (uint32_t x = 0; x < w; ++x) {
+            float u = ((float)x + 0.5f) / (float)w, sin_theta;
+            Vec3 d = uv_to_direction(u, v, sin_theta);
+            Rgb c = sky.radiance(d);
+            float* o = &rgb[3 * ((size_t)y * w + x)];
+            o[0] = c.r; o[1] = c.g; o[2] = c.b;
+            row += c.luminance() * d.z * sin_theta;
+        }
+        irradiance += row * cell;
+    }
+    irradiance = irradiance + 0.0f;
+    float strength = rmax(env.strength, 0.0f);
+    float target = strength * TAU * (rmax(env.horizon, 0.0f) / 6.0f + rmax(env.zenith, 0.0f) / 3.0f);
+    float scale = irradiance > 0.0f ? target / irradiance : 0.0f;
+    float ground = rmax(env.floor * strength, 0.0f);
+    for (size_t i = 0; i < rgb.size(); ++i) rgb[i] = i / (3 * (size_t)w) < h / 2 ? rgb[i] * scale : ground;
+    Image img;
+    img.width = w;
+    img.height = h;
+    img.linear = std::move(rgb);
+    return img;
+}
+
 EnvLight EnvLight::make(const Environment& env, const std::vector<Image>& bitmaps) {  // environment.rs:335
     EnvLight e;
     float strength = rmax(env.strength, 0.0f);
     if (env.kind == 1) { e.ramp = Ramp::make(env.horizon, env.horizon, env.horizon, strength); return e; }
+    if (env.kind == 2) {
+        e.owned = std::make_shared<Image>(sky_image(env));
+        if (EnvMap::make(e.owned.get(), 1.0f, 0.0f, e.map)) e.is_map = true;
+        else e.ramp = Ramp::make(0.0f, 0.0f, 0.0f, strength);
+        return e;
+    }
     if (env.kind == 3 && env.hdri_map != NO_BITMAP && env.hdri_map < bitmaps.size()) {
         if (EnvMap::make(&bitmaps[env.hdri_map], strength, env.rotation_deg, e.map)) e.is_map = true;
         else e.ramp = Ramp::make(0.0f, 0.0f, 0.0f, strength);

@@ -196,7 +196,7 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
                   r.opt_f32(e.backplate_rect[0], 0.0f) && r.opt_f32(e.backplate_rect[1], 0.0f) && r.opt_f32(e.backplate_rect[2], 1.0f) &&
                   r.opt_f32(e.backplate_rect[3], 1.0f) && r.opt_u32(e.sky_model, 0)))
                 return false;
-            if (e.kind == 2) { error = "unsupported: sky environment"; return false; }
+            if (e.kind == 2 && e.sky_model != 1) { error = "unsupported: physical sky model"; return false; }
         } else if (is("BMAP")) {  // rsb.rs:1057
             uint32_t format, w, h, n;
             if (!(r.u32(format) && r.u32(w) && r.u32(h) && r.u32(n))) return false;

@@ -2,6 +2,7 @@
 // camera, restated from engine/crates/rt-core/src/{scene/mod.rs, scene/rsb.rs, light.rs,
 // environment.rs}.
 #pragma once
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -117,8 +118,20 @@ struct EnvMap {
     float pdf(Vec3 dir) const;
     bool sample(float u0, float u1, Vec3& dir, float& pdf_out) const;
 };
+// sky.rs:245 the classic sky (Preetham, Shirley and Smits 1999) before scaling
+struct Preetham {
+    Vec3 sun;
+    float coefficients[3][5];
+    float zenith_over_perez[3];
+    static Preetham make(float azimuth_deg, float elevation_deg, float turbidity);
+    Rgb radiance(Vec3 dir) const;
+};
+// environment.rs:178 sky_image: the sky tabulated into a 256 x 128 map (the classic model only)
+Image sky_image(const Environment& env);
+
 // environment.rs:333 EnvLight: the ramp or a map
 struct EnvLight {
+    std::shared_ptr<Image> owned;  // the tabulated sky
     bool is_map = false;
     Ramp ramp;
     EnvMap map;

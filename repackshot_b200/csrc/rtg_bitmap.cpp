@@ -290,4 +290,112 @@ bool build_env_map(const HImage& img, float scale, float rotation_deg, HEnvMap& 
     return true;
 }
 
+// ---- the classic sky (sky.rs:200-348): Preetham, Shirley and Smits 1999 -----------------------------
+namespace {
+// The Perez coefficients A..E as (slope, intercept) in the turbidity for the luminance Y and the
+// chromaticities x, y, and the zenith chromaticity fits in (T^2, T, 1) x (theta^3, theta^2,
+// theta, 1): the paper's Appendix A.2.
+constexpr float kPerez[3][5][2] = {
+    {{0.1787f, -1.4630f}, {-0.3554f, 0.4275f}, {-0.0227f, 5.3251f}, {0.1206f, -2.5771f}, {-0.0670f, 0.3703f}},
+    {{-0.0193f, -0.2592f}, {-0.0665f, 0.0008f}, {-0.0004f, 0.2125f}, {-0.0641f, -0.8989f}, {-0.0033f, 0.0452f}},
+    {{-0.0167f, -0.2608f}, {-0.0950f, 0.0092f}, {-0.0079f, 0.2102f}, {-0.0441f, -1.6537f}, {-0.0109f, 0.0529f}}};
+constexpr float kZenithX[3][4] = {{0.00166f, -0.00375f, 0.00209f, 0.0f}, {-0.02903f, 0.06377f, -0.03202f, 0.00394f},
+                                  {0.11693f, -0.21196f, 0.06052f, 0.25886f}};
+constexpr float kZenithY[3][4] = {{0.00275f, -0.00610f, 0.00317f, 0.0f}, {-0.04214f, 0.08970f, -0.04153f, 0.00516f},
+                                  {0.15346f, -0.26756f, 0.06670f, 0.26688f}};
+
+float clamped_exp(float x) { return fexp(rclamp(x, -80.0f, 80.0f)); }
+// The Perez distribution F(theta, gamma) from cos theta, gamma and cos gamma.
+float perez_f(const float* c, float cos_theta, float gamma, float cos_gamma) {
+    return (1.0f + c[0] * clamped_exp(c[1] / cos_theta)) * (1.0f + c[2] * clamped_exp(c[3] * gamma) + c[4] * cos_gamma * cos_gamma);
+}
+
+struct ClassicSky {
+    V3 sun;
+    float coef[3][5], zenith_over_perez[3];
+    ClassicSky(float azimuth_deg, float elevation_deg, float turbidity) {
+        const float t = finitef(turbidity) ? rclamp(turbidity, 1.7f, 10.0f) : 3.0f;
+        const float elevation = finitef(elevation_deg) ? rclamp(elevation_deg, 1.0f, 90.0f) : 45.0f;
+        const float azimuth = finitef(azimuth_deg) ? azimuth_deg : 0.0f;
+        float se, ce, sa, ca;
+        sin_cos(elevation * (PI / 180.0f), se, ce);
+        sin_cos(azimuth * (PI / 180.0f), sa, ca);
+        sun = v3(ce * ca, ce * sa, se);
+        const float theta_s = (90.0f - elevation) * (PI / 180.0f);
+        for (int q = 0; q < 3; ++q)
+            for (int k = 0; k < 5; ++k) coef[q][k] = kPerez[q][k][0] * t + kPerez[q][k][1];
+        // zenith luminance (kcd/m^2) and chromaticity
+        const float chi = (4.0f / 9.0f - t / 120.0f) * (PI - 2.0f * theta_s);
+        float sc, cc;
+        sin_cos(chi, sc, cc);
+        const float y_z = (4.0453f * t - 4.9710f) * (sc / cc) - 0.2155f * t + 2.4192f;
+        const float th[4] = {theta_s * theta_s * theta_s, theta_s * theta_s, theta_s, 1.0f};
+        const float tt[3] = {t * t, t, 1.0f};
+        auto fit = [&](const float (*m)[4]) {
+            float sum = 0.0f;
+            for (int i = 0; i < 3; ++i) {
+                float r = 0.0f;
+                for (int j = 0; j < 4; ++j) r += m[i][j] * th[j];
+                sum += tt[i] * r;
+            }
+            return sum;
+        };
+        const float zenith[3] = {rmax(y_z, 1.0e-3f), fit(kZenithX), fit(kZenithY)};
+        const float cs = fcos(theta_s);
+        for (int q = 0; q < 3; ++q) zenith_over_perez[q] = zenith[q] / perez_f(coef[q], 1.0f, theta_s, cs);
+    }
+    // Linear Rec. 709 radiance in a unit direction above the horizon; black below.
+    Rgb radiance(V3 dir) const {
+        if (dir.z <= 0.0f) return rgb(0.0f, 0.0f, 0.0f);
+        const float cos_gamma = rclamp(dot(dir, sun), -1.0f, 1.0f);
+        const float gamma = facos(cos_gamma);
+        const float cos_theta = rmax(dir.z, 1.0e-3f);
+        float v[3];
+        for (int q = 0; q < 3; ++q) v[q] = zenith_over_perez[q] * perez_f(coef[q], cos_theta, gamma, cos_gamma);
+        const float lum = rmax(v[0], 0.0f), x = v[1], y = rmax(v[2], 1.0e-4f);
+        // CIE xyY to XYZ to linear Rec. 709 (IEC 61966-2-1, D65), negatives clamped
+        const float bx = x / y * lum, bz = (1.0f - x - y) / y * lum;
+        const float r = 3.2404542f * bx - 1.5371385f * lum - 0.4985314f * bz;
+        const float g = -0.969266f * bx + 1.8760108f * lum + 0.041556f * bz;
+        const float b = 0.0556434f * bx - 0.2040259f * lum + 1.0572252f * bz;
+        return rgb(rmax(r, 0.0f), rmax(g, 0.0f), rmax(b, 0.0f));
+    }
+};
+}  // namespace
+
+HImage classic_sky_image(const HScene& s) {
+    const ClassicSky sky(s.sun_azimuth_deg, s.sun_elevation_deg, s.sky_turbidity);
+    const uint32_t w = 256, h = 128;
+    HImage img;
+    img.width = w;
+    img.height = h;
+    img.texels.assign(3 * (size_t)w * h, 0.0f);
+    float irradiance = 0.0f;
+    const float cell = (PI / (float)h) * (TAU / (float)w);
+    for (uint32_t y = 0; y < h / 2; ++y) {
+        const float v = ((float)y + 0.5f) / (float)h;
+        float st, ct;
+        sin_cos(PI * v, st, ct);
+        float row = 0.0f;
+        for (uint32_t x = 0; x < w; ++x) {
+            const float u = ((float)x + 0.5f) / (float)w;
+            float sp, cp;
+            sin_cos(TAU * (u - 0.5f), sp, cp);
+            const V3 d = v3(st * cp, -st * sp, ct);  // uv_to_direction (environment.rs:53)
+            const Rgb c = sky.radiance(d);
+            float* o = &img.texels[3 * ((size_t)y * w + x)];
+            o[0] = c.r; o[1] = c.g; o[2] = c.b;
+            row += luminance(c) * d.z * st;
+        }
+        irradiance += row * cell;
+    }
+    const float strength = rmax(s.env_strength, 0.0f);
+    const float target = strength * TAU * (rmax(s.env_horizon, 0.0f) / 6.0f + rmax(s.env_zenith, 0.0f) / 3.0f);
+    const float scale = irradiance > 0.0f ? target / irradiance : 0.0f;
+    const float ground = rmax(s.env_floor * strength, 0.0f);
+    for (size_t i = 0; i < img.texels.size(); ++i)
+        img.texels[i] = i / (3 * (size_t)w) < h / 2 ? img.texels[i] * scale : ground;
+    return img;
+}
+
 }  // namespace rtg

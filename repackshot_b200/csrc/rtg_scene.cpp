@@ -178,14 +178,12 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (!(r.f32(s.env_floor) && r.f32(s.env_horizon) && r.f32(s.env_zenith) && r.f32(s.env_strength) && r.f32(s.env_rotation) &&
                   r.f3(s.background_color) && r.u32(s.background_mode)))
                 return false;
-            float turbidity, azimuth, elevation;
-            uint32_t sky_model;
             if (!(r.ou32(s.hdri_map, 0xffffffffu) && r.ou32(s.backplate_map, 0xffffffffu) && r.ou32(s.backplate_fit, 0) &&
-                  r.of32(turbidity, 3.0f) && r.of32(azimuth, 0.0f) && r.of32(elevation, 45.0f) && r.of32(s.backplate_rect[0], 0.0f) &&
-                  r.of32(s.backplate_rect[1], 0.0f) && r.of32(s.backplate_rect[2], 1.0f) && r.of32(s.backplate_rect[3], 1.0f) &&
-                  r.ou32(sky_model, 0)))
+                  r.of32(s.sky_turbidity, 3.0f) && r.of32(s.sun_azimuth_deg, 0.0f) && r.of32(s.sun_elevation_deg, 45.0f) &&
+                  r.of32(s.backplate_rect[0], 0.0f) && r.of32(s.backplate_rect[1], 0.0f) && r.of32(s.backplate_rect[2], 1.0f) &&
+                  r.of32(s.backplate_rect[3], 1.0f) && r.ou32(s.sky_model, 0)))
                 return false;
-            if (s.env_kind == 2) { error = "unsupported: sky environment"; return false; }
+            if (s.env_kind == 2 && s.sky_model != 1) { error = "unsupported: physical sky model"; return false; }
         } else if (is("BMAP")) {  // rsb.rs:1057
             uint32_t format, w, h, n;
             if (!(r.u32(format) && r.u32(w) && r.u32(h) && r.u32(n))) return false;
@@ -679,7 +677,15 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
     float strength = rmax(s.env_strength, 0.0f);
     float f0 = s.env_kind == 1 ? s.env_horizon : s.env_floor, h0 = s.env_horizon, z0 = s.env_kind == 1 ? s.env_horizon : s.env_zenith;
     F.env_image = nullptr;
-    if (s.env_kind == 3 && s.hdri_map < s.bitmaps.size()) {
+    if (s.env_kind == 2) {  // the sky, tabulated; scale 1 and no rotation
+        F.sky = classic_sky_image(s);
+        if (build_env_map(F.sky, 1.0f, 0.0f, F.env_map)) {
+            L.env_is_map = 1;
+            F.env_image = &F.sky;
+        } else {
+            f0 = h0 = z0 = 0.0f;
+        }
+    } else if (s.env_kind == 3 && s.hdri_map < s.bitmaps.size()) {
         if (build_env_map(s.bitmaps[s.hdri_map], strength, s.env_rotation, F.env_map)) {
             L.env_is_map = 1;
             F.env_image = &s.bitmaps[s.hdri_map];

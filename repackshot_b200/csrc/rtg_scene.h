@@ -60,6 +60,10 @@ bool decode_bitmap(uint32_t format, uint32_t width, uint32_t height, const uint8
                    bool& unsupported);
 // Map::new (environment.rs:60): false when the map has no light to sample.
 bool build_env_map(const HImage& img, float scale, float rotation_deg, HEnvMap& out);
+// sky_image (environment.rs:178) of the classic sky model (sky.rs:245, Preetham et al. 1999): the
+// sky tabulated into a 256 x 128 map, scaled to the dome's irradiance, the ground below.
+struct HScene;
+HImage classic_sky_image(const HScene& s);
 struct HScene {
     V3 cam_position{0, -1000, 0}, cam_target{0, 0, 0}, cam_up{0, 0, 1};
     float focal_mm = 50, sensor_mm = 36, fstop = 0, focus_dist = 1000, ortho_width = 1000;
@@ -76,6 +80,8 @@ struct HScene {
     uint32_t background_mode = 0;  // 0 environment, 1 colour, 2 transparent, 3 background image
     uint32_t hdri_map = 0xffffffffu, backplate_map = 0xffffffffu, backplate_fit = 0;
     float backplate_rect[4] = {0, 0, 1, 1};
+    float sky_turbidity = 3, sun_azimuth_deg = 0, sun_elevation_deg = 45;
+    uint32_t sky_model = 0;  // 0 physical, 1 classic
     uint32_t floor_mode = 0;
     float floor_z = 0;
     float floor_color[3] = {0.5f, 0.5f, 0.5f};
@@ -103,6 +109,7 @@ struct Flat {
     // the environment map's texels and sampling grid, the background image's texels (uploaded
     // with the shading; the pointers in `lights` and `scene` are set on upload)
     HEnvMap env_map;
+    HImage sky;  // the tabulated sky of a sky environment
     const HImage* env_image = nullptr;
     const HImage* plate = nullptr;
     std::vector<QNode> nodes;

@@ -316,11 +316,13 @@ def hdr_encode(width: int, height: int, rgb) -> bytes:
     return bytes(out)
 
 
-def e5_scene() -> Scene:
-    """example.rs:232 e5_scene(false): the example at 160 x 120 and depth 12 with clear blue glass
+def e5_scene(sky: bool = False) -> Scene:
+    """example.rs:232 e5_scene: the example at 160 x 120 and depth 12 with clear blue glass
     (absorption 80 mm), a lacquered floor, brushed metal (anisotropy 0.8), a thin glass card and a
     cut-out card (opacity 0.4), lit by its rect light and a 64 x 32 HDRI panorama (a grey gradient
-    with two bright panels, rotated 30 degrees) over a 16 x 8 background image."""
+    with two bright panels, rotated 30 degrees) over a 16 x 8 background image. With `sky`, the
+    classic sky (sun 35 degrees up at azimuth -60) seen as the background, lit by a sun of
+    irradiance 3 and a disc of 0.545 degrees instead of the rect light."""
     s = example_scene()
     s.width, s.height, s.max_depth = 160, 120, 12
     s.materials = [
@@ -347,6 +349,11 @@ def e5_scene() -> Scene:
     s.env_kind, s.hdri_map, s.backplate_map, s.background_mode = 3, 0, 1, 3
     s.env_floor, s.env_horizon, s.env_zenith, s.env_strength, s.env_rotation = 0.1, 0.3, 0.6, 1.0, 30.0
     s.background_color = (0.05, 0.05, 0.05)
+    if sky:
+        s.env_kind, s.sky_model, s.background_mode = 2, 1, 0
+        s.sun_azimuth_deg, s.sun_elevation_deg = -60.0, 35.0
+        s.lights = [Light(kind=LIGHT_SUN, position=(0.0, 0.0, 1000.0), direction=(-0.41, 0.71, -0.574), up=(0.0, 1.0, 0.0),
+                          size_x=500.0, size_y=500.0, color=(1.0, 0.91, 0.83), power=3.0, angle_deg=0.545, flags=3)]
     return s
 
 

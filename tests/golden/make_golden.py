@@ -7,8 +7,8 @@ its path tracer, read from the reference's own source tree (run where it is chec
 * SHA-256 of the six energy tables (engine/crates/rt-core/src/bsdf/energy_table.rs), as the
   little-endian bytes of their u16 values and f32 bit patterns;
 * SHA-256 of the example scene file (tests/fixtures/example.rsb);
-* the FNV-1a film hash of the E5 scene with its HDRI (render.rs:1106) and SHA-256 of its file
-  (tests/fixtures/e5.rsb).
+* the FNV-1a film hashes of the E5 scene with its HDRI and with the classic sky (render.rs:1106-1109)
+  and SHA-256 of the HDRI scene's file (tests/fixtures/e5.rsb).
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -41,6 +41,7 @@ def main():
         "tile_centre_240_176_s3": pinned(render, "PINNED_CENTRE"),
         "tile_small_sphere_48_144_s3": pinned(render, "PINNED_SMALL_SPHERE"),
         "e5_hdri_4spp": pinned(render, "PINNED_E5_HDRI_4SPP"),
+        "e5_sky_4spp": pinned(render, "PINNED_E5_SKY_4SPP"),
     }
     block = rng[rng.index("fn matches_the_reference_implementation"):]
     block = block[:block.index("]")]

@@ -2,7 +2,9 @@
 sampling, rotation), a background image, cut-outs (paths pass them without a vertex, in extra
 rounds of the wave) and thin walls, and shadow rays that walk through both.
 
-* The E5 scene at 4 samples has the reference's pinned film hash (render.rs:1086-1107).
+* The E5 scene at 4 samples has the reference's pinned film hash (render.rs:1086-1107), under its
+  HDRI and under the classic sky; other skies (low and high suns, turbidity, a sun below the
+  horizon) have the oracle's film bits.
 * Variants (background image fill, fit and stretch over a sub-rectangle; an 8-bit sRGB HDRI; the
   cut-out card alone; the thin card alone; a clamp on indirect light) have the oracle's film bits.
 * Per-path radiance equals the oracle's within 1e-4 (reported bit-exact share).
@@ -50,6 +52,33 @@ def test_e5_has_the_pinned_hash(rtg, pins):
     g = s.film()
     g.render_noalloc(0, 4)
     assert rtg.fnv1a(g.resolve()) == pins["film_hashes"]["e5_hdri_4spp"]
+
+
+def test_e5_under_the_classic_sky_has_the_pinned_hash(rtg, pins):
+    from repackshot_b200 import scenes
+    f = rtg.Scene(scenes.to_rsb(scenes.e5_scene(sky=True))).film()
+    f.render(0, 4)
+    assert rtg.fnv1a(f.resolve()) == pins["film_hashes"]["e5_sky_4spp"]
+
+
+def sky(**changes):
+    from repackshot_b200 import scenes
+    s = scenes.e5_scene(sky=True)
+    for k, v in changes.items():
+        setattr(s, k, v)
+    return s
+
+
+SKIES = {"low sun, hazy": dict(sun_elevation_deg=5.0, sky_turbidity=8.0), "high sun, clear": dict(sun_elevation_deg=80.0,
+                                                                                                   sky_turbidity=1.0),
+         "below the horizon, clamped": dict(sun_elevation_deg=-10.0, sun_azimuth_deg=200.0, env_strength=2.0),
+         "sky as background image": dict(background_mode=3)}
+
+
+@pytest.mark.parametrize("name", list(SKIES))
+def test_skies_have_the_oracle_bits(rtg, oracle_lib, name):
+    from repackshot_b200 import scenes
+    assert bits_equal_oracle(rtg, oracle_lib, scenes.to_rsb(sky(**SKIES[name])))
 
 
 def variants():

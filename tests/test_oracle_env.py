@@ -6,7 +6,8 @@ and hdr.rs (rgbe_pixels_round_trip_exactly, files_round_trip_through_the_writer,
 flat_and_old_rle_scanlines_and_bottom_up_files_read, bad_files_fail_cleanly), restated with the
 same inputs and tolerances; and the E5 scene (clear glass, coat, anisotropy, a thin glass card, a
 cut-out card, an HDRI over a background image), whose file is the reference's fixture byte for
-byte and whose 4-sample film has the reference's pinned FNV-1a hash (render.rs:1086-1107).
+byte and whose 4-sample film has the reference's pinned FNV-1a hash (render.rs:1086-1107), and
+the same scene under the classic sky with a sun, also pinned.
 """
 import hashlib
 import struct
@@ -131,6 +132,19 @@ def test_e5_at_four_samples_has_the_pinned_hash(oracle_lib, e5_rsb, pins):
     s = oracle_lib.OracleScene(e5_rsb)
     rgb, w, _, _, _ = s.render_film(0, 4, tile=32, threads=4)
     assert oracle_lib.fnv1a(oracle_lib.resolve(rgb, w)) == pins["film_hashes"]["e5_hdri_4spp"]
+
+
+def test_e5_under_the_classic_sky_has_the_pinned_hash(oracle_lib, pins):
+    s = oracle_lib.OracleScene(scenes.to_rsb(scenes.e5_scene(sky=True)))
+    rgb, w, _, _, _ = s.render_film(0, 4, tile=32, threads=4)
+    assert oracle_lib.fnv1a(oracle_lib.resolve(rgb, w)) == pins["film_hashes"]["e5_sky_4spp"]
+
+
+def test_the_physical_sky_is_refused(oracle_lib):
+    s = scenes.e5_scene(sky=True)
+    s.sky_model = 0
+    with pytest.raises(ValueError, match="physical sky"):
+        oracle_lib.OracleScene(scenes.to_rsb(s))
 
 
 def test_bad_bitmap_indices_are_refused(oracle_lib):
