@@ -55,6 +55,9 @@ def lib():
             "orc_light_crossed": (None, [u32, v, ctypes.c_float, v]),
             "orc_bitmap": (u32, [u32, u32, u32, ctypes.c_char_p, u32, v, v, u32, v, v]),
             "orc_dist2d": (u32, [u32, u32, v, u32, v, v]),
+            "orc_filter_offset": (None, [u32, v, u32, v]),
+            "orc_blackman_harris_table": (None, [v]),
+            "orc_edge_mask": (None, [u32, v]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -162,6 +165,12 @@ class OracleScene:
         lib().orc_light_crossed(self.handle, _p(r), -1.0 if bsdf_pdf is None else float(bsdf_pdf), _p(out))
         return out
 
+    def edge_mask(self):
+        """One byte per pixel: 1 on the pixels that take the edge samples."""
+        out = np.zeros((self.height, self.width), np.uint8)
+        lib().orc_edge_mask(self.handle, _p(out))
+        return out
+
     def occluded(self, rays):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
         out = np.zeros(len(rays), np.uint8)
@@ -190,6 +199,19 @@ def dist2d(w, h, weights, samples):
     out = np.zeros((len(s), 4), np.float32)
     if lib().orc_dist2d(w, h, _p(wts), len(s), _p(s), _p(out)):
         return None
+    return out
+
+
+def filter_offset(filter_kind, us):
+    u = np.ascontiguousarray(us, np.float32)
+    out = np.zeros_like(u)
+    lib().orc_filter_offset(filter_kind, _p(u), len(u), _p(out))
+    return out
+
+
+def blackman_harris_table():
+    out = np.zeros(256, np.float32)
+    lib().orc_blackman_harris_table(_p(out))
     return out
 
 

@@ -398,9 +398,48 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
     alpha_out = alpha;
 }
 
+// The inverse CDF of the Blackman-Harris window (F. J. Harris, Proc. IEEE 66, 1978: a0 - a1 cos 2pi t
+// + a2 cos 4pi t - a3 cos 6pi t) three pixels wide, at the 256 points u = q(i / 255), q(s) = 2 s^2
+// below one half and 1 - 2 (1 - s)^2 above: each by 100 bisections of the window's integral in
+// f64, rounded to f32 (pixel_filter.rs:56-95 and the generator of its table test).
+static const float* blackman_harris_table() {
+    static float table[256];
+    static bool ready = false;
+    if (!ready) {
+        const double a0 = 0.35875, a1 = 0.48829, a2 = 0.14128, a3 = 0.01168, pi = 3.14159265358979323846, r = 1.5;
+        auto cdf = [&](double x) {
+            double t = (x + r) / (2.0 * r);
+            t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+            return (a0 * t - a1 * std::sin(2.0 * pi * t) / (2.0 * pi) + a2 * std::sin(4.0 * pi * t) / (4.0 * pi) -
+                    a3 * std::sin(6.0 * pi * t) / (6.0 * pi)) /
+                   a0;
+        };
+        for (int i = 0; i < 256; ++i) {
+            double sq = (double)i / 255.0;
+            double u = sq < 0.5 ? 2.0 * sq * sq : 1.0 - 2.0 * (1.0 - sq) * (1.0 - sq);
+            double a = -r, b = r;
+            for (int k = 0; k < 100; ++k) {
+                double m = 0.5 * (a + b);
+                if (cdf(m) < u) a = m;
+                else b = m;
+            }
+            table[i] = (float)(0.5 * (a + b));
+        }
+        ready = true;
+    }
+    return table;
+}
 static float filter_offset(uint32_t filter, float u) {  // pixel_filter.rs:103
     if (filter == 1) return 0.5f;
     if (filter == 2) return 0.5f + (u < 0.5f ? std::sqrt(2.0f * u) - 1.0f : 1.0f - std::sqrt(2.0f - 2.0f * u));
+    if (filter == 3) {  // pixel_filter.rs:125: the table interpolated at s = q^-1(u)
+        const float* t = blackman_harris_table();
+        float s = u < 0.5f ? std::sqrt(0.5f * u) : 1.0f - std::sqrt(0.5f - 0.5f * u);
+        float f = rclamp(s * 255.0f, 0.0f, 255.0f);
+        size_t i = (size_t)f < 254 ? (size_t)f : 254;
+        float w = f - (float)i;
+        return 0.5f + (t[i] + (t[i + 1] - t[i]) * w);
+    }
     return u;
 }
 
@@ -426,6 +465,62 @@ static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, ui
     radiance(scene, prep, sampler, ray, rclamp(u, 0.0f, 1.0f), rclamp(v, 0.0f, 1.0f), c, alpha, st);
 }
 
+// The exact passes of a centre ray (passes.rs:168) that the edge mask compares: part and
+// material ids (instance or material + 1, FLOOR_ID for the floor, 0 for the background) and the
+// depth along the view axis.
+struct Exact { uint32_t part = 0, material = 0; float depth = F_INF; };
+constexpr uint32_t FLOOR_ID = 0xffffffffu;
+// render.rs:503 centre_ray and integrator/mod.rs:911 first_hit, as Exact::of reads them.
+static Exact centre_exact(const Scene& scene, const Prepared& prep, uint32_t x, uint32_t y) {
+    uint32_t width = scene.render.width ? scene.render.width : 1, height = scene.render.height ? scene.render.height : 1;
+    float aspect = (float)width / (float)height;
+    Ray ray = scene.camera.generate_ray(aspect, ((float)x + 0.5f) / (float)width, ((float)y + 0.5f) / (float)height, 0.0f, 0.0f);
+    RayHit hit;
+    bool got = scene.geometry.trace(ray, true, hit, nullptr);
+    float t_geometry = got ? hit.t : F_INF;
+    float t_floor = prep.floor_t(ray, true);
+    float t_nearest = rmin(t_geometry, t_floor);
+    Exact e;
+    if (t_nearest == F_INF || prep.lights.camera_sees_panel(ray, t_nearest)) return e;
+    float t;
+    if (t_floor < t_geometry) {
+        e.part = e.material = FLOOR_ID;
+        t = t_floor;
+    } else {
+        Hit d;
+        if (!scene.geometry.hit_details(ray, hit, d)) return e;
+        e.part = d.instance + 1;
+        uint32_t m = scene.geometry.instances[d.instance].material_id;
+        e.material = m < scene.materials.size() ? m + 1 : 0;
+        t = d.t;
+    }
+    Vec3 forward, right, upv;
+    scene.camera.basis(forward, right, upv);
+    e.depth = t * dot(ray.dir, forward) + dot(ray.origin - scene.camera.position, forward);
+    return e;
+}
+// EdgeMask::of (pixel_filter.rs:175) for the whole image (the same for any tile cut): a pixel is
+// an edge when one of its neighbours inside the image sees another part, another material or a
+// depth more than 2 % away through its centre.
+static std::vector<uint8_t> edge_mask(const Scene& scene, const Prepared& prep) {
+    uint32_t w = scene.render.width, h = scene.render.height;
+    std::vector<Exact> c((size_t)w * h);
+    for (uint32_t y = 0; y < h; ++y)
+        for (uint32_t x = 0; x < w; ++x) c[(size_t)y * w + x] = centre_exact(scene, prep, x, y);
+    auto differs = [](const Exact& a, const Exact& b) {
+        return a.part != b.part || a.material != b.material || std::fabs(a.depth - b.depth) > 0.02f * rmin(a.depth, b.depth);
+    };
+    std::vector<uint8_t> edge((size_t)w * h, 0);
+    for (uint32_t y = 0; y < h; ++y)
+        for (uint32_t x = 0; x < w; ++x) {
+            bool is = false;
+            for (uint32_t ny = y ? y - 1 : 0; ny < std::min(y + 2, h); ++ny)
+                for (uint32_t nx = x ? x - 1 : 0; nx < std::min(x + 2, w); ++nx) is |= differs(c[(size_t)y * w + x], c[(size_t)ny * w + nx]);
+            edge[(size_t)y * w + x] = is ? 1 : 0;
+        }
+    return edge;
+}
+
 struct Film {
     uint32_t ox, oy, w, h;
     std::vector<float> rgb, weight, alpha, lum2;
@@ -444,23 +539,39 @@ struct Film {
     }
 };
 
-// render_tile_traced (render.rs:388) into `film`, one sample index, no edge pixels.
-static void render_tile(const Scene& scene, const Prepared& prep, uint32_t tx, uint32_t ty, uint32_t tw, uint32_t th,
-                        uint32_t index, Film& film, PathStats& st) {
+// render_tile_traced (render.rs:388) into `film`, one sample index. `edges` (one byte per image
+// pixel, or empty): an edge pixel renders k = edge_supersample samples, indices index k .. index k +
+// k - 1, and splats their mean (render.rs:477).
+static void render_tile(const Scene& scene, const Prepared& prep, const std::vector<uint8_t>& edges, uint32_t tx, uint32_t ty,
+                        uint32_t tw, uint32_t th, uint32_t index, Film& film, PathStats& st) {
     uint32_t x_end = std::min<uint64_t>((uint64_t)tx + tw, scene.render.width);
     uint32_t y_end = std::min<uint64_t>((uint64_t)ty + th, scene.render.height);
+    const uint32_t k = scene.render.edge_supersample < 1 ? 1 : (scene.render.edge_supersample > 16 ? 16 : scene.render.edge_supersample);
     for (uint32_t y = ty; y < y_end; ++y)
         for (uint32_t x = tx; x < x_end; ++x) {
             Rgb c;
             float a;
-            shade_pixel(scene, prep, x, y, index, c, a, st);
-            film.splat(x, y, c * WHITE, a);
+            if (k <= 1 || edges.empty() || !edges[(size_t)y * scene.render.width + x]) {
+                shade_pixel(scene, prep, x, y, index, c, a, st);
+                film.splat(x, y, c * WHITE, a);
+                continue;
+            }
+            Rgb sum = BLACK;
+            float coverage = 0.0f;
+            for (uint32_t j = 0; j < k; ++j) {
+                shade_pixel(scene, prep, x, y, index * k + j, c, a, st);
+                sum = sum + c * WHITE;
+                coverage += a;
+            }
+            float inv = 1.0f / (float)k;
+            film.splat(x, y, sum * inv, coverage * inv);
         }
 }
 
 struct Loaded {
     Scene scene;
     Prepared prep;
+    std::vector<uint8_t> edges;  // the edge mask when edge_supersample > 1, else empty
     std::unique_ptr<Geometry> merged;  // statistics only (see PathStats)
 };
 
@@ -518,6 +629,7 @@ uint32_t orc_scene_load(const uint8_t* bytes, uint32_t len) {
         return 0;
     }
     l->prep = Prepared::make(l->scene);
+    if (l->scene.render.edge_supersample > 1) l->edges = edge_mask(l->scene, l->prep);
     std::lock_guard<std::mutex> lk(g_mu);
     g_error.clear();
     for (size_t i = 0; i < g_scenes.size(); ++i)
@@ -580,7 +692,7 @@ uint64_t orc_render_film(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint3
             uint32_t tx = tiles[2 * t], ty = tiles[2 * t + 1];
             uint32_t tw = std::min(tile, w - tx), th = std::min(tile, hgt - ty);
             Film film(x0 + tx, y0 + ty, tw, th);
-            for (uint32_t s = 0; s < count; ++s) render_tile(l->scene, l->prep, x0 + tx, y0 + ty, tw, th, first + s, film, st);
+            for (uint32_t s = 0; s < count; ++s) render_tile(l->scene, l->prep, l->edges, x0 + tx, y0 + ty, tw, th, first + s, film, st);
             for (uint32_t yy = 0; yy < th; ++yy)
                 for (uint32_t xx = 0; xx < tw; ++xx) {
                     size_t i = (size_t)yy * tw + xx, o = (size_t)(ty + yy) * w + (tx + xx);
@@ -632,7 +744,7 @@ uint64_t orc_render_tile(uint32_t h, uint32_t x, uint32_t y, uint32_t w, uint32_
     if (!l || !out_rgb) return 0;
     Film film(x, y, w, hgt);
     PathStats st;
-    render_tile(l->scene, l->prep, x, y, w, hgt, sample, film, st);
+    render_tile(l->scene, l->prep, l->edges, x, y, w, hgt, sample, film, st);
     for (size_t i = 0; i < (size_t)w * hgt; ++i) {
         float wt = film.weight[i];
         float inv = wt > 0.0f ? 1.0f / wt : 0.0f;
@@ -783,6 +895,21 @@ uint32_t orc_dist2d(uint32_t w, uint32_t h, const float* weights, uint32_t n, co
         out[4 * i] = u; out[4 * i + 1] = v; out[4 * i + 2] = p; out[4 * i + 3] = d.pdf(u, v);
     }
     return 0;
+}
+
+// The pixel filters (pixel_filter.rs:103): where n uniform numbers put a sample on one axis; and
+// the Blackman-Harris table itself (256 floats).
+void orc_filter_offset(uint32_t filter, const float* u, uint32_t n, float* out) {
+    for (uint32_t i = 0; i < n; ++i) out[i] = filter_offset(filter, u[i]);
+}
+void orc_blackman_harris_table(float* out256) { std::memcpy(out256, blackman_harris_table(), 256 * sizeof(float)); }
+// The edge mask of a scene (one byte per pixel; all zero without edge samples).
+void orc_edge_mask(uint32_t h, uint8_t* out) {
+    Loaded* l = get(h);
+    if (!l) return;
+    size_t n = (size_t)l->scene.render.width * l->scene.render.height;
+    if (l->edges.empty()) std::memset(out, 0, n);
+    else std::memcpy(out, l->edges.data(), n);
 }
 
 // Known-answer helpers: Pcg32, mix64, Sobol points, owen-scrambled sampler values, fmath.

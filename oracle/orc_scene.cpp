@@ -233,8 +233,7 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             if (s.width < 1 || s.width > 16384 || s.height < 1 || s.height > 16384)
                 return r.invalid("width and height must be between 1 and 16384");
             if (s.max_seconds < 0.0f || s.clamp_indirect < 0.0f) return r.invalid("max_seconds and clamp_indirect must not be negative");
-            if (s.edge_supersample > 1) { error = "unsupported: edge supersampling"; return false; }
-            if (s.pixel_filter == 3) { error = "unsupported: Blackman-Harris pixel filter"; return false; }
+
         } else {
             static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "SECT", "GLAS",
                                                  "WETP", "WETF", "WTP2", "WETG", "NEST", "IESP"};
@@ -709,6 +708,17 @@ Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, con
         sum = sum + light.radiance * (m * w);
     }
     return sum;
+}
+bool Lights::camera_sees_panel(const Ray& ray, float t_max) const {
+    for (const AreaLight& a : areas) {
+        float t, cos;
+        if (a.camera && a.intersect(ray, t_max, t, cos)) return true;
+    }
+    for (const SphereLight& l : spheres) {
+        float t;
+        if (l.camera && l.intersect(ray, t_max, t) && l.mask(ray.origin) > 0.0f) return true;
+    }
+    return false;
 }
 Rgb Lights::escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from) const {  // light.rs:1502
     Rgb sum = env.radiance(dir);

@@ -210,6 +210,9 @@ struct Lights {
     void pick_at(const Selection& s, float u, size_t& idx, float& rest, float& pmf_out) const;
     bool sample_selected(const Selection& s, float u_select, float u0, float u1, LightSample& out) const;
     Rgb crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, const Selection* from, float offset) const;
+    // light.rs:1490: a camera ray meets a light it sees (an area light flagged camera, or a sphere
+    // flagged camera lit towards the ray's origin) before t_max.
+    bool camera_sees_panel(const Ray& ray, float t_max) const;
     Rgb escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from) const;
 };
 inline float power_heuristic(float pa, float pb) {  // light.rs:129

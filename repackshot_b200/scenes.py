@@ -131,7 +131,8 @@ class Scene:
     tonemap: int = 1
     max_depth: int = 8
     clamp_indirect: float = 0.0
-    pixel_filter: int = 0
+    pixel_filter: int = 0  # 0 standard, 1 none, 2 tent, 3 Blackman-Harris
+    edge_supersample: int = 1  # samples per sample index of an edge pixel
 
 
 def _sec(tag: bytes, payload: bytes) -> bytes:
@@ -178,7 +179,7 @@ def to_rsb(s: Scene, meshes: bool = True) -> bytes:
     out.append(_sec(b"FLOR", _u(s.floor_mode) + _f(s.floor_z, *s.floor_color)))
     out.append(_sec(b"RNDR", _u(s.width, s.height, s.max_samples, s.seed) + _f(s.max_seconds, s.exposure_ev) +
                     _u(s.tonemap, s.max_depth) + _f(s.clamp_indirect) + _u(0, 0, 0) + _f(0.0, 1.0) +
-                    _u(s.pixel_filter, 1)))
+                    _u(s.pixel_filter, s.edge_supersample)))
     return b"".join(out)
 
 
@@ -354,6 +355,14 @@ def e5_scene(sky: bool = False) -> Scene:
         s.sun_azimuth_deg, s.sun_elevation_deg = -60.0, 35.0
         s.lights = [Light(kind=LIGHT_SUN, position=(0.0, 0.0, 1000.0), direction=(-0.41, 0.71, -0.574), up=(0.0, 1.0, 0.0),
                           size_x=500.0, size_y=500.0, color=(1.0, 0.91, 0.83), power=3.0, angle_deg=0.545, flags=3)]
+    return s
+
+
+def e11_scene() -> Scene:
+    """example.rs:1440 e11_scene: the example with the Blackman-Harris pixel filter and two samples
+    per sample index on its edges."""
+    s = example_scene()
+    s.pixel_filter, s.edge_supersample = 3, 2
     return s
 
 

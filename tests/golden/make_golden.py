@@ -8,7 +8,9 @@ its path tracer, read from the reference's own source tree (run where it is chec
   little-endian bytes of their u16 values and f32 bit patterns;
 * SHA-256 of the example scene file (tests/fixtures/example.rsb);
 * the FNV-1a film hashes of the E5 scene with its HDRI and with the classic sky (render.rs:1106-1109)
-  and SHA-256 of the HDRI scene's file (tests/fixtures/e5.rsb).
+  and SHA-256 of the HDRI scene's file (tests/fixtures/e5.rsb);
+* the E11 film hash (render.rs:1250) and SHA-256 of the Blackman-Harris inverse-CDF table
+  (pixel_filter.rs:64, 256 little-endian f32).
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -42,6 +44,7 @@ def main():
         "tile_small_sphere_48_144_s3": pinned(render, "PINNED_SMALL_SPHERE"),
         "e5_hdri_4spp": pinned(render, "PINNED_E5_HDRI_4SPP"),
         "e5_sky_4spp": pinned(render, "PINNED_E5_SKY_4SPP"),
+        "e11_edges_4spp": pinned(render, "PINNED_E11_EDGES_4SPP"),
     }
     block = rng[rng.index("fn matches_the_reference_implementation"):]
     block = block[:block.index("]")]
@@ -59,6 +62,11 @@ def main():
         else:
             raw = struct.pack("<%df" % len(vals), *[float(v) for v in vals])
         tables[name] = {"count": len(vals), "sha256": hashlib.sha256(raw).hexdigest()}
+    pf = (CORE / "pixel_filter.rs").read_text()
+    body = pf[pf.index("pub const BLACKMAN_HARRIS_INV_CDF"):]
+    body = body[body.index("= [") + 3:body.index("];")]
+    bh = [float(v) for v in re.findall(r"-?\d+\.\d+(?:e-?\d+)?", body)]
+    bh_raw = struct.pack("<%df" % len(bh), *bh)
     example = (REF / "tests" / "fixtures" / "example.rsb").read_bytes()
     e5 = (REF / "tests" / "fixtures" / "e5.rsb").read_bytes()
     out = {
@@ -70,6 +78,7 @@ def main():
         "energy_tables": tables,
         "example_rsb": {"bytes": len(example), "sha256": hashlib.sha256(example).hexdigest()},
         "e5_rsb": {"bytes": len(e5), "sha256": hashlib.sha256(e5).hexdigest()},
+        "blackman_harris_inv_cdf": {"count": len(bh), "sha256": hashlib.sha256(bh_raw).hexdigest()},
     }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(OUT)
