@@ -103,7 +103,8 @@ uint32_t rtg_render_progressive(uint32_t scene, uint32_t film, uint32_t first_sa
  * paths, so the film is rendered in bands of rows and waves of samples that fit; any film of a
  * loadable scene (images are at most 16384 pixels wide) is accepted. A row wider than
  * RTG_NOALLOC_MAX_PATHS pixels would not fit and is refused with RTG_STATUS_BAD_FILM and a
- * message.
+ * message. A scene with edge samples (RNDR edge_supersample above 1) is refused with
+ * RTG_STATUS_BAD_SCENE: its edge mask would need device memory.
  *
  * The first call on each device does the set-up: it looks up the array's address on the
  * current device (cudaGetSymbolAddress), which may load the library's device code there. Make

@@ -115,6 +115,8 @@ struct SceneDev {
     // render settings
     uint32_t width, height, seed, max_depth, pixel_filter;
     float clamp_indirect;
+    const float* filter_table;  // the Blackman-Harris inverse CDF, 256 points (pixel filter 3)
+    uint32_t edge_k;            // samples per sample index of an edge pixel (1: no edge samples)
     uint32_t background;  // 0 environment, 1 colour, 2 transparent, 3 background image
     float background_color[3];
     // The background image fitted to the frame (integrator/mod.rs:187): linear RGB texels.

@@ -31,6 +31,7 @@ std::string g_error;
 bool g_device_ready = false;
 void* g_energy_dev = nullptr;
 EnergyTables g_energy{};
+const float* g_filter_table = nullptr;  // the Blackman-Harris inverse CDF on the device
 int g_sms = 148;
 
 void cuda_fail(cudaError_t e, const char* what) {
@@ -70,6 +71,9 @@ struct Scene {
     uint32_t tonemap = 1, max_samples = 0;
     std::vector<uint32_t> light_source;  // scene light of each prepared light (areas, suns, spheres)
     DevBuf adjoint_mem;
+    // edge samples (E11): the image's edge mask, its centre-ray scratch and an edge-pixel list
+    DevBuf edge_mem;
+    bool edges_ready = false;
     cudaStream_t stream = nullptr;
     // path buffers
     PathBuffers P{};
@@ -94,6 +98,7 @@ struct Scene {
         shading.release();
         path_mem.release();
         adjoint_mem.release();
+        edge_mem.release();
         if (wt) {
             for (int i = 0; i < WaveTiming::MAX_EVENTS; ++i) cudaEventDestroy(wt->ev[i]);
             delete wt;
@@ -150,7 +155,7 @@ uint32_t device_init() {
     RTG_CHECK(cudaGetLastError());
     const EnergyData& E = energy_data();
     size_t n16 = E.albedo.size() + E.schlick.size() + E.clear_in.size() + E.clear_out.size();
-    size_t bytes = n16 * 2 + 64 * 4;
+    size_t bytes = n16 * 2 + 64 * 4 + 256 * 4;
     RTG_CHECK(cudaMalloc(&g_energy_dev, bytes));
     std::vector<uint8_t> host(bytes);
     uint8_t* p = host.data();
@@ -161,6 +166,7 @@ uint32_t device_init() {
     put(E.clear_out.data(), E.clear_out.size() * 2);
     put(E.albedo_avg.data(), 32 * 4);
     put(E.schlick_avg.data(), 32 * 4);
+    put(blackman_harris_table(), 256 * 4);
     RTG_CHECK(cudaMemcpy(g_energy_dev, host.data(), bytes, cudaMemcpyHostToDevice));
     const uint8_t* d = (const uint8_t*)g_energy_dev;
     g_energy.albedo = (const uint16_t*)d;
@@ -169,6 +175,7 @@ uint32_t device_init() {
     g_energy.clear_out = g_energy.clear_in + E.clear_in.size();
     g_energy.albedo_avg = (const float*)(g_energy.clear_out + E.clear_out.size());
     g_energy.schlick_avg = g_energy.albedo_avg + 32;
+    g_filter_table = g_energy.schlick_avg + 32;
     RTG_CHECK(cudaDeviceSynchronize());
     g_device_ready = true;
     return RTG_STATUS_OK;
@@ -241,6 +248,7 @@ SceneDev compose(const SceneDev& constants, const SceneDev& geom, const SceneDev
     S.tlas_root = geom.tlas_root; S.stack_need = geom.stack_need;
     S.instances = shade.instances; S.materials = shade.materials; S.bsdfs = shade.bsdfs; S.plate = shade.plate;
     S.energy = g_energy;
+    S.filter_table = g_filter_table;
     return S;
 }
 
@@ -353,6 +361,38 @@ uint32_t finish(Scene& sc, uint64_t* rays_out) {
 
 // Renders samples [first, first + count) of the image rectangle (x, y, w, h) (clipped to the
 // image) into `film`, every pixel's samples added in index order.
+// The image's edge mask (built once per scene state, pixel_filter.rs:175) and the edge pixels of
+// the rectangle (x, y, w, h): their packed list on the device and their count.
+uint32_t edge_pixels(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, const uint8_t*& mask, const uint32_t*& list,
+                     uint32_t& count) {
+    const size_t npix = (size_t)sc.width * sc.height;
+    const size_t mask_bytes = (npix + 15) & ~(size_t)15;
+    const size_t need = mask_bytes + npix * sizeof(uint4) + npix * 4 + 16;
+    if (sc.edge_mem.bytes < need) {
+        sc.edge_mem.release();
+        RTG_CHECK(cudaMalloc(&sc.edge_mem.p, need));
+        sc.edge_mem.bytes = need;
+        sc.edges_ready = false;
+    }
+    uint8_t* base = (uint8_t*)sc.edge_mem.p;
+    uint8_t* m = base;
+    uint4* exact = (uint4*)(base + mask_bytes);
+    uint32_t* l = (uint32_t*)(base + mask_bytes + npix * sizeof(uint4));
+    uint32_t* c = l + npix;
+    if (!sc.edges_ready) {
+        RTG_CHECK(launch_edge_mask(sc.S, sc.d_lights, exact, m, sc.stream, grid_for(npix, 128)));
+        sc.launches += 2;
+        sc.edges_ready = true;
+    }
+    RTG_CHECK(launch_edge_list(m, sc.width, x, y, w, h, l, c, sc.stream, grid_for((uint64_t)w * h, 256)));
+    sc.launches += 1;
+    RTG_CHECK(cudaMemcpyAsync(&count, c, 4, cudaMemcpyDeviceToHost, sc.stream));
+    RTG_CHECK(cudaStreamSynchronize(sc.stream));
+    mask = m;
+    list = l;
+    return RTG_STATUS_OK;
+}
+
 uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t first, uint32_t count, const FilmDev& film,
                        uint64_t* rays_out) {
     uint64_t x_end = std::min<uint64_t>((uint64_t)x + w, sc.width), y_end = std::min<uint64_t>((uint64_t)y + h, sc.height);
@@ -370,15 +410,45 @@ uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h
         uint64_t bpix = (uint64_t)cw * bh;
         uint32_t per_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(count, cap / bpix));
         uint32_t need = (uint32_t)(bpix * per_wave);
-        uint32_t st = ensure_capacity(sc, need);
+        // Edge samples (E11): the band's edge pixels splat from edge waves of their own, the
+        // mean of k samples per sample index (render.rs:477); the rectangle waves skip them. The
+        // edge waves take as many edge pixels (k samples each) and sample indices as fit.
+        const uint8_t* mask = nullptr;
+        const uint32_t* elist = nullptr;
+        uint32_t ne = 0, chunk = 0;
+        const uint32_t k = sc.S.edge_k;
+        uint32_t st;
+        if (k > 1 && (st = edge_pixels(sc, x, y + by, cw, bh, mask, elist, ne))) return st;
+        if (ne) {
+            chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ne, cap / k));
+            need = std::max<uint32_t>(need, (uint32_t)((uint64_t)chunk * k));
+        }
+        st = ensure_capacity(sc, need);
         if (st) return st;
         RTG_CHECK(cudaMemsetAsync(sc.P.counters, 0, 16, sc.stream));
         RTG_CHECK(cudaMemsetAsync(sc.P.rays, 0, 16, sc.stream));
         for (uint32_t s = 0; s < count; s += per_wave) {
             uint32_t ns = std::min(per_wave, count - s);
             WaveDesc wd{x, y + by, cw, bh, first + s, (uint32_t)(bpix * ns), nullptr};
+            if (ne) {
+                wd.edge = mask;
+                wd.edge_stride = sc.width;
+            }
             st = run_wave(sc, wd, &film);
             if (st) return st;
+        }
+        for (uint32_t e0 = 0; e0 < ne; e0 += chunk) {
+            const uint32_t en = std::min(chunk, ne - e0);
+            const uint32_t per_edge_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(count, sc.capacity / ((uint64_t)en * k)));
+            for (uint32_t s = 0; s < count; s += per_edge_wave) {
+                const uint32_t ns = std::min(per_edge_wave, count - s);
+                WaveDesc wd{x, y + by, cw, bh, first + s, (uint32_t)((uint64_t)en * k * ns), nullptr};
+                wd.epix = elist + e0;
+                wd.ne = en;
+                wd.ek = k;
+                st = run_wave(sc, wd, &film);
+                if (st) return st;
+            }
         }
         uint64_t r = 0;
         st = finish(sc, &r);
@@ -519,6 +589,7 @@ uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
     }
     sc->shading.release();
     sc->shading = std::move(shading);
+    sc->edges_ready = false;
     sc->S = compose(F.scene, geom, shade);
     sc->d_lights = sc->shading.lights;
     keep_shading(*sc, hs, F);
@@ -597,6 +668,10 @@ uint32_t rtg_render_progressive_noalloc(uint32_t handle, uint32_t film, uint32_t
     Film* f = film_of(film);
     if (!f || f->scene != handle) return RTG_STATUS_BAD_FILM;
     if (rays) *rays = 0;
+    if (sc->S.edge_k > 1) {
+        g_error = "rtg_render_progressive_noalloc: unsupported: edge samples (their mask needs device memory)";
+        return RTG_STATUS_BAD_SCENE;
+    }
     NoallocJob job{&sc->S, sc->d_lights, f->dev, sc->width, sc->height, first_sample, count, sc->stream, g_sms};
     NoallocResult res;
     const char* why = "";
@@ -647,6 +722,7 @@ uint32_t rtg_queue_add(uint32_t queue, const uint8_t* bytes, uint32_t len, uint3
     }
     Flat F;
     if (!flatten_scene(hs, F, err, false)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
+    if (F.scene.edge_k > 1) { g_error = "unsupported in the batched queue: edge samples"; return RTG_STATUS_BAD_SCENE; }
     auto job = std::make_unique<QueueJob>();
     job->constants = F.scene;
     job->shade = F.scene;
@@ -835,6 +911,10 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     if (!target || !loss || !grads) { g_error = "rtg_render_adjoint: null pointer"; return RTG_STATUS_NULL_POINTER; }
     if (sc->S.any_passable) {
         g_error = "rtg_render_adjoint: unsupported: cut-outs and thin walls (their shadow rays are not replayed)";
+        return RTG_STATUS_BAD_SCENE;
+    }
+    if (sc->S.edge_k > 1) {
+        g_error = "rtg_render_adjoint: unsupported: edge samples (the replay takes one sample per index)";
         return RTG_STATUS_BAD_SCENE;
     }
     const FilmDev& F = f->dev;

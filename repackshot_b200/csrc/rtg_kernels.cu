@@ -27,6 +27,14 @@ constexpr uint32_t MAX_CUTOUTS = 64;
 RTG_D uint32_t cutout_dim(uint32_t bounce, uint32_t crossing) { return (1u << 20) + bounce * 64u + (crossing < 63u ? crossing : 63u); }
 
 __device__ __forceinline__ void wave_slot(const WaveDesc& w, uint32_t slot, uint32_t& x, uint32_t& y, uint32_t& index) {
+    if (w.epix) {
+        const uint32_t j = slot % w.ek, r = slot / w.ek, s = r / w.ne, e = r - s * w.ne;
+        const uint32_t packed = w.epix[e];
+        x = packed & 0xffffu;
+        y = packed >> 16;
+        index = (w.first + s) * w.ek + j;  // render.rs:376 sub_sample (wrapping)
+        return;
+    }
     if (w.xys) {
         x = w.xys[3 * slot];
         y = w.xys[3 * slot + 1];
@@ -533,7 +541,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow_walk(SceneDev S, PathB
             if (res.inst >= J.n_instances || !J.instances[res.inst].passable) break;
             HitInfo h;
             uint4 idx;
-            const DevInstance* I;
+            const DevInstance* I = nullptr;
             if (!hit_details(J, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, h, I, idx)) break;
             const uint32_t m = I->material;
             const float opacity = rclamp(J.materials[m].opacity, 0.0f, 1.0f);
@@ -593,8 +601,121 @@ __device__ __forceinline__ void accumulate_pixel(const FilmDev& F, uint32_t x, u
 __global__ void k_accumulate(WaveDesc w, PathBuffers P, FilmDev F) {
     uint32_t npix = w.w * w.h;
     uint32_t ns = w.n / npix;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x)
-        accumulate_pixel(F, w.x0 + p % w.w, w.y0 + p / w.w, P, p, npix, ns);
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        const uint32_t x = w.x0 + p % w.w, y = w.y0 + p / w.w;
+        if (w.edge && w.edge[(size_t)y * w.edge_stride + x]) continue;  // splatted by the edge waves
+        accumulate_pixel(F, x, y, P, p, npix, ns);
+    }
+}
+
+// An edge wave: per edge pixel and sample index, the mean of its k samples (summed in order,
+// times 1 / k), splatted once (render.rs:477-488), sample indices in order.
+__global__ void k_accumulate_edges(WaveDesc w, PathBuffers P, FilmDev F) {
+    const uint32_t k = w.ek, ns = w.n / (w.ne * k);
+    const float inv = 1.0f / (float)k;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < w.ne; e += gridDim.x * blockDim.x) {
+        const uint32_t x = w.epix[e] & 0xffffu, y = w.epix[e] >> 16;
+        if (x < F.ox || y < F.oy || x - F.ox >= F.w || y - F.oy >= F.h) continue;
+        const size_t fi = (size_t)(y - F.oy) * F.w + (x - F.ox);
+        float r = F.rgb[3 * fi], g = F.rgb[3 * fi + 1], b = F.rgb[3 * fi + 2];
+        float wt = F.weight[fi], al = F.alpha[fi], l2 = F.lum2[fi];
+        for (uint32_t s = 0; s < ns; ++s) {
+            float sr = 0.0f, sg = 0.0f, sb = 0.0f, cov = 0.0f;
+            for (uint32_t j = 0; j < k; ++j) {
+                const uint32_t slot = (s * w.ne + e) * k + j;
+                const float4 c = P.sum[slot];
+                sr = sr + c.x; sg = sg + c.y; sb = sb + c.z;
+                cov = cov + P.thr[slot].w;
+            }
+            const Rgb m = rgb(sr * inv, sg * inv, sb * inv);
+            r = r + m.r; g = g + m.g; b = b + m.b;
+            wt = wt + 1.0f;
+            al = al + cov * inv;
+            const float l = luminance(m);
+            l2 = l2 + l * l;
+        }
+        F.rgb[3 * fi] = r; F.rgb[3 * fi + 1] = g; F.rgb[3 * fi + 2] = b;
+        F.weight[fi] = wt; F.alpha[fi] = al; F.lum2[fi] = l2;
+    }
+}
+
+// ---- edge mask (pixel_filter.rs:149-268) -------------------------------------------------------------
+// What the centre ray of a pixel meets first (render.rs:503 centre_ray, integrator/mod.rs:911
+// first_hit, passes.rs:168 Exact::of): x = part (instance + 1, 0xffffffff the floor, 0 the
+// background), y = material (+ 1, the same codes), z = depth along the view axis (bits).
+__global__ void __launch_bounds__(TRACE_THREADS) k_edge_exact(SceneDev S, const LightsDev* __restrict__ Lg, uint4* exact) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const LightsDev& L = *Lg;
+    const uint32_t n = S.width * S.height;
+    uint32_t err = 0;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t x = p % S.width, y = p / S.width;
+        V3 o, d;
+        camera_ray_at(S, ((float)x + 0.5f) / (float)S.width, ((float)y + 0.5f) / (float)S.height, 0.0f, 0.0f, o, d);
+        TraceResult res;
+        const bool got = traverse<false>(S, o, d, 1.0e-3f, f_inf(), true, res, &err, stack);
+        const float t_geometry = got ? res.t : f_inf();
+        float t_floor = f_inf();
+        if (S.floor_mode == 1 && d.z != 0.0f) {
+            const float t = (S.floor_z - o.z) / d.z;
+            if (t > 1.0e-3f && t < f_inf()) t_floor = t;
+        }
+        const float t_nearest = rmin(t_geometry, t_floor);
+        uint4 e = make_uint4(0u, 0u, __float_as_uint(f_inf()), 0u);
+        if (!(t_nearest == f_inf() || camera_sees_panel(L, o, d, t_nearest))) {
+            float t = t_floor;
+            bool ok = true;
+            if (t_floor < t_geometry) {
+                e.x = e.y = 0xffffffffu;
+            } else {
+                HitInfo h;
+                uint4 idx;
+                const DevInstance* I = nullptr;
+                ok = hit_details(S, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, h, I, idx) && I != nullptr;
+                if (ok) {
+                    e.x = res.inst + 1u;
+                    e.y = I->material < S.n_materials ? I->material + 1u : 0u;
+                }
+                t = res.t;
+            }
+            if (ok) {
+                const V3 fwd = ld3(S.cam_fwd);
+                e.z = __float_as_uint(t * dot(d, fwd) + dot(o - ld3(S.cam_pos), fwd));
+            } else {
+                e = make_uint4(0u, 0u, __float_as_uint(f_inf()), 0u);
+            }
+        }
+        exact[p] = e;
+    }
+    (void)err;
+}
+// A pixel is an edge when a neighbour inside the image sees another part, another material, or
+// a depth more than 2 % away (two background pixels never differ).
+__global__ void k_edge_mask(SceneDev S, const uint4* __restrict__ exact, uint8_t* mask) {
+    const uint32_t w = S.width, h = S.height, n = w * h;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t x = p % w, y = p / w;
+        const uint4 c = exact[p];
+        const float cd = __uint_as_float(c.z);
+        bool edge = false;
+        for (uint32_t ny = y ? y - 1 : 0; ny < min(y + 2, h); ++ny)
+            for (uint32_t nx = x ? x - 1 : 0; nx < min(x + 2, w); ++nx) {
+                const uint4 o = exact[ny * w + nx];
+                const float od = __uint_as_float(o.z);
+                edge |= c.x != o.x || c.y != o.y || absf(cd - od) > 0.02f * rmin(cd, od);
+            }
+        mask[p] = edge ? 1 : 0;
+    }
+}
+__global__ void k_edge_list(const uint8_t* __restrict__ mask, uint32_t stride, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                            uint32_t* list, uint32_t* count) {
+    const uint32_t n = w * h;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t x = x0 + p % w, y = y0 + p / w;
+        if (mask[(size_t)y * stride + x]) list[atomicAdd(count, 1u)] = x | (y << 16);
+    }
 }
 
 // A batched wave: every pixel of every segment into its job's film. A job has at most one segment
@@ -705,7 +826,20 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
         cur ^= 1;
     }
     if (batch) k_accumulate_jobs<<<g, 256, 0, st>>>(w, P);
+    else if (film && w.epix) k_accumulate_edges<<<g, 256, 0, st>>>(w, P, *film);
     else if (film) k_accumulate<<<g, 256, 0, st>>>(w, P, *film);
+}
+
+cudaError_t launch_edge_mask(const SceneDev& S, const LightsDev* L, uint4* exact, uint8_t* mask, cudaStream_t st, int grid) {
+    k_edge_exact<<<grid, TRACE_THREADS, 0, st>>>(S, L, exact);
+    k_edge_mask<<<grid, 256, 0, st>>>(S, exact, mask);
+    return cudaGetLastError();
+}
+cudaError_t launch_edge_list(const uint8_t* mask, uint32_t stride, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t* list,
+                             uint32_t* count, cudaStream_t st, int grid) {
+    cudaMemsetAsync(count, 0, 4, st);
+    k_edge_list<<<grid, 256, 0, st>>>(mask, stride, x0, y0, w, h, list, count);
+    return cudaGetLastError();
 }
 
 void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, const PathBuffers& P, uint32_t count, cudaStream_t st,

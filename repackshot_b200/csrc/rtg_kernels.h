@@ -12,6 +12,15 @@ struct JobDev;
 // cut-out a path may pass (at most 64; a pass is no vertex).
 inline uint32_t wave_rounds(const SceneDev& S) { return S.max_depth + 1u + (S.any_cutout ? 64u : 0u); }
 
+// The edge mask of an image (pixel_filter.rs:175, the same for any tile cut): one byte per pixel,
+// 1 where a neighbour's centre ray sees another part, material or depth. `exact` is scratch of
+// w h uint4. Returns the launch status.
+cudaError_t launch_edge_mask(const SceneDev& S, const LightsDev* L, uint4* exact, uint8_t* mask, cudaStream_t st, int grid);
+// The packed (x | y << 16) edge pixels of the rectangle (x0, y0, w, h) of a mask, in any order;
+// their count in *count (device).
+cudaError_t launch_edge_list(const uint8_t* mask, uint32_t stride, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t* list,
+                             uint32_t* count, cudaStream_t st, int grid);
+
 // A segment of a batched wave: samples [first, first + ns) of the full-width rows [y0, y0 + h) of
 // one job's image. Its slots start at slot_begin (sample-major, then row-major pixels); its pixels
 // start at pix_begin in the wave's accumulation order.
@@ -30,6 +39,15 @@ struct WaveDesc {
     const SegDev* segs;
     const JobDev* jobs;
     uint32_t nseg, npix;
+    // An edge wave (render.rs:477, E11) when `epix` is set: the k = `ek` samples of each sample
+    // index of `ne` edge pixels (packed x | y << 16): slot ((s ne) + e) k + j holds sample index
+    // (first + s) k + j of pixel e.
+    const uint32_t* epix;
+    uint32_t ne, ek;
+    // A rectangle wave of a scene with edge samples: the image's edge mask (row stride
+    // `edge_stride`); its pixels splat from the edge waves, not from this one.
+    const uint8_t* edge;
+    uint32_t edge_stride;
 };
 
 // Structure-of-arrays path state of one wave (device pointers).

@@ -219,8 +219,7 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (s.width < 1 || s.width > 16384 || s.height < 1 || s.height > 16384)
                 return r.invalid("width and height must be between 1 and 16384");
             if (s.max_seconds < 0.0f || s.clamp_indirect < 0.0f) return r.invalid("max_seconds and clamp_indirect must not be negative");
-            if (s.edge_supersample > 1) { error = "unsupported: edge supersampling"; return false; }
-            if (s.pixel_filter == 3) { error = "unsupported: Blackman-Harris pixel filter"; return false; }
+
         } else {
             static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "SECT",
                                                  "GLAS", "WETP", "WETF", "WTP2", "WETG", "NEST", "IESP"};
@@ -1014,6 +1013,7 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
     S.width = s.width; S.height = s.height; S.seed = s.seed;
     S.max_depth = s.max_depth == 0 ? 8 : (s.max_depth < 1024 ? s.max_depth : 1024);
     S.pixel_filter = s.pixel_filter;
+    S.edge_k = s.edge_supersample < 1 ? 1 : (s.edge_supersample > 16 ? 16 : s.edge_supersample);  // RenderSettings::edge_factor
     S.clamp_indirect = s.clamp_indirect;
     // The background image fitted to the frame (integrator/mod.rs:317); without one a background
     // image shows the colour.

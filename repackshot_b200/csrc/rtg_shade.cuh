@@ -360,6 +360,21 @@ RTG_D_NI Rgb add_suns(const LightsDev& L, Rgb sum, V3 dir, bool has_pdf, float p
     }
     return sum;
 }
+// Lights::camera_sees_panel (light.rs:1490): a camera ray meets a light it sees (an area light
+// flagged camera, or a sphere flagged camera that lights the ray's origin) before t_max.
+RTG_D bool camera_sees_panel(const LightsDev& L, V3 o, V3 d, float t_max) {
+    for (int i = 0; i < L.n_areas; ++i) {
+        float t, cos;
+        if (L.lights[i].camera && area_intersect(L.lights[i], o, d, 1.0e-3f, t_max, t, cos)) return true;
+    }
+    const int first = L.n_areas + (int)L.n_suns;
+    for (int i = first; i < first + (int)L.n_spheres; ++i) {
+        float t;
+        const LightDev& l = L.lights[i];
+        if (l.camera && sphere_intersect(l, o, d, 1.0e-3f, t_max, t) && sphere_mask(l, o) > 0.0f) return true;
+    }
+    return false;
+}
 // Lights::escaped (light.rs:1502): the ramp environment, then the sun discs.
 RTG_D Rgb escaped(const LightsDev& L, V3 dir, bool has_pdf, float pdf, const Sel& from) {
     Rgb sum = env_radiance(L, dir);
@@ -368,28 +383,36 @@ RTG_D Rgb escaped(const LightsDev& L, V3 dir, bool has_pdf, float pdf, const Sel
 }
 
 // ---- camera (render.rs:79, scene/mod.rs:280) -------------------------------------------------------
-RTG_D float filter_offset(uint32_t filter, float u) {
+// pixel_filter.rs:103: where a uniform number puts a camera sample on one axis, in pixels from
+// the pixel's side: the standard box (u), none (the centre), the tent, or Blackman-Harris (its
+// tabulated inverse CDF, linear between the points s = q^-1(u)).
+RTG_D float filter_offset(const SceneDev& S, float u) {
+    const uint32_t filter = S.pixel_filter;
     if (filter == 1) return 0.5f;
     if (filter == 2) return 0.5f + (u < 0.5f ? sqrt_(2.0f * u) - 1.0f : 1.0f - sqrt_(2.0f - 2.0f * u));
+    if (filter == 3) {
+        const float s = u < 0.5f ? sqrt_(0.5f * u) : 1.0f - sqrt_(0.5f - 0.5f * u);
+        const float f = rclamp(s * 255.0f, 0.0f, 255.0f);
+        const uint32_t i = min((uint32_t)f, 254u);
+        const float t = f - (float)i, a = S.filter_table[i], b = S.filter_table[i + 1];
+        return 0.5f + (a + (b - a) * t);
+    }
     return u;
 }
 // The screen position (u, v) in [0, 1]^2 of a camera sample (render.rs:96).
 RTG_D void screen_of(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, float& su, float& sv) {
     uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
     uint64_t key = pixel_key(S.seed, x, y);
-    float du = filter_offset(S.pixel_filter, sample1(T, key, index, DIM_CAMERA));
-    float dv = filter_offset(S.pixel_filter, sample1(T, key, index, DIM_CAMERA + 1));
+    float du = filter_offset(S, sample1(T, key, index, DIM_CAMERA));
+    float dv = filter_offset(S, sample1(T, key, index, DIM_CAMERA + 1));
     su = rclamp(((float)x + du) / (float)width, 0.0f, 1.0f);
     sv = rclamp(((float)y + dv) / (float)height, 0.0f, 1.0f);
 }
-RTG_D void camera_ray(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, V3& o, V3& d) {
+// Camera::generate_ray (scene/mod.rs:280) through the image point (u, v) and the lens point
+// (lx, ly) of the unit disc.
+RTG_D void camera_ray_at(const SceneDev& S, float u, float v, float lx, float ly, V3& o, V3& d) {
     uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
     float aspect = (float)width / (float)height;
-    uint64_t key = pixel_key(S.seed, x, y);
-    float du = filter_offset(S.pixel_filter, sample1(T, key, index, DIM_CAMERA));
-    float dv = filter_offset(S.pixel_filter, sample1(T, key, index, DIM_CAMERA + 1));
-    float u = ((float)x + du) / (float)width;
-    float v = ((float)y + dv) / (float)height;
     V3 pos = ld3(S.cam_pos), fwd = ld3(S.cam_fwd), right = ld3(S.cam_right), up = ld3(S.cam_up);
     if (S.ortho) {
         float w = S.ortho_width;
@@ -404,11 +427,22 @@ RTG_D void camera_ray(const SceneDev& S, const SobolTable& T, uint32_t x, uint32
     float py = (0.5f - v) * sh;
     V3 dir = normalize(fwd * S.focal_mm + right * px + up * py);
     if (S.lens_radius == 0.0f) { o = pos; d = dir; return; }
-    float lx = 0.0f, ly = 0.0f;
-    if (S.lens_radius > 0.0f) concentric_disk(sample1(T, key, index, DIM_LENS), sample1(T, key, index, DIM_LENS + 1), lx, ly);
     V3 focus = pos + dir * (S.focus_dist / dot(dir, fwd));
     o = pos + (right * lx + up * ly) * S.lens_radius;
     d = normalize(focus - o);
+}
+// The camera sample of (pixel, index): camera_sample_weighted (render.rs:79) with the plain thin lens.
+RTG_D void camera_ray(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, V3& o, V3& d) {
+    uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
+    uint64_t key = pixel_key(S.seed, x, y);
+    float du = filter_offset(S, sample1(T, key, index, DIM_CAMERA));
+    float dv = filter_offset(S, sample1(T, key, index, DIM_CAMERA + 1));
+    float u = ((float)x + du) / (float)width;
+    float v = ((float)y + dv) / (float)height;
+    float lx = 0.0f, ly = 0.0f;
+    if (!S.ortho && S.lens_radius > 0.0f)
+        concentric_disk(sample1(T, key, index, DIM_LENS), sample1(T, key, index, DIM_LENS + 1), lx, ly);
+    camera_ray_at(S, u, v, lx, ly, o, d);
 }
 
 }  // namespace rtg

@@ -29,6 +29,8 @@
 //   ANY WAY OUT OF THE USE OF THIS SOFTWARE, EVEN IF ADVISED OF THE POSSIBILITY OF SUCH DAMAGE.
 #include "rtg_tables.h"
 
+#include <cmath>
+
 namespace rtg {
 
 namespace {
@@ -121,6 +123,37 @@ void build_sobol_table(SobolTable& t) {
         }
     }
     for (int i = 0; i < 64; ++i) t.layout[i] = LAYOUT[i];
+}
+
+// The window of F. J. Harris (Proc. IEEE 66, 1978), a0 - a1 cos 2 pi t + a2 cos 4 pi t - a3 cos 6 pi t,
+// three pixels wide: each point of the table by 100 bisections of its integral in double, rounded
+// to float, as the reference makes its table.
+const float* blackman_harris_table() {
+    static float table[256];
+    static bool ready = false;
+    if (ready) return table;
+    const double a0 = 0.35875, a1 = 0.48829, a2 = 0.14128, a3 = 0.01168, radius = 1.5;
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    auto integral = [&](double x) {  // of the normalised window, from its left end to x pixels
+        double t = (x + radius) / (2.0 * radius);
+        t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+        return (a0 * t - a1 * std::sin(two_pi * t) / two_pi + a2 * std::sin(2.0 * two_pi * t) / (2.0 * two_pi) -
+                a3 * std::sin(3.0 * two_pi * t) / (3.0 * two_pi)) /
+               a0;
+    };
+    for (int i = 0; i < 256; ++i) {
+        const double s = (double)i / 255.0;
+        const double u = s < 0.5 ? 2.0 * s * s : 1.0 - 2.0 * (1.0 - s) * (1.0 - s);
+        double lo = -radius, hi = radius;
+        for (int k = 0; k < 100; ++k) {
+            const double mid = 0.5 * (lo + hi);
+            if (integral(mid) < u) lo = mid;
+            else hi = mid;
+        }
+        table[i] = (float)(0.5 * (lo + hi));
+    }
+    ready = true;
+    return table;
 }
 
 }  // namespace rtg

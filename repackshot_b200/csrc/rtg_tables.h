@@ -18,4 +18,8 @@ struct EnergyData {
 // The tables as built into the library (generated by rtg_energy_gen at build time).
 const EnergyData& energy_data();
 
+// The inverse CDF of the Blackman-Harris pixel filter (pixel_filter.rs:56-138): 256 points, in
+// pixels from the centre, at u = q(i / 255) (q(s) = 2 s^2 below one half, 1 - 2 (1 - s)^2 above).
+const float* blackman_harris_table();
+
 }  // namespace rtg
