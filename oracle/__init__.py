@@ -56,6 +56,7 @@ def lib():
             "orc_bitmap": (u32, [u32, u32, u32, ctypes.c_char_p, u32, v, v, u32, v, v]),
             "orc_dist2d": (u32, [u32, u32, v, u32, v, v]),
             "orc_filter_offset": (None, [u32, v, u32, v]),
+            "orc_ies": (u32, [ctypes.c_char_p, u32, v, u32, v, v, u32, v, v]),
             "orc_blackman_harris_table": (None, [v]),
             "orc_edge_mask": (None, [u32, v]),
         }
@@ -200,6 +201,20 @@ def dist2d(w, h, weights, samples):
     if lib().orc_dist2d(w, h, _p(wts), len(s), _p(s), _p(out)):
         return None
     return out
+
+
+def ies(text, angles=(), dirs=()):
+    """IesProfile::parse: (peak, flux, symmetry, intensities at (gamma, phi) pairs, shapes towards
+    local directions), or raises ValueError with the reason."""
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    gp = np.ascontiguousarray(angles, np.float32).reshape(-1, 2)
+    dd = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+    out3 = np.zeros(3, np.float32)
+    inten = np.zeros(len(gp), np.float32)
+    shp = np.zeros(len(dd), np.float32)
+    if lib().orc_ies(data, len(data), _p(out3), len(gp), _p(gp), _p(inten), len(dd), _p(dd), _p(shp)):
+        raise ValueError(error())
+    return float(out3[0]), float(out3[1]), int(out3[2]), inten, shp
 
 
 def filter_offset(filter_kind, us):

@@ -897,6 +897,27 @@ uint32_t orc_dist2d(uint32_t w, uint32_t h, const float* weights, uint32_t n, co
     return 0;
 }
 
+// IES profiles (ies.rs tests): parses a file into out3 = peak, flux, symmetry (0 rotational,
+// 1 quadrant, 2 bilateral 0-180, 3 bilateral 90-270, 4 full); 0 on success, 1 with the reason in
+// orc_error. Then n intensities at (gamma, phi) degree pairs, and n shares of the peak towards
+// local unit directions (3 floats each).
+uint32_t orc_ies(const uint8_t* bytes, uint32_t len, float* out3, uint32_t n, const float* gamma_phi, float* intensities,
+                 uint32_t m, const float* dirs, float* shapes) {
+    IesProfile p;
+    std::string reason;
+    if (!IesProfile::parse(bytes, len, p, reason)) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_error = reason;
+        return 1;
+    }
+    out3[0] = p.peak;
+    out3[1] = p.flux;
+    out3[2] = (float)p.symmetry;
+    for (uint32_t i = 0; i < n; ++i) intensities[i] = p.intensity(gamma_phi[2 * i], gamma_phi[2 * i + 1]);
+    for (uint32_t i = 0; i < m; ++i) shapes[i] = p.shape(Vec3(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+    return 0;
+}
+
 // The pixel filters (pixel_filter.rs:103): where n uniform numbers put a sample on one axis; and
 // the Blackman-Harris table itself (256 floats).
 void orc_filter_offset(uint32_t filter, const float* u, uint32_t n, float* out) {

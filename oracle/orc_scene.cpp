@@ -181,7 +181,12 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             if (!(r.vec3(l.position) && r.vec3(l.direction) && r.vec3(l.up) && r.f32(l.size_x) && r.f32(l.size_y) &&
                   r.rgb(l.color) && r.f32(l.power) && r.f32(l.spread_deg) && r.f32(l.angle_deg) && r.u32(l.flags)))
                 return false;
-            if (l.kind == 5) { error = "unsupported: IES light"; return false; }
+            if (l.kind == 5) {  // rsb.rs:1006: the profile, an IESP section's position
+                uint32_t profile;
+                if (!r.opt_u32(profile, 0xffffffffu)) return false;
+                l.profile = profile == 0xffffffffu ? -1 : (int)profile;
+                if (profile > 0x7fffffffu) l.profile = -2;  // refers to no section
+            }
             scene.lights.push_back(l);
         } else if (is("ENVR")) {
             if (dup(have_env)) return false;
@@ -197,6 +202,15 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
                   r.opt_f32(e.backplate_rect[3], 1.0f) && r.opt_u32(e.sky_model, 0)))
                 return false;
             if (e.kind == 2 && e.sky_model != 1) { error = "unsupported: physical sky model"; return false; }
+        } else if (is("IESP")) {  // rsb.rs:1018
+            uint32_t n;
+            if (!r.u32(n)) return false;
+            if ((size_t)n > r.remaining()) return r.too_short();
+            IesProfile prof;
+            std::string reason;
+            if (!IesProfile::parse(r.data + r.pos, n, prof, reason)) return r.invalid(reason.c_str());
+            r.pos += n;
+            scene.profiles.push_back(std::move(prof));
         } else if (is("BMAP")) {  // rsb.rs:1057
             uint32_t format, w, h, n;
             if (!(r.u32(format) && r.u32(w) && r.u32(h) && r.u32(n))) return false;
@@ -236,11 +250,16 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
 
         } else {
             static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "SECT", "GLAS",
-                                                 "WETP", "WETF", "WTP2", "WETG", "NEST", "IESP"};
+                                                 "WETP", "WETF", "WTP2", "WETG", "NEST"};
             for (const char* t : feature_tags)
                 if (is(t)) { error = std::string("unsupported: RSB section ") + t; return false; }
         }
     }
+    for (const Light& l : scene.lights)  // rsb.rs:1354
+        if (l.kind == 5 && !(l.profile >= 0 && (size_t)l.profile < scene.profiles.size())) {
+            error = "RSB section LGHT is invalid: an IES light needs a profile that is an IESP section";
+            return false;
+        }
     for (uint32_t map : {scene.environment.hdri_map, scene.environment.backplate_map})
         if (map != NO_BITMAP && map >= scene.bitmaps.size()) {
             error = "RSB section ENVR is invalid: bitmap index does not refer to a BMAP section";
@@ -400,6 +419,12 @@ static Vec3 uniform_cone(float u0, float u1, float one_minus_cos_max) {  // warp
     return Vec3(sin * cp, sin * sp, cos);
 }
 float SphereLight::mask(Vec3 x) const {  // light.rs:368
+    if (ies) {
+        Vec3 d = x - centre;
+        float len2 = length_squared(d);
+        if (!(len2 > 0.0f)) return 0.0f;
+        return ies->shape(ies_frame.to_local(d / std::sqrt(len2)));
+    }
     if (cos_outer < -1.0f) return 1.0f;
     Vec3 d = x - centre;
     float len2 = length_squared(d);
@@ -484,11 +509,17 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
             L.suns.push_back(sun);
             continue;
         }
-        if (light.kind == (uint32_t)LightKind::Point || light.kind == (uint32_t)LightKind::Spot) {  // light.rs:780
+        if (light.kind == (uint32_t)LightKind::Point || light.kind == (uint32_t)LightKind::Spot ||
+            light.kind == (uint32_t)LightKind::Ies) {  // light.rs:780
             SphereLight sp{};
             sp.intensity = color * (power / (4.0f * PI));
-            float radius = 0.5f * std::fabs(light.size_x);
-            sp.radius = finite(radius) ? radius : 0.0f;
+            float r_light = 0.5f * std::fabs(light.size_x);
+            sp.radius = finite(r_light) ? r_light : 0.0f;
+            if (light.kind == (uint32_t)LightKind::Ies) {  // L5: masked by its profile in its own frame
+                sp.ies = &scene.profiles[light.profile];
+                sp.ies_frame = light_frame(light.direction, light.up);
+                if (length_squared(sp.ies_frame.z) < 0.5f) continue;
+            }
             if (light.kind == (uint32_t)LightKind::Spot) {
                 Vec3 axis = normalize(light.direction);
                 if (length_squared(axis) < 0.5f) continue;
@@ -514,7 +545,8 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
             sp.entry = entry;
             sp.base = sp.intensity.luminance();
             sp.near2 = rmax(r_m * r_m, 1.0e-6f);  // MIN_DISTANCE2_M2
-            float toward = 0.05f + 0.95f * sp.mask(centre);
+            // An IES light inside the sphere that bounds the scene sends it its whole flux.
+            float toward = (sp.ies && length(light.position - centre) <= radius) ? sp.ies->efficiency() : 0.05f + 0.95f * sp.mask(centre);
             weights.push_back(flux * toward * reach(light.position, nullptr));
             L.entries.push_back({LightRef::Sphere, (uint32_t)L.spheres.size()});
             L.spheres.push_back(sp);

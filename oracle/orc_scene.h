@@ -24,8 +24,23 @@ struct Camera {  // scene/mod.rs:91
 };
 enum class LightKind : uint32_t { Rect = 0, Disk = 1, Sun = 2, Point = 3, Spot = 4, Ies = 5 };
 constexpr uint32_t LIGHT_FLAG_GLOSSY = 1, LIGHT_FLAG_CAMERA = 2, LIGHT_FLAG_NO_SHADOW = 4;
+// ies.rs: an IES LM-63 type C photometric profile (candela by vertical and horizontal angle)
+struct IesProfile {
+    enum Symmetry : uint32_t { Rotational, Quadrant, Bilateral0, Bilateral90, Full } symmetry = Rotational;
+    std::vector<float> vertical, horizontal, candela;  // degrees; horizontal.size() rows of vertical.size()
+    float peak = 0, flux = 0;
+    // IesProfile::parse (ies.rs:227): false with the reference's reason
+    static bool parse(const uint8_t* bytes, size_t len, IesProfile& out, std::string& reason);
+    float intensity(float gamma, float phi) const;  // candela, degrees
+    float shape(Vec3 local) const;                  // intensity towards a local unit direction over the peak
+    float efficiency() const { return flux / (4.0f * PI * peak); }
+    float fold(float phi) const;
+    float row_integral(size_t row) const;
+    float integrate() const;
+};
 struct Light {
     uint32_t kind = 0;
+    int profile = -1;  // an IES light's profile among the scene's
     Vec3 position, direction{0, 0, -1}, up{0, 1, 0};
     float size_x = 0, size_y = 0;
     Rgb color = WHITE;
@@ -82,6 +97,7 @@ struct RenderSettings {  // scene/mod.rs:911
 struct Scene {
     Camera camera;
     std::vector<Image> bitmaps;
+    std::vector<IesProfile> profiles;
     std::vector<Material> materials;
     Geometry geometry;
     std::vector<Light> lights;
@@ -169,7 +185,9 @@ struct SunLight {  // light.rs:300
     float base;
     bool contains(Vec3 dir) const { return !delta && dot(dir, frame.z) >= cos_max; }
 };
-struct SphereLight {  // light.rs:330 (point lights and spots)
+struct SphereLight {  // light.rs:330 (point lights, spots and IES lights)
+    const IesProfile* ies = nullptr;
+    Frame ies_frame;  // an IES light's axis (z) and horizontal angle 0 (y)
     Vec3 centre;
     float radius;
     Rgb intensity, radiance;

@@ -59,6 +59,7 @@ class Light:
     spread_deg: float = 180.0
     angle_deg: float = 0.0
     flags: int = 3  # glossy | camera
+    profile: int = 0xFFFFFFFF  # kind 5 (IES): its profile among the scene's IESP sections
 
 
 @dataclass
@@ -103,6 +104,7 @@ class Scene:
     instances: List[Instance] = field(default_factory=list)
     lights: List[Light] = field(default_factory=list)
     bitmaps: List[Bitmap] = field(default_factory=list)
+    profiles: List[bytes] = field(default_factory=list)  # IES LM-63 files (IESP sections)
     env_kind: int = 0  # 0 studio, 1 flat, 2 sky, 3 HDRI
     env_floor: float = 0.1
     env_horizon: float = 0.3
@@ -169,7 +171,9 @@ def to_rsb(s: Scene, meshes: bool = True) -> bytes:
         out.append(_sec(b"INST", _u(inst.mesh) + _f(*inst.rows) + _u(inst.material_id, inst.flags)))
     for l in s.lights:
         out.append(_sec(b"LGHT", _u(l.kind) + _f(*l.position, *l.direction, *l.up, l.size_x, l.size_y, *l.color, l.power,
-                                                 l.spread_deg, l.angle_deg) + _u(l.flags)))
+                                                 l.spread_deg, l.angle_deg) + _u(l.flags) + (_u(l.profile) if l.kind == 5 else b"")))
+    for p in s.profiles:
+        out.append(_sec(b"IESP", _u(len(p)) + bytes(p) + bytes((4 - len(p) % 4) % 4)))
     for b in s.bitmaps:
         out.append(_sec(b"BMAP", _u(b.format, b.width, b.height, len(b.data)) + bytes(b.data) + bytes((4 - len(b.data) % 4) % 4)))
     out.append(_sec(b"ENVR", _u(s.env_kind) + _f(s.env_floor, s.env_horizon, s.env_zenith, s.env_strength, s.env_rotation,
@@ -363,6 +367,29 @@ def e11_scene() -> Scene:
     per sample index on its edges."""
     s = example_scene()
     s.pixel_filter, s.edge_supersample = 3, 2
+    return s
+
+
+LIGHT_IES = 5
+
+
+def l5_scene(downlight: bytes, wall_washer: bytes) -> Scene:
+    """example.rs:1453 l5_scene: the example at 160 x 120 lit by its panel at 1 W and two IES
+    lights: a downlight profile on a sphere of 24 mm above and in front of the big sphere, and a
+    wall-washer profile as a warm point on the left, turned about its axis (`up`) so that its
+    horizontal angles do not line up with the world. The two profiles are the files' bytes."""
+    s = example_scene()
+    s.width, s.height = 160, 120
+    s.lights[0].power = 1.0
+    above, washer = (0.0, -250.0, 760.0), (-620.0, -180.0, 380.0)
+    to = lambda a, b: tuple(float(v) for v in _normalize32([f32(b[i]) - f32(a[i]) for i in range(3)]))
+    s.profiles = [bytes(downlight), bytes(wall_washer)]
+    s.lights.append(Light(kind=LIGHT_IES, position=above, direction=to(above, (0.0, 0.0, 100.0)), up=(0.0, 1.0, 0.0),
+                          size_x=24.0, size_y=24.0, color=(1.0, 1.0, 1.0), power=18.0, spread_deg=180.0, angle_deg=0.0,
+                          flags=3, profile=0))
+    s.lights.append(Light(kind=LIGHT_IES, position=washer, direction=to(washer, (-330.0, 120.0, 60.0)), up=(0.35, -0.2, 0.9),
+                          size_x=0.0, size_y=0.0, color=(1.0, 0.82, 0.62), power=7.0, spread_deg=180.0, angle_deg=0.0,
+                          flags=1, profile=1))
     return s
 
 

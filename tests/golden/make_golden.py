@@ -10,7 +10,10 @@ its path tracer, read from the reference's own source tree (run where it is chec
 * the FNV-1a film hashes of the E5 scene with its HDRI and with the classic sky (render.rs:1106-1109)
   and SHA-256 of the HDRI scene's file (tests/fixtures/e5.rsb);
 * the E11 film hash (render.rs:1250) and SHA-256 of the Blackman-Harris inverse-CDF table
-  (pixel_filter.rs:64, 256 little-endian f32).
+  (pixel_filter.rs:64, 256 little-endian f32);
+* the L5 film hash (render.rs:1531), SHA-256 of its file (tests/fixtures/l5.rsb), and the two
+  hand-written test profiles it carries (tests/fixtures/ies/*.ies), written to
+  tests/golden/ies_profiles.json.
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -45,6 +48,7 @@ def main():
         "e5_hdri_4spp": pinned(render, "PINNED_E5_HDRI_4SPP"),
         "e5_sky_4spp": pinned(render, "PINNED_E5_SKY_4SPP"),
         "e11_edges_4spp": pinned(render, "PINNED_E11_EDGES_4SPP"),
+        "l5_ies_4spp": pinned(render, "PINNED_L5_IES_4SPP"),
     }
     block = rng[rng.index("fn matches_the_reference_implementation"):]
     block = block[:block.index("]")]
@@ -69,6 +73,9 @@ def main():
     bh_raw = struct.pack("<%df" % len(bh), *bh)
     example = (REF / "tests" / "fixtures" / "example.rsb").read_bytes()
     e5 = (REF / "tests" / "fixtures" / "e5.rsb").read_bytes()
+    l5 = (REF / "tests" / "fixtures" / "l5.rsb").read_bytes()
+    ies = {name: (REF / "tests" / "fixtures" / "ies" / (name + ".ies")).read_text() for name in ("downlight-symmetric", "wall-washer")}
+    (OUT.parent / "ies_profiles.json").write_text(json.dumps(ies, indent=1) + "\n")
     out = {
         "source": "Repackshot reference tree (engine crate rt-core), read by tests/golden/make_golden.py",
         "film_hashes": pins,
@@ -78,6 +85,7 @@ def main():
         "energy_tables": tables,
         "example_rsb": {"bytes": len(example), "sha256": hashlib.sha256(example).hexdigest()},
         "e5_rsb": {"bytes": len(e5), "sha256": hashlib.sha256(e5).hexdigest()},
+        "l5_rsb": {"bytes": len(l5), "sha256": hashlib.sha256(l5).hexdigest()},
         "blackman_harris_inv_cdf": {"count": len(bh), "sha256": hashlib.sha256(bh_raw).hexdigest()},
     }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
