@@ -41,11 +41,11 @@ uint32_t rtg_version(void);
 
 /* rt_scene_load (ffi.rs:56-66, lib.rs:145): parses an RSB scene (copied; the caller keeps its
  * bytes), builds its BVHs and uploads it. Returns a handle > 0, or 0 after recording the error
- * (rtg_scene_error_len / _copy). Lights of kinds 0-4 (rect, disk, sun, point, spot), HDRI
+ * (rtg_scene_error_len / _copy). Lights of kinds 0-5 (rect, disk, sun, point, spot, IES), HDRI
  * environments and background images (BMAP sections: 8-bit sRGB, linear f32, Radiance files), the
  * classic sky, cut-outs and thin walls render; features outside the path tracer's core (textures,
- * lens optics, particles, the physical sky, OpenEXR bitmaps, IES lights, scattering media, bevels,
- * the shadow catcher) are refused with a message that starts with "unsupported:". */
+ * lens optics, particles, the physical sky, OpenEXR bitmaps, emissive mesh lights, scattering
+ * media, bevels, the shadow catcher) are refused with a message that starts with "unsupported:". */
 uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len);
 
 /* rt_scene_update (ffi.rs:68-88, rt-wasm/src/lib.rs:171-193, Scene::update_from_rsb

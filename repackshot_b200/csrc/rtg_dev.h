@@ -72,6 +72,11 @@ struct LightDev {
     float cos_max, one_minus_cos_max, solid_angle;  // sun
     float intensity[3];                             // sphere: W/sr
     float cos_outer, cos_inner, near2;              // sphere: cos_outer below -1 means no mask
+    // an IES light (a sphere masked by its profile in the frame fx, fy, fz: axis z, angle 0 along
+    // y): vertical angles, horizontal angles, candela rows
+    const float* ies;
+    uint32_t ies_nv, ies_nh, ies_sym;
+    float ies_peak;
     uint32_t kind, rect, delta;
     uint32_t glossy, camera, shadow, entry;
     uint32_t source;  // index of the scene light it was built from

@@ -215,6 +215,12 @@ uint32_t upload_shading(const Flat& F, BufSet& set, SceneDev& S) {
         (st = upload(set, F.bsdfs, S.bsdfs)))
         return st;
     LightsDev L = F.lights;
+    if (!F.ies_data.empty()) {  // the IES lights point into their tables on the device
+        const float* dev = nullptr;
+        if ((st = upload(set, F.ies_data, dev))) return st;
+        for (uint32_t i = 0; i < L.n_lights; ++i)
+            if (L.lights[i].ies) L.lights[i].ies = dev + (F.lights.lights[i].ies - F.ies_data.data());
+    }
     if (L.env_is_map && F.env_image) {
         if ((st = upload(set, F.env_image->texels, L.env_map.texels)) || (st = upload(set, F.env_map.weights, L.env_map.weights)) ||
             (st = upload(set, F.env_map.conditional, L.env_map.conditional)) || (st = upload(set, F.env_map.marginal, L.env_map.marginal)))

@@ -62,10 +62,78 @@ RTG_HD V3 uniform_cone(float u0, float u1, float one_minus_cos_max) {
     return v3(sin * cp, sin * sp, cos);
 }
 
-// ---- sphere lights (points and spots) -------------------------------------------------------------
+// ---- IES profiles (ies.rs:350-430) ----------------------------------------------------------------
+// The cell of an increasing list of n >= 2 angles that holds x: the last one at or below x, at
+// most the second last (partition_point(a <= x) - 1, saturating).
+RTG_HD uint32_t ies_cell(const float* a, uint32_t n, float x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] <= x) lo = mid + 1;
+        else hi = mid;
+    }
+    const uint32_t i = lo ? lo - 1 : 0;
+    return i < n - 2 ? i : n - 2;
+}
+// phi (degrees) folded into the stored range by the table's symmetry (0 rotational, 1 quadrant,
+// 2 bilateral 0-180, 3 bilateral 90-270, 4 full).
+RTG_HD float ies_fold(uint32_t sym, float phi) {
+    const float p = phi - 360.0f * floor_(phi / 360.0f);
+    if (sym == 2) return p > 180.0f ? 360.0f - p : p;
+    if (sym == 1) {
+        const float q = p > 180.0f ? 360.0f - p : p;
+        return q > 90.0f ? 180.0f - q : q;
+    }
+    if (sym == 3) {
+        if (p >= 90.0f && p <= 270.0f) return p;
+        const float q = 180.0f - p;
+        return q < 0.0f ? q + 360.0f : q;
+    }
+    return p;
+}
+// The share of its peak an IES light sends towards the unit direction `local` of its own frame
+// (+z its axis, phi = 0 along +y, increasing towards +x): the candela interpolated bilinearly in
+// gamma and phi, 0 outside the vertical range, over the peak, at most 1.
+RTG_HD float ies_shape(const LightDev& l, V3 local) {
+    constexpr float kRad = 180.0f / PI;
+    const float* v = l.ies;
+    const float* hz = l.ies + l.ies_nv;
+    const float* cd = hz + l.ies_nh;
+    const uint32_t nv = l.ies_nv, nh = l.ies_nh;
+    const float rho = sqrt_(local.x * local.x + local.y * local.y);
+    const float gamma = fatan2(rho, local.z) * kRad;
+    float intensity = 0.0f;
+    if (gamma >= v[0] && gamma <= v[nv - 1]) {
+        const uint32_t i = ies_cell(v, nv, gamma);
+        const float t = (gamma - v[i]) / (v[i + 1] - v[i]);
+        auto along = [&](uint32_t row) {
+            const float a = cd[row * nv + i], b = cd[row * nv + i + 1];
+            return a + (b - a) * t;
+        };
+        if (nh == 1) {
+            intensity = along(0);
+        } else {
+            const float p = ies_fold(l.ies_sym, fatan2(local.x, local.y) * kRad);
+            const uint32_t j = ies_cell(hz, nh, p);
+            const float s = (p - hz[j]) / (hz[j + 1] - hz[j]);
+            const float a = along(j), b = along(j + 1);
+            intensity = a + (b - a) * s;
+        }
+    }
+    return rmin(intensity / l.ies_peak, 1.0f);
+}
+
+// ---- sphere lights (points, spots and IES lights) --------------------------------------------------
 // How much of its light reaches x: 1 for a point light; for a spot a smoothstep from 0 at the
 // edge of its cone to 1 at its inner cone, by the direction from its centre (light.rs:368).
 RTG_HD float sphere_mask(const LightDev& l, V3 x) {
+    if (l.ies) {  // L5: the profile's share of its peak towards x, seen from the centre
+        const V3 d = x - ld3(l.centre);
+        const float n2 = len2(d);
+        if (!(n2 > 0.0f)) return 0.0f;
+        const V3 u = d / sqrt_(n2);
+        return ies_shape(l, v3(dot(u, ld3(l.fx)), dot(u, ld3(l.fy)), dot(u, ld3(l.fz))));
+    }
     if (l.cos_outer < -1.0f) return 1.0f;
     V3 d = x - ld3(l.centre);
     float n2 = len2(d);

@@ -169,7 +169,7 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (!(r.vec3(l.position) && r.vec3(l.direction) && r.vec3(l.up) && r.f32(l.size_x) && r.f32(l.size_y) && r.f3(l.color) &&
                   r.f32(l.power) && r.f32(l.spread_deg) && r.f32(l.angle_deg) && r.u32(l.flags)))
                 return false;
-            if (l.kind == 5) { error = "unsupported: IES light"; return false; }
+            if (l.kind == 5 && !r.ou32(l.profile, 0xffffffffu)) return false;  // rsb.rs:1006
             s.lights.push_back(l);
         } else if (is("ENVR")) {
             if (!once(seen_env)) return false;
@@ -184,6 +184,15 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
                   r.of32(s.backplate_rect[3], 1.0f) && r.ou32(s.sky_model, 0)))
                 return false;
             if (s.env_kind == 2 && s.sky_model != 1) { error = "unsupported: physical sky model"; return false; }
+        } else if (is("IESP")) {  // rsb.rs:1018: an IES file
+            uint32_t n;
+            if (!r.u32(n)) return false;
+            if ((size_t)n > r.remaining()) return r.too_short();
+            HIes prof;
+            std::string reason;
+            if (!parse_ies(r.d + r.pos, n, prof, reason)) return r.invalid(reason.c_str());
+            r.pos += n;
+            s.profiles.push_back(std::move(prof));
         } else if (is("BMAP")) {  // rsb.rs:1057
             uint32_t format, w, h, n;
             if (!(r.u32(format) && r.u32(w) && r.u32(h) && r.u32(n))) return false;
@@ -222,7 +231,7 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
 
         } else {
             static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "SECT",
-                                                 "GLAS", "WETP", "WETF", "WTP2", "WETG", "NEST", "IESP"};
+                                                 "GLAS", "WETP", "WETF", "WTP2", "WETG", "NEST"};
             for (const char* t : feature_tags)
                 if (is(t)) { error = std::string("unsupported: RSB section ") + t; return false; }
         }
@@ -232,6 +241,11 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
         if (used_kept) *used_kept = true;
     }
     if (s.bitmaps.empty() && kept_bitmaps) s.bitmaps = *kept_bitmaps;
+    for (const HLight& l : s.lights)  // rsb.rs:1354
+        if (l.kind == 5 && l.profile >= s.profiles.size()) {
+            error = "RSB section LGHT is invalid: an IES light needs a profile that is an IESP section";
+            return false;
+        }
     for (uint32_t map : {s.hdri_map, s.backplate_map})
         if (map != 0xffffffffu && map >= s.bitmaps.size()) {
             error = "RSB section ENVR is invalid: bitmap index does not refer to a BMAP section";
@@ -557,6 +571,17 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
     // point into lights[] once the kinds are laid out as areas, then suns, then spheres.
     std::vector<float> weights;
     std::vector<LightDev> kinds[3];
+    // The IES lights' tables, laid out once so that the lights can point into them.
+    std::vector<size_t> ies_at(s.lights.size(), 0);
+    F.ies_data.clear();
+    for (size_t li = 0; li < s.lights.size(); ++li)
+        if (s.lights[li].kind == 5) {
+            const HIes& p = s.profiles[s.lights[li].profile];
+            ies_at[li] = F.ies_data.size();
+            F.ies_data.insert(F.ies_data.end(), p.vertical.begin(), p.vertical.end());
+            F.ies_data.insert(F.ies_data.end(), p.horizontal.begin(), p.horizontal.end());
+            F.ies_data.insert(F.ies_data.end(), p.candela.begin(), p.candela.end());
+        }
     std::vector<std::pair<uint32_t, uint32_t>> refs;  // (kind, index in its kind) per entry
     auto put3 = [](float* d, V3 v) { d[0] = v.x; d[1] = v.y; d[2] = v.z; };
     for (size_t li = 0; li < s.lights.size(); ++li) {
@@ -593,13 +618,30 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
             a.cos_max = 1.0f - a.one_minus_cos_max;
             a.solid_angle = TAU * a.one_minus_cos_max;
             a.base = luminance(irr);
-        } else if (l.kind == 3 || l.kind == 4) {  // point light or spot (light.rs:780)
+        } else if (l.kind == 3 || l.kind == 4 || l.kind == 5) {  // point light, spot or IES light (light.rs:780)
             a.kind = LIGHT_SPHERE;
             float k = power / (4.0f * PI);
             a.intensity[0] = color[0] * k; a.intensity[1] = color[1] * k; a.intensity[2] = color[2] * k;
-            float radius = 0.5f * absf(l.size_x);
-            a.radius = finitef(radius) ? radius : 0.0f;
+            const float r_light = 0.5f * absf(l.size_x);
+            a.radius = finitef(r_light) ? r_light : 0.0f;
             V3 axis = v3(0.0f, 0.0f, -1.0f);
+            const HIes* ies = nullptr;
+            if (l.kind == 5) {  // L5: masked by its profile in the frame of its axis and its up
+                ies = &s.profiles[l.profile];
+                V3 z = normalize(l.direction);
+                V3 y = normalize(l.up - z * dot(z, l.up));
+                Frame f;
+                if (len2(y) < 0.5f) f = frame_from_normal(z);
+                else { f.x = cross(y, z); f.y = y; f.z = z; }
+                if (len2(f.z) < 0.5f) continue;
+                put3(a.fx, f.x); put3(a.fy, f.y);
+                axis = f.z;
+                a.ies = F.ies_data.data() + ies_at[li];
+                a.ies_nv = (uint32_t)ies->vertical.size();
+                a.ies_nh = (uint32_t)ies->horizontal.size();
+                a.ies_sym = ies->symmetry;
+                a.ies_peak = ies->peak;
+            }
             if (l.kind == 4) {
                 axis = normalize(l.direction);
                 if (len2(axis) < 0.5f) continue;
@@ -623,7 +665,10 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
             put3(a.centre, l.position);
             a.base = luminance(rgb(a.intensity[0], a.intensity[1], a.intensity[2]));
             a.near2 = rmax(r_m * r_m, 1.0e-6f);
-            float toward = 0.05f + 0.95f * sphere_mask(a, centre);
+            // An IES light inside the sphere that bounds the scene sends it its whole flux:
+            // flux / (4 pi peak) of its peak's worth.
+            const float toward = (ies && len(l.position - centre) <= radius) ? ies->flux / (4.0f * PI * ies->peak)
+                                                                               : 0.05f + 0.95f * sphere_mask(a, centre);
             weights.push_back(flux * toward * reach(l.position, nullptr));
         } else {  // rect or disk
             a.kind = LIGHT_AREA;

@@ -28,6 +28,7 @@ struct HLight {
     float color[3] = {1, 1, 1};
     float power = 0, spread_deg = 180, angle_deg = 0;
     uint32_t flags = 0;
+    uint32_t profile = 0xffffffffu;  // an IES light's profile among the scene's IESP sections
 };
 struct HMesh {
     std::vector<V3> positions, normals;  // normals empty: none
@@ -42,6 +43,18 @@ struct HInstance {
     float rows[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
     uint32_t material_id = 0, flags = 0;
 };
+// An IES LM-63 type C profile (ies.rs:207): vertical and horizontal angles in degrees, the candela
+// table (a row of vertical values per horizontal angle, the file's multiplier applied), its
+// symmetry, peak and flux (candela steradians of the bilinear interpolant).
+enum : uint32_t { IES_ROTATIONAL = 0, IES_QUADRANT = 1, IES_BILATERAL0 = 2, IES_BILATERAL90 = 3, IES_FULL = 4 };
+struct HIes {
+    uint32_t symmetry = IES_ROTATIONAL;
+    std::vector<float> vertical, horizontal, candela;
+    float peak = 0, flux = 0;
+};
+// IesProfile::parse (ies.rs:227): false with the reference's reason.
+bool parse_ies(const uint8_t* bytes, size_t len, HIes& out, std::string& reason);
+
 // A decoded bitmap: linear RGB texels (3 per pixel), rows top to bottom.
 struct HImage {
     uint32_t width = 0, height = 0;
@@ -74,6 +87,7 @@ struct HScene {
     std::vector<HInstance> instances;
     std::vector<HLight> lights;
     std::vector<HImage> bitmaps;
+    std::vector<HIes> profiles;
     uint32_t env_kind = 0;  // 0 studio, 1 flat, 2 sky, 3 HDRI
     float env_floor = 0.1f, env_horizon = 0.3f, env_zenith = 0.6f, env_strength = 1, env_rotation = 0;
     float background_color[3] = {0.05f, 0.05f, 0.05f};
@@ -110,6 +124,7 @@ struct Flat {
     // with the shading; the pointers in `lights` and `scene` are set on upload)
     HEnvMap env_map;
     HImage sky;  // the tabulated sky of a sky environment
+    std::vector<float> ies_data;  // per IES light: vertical angles, horizontal angles, candela
     const HImage* env_image = nullptr;
     const HImage* plate = nullptr;
     std::vector<QNode> nodes;
