@@ -59,6 +59,9 @@ def lib():
             "orc_ies": (u32, [ctypes.c_char_p, u32, v, u32, v, v, u32, v, v]),
             "orc_blackman_harris_table": (None, [v]),
             "orc_edge_mask": (None, [u32, v]),
+            "orc_adaptive_decide": (u32, [u32, u32, ctypes.c_float, ctypes.c_float, u32, v, v, v, v, v]),
+            "orc_adaptive_film": (u32, [u32, u32, u32, u32, v, v, v, v, v, v]),
+            "orc_pixel_error": (ctypes.c_float, [ctypes.c_float] * 4 + [u32, ctypes.c_float]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -172,6 +175,21 @@ class OracleScene:
         lib().orc_edge_mask(self.handle, _p(out))
         return out
 
+    def adaptive_film(self, cap, pass_samples=16, threads=8):
+        """The scene rendered adaptively to convergence or `cap` samples a pixel
+        (adaptive/tests.rs:294): (rgb, weight, alpha, lum2, counts per block (rows, cols),
+        (fewest, most samples of a pixel, decisions taken, rays mod 2^32))."""
+        w, h = self.width, self.height
+        n = w * h
+        rgb, wt, al, l2 = (np.zeros(3 * n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32))
+        cols, rows = (w + 7) // 8, (h + 7) // 8
+        counts = np.zeros(cols * rows, np.uint32)
+        st = np.zeros(4, np.uint32)
+        if lib().orc_adaptive_film(self.handle, cap, pass_samples, threads, _p(rgb), _p(wt), _p(al), _p(l2), _p(counts), _p(st)):
+            raise ValueError("bad scene handle")
+        return (rgb.reshape(h, w, 3), wt.reshape(h, w), al.reshape(h, w), l2.reshape(h, w), counts.reshape(rows, cols),
+                tuple(int(v) for v in st))
+
     def occluded(self, rays):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
         out = np.zeros(len(rays), np.uint8)
@@ -215,6 +233,27 @@ def ies(text, angles=(), dirs=()):
     if lib().orc_ies(data, len(data), _p(out3), len(gp), _p(gp), _p(inten), len(dd), _p(dd), _p(shp)):
         raise ValueError(error())
     return float(out3[0]), float(out3[1]), int(out3[2]), inten, shp
+
+
+def adaptive_decide(width, height, ev, target, cap, counts, sums, lum2):
+    """rt_adaptive_decide (rt-wasm/src/lib.rs:660): (active bytes per block, six words: round,
+    active, blocks, and the bits of threshold, max_error, remaining)."""
+    cols, rows = (width + 7) // 8, (height + 7) // 8
+    counts = np.ascontiguousarray(counts, np.uint32).reshape(-1)
+    sums = np.ascontiguousarray(sums, np.float32).reshape(-1)
+    lum2 = np.ascontiguousarray(lum2, np.float32).reshape(-1)
+    if counts.size != cols * rows or sums.size != 4 * width * height or lum2.size != width * height:
+        raise ValueError("plane sizes do not match the image")
+    active = np.zeros(max(cols * rows, 1), np.uint8)
+    words = np.zeros(6, np.uint32)
+    st = lib().orc_adaptive_decide(width, height, float(ev), float(target), cap, _p(counts), _p(sums), _p(lum2), _p(active), _p(words))
+    if st:
+        raise ValueError(f"status {st}")
+    return active[:cols * rows], words
+
+
+def pixel_error(r, g, b, lum2, n, floor):
+    return float(lib().orc_pixel_error(float(r), float(g), float(b), float(lum2), int(n), float(floor)))
 
 
 def filter_offset(filter_kind, us):

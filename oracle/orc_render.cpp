@@ -7,6 +7,7 @@
 #include <mutex>
 #include <thread>
 
+#include "orc_adaptive.h"
 #include "orc_scene.h"
 
 namespace orc {
@@ -722,6 +723,62 @@ uint64_t orc_render_film(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint3
         std::memcpy(stats11, v, sizeof(v));
     }
     return rays;
+}
+
+// E10 (adaptive/tests.rs:294 adaptive_film, a scene without photon maps): renders scene `h`
+// adaptively, at most `cap` samples a pixel (0: none), in passes of `pass` samples cut at the
+// rounds, straight into one whole-image film: each active block renders its samples of the pass
+// in index order (render.rs:352 render_block). The blocks of a pass are shared by `threads`
+// workers; a block's pixels are its own, so any split gives the same film. Outputs the film's
+// sums, each block's samples (counts, row by row) and state4 = the fewest and the most samples of
+// a pixel, the decisions taken and the rays traced (low 32 bits). 0, or 1 for a bad handle.
+uint32_t orc_adaptive_film(uint32_t h, uint32_t cap, uint32_t pass, uint32_t threads, float* rgb, float* weight, float* alpha,
+                           float* lum2, uint32_t* counts, uint32_t* state4) {
+    Loaded* l = get(h);
+    if (!l || !rgb || !weight || !alpha || !lum2 || !counts || !state4) return 1;
+    const RenderSettings& rs = l->scene.render;
+    if (pass == 0) pass = AD_ROUND;
+    if (threads == 0) threads = 1;
+    Film film(0, 0, rs.width, rs.height);
+    Adaptive ad(rs.width, rs.height, rs.exposure_ev, rs.noise_threshold, cap);
+    std::vector<BlockWork> work;
+    uint32_t decisions = 0;
+    std::atomic<uint64_t> rays(0);
+    for (;;) {
+        if (ad.left() == 0) {
+            ad.decide(film.rgb.data(), 3, film.lum2.data());
+            ++decisions;
+            if (ad.converged()) break;
+        }
+        const uint32_t count = std::min(pass, ad.left());
+        ad.work(0, 0, rs.width, rs.height, count, work);
+        std::atomic<size_t> next(0);
+        auto worker = [&]() {
+            PathStats st;
+            for (;;) {
+                const size_t i = next.fetch_add(1);
+                if (i >= work.size()) break;
+                const BlockWork& wk = work[i];
+                for (uint32_t j = 0; j < wk.count; ++j)
+                    render_tile(l->scene, l->prep, l->edges, wk.x, wk.y, wk.w, wk.h, wk.first + j, film, st);
+            }
+            rays += st.rays;
+        };
+        std::vector<std::thread> pool;
+        for (uint32_t i = 0; i < threads; ++i) pool.emplace_back(worker);
+        for (auto& t : pool) t.join();
+        ad.advance(count);
+    }
+    const size_t n = (size_t)rs.width * rs.height;
+    std::memcpy(rgb, film.rgb.data(), n * 12);
+    std::memcpy(weight, film.weight.data(), n * 4);
+    std::memcpy(alpha, film.alpha.data(), n * 4);
+    std::memcpy(lum2, film.lum2.data(), n * 4);
+    std::memcpy(counts, ad.counts.data(), ad.counts.size() * 4);
+    ad.min_max(state4[0], state4[1]);
+    state4[2] = decisions;
+    state4[3] = (uint32_t)rays.load();
+    return 0;
 }
 
 // Also counts every query's visits in a single reference-layout BVH8 over the identity

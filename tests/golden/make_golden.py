@@ -13,7 +13,9 @@ its path tracer, read from the reference's own source tree (run where it is chec
   (pixel_filter.rs:64, 256 little-endian f32);
 * the L5 film hash (render.rs:1531), SHA-256 of its file (tests/fixtures/l5.rsb), and the two
   hand-written test profiles it carries (tests/fixtures/ies/*.ies), written to
-  tests/golden/ies_profiles.json.
+  tests/golden/ies_profiles.json;
+* the hash of six adaptive-sampling decisions of the synthetic 45 x 37 image
+  (engine/crates/rt-core/src/adaptive/tests.rs:497-534).
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -87,6 +89,7 @@ def main():
         "e5_rsb": {"bytes": len(e5), "sha256": hashlib.sha256(e5).hexdigest()},
         "l5_rsb": {"bytes": len(l5), "sha256": hashlib.sha256(l5).hexdigest()},
         "blackman_harris_inv_cdf": {"count": len(bh), "sha256": hashlib.sha256(bh_raw).hexdigest()},
+        "e10_synthetic_decisions": pinned((CORE / "adaptive" / "tests.rs").read_text(), "PINNED_E10_DECISIONS"),
     }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(OUT)
