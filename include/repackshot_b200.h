@@ -227,6 +227,53 @@ uint32_t rtg_set_stream(uint32_t scene, void* stream);
 
 uint32_t rtg_synchronize(uint32_t scene);
 
+/* ---- Adaptive sampling (E10, rt-core/src/adaptive.rs) ------------------------------------------
+ * The image is sampled in rounds: every pixel gets 16 samples first, then each round goes to the
+ * 8 x 8 blocks whose smoothed relative error of the mean is at or above the median of those still
+ * above the noise target (RNDR.noise_threshold) and under the cap; the round's size grows when few
+ * blocks are active. A block that stops keeps its samples: every pixel stays the plain mean of its
+ * own samples 0..n, the pixel a progressive render of n samples gives it.
+ *
+ * rt_adaptive_decide (rt-wasm/src/ffi.rs:237-289): the decision of a width x height image from
+ * its blocks' samples (`counts`, u32 each, ceil(width/8) x ceil(height/8) of them, row by row), its
+ * RGBA sums (`sums`, 4 f32 a pixel), its squared-luminance sums (`lum2`, f32), the exposure `ev`,
+ * the noise `target` and the sample `cap` (0: none). Writes one byte a block to `active` (1: in the
+ * next round) and six u32 words to `decision`: the round's samples (0: converged), the active
+ * blocks, the blocks, then the bits of the threshold, the largest block error and the pixel-samples
+ * still needed. Pointers need no alignment. RTG_STATUS_NULL_POINTER for a null pointer,
+ * RTG_STATUS_BAD_TILE for an empty image (or a side above 16384). The per-pixel errors are found
+ * on the GPU, the per-block choice on the host, with the reference's bits. */
+uint32_t rtg_adaptive_decide(uint32_t width, uint32_t height, float ev, float target, uint32_t cap, const uint8_t* counts,
+                             const uint8_t* sums, const uint8_t* lum2, uint8_t* active, uint8_t* decision);
+
+/* rt_render_block_rgba (rt-wasm/src/ffi.rs:196-235): sample `sample_index` of the pixel rectangle
+ * (x, y, w, h), a block of a round, as rtg_render_tile_rgba gives it (w*h*4 floats, RGBA; edge
+ * pixels take their edge samples). `iteration` names the photon map of the reference's caustics;
+ * scenes with caustics are refused at load, so it is unused. Status as rtg_render_tile_rgba. */
+uint32_t rtg_render_block_rgba(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index,
+                               uint32_t iteration, float* out);
+
+/* An adaptive render of `scene` into `film` (one of the scene's films covering its whole image,
+ * normally cleared) with at most `cap` samples a pixel (0: none), the noise target and exposure of
+ * the scene's RNDR section (adaptive.rs:349 Adaptive::new). Returns its handle, or 0 (the reason
+ * in rtg_scene_error_*). */
+uint32_t rtg_adaptive_create(uint32_t scene, uint32_t film, uint32_t cap);
+/* Runs the host loop of an adaptive render (adaptive/tests.rs:311): at the end of a round decides
+ * the next (block errors on the GPU from the film where it lies); renders passes of at most `pass`
+ * samples (0: 16) of the round, the first round over the whole image, later ones over the pixels
+ * of the active blocks only; stops when converged or after `max_passes` passes (0: no limit).
+ * `passes` and `rays` (may be null) get the passes rendered and the rays cast. The film is the
+ * same for any `pass` and any split into calls. */
+uint32_t rtg_adaptive_run(uint32_t ad, uint32_t pass, uint32_t max_passes, uint32_t* passes, uint64_t* rays);
+/* out16: the round's samples, the samples of it rendered, those left, the photon-map iteration of
+ * the next sample, converged (0/1), decisions taken, the fewest and the most samples of a pixel,
+ * the last decision's six words (as rtg_adaptive_decide's), the columns and rows of blocks. */
+uint32_t rtg_adaptive_state(uint32_t ad, uint32_t* out16);
+/* Each block's samples now (u32, row by row) and whether it is in the round (one byte each);
+ * either pointer may be null, not both. */
+uint32_t rtg_adaptive_counts(uint32_t ad, uint32_t* samples, uint8_t* active);
+uint32_t rtg_adaptive_free(uint32_t ad);
+
 #ifdef __cplusplus
 }
 #endif

@@ -244,6 +244,7 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             if (!(s.denoise_strength >= 0.0f && s.denoise_strength <= 1.0f)) return r.invalid("denoise_strength must be between 0 and 1");
             if (s.caustic_photons > (1u << 22)) return r.invalid("caustic_photons must be at most 4194304");
             if (s.caustic_radius < 0.0f) return r.invalid("caustic_radius must not be negative");
+            if (s.caustic_photons > 0) { error = "unsupported: caustic photon maps (caustic_photons above 0)"; return false; }
             if (s.width < 1 || s.width > 16384 || s.height < 1 || s.height > 16384)
                 return r.invalid("width and height must be between 1 and 16384");
             if (s.max_seconds < 0.0f || s.clamp_indirect < 0.0f) return r.invalid("max_seconds and clamp_indirect must not be negative");

@@ -69,6 +69,13 @@ ABI = {
     "rtg_timing": (_u32, [_u32, _u32, _u32, _f]),
     "rtg_set_stream": (_u32, [_u32, ctypes.c_void_p]),
     "rtg_synchronize": (_u32, [_u32]),
+    "rtg_adaptive_decide": (_u32, [_u32, _u32, ctypes.c_float, ctypes.c_float, _u32, _f, _f, _f, _f, _f]),
+    "rtg_render_block_rgba": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _u32, _f]),
+    "rtg_adaptive_create": (_u32, [_u32, _u32, _u32]),
+    "rtg_adaptive_run": (_u32, [_u32, _u32, _u32, ctypes.POINTER(_u32), ctypes.POINTER(_u64)]),
+    "rtg_adaptive_state": (_u32, [_u32, _f]),
+    "rtg_adaptive_counts": (_u32, [_u32, _f, _f]),
+    "rtg_adaptive_free": (_u32, [_u32]),
 }
 
 
@@ -287,6 +294,75 @@ class Film:
     def close(self):
         if self.handle:
             lib().rtg_film_free(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def adaptive_decide(width: int, height: int, ev: float, target: float, cap: int, counts, sums, lum2):
+    """rt_adaptive_decide (rt-wasm/src/lib.rs:660) through rtg_adaptive_decide: (active bytes per
+    block, six u32 words: round, active blocks, blocks, then the bits of the threshold, the largest
+    error and the remaining pixel-samples). ``sums`` holds 4 floats a pixel (RGBA)."""
+    cols, rows = (width + 7) // 8, (height + 7) // 8
+    counts = np.ascontiguousarray(counts, np.uint32).reshape(-1)
+    sums = np.ascontiguousarray(sums, np.float32).reshape(-1)
+    lum2 = np.ascontiguousarray(lum2, np.float32).reshape(-1)
+    if counts.size != cols * rows or sums.size != 4 * width * height or lum2.size != width * height:
+        raise ValueError("plane sizes do not match the image")
+    active = np.zeros(max(cols * rows, 1), np.uint8)
+    words = np.zeros(6, np.uint32)
+    _check(lib().rtg_adaptive_decide(width, height, float(ev), float(target), cap, _ptr(counts), _ptr(sums), _ptr(lum2), _ptr(active),
+                                     _ptr(words)))
+    return active[:cols * rows], words
+
+
+def render_block_rgba(handle: int, x: int, y: int, w: int, h: int, sample_index: int, iteration: int = 0):
+    """rt_render_block_rgba: (status, w*h*4 float32 array)."""
+    out = np.zeros(w * h * 4, np.float32) if 0 < w * h <= MAX_TILE_PIXELS else np.zeros(0, np.float32)
+    status = lib().rtg_render_block_rgba(handle, x, y, w, h, sample_index, iteration, _ptr(out) if out.size else None)
+    return status, out
+
+
+class Adaptive:
+    """An adaptive render (E10, rt-core/src/adaptive.rs) of a scene into one of its whole-image
+    films, to convergence or ``cap`` samples a pixel (0: none)."""
+
+    def __init__(self, scene: Scene, film: Film, cap: int):
+        self.scene, self.film = scene, film
+        self.handle = lib().rtg_adaptive_create(scene.handle, film.handle, cap)
+        if self.handle == 0:
+            raise RtgError(STATUS_BAD_ARGUMENT, error_message())
+
+    def run(self, pass_samples: int = 16, max_passes: int = 0):
+        """Renders passes until converged (or ``max_passes``): (passes, rays)."""
+        passes, rays = _u32(0), _u64(0)
+        _check(lib().rtg_adaptive_run(self.handle, pass_samples, max_passes, ctypes.byref(passes), ctypes.byref(rays)))
+        return int(passes.value), int(rays.value)
+
+    def state(self) -> dict:
+        w = np.zeros(16, np.uint32)
+        _check(lib().rtg_adaptive_state(self.handle, _ptr(w)))
+        keys = ("round", "done", "left", "iteration", "converged", "decisions", "lo", "hi")
+        out = {k: int(v) for k, v in zip(keys, w[:8])}
+        out["last"] = w[8:14].copy()
+        out["cols"], out["rows"] = int(w[14]), int(w[15])
+        return out
+
+    def counts(self):
+        """(samples per block now, (rows, cols) u32; active blocks, (rows, cols) u8)."""
+        st = self.state()
+        samples = np.zeros(st["rows"] * st["cols"], np.uint32)
+        active = np.zeros(st["rows"] * st["cols"], np.uint8)
+        _check(lib().rtg_adaptive_counts(self.handle, _ptr(samples), _ptr(active)))
+        return samples.reshape(st["rows"], st["cols"]), active.reshape(st["rows"], st["cols"])
+
+    def close(self):
+        if self.handle:
+            lib().rtg_adaptive_free(self.handle)
             self.handle = 0
 
     def __del__(self):

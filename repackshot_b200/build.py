@@ -28,8 +28,8 @@ DEVICE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true
                 "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v"]
 HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-pthread", f"-I{CUDA_HOME}/include"]
 
-HOST_SOURCES = ["rtg_scene.cpp", "rtg_bitmap.cpp", "rtg_ies.cpp", "rtg_tables.cpp", "rtg_energy.cpp", "rtg_engine.cpp"]
-DEVICE_SOURCES = ["rtg_kernels.cu", "rtg_noalloc.cu"]
+HOST_SOURCES = ["rtg_scene.cpp", "rtg_bitmap.cpp", "rtg_ies.cpp", "rtg_tables.cpp", "rtg_energy.cpp", "rtg_adaptive.cpp", "rtg_engine.cpp"]
+DEVICE_SOURCES = ["rtg_kernels.cu", "rtg_noalloc.cu", "rtg_adaptive.cu"]
 
 
 def _run(cmd, log=None):

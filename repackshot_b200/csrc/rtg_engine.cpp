@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/repackshot_b200.h"
+#include "rtg_adaptive.h"
 #include "rtg_kernels.h"
 #include "rtg_noalloc.h"
 #include "rtg_scene.h"
@@ -69,6 +70,8 @@ struct Scene {
     std::vector<float> light_power;
     float exposure_ev = 0.0f;  // RNDR's output settings
     uint32_t tonemap = 1, max_samples = 0;
+    uint32_t adaptive = 0;          // RNDR.adaptive and RNDR.noise_threshold (E10)
+    float noise_threshold = 0.0f;
     std::vector<uint32_t> light_source;  // scene light of each prepared light (areas, suns, spheres)
     DevBuf adjoint_mem;
     // edge samples (E11): the image's edge mask, its centre-ray scratch and an edge-pixel list
@@ -240,6 +243,8 @@ void keep_shading(Scene& sc, const HScene& hs, const Flat& F) {
     sc.exposure_ev = hs.exposure_ev;
     sc.tonemap = hs.tonemap;
     sc.max_samples = hs.max_samples;
+    sc.adaptive = hs.adaptive;
+    sc.noise_threshold = hs.noise_threshold;
     sc.light_power.clear();
     for (const HLight& l : hs.lights) sc.light_power.push_back(l.power);
     sc.light_source.clear();
@@ -365,12 +370,9 @@ uint32_t finish(Scene& sc, uint64_t* rays_out) {
     return RTG_STATUS_OK;
 }
 
-// Renders samples [first, first + count) of the image rectangle (x, y, w, h) (clipped to the
-// image) into `film`, every pixel's samples added in index order.
-// The image's edge mask (built once per scene state, pixel_filter.rs:175) and the edge pixels of
-// the rectangle (x, y, w, h): their packed list on the device and their count.
-uint32_t edge_pixels(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, const uint8_t*& mask, const uint32_t*& list,
-                     uint32_t& count) {
+// The image's edge mask on the device (built once per scene state, pixel_filter.rs:175), with an
+// edge-pixel list and its count after it.
+uint32_t edge_mask_of(Scene& sc, const uint8_t*& mask, uint32_t*& list, uint32_t*& count) {
     const size_t npix = (size_t)sc.width * sc.height;
     const size_t mask_bytes = (npix + 15) & ~(size_t)15;
     const size_t need = mask_bytes + npix * sizeof(uint4) + npix * 4 + 16;
@@ -383,22 +385,34 @@ uint32_t edge_pixels(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, 
     uint8_t* base = (uint8_t*)sc.edge_mem.p;
     uint8_t* m = base;
     uint4* exact = (uint4*)(base + mask_bytes);
-    uint32_t* l = (uint32_t*)(base + mask_bytes + npix * sizeof(uint4));
-    uint32_t* c = l + npix;
+    list = (uint32_t*)(base + mask_bytes + npix * sizeof(uint4));
+    count = list + npix;
     if (!sc.edges_ready) {
         RTG_CHECK(launch_edge_mask(sc.S, sc.d_lights, exact, m, sc.stream, grid_for(npix, 128)));
         sc.launches += 2;
         sc.edges_ready = true;
     }
-    RTG_CHECK(launch_edge_list(m, sc.width, x, y, w, h, l, c, sc.stream, grid_for((uint64_t)w * h, 256)));
+    mask = m;
+    return RTG_STATUS_OK;
+}
+
+// The edge pixels of the rectangle (x, y, w, h): the image's edge mask, their packed list on the
+// device and their count.
+uint32_t edge_pixels(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, const uint8_t*& mask, const uint32_t*& list,
+                     uint32_t& count) {
+    uint32_t *l = nullptr, *c = nullptr;
+    const uint32_t st = edge_mask_of(sc, mask, l, c);
+    if (st) return st;
+    RTG_CHECK(launch_edge_list(mask, sc.width, x, y, w, h, l, c, sc.stream, grid_for((uint64_t)w * h, 256)));
     sc.launches += 1;
     RTG_CHECK(cudaMemcpyAsync(&count, c, 4, cudaMemcpyDeviceToHost, sc.stream));
     RTG_CHECK(cudaStreamSynchronize(sc.stream));
-    mask = m;
     list = l;
     return RTG_STATUS_OK;
 }
 
+// Renders samples [first, first + count) of the image rectangle (x, y, w, h) (clipped to the
+// image) into `film`, every pixel's samples added in index order.
 uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t first, uint32_t count, const FilmDev& film,
                        uint64_t* rays_out) {
     uint64_t x_end = std::min<uint64_t>((uint64_t)x + w, sc.width), y_end = std::min<uint64_t>((uint64_t)y + h, sc.height);
@@ -511,6 +525,145 @@ uint32_t render_tile_impl(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, u
         if (rgba) out[o + 3] = wt[i] > 0.0f ? al[i] * inv : 0.0f;
     }
     return RTG_STATUS_OK;
+}
+
+// ---- adaptive sampling (E10, adaptive.rs:318-551) --------------------------------------------------
+// An adaptive render: the round state on the host (each block's samples when the round began,
+// the blocks of the round and its size, the samples of it rendered so far, the photon-map
+// iteration, the cap, the noise target, the floor of the mean) and the device buffers of the
+// decision and of the pass lists; the film lives on the device and covers the whole image.
+struct AdaptiveRun {
+    uint32_t scene = 0, film = 0;
+    uint32_t width = 0, height = 0, cols = 0, rows = 0;
+    std::vector<uint32_t> counts;
+    std::vector<uint8_t> active;
+    uint32_t round = 0, done = 0, iteration = 0, cap = 0, decisions = 0;
+    float target = 0.0f, floor = 0.0f;
+    AdDecision last;
+    DevBuf mem;
+    uint32_t* d_counts = nullptr;
+    float* d_error = nullptr;
+    AdEntry* d_entries = nullptr;
+    uint32_t *d_pixels = nullptr, *d_plain = nullptr, *d_plain_base = nullptr, *d_edge = nullptr, *d_edge_base = nullptr;
+    size_t blocks() const { return counts.size(); }
+    uint32_t left() const { return round - done; }
+    uint32_t quota(size_t b) const {  // adaptive.rs:409
+        if (!active[b]) return 0;
+        if (cap > 0) return std::min(round, cap > counts[b] ? cap - counts[b] : 0u);
+        return round;
+    }
+    uint32_t samples_of(size_t b) const { return counts[b] + std::min(quota(b), done); }
+    ~AdaptiveRun() { mem.release(); }
+};
+std::vector<std::unique_ptr<AdaptiveRun>> g_adaptive;
+AdaptiveRun* adaptive_of(uint32_t h) { return (h == 0 || h > g_adaptive.size()) ? nullptr : g_adaptive[h - 1].get(); }
+
+// The end of a round (adaptive.rs:513): its samples counted, the iteration moved past it, and the
+// image's decision of the next one: block errors on the device from the film where it lies, the
+// choice on the host.
+uint32_t adaptive_decide_round(Scene& sc, const Film& f, AdaptiveRun& a) {
+    for (size_t b = 0; b < a.blocks(); ++b) a.counts[b] += a.quota(b);
+    a.iteration += a.round;
+    a.done = 0;
+    const size_t nb = a.blocks();
+    RTG_CHECK(cudaMemcpyAsync(a.d_counts, a.counts.data(), nb * 4, cudaMemcpyHostToDevice, sc.stream));
+    RTG_CHECK(launch_block_error(f.dev.rgb, 3, f.dev.lum2, a.d_counts, a.width, a.height, a.floor, a.d_error, sc.stream,
+                                 grid_for((uint32_t)nb, 1)));
+    sc.launches += 1;
+    std::vector<float> err(nb);
+    RTG_CHECK(cudaMemcpyAsync(err.data(), a.d_error, nb * 4, cudaMemcpyDeviceToHost, sc.stream));
+    RTG_CHECK(cudaStreamSynchronize(sc.stream));
+    a.last = ad_decide_blocks(a.width, a.height, a.counts.data(), err.data(), a.target, a.cap, a.active);
+    a.round = a.last.round;
+    a.decisions += 1;
+    return RTG_STATUS_OK;
+}
+
+// Waves over `n` listed pixels (k samples a sample index, first sample index `first` past each
+// entry's base), `count` sample indices, each wave at most `cap` paths.
+uint32_t list_waves(Scene& sc, const FilmDev& film, const uint32_t* list, const uint32_t* base, uint32_t n, uint32_t k, uint32_t first,
+                    uint32_t count, uint64_t cap) {
+    if (n == 0 || count == 0) return RTG_STATUS_OK;
+    const uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n, cap / k));
+    for (uint32_t e0 = 0; e0 < n; e0 += chunk) {
+        const uint32_t en = std::min(chunk, n - e0);
+        const uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(count, cap / ((uint64_t)en * k)));
+        for (uint32_t s = 0; s < count; s += per) {
+            const uint32_t ns = std::min(per, count - s);
+            WaveDesc wd{0, 0, sc.width, sc.height, first + s, (uint32_t)((uint64_t)en * k * ns), nullptr};
+            wd.epix = list + e0;
+            wd.ne = en;
+            wd.ek = k;
+            wd.ebase = base + e0;
+            const uint32_t st = run_wave(sc, wd, &film);
+            if (st) return st;
+        }
+    }
+    return RTG_STATUS_OK;
+}
+
+// A pass of `count` samples of the round (adaptive.rs:471 work): the first round renders the whole
+// image as the progressive renderer does (every block active, sample indices from 0, the same
+// pixels); a later one renders the pixels of its active blocks from lists, the blocks with the most
+// samples to go first, so that sample s of the pass covers a prefix of the lists.
+uint32_t adaptive_pass(Scene& sc, const Film& f, AdaptiveRun& a, uint32_t count, uint64_t& rays) {
+    rays = 0;
+    if (a.decisions == 0) return render_region(sc, 0, 0, a.width, a.height, a.iteration + a.done, count, f.dev, &rays);
+    const size_t nb = a.blocks();
+    const uint32_t k = sc.S.edge_k > 1 ? sc.S.edge_k : 1;
+    const uint8_t* mask = nullptr;
+    if (k > 1) {
+        uint32_t *l = nullptr, *c = nullptr;
+        const uint32_t st = edge_mask_of(sc, mask, l, c);
+        if (st) return st;
+    }
+    RTG_CHECK(launch_block_pixels(mask, a.width, a.height, a.d_pixels, sc.stream, grid_for((uint32_t)nb, 128)));
+    sc.launches += 1;
+    std::vector<uint32_t> pixels(2 * nb);
+    RTG_CHECK(cudaMemcpyAsync(pixels.data(), a.d_pixels, nb * 8, cudaMemcpyDeviceToHost, sc.stream));
+    RTG_CHECK(cudaStreamSynchronize(sc.stream));
+    std::vector<std::pair<uint32_t, uint32_t>> order;  // (quota, block)
+    for (size_t b = 0; b < nb; ++b) {
+        const uint32_t q = a.quota(b);
+        if (q > a.done) order.push_back({q, (uint32_t)b});
+    }
+    if (order.empty()) return RTG_STATUS_OK;
+    std::stable_sort(order.begin(), order.end(), [](const auto& p, const auto& q) { return p.first > q.first; });
+    std::vector<AdEntry> entries(order.size());
+    std::vector<uint32_t> plain_end(order.size()), edge_end(order.size());
+    uint32_t off_p = 0, off_e = 0;
+    uint64_t total = 0;
+    for (size_t i = 0; i < order.size(); ++i) {
+        const uint32_t b = order[i].second;
+        entries[i] = AdEntry{b, a.counts[b], off_p, off_e};
+        off_p += pixels[2 * b];
+        off_e += pixels[2 * b + 1];
+        plain_end[i] = off_p;
+        edge_end[i] = off_e;
+        total += (uint64_t)std::min(order[i].first - a.done, count) * (pixels[2 * b] + (uint64_t)k * pixels[2 * b + 1]);
+    }
+    RTG_CHECK(cudaMemcpyAsync(a.d_entries, entries.data(), entries.size() * sizeof(AdEntry), cudaMemcpyHostToDevice, sc.stream));
+    RTG_CHECK(launch_block_expand(a.d_entries, (uint32_t)entries.size(), mask, a.width, a.height, a.d_plain, a.d_plain_base, a.d_edge,
+                                  a.d_edge_base, sc.stream, grid_for((uint32_t)entries.size(), 1)));
+    sc.launches += 1;
+    const uint64_t cap = std::max<uint64_t>(std::min<uint64_t>(wave_limit(sc, total), total), off_e ? k : 1);
+    uint32_t st = ensure_capacity(sc, (uint32_t)cap);
+    if (st) return st;
+    RTG_CHECK(cudaMemsetAsync(sc.P.counters, 0, 16, sc.stream));
+    RTG_CHECK(cudaMemsetAsync(sc.P.rays, 0, 16, sc.stream));
+    // Sample s of the pass covers the entries whose quota is above done + s: a prefix.
+    size_t n_in = order.size();
+    for (uint32_t s = 0; s < count;) {
+        while (n_in > 0 && order[n_in - 1].first <= a.done + s) --n_in;
+        if (n_in == 0) break;
+        const uint32_t s1 = std::min(count, order[n_in - 1].first - a.done);
+        st = list_waves(sc, f.dev, a.d_plain, a.d_plain_base, plain_end[n_in - 1], 1, a.done + s, s1 - s, cap);
+        if (st) return st;
+        st = list_waves(sc, f.dev, a.d_edge, a.d_edge_base, edge_end[n_in - 1], k, a.done + s, s1 - s, cap);
+        if (st) return st;
+        s = s1;
+    }
+    return finish(sc, &rays);
 }
 
 }  // namespace
@@ -1221,6 +1374,177 @@ uint32_t rtg_synchronize(uint32_t handle) {
     Scene* sc = scene_of(handle);
     if (!sc) return RTG_STATUS_BAD_HANDLE;
     RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    return RTG_STATUS_OK;
+}
+
+// ---- adaptive sampling (E10) -------------------------------------------------------------------------
+uint32_t rtg_adaptive_decide(uint32_t width, uint32_t height, float ev, float target, uint32_t cap, const uint8_t* counts,
+                             const uint8_t* sums, const uint8_t* lum2, uint8_t* active, uint8_t* decision) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!counts || !sums || !lum2 || !active || !decision) return RTG_STATUS_NULL_POINTER;
+    if (width == 0 || height == 0 || width > 16384 || height > 16384) return RTG_STATUS_BAD_TILE;
+    uint32_t st = device_init();
+    if (st) return st;
+    const size_t nb = (size_t)ad_cols(width) * ad_rows(height), npix = (size_t)width * height;
+    std::vector<uint32_t> c(nb);
+    std::memcpy(c.data(), counts, nb * 4);
+    DevBuf m;
+    struct Release { DevBuf& b; ~Release() { b.release(); } } release{m};
+    const size_t sums_bytes = npix * 16, lum_bytes = (npix * 4 + 255) & ~(size_t)255, nb_bytes = (nb * 4 + 255) & ~(size_t)255;
+    m.bytes = sums_bytes + lum_bytes + 2 * nb_bytes;
+    RTG_CHECK(cudaMalloc(&m.p, m.bytes));
+    uint8_t* base = (uint8_t*)m.p;
+    float* d_sums = (float*)base;
+    float* d_lum2 = (float*)(base + sums_bytes);
+    uint32_t* d_counts = (uint32_t*)(base + sums_bytes + lum_bytes);
+    float* d_err = (float*)(base + sums_bytes + lum_bytes + nb_bytes);
+    RTG_CHECK(cudaMemcpy(d_sums, sums, sums_bytes, cudaMemcpyHostToDevice));
+    RTG_CHECK(cudaMemcpy(d_lum2, lum2, npix * 4, cudaMemcpyHostToDevice));
+    RTG_CHECK(cudaMemcpy(d_counts, c.data(), nb * 4, cudaMemcpyHostToDevice));
+    RTG_CHECK(launch_block_error(d_sums, 4, d_lum2, d_counts, width, height, ad_floor_for(ev), d_err, 0, grid_for((uint32_t)nb, 1)));
+    std::vector<float> err(nb);
+    RTG_CHECK(cudaMemcpy(err.data(), d_err, nb * 4, cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> act;
+    const AdDecision d = ad_decide_blocks(width, height, c.data(), err.data(), target, cap, act);
+    std::memcpy(active, act.data(), nb);
+    uint32_t words[6] = {d.round, d.active, d.blocks, 0, 0, 0};
+    std::memcpy(&words[3], &d.threshold, 4);
+    std::memcpy(&words[4], &d.max_error, 4);
+    std::memcpy(&words[5], &d.remaining, 4);
+    std::memcpy(decision, words, sizeof(words));
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_render_block_rgba(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index,
+                               uint32_t iteration, float* out) {
+    (void)iteration;  // the photon map of an iteration: scenes with caustics are refused at load
+    if (!out) return RTG_STATUS_NULL_POINTER;
+    std::lock_guard<std::mutex> lk(g_mu);
+    return render_tile_impl(handle, x, y, w, h, sample_index, out, true);
+}
+
+uint32_t rtg_adaptive_create(uint32_t scene, uint32_t film, uint32_t cap) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(scene);
+    if (!sc) { g_error = "rtg_adaptive_create: bad scene handle"; return 0; }
+    Film* f = film_of(film);
+    if (!f || f->scene != scene || f->dev.ox || f->dev.oy || f->dev.w != sc->width || f->dev.h != sc->height) {
+        g_error = "rtg_adaptive_create: the film must be one of the scene's and cover its whole image";
+        return 0;
+    }
+    auto a = std::make_unique<AdaptiveRun>();
+    a->scene = scene;
+    a->film = film;
+    a->width = sc->width;
+    a->height = sc->height;
+    a->cols = ad_cols(sc->width);
+    a->rows = ad_rows(sc->height);
+    const size_t nb = (size_t)a->cols * a->rows, npix = (size_t)sc->width * sc->height;
+    a->counts.assign(nb, 0);
+    a->active.assign(nb, 1);
+    a->cap = cap;
+    a->round = cap > 0 ? std::min(AD_WARMUP, cap) : AD_WARMUP;  // adaptive.rs:349
+    a->target = sc->noise_threshold > 0.0f ? sc->noise_threshold : 0.0f;
+    a->floor = ad_floor_for(sc->exposure_ev);
+    auto round_up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t nb4 = round_up(nb * 4), list = round_up(npix * 4);
+    a->mem.bytes = 2 * nb4 + round_up(nb * sizeof(AdEntry)) + round_up(nb * 8) + 4 * list;
+    if (cudaMalloc(&a->mem.p, a->mem.bytes) != cudaSuccess) {
+        a->mem.p = nullptr;
+        g_error = "rtg_adaptive_create: out of device memory";
+        return 0;
+    }
+    uint8_t* p = (uint8_t*)a->mem.p;
+    a->d_counts = (uint32_t*)p; p += nb4;
+    a->d_error = (float*)p; p += nb4;
+    a->d_entries = (AdEntry*)p; p += round_up(nb * sizeof(AdEntry));
+    a->d_pixels = (uint32_t*)p; p += round_up(nb * 8);
+    a->d_plain = (uint32_t*)p; p += list;
+    a->d_plain_base = (uint32_t*)p; p += list;
+    a->d_edge = (uint32_t*)p; p += list;
+    a->d_edge_base = (uint32_t*)p;
+    for (size_t i = 0; i < g_adaptive.size(); ++i)
+        if (!g_adaptive[i]) { g_adaptive[i] = std::move(a); return (uint32_t)i + 1; }
+    g_adaptive.push_back(std::move(a));
+    return (uint32_t)g_adaptive.size();
+}
+
+uint32_t rtg_adaptive_run(uint32_t ad, uint32_t pass, uint32_t max_passes, uint32_t* passes_out, uint64_t* rays) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (passes_out) *passes_out = 0;
+    if (rays) *rays = 0;
+    AdaptiveRun* a = adaptive_of(ad);
+    if (!a) return RTG_STATUS_BAD_HANDLE;
+    Scene* sc = scene_of(a->scene);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    Film* f = film_of(a->film);
+    if (!f) return RTG_STATUS_BAD_FILM;
+    if (sc->width != a->width || sc->height != a->height) {
+        g_error = "rtg_adaptive_run: the scene's image size changed since rtg_adaptive_create";
+        return RTG_STATUS_BAD_SCENE;
+    }
+    if (pass == 0) pass = AD_ROUND;
+    uint32_t passes = 0;
+    uint64_t total = 0;
+    for (;;) {  // adaptive/tests.rs:311
+        if (a->left() == 0) {
+            if (a->decisions && a->round == 0) break;  // converged
+            const uint32_t st = adaptive_decide_round(*sc, *f, *a);
+            if (st) return st;
+            if (a->round == 0) break;
+        }
+        if (max_passes && passes >= max_passes) break;
+        const uint32_t count = std::min(pass, a->left());
+        uint64_t r = 0;
+        const uint32_t st = adaptive_pass(*sc, *f, *a, count, r);
+        if (st) return st;
+        total += r;
+        a->done = std::min(a->done + count, a->round);  // adaptive.rs:502
+        ++passes;
+        if (passes_out) *passes_out = passes;
+        if (rays) *rays = total;
+    }
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_adaptive_state(uint32_t ad, uint32_t* out16) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    AdaptiveRun* a = adaptive_of(ad);
+    if (!a) return RTG_STATUS_BAD_HANDLE;
+    if (!out16) return RTG_STATUS_NULL_POINTER;
+    uint32_t lo = UINT32_MAX, hi = 0;
+    for (size_t b = 0; b < a->blocks(); ++b) {
+        lo = std::min(lo, a->samples_of(b));
+        hi = std::max(hi, a->samples_of(b));
+    }
+    if (lo == UINT32_MAX) lo = hi = 0;
+    uint32_t w[16] = {a->round, a->done, a->left(), a->iteration + a->done, (a->decisions && a->round == 0) ? 1u : 0u, a->decisions,
+                      lo, hi, a->last.round, a->last.active, a->last.blocks, 0, 0, 0, a->cols, a->rows};
+    std::memcpy(&w[11], &a->last.threshold, 4);
+    std::memcpy(&w[12], &a->last.max_error, 4);
+    std::memcpy(&w[13], &a->last.remaining, 4);
+    std::memcpy(out16, w, sizeof(w));
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_adaptive_counts(uint32_t ad, uint32_t* samples, uint8_t* active) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    AdaptiveRun* a = adaptive_of(ad);
+    if (!a) return RTG_STATUS_BAD_HANDLE;
+    if (!samples && !active) return RTG_STATUS_NULL_POINTER;
+    for (size_t b = 0; b < a->blocks(); ++b) {
+        if (samples) samples[b] = a->samples_of(b);
+        if (active) active[b] = a->active[b];
+    }
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_adaptive_free(uint32_t ad) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!adaptive_of(ad)) return RTG_STATUS_BAD_HANDLE;
+    Scene* sc = scene_of(g_adaptive[ad - 1]->scene);
+    if (sc) cudaStreamSynchronize(sc->stream);
+    g_adaptive[ad - 1].reset();
     return RTG_STATUS_OK;
 }
 

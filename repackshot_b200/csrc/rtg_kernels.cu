@@ -32,7 +32,7 @@ __device__ __forceinline__ void wave_slot(const WaveDesc& w, uint32_t slot, uint
         const uint32_t packed = w.epix[e];
         x = packed & 0xffffu;
         y = packed >> 16;
-        index = (w.first + s) * w.ek + j;  // render.rs:376 sub_sample (wrapping)
+        index = ((w.ebase ? __ldg(&w.ebase[e]) : 0u) + w.first + s) * w.ek + j;  // render.rs:376 sub_sample (wrapping)
         return;
     }
     if (w.xys) {

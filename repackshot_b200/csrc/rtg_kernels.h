@@ -39,11 +39,13 @@ struct WaveDesc {
     const SegDev* segs;
     const JobDev* jobs;
     uint32_t nseg, npix;
-    // An edge wave (render.rs:477, E11) when `epix` is set: the k = `ek` samples of each sample
-    // index of `ne` edge pixels (packed x | y << 16): slot ((s ne) + e) k + j holds sample index
-    // (first + s) k + j of pixel e.
+    // A list wave when `epix` is set: the k = `ek` samples of each sample index of `ne` listed
+    // pixels (packed x | y << 16): slot ((s ne) + e) k + j holds sample index (b + first + s) k + j
+    // of pixel e, b = ebase[e] (0 without `ebase`). Edge pixels (render.rs:477, E11) take ek > 1;
+    // the pixels of an adaptive pass (adaptive.rs:471, E10) carry their block's first index in b.
     const uint32_t* epix;
     uint32_t ne, ek;
+    const uint32_t* ebase;
     // A rectangle wave of a scene with edge samples: the image's edge mask (row stride
     // `edge_stride`); its pixels splat from the edge waves, not from this one.
     const uint8_t* edge;

@@ -213,18 +213,21 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (s.floor_mode == 2) { error = "unsupported: shadow catcher floor"; return false; }
         } else if (is("RNDR")) {
             if (!once(seen_render)) return false;
-            uint32_t passes, denoise, photons, adaptive;
-            float radius, strength, threshold;
+            uint32_t passes, denoise, photons;
+            float radius, strength;
             if (!(r.u32(s.width) && r.u32(s.height) && r.u32(s.max_samples) && r.u32(s.seed) && r.f32(s.max_seconds) &&
                   r.f32(s.exposure_ev) && r.u32(s.tonemap) && r.ou32(s.max_depth, 8) && r.of32(s.clamp_indirect, 0) &&
                   r.ou32(passes, 0) && r.ou32(denoise, 0) && r.ou32(photons, 0) && r.of32(radius, 0) && r.of32(strength, 1) &&
-                  r.ou32(s.pixel_filter, 0) && r.ou32(s.edge_supersample, 1) && r.ou32(adaptive, 0) && r.of32(threshold, 0)))
+                  r.ou32(s.pixel_filter, 0) && r.ou32(s.edge_supersample, 1) && r.ou32(s.adaptive, 0) && r.of32(s.noise_threshold, 0)))
                 return false;
-            if (!(threshold >= 0.0f && threshold <= 1.0f)) return r.invalid("noise_threshold must be between 0 and 1");
+            if (!(s.noise_threshold >= 0.0f && s.noise_threshold <= 1.0f)) return r.invalid("noise_threshold must be between 0 and 1");
             if (s.edge_supersample > 16) return r.invalid("edge_supersample must be at most 16");
             if (!(strength >= 0.0f && strength <= 1.0f)) return r.invalid("denoise_strength must be between 0 and 1");
             if (photons > (1u << 22)) return r.invalid("caustic_photons must be at most 4194304");
             if (radius < 0.0f) return r.invalid("caustic_radius must not be negative");
+            // The photon maps of caustics (caustics.rs) are not built: a scene that asks for them is
+            // refused rather than rendered without them.
+            if (photons > 0) { error = "unsupported: caustic photon maps (caustic_photons above 0)"; return false; }
             if (s.width < 1 || s.width > 16384 || s.height < 1 || s.height > 16384)
                 return r.invalid("width and height must be between 1 and 16384");
             if (s.max_seconds < 0.0f || s.clamp_indirect < 0.0f) return r.invalid("max_seconds and clamp_indirect must not be negative");

@@ -102,6 +102,8 @@ struct HScene {
     uint32_t width = 640, height = 360, max_samples = 64, seed = 0, tonemap = 1, max_depth = 8;
     float max_seconds = 0, exposure_ev = 0, clamp_indirect = 0;
     uint32_t pixel_filter = 0, edge_supersample = 1;
+    uint32_t adaptive = 0;        // RNDR.adaptive (E10): bit 0 asks the host for adaptive sampling
+    float noise_threshold = 0;    // RNDR.noise_threshold: the relative error a block stops at (0: none)
 };
 
 // Parses the RSB subset the path tracer reads. Returns false with `error` set (the reference's

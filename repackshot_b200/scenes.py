@@ -135,6 +135,7 @@ class Scene:
     clamp_indirect: float = 0.0
     pixel_filter: int = 0  # 0 standard, 1 none, 2 tent, 3 Blackman-Harris
     edge_supersample: int = 1  # samples per sample index of an edge pixel
+    caustic_photons: int = 0  # photons of the caustic maps a sample index (0: none)
     adaptive: int = 0  # bit 0: the host samples adaptively (E10)
     noise_threshold: float = 0.0  # relative error a block stops at (0: none)
 
@@ -184,7 +185,7 @@ def to_rsb(s: Scene, meshes: bool = True) -> bytes:
                     _f(s.sky_turbidity, s.sun_azimuth_deg, s.sun_elevation_deg, *s.backplate_rect) + _u(s.sky_model)))
     out.append(_sec(b"FLOR", _u(s.floor_mode) + _f(s.floor_z, *s.floor_color)))
     out.append(_sec(b"RNDR", _u(s.width, s.height, s.max_samples, s.seed) + _f(s.max_seconds, s.exposure_ev) +
-                    _u(s.tonemap, s.max_depth) + _f(s.clamp_indirect) + _u(0, 0, 0) + _f(0.0, 1.0) +
+                    _u(s.tonemap, s.max_depth) + _f(s.clamp_indirect) + _u(0, 0, s.caustic_photons) + _f(0.0, 1.0) +
                     _u(s.pixel_filter, s.edge_supersample) +
                     (_u(s.adaptive) + _f(s.noise_threshold) if s.adaptive or s.noise_threshold else b"")))
     return b"".join(out)

@@ -73,6 +73,16 @@ def test_bad_handles_and_null_pointers(rtg):
     assert L.rtg_scene_update(4096, b"RSB1", 4) == rtg.STATUS_BAD_HANDLE
     assert L.rtg_scene_load(None, 0) == 0
     assert rtg.error_message() == "null pointer"
+    # adaptive sampling: null pointers and empty images before any device work
+    planes = (ctypes.c_uint32 * 16)()
+    assert L.rtg_adaptive_decide(8, 8, 0.0, 0.0, 0, planes, None, planes, planes, planes) == rtg.STATUS_NULL_POINTER
+    assert L.rtg_adaptive_decide(0, 8, 0.0, 0.0, 0, planes, planes, planes, planes, planes) == rtg.STATUS_BAD_TILE
+    assert L.rtg_render_block_rgba(4096, 0, 0, 1, 1, 0, 0, None) == rtg.STATUS_NULL_POINTER
+    assert L.rtg_render_block_rgba(4096, 0, 0, 1, 1, 0, 0, out) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_adaptive_create(4096, 1, 0) == 0
+    assert L.rtg_adaptive_run(4096, 16, 0, None, None) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_adaptive_state(0, planes) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_adaptive_free(4096) == rtg.STATUS_BAD_HANDLE
 
 
 def test_malformed_scenes_are_refused_with_a_message(rtg, example_rsb):
@@ -87,6 +97,7 @@ def test_malformed_scenes_are_refused_with_a_message(rtg, example_rsb):
     (lambda s: setattr(s, "floor_mode", 2), "shadow catcher"),
     (lambda s: setattr(s.materials[0], "bevel_mm", 1.0), "bevel"),
     (lambda s: setattr(s.materials[0], "abbe", 30.0) or setattr(s.materials[0], "transmission", 1.0), "dispersive"),
+    (lambda s: setattr(s, "caustic_photons", 100000), "caustic photon maps"),
 ])
 def test_features_outside_the_path_are_refused(rtg, change, words):
     from repackshot_b200 import scenes
