@@ -173,6 +173,39 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def adaptive_comparison(rtg, scene, dist, world, target, uniform_ms):
+    """The frame rendered adaptively (E10): the product scene with a noise target and its 64 spp as
+    the cap, updated into the loaded scene (same geometry), to convergence, a pass a round.
+    Wall time around the synchronous run, max over ranks; its pixel-samples against the uniform
+    frame's, and its throughput against the uniform frame's time."""
+    from repackshot_b200 import scenes, shards
+    s = scenes.product_scene(width=WIDTH, height=HEIGHT, spp=SPP, depth=DEPTH)
+    s.adaptive, s.noise_threshold = 1, target
+    scene.update(scenes.to_rsb(s, meshes=False))
+    film = scene.film()
+    warm = rtg.Adaptive(scene, film, 2)  # warm-up: the kernels of a pass and of a decision
+    warm.run(2)
+    warm.close()
+    film.clear()
+    ad = rtg.Adaptive(scene, film, SPP)
+    scene.synchronize()
+    t0 = time.perf_counter()
+    passes, rays = ad.run(0)
+    scene.synchronize()
+    dt = shards.max_over_ranks(time.perf_counter() - t0, dist)
+    st = ad.state()
+    samples, _ = ad.counts()
+    per_pixel = np.repeat(np.repeat(samples, 8, 0), 8, 1)[:HEIGHT, :WIDTH]
+    paths = int(per_pixel.astype(np.int64).sum())
+    ad.close()
+    return {"noise_target": target, "cap": SPP, "passes": passes, "decisions": st["decisions"], "converged": bool(st["converged"]),
+            "samples_lo_hi": [st["lo"], st["hi"]], "paths_per_gpu": paths, "pixel_samples_vs_uniform": paths / (WIDTH * HEIGHT * SPP),
+            "ms": dt * 1e3, "mpaths_s": world * paths / dt / 1e6, "uniform_frame_ms": uniform_ms,
+            "last_max_error": float(np.frombuffer(np.uint32(st["last"][4]).tobytes(), np.float32)[0]),
+            "path": "rtg_adaptive_create + rtg_adaptive_run (first round: the progressive renderer over the image; later "
+                    "rounds: list waves over the active 8x8 blocks; block errors on the device, the choice on the host)"}
+
+
 def batched_comparison(rtg, scene, spp_scale, dist, world):
     """The metric's plain-vs-batched half: the 64 camera x light-rig jobs of uneven resolution and
     spp on this scene's geometry, rendered back to back through the plain path (rtg_scene_update +
@@ -329,6 +362,7 @@ def run_ours(args, world, rank, local, dist):
     e2e_local = shards.max_over_ranks(time.perf_counter() - t0, dist)
     e2e_value = world * e2e_steps * paths_step / e2e_local / 1e6
     img = film.resolve()
+    adaptive = adaptive_comparison(rtg, scene, dist, world, args.adaptive_target, total_ms / args.steps) if args.adaptive_target > 0 else None
     # The metric's other halves (0 leaves a section out, e.g. for a profiler's launch list).
     batched = batched_comparison(rtg, scene, args.batched_spp_scale, dist, world) if args.batched_spp_scale > 0 else None
     adjoint = adjoint_comparison(rtg, dist, world, args.fit_iterations) if args.fit_iterations > 0 else None
@@ -389,6 +423,7 @@ def run_ours(args, world, rank, local, dist):
         "image_mean": float(img.mean()),
         "batched": batched,
         "adjoint": adjoint,
+        "adaptive": adaptive,
     }
     print(json.dumps(line), flush=True)
 
@@ -403,6 +438,8 @@ def main():
     ap.add_argument("--fit-iterations", type=int, default=200, help="adjoint fit iterations of the differentiable workload")
     ap.add_argument("--batched-spp-scale", type=float, default=0.25,
                     help="spp of the batched-queue comparison's 64 jobs, as a fraction of theirs (1: the full 6.5 G paths)")
+    ap.add_argument("--adaptive-target", type=float, default=0.02,
+                    help="noise target of the adaptive-sampling comparison (0 leaves it out)")
     args = ap.parse_args()
     if args.impl == "reference":
         # The CPU reference runs on rank 0 alone; the other ranks have no work.

@@ -260,7 +260,8 @@ uint32_t rtg_render_block_rgba(uint32_t handle, uint32_t x, uint32_t y, uint32_t
 uint32_t rtg_adaptive_create(uint32_t scene, uint32_t film, uint32_t cap);
 /* Runs the host loop of an adaptive render (adaptive/tests.rs:311): at the end of a round decides
  * the next (block errors on the GPU from the film where it lies); renders passes of at most `pass`
- * samples (0: 16) of the round, the first round over the whole image, later ones over the pixels
+ * samples of the round (0: the whole round, the fewest and largest waves), the first round over
+ * the whole image, later ones over the pixels
  * of the active blocks only; stops when converged or after `max_passes` passes (0: no limit).
  * `passes` and `rays` (may be null) get the passes rendered and the rays cast. The film is the
  * same for any `pass` and any split into calls. */

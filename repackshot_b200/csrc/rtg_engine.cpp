@@ -77,6 +77,7 @@ struct Scene {
     // edge samples (E11): the image's edge mask, its centre-ray scratch and an edge-pixel list
     DevBuf edge_mem;
     bool edges_ready = false;
+    uint64_t edge_builds = 0;  // masks built so far: what depends on the mask checks it
     cudaStream_t stream = nullptr;
     // path buffers
     PathBuffers P{};
@@ -391,6 +392,7 @@ uint32_t edge_mask_of(Scene& sc, const uint8_t*& mask, uint32_t*& list, uint32_t
         RTG_CHECK(launch_edge_mask(sc.S, sc.d_lights, exact, m, sc.stream, grid_for(npix, 128)));
         sc.launches += 2;
         sc.edges_ready = true;
+        sc.edge_builds += 1;
     }
     mask = m;
     return RTG_STATUS_OK;
@@ -540,6 +542,10 @@ struct AdaptiveRun {
     uint32_t round = 0, done = 0, iteration = 0, cap = 0, decisions = 0;
     float target = 0.0f, floor = 0.0f;
     AdDecision last;
+    // per block: its plain and its edge pixels, for the edge factor and mask they were found with
+    std::vector<uint32_t> pixels;
+    uint32_t pixels_k = 0;
+    uint64_t pixels_mask = 0;
     DevBuf mem;
     uint32_t* d_counts = nullptr;
     float* d_error = nullptr;
@@ -617,11 +623,24 @@ uint32_t adaptive_pass(Scene& sc, const Film& f, AdaptiveRun& a, uint32_t count,
         const uint32_t st = edge_mask_of(sc, mask, l, c);
         if (st) return st;
     }
-    RTG_CHECK(launch_block_pixels(mask, a.width, a.height, a.d_pixels, sc.stream, grid_for((uint32_t)nb, 128)));
-    sc.launches += 1;
-    std::vector<uint32_t> pixels(2 * nb);
-    RTG_CHECK(cudaMemcpyAsync(pixels.data(), a.d_pixels, nb * 8, cudaMemcpyDeviceToHost, sc.stream));
-    RTG_CHECK(cudaStreamSynchronize(sc.stream));
+    // Each block's plain and edge pixels: its size inside the image without edge samples, else
+    // counted on the device once per edge mask.
+    if (a.pixels.size() != 2 * nb || a.pixels_k != k || (k > 1 && a.pixels_mask != sc.edge_builds)) {
+        a.pixels.assign(2 * nb, 0);
+        if (k > 1) {
+            RTG_CHECK(launch_block_pixels(mask, a.width, a.height, a.d_pixels, sc.stream, grid_for((uint32_t)nb, 128)));
+            sc.launches += 1;
+            RTG_CHECK(cudaMemcpyAsync(a.pixels.data(), a.d_pixels, nb * 8, cudaMemcpyDeviceToHost, sc.stream));
+            RTG_CHECK(cudaStreamSynchronize(sc.stream));
+        } else {
+            for (size_t b = 0; b < nb; ++b)
+                a.pixels[2 * b] = std::min(AD_BLOCK, a.width - (uint32_t)(b % a.cols) * AD_BLOCK) *
+                                  std::min(AD_BLOCK, a.height - (uint32_t)(b / a.cols) * AD_BLOCK);
+        }
+        a.pixels_k = k;
+        a.pixels_mask = sc.edge_builds;
+    }
+    const std::vector<uint32_t>& pixels = a.pixels;
     std::vector<std::pair<uint32_t, uint32_t>> order;  // (quota, block)
     for (size_t b = 0; b < nb; ++b) {
         const uint32_t q = a.quota(b);
@@ -1483,7 +1502,7 @@ uint32_t rtg_adaptive_run(uint32_t ad, uint32_t pass, uint32_t max_passes, uint3
         g_error = "rtg_adaptive_run: the scene's image size changed since rtg_adaptive_create";
         return RTG_STATUS_BAD_SCENE;
     }
-    if (pass == 0) pass = AD_ROUND;
+    if (pass == 0) pass = UINT32_MAX;  // a whole round a pass: the fewest, largest waves
     uint32_t passes = 0;
     uint64_t total = 0;
     for (;;) {  // adaptive/tests.rs:311

@@ -106,7 +106,7 @@ def assert_same_film(gpu, oracle):
         assert np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
 
 
-@pytest.mark.parametrize("pass_samples, single, capacity", [(16, False, 0), (5, False, 0), (3, True, 0), (16, False, 700)])
+@pytest.mark.parametrize("pass_samples, single, capacity", [(16, False, 0), (0, False, 0), (5, False, 0), (3, True, 0), (16, False, 700)])
 def test_adaptive_film_is_the_oracle_film(rtg, example_oracle, pass_samples, single, capacity):
     rsb, (rgb, w, al, l2, counts, (lo, hi, decisions, _)) = example_oracle
     (grgb, gw, gal, gl2), samples, st = gpu_adaptive(rtg, rsb, 96, pass_samples, single, capacity)
