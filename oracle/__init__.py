@@ -62,6 +62,10 @@ def lib():
             "orc_adaptive_decide": (u32, [u32, u32, ctypes.c_float, ctypes.c_float, u32, v, v, v, v, v]),
             "orc_adaptive_film": (u32, [u32, u32, u32, u32, v, v, v, v, v, v]),
             "orc_pixel_error": (ctypes.c_float, [ctypes.c_float] * 4 + [u32, ctypes.c_float]),
+            "orc_render_passes": (u32, [u32, u32, u32, u32, u32, v, v, v, v]),
+            "orc_render_albedo": (u32, [u32, u32, u32, u32, u32, u32, v]),
+            "orc_denoise": (u32, [u32, ctypes.c_float, u32, u32, u32, u32, u32, u32, u32, v, u32, v]),
+            "orc_denoise_halo": (u32, [u32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -190,6 +194,35 @@ class OracleScene:
         return (rgb.reshape(h, w, 3), wt.reshape(h, w), al.reshape(h, w), l2.reshape(h, w), counts.reshape(rows, cols),
                 tuple(int(v) for v in st))
 
+    def passes(self, x=0, y=0, w=None, h=None):
+        """The exact passes of the rectangle's centre rays (rt_render_tile_passes): normal (h, w, 3),
+        depth, part id, material id (h, w)."""
+        w = self.width if w is None else w
+        h = self.height if h is None else h
+        normal, depth = np.zeros((h, w, 3), np.float32), np.zeros((h, w), np.float32)
+        part, material = np.zeros((h, w), np.uint32), np.zeros((h, w), np.uint32)
+        lib().orc_render_passes(self.handle, x, y, w, h, _p(normal), _p(depth), _p(part), _p(material))
+        return normal, depth, part, material
+
+    def albedo(self, sample, x=0, y=0, w=None, h=None):
+        """The albedo of sample `sample` of the rectangle (rt_render_tile_albedo): (h, w, 3)."""
+        w = self.width if w is None else w
+        h = self.height if h is None else h
+        out = np.zeros((h, w, 3), np.float32)
+        lib().orc_render_albedo(self.handle, x, y, w, h, sample, _p(out))
+        return out
+
+    def guides(self, samples):
+        """The denoiser's guides of the whole image (rt-post denoise/tests.rs:338): the albedo
+        summed over samples 0..samples in order and divided as Film::resolve divides, and the
+        exact passes."""
+        acc = np.zeros((self.height, self.width, 3), np.float32)
+        for s in range(samples):
+            acc = (acc + self.albedo(s)).astype(np.float32)
+        albedo = (acc * (np.float32(1.0) / np.float32(samples))).astype(np.float32) if samples else acc
+        normal, depth, part, material = self.passes()
+        return albedo, normal, depth, part, material
+
     def occluded(self, rays):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
         out = np.zeros(len(rays), np.uint8)
@@ -250,6 +283,33 @@ def adaptive_decide(width, height, ev, target, cap, counts, sums, lum2):
     if st:
         raise ValueError(f"status {st}")
     return active[:cols * rows], words
+
+
+def denoise_words(sums_rgba, lum2, albedo, normal, depth, part, material, counts=None):
+    """The denoiser's input (rt-wasm/src/lib.rs:420): the planes one after another as u32 words."""
+    planes = [np.ascontiguousarray(a, np.float32).reshape(-1).view(np.uint32) for a in (sums_rgba, lum2, albedo, normal, depth)]
+    planes += [np.ascontiguousarray(a, np.uint32).reshape(-1) for a in (part, material)]
+    if counts is not None:
+        planes.append(np.ascontiguousarray(counts, np.float32).reshape(-1).view(np.uint32))
+    return np.concatenate(planes)
+
+
+def denoise(words, width, height, samples, preset=0, strength=1.0, origin_y=0, rows=None, y0=None, y1=None):
+    """rt_denoise_with: the denoised RGBA sums of rows y0..y1 of the band (float32, (y1 - y0) * width * 4)."""
+    rows = height if rows is None else rows
+    y0 = origin_y if y0 is None else y0
+    y1 = origin_y + rows if y1 is None else y1
+    words = np.ascontiguousarray(words, np.uint32)
+    per_pixel = words.size // max(width * rows, 1)
+    out = np.zeros(max((y1 - y0) * width * 4, 1), np.float32)
+    st = lib().orc_denoise(preset, float(strength), width, height, origin_y, rows, samples, y0, y1, _p(words), per_pixel, _p(out))
+    if st:
+        raise ValueError(f"status {st}")
+    return out[:(y1 - y0) * width * 4]
+
+
+def denoise_halo(preset):
+    return int(lib().orc_denoise_halo(preset))
 
 
 def pixel_error(r, g, b, lum2, n, floor):

@@ -444,6 +444,26 @@ static float filter_offset(uint32_t filter, float u) {  // pixel_filter.rs:103
     return u;
 }
 
+// The camera ray of sample `index` of pixel (x, y) (render.rs:79 camera_sample_weighted); (u, v)
+// its screen position.
+static Ray sample_ray(const Scene& scene, const PixelSampler& sampler, uint32_t x, uint32_t y, float& u, float& v) {
+    uint32_t width = scene.render.width ? scene.render.width : 1, height = scene.render.height ? scene.render.height : 1;
+    float aspect = (float)width / (float)height;
+    float du, dv;
+    sampler.get2(DIM_CAMERA, du, dv);
+    du = filter_offset(scene.render.pixel_filter, du);
+    dv = filter_offset(scene.render.pixel_filter, dv);
+    u = ((float)x + du) / (float)width;
+    v = ((float)y + dv) / (float)height;
+    float lx = 0.0f, ly = 0.0f;
+    if (scene.camera.lens_radius() > 0.0f) {
+        float a, b;
+        sampler.get2(DIM_LENS, a, b);
+        concentric_disk(a, b, lx, ly);
+    }
+    return scene.camera.generate_ray(aspect, u, v, lx, ly);
+}
+
 // camera_sample_weighted (render.rs:79) and the shade of render_tile_traced (render.rs:388).
 static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, uint32_t y, uint32_t index, Rgb& c,
                         float& alpha, PathStats& st) {
@@ -469,8 +489,23 @@ static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, ui
 // The exact passes of a centre ray (passes.rs:168) that the edge mask compares: part and
 // material ids (instance or material + 1, FLOOR_ID for the floor, 0 for the background) and the
 // depth along the view axis.
-struct Exact { uint32_t part = 0, material = 0; float depth = F_INF; };
+struct Exact { uint32_t part = 0, material = 0; float depth = F_INF; Vec3 normal; };
 constexpr uint32_t FLOOR_ID = 0xffffffffu;
+// first_hit (integrator/mod.rs:911) for the albedo pass (passes.rs:209 albedo_of): the base colour
+// of the material of what the ray met (the default material's for an index out of range), the
+// floor's colour, black for the background.
+static Rgb first_albedo(const Scene& scene, const Prepared& prep, const Ray& ray) {
+    RayHit hit;
+    bool got = scene.geometry.trace(ray, true, hit, nullptr);
+    float t_geometry = got ? hit.t : F_INF;
+    float t_floor = prep.floor_t(ray, true);
+    float t_nearest = rmin(t_geometry, t_floor);
+    if (t_nearest == F_INF || prep.lights.camera_sees_panel(ray, t_nearest)) return BLACK;
+    if (t_floor < t_geometry) return scene.floor.color;
+    Hit d;
+    if (!scene.geometry.hit_details(ray, hit, d)) return BLACK;
+    return prep.material(scene, d.instance).base_color;
+}
 // render.rs:503 centre_ray and integrator/mod.rs:911 first_hit, as Exact::of reads them.
 static Exact centre_exact(const Scene& scene, const Prepared& prep, uint32_t x, uint32_t y) {
     uint32_t width = scene.render.width ? scene.render.width : 1, height = scene.render.height ? scene.render.height : 1;
@@ -486,10 +521,12 @@ static Exact centre_exact(const Scene& scene, const Prepared& prep, uint32_t x, 
     float t;
     if (t_floor < t_geometry) {
         e.part = e.material = FLOOR_ID;
+        e.normal = Vec3(0.0f, 0.0f, ray.dir.z < 0.0f ? 1.0f : -1.0f);
         t = t_floor;
     } else {
         Hit d;
         if (!scene.geometry.hit_details(ray, hit, d)) return e;
+        e.normal = d.normal;
         e.part = d.instance + 1;
         uint32_t m = scene.geometry.instances[d.instance].material_id;
         e.material = m < scene.materials.size() ? m + 1 : 0;
@@ -723,6 +760,58 @@ uint64_t orc_render_film(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint3
         std::memcpy(stats11, v, sizeof(v));
     }
     return rays;
+}
+
+// rt_render_tile_passes (rt-wasm/src/lib.rs:484, render.rs:515 render_tile_exact): the exact passes
+// of the rectangle's centre rays, background outside the image: normal (3 a pixel), depth, part
+// id and material id (each may be null).
+uint32_t orc_render_passes(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint32_t hh, float* normal, float* depth, uint32_t* part,
+                           uint32_t* material) {
+    Loaded* l = get(h);
+    if (!l) return 1;
+    const uint32_t W = l->scene.render.width, H = l->scene.render.height;
+    for (uint32_t y = 0; y < hh; ++y)
+        for (uint32_t x = 0; x < w; ++x) {
+            const size_t i = (size_t)y * w + x;
+            Exact e;
+            if ((uint64_t)x0 + x < W && (uint64_t)y0 + y < H) e = centre_exact(l->scene, l->prep, x0 + x, y0 + y);
+            if (normal) { normal[3 * i] = e.normal.x; normal[3 * i + 1] = e.normal.y; normal[3 * i + 2] = e.normal.z; }
+            if (depth) depth[i] = e.depth;
+            if (part) part[i] = e.part;
+            if (material) material[i] = e.material;
+        }
+    return 0;
+}
+
+// rt_render_tile_albedo (rt-wasm/src/lib.rs:510, render.rs:590): the albedo of sample `index` of
+// the rectangle's pixels, 3 floats a pixel (0 outside the image); an edge pixel gives the mean of
+// its k sub-samples.
+uint32_t orc_render_albedo(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint32_t hh, uint32_t index, float* out) {
+    Loaded* l = get(h);
+    if (!l || !out) return 1;
+    const Scene& sc = l->scene;
+    const uint32_t W = sc.render.width, H = sc.render.height;
+    const uint32_t k = sc.render.edge_supersample < 1 ? 1 : (sc.render.edge_supersample > 16 ? 16 : sc.render.edge_supersample);
+    for (uint32_t y = 0; y < hh; ++y)
+        for (uint32_t x = 0; x < w; ++x) {
+            const size_t i = (size_t)y * w + x;
+            Rgb a = BLACK;
+            const uint32_t px = x0 + x, py = y0 + y;
+            if ((uint64_t)x0 + x < W && (uint64_t)y0 + y < H) {
+                const bool edge = k > 1 && !l->edges.empty() && l->edges[(size_t)py * W + px];
+                float u, v;
+                if (!edge) {
+                    a = first_albedo(sc, l->prep, sample_ray(sc, PixelSampler(sc.render.seed, px, py, index), px, py, u, v));
+                } else {
+                    Rgb sum = BLACK;
+                    for (uint32_t j = 0; j < k; ++j)
+                        sum = sum + first_albedo(sc, l->prep, sample_ray(sc, PixelSampler(sc.render.seed, px, py, index * k + j), px, py, u, v));
+                    a = sum * (1.0f / (float)k);
+                }
+            }
+            out[3 * i] = a.r; out[3 * i + 1] = a.g; out[3 * i + 2] = a.b;
+        }
+    return 0;
 }
 
 // E10 (adaptive/tests.rs:294 adaptive_film, a scene without photon maps): renders scene `h`

@@ -15,7 +15,9 @@ its path tracer, read from the reference's own source tree (run where it is chec
   hand-written test profiles it carries (tests/fixtures/ies/*.ies), written to
   tests/golden/ies_profiles.json;
 * the hash of six adaptive-sampling decisions of the synthetic 45 x 37 image
-  (engine/crates/rt-core/src/adaptive/tests.rs:497-534).
+  (engine/crates/rt-core/src/adaptive/tests.rs:497-534);
+* the hashes of the denoised example: the full filter at 4 spp and the viewport's at 2 and 4 spp
+  (engine/crates/rt-post/src/denoise/tests.rs:392, 527-528).
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -40,6 +42,7 @@ def pinned(src: str, name: str) -> int:
 
 def main():
     render = (CORE / "render.rs").read_text()
+    denoise = (REF / "engine" / "crates" / "rt-post" / "src" / "denoise" / "tests.rs").read_text()
     rng = (CORE / "rng.rs").read_text()
     sampler = (CORE / "sampler.rs").read_text()
     table = (CORE / "bsdf" / "energy_table.rs").read_text()
@@ -90,6 +93,8 @@ def main():
         "l5_rsb": {"bytes": len(l5), "sha256": hashlib.sha256(l5).hexdigest()},
         "blackman_harris_inv_cdf": {"count": len(bh), "sha256": hashlib.sha256(bh_raw).hexdigest()},
         "e10_synthetic_decisions": pinned((CORE / "adaptive" / "tests.rs").read_text(), "PINNED_E10_DECISIONS"),
+        "denoised": {k: pinned(denoise, "PINNED_DENOISED_" + k.upper()) for k in
+                     ("example_4spp", "viewport_example_2spp", "viewport_example_4spp")},
     }
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     print(OUT)
