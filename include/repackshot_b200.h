@@ -28,6 +28,7 @@ extern "C" {
 #define RTG_STATUS_BAD_TILE 2u      /* empty tile or more than RTG_MAX_TILE_PIXELS pixels */
 #define RTG_STATUS_NULL_POINTER 3u
 #define RTG_STATUS_BAD_SCENE 4u
+#define RTG_STATUS_BAD_DENOISE 5u   /* the denoiser's preset, sizes, band or halo do not fit */
 #define RTG_STATUS_CUDA_ERROR 16u   /* the message is in rtg_scene_error_* */
 #define RTG_STATUS_STACK_OVERFLOW 17u
 #define RTG_STATUS_BAD_FILM 18u
@@ -274,6 +275,42 @@ uint32_t rtg_adaptive_state(uint32_t ad, uint32_t* out16);
  * either pointer may be null, not both. */
 uint32_t rtg_adaptive_counts(uint32_t ad, uint32_t* samples, uint8_t* active);
 uint32_t rtg_adaptive_free(uint32_t ad);
+
+/* ---- Guide passes and the denoiser (rt-post/src/denoise.rs, rt-core/src/passes.rs) ----------------
+ * rt_render_tile_passes (rt-wasm/src/ffi.rs:303-343, lib.rs:484): the exact passes of `mask`
+ * (normal 2, depth 4, part id 8, material id 16, circle of confusion 32; the albedo bit 1, the
+ * alpha bit 64 and unknown bits are ignored) of the rectangle (x, y, w, h), from one ray through
+ * each pixel's centre: the planes one after another in that order, w*h*3 words for the normal and
+ * w*h for the others (f32; u32 for the ids), rows from the top. Status as rtg_render_tile. */
+uint32_t rtg_render_tile_passes(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t mask, uint8_t* out);
+/* rt_render_tile_albedo (ffi.rs:345-384, lib.rs:510): the albedo of sample `sample_index` of the
+ * rectangle's pixels, w*h*3 floats: the base colour of what that sample's camera ray met first
+ * (0 for the background and outside the image; an edge pixel's mean over its sub-samples). */
+uint32_t rtg_render_tile_albedo(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index, float* out);
+/* rt_denoise / rt_denoise_with (ffi.rs:599-683, lib.rs:420-475): the denoiser on a band of `rows`
+ * image rows from `origin_y` of a width x height image of `samples` samples a pixel. `in` holds
+ * width*rows*14 little-endian words: the planes sums (RGBA), lum2, albedo (3), normal (3), depth,
+ * part id and material id, one after another. Writes the denoised RGBA sums of image rows y0 .. y1
+ * (width*(y1-y0)*4 floats) to `out`. `preset` 0 is the full filter, 1 the viewport's; `strength`
+ * (0..1, NaN: 1) blends noisy x (1 - s) + denoised x s per colour channel, and at 0 no filter runs.
+ * RTG_STATUS_NULL_POINTER, or RTG_STATUS_BAD_DENOISE when the preset, the sizes, the band or its
+ * halo do not fit. The filter runs on the GPU with the reference's bits. */
+uint32_t rtg_denoise(uint32_t width, uint32_t height, uint32_t origin_y, uint32_t rows, uint32_t samples, uint32_t y0, uint32_t y1,
+                     const uint8_t* in, float* out);
+uint32_t rtg_denoise_with(uint32_t preset, float strength, uint32_t width, uint32_t height, uint32_t origin_y, uint32_t rows, uint32_t samples,
+                          uint32_t y0, uint32_t y1, const uint8_t* in, float* out);
+/* rt_denoise_halo (ffi.rs:685-691): rows a band of `preset` holds above and below the rows it
+ * computes (72 for the full filter, 24 for the viewport's), 0 for an unknown preset. */
+uint32_t rtg_denoise_halo(uint32_t preset);
+/* No counterpart in the reference (its hosts render the passes tile by tile and hand the planes
+ * to rt_denoise): the guide passes of a film on the device. Writes the exact passes of the film's
+ * pixels and adds the albedo of samples [first_sample, first_sample + count) to the film's albedo
+ * sums (rtg_film_clear clears them with the film). */
+uint32_t rtg_film_guides(uint32_t scene, uint32_t film, uint32_t first_sample, uint32_t count);
+/* The denoiser on a film that covers the whole image, with its guide passes, as rtg_denoise_with
+ * on the film's planes (`samples` the samples of every pixel): the film stays on the device, and
+ * `out` (may be null: the result stays on the device) gets width*height*4 floats of RGBA sums. */
+uint32_t rtg_film_denoise(uint32_t film, uint32_t preset, float strength, uint32_t samples, float* out);
 
 #ifdef __cplusplus
 }

@@ -76,6 +76,13 @@ ABI = {
     "rtg_adaptive_state": (_u32, [_u32, _f]),
     "rtg_adaptive_counts": (_u32, [_u32, _f, _f]),
     "rtg_adaptive_free": (_u32, [_u32]),
+    "rtg_render_tile_passes": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _f]),
+    "rtg_render_tile_albedo": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _f]),
+    "rtg_denoise": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _u32, _f, _f]),
+    "rtg_denoise_with": (_u32, [_u32, ctypes.c_float, _u32, _u32, _u32, _u32, _u32, _u32, _u32, _f, _f]),
+    "rtg_denoise_halo": (_u32, [_u32]),
+    "rtg_film_guides": (_u32, [_u32, _u32, _u32, _u32]),
+    "rtg_film_denoise": (_u32, [_u32, _u32, ctypes.c_float, _u32, _f]),
 }
 
 
@@ -291,6 +298,21 @@ class Film:
     def clear(self):
         _check(lib().rtg_film_clear(self.handle))
 
+    def guides(self, first: int, count: int):
+        """Renders the film's guide passes: the exact passes, and the albedo of samples
+        [first, first + count) added to its albedo sums (rtg_film_guides)."""
+        _check(lib().rtg_film_guides(self.scene.handle, self.handle, first, count))
+
+    def denoise(self, samples: int, preset: int = 0, strength: float = 1.0, out=None):
+        """The film denoised on the device (rtg_film_denoise): (h, w, 4) RGBA sums; ``out=False``
+        leaves the result on the device and returns None."""
+        if out is False:
+            _check(lib().rtg_film_denoise(self.handle, preset, float(strength), samples, None))
+            return None
+        out = np.zeros((self.h, self.w, 4), np.float32) if out is None else out
+        _check(lib().rtg_film_denoise(self.handle, preset, float(strength), samples, _ptr(out)))
+        return out
+
     def close(self):
         if self.handle:
             lib().rtg_film_free(self.handle)
@@ -325,6 +347,37 @@ def render_block_rgba(handle: int, x: int, y: int, w: int, h: int, sample_index:
     out = np.zeros(w * h * 4, np.float32) if 0 < w * h <= MAX_TILE_PIXELS else np.zeros(0, np.float32)
     status = lib().rtg_render_block_rgba(handle, x, y, w, h, sample_index, iteration, _ptr(out) if out.size else None)
     return status, out
+
+
+STATUS_BAD_DENOISE = 5
+
+
+def denoise(words, width: int, height: int, samples: int, preset: int = 0, strength: float = 1.0, origin_y: int = 0, rows=None,
+            y0=None, y1=None):
+    """rt_denoise_with through rtg_denoise_with: the denoised RGBA sums of rows y0..y1 of the band.
+    ``words`` holds the band's planes as u32 words (14 a pixel)."""
+    rows = height if rows is None else rows
+    y0 = origin_y if y0 is None else y0
+    y1 = origin_y + rows if y1 is None else y1
+    words = np.ascontiguousarray(words, np.uint32)
+    out = np.zeros(max((y1 - y0) * width * 4, 1), np.float32)
+    _check(lib().rtg_denoise_with(preset, float(strength), width, height, origin_y, rows, samples, y0, y1, _ptr(words), _ptr(out)))
+    return out[:(y1 - y0) * width * 4]
+
+
+def tile_passes(handle: int, x: int, y: int, w: int, h: int, mask: int = 0x3E):
+    """rt_render_tile_passes: the planes of ``mask`` as u32 words (status, words)."""
+    per = sum(c for bit, c in ((2, 3), (4, 1), (8, 1), (16, 1), (32, 1)) if mask & bit)
+    out = np.zeros(max(w * h * per, 1), np.uint32)
+    st = lib().rtg_render_tile_passes(handle, x, y, w, h, mask, _ptr(out))
+    return st, out[:w * h * per]
+
+
+def tile_albedo(handle: int, x: int, y: int, w: int, h: int, sample_index: int):
+    """rt_render_tile_albedo: (status, w*h*3 float32)."""
+    out = np.zeros(max(w * h * 3, 1), np.float32)
+    st = lib().rtg_render_tile_albedo(handle, x, y, w, h, sample_index, _ptr(out))
+    return st, out[:w * h * 3]
 
 
 class Adaptive:

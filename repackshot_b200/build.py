@@ -29,7 +29,7 @@ DEVICE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true
 HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-pthread", f"-I{CUDA_HOME}/include"]
 
 HOST_SOURCES = ["rtg_scene.cpp", "rtg_bitmap.cpp", "rtg_ies.cpp", "rtg_tables.cpp", "rtg_energy.cpp", "rtg_adaptive.cpp", "rtg_engine.cpp"]
-DEVICE_SOURCES = ["rtg_kernels.cu", "rtg_noalloc.cu", "rtg_adaptive.cu"]
+DEVICE_SOURCES = ["rtg_kernels.cu", "rtg_noalloc.cu", "rtg_adaptive.cu", "rtg_denoise.cu"]
 
 
 def _run(cmd, log=None):

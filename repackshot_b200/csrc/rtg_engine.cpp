@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -13,6 +14,7 @@
 
 #include "../../include/repackshot_b200.h"
 #include "rtg_adaptive.h"
+#include "rtg_denoise.h"
 #include "rtg_kernels.h"
 #include "rtg_noalloc.h"
 #include "rtg_scene.h"
@@ -115,10 +117,23 @@ struct Film {
     FilmDev dev{};
     DevBuf mem;
     DevBuf encoded;  // the last 8- or 16-bit image, on its way to the host
+    // The denoiser's guide passes (rtg_film_guides): albedo sums (3 a pixel) and their samples,
+    // normal (3), depth, part and material ids; and the denoiser's scratch and result.
+    DevBuf guides;
+    DevBuf denoise;
     ~Film() {
         mem.release();
         encoded.release();
+        guides.release();
+        denoise.release();
     }
+    size_t pixels() const { return (size_t)dev.w * dev.h; }
+    float* albedo_sum() const { return (float*)guides.p; }
+    float* albedo_weight() const { return albedo_sum() + 3 * pixels(); }
+    float* normal() const { return albedo_weight() + pixels(); }
+    float* depth() const { return normal() + 3 * pixels(); }
+    uint32_t* part() const { return (uint32_t*)(depth() + pixels()); }
+    uint32_t* material() const { return part() + pixels(); }
 };
 // A job of a render queue: one variant of the queue's scene (its own camera, image, materials,
 // lights and settings over the scene's geometry), a sample range and the film it renders into.
@@ -827,6 +842,7 @@ uint32_t rtg_film_clear(uint32_t film) {
     if (!f) return RTG_STATUS_BAD_FILM;
     Scene* sc = scene_of(f->scene);
     RTG_CHECK(cudaMemsetAsync(f->mem.p, 0, f->mem.bytes, sc ? sc->stream : 0));
+    if (f->guides.p) RTG_CHECK(cudaMemsetAsync(f->guides.p, 0, f->guides.bytes, sc ? sc->stream : 0));
     if (sc) RTG_CHECK(cudaStreamSynchronize(sc->stream));
     return RTG_STATUS_OK;
 }
@@ -1556,6 +1572,224 @@ uint32_t rtg_adaptive_counts(uint32_t ad, uint32_t* samples, uint8_t* active) {
         if (active) active[b] = a->active[b];
     }
     return RTG_STATUS_OK;
+}
+
+// ---- guide passes and the denoiser (rt-post/src/denoise.rs) -----------------------------------------
+uint32_t rtg_render_tile_passes(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t mask, uint8_t* out) {
+    if (!out) return RTG_STATUS_NULL_POINTER;
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    const uint64_t px = (uint64_t)w * h;
+    if (px == 0 || px > RTG_MAX_TILE_PIXELS) return RTG_STATUS_BAD_TILE;
+    DevBuf m;
+    struct Release { DevBuf& b; ~Release() { b.release(); } } release{m};
+    m.bytes = px * 24;
+    RTG_CHECK(cudaMalloc(&m.p, m.bytes));
+    float* normal = (float*)m.p;
+    float* depth = normal + 3 * px;
+    uint32_t* part = (uint32_t*)(depth + px);
+    uint32_t* material = part + px;
+    RTG_CHECK(launch_exact_passes(sc->S, sc->d_lights, x, y, w, h, normal, depth, part, material, sc->stream, grid_for((uint32_t)px, 128)));
+    sc->launches += 1;
+    std::vector<uint32_t> host(px * 6);
+    RTG_CHECK(cudaMemcpyAsync(host.data(), m.p, px * 24, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    // The planes of `mask` in the order normal, depth, part id, material id, circle of confusion
+    // (passes.rs:475 planes); the albedo and alpha bits and unknown bits are ignored.
+    size_t o = 0;
+    auto put = [&](const void* src, size_t words) {
+        std::memcpy(out + o, src, words * 4);
+        o += words * 4;
+    };
+    if (mask & 2u) put(host.data(), 3 * px);
+    if (mask & 4u) put(host.data() + 3 * px, px);
+    if (mask & 8u) put(host.data() + 4 * px, px);
+    if (mask & 16u) put(host.data() + 5 * px, px);
+    if (mask & 32u) {  // passes.rs:130 coc_diameter
+        std::vector<float> coc(px, 0.0f);
+        const SceneDev& S = sc->S;
+        const uint32_t long_side = std::max<uint32_t>(std::max(sc->width, sc->height), 1);
+        for (size_t i = 0; i < px; ++i) {
+            float depth_v;
+            std::memcpy(&depth_v, &host[3 * px + i], 4);
+            if (S.lens_radius <= 0.0f || !(depth_v > 0.0f && std::isfinite(depth_v))) continue;
+            const float aperture = S.lens_radius * 2.0f;  // focal / fstop, exactly
+            const float on_focus_plane = aperture * std::fabs(depth_v - S.focus_dist) / depth_v;
+            const float pixel_on_focus_plane = S.sensor_mm / (float)long_side * (S.focus_dist / S.focal_mm);
+            coc[i] = on_focus_plane / pixel_on_focus_plane;
+        }
+        put(coc.data(), px);
+    }
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_render_tile_albedo(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index, float* out) {
+    if (!out) return RTG_STATUS_NULL_POINTER;
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    const uint64_t px = (uint64_t)w * h;
+    if (px == 0 || px > RTG_MAX_TILE_PIXELS) return RTG_STATUS_BAD_TILE;
+    const uint8_t* mask = nullptr;
+    if (sc->S.edge_k > 1) {
+        uint32_t *l = nullptr, *c = nullptr;
+        const uint32_t st = edge_mask_of(*sc, mask, l, c);
+        if (st) return st;
+    }
+    DevBuf m;
+    struct Release { DevBuf& b; ~Release() { b.release(); } } release{m};
+    m.bytes = px * 16;
+    RTG_CHECK(cudaMalloc(&m.p, m.bytes));
+    RTG_CHECK(cudaMemsetAsync(m.p, 0, m.bytes, sc->stream));
+    float* sum = (float*)m.p;
+    RTG_CHECK(launch_albedo_pass(sc->S, sc->d_lights, mask, x, y, w, h, sample_index, 1, sum, sum + 3 * px, sc->stream,
+                                 grid_for((uint32_t)px, 128)));
+    sc->launches += 1;
+    RTG_CHECK(cudaMemcpyAsync(out, sum, px * 12, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_film_guides(uint32_t scene, uint32_t film, uint32_t first_sample, uint32_t count) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(scene);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    Film* f = film_of(film);
+    if (!f || f->scene != scene) return RTG_STATUS_BAD_FILM;
+    const size_t n = f->pixels();
+    if (!f->guides.p) {
+        f->guides.bytes = n * 10 * 4;
+        RTG_CHECK(cudaMalloc(&f->guides.p, f->guides.bytes));
+        RTG_CHECK(cudaMemsetAsync(f->guides.p, 0, f->guides.bytes, sc->stream));
+    }
+    const uint8_t* mask = nullptr;
+    if (sc->S.edge_k > 1) {
+        uint32_t *l = nullptr, *c = nullptr;
+        const uint32_t st = edge_mask_of(*sc, mask, l, c);
+        if (st) return st;
+    }
+    const FilmDev& d = f->dev;
+    RTG_CHECK(launch_exact_passes(sc->S, sc->d_lights, d.ox, d.oy, d.w, d.h, f->normal(), f->depth(), f->part(), f->material(), sc->stream,
+                                  grid_for((uint32_t)n, 128)));
+    if (count)
+        RTG_CHECK(launch_albedo_pass(sc->S, sc->d_lights, mask, d.ox, d.oy, d.w, d.h, first_sample, count, f->albedo_sum(), f->albedo_weight(),
+                                     sc->stream, grid_for((uint32_t)n, 128)));
+    sc->launches += count ? 2 : 1;
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    return RTG_STATUS_OK;
+}
+
+namespace {
+float strength_of(float s) { return std::isnan(s) ? 1.0f : (s < 0.0f ? 0.0f : (s > 1.0f ? 1.0f : s)); }  // denoise.rs:386
+}  // namespace
+
+uint32_t rtg_film_denoise(uint32_t film, uint32_t preset, float strength, uint32_t samples, float* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Film* f = film_of(film);
+    if (!f) return RTG_STATUS_BAD_FILM;
+    Scene* sc = scene_of(f->scene);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (preset > 1) return RTG_STATUS_BAD_DENOISE;
+    if (!f->guides.p) { g_error = "rtg_film_denoise: the film has no guide passes (rtg_film_guides)"; return RTG_STATUS_BAD_FILM; }
+    if (f->dev.ox || f->dev.oy || f->dev.w != sc->width || f->dev.h != sc->height) {
+        g_error = "rtg_film_denoise: the film must cover the whole image";
+        return RTG_STATUS_BAD_FILM;
+    }
+    const size_t n = f->pixels();
+    const size_t need = dn_scratch_bytes(n) + n * 16;
+    if (f->denoise.bytes < need) {
+        f->denoise.release();
+        RTG_CHECK(cudaMalloc(&f->denoise.p, need));
+        f->denoise.bytes = need;
+    }
+    float* result = (float*)((uint8_t*)f->denoise.p + dn_scratch_bytes(n));
+    const float s = strength_of(strength);
+    const FilmDev& d = f->dev;
+    if (s > 0.0f) {
+        const DnSrc src{d.rgb, 3, d.alpha, 1, d.lum2, f->albedo_sum(), f->albedo_weight(), f->normal(), f->depth(), f->part(), f->material(),
+                        nullptr};
+        RTG_CHECK(denoise_band(src, d.w, d.h, samples, dn_preset(preset), f->denoise.p, result, sc->stream, grid_for((uint32_t)n, 256),
+                               sc->launches));
+    }
+    if (out) {
+        std::vector<float> rgb, alpha;
+        if (s < 1.0f) {  // the noisy sums, for strength 0 and the blend (denoise.rs:396)
+            rgb.resize(3 * n);
+            alpha.resize(n);
+            RTG_CHECK(cudaMemcpyAsync(rgb.data(), d.rgb, n * 12, cudaMemcpyDeviceToHost, sc->stream));
+            RTG_CHECK(cudaMemcpyAsync(alpha.data(), d.alpha, n * 4, cudaMemcpyDeviceToHost, sc->stream));
+        }
+        if (s > 0.0f) RTG_CHECK(cudaMemcpyAsync(out, result, n * 16, cudaMemcpyDeviceToHost, sc->stream));
+        RTG_CHECK(cudaStreamSynchronize(sc->stream));
+        if (s <= 0.0f) {
+            for (size_t p = 0; p < n; ++p) {
+                for (int k = 0; k < 3; ++k) out[4 * p + k] = rgb[3 * p + k];
+                out[4 * p + 3] = alpha[p];
+            }
+        } else if (s < 1.0f) {
+            const float k1 = 1.0f - s;
+            for (size_t p = 0; p < n; ++p)
+                for (int k = 0; k < 3; ++k) out[4 * p + k] = rgb[3 * p + k] * k1 + out[4 * p + k] * s;
+        }
+    } else {
+        RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    }
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_denoise_halo(uint32_t preset) { return preset > 1 ? 0u : dn_halo(dn_preset(preset)); }
+
+uint32_t rtg_denoise_with(uint32_t preset, float strength, uint32_t width, uint32_t height, uint32_t origin_y, uint32_t rows, uint32_t samples,
+                          uint32_t y0, uint32_t y1, const uint8_t* in, float* out) {
+    if (!in || !out) return RTG_STATUS_NULL_POINTER;
+    if (preset > 1) return RTG_STATUS_BAD_DENOISE;
+    std::lock_guard<std::mutex> lk(g_mu);
+    // denoise.rs:274 check and :347 check_rows
+    if (width == 0 || (uint64_t)origin_y + rows > height) return RTG_STATUS_BAD_DENOISE;
+    const DnPreset pr = dn_preset(preset);
+    const uint32_t halo = dn_halo(pr), band_end = origin_y + rows;
+    const uint32_t low = y0 > halo ? y0 - halo : 0;
+    const uint64_t high = std::min<uint64_t>((uint64_t)y1 + halo, height);
+    if (y0 > y1 || y0 < origin_y || y1 > band_end || origin_y > low || band_end < high) return RTG_STATUS_BAD_DENOISE;
+    const size_t n = (size_t)width * rows;
+    const size_t a = (size_t)(y0 - origin_y) * width * 4, b = (size_t)(y1 - origin_y) * width * 4;
+    const float s = strength_of(strength);
+    if (s <= 0.0f) {
+        std::memcpy(out, in + a * 4, (b - a) * 4);
+        return RTG_STATUS_OK;
+    }
+    uint32_t st = device_init();
+    if (st) return st;
+    DevBuf m;
+    struct Release { DevBuf& bb; ~Release() { bb.release(); } } release{m};
+    const size_t in_bytes = n * 14 * 4, scratch = dn_scratch_bytes(n);
+    m.bytes = ((in_bytes + 255) & ~(size_t)255) + scratch + n * 16;
+    RTG_CHECK(cudaMalloc(&m.p, m.bytes));
+    uint8_t* base = (uint8_t*)m.p;
+    const float* words = (const float*)base;
+    void* scr = base + ((in_bytes + 255) & ~(size_t)255);
+    float* result = (float*)((uint8_t*)scr + scratch);
+    RTG_CHECK(cudaMemcpy(base, in, in_bytes, cudaMemcpyHostToDevice));
+    // rt-wasm/src/lib.rs:448-455: sums (4), lum2, albedo (3), normal (3), depth, part, material
+    const DnSrc src{words, 4, words + 3, 4, words + n * 4, words + n * 5, nullptr, words + n * 8, words + n * 11,
+                    (const uint32_t*)(words + n * 12), (const uint32_t*)(words + n * 13), nullptr};
+    uint64_t launches = 0;
+    RTG_CHECK(denoise_band(src, width, rows, samples, pr, scr, result, 0, grid_for((uint32_t)n, 256), launches));
+    RTG_CHECK(cudaMemcpy(out, result + a, (b - a) * 4, cudaMemcpyDeviceToHost));
+    if (s < 1.0f) {
+        std::vector<float> noisy(b - a);
+        std::memcpy(noisy.data(), in + a * 4, (b - a) * 4);
+        const float k1 = 1.0f - s;
+        for (size_t i = 0; i < b - a; ++i)
+            if (i % 4 != 3) out[i] = noisy[i] * k1 + out[i] * s;
+    }
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_denoise(uint32_t width, uint32_t height, uint32_t origin_y, uint32_t rows, uint32_t samples, uint32_t y0, uint32_t y1,
+                     const uint8_t* in, float* out) {
+    return rtg_denoise_with(0, 1.0f, width, height, origin_y, rows, samples, y0, y1, in, out);
 }
 
 uint32_t rtg_adaptive_free(uint32_t ad) {

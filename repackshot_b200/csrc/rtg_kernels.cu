@@ -691,6 +691,123 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_edge_exact(SceneDev S, const 
     }
     (void)err;
 }
+// ---- guide passes (passes.rs:141-229, render.rs:515-640) --------------------------------------------
+// What a camera ray (o, d) meets first (integrator/mod.rs:911 first_hit): `e` = part, material
+// and depth bits as k_edge_exact writes them, the normal facing the ray (the floor's +-z), and the
+// albedo (passes.rs:209: the material's base colour, the default material's for an index out of
+// range, the floor's colour, black for the background).
+__device__ void first_hit_passes(const SceneDev& S, const LightsDev& L, V3 o, V3 d, SplitStack& stack, uint32_t* err, uint4& e, V3& normal,
+                                 Rgb& albedo) {
+    TraceResult res;
+    const bool got = traverse<false>(S, o, d, 1.0e-3f, f_inf(), true, res, err, stack);
+    const float t_geometry = got ? res.t : f_inf();
+    float t_floor = f_inf();
+    if (S.floor_mode == 1 && d.z != 0.0f) {
+        const float t = (S.floor_z - o.z) / d.z;
+        if (t > 1.0e-3f && t < f_inf()) t_floor = t;
+    }
+    const float t_nearest = rmin(t_geometry, t_floor);
+    e = make_uint4(0u, 0u, __float_as_uint(f_inf()), 0u);
+    normal = v3(0.0f, 0.0f, 0.0f);
+    albedo = rgb(0.0f, 0.0f, 0.0f);
+    if (t_nearest == f_inf() || camera_sees_panel(L, o, d, t_nearest)) return;
+    float t = t_floor;
+    if (t_floor < t_geometry) {
+        e.x = e.y = 0xffffffffu;
+        normal = v3(0.0f, 0.0f, d.z < 0.0f ? 1.0f : -1.0f);
+        albedo = rgb(S.floor_color[0], S.floor_color[1], S.floor_color[2]);
+    } else {
+        HitInfo h;
+        uint4 idx;
+        const DevInstance* I = nullptr;
+        if (!(hit_details(S, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, h, I, idx) && I != nullptr)) return;
+        e.x = res.inst + 1u;
+        const bool known = I->material < S.n_materials;
+        e.y = known ? I->material + 1u : 0u;
+        normal = h.normal;
+        albedo = known ? rgb(S.materials[I->material].base[0], S.materials[I->material].base[1], S.materials[I->material].base[2])
+                       : rgb(0.8f, 0.8f, 0.8f);
+        t = res.t;
+    }
+    const V3 fwd = ld3(S.cam_fwd);
+    e.z = __float_as_uint(t * dot(d, fwd) + dot(o - ld3(S.cam_pos), fwd));
+}
+
+// The exact passes of the centre rays of a rectangle (render.rs:529), background outside the image.
+__global__ void __launch_bounds__(TRACE_THREADS) k_exact_passes(SceneDev S, const LightsDev* __restrict__ Lg, uint32_t x0, uint32_t y0,
+                                                                 uint32_t w, uint32_t h, float* normal, float* depth, uint32_t* part,
+                                                                 uint32_t* material) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    uint32_t err = 0;
+    const uint32_t n = w * h;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t x = x0 + p % w, y = y0 + p / w;
+        uint4 e = make_uint4(0u, 0u, __float_as_uint(f_inf()), 0u);
+        V3 nn = v3(0.0f, 0.0f, 0.0f);
+        Rgb a;
+        if (x < S.width && y < S.height) {
+            V3 o, d;
+            camera_ray_at(S, ((float)x + 0.5f) / (float)S.width, ((float)y + 0.5f) / (float)S.height, 0.0f, 0.0f, o, d);
+            first_hit_passes(S, *Lg, o, d, stack, &err, e, nn, a);
+        }
+        normal[3 * p] = nn.x;
+        normal[3 * p + 1] = nn.y;
+        normal[3 * p + 2] = nn.z;
+        depth[p] = __uint_as_float(e.z);
+        part[p] = e.x;
+        material[p] = e.y;
+    }
+    (void)err;
+}
+
+// The albedo of samples [first, first + count) of a rectangle's pixels inside the image, added in
+// sample order to `sum` (3 a pixel) with `weight` += 1 each (render.rs:590 render_tile_albedo_traced):
+// an edge pixel (`edge`, the image's mask, may be null) adds the mean of its k sub-samples.
+__global__ void __launch_bounds__(TRACE_THREADS) k_albedo_pass(SceneDev S, const LightsDev* __restrict__ Lg, const uint8_t* __restrict__ edge,
+                                                                uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t first,
+                                                                uint32_t count, float* sum, float* weight) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    uint32_t err = 0;
+    const uint32_t n = w * h;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t x = x0 + p % w, y = y0 + p / w;
+        if (x >= S.width || y >= S.height) continue;
+        const uint32_t k = (edge && S.edge_k > 1 && edge[(size_t)y * S.width + x]) ? S.edge_k : 1u;
+        float r = sum[3 * p], g = sum[3 * p + 1], b = sum[3 * p + 2], wt = weight[p];
+        for (uint32_t s = 0; s < count; ++s) {
+            uint4 e;
+            V3 nn, o, d;
+            Rgb a;
+            if (k <= 1) {
+                camera_ray(S, c_sobol, x, y, first + s, o, d);
+                first_hit_passes(S, *Lg, o, d, stack, &err, e, nn, a);
+            } else {
+                Rgb acc = rgb(0.0f, 0.0f, 0.0f);
+                for (uint32_t j = 0; j < k; ++j) {
+                    camera_ray(S, c_sobol, x, y, (first + s) * k + j, o, d);  // render.rs:376 sub_sample
+                    first_hit_passes(S, *Lg, o, d, stack, &err, e, nn, a);
+                    acc = rgb(acc.r + a.r, acc.g + a.g, acc.b + a.b);
+                }
+                const float inv = 1.0f / (float)k;
+                a = rgb(acc.r * inv, acc.g * inv, acc.b * inv);
+            }
+            r = r + a.r;
+            g = g + a.g;
+            b = b + a.b;
+            wt = wt + 1.0f;
+        }
+        sum[3 * p] = r;
+        sum[3 * p + 1] = g;
+        sum[3 * p + 2] = b;
+        weight[p] = wt;
+    }
+    (void)err;
+}
+
 // A pixel is an edge when a neighbour inside the image sees another part, another material, or
 // a depth more than 2 % away (two background pixels never differ).
 __global__ void k_edge_mask(SceneDev S, const uint4* __restrict__ exact, uint8_t* mask) {
@@ -833,6 +950,16 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
 cudaError_t launch_edge_mask(const SceneDev& S, const LightsDev* L, uint4* exact, uint8_t* mask, cudaStream_t st, int grid) {
     k_edge_exact<<<grid, TRACE_THREADS, 0, st>>>(S, L, exact);
     k_edge_mask<<<grid, 256, 0, st>>>(S, exact, mask);
+    return cudaGetLastError();
+}
+cudaError_t launch_exact_passes(const SceneDev& S, const LightsDev* L, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, float* normal,
+                                float* depth, uint32_t* part, uint32_t* material, cudaStream_t st, int grid) {
+    k_exact_passes<<<grid, TRACE_THREADS, 0, st>>>(S, L, x0, y0, w, h, normal, depth, part, material);
+    return cudaGetLastError();
+}
+cudaError_t launch_albedo_pass(const SceneDev& S, const LightsDev* L, const uint8_t* edge, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                               uint32_t first, uint32_t count, float* sum, float* weight, cudaStream_t st, int grid) {
+    k_albedo_pass<<<grid, TRACE_THREADS, 0, st>>>(S, L, edge, x0, y0, w, h, first, count, sum, weight);
     return cudaGetLastError();
 }
 cudaError_t launch_edge_list(const uint8_t* mask, uint32_t stride, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t* list,

@@ -18,6 +18,12 @@ inline uint32_t wave_rounds(const SceneDev& S) { return S.max_depth + 1u + (S.an
 cudaError_t launch_edge_mask(const SceneDev& S, const LightsDev* L, uint4* exact, uint8_t* mask, cudaStream_t st, int grid);
 // The packed (x | y << 16) edge pixels of the rectangle (x0, y0, w, h) of a mask, in any order;
 // their count in *count (device).
+// The exact passes (normal, depth, part and material ids) of a rectangle's centre rays, and the
+// albedo of a range of its samples added to sums (passes.rs, render.rs:515-640).
+cudaError_t launch_exact_passes(const SceneDev& S, const LightsDev* L, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, float* normal,
+                                float* depth, uint32_t* part, uint32_t* material, cudaStream_t st, int grid);
+cudaError_t launch_albedo_pass(const SceneDev& S, const LightsDev* L, const uint8_t* edge, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                               uint32_t first, uint32_t count, float* sum, float* weight, cudaStream_t st, int grid);
 cudaError_t launch_edge_list(const uint8_t* mask, uint32_t stride, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t* list,
                              uint32_t* count, cudaStream_t st, int grid);
 
