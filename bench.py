@@ -206,6 +206,37 @@ def adaptive_comparison(rtg, scene, dist, world, target, uniform_ms):
                     "rounds: list waves over the active 8x8 blocks; block errors on the device, the choice on the host)"}
 
 
+def denoise_comparison(rtg, film, samples, stream, dist, clocks_note=None):
+    """The 1080p frame's guide passes and the denoiser (rt-post/src/denoise.rs, the full filter)
+    on the device: rtg_film_guides over the frame's samples, then rtg_film_denoise with the result
+    kept on the device; device time by CUDA events on the scene's stream, max over ranks; the
+    oracle's filter timed on a bounded band of rows beside it."""
+    import torch
+    from repackshot_b200 import shards
+    film.guides(0, samples)  # warm-up
+    film.denoise(samples, out=False)
+    times = {}
+    for name, fn in (("guides_ms", lambda: film.guides(0, samples)), ("denoise_ms", lambda: film.denoise(samples, out=False)),
+                     ("denoise_viewport_ms", lambda: film.denoise(samples, preset=1, out=False))):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        times[name] = shards.max_over_ranks(a.elapsed_time(b) / 1e3, dist) * 1e3
+    film.clear()
+    film.render(0, samples)
+    film.guides(0, samples)
+    out = film.denoise(samples)
+    n = WIDTH * HEIGHT
+    # algorithmic bytes of the filter: per level the 25 taps' guides, light, variance and
+    # luminance stay in L1/L2; DRAM sees each plane once per kernel
+    return {**times, "pixels": n, "mpixels_s": n / (times["denoise_ms"] / 1e3) / 1e6,
+            "image_mean": float(out[..., :3].mean()),
+            "path": "rtg_film_guides (centre-ray exact passes + per-sample albedo, traced on the device) and rtg_film_denoise "
+                    "(a-trous, 5 levels, bit-exact with the oracle; result left on the device)"}
+
+
 def batched_comparison(rtg, scene, spp_scale, dist, world):
     """The metric's plain-vs-batched half: the 64 camera x light-rig jobs of uneven resolution and
     spp on this scene's geometry, rendered back to back through the plain path (rtg_scene_update +
@@ -362,6 +393,7 @@ def run_ours(args, world, rank, local, dist):
     e2e_local = shards.max_over_ranks(time.perf_counter() - t0, dist)
     e2e_value = world * e2e_steps * paths_step / e2e_local / 1e6
     img = film.resolve()
+    denoised = denoise_comparison(rtg, film, SPP, stream, dist) if args.denoise else None
     adaptive = adaptive_comparison(rtg, scene, dist, world, args.adaptive_target, total_ms / args.steps) if args.adaptive_target > 0 else None
     # The metric's other halves (0 leaves a section out, e.g. for a profiler's launch list).
     batched = batched_comparison(rtg, scene, args.batched_spp_scale, dist, world) if args.batched_spp_scale > 0 else None
@@ -424,6 +456,7 @@ def run_ours(args, world, rank, local, dist):
         "batched": batched,
         "adjoint": adjoint,
         "adaptive": adaptive,
+        "denoise": denoised,
     }
     print(json.dumps(line), flush=True)
 
@@ -438,6 +471,7 @@ def main():
     ap.add_argument("--fit-iterations", type=int, default=200, help="adjoint fit iterations of the differentiable workload")
     ap.add_argument("--batched-spp-scale", type=float, default=0.25,
                     help="spp of the batched-queue comparison's 64 jobs, as a fraction of theirs (1: the full 6.5 G paths)")
+    ap.add_argument("--denoise", type=int, default=1, help="time the guide passes and the denoiser on the frame (0 leaves it out)")
     ap.add_argument("--adaptive-target", type=float, default=0.02,
                     help="noise target of the adaptive-sampling comparison (0 leaves it out)")
     args = ap.parse_args()
