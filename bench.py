@@ -237,6 +237,57 @@ def denoise_comparison(rtg, film, samples, stream, dist, clocks_note=None):
                     "(a-trous, 5 levels, bit-exact with the oracle; result left on the device)"}
 
 
+def stress_comparison(rtg, spp, dist, world, stream):
+    """The large stress workload at `spp` samples: 10 M triangles (1000 rigid instances of a
+    10,000-triangle displaced sphere), 3840 x 2160, depth 16, 16 materials: one rig rendered plainly,
+    its 8 rig variants as one batched queue, then the adjoint (35+ parameters) on a 1024 x 1024
+    crop. Device time by CUDA events (plain), wall time around synchronous calls (queue, adjoint),
+    max over ranks."""
+    import torch
+    from repackshot_b200 import scenes, shards
+    W4, H4, D4 = 3840, 2160, 16
+    t0 = time.perf_counter()
+    base = scenes.cfg4_scene(width=W4, height=H4, spp=spp, depth=D4)
+    s = rtg.Scene(scenes.to_rsb(base))
+    load_s = time.perf_counter() - t0
+    s.set_stream(stream.cuda_stream)
+    f = s.film()
+    f.render(1_000_000, 1)  # warm-up
+    f.clear()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    f.render(0, spp)
+    b.record(stream)
+    torch.cuda.synchronize()
+    plain_s = shards.max_over_ranks(a.elapsed_time(b) / 1e3, dist)
+    paths = W4 * H4 * spp
+    rigs = [scenes.to_rsb(scenes.cfg4_scene(width=W4, height=H4, spp=spp, depth=D4, rig=scenes.light_rig(r), seed=1 + r), meshes=False)
+            for r in range(8)]
+    q = rtg.Queue(s)
+    s.synchronize()
+    t0 = time.perf_counter()
+    films = [q.add(r, 0, spp, W4, H4) for r in rigs]
+    q.run()
+    queue_s = shards.max_over_ranks(time.perf_counter() - t0, dist)
+    del films
+    q.close()
+    s.update(scenes.to_rsb(base, meshes=False))
+    crop = ((W4 - 1024) // 2, (H4 - 1024) // 2, 1024, 1024)
+    target = np.full((1024, 1024, 3), 0.5, np.float32)
+    fc = s.film(*crop)
+    s.adjoint(fc, target, 0, 2, correlated=False)  # warm-up
+    s.synchronize()
+    t0 = time.perf_counter()
+    loss, grads, _ = s.adjoint(fc, target, 0, spp, correlated=False)
+    adjoint_s = shards.max_over_ranks(time.perf_counter() - t0, dist)
+    nm, nl = s.adjoint_params()
+    return {"workload": "10,000,002 triangles (1000 rigid instances, PCG32 seed 11, of a 10,000-triangle displaced sphere, "
+                        "two-level) + floor, 3840x2160, depth 16, 16 materials", "spp": spp, "scene_load_s": load_s,
+            "plain_mpaths_s": world * paths / plain_s / 1e6, "plain_ms": plain_s * 1e3,
+            "queue_8_rigs_mpaths_s": world * 8 * paths / queue_s / 1e6, "queue_8_rigs_s": queue_s,
+            "adjoint_crop_1024_ms": adjoint_s * 1e3, "adjoint_params": 4 * nm + nl, "adjoint_loss": float(loss)}
+
+
 def batched_comparison(rtg, scene, spp_scale, dist, world):
     """The metric's plain-vs-batched half: the 64 camera x light-rig jobs of uneven resolution and
     spp on this scene's geometry, rendered back to back through the plain path (rtg_scene_update +
@@ -394,6 +445,7 @@ def run_ours(args, world, rank, local, dist):
     e2e_value = world * e2e_steps * paths_step / e2e_local / 1e6
     img = film.resolve()
     denoised = denoise_comparison(rtg, film, SPP, stream, dist) if args.denoise else None
+    stress = stress_comparison(rtg, args.stress_spp, dist, world, stream) if args.stress_spp > 0 else None
     adaptive = adaptive_comparison(rtg, scene, dist, world, args.adaptive_target, total_ms / args.steps) if args.adaptive_target > 0 else None
     # The metric's other halves (0 leaves a section out, e.g. for a profiler's launch list).
     batched = batched_comparison(rtg, scene, args.batched_spp_scale, dist, world) if args.batched_spp_scale > 0 else None
@@ -457,6 +509,7 @@ def run_ours(args, world, rank, local, dist):
         "adjoint": adjoint,
         "adaptive": adaptive,
         "denoise": denoised,
+        "stress": stress,
     }
     print(json.dumps(line), flush=True)
 
@@ -471,6 +524,8 @@ def main():
     ap.add_argument("--fit-iterations", type=int, default=200, help="adjoint fit iterations of the differentiable workload")
     ap.add_argument("--batched-spp-scale", type=float, default=0.25,
                     help="spp of the batched-queue comparison's 64 jobs, as a fraction of theirs (1: the full 6.5 G paths)")
+    ap.add_argument("--stress-spp", type=int, default=8,
+                    help="spp of the 10 M-triangle 4K stress section (plain, 8-rig queue, adjoint on a crop; 0 leaves it out)")
     ap.add_argument("--denoise", type=int, default=1, help="time the guide passes and the denoiser on the frame (0 leaves it out)")
     ap.add_argument("--adaptive-target", type=float, default=0.02,
                     help="noise target of the adaptive-sampling comparison (0 leaves it out)")

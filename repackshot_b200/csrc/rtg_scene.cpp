@@ -469,6 +469,12 @@ struct Flattener {
     // emit(prims) -> leaf reference
     std::function<uint32_t(const uint32_t*, uint32_t)> emit;
     uint32_t max_depth = 0;
+    // The top level: a child box that is flat on an axis but not at its node's lower corner
+    // there (a floor under instances whose rotated boxes reach below it) is wrapped into a node
+    // of its own, whose origin is the box itself, so that it decodes to the exact plane and the
+    // slab test drops the hits just before t_min as the reference's tree does.
+    bool exact_flat = false;
+    bool wrapped = false;
 
     void quantise(QNode& q, const Box* kids, int nk) {
         Box nb;
@@ -545,6 +551,24 @@ struct Flattener {
         for (int s = 0; s < n; ++s) boxes[s] = (*bn)[kids[s]].box;
         uint32_t refs[8];
         for (int s = 0; s < n; ++s) refs[s] = reference(kids[s], depth + 1);
+        if (exact_flat) {
+            Box nb;
+            for (int s = 0; s < n; ++s) nb = nb.uni(boxes[s]);
+            for (int s = 0; s < n; ++s)
+                for (int a = 0; a < 3; ++a) {
+                    const float lo = comp(boxes[s].lo, a);
+                    if (lo != comp(boxes[s].hi, a) || lo == comp(nb.lo, a)) continue;
+                    QNode qw;
+                    std::memset(&qw, 0, sizeof(qw));
+                    quantise(qw, &boxes[s], 1);
+                    qw.child[0] = refs[s];
+                    for (int k = 1; k < 8; ++k) qw.child[k] = NODE_EMPTY;
+                    refs[s] = (uint32_t)F.nodes.size();
+                    F.nodes.push_back(qw);
+                    wrapped = true;
+                    break;
+                }
+        }
         QNode q;
         std::memset(&q, 0, sizeof(q));
         quantise(q, boxes, n);
@@ -1031,8 +1055,11 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
             fl.order = &sb.order;
             fl.max_depth = 0;
             fl.emit = [&](const uint32_t* p, uint32_t) { return make_leaf(p[0], 1); };
+            fl.exact_flat = true;
+            fl.wrapped = false;
             F.tlas_root = fl.reference(0, 0);
-            tlas_depth = fl.max_depth;
+            fl.exact_flat = false;
+            tlas_depth = fl.max_depth + (fl.wrapped ? 1 : 0);  // a wrapper adds one level
         }
         F.stack_need = 7 * (tlas_depth + blas_depth) + 2;
         if (F.stack_need > 96) { error = "unsupported: BVH too deep for the traversal stack"; return false; }

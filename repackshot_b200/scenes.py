@@ -690,6 +690,60 @@ def product_scene(width: int = 1920, height: int = 1080, spp: int = 64, depth: i
                  seed=seed, max_depth=depth)
 
 
+def displaced_sphere(triangles: int = 10000, material_id: int = 0) -> Mesh:
+    """rt-cli/src/bench.rs:113 displaced_sphere: a latitude/longitude grid of about `triangles`
+    triangles (lat = sqrt(triangles / 4), lon = 2 lat: 10,000 exactly at 10,000) whose radius of
+    about 100 mm is modulated by a few waves; no vertex normals."""
+    lat = max(int(math.sqrt(triangles / 4.0)), 2)
+    lon = lat * 2
+    i, j = np.meshgrid(np.arange(lat + 1, dtype=np.float32), np.arange(lon, dtype=np.float32), indexing="ij")
+    theta = np.float32(math.pi) * i / np.float32(lat)
+    phi = np.float32(2.0 * math.pi) * j / np.float32(lon)
+    r = np.float32(100.0) * (np.float32(1.0) + np.float32(0.12) * np.sin(np.float32(7.0) * theta) * np.cos(np.float32(5.0) * phi)
+                             + np.float32(0.04) * np.sin(np.float32(23.0) * theta + np.float32(3.0) * phi))
+    pos = np.stack([r * np.sin(theta) * np.cos(phi), r * np.sin(theta) * np.sin(phi), r * np.cos(theta)], axis=-1).reshape(-1, 3)
+    ii, jj = np.meshgrid(np.arange(lat, dtype=np.uint32), np.arange(lon, dtype=np.uint32), indexing="ij")
+    a = ii * lon + jj
+    b = ii * lon + (jj + 1) % lon
+    c, d = a + lon, b + lon
+    idx = np.stack([a, c, b, b, c, d], axis=-1).reshape(-1).astype(np.uint32)
+    return Mesh(pos.astype(np.float32), np.zeros_like(pos, dtype=np.float32), idx, material_id)
+
+
+def _random_rotation(g: "Pcg32"):
+    """A uniform random rotation (Shoemake's quaternion from three uniforms) as 3 x 3 rows."""
+    u1, u2, u3 = g.next_f32(), g.next_f32(), g.next_f32()
+    a, b = math.sqrt(1.0 - u1), math.sqrt(u1)
+    qx, qy, qz, qw = a * math.sin(2 * math.pi * u2), a * math.cos(2 * math.pi * u2), b * math.sin(2 * math.pi * u3), b * math.cos(2 * math.pi * u3)
+    return ((1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qz * qw), 2 * (qx * qz + qy * qw)),
+            (2 * (qx * qy + qz * qw), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qx * qw)),
+            (2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)))
+
+
+def cfg4_scene(width: int = 3840, height: int = 2160, spp: int = 256, depth: int = 16, n_instances: int = 1000,
+               rig: Sequence[Light] | None = None, seed: int = 1) -> Scene:
+    """The large stress scene: `n_instances` (1000: 10 M triangles) instances of one 10,000-triangle
+    displaced sphere under random rigid transforms (PCG32 seed 11: a uniform rotation and a
+    position in a 6 x 6 x 1.6 m box over the floor), instance i with material i % 16 of the product
+    table, on the product floor, lit by light rig `rig` (default: rig 0) and the gradient dome.
+    Instances share the sphere's tree (two levels), as the reference's instanced geometry does."""
+    g = Pcg32(11, 0)
+    mats = product_materials() + [Material(base_color=(0.6, 0.6, 0.6), ior=1.0, roughness=1.0)]
+    meshes = [displaced_sphere(10000), floor_quad(0.0, 20000.0, 16)]
+    insts = []
+    for k in range(n_instances):
+        rot = _random_rotation(g)
+        t = (6000.0 * (g.next_f32() - 0.5), 6000.0 * (g.next_f32() - 0.5), 150.0 + 1600.0 * g.next_f32())
+        rows = tuple(v for r in range(3) for v in (*rot[r], t[r]))
+        insts.append(Instance(0, rows=rows, material_id=k % 16))
+    insts.append(Instance(1, material_id=16))
+    cam = (0.0, -7800.0, 3200.0)
+    return Scene(camera_position=cam, camera_target=(0.0, 0.0, 700.0), camera_up=(0.0, 0.0, 1.0), focal_mm=35.0, sensor_mm=36.0,
+                 materials=mats, meshes=meshes, instances=insts, lights=list(rig if rig is not None else light_rig(0)), env_kind=0,
+                 env_floor=0.05, env_horizon=0.3, env_zenith=0.6, env_strength=1.0, width=width, height=height,
+                 max_samples=spp, seed=seed, max_depth=depth)
+
+
 def _normalize_py(v):
     n = math.sqrt(sum(x * x for x in v))
     return [x / n for x in v]
