@@ -224,9 +224,19 @@ def denoise_comparison(rtg, film, samples, stream, dist, clocks_note=None):
         b.record(stream)
         torch.cuda.synchronize()
         times[name] = shards.max_over_ranks(a.elapsed_time(b) / 1e3, dist) * 1e3
+    # the guides read from the render's own first hits instead (rtg_film_guides_fused)
     film.clear()
+    film.fuse_guides(True)
+    film.render(0, 1)  # warm-up of the fused kernels
+    film.clear()
+    film.fuse_guides(True)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
     film.render(0, samples)
-    film.guides(0, samples)
+    b.record(stream)
+    torch.cuda.synchronize()
+    times["render_with_fused_guides_ms"] = shards.max_over_ranks(a.elapsed_time(b) / 1e3, dist) * 1e3
+    film.fuse_guides(False)
     out = film.denoise(samples)
     n = WIDTH * HEIGHT
     # algorithmic bytes of the filter: per level the 25 taps' guides, light, variance and
@@ -234,7 +244,8 @@ def denoise_comparison(rtg, film, samples, stream, dist, clocks_note=None):
     return {**times, "pixels": n, "mpixels_s": n / (times["denoise_ms"] / 1e3) / 1e6,
             "image_mean": float(out[..., :3].mean()),
             "path": "rtg_film_guides (centre-ray exact passes + per-sample albedo, traced on the device) and rtg_film_denoise "
-                    "(a-trous, 5 levels, bit-exact with the oracle; result left on the device)"}
+                    "(a-trous, 5 levels, bit-exact with the oracle; result left on the device); render_with_fused_guides_ms: the "
+                    "frame's render with rtg_film_guides_fused (the albedo from its own first hits), against the plain frame"}
 
 
 def stress_comparison(rtg, spp, dist, world, stream):

@@ -307,6 +307,11 @@ uint32_t rtg_denoise_halo(uint32_t preset);
  * pixels and adds the albedo of samples [first_sample, first_sample + count) to the film's albedo
  * sums (rtg_film_clear clears them with the film). */
 uint32_t rtg_film_guides(uint32_t scene, uint32_t film, uint32_t first_sample, uint32_t count);
+/* No counterpart in the reference. With `enable`, writes the film's exact passes now and makes
+ * every later rtg_render_progressive on the film add each sample's albedo to the film's albedo
+ * sums as well, read from the first hit its camera ray already traced: the guides of
+ * rtg_film_guides, bit for bit, without tracing the camera rays a second time. 0 stops it. */
+uint32_t rtg_film_guides_fused(uint32_t scene, uint32_t film, uint32_t enable);
 /* The denoiser on a film that covers the whole image, with its guide passes, as rtg_denoise_with
  * on the film's planes (`samples` the samples of every pixel): the film stays on the device, and
  * `out` (may be null: the result stays on the device) gets width*height*4 floats of RGBA sums. */

@@ -82,6 +82,7 @@ ABI = {
     "rtg_denoise_with": (_u32, [_u32, ctypes.c_float, _u32, _u32, _u32, _u32, _u32, _u32, _u32, _f, _f]),
     "rtg_denoise_halo": (_u32, [_u32]),
     "rtg_film_guides": (_u32, [_u32, _u32, _u32, _u32]),
+    "rtg_film_guides_fused": (_u32, [_u32, _u32, _u32]),
     "rtg_film_denoise": (_u32, [_u32, _u32, ctypes.c_float, _u32, _f]),
 }
 
@@ -302,6 +303,11 @@ class Film:
         """Renders the film's guide passes: the exact passes, and the albedo of samples
         [first, first + count) added to its albedo sums (rtg_film_guides)."""
         _check(lib().rtg_film_guides(self.scene.handle, self.handle, first, count))
+
+    def fuse_guides(self, enable: bool = True):
+        """rtg_film_guides_fused: the exact passes now, and the albedo of every later render
+        taken from its own camera rays."""
+        _check(lib().rtg_film_guides_fused(self.scene.handle, self.handle, int(enable)))
 
     def denoise(self, samples: int, preset: int = 0, strength: float = 1.0, out=None):
         """The film denoised on the device (rtg_film_denoise): (h, w, 4) RGBA sums; ``out=False``

@@ -79,6 +79,7 @@ struct Scene {
     // edge samples (E11): the image's edge mask, its centre-ray scratch and an edge-pixel list
     DevBuf edge_mem;
     bool edges_ready = false;
+    DevBuf alb_mem;  // one float4 a path slot: the albedo of renders that fill a film's guides
     uint64_t edge_builds = 0;  // masks built so far: what depends on the mask checks it
     cudaStream_t stream = nullptr;
     // path buffers
@@ -105,6 +106,7 @@ struct Scene {
         path_mem.release();
         adjoint_mem.release();
         edge_mem.release();
+        alb_mem.release();
         if (wt) {
             for (int i = 0; i < WaveTiming::MAX_EVENTS; ++i) cudaEventDestroy(wt->ev[i]);
             delete wt;
@@ -121,6 +123,7 @@ struct Film {
     // normal (3), depth, part and material ids; and the denoiser's scratch and result.
     DevBuf guides;
     DevBuf denoise;
+    bool fuse_guides = false;  // rtg_film_guides_fused: renders add their albedo to `guides`
     ~Film() {
         mem.release();
         encoded.release();
@@ -431,7 +434,7 @@ uint32_t edge_pixels(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, 
 // Renders samples [first, first + count) of the image rectangle (x, y, w, h) (clipped to the
 // image) into `film`, every pixel's samples added in index order.
 uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t first, uint32_t count, const FilmDev& film,
-                       uint64_t* rays_out) {
+                       uint64_t* rays_out, float* guide_sum = nullptr, float* guide_weight = nullptr) {
     uint64_t x_end = std::min<uint64_t>((uint64_t)x + w, sc.width), y_end = std::min<uint64_t>((uint64_t)y + h, sc.height);
     if (rays_out) *rays_out = 0;
     if (x >= x_end || y >= y_end || count == 0) return RTG_STATUS_OK;
@@ -462,6 +465,17 @@ uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h
         }
         st = ensure_capacity(sc, need);
         if (st) return st;
+        if (guide_sum && sc.alb_mem.bytes < (size_t)sc.capacity * 16) {
+            sc.alb_mem.release();
+            RTG_CHECK(cudaMalloc(&sc.alb_mem.p, (size_t)sc.capacity * 16));
+            sc.alb_mem.bytes = (size_t)sc.capacity * 16;
+        }
+        auto guides = [&](WaveDesc& wd) {
+            if (!guide_sum) return;
+            wd.alb = (float4*)sc.alb_mem.p;
+            wd.guide_sum = guide_sum;
+            wd.guide_weight = guide_weight;
+        };
         RTG_CHECK(cudaMemsetAsync(sc.P.counters, 0, 16, sc.stream));
         RTG_CHECK(cudaMemsetAsync(sc.P.rays, 0, 16, sc.stream));
         for (uint32_t s = 0; s < count; s += per_wave) {
@@ -471,6 +485,7 @@ uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h
                 wd.edge = mask;
                 wd.edge_stride = sc.width;
             }
+            guides(wd);
             st = run_wave(sc, wd, &film);
             if (st) return st;
         }
@@ -483,6 +498,7 @@ uint32_t render_region(Scene& sc, uint32_t x, uint32_t y, uint32_t w, uint32_t h
                 wd.epix = elist + e0;
                 wd.ne = en;
                 wd.ek = k;
+                guides(wd);
                 st = run_wave(sc, wd, &film);
                 if (st) return st;
             }
@@ -852,6 +868,9 @@ uint32_t rtg_render_progressive(uint32_t handle, uint32_t film, uint32_t first_s
     if (!sc) return RTG_STATUS_BAD_HANDLE;
     Film* f = film_of(film);
     if (!f || f->scene != handle) return RTG_STATUS_BAD_FILM;
+    if (f->fuse_guides)
+        return render_region(*sc, f->dev.ox, f->dev.oy, f->dev.w, f->dev.h, first_sample, count, f->dev, rays, f->albedo_sum(),
+                             f->albedo_weight());
     return render_region(*sc, f->dev.ox, f->dev.oy, f->dev.w, f->dev.h, first_sample, count, f->dev, rays);
 }
 uint32_t rtg_render_progressive_noalloc(uint32_t handle, uint32_t film, uint32_t first_sample, uint32_t count,
@@ -1676,6 +1695,28 @@ uint32_t rtg_film_guides(uint32_t scene, uint32_t film, uint32_t first_sample, u
         RTG_CHECK(launch_albedo_pass(sc->S, sc->d_lights, mask, d.ox, d.oy, d.w, d.h, first_sample, count, f->albedo_sum(), f->albedo_weight(),
                                      sc->stream, grid_for((uint32_t)n, 128)));
     sc->launches += count ? 2 : 1;
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_film_guides_fused(uint32_t scene, uint32_t film, uint32_t enable) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(scene);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    Film* f = film_of(film);
+    if (!f || f->scene != scene) return RTG_STATUS_BAD_FILM;
+    f->fuse_guides = enable != 0;
+    if (!enable) return RTG_STATUS_OK;
+    const size_t n = f->pixels();
+    if (!f->guides.p) {
+        f->guides.bytes = n * 10 * 4;
+        RTG_CHECK(cudaMalloc(&f->guides.p, f->guides.bytes));
+        RTG_CHECK(cudaMemsetAsync(f->guides.p, 0, f->guides.bytes, sc->stream));
+    }
+    const FilmDev& d = f->dev;
+    RTG_CHECK(launch_exact_passes(sc->S, sc->d_lights, d.ox, d.oy, d.w, d.h, f->normal(), f->depth(), f->part(), f->material(), sc->stream,
+                                  grid_for((uint32_t)n, 128)));
+    sc->launches += 1;
     RTG_CHECK(cudaStreamSynchronize(sc->stream));
     return RTG_STATUS_OK;
 }

@@ -808,6 +808,97 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_albedo_pass(SceneDev S, const
     (void)err;
 }
 
+// The albedo of each camera ray's first hit from the wave's first extend (the ray in P.o / P.d,
+// the hit in P.hit): first_hit_passes without its traversal, which the extend has done with the
+// same ray, class and interval.
+__global__ void k_albedo_hits(SceneDev S, const LightsDev* __restrict__ Lg, WaveDesc w, PathBuffers P) {
+    const LightsDev& L = *Lg;
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n; slot += gridDim.x * blockDim.x) {
+        const float4 of = P.o[slot], df = P.d[slot];
+        const V3 o = v3(of.x, of.y, of.z), d = v3(df.x, df.y, df.z);
+        const uint4 hit = P.hit[slot];
+        const bool got = hit.w != 0u;
+        const float t_geometry = got ? __uint_as_float(hit.z) : f_inf();
+        float t_floor = f_inf();
+        if (S.floor_mode == 1 && d.z != 0.0f) {
+            const float t = (S.floor_z - o.z) / d.z;
+            if (t > 1.0e-3f && t < f_inf()) t_floor = t;
+        }
+        const float t_nearest = rmin(t_geometry, t_floor);
+        float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (!(t_nearest == f_inf() || camera_sees_panel(L, o, d, t_nearest))) {
+            if (t_floor < t_geometry) {
+                a = make_float4(S.floor_color[0], S.floor_color[1], S.floor_color[2], 0.0f);
+            } else {
+                HitInfo h;
+                uint4 idx;
+                const DevInstance* I = nullptr;
+                if (hit_details(S, o, d, 1.0e-3f, f_inf(), hit.x, hit.y, h, I, idx) && I != nullptr) {
+                    if (I->material < S.n_materials) {
+                        const float* b = S.materials[I->material].base;
+                        a = make_float4(b[0], b[1], b[2], 0.0f);
+                    } else {
+                        a = make_float4(0.8f, 0.8f, 0.8f, 0.0f);
+                    }
+                }
+            }
+        }
+        w.alb[slot] = a;
+    }
+}
+
+// The wave's albedo into the film's guide sums, each pixel's samples in index order (the edge
+// pixels of a list wave the mean of their k sub-samples, render.rs:590).
+__global__ void k_accumulate_albedo(WaveDesc w, FilmDev F) {
+    const bool list = w.epix != nullptr;
+    const uint32_t k = list ? w.ek : 1u;
+    const uint32_t units = list ? w.ne : w.w * w.h;
+    const uint32_t ns = w.n / (units * k);
+    const float inv = 1.0f / (float)k;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < units; e += gridDim.x * blockDim.x) {
+        uint32_t x, y;
+        if (list) {
+            x = w.epix[e] & 0xffffu;
+            y = w.epix[e] >> 16;
+        } else {
+            x = w.x0 + e % w.w;
+            y = w.y0 + e / w.w;
+            if (w.edge && w.edge[(size_t)y * w.edge_stride + x]) continue;  // from the edge waves
+        }
+        if (x < F.ox || y < F.oy || x - F.ox >= F.w || y - F.oy >= F.h) continue;
+        const size_t fi = (size_t)(y - F.oy) * F.w + (x - F.ox);
+        float r = w.guide_sum[3 * fi], g = w.guide_sum[3 * fi + 1], b = w.guide_sum[3 * fi + 2], wt = w.guide_weight[fi];
+        for (uint32_t s = 0; s < ns; ++s) {
+            float ar, ag, ab;
+            if (k > 1) {
+                ar = ag = ab = 0.0f;
+                for (uint32_t j = 0; j < k; ++j) {
+                    const float4 c = w.alb[(s * units + e) * k + j];
+                    ar = ar + c.x;
+                    ag = ag + c.y;
+                    ab = ab + c.z;
+                }
+                ar = ar * inv;
+                ag = ag * inv;
+                ab = ab * inv;
+            } else {
+                const float4 c = w.alb[s * units + e];
+                ar = c.x;
+                ag = c.y;
+                ab = c.z;
+            }
+            r = r + ar;
+            g = g + ag;
+            b = b + ab;
+            wt = wt + 1.0f;
+        }
+        w.guide_sum[3 * fi] = r;
+        w.guide_sum[3 * fi + 1] = g;
+        w.guide_sum[3 * fi + 2] = b;
+        w.guide_weight[fi] = wt;
+    }
+}
+
 // A pixel is an edge when a neighbour inside the image sees another part, another material, or
 // a depth more than 2 % away (two background pixels never differ).
 __global__ void k_edge_mask(SceneDev S, const uint4* __restrict__ exact, uint8_t* mask) {
@@ -932,6 +1023,7 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
         } else {
             k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur);
         }
+        if (round == 0 && w.alb && film && !batch) k_albedo_hits<<<g, 256, 0, st>>>(S, L, w, P);
         k_scan<<<1, 32, 0, st>>>(P);
         k_scatter<<<g, 256, 0, st>>>(P, cur);
         if (batch) k_shade<true><<<g, 128, 0, st>>>(S, L, P, cur, w);
@@ -945,6 +1037,7 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
     if (batch) k_accumulate_jobs<<<g, 256, 0, st>>>(w, P);
     else if (film && w.epix) k_accumulate_edges<<<g, 256, 0, st>>>(w, P, *film);
     else if (film) k_accumulate<<<g, 256, 0, st>>>(w, P, *film);
+    if (w.alb && film && !batch) k_accumulate_albedo<<<g, 256, 0, st>>>(w, *film);
 }
 
 cudaError_t launch_edge_mask(const SceneDev& S, const LightsDev* L, uint4* exact, uint8_t* mask, cudaStream_t st, int grid) {

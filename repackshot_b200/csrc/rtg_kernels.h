@@ -56,6 +56,13 @@ struct WaveDesc {
     // `edge_stride`); its pixels splat from the edge waves, not from this one.
     const uint8_t* edge;
     uint32_t edge_stride;
+    // Guides taken from the wave itself (the film's albedo pass, passes.rs:209): when `alb` is set
+    // (one float4 a path slot), the albedo of each camera ray's first hit is read from the first
+    // extend, and after the film's accumulate each pixel adds its samples' albedo (an edge pixel
+    // the mean of its k) to `guide_sum` (3 a film pixel) with `guide_weight` += 1, in sample order.
+    float4* alb;
+    float* guide_sum;
+    float* guide_weight;
 };
 
 // Structure-of-arrays path state of one wave (device pointers).

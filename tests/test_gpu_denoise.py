@@ -145,3 +145,30 @@ def test_random_planes_are_the_oracle_image(rtg, oracle_lib, seed, samples):
         b = oracle_lib.denoise(words, w, h, samples, preset=preset)
         assert np.array_equal(bits(a), bits(b)), preset
     assert n == w * h
+
+
+@pytest.mark.parametrize("name, capacity", [("example", 0), ("e11 small", 0), ("e11 small", 5000)])
+def test_fused_guides_are_the_traced_ones(rtg, pins, name, capacity):
+    """rtg_film_guides_fused: the albedo read from the render's own first hits (edge pixels the
+    mean of their sub-samples, in waves of any size) gives rtg_film_guides' guides bit for bit,
+    so the same denoised image, and leaves the film itself as it was."""
+    from repackshot_b200 import scenes
+    sc = scenes.example_scene() if name == "example" else scenes.e11_scene()
+    if name != "example":
+        sc.width, sc.height = 160, 120
+    s = rtg.Scene(scenes.to_rsb(sc))
+    if capacity:
+        s.set_path_capacity(capacity)
+    a = s.film()
+    a.render(0, 4)
+    a.guides(0, 4)
+    b = s.film()
+    b.fuse_guides()
+    b.render(0, 1)
+    b.render(1, 3)
+    for x, y in zip(a.read(), b.read()):
+        assert np.array_equal(bits(x), bits(y))
+    da, db = a.denoise(4), b.denoise(4)
+    assert np.array_equal(bits(da), bits(db))
+    if name == "example":
+        assert fnv1a_floats(means(db, 4)) == pins["denoised"]["example_4spp"]
