@@ -313,8 +313,12 @@ uint32_t rtg_film_guides(uint32_t scene, uint32_t film, uint32_t first_sample, u
  * rtg_film_guides, bit for bit, without tracing the camera rays a second time. 0 stops it. */
 uint32_t rtg_film_guides_fused(uint32_t scene, uint32_t film, uint32_t enable);
 /* The denoiser on a film that covers the whole image, with its guide passes, as rtg_denoise_with
- * on the film's planes (`samples` the samples of every pixel): the film stays on the device, and
- * `out` (may be null: the result stays on the device) gets width*height*4 floats of RGBA sums. */
+ * on the film's planes: the film stays on the device, and `out` (may be null: the result stays on
+ * the device) gets width*height*4 floats of RGBA sums of `samples` samples. A film whose pixels
+ * have their own counts (an adaptive render) is denoised as the reference's CLI does it
+ * (rt-cli/src/lib.rs:104): its sums rescaled to `samples` samples (adaptive.rs:260) and each
+ * pixel's variance divided by its own count; a film whose every pixel has `samples` samples gives
+ * the plain result bit for bit. */
 uint32_t rtg_film_denoise(uint32_t film, uint32_t preset, float strength, uint32_t samples, float* out);
 
 #ifdef __cplusplus

@@ -335,9 +335,28 @@ __global__ void k_dn_final(DnSrc src, uint32_t w, uint32_t h, uint32_t samples, 
     }
 }
 
+// adaptive.rs:260 rescale: a pixel's sums of n samples as sums of s, RGBA interleaved, and its
+// squared-luminance sum (the film of a uniform render keeps its bits: n == s).
+__device__ __forceinline__ float rescale(float sum, float n, float s) { return n == s ? sum : (n > 0.0f ? sum * (1.0f / n) * s : 0.0f); }
+__global__ void k_dn_rescale(const float* rgb, const float* alpha, const float* lum2, const float* weight, size_t n, float s, float* rgba,
+                             float* lum2_out) {
+    DN_LOOP(n) {
+        const float w = weight[p];
+        for (int k = 0; k < 3; ++k) rgba[4 * p + k] = rescale(rgb[3 * p + k], w, s);
+        rgba[4 * p + 3] = rescale(alpha[p], w, s);
+        lum2_out[p] = rescale(lum2[p], w, s);
+    }
+}
+
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 }  // namespace
+
+cudaError_t launch_dn_rescale(const float* rgb, const float* alpha, const float* lum2, const float* weight, size_t n, uint32_t samples, float* rgba,
+                              float* lum2_out, cudaStream_t st, int grid) {
+    k_dn_rescale<<<grid, 256, 0, st>>>(rgb, alpha, lum2, weight, n, (float)samples, rgba, lum2_out);
+    return cudaGetLastError();
+}
 
 size_t dn_scratch_bytes(size_t n) {
     // 3 guide float4 planes; divisor and two light planes (3 floats); var x 3, lum x 2, gvar,

@@ -48,4 +48,10 @@ size_t dn_scratch_bytes(size_t n);
 cudaError_t denoise_band(const DnSrc& src, uint32_t width, uint32_t rows, uint32_t samples, DnPreset preset, void* scratch, float* out,
                          cudaStream_t st, int grid, uint64_t& launches);
 
+// The sums of a film whose pixels have their own sample counts (`weight`) as sums of `samples`
+// samples (adaptive.rs:260 rescale; rt-cli/src/lib.rs:104 denoise_film_at): RGBA interleaved and
+// the squared-luminance sums. A pixel with `samples` samples keeps its bits.
+cudaError_t launch_dn_rescale(const float* rgb, const float* alpha, const float* lum2, const float* weight, size_t n, uint32_t samples, float* rgba,
+                              float* lum2_out, cudaStream_t st, int grid);
+
 }  // namespace rtg

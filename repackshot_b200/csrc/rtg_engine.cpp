@@ -1738,40 +1738,43 @@ uint32_t rtg_film_denoise(uint32_t film, uint32_t preset, float strength, uint32
         return RTG_STATUS_BAD_FILM;
     }
     const size_t n = f->pixels();
-    const size_t need = dn_scratch_bytes(n) + n * 16;
+    const size_t need = dn_scratch_bytes(n) + n * 16 + n * 20;
     if (f->denoise.bytes < need) {
         f->denoise.release();
         RTG_CHECK(cudaMalloc(&f->denoise.p, need));
         f->denoise.bytes = need;
     }
     float* result = (float*)((uint8_t*)f->denoise.p + dn_scratch_bytes(n));
+    float* rgba = result + 4 * n;
+    float* lum2 = rgba + 4 * n;
     const float s = strength_of(strength);
     const FilmDev& d = f->dev;
+    // rt-cli/src/lib.rs:104 denoise_film_at: the sums as sums of `samples` samples and each pixel's
+    // variance with its own count (its weight). For a film whose every pixel has `samples` samples
+    // this is the plain call bit for bit: the sums keep their bits, and the counts give the same
+    // degrees of freedom and the same few-samples test.
+    RTG_CHECK(launch_dn_rescale(d.rgb, d.alpha, d.lum2, d.weight, n, samples > 1 ? samples : 1, rgba, lum2, sc->stream, grid_for((uint32_t)n, 256)));
+    sc->launches += 1;
     if (s > 0.0f) {
-        const DnSrc src{d.rgb, 3, d.alpha, 1, d.lum2, f->albedo_sum(), f->albedo_weight(), f->normal(), f->depth(), f->part(), f->material(),
-                        nullptr};
+        const DnSrc src{rgba, 4, rgba + 3, 4, lum2, f->albedo_sum(), f->albedo_weight(), f->normal(), f->depth(), f->part(), f->material(),
+                        d.weight};
         RTG_CHECK(denoise_band(src, d.w, d.h, samples, dn_preset(preset), f->denoise.p, result, sc->stream, grid_for((uint32_t)n, 256),
                                sc->launches));
     }
     if (out) {
-        std::vector<float> rgb, alpha;
-        if (s < 1.0f) {  // the noisy sums, for strength 0 and the blend (denoise.rs:396)
-            rgb.resize(3 * n);
-            alpha.resize(n);
-            RTG_CHECK(cudaMemcpyAsync(rgb.data(), d.rgb, n * 12, cudaMemcpyDeviceToHost, sc->stream));
-            RTG_CHECK(cudaMemcpyAsync(alpha.data(), d.alpha, n * 4, cudaMemcpyDeviceToHost, sc->stream));
+        std::vector<float> noisy;
+        if (s < 1.0f) {  // the (rescaled) noisy sums, for strength 0 and the blend (denoise.rs:396)
+            noisy.resize(4 * n);
+            RTG_CHECK(cudaMemcpyAsync(noisy.data(), rgba, n * 16, cudaMemcpyDeviceToHost, sc->stream));
         }
         if (s > 0.0f) RTG_CHECK(cudaMemcpyAsync(out, result, n * 16, cudaMemcpyDeviceToHost, sc->stream));
         RTG_CHECK(cudaStreamSynchronize(sc->stream));
         if (s <= 0.0f) {
-            for (size_t p = 0; p < n; ++p) {
-                for (int k = 0; k < 3; ++k) out[4 * p + k] = rgb[3 * p + k];
-                out[4 * p + 3] = alpha[p];
-            }
+            std::memcpy(out, noisy.data(), n * 16);
         } else if (s < 1.0f) {
             const float k1 = 1.0f - s;
             for (size_t p = 0; p < n; ++p)
-                for (int k = 0; k < 3; ++k) out[4 * p + k] = rgb[3 * p + k] * k1 + out[4 * p + k] * s;
+                for (int k = 0; k < 3; ++k) out[4 * p + k] = noisy[4 * p + k] * k1 + out[4 * p + k] * s;
         }
     } else {
         RTG_CHECK(cudaStreamSynchronize(sc->stream));

@@ -172,3 +172,38 @@ def test_fused_guides_are_the_traced_ones(rtg, pins, name, capacity):
     assert np.array_equal(bits(da), bits(db))
     if name == "example":
         assert fnv1a_floats(means(db, 4)) == pins["denoised"]["example_4spp"]
+
+
+def test_an_adaptive_film_is_denoised_with_its_own_counts(rtg, oracle_lib):
+    """An adaptive film (pixels with their own counts) denoised on the device equals the oracle's
+    denoiser on its sums rescaled to `samples` samples with the counts plane (rt-cli/src/lib.rs:104,
+    adaptive.rs:260), also at half strength."""
+    from repackshot_b200 import scenes
+    sc = scenes.example_scene()
+    sc.width, sc.height = 96, 64
+    sc.adaptive, sc.noise_threshold = 1, 0.05
+    rsb = scenes.to_rsb(sc)
+    s = rtg.Scene(rsb)
+    f = s.film()
+    ad = rtg.Adaptive(s, f, 48)
+    ad.run(0)
+    ad.close()
+    samples = 48
+    f.guides(0, 16)
+    rgb, weight, alpha, lum2 = f.read()
+    assert weight.min() < weight.max()
+    f32 = np.float32
+
+    def rescale(x):
+        x = np.asarray(x, f32)
+        wt = weight if x.ndim == 2 else weight[..., None]
+        scaled = ((x * (f32(1.0) / np.where(wt > 0, wt, f32(1.0)))).astype(f32) * f32(samples)).astype(f32)
+        return np.where(wt == f32(samples), x, np.where(wt > 0, scaled, f32(0.0))).astype(f32)
+
+    sums = np.concatenate([rescale(rgb), rescale(alpha)[..., None]], axis=-1)
+    albedo, normal, depth, part, material = oracle_lib.OracleScene(rsb).guides(16)
+    words = oracle_lib.denoise_words(sums, rescale(lum2), albedo, normal, depth, part, material, counts=weight)
+    for strength in (1.0, 0.5):
+        want = oracle_lib.denoise(words, 96, 64, samples, strength=strength)
+        got = f.denoise(samples, strength=strength)
+        assert np.array_equal(bits(got).reshape(-1), bits(want))
