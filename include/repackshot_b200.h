@@ -310,7 +310,9 @@ uint32_t rtg_film_guides(uint32_t scene, uint32_t film, uint32_t first_sample, u
 /* No counterpart in the reference. With `enable`, writes the film's exact passes now and makes
  * every later rtg_render_progressive on the film add each sample's albedo to the film's albedo
  * sums as well, read from the first hit its camera ray already traced: the guides of
- * rtg_film_guides, bit for bit, without tracing the camera rays a second time. 0 stops it. */
+ * rtg_film_guides, bit for bit, without tracing the camera rays a second time. 0 stops it.
+ * Only rtg_render_progressive fills the guides this way; the allocation-free render, the queue
+ * and the adaptive passes do not, so call rtg_film_guides for films rendered through them. */
 uint32_t rtg_film_guides_fused(uint32_t scene, uint32_t film, uint32_t enable);
 /* The denoiser on a film that covers the whole image, with its guide passes, as rtg_denoise_with
  * on the film's planes: the film stays on the device, and `out` (may be null: the result stays on
