@@ -274,6 +274,19 @@ def stress_comparison(rtg, spp, dist, world, stream):
     paths = W4 * H4 * spp
     rigs = [scenes.to_rsb(scenes.cfg4_scene(width=W4, height=H4, spp=spp, depth=D4, rig=scenes.light_rig(r), seed=1 + r), meshes=False)
             for r in range(8)]
+    # the 8 rigs back to back through the plain path (rtg_scene_update + rtg_render_progressive),
+    # then as one batched queue: wall time around synchronous calls for both
+    s.synchronize()
+    t0 = time.perf_counter()
+    keep = []
+    for r in rigs:
+        s.update(r)
+        fr = s.film()
+        fr.render(0, spp)
+        keep.append(fr)
+    s.synchronize()
+    plain8_s = shards.max_over_ranks(time.perf_counter() - t0, dist)
+    del keep
     q = rtg.Queue(s)
     s.synchronize()
     t0 = time.perf_counter()
@@ -295,6 +308,7 @@ def stress_comparison(rtg, spp, dist, world, stream):
     return {"workload": "10,000,002 triangles (1000 rigid instances, PCG32 seed 11, of a 10,000-triangle displaced sphere, "
                         "two-level) + floor, 3840x2160, depth 16, 16 materials", "spp": spp, "scene_load_s": load_s,
             "plain_mpaths_s": world * paths / plain_s / 1e6, "plain_ms": plain_s * 1e3,
+            "plain_8_rigs_back_to_back_mpaths_s": world * 8 * paths / plain8_s / 1e6, "plain_8_rigs_s": plain8_s,
             "queue_8_rigs_mpaths_s": world * 8 * paths / queue_s / 1e6, "queue_8_rigs_s": queue_s,
             "adjoint_crop_1024_ms": adjoint_s * 1e3, "adjoint_params": 4 * nm + nl, "adjoint_loss": float(loss)}
 
