@@ -286,6 +286,7 @@ SceneDev compose(const SceneDev& constants, const SceneDev& geom, const SceneDev
 // medium, queue[0], queue[1], sorted, key (4 each).
 constexpr size_t PATH_BYTES = 9 * 16 + 6 * 4;
 constexpr uint64_t AUTO_MIN_PATHS = 1u << 20;
+constexpr uint64_t PLAIN_JOB_PATHS = 1u << 24;  // a queue job this large runs as plain waves
 constexpr uint64_t MAX_WAVE_PATHS = 0x7fffffffu;
 
 // Paths one wave of a call may hold: the limit set by rtg_set_path_capacity, or by default every
@@ -349,7 +350,7 @@ int grid_for(uint32_t n, int per_block) {
 
 // Runs one wave and (when timing) adds the extend-kernel time.
 // `S` (default: the scene's) gives the launch its bounce count; batched waves pass the deepest job's.
-uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film, const SceneDev* S = nullptr) {
+uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film, const SceneDev* S = nullptr, const LightsDev* lights = nullptr) {
     const SceneDev& Sw = S ? *S : sc.S;
     WaveTiming* t = nullptr;
     if (sc.timing) {
@@ -360,7 +361,7 @@ uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film, const Scene
         sc.wt->ev_count = 0;
         t = sc.wt;
     }
-    launch_wave(Sw, sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t);
+    launch_wave(Sw, lights ? lights : sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t);
     RTG_CHECK(cudaGetLastError());
     sc.launches += 2 + 6 * (uint64_t)wave_rounds(Sw) - ((film || w.segs) ? 0 : 1);
     if (t) {
@@ -960,7 +961,7 @@ namespace {
 // most (whole images over a run of samples, or a band of rows of one sample), so a pixel receives
 // its samples in index order: wave by wave, and within a wave from one segment only.
 void pack_waves(const std::vector<std::unique_ptr<QueueJob>>& jobs, uint64_t cap, std::vector<std::vector<SegDev>>& waves,
-                std::vector<uint64_t>& wave_paths) {
+                std::vector<uint64_t>& wave_paths, const std::vector<uint8_t>& skip) {
     std::vector<SegDev> cur;
     uint64_t used = 0;
     auto flush = [&]() {
@@ -971,6 +972,7 @@ void pack_waves(const std::vector<std::unique_ptr<QueueJob>>& jobs, uint64_t cap
         used = 0;
     };
     for (uint32_t j = 0; j < jobs.size(); ++j) {
+        if (j < skip.size() && skip[j]) continue;
         const QueueJob& J = *jobs[j];
         const uint64_t W = J.width, H = J.height, npix = W * H;
         uint32_t s = J.first, row = 0;
@@ -1038,10 +1040,26 @@ uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays) {
     uint64_t widest = 0;
     for (auto& j : q->jobs) widest = std::max<uint64_t>(widest, j->width);
     cap = std::max(cap, widest);  // a wave holds at least one row of every job
+    // A job that fills waves on its own (at least PLAIN_JOB_PATHS paths, a whole sample in one
+    // wave) gains nothing from sharing them and would pay the batched kernels' segment lookups and
+    // the deepest job's bounce count: it runs as the plain path's waves, with its own scene
+    // constants and lights. Its film gets the same bits either way.
+    const bool graph = (flags & RTG_QUEUE_GRAPH) != 0;
+    std::vector<uint8_t> plain(q->jobs.size(), 0);
+    uint64_t plain_need = 0;
+    for (size_t j = 0; j < q->jobs.size(); ++j) {
+        const QueueJob& J = *q->jobs[j];
+        const uint64_t npix = (uint64_t)J.width * J.height;
+        if (!graph && npix * J.count >= PLAIN_JOB_PATHS && npix <= cap) {
+            plain[j] = 1;
+            plain_need = std::max(plain_need, npix * std::min<uint64_t>(J.count, cap / npix));
+        }
+    }
     std::vector<std::vector<SegDev>> waves;
     std::vector<uint64_t> wave_paths;
-    pack_waves(q->jobs, cap, waves, wave_paths);
-    uint64_t max_wave = *std::max_element(wave_paths.begin(), wave_paths.end());
+    pack_waves(q->jobs, cap, waves, wave_paths, plain);
+    uint64_t max_wave = wave_paths.empty() ? 0 : *std::max_element(wave_paths.begin(), wave_paths.end());
+    max_wave = std::max(max_wave, plain_need);
     if (max_wave > MAX_WAVE_PATHS) { g_error = "a queue wave exceeds 2^31 paths"; return RTG_STATUS_BAD_SCENE; }
     uint32_t st = ensure_capacity(*sc, (uint32_t)max_wave);
     if (st) return st;
@@ -1065,7 +1083,6 @@ uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays) {
     const JobDev* jobs_d = (const JobDev*)q->tables.p;
     const SegDev* segs_d = (const SegDev*)((const uint8_t*)q->tables.p + jobs_h.size() * sizeof(JobDev));
     // The waves: enqueued back to back, or captured into one CUDA graph and launched as one.
-    const bool graph = (flags & RTG_QUEUE_GRAPH) != 0;
     const bool timing = sc->timing;
     if (graph) {
         sc->timing = false;
@@ -1074,6 +1091,17 @@ uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays) {
     }
     cudaError_t e = cudaMemsetAsync(sc->P.counters, 0, 16, sc->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(sc->P.rays, 0, 16, sc->stream);
+    for (size_t j = 0; j < q->jobs.size() && e == cudaSuccess && st == RTG_STATUS_OK; ++j) {
+        if (!plain[j]) continue;
+        const QueueJob& J = *q->jobs[j];
+        const uint64_t npix = (uint64_t)J.width * J.height;
+        const uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(J.count, cap / npix));
+        for (uint32_t s = 0; s < J.count && st == RTG_STATUS_OK; s += per) {
+            const uint32_t ns = std::min(per, J.count - s);
+            WaveDesc wd{0, 0, J.width, J.height, J.first + s, (uint32_t)(npix * ns), nullptr};
+            st = run_wave(*sc, wd, &jobs_h[j].film, &jobs_h[j].S, jobs_h[j].lights);
+        }
+    }
     size_t seg_off = 0;
     for (size_t k = 0; k < waves.size() && e == cudaSuccess && st == RTG_STATUS_OK; ++k) {
         uint32_t npix = waves[k].back().pix_begin + waves[k].back().w * waves[k].back().h;

@@ -99,3 +99,23 @@ def test_adjoint_on_a_crop_matches_finite_differences(rtg):
         print(f"cfg4 crop light {j}: adjoint {adj:.6g} finite difference {fd:.6g}")
         assert abs(adj - fd) <= 1e-1 * abs(fd) + 2e-2 * np.abs(grads[4 * nm:]).max()
     s.update(scenes.to_rsb(base, meshes=False))
+
+
+def test_a_queue_job_that_fills_waves_alone_runs_plain_and_keeps_its_bits(rtg):
+    """A queue job of at least 2^24 paths runs as the plain path's waves, with its own camera and
+    lights, beside small jobs batched as before: every film equals its plain render bit for bit."""
+    from repackshot_b200 import scenes
+    base = scenes.cfg4_scene(width=64, height=36, spp=1)
+    s = rtg.Scene(scenes.to_rsb(base))
+    sizes = [(2048, 2048, 4, 3), (64, 36, 2, 5), (96, 54, 3, 6)]  # the first: 16,777,216 paths
+    jobs = [(scenes.to_rsb(scenes.cfg4_scene(width=w, height=h, spp=n, rig=scenes.light_rig(r), seed=1 + r), meshes=False), w, h, n)
+            for w, h, n, r in sizes]
+    q = rtg.Queue(s)
+    films = [q.add(b, 0, n, w, h) for b, w, h, n in jobs]
+    q.run()
+    for (b, w, h, n), qf in zip(jobs, films):
+        s.update(b)
+        f = s.film()
+        f.render(0, n)
+        for x, y in zip(qf.read(), f.read()):
+            assert np.array_equal(np.asarray(x).view(np.uint32), np.asarray(y).view(np.uint32)), (w, h)
