@@ -246,14 +246,12 @@ __global__ void k_dn_lum(size_t n, const float* light, float* lum) {
     DN_LOOP(n) lum[p] = lum3(light[3 * p], light[3 * p + 1], light[3 * p + 2]);
 }
 
-// The variance blurred by a 3 x 3 Gaussian on the same surface (denoise.rs:628-654).
-__global__ void k_dn_gvar(uint32_t w, uint32_t h, Guides G_, const float* var, float* gvar) {
-    const size_t n = (size_t)w * h;
-    DN_LOOP(n) {
-        const uint2 id = G_.ids(p);
-        if (id.x == 0) continue;
-        const int x = (int)(p % w), y = (int)(p / w);
-        float sw = 0.0f, sv = 0.0f;
+// The variance of pixel p blurred by a 3 x 3 Gaussian on the same surface (denoise.rs:628-654).
+// Only the a-trous pass of the same level reads it, for its own pixel, so the pass computes it.
+__device__ __forceinline__ float gauss_var(uint32_t w, uint32_t h, const Guides& G_, const float* var, size_t p, uint2 id) {
+    const int x = (int)(p % w), y = (int)(p / w);
+    float sw = 0.0f, sv = 0.0f;
+    {
         for (int j = 0; j < 3; ++j) {
             const int qy = y + j - 1;
             if (qy < 0 || qy >= (int)h) continue;
@@ -268,20 +266,21 @@ __global__ void k_dn_gvar(uint32_t w, uint32_t h, Guides G_, const float* var, f
                 sv = sv + k * var[q];
             }
         }
-        gvar[p] = sw > 0.0f ? sv / sw : var[p];
     }
+    return sw > 0.0f ? sv / sw : var[p];
 }
 
 // One a-trous pass, taps `step` pixels apart (denoise.rs:655-708), and the luminance of its result.
 __global__ void k_dn_atrous(uint32_t w, uint32_t h, int step, Guides G_, const float* light, const float* var, const float* lum,
-                            const float* gvar, float* light_next, float* var_next, float* lum_next) {
+                            float* light_next, float* var_next, float* lum_next) {
     const size_t n = (size_t)w * h;
     DN_LOOP(n) {
         const G g = G_.load(p);
         if (!g.fg()) continue;
         const int x = (int)(p % w), y = (int)(p / w);
         const float lp = lum[p];
-        const float inv_sigma_l = 1.0f / (SIGMA_LUMINANCE * sqrt_(max_rs(gvar[p], 0.0f) + 1.0e-10f));
+        const float gv = gauss_var(w, h, G_, var, p, make_uint2(g.part, g.material));
+        const float inv_sigma_l = 1.0f / (SIGMA_LUMINANCE * sqrt_(max_rs(gv, 0.0f) + 1.0e-10f));
         float sw = 0.0f, sv = 0.0f, sc0 = 0.0f, sc1 = 0.0f, sc2 = 0.0f;
         for (int j = 0; j < 5; ++j) {
             const int dy = (j - 2) * step;
@@ -376,7 +375,8 @@ cudaError_t denoise_band(const DnSrc& src, uint32_t width, uint32_t rows, uint32
     float* var[2] = {(float*)take(n * 4), (float*)take(n * 4)};
     float* var0 = (float*)take(n * 4);
     float* lum[2] = {(float*)take(n * 4), (float*)take(n * 4)};
-    float* gvar = (float*)take(n * 4);
+    float* gvar = (float*)take(n * 4);  // (kept in the layout; the a-trous pass blurs the variance itself)
+    (void)gvar;
     float* before = (float*)take(n * 4);
     uint32_t* ffly = (uint32_t*)take(n * 4);
     uint32_t* changed = (uint32_t*)take(256);
@@ -407,10 +407,8 @@ cudaError_t denoise_band(const DnSrc& src, uint32_t width, uint32_t rows, uint32
     if ((e = cudaMemcpyAsync(var[cur ^ 1], var[cur], n * 4, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
     int l = 0;
     for (uint32_t level = 0; level < preset.levels; ++level) {
-        k_dn_gvar<<<grid, 256, 0, st>>>(width, rows, G_, var[cur], gvar);
-        k_dn_atrous<<<grid, 256, 0, st>>>(width, rows, 1 << level, G_, light[l], var[cur], lum[l], gvar, light[l ^ 1], var[cur ^ 1],
-                                          lum[l ^ 1]);
-        launches += 2;
+        k_dn_atrous<<<grid, 256, 0, st>>>(width, rows, 1 << level, G_, light[l], var[cur], lum[l], light[l ^ 1], var[cur ^ 1], lum[l ^ 1]);
+        launches += 1;
         l ^= 1;
         cur ^= 1;
     }
