@@ -35,8 +35,8 @@ def lib():
             "orc_scene_info": (u32, [u32, v]),
             "orc_render_film": (u64, [u32, u32, u32, u32, u32, u32, u32, u32, u32, v, v, v, v, v]),
             "orc_render_tile": (u64, [u32, u32, u32, u32, u32, u32, v, v]),
-            "orc_paths": (None, [u32, v, u32, v]),
-            "orc_trace": (None, [u32, v, u32, u32, u32, v, v]),
+            "orc_paths": (None, [u32, v, u32, v, u32]),
+            "orc_trace": (None, [u32, v, u32, u32, u32, v, v, u32]),
             "orc_occluded": (None, [u32, v, u32, v]),
             "orc_energy_tables": (None, [v, v]),
             "orc_enable_merged_stats": (u32, [u32]),
@@ -58,6 +58,7 @@ def lib():
             "orc_filter_offset": (None, [u32, v, u32, v]),
             "orc_ies": (u32, [ctypes.c_char_p, u32, v, u32, v, v, u32, v, v]),
             "orc_blackman_harris_table": (None, [v]),
+            "orc_set_sky_table": (None, [v, u32]),
             "orc_edge_mask": (None, [u32, v]),
             "orc_adaptive_decide": (u32, [u32, u32, ctypes.c_float, ctypes.c_float, u32, v, v, v, v, v]),
             "orc_adaptive_film": (u32, [u32, u32, u32, u32, v, v, v, v, v, v]),
@@ -71,6 +72,9 @@ def lib():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
+        # the physical sky's fitted table: the same data file the product compiles in
+        table = np.fromfile(HERE.parent / "repackshot_b200" / "data" / "sky_table.f32", dtype="<f4")
+        L.orc_set_sky_table(table.ctypes.data_as(ctypes.c_void_p), len(table))
         _lib = L
     return _lib
 
@@ -130,17 +134,19 @@ class OracleScene:
             return rgb
         return np.concatenate([rgb.reshape(-1, 3), al.reshape(-1, 1)], axis=1).reshape(-1)
 
-    def paths(self, xys):
+    def paths(self, xys, threads=0):
+        """Per-path radiance (r, g, b, alpha, rays) of (x, y, sample) triples; `threads` workers
+        (0: the host's cores)."""
         xys = np.ascontiguousarray(xys, dtype=np.uint32).reshape(-1, 3)
         out = np.zeros((len(xys), 5), np.float32)
-        lib().orc_paths(self.handle, _p(xys), len(xys), _p(out))
+        lib().orc_paths(self.handle, _p(xys), len(xys), _p(out), int(threads))
         return out
 
-    def trace(self, rays, camera=False, brute=False):
+    def trace(self, rays, camera=False, brute=False, threads=0):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
         hits = np.zeros((len(rays), 3), np.uint32)
         st = np.zeros(2, np.uint64)
-        lib().orc_trace(self.handle, _p(rays), len(rays), int(camera), int(brute), _p(hits), _p(st))
+        lib().orc_trace(self.handle, _p(rays), len(rays), int(camera), int(brute), _p(hits), _p(st), int(threads))
         return hits, (int(st[0]), int(st[1]))
 
     def light_count(self):

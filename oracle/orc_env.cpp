@@ -483,29 +483,103 @@ Rgb Preetham::radiance(Vec3 dir) const {
     for (int q = 0; q < 3; ++q) v[q] = zenith_over_perez[q] * perez(coefficients[q], cos_theta, gamma, cos_gamma);
     return xyy_to_rgb(v[1], rmax(v[2], 1.0e-4f), rmax(v[0], 0.0f));
 }
-// environment.rs:207 tabulate_sky for the classic model (plain sums): the upper half from the
-// model, scaled so that a horizontal surface gets the dome's irradiance 2 pi (horizon / 6 +
-// zenith / 3) strength; the lower half the ground, floor * strength.
-Image sky_image(const Environment& env) {
-    Preetham sky = Preetham::make(env.sun_azimuth_deg, env.sun_elevation_deg, env.sky_turbidity);
+// ---- sky.rs:96-198 the physical sky: the Hosek-Wilkie form, coefficients from the fitted table ----
+// The table (set by orc_set_sky_table): 3240 coefficients [turbidity 1..10][albedo 0, 1][R, G, B]
+// [control point 0..5][A..I], then 360 radiances [turbidity][albedo][R, G, B][control point].
+static std::vector<float> g_sky_table;
+PhysicalSky PhysicalSky::make(float azimuth_deg, float elevation_deg, float turbidity, float albedo) {  // sky.rs:113
+    PhysicalSky p;
+    float t = finite(turbidity) ? rclamp(turbidity, 1.0f, 10.0f) : 3.0f;
+    float elevation = finite(elevation_deg) ? rclamp(elevation_deg, 0.0f, 90.0f) : 45.0f;
+    float azimuth = finite(azimuth_deg) ? azimuth_deg : 0.0f;
+    float a = finite(albedo) ? rclamp(albedo, 0.0f, 1.0f) : 0.2f;
+    float se, ce, sa, ca;
+    sin_cos(elevation * DEG_TO_RAD, se, ce);
+    sin_cos(azimuth * DEG_TO_RAD, sa, ca);
+    p.sun = Vec3(ce * ca, ce * sa, se);
+    float x = powf_(elevation / 90.0f, 1.0f / 3.0f);
+    float y = 1.0f - x, x2 = x * x, y2 = y * y, x3 = x2 * x, y3 = y2 * y;
+    float bern[6] = {y3 * y2, 5.0f * x * y2 * y2, 10.0f * x2 * y3, 10.0f * x3 * y2, 5.0f * x2 * x2 * y, x3 * x2};  // sky.rs:91
+    float tt = t - 1.0f;
+    int i = std::min((int)std::floor(tt), 8);
+    float f = tt - (float)i;
+    int tis[2] = {i, i + 1};
+    float wts[2] = {1.0f - f, f}, was[2] = {1.0f - a, a};
+    p.n = 0;
+    if (g_sky_table.size() != 3600) return p;
+    for (int u = 0; u < 2; ++u)
+        for (int ai = 0; ai < 2; ++ai) {
+            float weight = wts[u] * was[ai];
+            if (weight <= 0.0f) continue;
+            Knot& k = p.knots[p.n++];
+            k = Knot{};
+            k.weight = weight;
+            for (int c = 0; c < 3; ++c) {
+                int base = (tis[u] * 2 + ai) * 3 + c;
+                for (int m = 0; m < 6; ++m) {
+                    for (int j = 0; j < 9; ++j) k.coefficients[c][j] += bern[m] * g_sky_table[(base * 6 + m) * 9 + j];
+                    k.radiance[c] += bern[m] * g_sky_table[3240 + base * 6 + m];
+                }
+            }
+        }
+    return p;
+}
+Rgb PhysicalSky::radiance(Vec3 dir) const {  // sky.rs:170
+    if (dir.z <= 0.0f) return BLACK;
+    float cos_theta = dir.z;
+    float cos_gamma = rclamp(dot(dir, sun), -1.0f, 1.0f);
+    float gamma = fatan2(length(cross(dir, sun)), dot(dir, sun));
+    Vec3 chord = dir - sun;
+    float chord2 = dot(chord, chord);
+    float cg2 = cos_gamma * cos_gamma;
+    float horizon = 1.0f / (cos_theta + 0.01f);
+    float sq = std::sqrt(cos_theta);
+    float out[3] = {0.0f, 0.0f, 0.0f};
+    for (int k = 0; k < n; ++k)
+        for (int c = 0; c < 3; ++c) {
+            const float* q = knots[k].coefficients[c];
+            float den = (1.0f - q[7]) * (1.0f - q[7]) + q[7] * chord2;
+            float chi = (1.0f + cg2) / (den * std::sqrt(den));
+            float value = (1.0f + q[0] * sky_exp(q[1] * horizon)) * (q[2] + q[3] * sky_exp(q[4] * gamma) + q[5] * cg2 + q[6] * chi + q[8] * sq);
+            out[c] += knots[k].weight * value * knots[k].radiance[c];
+        }
+    return Rgb(rmax(out[0], 0.0f), rmax(out[1], 0.0f), rmax(out[2], 0.0f));
+}
+
+// environment.rs:204 add_compensated: sum += x with Neumaier's compensation c.
+static void add_compensated(float& sum, float& c, float x) {
+    float t = sum + x;
+    if (std::fabs(sum) >= std::fabs(x)) c += (sum - t) + x;
+    else c += (x - t) + sum;
+    sum = t;
+}
+
+// environment.rs:216 tabulate_sky: the upper half from the model, scaled so that a horizontal
+// surface gets the dome's irradiance 2 pi (horizon / 6 + zenith / 3) strength; the lower half the
+// ground, floor * strength. The physical sky sums with compensation, the classic one plainly.
+template <class Sky>
+static Image tabulate_sky(const Environment& env, const Sky& sky, bool compensated) {
     const uint32_t w = 256, h = 128;
     std::vector<float> rgb(3 * (size_t)w * h, 0.0f);
-    float irradiance = 0.0f;
+    float irradiance = 0.0f, irradiance_c = 0.0f;
     const float cell = (PI / (float)h) * (TAU / (float)w);
     for (uint32_t y = 0; y < h / 2; ++y) {
         float v = ((float)y + 0.5f) / (float)h;
-        float row = 0.0f;
+        float row = 0.0f, row_c = 0.0f;
         for (uint32_t x = 0; x < w; ++x) {
             float u = ((float)x + 0.5f) / (float)w, sin_theta;
             Vec3 d = uv_to_direction(u, v, sin_theta);
             Rgb c = sky.radiance(d);
             float* o = &rgb[3 * ((size_t)y * w + x)];
             o[0] = c.r; o[1] = c.g; o[2] = c.b;
-            row += c.luminance() * d.z * sin_theta;
+            float term = c.luminance() * d.z * sin_theta;
+            if (compensated) add_compensated(row, row_c, term);
+            else row += term;
         }
-        irradiance += row * cell;
+        if (compensated) add_compensated(irradiance, irradiance_c, (row + row_c) * cell);
+        else irradiance += row * cell;
     }
-    irradiance = irradiance + 0.0f;
+    irradiance = irradiance + irradiance_c;
     float strength = rmax(env.strength, 0.0f);
     float target = strength * TAU * (rmax(env.horizon, 0.0f) / 6.0f + rmax(env.zenith, 0.0f) / 3.0f);
     float scale = irradiance > 0.0f ? target / irradiance : 0.0f;
@@ -517,6 +591,22 @@ Image sky_image(const Environment& env) {
     img.linear = std::move(rgb);
     return img;
 }
+
+// environment.rs:178 sky_image: the scene's sky model tabulated.
+Image sky_image(const Environment& env) {
+    if (env.sky_model == 1)
+        return tabulate_sky(env, Preetham::make(env.sun_azimuth_deg, env.sun_elevation_deg, env.sky_turbidity), false);
+    return tabulate_sky(env, PhysicalSky::make(env.sun_azimuth_deg, env.sun_elevation_deg, env.sky_turbidity, 0.2f), true);
+}
+
+}  // namespace orc
+
+extern "C" {
+// The physical sky's fitted table: n = 3600 floats (3240 coefficients, then 360 radiances).
+void orc_set_sky_table(const float* values, uint32_t n) { orc::g_sky_table.assign(values, values + n); }
+}
+
+namespace orc {
 
 EnvLight EnvLight::make(const Environment& env, const std::vector<Image>& bitmaps) {  // environment.rs:335
     EnvLight e;

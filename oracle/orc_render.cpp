@@ -300,8 +300,11 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
         if (material && material->is_emissive()) {
             bool one_sided = (geo.instances[inst].flags & INSTANCE_ONE_SIDED) != 0;
             if (s_front || !one_sided) {
-                // Emitters that are not mesh lights weigh 1 (light.rs:1541).
-                prep.add(sum, throughput * material->radiance() * 1.0f, bounce >= 2);
+                // A BSDF-sampled ray that finds a mesh light weighs its emission against the light's
+                // next-event sample; other emitters (and camera rays) weigh 1 (integrator/mod.rs:1556,
+                // light.rs:1543).
+                float weight = has_pdf ? lights.emitter_weight(inst, bsdf_pdf, sampled_at, offset + t_geometry, dot(s_geometric, ray.dir)) : 1.0f;
+                prep.add(sum, throughput * material->radiance() * weight, bounce >= 2);
             }
             break;
         }
@@ -654,6 +657,20 @@ Loaded* get(uint32_t h) {
 }
 }  // namespace
 
+// Runs fn(begin, end, worker) over [0, n) in `threads` contiguous chunks (0: the host's cores).
+template <class F>
+static void parallel_chunks(uint32_t n, uint32_t threads, F fn) {
+    if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+    threads = std::max(1u, std::min(threads, n / 16 + 1));
+    std::vector<std::thread> pool;
+    const uint32_t per = (n + threads - 1) / threads;
+    for (uint32_t t = 0; t < threads; ++t) {
+        const uint32_t b = std::min(n, t * per), e = std::min(n, b + per);
+        pool.emplace_back([=]() { fn(b, e, t); });
+    }
+    for (auto& th : pool) th.join();
+}
+
 extern "C" {
 
 // Loads an RSB scene; 0 on error (orc_error gives the message).
@@ -901,26 +918,34 @@ uint64_t orc_render_tile(uint32_t h, uint32_t x, uint32_t y, uint32_t w, uint32_
 }
 
 // Per-path radiance of explicit (pixel x, pixel y, sample) triples: out = r, g, b, alpha, rays.
-void orc_paths(uint32_t h, const uint32_t* xys, uint32_t n, float* out5) {
+// Every path is independent, so `threads` workers (0: the host's cores) give the same output.
+void orc_paths(uint32_t h, const uint32_t* xys, uint32_t n, float* out5, uint32_t threads) {
     Loaded* l = get(h);
     if (!l) return;
-    for (uint32_t i = 0; i < n; ++i) {
+    parallel_chunks(n, threads, [&](uint32_t b, uint32_t e, uint32_t) {
+    for (uint32_t i = b; i < e; ++i) {
         PathStats st;
         Rgb c;
         float a;
         shade_pixel(l->scene, l->prep, xys[3 * i], xys[3 * i + 1], xys[3 * i + 2], c, a, st);
         out5[5 * i] = c.r; out5[5 * i + 1] = c.g; out5[5 * i + 2] = c.b; out5[5 * i + 3] = a; out5[5 * i + 4] = (float)st.rays;
     }
+    });
 }
 
 // Nearest hits of a ray batch (ray = ox oy oz dx dy dz tmin tmax); hits = instance, triangle,
 // t bits (0xffffffff instance: miss). `brute` uses every triangle instead of the BVH. stats2
-// (may be null) gets inner-node visits and packet tests summed over the batch.
-void orc_trace(uint32_t h, const float* rays, uint32_t n, uint32_t camera, uint32_t brute, uint32_t* hits, uint64_t* stats2) {
+// (may be null) gets inner-node visits and packet tests summed over the batch. `threads` workers
+// (0: the host's cores) share the batch.
+void orc_trace(uint32_t h, const float* rays, uint32_t n, uint32_t camera, uint32_t brute, uint32_t* hits, uint64_t* stats2,
+               uint32_t threads) {
     Loaded* l = get(h);
     if (!l) return;
+    std::mutex mu;
+    uint64_t nodes = 0, packets = 0;
+    parallel_chunks(n, threads, [&](uint32_t b, uint32_t e, uint32_t) {
     TraceStats st;
-    for (uint32_t i = 0; i < n; ++i) {
+    for (uint32_t i = b; i < e; ++i) {
         const float* r = rays + 8 * i;
         Ray ray(Vec3(r[0], r[1], r[2]), Vec3(r[3], r[4], r[5]));
         ray.t_min = r[6];
@@ -931,7 +956,11 @@ void orc_trace(uint32_t h, const float* rays, uint32_t n, uint32_t camera, uint3
         hits[3 * i + 1] = got ? hit.triangle : 0xffffffffu;
         hits[3 * i + 2] = got ? fbits(hit.t) : 0u;
     }
-    if (stats2) { stats2[0] = st.nodes; stats2[1] = st.packets; }
+    std::lock_guard<std::mutex> lk(mu);
+    nodes += st.nodes;
+    packets += st.packets;
+    });
+    if (stats2) { stats2[0] = nodes; stats2[1] = packets; }
 }
 // Any-hit of a ray batch: occluded[i] = 1 when something lies in [tmin, tmax].
 void orc_occluded(uint32_t h, const float* rays, uint32_t n, uint8_t* occluded) {

@@ -201,7 +201,6 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
                   r.opt_f32(e.backplate_rect[0], 0.0f) && r.opt_f32(e.backplate_rect[1], 0.0f) && r.opt_f32(e.backplate_rect[2], 1.0f) &&
                   r.opt_f32(e.backplate_rect[3], 1.0f) && r.opt_u32(e.sky_model, 0)))
                 return false;
-            if (e.kind == 2 && e.sky_model != 1) { error = "unsupported: physical sky model"; return false; }
         } else if (is("IESP")) {  // rsb.rs:1018
             uint32_t n;
             if (!r.u32(n)) return false;
@@ -282,7 +281,6 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
     }
     // Material features outside this path (their branches of the reference integrator).
     for (const Material& m : scene.materials) {
-        if (m.is_emissive() && (m.flags & MATERIAL_FLAG_LIGHT)) { error = "unsupported: emissive mesh lights"; return false; }
         if (m.scatter_mm > 0.0f && m.transmission > 0.0f) { error = "unsupported: scattering media"; return false; }
         if (m.abbe > 0.0f && m.transmission > 0.0f) { error = "unsupported: dispersive glass"; return false; }
         if (m.bevel_mm > 0.0f) { error = "unsupported: edge bevel"; return false; }
@@ -369,6 +367,13 @@ bool AreaLight::intersect(const Ray& ray, float t_max, float& t, float& cos) con
     if (!inside) return false;
     cos = -denom;
     return true;
+}
+float MeshEmitter::weight(Vec3 x) const {  // light.rs:468: lum(L) A cos' / max(d^2, A) from its centroid
+    Vec3 v = x - centroid;
+    float d2 = length_squared(v);
+    float o = cos_o <= -1.0f ? 1.0f : orientation_bound(v, d2, axis, cos_o, sin_o, bound);
+    if (o <= 0.0f) return 0.0f;
+    return base * o / (rmax(d2, area) * 1.0e-6f);
 }
 float AreaLight::weight(Vec3 x) const {
     Vec3 v = x - centre;
@@ -581,6 +586,72 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
         a.base = a.radiance.luminance() * a.area * 1.0e-6f;
         L.areas.push_back(a);
     }
+    // light.rs:867-958: every emissive instance whose material is flagged as a light, sampled by
+    // area over its world-space triangles.
+    const Geometry& geo = scene.geometry;
+    L.instance_emitter.assign(geo.instances.size(), -1);
+    for (size_t i = 0; i < geo.instances.size(); ++i) {
+        const Instance& inst = geo.instances[i];
+        if (inst.material_id >= scene.materials.size()) continue;
+        const Material& mat = scene.materials[inst.material_id];
+        Rgb radiance = mat.radiance();
+        if (!(mat.flags & MATERIAL_FLAG_LIGHT) || !(radiance.luminance() > 0.0f)) continue;
+        if (inst.mesh >= geo.meshes.size()) continue;
+        const Mesh& mesh = geo.meshes[inst.mesh];
+        Transform inv;
+        if (!inst.transform.inverse(inv)) continue;  // never hit, so never lit either
+        MeshEmitter em{};
+        std::vector<float> tri_areas;
+        Vec3 centroid(0, 0, 0);
+        for (size_t t = 0; t < mesh.triangle_count(); ++t) {
+            uint32_t ia = mesh.indices[3 * t], ib = mesh.indices[3 * t + 1], ic = mesh.indices[3 * t + 2];
+            if (ia >= mesh.positions.size() || ib >= mesh.positions.size() || ic >= mesh.positions.size()) continue;
+            std::array<Vec3, 3> w = {inst.transform.point(mesh.positions[ia]), inst.transform.point(mesh.positions[ib]),
+                                     inst.transform.point(mesh.positions[ic])};
+            Vec3 c = cross(w[1] - w[0], w[2] - w[0]);
+            float a = 0.5f * length(c);
+            if (!(a > 0.0f && finite(a))) continue;
+            centroid = centroid + (w[0] + w[1] + w[2]) * (a / 3.0f);
+            em.corners.push_back(w);
+            em.normals.push_back(normalize(c));
+            tri_areas.push_back(a);
+        }
+        float area = 0.0f;
+        for (float a : tri_areas) area += a;
+        em.cdf = build_cdf(tri_areas);
+        if (em.cdf.empty()) continue;
+        em.two_sided = (inst.flags & INSTANCE_ONE_SIDED) == 0;
+        float sides = em.two_sided ? 2.0f : 1.0f;
+        float flux = radiance.luminance() * PI * area * 1.0e-6f * sides;
+        centroid = centroid / area;
+        float bound = 0.0f;
+        for (const auto& w : em.corners)
+            for (const Vec3& q : w) bound = rmax(bound, length(q - centroid));
+        Vec3 mean(0, 0, 0);
+        for (size_t k = 0; k < em.normals.size(); ++k) mean = mean + em.normals[k] * tri_areas[k];
+        float len = length(mean);
+        if (em.two_sided || len <= 1.0e-3f * area) {
+            em.axis = Vec3(0, 0, 1);
+            em.cos_o = -1.0f;
+            em.sin_o = 0.0f;
+        } else {
+            em.axis = mean / len;
+            float c = 1.0f;
+            for (const Vec3& n : em.normals) c = rmin(c, dot(n, em.axis));
+            em.cos_o = rclamp(c, -1.0f, 1.0f);
+            em.sin_o = std::sqrt(rmax(1.0f - em.cos_o * em.cos_o, 0.0f));
+        }
+        weights.push_back(flux * reach(centroid, nullptr));
+        em.entry = (uint32_t)L.entries.size();
+        L.entries.push_back({LightRef::Mesh, (uint32_t)L.meshes.size()});
+        L.instance_emitter[i] = (int)L.meshes.size();
+        em.area = area;
+        em.radiance = radiance;
+        em.centroid = centroid;
+        em.bound = bound;
+        em.base = radiance.luminance() * area * 1.0e-6f;
+        L.meshes.push_back(std::move(em));
+    }
     L.env = EnvLight::make(scene.environment, scene.bitmaps);
     L.env_base = PI * L.env.mean_radiance();
     if (!L.env.is_black()) {
@@ -602,6 +673,7 @@ float Lights::weight(size_t entry, Vec3 x) const {  // light.rs:1014
         case LightRef::Area: return areas[e.index].weight(x);
         case LightRef::Sun: return suns[e.index].base;
         case LightRef::Sphere: return spheres[e.index].weight(x);
+        case LightRef::Mesh: return meshes[e.index].weight(x);
         default: return env_base;
     }
 }
@@ -699,6 +771,24 @@ bool Lights::sample_selected(const Selection& from, float u_select, float u0, fl
         if (!(cos > 0.0f && distance > 0.0f)) return false;
         out = {wi, distance, light.radiance_at(cos), pmf_v * dist2 / (light.area * cos), false, light.glossy, light.glossy,
                light.shadow};
+    } else if (e.kind == LightRef::Mesh) {  // light.rs:1270: a triangle by area, a point on it uniformly
+        const MeshEmitter& em = meshes[e.index];
+        size_t t;
+        float unused;
+        pick(em.cdf, rest, t, unused);
+        const std::array<Vec3, 3>& c = em.corners[t];
+        float su = std::sqrt(u0);  // warp.rs:57 uniform_triangle
+        float b0 = 1.0f - su, b1 = u1 * su, b2 = 1.0f - b0 - b1;
+        Vec3 p = c[0] * b0 + c[1] * b1 + c[2] * b2;
+        Vec3 d = p - x;
+        float dist2 = length_squared(d);
+        float distance = std::sqrt(dist2);
+        Vec3 wi = d / distance;
+        float facing = -dot(wi, em.normals[t]);
+        if (!(distance > 0.0f) || (!em.two_sided && facing <= 0.0f)) return false;
+        float cos = std::fabs(facing);
+        if (!(cos > 0.0f)) return false;
+        out = {wi, distance, em.radiance, pmf_v * dist2 / (em.area * cos), false, true, true, true};
     } else {
         Vec3 wi;
         float p;
@@ -741,6 +831,12 @@ Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, con
         sum = sum + light.radiance * (m * w);
     }
     return sum;
+}
+float Lights::emitter_weight(uint32_t instance, float bsdf_pdf, const Selection& from, float t, float cos) const {
+    if (instance >= instance_emitter.size() || instance_emitter[instance] < 0) return 1.0f;
+    const MeshEmitter& em = meshes[(size_t)instance_emitter[instance]];
+    float light_pdf = pmf(em.entry, from) * t * t / (em.area * rmax(std::fabs(cos), 1.0e-7f));
+    return power_heuristic(bsdf_pdf, light_pdf);  // light.rs:1090 found_weight
 }
 bool Lights::camera_sees_panel(const Ray& ray, float t_max) const {
     for (const AreaLight& a : areas) {

@@ -2,6 +2,7 @@
 // camera, restated from engine/crates/rt-core/src/{scene/mod.rs, scene/rsb.rs, light.rs,
 // environment.rs}.
 #pragma once
+#include <array>
 #include <memory>
 #include <string>
 #include <vector>
@@ -142,7 +143,22 @@ struct Preetham {
     static Preetham make(float azimuth_deg, float elevation_deg, float turbidity);
     Rgb radiance(Vec3 dir) const;
 };
-// environment.rs:178 sky_image: the sky tabulated into a 256 x 128 map (the classic model only)
+// sky.rs:96 the physical sky (the Hosek-Wilkie form with the fitted table) before scaling: up to
+// four knots (two turbidities times two ground albedos), blended by radiance.
+struct PhysicalSky {
+    struct Knot {
+        float weight;
+        float coefficients[3][9];
+        float radiance[3];
+    };
+    Vec3 sun;
+    Knot knots[4];
+    int n = 0;
+    static PhysicalSky make(float azimuth_deg, float elevation_deg, float turbidity, float albedo);
+    Rgb radiance(Vec3 dir) const;
+};
+// environment.rs:178 sky_image: the sky (physical, or classic with sky_model 1) tabulated into a
+// 256 x 128 map
 Image sky_image(const Environment& env);
 
 // environment.rs:333 EnvLight: the ramp or a map
@@ -201,16 +217,33 @@ struct SphereLight {  // light.rs:330 (point lights, spots and IES lights)
     bool intersect(const Ray& ray, float t_max, float& t) const;
     float weight(Vec3 x) const;
 };
+struct MeshEmitter {  // light.rs:440: an emissive instance sampled as an area light
+    std::vector<std::array<Vec3, 3>> corners;  // world-space corners of each triangle
+    std::vector<Vec3> normals;                 // unit normal of each (winding order: the front)
+    std::vector<float> cdf;                    // cumulative area fractions
+    float area;                                // mm^2
+    Rgb radiance;
+    bool two_sided;
+    uint32_t entry;
+    Vec3 centroid;       // area-weighted centre of its triangles
+    float bound;         // radius of the sphere around the centroid that holds it
+    Vec3 axis;           // the cone of its front faces' normals: axis, cos, sin (cos -1: any)
+    float cos_o, sin_o;
+    float base;          // lum(L) A, A in m^2
+    float weight(Vec3 x) const;
+};
 struct Selection { Vec3 point; float total = 0; bool by_flux = true; float weights[8] = {}; };
 struct LightSample { Vec3 wi; float distance; Rgb radiance; float pdf; bool delta, glossy, photon, shadow; };
 struct LightRef {  // light.rs:488
-    enum Kind : uint32_t { Area, Sun, Sphere, Environment } kind;
+    enum Kind : uint32_t { Area, Sun, Sphere, Mesh, Environment } kind;
     uint32_t index;
 };
 struct Lights {
     std::vector<AreaLight> areas;
     std::vector<SunLight> suns;
     std::vector<SphereLight> spheres;
+    std::vector<MeshEmitter> meshes;
+    std::vector<int> instance_emitter;  // per instance: its mesh emitter, or -1
     EnvLight env;
     bool env_is_entry = false;
     uint32_t env_entry = 0;
@@ -228,6 +261,10 @@ struct Lights {
     void pick_at(const Selection& s, float u, size_t& idx, float& rest, float& pmf_out) const;
     bool sample_selected(const Selection& s, float u_select, float u0, float u1, LightSample& out) const;
     Rgb crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, const Selection* from, float offset) const;
+    // light.rs:1536-1550: for a BSDF-sampled ray that hit emissive instance `instance` at
+    // distance t with `cos` between the ray and the geometric normal, the MIS weight of the emission
+    // found (1 when the instance is not a mesh light).
+    float emitter_weight(uint32_t instance, float bsdf_pdf, const Selection& from, float t, float cos) const;
     // light.rs:1490: a camera ray meets a light it sees (an area light flagged camera, or a sphere
     // flagged camera lit towards the ray's origin) before t_max.
     bool camera_sees_panel(const Ray& ray, float t_max) const;

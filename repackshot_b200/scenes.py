@@ -268,6 +268,8 @@ def example_scene() -> Scene:
 
 LIGHT_SUN, LIGHT_POINT, LIGHT_SPOT = 2, 3, 4
 MATERIAL_GLASS, MATERIAL_FLAG_THIN = 1, 2
+MATERIAL_EMISSIVE, MATERIAL_FLAG_LIGHT = 2, 1  # scene/mod.rs:367-370: an emitter; sampled as a light
+INSTANCE_ONE_SIDED = 1  # geometry/mod.rs:54
 
 
 def _rgb_to_rgbe(c) -> bytes:
@@ -363,6 +365,19 @@ def e5_scene(sky: bool = False) -> Scene:
         s.sun_azimuth_deg, s.sun_elevation_deg = -60.0, 35.0
         s.lights = [Light(kind=LIGHT_SUN, position=(0.0, 0.0, 1000.0), direction=(-0.41, 0.71, -0.574), up=(0.0, 1.0, 0.0),
                           size_x=500.0, size_y=500.0, color=(1.0, 0.91, 0.83), power=3.0, angle_deg=0.545, flags=3)]
+    return s
+
+
+def e5c_scene() -> Scene:
+    """example.rs:361 e5c_scene: the E5 sky scene under the physical sky (turbidity 2.5, the sun 12
+    degrees up at azimuth -60). The sun light points along the sky's sun, -(cos e cos a, cos e sin a,
+    sin e), from the reference's deterministic sin/cos of those angles (fmath.rs), written here as
+    the f32 values they give; its colour is (1, 0.78, 0.6)."""
+    s = e5_scene(sky=True)
+    s.sky_model, s.sky_turbidity = 0, 2.5
+    s.sun_azimuth_deg, s.sun_elevation_deg = -60.0, 12.0
+    s.lights[0].direction = (float.fromhex("-0x1.f4cfc2p-2"), float.fromhex("0x1.b1b73p-1"), float.fromhex("-0x1.a9cd9cp-3"))
+    s.lights[0].color = (1.0, 0.78, 0.6)
     return s
 
 
@@ -463,6 +478,21 @@ def cfg0_scene() -> Scene:
                       size_x=2000.0, size_y=2000.0, power=rect_power(10.0, 2.0, 2.0), flags=3)],
         env_kind=1, env_floor=0.1, env_horizon=0.1, env_zenith=0.1, env_strength=1.0,
         width=w, height=h, max_samples=16, seed=1, max_depth=8)
+
+
+def emissive_scene(width: int = 96, height: int = 96, spp: int = 8) -> Scene:
+    """The small scene with two emissive meshes sampled as lights beside its rect light: a warm
+    two-sided icosphere (subdivision 1, radius 0.25 m) above the floor to the left and a one-sided
+    0.6 m square facing down-right, both in materials flagged as lights (light.rs:440-495)."""
+    s = cfg0_scene()
+    s.width, s.height, s.max_samples = width, height, spp
+    s.materials += [Material(kind=MATERIAL_EMISSIVE, emission=(1.0, 0.8, 0.6), emission_power=6.0, flags=MATERIAL_FLAG_LIGHT),
+                    Material(kind=MATERIAL_EMISSIVE, emission=(0.6, 0.8, 1.0), emission_power=12.0, flags=MATERIAL_FLAG_LIGHT)]
+    s.meshes.append(icosphere(yup_m_to_mm((-1.3, 0.5, 0.6)), 250.0, 1, 2))
+    q = np.array([(900.0, -300.0, 1500.0), (900.0, 300.0, 1500.0), (1500.0, 300.0, 2100.0), (1500.0, -300.0, 2100.0)], np.float32)
+    s.meshes.append(Mesh(q, np.zeros((4, 3), np.float32), np.array([0, 2, 1, 0, 3, 2], np.uint32), 3))
+    s.instances += [Instance(2, material_id=2), Instance(3, material_id=3, flags=INSTANCE_ONE_SIDED)]
+    return s
 
 
 def _value_noise3(p: np.ndarray, seed: int) -> np.ndarray:

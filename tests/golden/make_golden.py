@@ -8,7 +8,8 @@ its path tracer, read from the reference's own source tree (run where it is chec
   little-endian bytes of their u16 values and f32 bit patterns;
 * SHA-256 of the example scene file (tests/fixtures/example.rsb);
 * the FNV-1a film hashes of the E5 scene with its HDRI and with the classic sky (render.rs:1106-1109)
-  and SHA-256 of the HDRI scene's file (tests/fixtures/e5.rsb);
+  and SHA-256 of the HDRI scene's file (tests/fixtures/e5.rsb); the E5c scene's hash with the
+  physical sky (render.rs:1128);
 * the E11 film hash (render.rs:1250) and SHA-256 of the Blackman-Harris inverse-CDF table
   (pixel_filter.rs:64, 256 little-endian f32);
 * the L5 film hash (render.rs:1531), SHA-256 of its file (tests/fixtures/l5.rsb), and the two
@@ -19,7 +20,7 @@ its path tracer, read from the reference's own source tree (run where it is chec
 * the hashes of the denoised example: the full filter at 4 spp and the viewport's at 2 and 4 spp
   (engine/crates/rt-post/src/denoise/tests.rs:392, 527-528).
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/reference
 """
 from __future__ import annotations
 
@@ -30,7 +31,9 @@ import struct
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py /path/to/reference (the Repackshot checkout to read)")
+REF = Path(sys.argv[1])
 CORE = REF / "engine" / "crates" / "rt-core" / "src"
 OUT = Path(__file__).resolve().parent / "reference_pins.json"
 
@@ -52,6 +55,7 @@ def main():
         "tile_small_sphere_48_144_s3": pinned(render, "PINNED_SMALL_SPHERE"),
         "e5_hdri_4spp": pinned(render, "PINNED_E5_HDRI_4SPP"),
         "e5_sky_4spp": pinned(render, "PINNED_E5_SKY_4SPP"),
+        "e5c_physical_sky_4spp": pinned(render, "PINNED_E5C_SKY_4SPP"),
         "e11_edges_4spp": pinned(render, "PINNED_E11_EDGES_4SPP"),
         "l5_ies_4spp": pinned(render, "PINNED_L5_IES_4SPP"),
     }

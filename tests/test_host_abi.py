@@ -93,7 +93,7 @@ def test_malformed_scenes_are_refused_with_a_message(rtg, example_rsb):
 
 
 @pytest.mark.parametrize("change, words", [
-    (lambda s: setattr(s, "env_kind", 2), "physical sky"),
+    (lambda s: setattr(s.materials[0], "scatter_mm", 5.0) or setattr(s.materials[0], "transmission", 1.0), "scattering media"),
     (lambda s: setattr(s, "floor_mode", 2), "shadow catcher"),
     (lambda s: setattr(s.materials[0], "bevel_mm", 1.0), "bevel"),
     (lambda s: setattr(s.materials[0], "abbe", 30.0) or setattr(s.materials[0], "transmission", 1.0), "dispersive"),

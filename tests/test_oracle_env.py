@@ -10,6 +10,7 @@ byte and whose 4-sample film has the reference's pinned FNV-1a hash (render.rs:1
 the same scene under the classic sky with a sun, also pinned.
 """
 import hashlib
+from pathlib import Path
 import struct
 
 import numpy as np
@@ -140,11 +141,18 @@ def test_e5_under_the_classic_sky_has_the_pinned_hash(oracle_lib, pins):
     assert oracle_lib.fnv1a(oracle_lib.resolve(rgb, w)) == pins["film_hashes"]["e5_sky_4spp"]
 
 
-def test_the_physical_sky_is_refused(oracle_lib):
-    s = scenes.e5_scene(sky=True)
-    s.sky_model = 0
-    with pytest.raises(ValueError, match="physical sky"):
-        oracle_lib.OracleScene(scenes.to_rsb(s))
+def test_e5c_under_the_physical_sky_has_the_pinned_hash(oracle_lib, pins):
+    # render.rs:1112-1128: the physical sky (the fitted Hosek-Wilkie table) at 4 spp.
+    s = oracle_lib.OracleScene(scenes.to_rsb(scenes.e5c_scene()))
+    rgb, w, _, _, _ = s.render_film(0, 4, tile=32, threads=4)
+    assert oracle_lib.fnv1a(oracle_lib.resolve(rgb, w)) == pins["film_hashes"]["e5c_physical_sky_4spp"]
+
+
+def test_the_physical_sky_table_is_the_published_one():
+    # The table the product compiles in and the oracle loads: SHA-256 as sky_table.rs states it.
+    data = (Path(__file__).resolve().parent.parent / "repackshot_b200" / "data" / "sky_table.f32").read_bytes()
+    assert len(data) == 4 * 3600
+    assert hashlib.sha256(data).hexdigest() == "2329ac7376204749a317d5b31e23e17fa27950515be0f0d50018cd9c16e8a721"
 
 
 def test_bad_bitmap_indices_are_refused(oracle_lib):

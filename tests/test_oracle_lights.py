@@ -191,3 +191,43 @@ def test_ies_lights_are_refused(oracle_lib):
     s = lights_only(Light(kind=5, position=(0.0, 0.0, 400.0), power=1.0))
     with pytest.raises(ValueError, match="IES"):
         load(oracle_lib, s)
+
+
+def emissive_quad_scene(power=2.0, flags=scenes.MATERIAL_FLAG_LIGHT):
+    """light.rs:2032: two triangles of different size forming one 100 x 100 quad at z = 100,
+    facing down (winding 0 2 1, 0 3 2), in an emissive material of white emission at power 2."""
+    p = np.array([(-50.0, -50.0, 100.0), (50.0, -50.0, 100.0), (50.0, 50.0, 100.0), (-50.0, 50.0, 100.0)], np.float32)
+    quad = scenes.Mesh(p, np.zeros((4, 3), np.float32), np.array([0, 2, 1, 0, 3, 2], np.uint32), 0)
+    s = lights_only(meshes=[quad])
+    s.materials = [scenes.Material(kind=scenes.MATERIAL_EMISSIVE, emission=(1.0, 1.0, 1.0), emission_power=power, flags=flags)]
+    return s
+
+
+def test_emissive_meshes_are_sampled_by_area(oracle_lib):
+    # light.rs:2032 emissive_meshes_are_sampled_by_area: one mesh light; the irradiance at the
+    # origin below it by 64 x 64 stratified samples (the selection spread over the CDF as well)
+    # matches the square's form factor, 2 * 4 pi F(1/2, 1/2) for radiance 2, within 1%.
+    o = load(oracle_lib, emissive_quad_scene())
+    assert o.light_count() == 1
+    e = 0.0
+    for i in range(64):
+        for j in range(64):
+            sel = ((i * 64 + j) + 0.5) / 4096.0
+            s = o.light_sample((0.0, 0.0, 0.0), sel, ((i + 0.5) / 64, (j + 0.5) / 64))
+            assert s is not None
+            wi, dist, rad, pdf, delta, shadow = s
+            assert not delta and shadow and dist > 0.0
+            e += float(np.float32(rad[1] * wi[2] / pdf))
+
+    def f(x, y):
+        return (x / math.sqrt(1 + x * x) * math.atan(y / math.sqrt(1 + x * x))
+                + y / math.sqrt(1 + y * y) * math.atan(x / math.sqrt(1 + y * y))) / (2 * math.pi)
+
+    want = 2.0 * 4.0 * math.pi * f(0.5, 0.5)
+    assert abs(e / 4096.0 / want - 1.0) < 0.01
+
+
+def test_emitters_without_the_light_flag_are_not_sampled(oracle_lib):
+    o = load(oracle_lib, emissive_quad_scene(flags=0))
+    assert o.light_count() == 0
+    assert o.light_sample((0.0, 0.0, 0.0), 0.5, (0.5, 0.5)) is None
