@@ -41,9 +41,8 @@ WORKLOAD = ("1080p product scene: 1920x1080, 64 spp, max depth 12, seeded displa
 DATA = "synthetic (seeded procedural scene; no dataset)"
 FALLBACK_HBM_GBS = 6650.0
 BYTES_RAY_IO = 32 + 12  # ray in, hit out
-# DRAM bytes (read + write) per extend ray, from one full ncu capture of k_extend on this scene
-# (bounce 0 of a 4 Mi-path wave: 286 MB for 4,147,200 rays; profiles/k_extend_k_shadow_k_shade_
-# 1080p_product_4Mi_wave.md). Scaled to a launch by the rays it traces.
+# DRAM bytes (read + write) per extend ray, from one ncu capture of k_extend on this scene (bounce 0
+# of a 4 Mi-path wave: 286 MB for 4,147,200 rays). Scaled to a launch by the rays it traces.
 DRAM_BYTES_PER_EXTEND_RAY = 69.0
 
 
@@ -66,16 +65,27 @@ def sample_bands(n_bands: int, rows: int = 8):
     return [(i * step + (step - rows) // 2, rows) for i in range(n_bands)]
 
 
-def oracle_sample(orc_scene, bands, first, count, threads):
-    """Renders the bands with the oracle; returns (seconds, paths, stats summed)."""
+def oracle_sample(orc_scene, bands, first, count, threads, images=None):
+    """Renders the bands with the oracle; returns (seconds, paths, stats summed). With `images`
+    (a list), each band's resolved pixels are appended to it."""
+    import oracle
     t0 = time.perf_counter()
     stats = np.zeros(11, np.int64)
     paths = 0
     for y, rows in bands:
-        *_, st = orc_scene.render_film(first, count, x=0, y=y, w=WIDTH, h=rows, tile=32, threads=threads)
+        rgb, wt, _, _, st = orc_scene.render_film(first, count, x=0, y=y, w=WIDTH, h=rows, tile=32, threads=threads)
+        if images is not None:
+            images.append(oracle.resolve(rgb, wt))
         stats += np.array(st, np.int64)
         paths += WIDTH * rows * count
     return time.perf_counter() - t0, paths, stats
+
+
+def rel_mse(a, b, eps=1.0e-2) -> float:
+    """Mean over pixels and channels of (a - b)^2 / (b^2 + eps): the image error at equal spp
+    (the reference defines none; the epsilon is this benchmark's)."""
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.mean((a - b) ** 2 / (b * b + eps)))
 
 
 def traversal_bytes(stats, merged=True) -> float:
@@ -141,25 +151,27 @@ def dist_setup(args):
 
 
 def run_reference(args, world, rank):
-    """The reference arm: the CPU path tracer on the host's cores, bounded samples."""
+    """The reference arm: the CPU path tracer on the host's cores over the whole frame, a bounded
+    number of samples per step (each step the next sample indices of the 64)."""
     import oracle
     threads = os.cpu_count() or 1
     rsb = product_rsb()
     o = oracle.OracleScene(rsb)
-    # Calibrate: one band at 1 spp, then size a step to about 4 s of work.
-    bands = sample_bands(16)
+    # Calibrate on a band at 1 spp, then size a step to about 2.5 s of whole-frame work.
     o.render_tile(WIDTH // 2, HEIGHT // 2, 8, 8, 0)  # first use generates the energy tables
-    dt, paths, _ = oracle_sample(o, bands[::4], 0, 1, threads)
+    dt, paths, _ = oracle_sample(o, sample_bands(4), 0, 1, threads)
     rate = paths / max(dt, 1e-6)
-    spp_step = int(max(1, min(SPP, rate * 4.0 / (WIDTH * 8 * len(bands)))))
+    spp_step = int(max(1, min(SPP, rate * 2.5 / (WIDTH * HEIGHT))))
     times, total_paths = [], 0
     for i in range(args.warmup + args.steps):
-        dt, paths, _ = oracle_sample(o, bands, i * spp_step, spp_step, threads)
+        t0 = time.perf_counter()
+        o.render_film((i * spp_step) % SPP, spp_step, tile=32, threads=threads)
+        dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)
-            total_paths += paths
+            total_paths += WIDTH * HEIGHT * spp_step
     value = total_paths / sum(times) / 1e6
-    sample = f"{len(bands)} bands of 8 rows x 1920 px spread over the frame, {spp_step} spp per step"
+    sample = f"the whole 1920x1080 frame at {spp_step} spp per step (sample indices cycling through the frame's 64)"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
@@ -491,10 +503,16 @@ def run_ours(args, world, rank, local, dist):
     b_ray_two_level = traversal_bytes(stats, merged=False)
     achieved = ext_rays * b_ray / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
     o = oracle.OracleScene(rsb)  # without the statistics tree, for the timed CPU baseline
-    # CPU baseline: the oracle (C++ restatement of the reference) on this host, ~10 s of work.
-    spp_cpu = int(max(1, min(SPP, (st_paths / st_dt) * 10.0 / (WIDTH * 8 * len(bands)))))
-    cpu_dt, cpu_paths, _ = oracle_sample(o, bands, 0, spp_cpu, threads)
+    # CPU baseline: the oracle (C++ restatement of the reference) on this host over the 16 bands
+    # at the frame's own samples (10-30 s of work); the same rows of the device frame against
+    # them give the image error at equal spp.
+    cpu_images = []
+    cpu_dt, cpu_paths, _ = oracle_sample(o, bands, base, SPP, threads, images=cpu_images)
     cpu_value = cpu_paths / cpu_dt / 1e6
+    gpu_rows = np.concatenate([img[y:y + rows] for y, rows in bands])
+    cpu_rows = np.concatenate(cpu_images)
+    rel_mse_cpu = rel_mse(gpu_rows, cpu_rows)
+    bit_equal_cpu = float(np.mean(gpu_rows.astype(np.float32).view(np.uint32) == cpu_rows.astype(np.float32).view(np.uint32)))
     line = {
         "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -522,8 +540,12 @@ def run_ours(args, world, rank, local, dist):
                              "layout BVH8 over all triangles; the reference's own two-level tree of 16 interleaved per-material "
                              "instances visits ~10x more (bytes_per_ray_reference_two_level)."},
         "cpu_baseline": {"value": cpu_value, "unit": "Mpaths/s", "cores": threads, "kind": "port",
-                         "sample": f"{len(bands)} bands of 8 rows x 1920 px spread over the frame at {spp_cpu} spp "
+                         "sample": f"{len(bands)} bands of 8 rows x 1920 px spread over the frame at the frame's {SPP} spp "
                                    "(C++ restatement of the reference, bit-exact with its pinned hashes)"},
+        "rel_mse_vs_cpu": rel_mse_cpu,
+        "rel_mse_note": f"the device frame's {len(bands)} bands against the CPU path's render of the same pixels and "
+                        f"samples (64 spp): mean of (a - b)^2 / (b^2 + 1e-2); {bit_equal_cpu * 100:.4f}% of the values "
+                        "bit-equal",
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 24 * n,
                 "path": "rtg_film_clear + rtg_render_progressive + rtg_film_read into pinned host buffers (C ABI); the scene "
                         "is resident after rtg_scene_load (scene_load_s in config)"},

@@ -109,7 +109,9 @@ uint32_t rtg_render_progressive(uint32_t scene, uint32_t film, uint32_t first_sa
  *
  * The first call on each device does the set-up: it looks up the array's address on the
  * current device (cudaGetSymbolAddress), which may load the library's device code there. Make
- * that first call before any stream capture. Each call zeroes the array's queue counters
+ * that first call before any stream capture. Later calls check the remembered address against
+ * the device's mappings (cudaPointerGetAttributes) and look it up again when it is gone, as after
+ * a cudaDeviceReset (which also ends every scene and film of that device). Each call zeroes the array's queue counters
  * itself before it renders; nothing else in the array has to start at zero.
  *
  * There is one array per device, shared by every call on that device. Calls through this
@@ -117,7 +119,8 @@ uint32_t rtg_render_progressive(uint32_t scene, uint32_t film, uint32_t first_sa
  * overlap; work of two calls that ran on the device at the same time would race on the array.
  *
  * Arguments, film result and status codes are those of rtg_render_progressive; the film's bits
- * are the same. Extend-kernel timing (rtg_timing) counts its rays and launches but brackets no
+ * are the same, and so are its guide sums when the film has fused guides
+ * (rtg_film_guides_fused): the first hits' albedo goes through a slice of the same array. Extend-kernel timing (rtg_timing) counts its rays and launches but brackets no
  * launch with events. */
 #define RTG_NOALLOC_SCRATCH_BYTES (12ull << 20)
 #define RTG_NOALLOC_MAX_PATHS 65536u
@@ -167,7 +170,7 @@ uint32_t rtg_queue_free(uint32_t queue);
  * carry correlated noise, a bias towards less noise, e.g. dimmer lights). With
  * RTG_ADJOINT_CORRELATED every path uses the residual of the whole film: the derivative of this
  * very estimate, as a same-seed finite difference measures it.
- * The film must lie inside the image; every path of the call is held in one wave (168 bytes each).
+ * The film must lie inside the image; every path of the call is held in one wave (172 bytes each).
  * `residual` (may be null) receives the sum over replayed paths of |radiance left after the
  * replay| and of |radiance|: the first is 0 up to rounding when the replay retraced the forward
  * paths. A scene with cut-outs or thin walls is refused (RTG_STATUS_BAD_SCENE): the replay does not
@@ -210,11 +213,25 @@ uint32_t rtg_trace_rays(uint32_t scene, const float* rays, uint32_t n, uint32_t 
  * triangles, BVH build seconds, rays cast so far. */
 uint32_t rtg_scene_stats(uint32_t scene, double* out8);
 
-/* Largest number of paths one wave holds (168 bytes of device memory per path, kept until the
+/* Largest number of paths one wave holds (172 bytes of device memory per path, kept until the
  * scene is freed). 0, the default, sizes each wave to every path of the call, bounded by half of
  * the device memory then free: a call then runs as few waves as memory allows, and each wave's
  * tail of long paths is paid once. */
 uint32_t rtg_set_path_capacity(uint32_t scene, uint32_t paths);
+
+/* No counterpart in the reference: how the scene's waves order their work. None of it changes a
+ * film's bits; it changes how fast the traversal and shading kernels run.
+ * values[0]: ray-sort bits per axis, 0-5 (0: off). Before each traversal after the camera rays,
+ *   the extension rays are ordered by the octant of their direction over the Morton code of their
+ *   origin's cell on a grid of 2^bits cells per axis over the box of the scene's main instances.
+ * values[1]: 1 sorts the shadow rays the same way (with ray-sort bits above 0).
+ * values[2]: 1 shades the paths ordered by the material they hit; 0 in traversal order.
+ * values[3]: paths per wave, as rtg_set_path_capacity (0: automatic).
+ * rtg_set_tuning sets the first n values (n <= 4; later ones keep theirs); RTG_STATUS_BAD_SCENE for
+ * ray-sort bits above 5. rtg_get_tuning writes the first n (n <= 4). A loaded scene starts at
+ * 4, 1, 1, 0. */
+uint32_t rtg_set_tuning(uint32_t scene, const uint32_t* values, uint32_t n);
+uint32_t rtg_get_tuning(uint32_t scene, uint32_t* values, uint32_t n);
 
 /* Extend-kernel timing: when enabled, every extend launch is bracketed by CUDA events on the
  * scene's stream. out5 = total extend milliseconds, extend launches, camera + extension rays,

@@ -66,6 +66,8 @@ ABI = {
     "rtg_trace_rays": (_u32, [_u32, _f, _u32, _u32, _f]),
     "rtg_scene_stats": (_u32, [_u32, _f]),
     "rtg_set_path_capacity": (_u32, [_u32, _u32]),
+    "rtg_set_tuning": (_u32, [_u32, _f, _u32]),
+    "rtg_get_tuning": (_u32, [_u32, _f, _u32]),
     "rtg_timing": (_u32, [_u32, _u32, _u32, _f]),
     "rtg_set_stream": (_u32, [_u32, ctypes.c_void_p]),
     "rtg_synchronize": (_u32, [_u32]),
@@ -232,6 +234,23 @@ class Scene:
 
     def set_path_capacity(self, paths: int):
         _check(lib().rtg_set_path_capacity(self.handle, paths))
+
+    def set_tuning(self, ray_bits: int | None = None, shadow_sort: bool | None = None, material_sort: bool | None = None,
+                   capacity: int | None = None):
+        """rtg_set_tuning: how the scene's waves order their rays and paths (None keeps a value)."""
+        cur = self.tuning()
+        new = [cur["ray_bits"] if ray_bits is None else int(ray_bits),
+               cur["shadow_sort"] if shadow_sort is None else int(bool(shadow_sort)),
+               cur["material_sort"] if material_sort is None else int(bool(material_sort)),
+               cur["capacity"] if capacity is None else int(capacity)]
+        v = np.array(new, np.uint32)
+        _check(lib().rtg_set_tuning(self.handle, _ptr(v), 4))
+
+    def tuning(self) -> dict:
+        """rtg_get_tuning: ray-sort bits, shadow sort, material sort, paths per wave (0: automatic)."""
+        v = np.zeros(4, np.uint32)
+        _check(lib().rtg_get_tuning(self.handle, _ptr(v), 4))
+        return {"ray_bits": int(v[0]), "shadow_sort": int(v[1]), "material_sort": int(v[2]), "capacity": int(v[3])}
 
     def timing(self, enable: bool, reset: bool = False):
         """(extend ms, extend launches, camera+extension rays, shadow rays, kernels launched)

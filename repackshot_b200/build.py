@@ -32,6 +32,23 @@ HOST_SOURCES = ["rtg_scene.cpp", "rtg_bitmap.cpp", "rtg_ies.cpp", "rtg_tables.cp
 DEVICE_SOURCES = ["rtg_kernels.cu", "rtg_noalloc.cu", "rtg_adaptive.cu", "rtg_denoise.cu"]
 
 
+SKY_TABLE = PKG / "data" / "sky_table.f32"
+# SHA-256 of the physical sky's table (little-endian f32: 3240 coefficients, then 360 radiances),
+# as engine/crates/rt-core/src/sky_table.rs states it.
+SKY_TABLE_SHA256 = "2329ac7376204749a317d5b31e23e17fa27950515be0f0d50018cd9c16e8a721"
+
+
+def sky_table_inc() -> str:
+    """The sky table as C float literals (hexadecimal: exact), after checking its SHA-256."""
+    import hashlib
+    import struct
+    data = SKY_TABLE.read_bytes()
+    if hashlib.sha256(data).hexdigest() != SKY_TABLE_SHA256:
+        raise RuntimeError(f"{SKY_TABLE} does not have the physical sky table's SHA-256")
+    vals = struct.unpack(f"<{len(data) // 4}f", data)
+    return ",\n".join(", ".join(f"{float(v).hex()}f" for v in vals[i:i + 6]) for i in range(0, len(vals), 6)) + "\n"
+
+
 def _run(cmd, log=None):
     res = subprocess.run(cmd, capture_output=True, text=True)
     if log is not None:
@@ -63,10 +80,14 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         _run([CXX, *HOST_FLAGS, "-O2", str(CSRC / "rtg_energy_gen.cpp"), "-o", str(gen_exe)], log)
     if force or _stale(inc, [gen_exe]):
         _run([str(gen_exe), str(inc)], log)
+    # 2. the physical sky's fitted table (data, checked against its SHA-256, compiled in)
+    sky_inc = GEN / "rtg_sky_table.inc"
+    if force or _stale(sky_inc, [SKY_TABLE]):
+        sky_inc.write_text(sky_table_inc())
     objs = []
     for src in HOST_SOURCES:
         o = OBJ / (src + ".o")
-        deps = [CSRC / src, inc] + headers
+        deps = [CSRC / src, inc, sky_inc] + headers
         if force or _stale(o, deps):
             _run([CXX, *HOST_FLAGS, "-c", str(CSRC / src), "-o", str(o)], log)
         objs.append(o)

@@ -234,8 +234,9 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
             mat = S.materials + I->material;
             if (mat->kind == MATERIAL_EMISSIVE) {
                 if (h.front || !(I->flags & 1u)) {
+                    const float wgt = has_pdf ? emitter_weight(L, I->emitter, pdf, from, offset + t_geometry, dot(ng, rd)) : 1.0f;
                     float4 c4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    add_clamped(c4, thr * rgb(mat->emission[0], mat->emission[1], mat->emission[2]) * 1.0f, bounce >= 2, S.clamp_indirect);
+                    add_clamped(c4, thr * rgb(mat->emission[0], mat->emission[1], mat->emission[2]) * wgt, bounce >= 2, S.clamp_indirect);
                     rem = rgb_sub(rem, rgb(c4.x, c4.y, c4.z));
                 }
                 break;

@@ -363,20 +363,115 @@ struct ClassicSky {
 };
 }  // namespace
 
-HImage classic_sky_image(const HScene& s) {
-    const ClassicSky sky(s.sun_azimuth_deg, s.sun_elevation_deg, s.sky_turbidity);
+// ---- the physical sky (sky.rs:96-198): the Hosek-Wilkie functional form with the Repackshot fit ----
+namespace {
+// The fitted table (data/sky_table.f32, embedded at build time): 3240 coefficients
+// [turbidity 1..10][ground albedo 0, 1][R, G, B][control point 0..5][A..I], then 360 radiances
+// [turbidity][albedo][R, G, B][control point].
+constexpr float kSkyTable[] = {
+#include "_gen/rtg_sky_table.inc"
+};
+constexpr int kSkyParams = 9, kSkyControl = 6, kSkyCoefficients = 3240;
+static_assert(sizeof(kSkyTable) / sizeof(float) == kSkyCoefficients + 360, "sky table size");
+constexpr float kGroundAlbedo = 0.2f;  // sky.rs:68 GROUND_ALBEDO
+
+struct SkyKnot {
+    float weight, coef[3][kSkyParams], radiance[3];
+};
+
+// The sky for one sun position, turbidity and albedo: up to four knots (two turbidities times two
+// albedos), each the table's quintic Bezier curves at x = (elevation / 90)^(1/3); radiances blended.
+struct PhysicalSky {
+    V3 sun;
+    SkyKnot knots[4];
+    int n = 0;
+    PhysicalSky(float azimuth_deg, float elevation_deg, float turbidity, float albedo) {
+        const float t = finitef(turbidity) ? rclamp(turbidity, 1.0f, 10.0f) : 3.0f;
+        const float elevation = finitef(elevation_deg) ? rclamp(elevation_deg, 0.0f, 90.0f) : 45.0f;
+        const float azimuth = finitef(azimuth_deg) ? azimuth_deg : 0.0f;
+        const float a = finitef(albedo) ? rclamp(albedo, 0.0f, 1.0f) : kGroundAlbedo;
+        float se, ce, sa, ca;
+        sin_cos(elevation * (PI / 180.0f), se, ce);
+        sin_cos(azimuth * (PI / 180.0f), sa, ca);
+        sun = v3(ce * ca, ce * sa, se);
+        const float x = fpow(elevation / 90.0f, 1.0f / 3.0f);
+        // the six quintic Bernstein polynomials at x
+        const float y = 1.0f - x, x2 = x * x, y2 = y * y, x3 = x2 * x, y3 = y2 * y;
+        const float b[kSkyControl] = {y3 * y2, 5.0f * x * y2 * y2, 10.0f * x2 * y3, 10.0f * x3 * y2, 5.0f * x2 * x2 * y, x3 * x2};
+        const float tt = t - 1.0f;
+        const int i = std::min((int)std::floor(tt), 8);
+        const float f = tt - (float)i;
+        const int ti[2] = {i, i + 1};
+        const float wt[2] = {1.0f - f, f}, wa[2] = {1.0f - a, a};
+        for (int p = 0; p < 2; ++p)
+            for (int q = 0; q < 2; ++q) {
+                const float weight = wt[p] * wa[q];
+                if (weight <= 0.0f) continue;
+                SkyKnot& k = knots[n++];
+                k = SkyKnot{};
+                k.weight = weight;
+                for (int c = 0; c < 3; ++c) {
+                    const int base = (ti[p] * 2 + q) * 3 + c;
+                    for (int m = 0; m < kSkyControl; ++m) {
+                        for (int j = 0; j < kSkyParams; ++j) k.coef[c][j] += b[m] * kSkyTable[(base * kSkyControl + m) * kSkyParams + j];
+                        k.radiance[c] += b[m] * kSkyTable[kSkyCoefficients + base * kSkyControl + m];
+                    }
+                }
+            }
+    }
+    // Linear Rec. 709 radiance in a unit direction above the horizon, in the model's units; black
+    // below. 1 + H^2 - 2 H cos gamma as (1 - H)^2 + H |v - s|^2 and gamma as atan2(|v x s|, v . s).
+    Rgb radiance(V3 dir) const {
+        if (dir.z <= 0.0f) return rgb(0.0f, 0.0f, 0.0f);
+        const float cos_theta = dir.z;
+        const float cos_gamma = rclamp(dot(dir, sun), -1.0f, 1.0f);
+        const float gamma = fatan2(len(cross(dir, sun)), dot(dir, sun));
+        const V3 chord = dir - sun;
+        const float chord2 = dot(chord, chord);
+        const float cg2 = cos_gamma * cos_gamma;
+        const float horizon = 1.0f / (cos_theta + 0.01f);
+        const float sq = sqrt_(cos_theta);
+        float out[3] = {0.0f, 0.0f, 0.0f};
+        for (int k = 0; k < n; ++k)
+            for (int c = 0; c < 3; ++c) {
+                const float* q = knots[k].coef[c];
+                const float den = (1.0f - q[7]) * (1.0f - q[7]) + q[7] * chord2;
+                const float chi = (1.0f + cg2) / (den * sqrt_(den));
+                const float value = (1.0f + q[0] * clamped_exp(q[1] * horizon)) *
+                                    (q[2] + q[3] * clamped_exp(q[4] * gamma) + q[5] * cg2 + q[6] * chi + q[8] * sq);
+                out[c] += knots[k].weight * value * knots[k].radiance[c];
+            }
+        return rgb(rmax(out[0], 0.0f), rmax(out[1], 0.0f), rmax(out[2], 0.0f));
+    }
+};
+
+// sum += x with Neumaier's compensation c (environment.rs:204): the total is sum + c.
+inline void add_compensated(float& sum, float& c, float x) {
+    const float t = sum + x;
+    if (absf(sum) >= absf(x)) c += (sum - t) + x;
+    else c += (x - t) + sum;
+    sum = t;
+}
+}  // namespace
+
+// environment.rs:216 tabulate_sky: the sky's upper half from the model, scaled so that a horizontal
+// surface gets the dome's irradiance 2 pi (horizon / 6 + zenith / 3) strength; the lower half the
+// ground, floor * strength. The physical sky sums the irradiance with compensation, the classic
+// one plainly.
+template <class Sky>
+static HImage tabulate_sky(const HScene& s, const Sky& sky, bool compensated) {
     const uint32_t w = 256, h = 128;
     HImage img;
     img.width = w;
     img.height = h;
     img.texels.assign(3 * (size_t)w * h, 0.0f);
-    float irradiance = 0.0f;
+    float irradiance = 0.0f, irradiance_c = 0.0f;
     const float cell = (PI / (float)h) * (TAU / (float)w);
     for (uint32_t y = 0; y < h / 2; ++y) {
         const float v = ((float)y + 0.5f) / (float)h;
         float st, ct;
         sin_cos(PI * v, st, ct);
-        float row = 0.0f;
+        float row = 0.0f, row_c = 0.0f;
         for (uint32_t x = 0; x < w; ++x) {
             const float u = ((float)x + 0.5f) / (float)w;
             float sp, cp;
@@ -385,10 +480,14 @@ HImage classic_sky_image(const HScene& s) {
             const Rgb c = sky.radiance(d);
             float* o = &img.texels[3 * ((size_t)y * w + x)];
             o[0] = c.r; o[1] = c.g; o[2] = c.b;
-            row += luminance(c) * d.z * st;
+            const float term = luminance(c) * d.z * st;
+            if (compensated) add_compensated(row, row_c, term);
+            else row += term;
         }
-        irradiance += row * cell;
+        if (compensated) add_compensated(irradiance, irradiance_c, (row + row_c) * cell);
+        else irradiance += row * cell;
     }
+    irradiance = irradiance + irradiance_c;
     const float strength = rmax(s.env_strength, 0.0f);
     const float target = strength * TAU * (rmax(s.env_horizon, 0.0f) / 6.0f + rmax(s.env_zenith, 0.0f) / 3.0f);
     const float scale = irradiance > 0.0f ? target / irradiance : 0.0f;
@@ -396,6 +495,11 @@ HImage classic_sky_image(const HScene& s) {
     for (size_t i = 0; i < img.texels.size(); ++i)
         img.texels[i] = i / (3 * (size_t)w) < h / 2 ? img.texels[i] * scale : ground;
     return img;
+}
+
+HImage sky_image(const HScene& s) {
+    if (s.sky_model == 1) return tabulate_sky(s, ClassicSky(s.sun_azimuth_deg, s.sun_elevation_deg, s.sky_turbidity), false);
+    return tabulate_sky(s, PhysicalSky(s.sun_azimuth_deg, s.sun_elevation_deg, s.sky_turbidity, kGroundAlbedo), true);
 }
 
 }  // namespace rtg

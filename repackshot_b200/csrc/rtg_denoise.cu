@@ -358,9 +358,9 @@ cudaError_t launch_dn_rescale(const float* rgb, const float* alpha, const float*
 }
 
 size_t dn_scratch_bytes(size_t n) {
-    // 3 guide float4 planes; divisor and two light planes (3 floats); var x 3, lum x 2, gvar,
-    // before (floats); firefly flags; two counters.
-    return 3 * align256(n * 16) + 3 * align256(n * 12) + 7 * align256(n * 4) + align256(n * 4) + 256;
+    // 3 guide float4 planes; divisor and two light planes (3 floats); var x 3, lum x 2, before
+    // (floats); firefly flags; two counters.
+    return 3 * align256(n * 16) + 3 * align256(n * 12) + 6 * align256(n * 4) + align256(n * 4) + 256;
 }
 
 cudaError_t denoise_band(const DnSrc& src, uint32_t width, uint32_t rows, uint32_t samples, DnPreset preset, void* scratch, float* out,
@@ -375,8 +375,6 @@ cudaError_t denoise_band(const DnSrc& src, uint32_t width, uint32_t rows, uint32
     float* var[2] = {(float*)take(n * 4), (float*)take(n * 4)};
     float* var0 = (float*)take(n * 4);
     float* lum[2] = {(float*)take(n * 4), (float*)take(n * 4)};
-    float* gvar = (float*)take(n * 4);  // (kept in the layout; the a-trous pass blurs the variance itself)
-    (void)gvar;
     float* before = (float*)take(n * 4);
     uint32_t* ffly = (uint32_t*)take(n * 4);
     uint32_t* changed = (uint32_t*)take(256);

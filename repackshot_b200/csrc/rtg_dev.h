@@ -54,14 +54,16 @@ struct alignas(16) DevInstance {
     float to_world[12];
     uint32_t identity, active, material, mesh;
     uint32_t flags, inside_out, has_normals, tri_base;  // tri_base: first global triangle of its mesh
-    uint32_t tangent_on, passable, pad1, pad2;  // passable: shadow rays cross it (cut-out or thin wall)
+    uint32_t tangent_on, passable, emitter, pad2;  // passable: shadow rays cross it (cut-out or thin wall);
+                                                   // emitter: its mesh light's index in lights[] + 1, or 0
     float tan_centre[3], tan_axis[3], tan_x[3];
     float pad3[3];
 };
 
-// One light of the selection (light.rs:300-360): an area light (rect or disk), a sun, or a sphere
-// light (a point light or a spot; radius 0 is a point). Each kind reads its own fields.
-enum : uint32_t { LIGHT_AREA = 0, LIGHT_SUN = 1, LIGHT_SPHERE = 2 };
+// One light of the selection (light.rs:300-495): an area light (rect or disk), a sun, a sphere
+// light (a point light or a spot; radius 0 is a point) or an emissive mesh sampled by area. Each
+// kind reads its own fields.
+enum : uint32_t { LIGHT_AREA = 0, LIGHT_SUN = 1, LIGHT_SPHERE = 2, LIGHT_MESH = 3 };
 struct LightDev {
     float centre[3];
     // area: its frame; sun: a frame whose z points at the sun; sphere: fz is a spot's axis
@@ -79,7 +81,14 @@ struct LightDev {
     float ies_peak;
     uint32_t kind, rect, delta;
     uint32_t glossy, camera, shadow, entry;
-    uint32_t source;  // index of the scene light it was built from
+    uint32_t source;  // index of the scene light it was built from (0xffffffff: an emissive mesh)
+    // an emissive mesh (light.rs:440): per world-space triangle four float4s -- corner a with the
+    // cumulative area fraction in w, corners b and c, the unit normal (winding order: the front);
+    // the cone of the front faces' normals about fz (cos_o -1: any direction); centre, bound, area
+    // (mm^2), radiance and base as an area light's
+    const float4* tris;
+    uint32_t n_tris, two_sided;
+    float cos_o, sin_o;
 };
 constexpr int MAX_ENTRIES = 64;
 constexpr int MAX_LIGHTS = 63;
@@ -101,7 +110,7 @@ struct EnvMapDev {
 struct LightsDev {
     // lights[] holds the area lights, then the suns, then the sphere lights, each in scene order
     int n_areas, n_entries, per_point, env_is_entry;
-    uint32_t env_entry, n_suns, n_spheres, n_lights;
+    uint32_t env_entry, n_suns, n_spheres, n_lights;  // n_lights counts the mesh lights after the spheres
     float env_floor, env_horizon, env_zenith, env_lower, env_total, env_base;
     uint32_t env_is_map;  // the environment is `env_map`, else the ramp above
     EnvMapDev env_map;

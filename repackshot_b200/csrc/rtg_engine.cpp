@@ -87,6 +87,8 @@ struct Scene {
     DevBuf path_mem;
     uint32_t capacity = 0;
     uint32_t max_capacity = 0;  // paths per wave; 0: automatic (wave_limit)
+    RaySort order;              // how waves order their rays and paths (rtg_set_tuning)
+    float sort_lo[3] = {0, 0, 0}, sort_hi[3] = {0, 0, 0};  // the box the ray sort grids
     // statistics
     uint64_t rays = 0;
     double build_seconds = 0;
@@ -243,6 +245,13 @@ uint32_t upload_shading(const Flat& F, BufSet& set, SceneDev& S) {
         for (uint32_t i = 0; i < L.n_lights; ++i)
             if (L.lights[i].ies) L.lights[i].ies = dev + (F.lights.lights[i].ies - F.ies_data.data());
     }
+    if (!F.mesh_light_data.empty()) {  // the mesh lights point into their triangles on the device
+        const float* dev = nullptr;
+        if ((st = upload(set, F.mesh_light_data, dev))) return st;
+        for (uint32_t i = 0; i < L.n_lights; ++i)
+            if (L.lights[i].kind == LIGHT_MESH)
+                L.lights[i].tris = reinterpret_cast<const float4*>(dev + reinterpret_cast<size_t>(F.lights.lights[i].tris));
+    }
     if (L.env_is_map && F.env_image) {
         if ((st = upload(set, F.env_image->texels, L.env_map.texels)) || (st = upload(set, F.env_map.weights, L.env_map.weights)) ||
             (st = upload(set, F.env_map.conditional, L.env_map.conditional)) || (st = upload(set, F.env_map.marginal, L.env_map.marginal)))
@@ -283,8 +292,12 @@ SceneDev compose(const SceneDev& constants, const SceneDev& geom, const SceneDev
 }
 
 // Device bytes of one path slot: o, d, thr, sum, sel, hit, sh_o, sh_d, sh_c (16 each), flags,
-// medium, queue[0], queue[1], sorted, key (4 each).
-constexpr size_t PATH_BYTES = 9 * 16 + 6 * 4;
+// medium, queue[0], queue[1], sorted, key, sh_key (4 each).
+constexpr size_t PATH_BYTES = 9 * 16 + 7 * 4;
+// The ray sort's two key histograms with their cursors, at the largest key count.
+constexpr size_t SORT_BINS_BYTES = 2 * 2 * (size_t)(8u << (3u * RAY_SORT_MAX_BITS)) * 4;
+// The ray sort's default: octant over a 16^3 grid, shadow rays too, material sort kept.
+constexpr uint32_t DEFAULT_RAY_BITS = 4, DEFAULT_SHADOW_SORT = 1, DEFAULT_MATERIAL_SORT = 1;
 constexpr uint64_t AUTO_MIN_PATHS = 1u << 20;
 constexpr uint64_t PLAIN_JOB_PATHS = 1u << 24;  // a queue job this large runs as plain waves
 constexpr uint64_t MAX_WAVE_PATHS = 0x7fffffffu;
@@ -294,6 +307,24 @@ constexpr uint64_t MAX_WAVE_PATHS = 0x7fffffffu;
 // own path buffers). Each wave ends with a tail of long paths that leaves the GPU part-idle, so
 // the fewer waves a call takes, the faster it runs: a 1080p frame at 64 spp is one wave of
 // 132.7 M paths (22 GB).
+// The ray sort's grid over the scene's sort box at the current bits per axis.
+void refresh_order(Scene& sc) {
+    const float cells = (float)(1u << sc.order.ray_bits);
+    for (int k = 0; k < 3; ++k) {
+        const float extent = sc.sort_hi[k] - sc.sort_lo[k];
+        const bool ok = extent > 0.0f && extent < 3.0e38f;
+        sc.order.lo[k] = ok ? sc.sort_lo[k] : 0.0f;
+        sc.order.scale[k] = ok ? cells / extent : 0.0f;
+    }
+}
+void set_sort_box(Scene& sc, const Flat& F) {
+    for (int k = 0; k < 3; ++k) {
+        sc.sort_lo[k] = F.box_lo[k];
+        sc.sort_hi[k] = F.box_hi[k];
+    }
+    refresh_order(sc);
+}
+
 uint64_t wave_limit(const Scene& sc, uint64_t call_paths) {
     if (sc.max_capacity) return sc.max_capacity;
     uint64_t by_memory = AUTO_MIN_PATHS;
@@ -308,7 +339,7 @@ uint32_t ensure_capacity(Scene& sc, uint32_t paths) {
     sc.path_mem.release();
     sc.capacity = 0;
     size_t n = paths;
-    size_t bytes = n * PATH_BYTES + 16 * 256 + 256 + 512 * 4;
+    size_t bytes = n * PATH_BYTES + 17 * 256 + 256 + 512 * 4 + SORT_BINS_BYTES;
     RTG_CHECK(cudaMalloc(&sc.path_mem.p, bytes));
     sc.path_mem.bytes = bytes;
     uint8_t* p = (uint8_t*)sc.path_mem.p;
@@ -331,6 +362,11 @@ uint32_t ensure_capacity(Scene& sc, uint32_t paths) {
     sc.P.sh_o = (float4*)take(16);
     sc.P.sh_d = (float4*)take(16);
     sc.P.sh_c = (float4*)take(16);
+    sc.P.sh_key = (uint32_t*)take(4);
+    sc.P.rbins = (uint32_t*)p;
+    sc.P.sbins = sc.P.rbins + SORT_BINS_BYTES / 8;
+    p += SORT_BINS_BYTES;
+    RTG_CHECK(cudaMemsetAsync(sc.P.rbins, 0, SORT_BINS_BYTES, sc.stream));  // histograms start at zero
     sc.P.counters = (uint32_t*)p;
     p += 64;
     sc.P.rays = (unsigned long long*)p;
@@ -361,9 +397,9 @@ uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film, const Scene
         sc.wt->ev_count = 0;
         t = sc.wt;
     }
-    launch_wave(Sw, lights ? lights : sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t);
+    launch_wave(Sw, lights ? lights : sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t, sc.order);
     RTG_CHECK(cudaGetLastError());
-    sc.launches += 2 + 6 * (uint64_t)wave_rounds(Sw) - ((film || w.segs) ? 0 : 1);
+    sc.launches += wave_launches(Sw, sc.order, sc.P) - ((film || w.segs) ? 0 : 1) + ((w.alb && film && !w.segs) ? 2 : 0);
     if (t) {
         RTG_CHECK(cudaStreamSynchronize(sc.stream));
         for (int i = 0; i + 1 < t->ev_count; i += 2) {
@@ -754,6 +790,10 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     sc->width = F.scene.width;
     sc->height = F.scene.height;
     sc->max_depth = F.scene.max_depth;
+    sc->order.ray_bits = DEFAULT_RAY_BITS;
+    sc->order.shadow_sort = DEFAULT_SHADOW_SORT;
+    sc->order.material_sort = DEFAULT_MATERIAL_SORT;
+    set_sort_box(*sc, F);
     g_error.clear();
     for (size_t i = 0; i < g_scenes.size(); ++i)
         if (!g_scenes[i]) { g_scenes[i] = std::move(sc); return (uint32_t)i + 1; }
@@ -791,6 +831,7 @@ uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
     } else {
         geom.tlas_root = F.scene.tlas_root;
         geom.stack_need = F.scene.stack_need;
+        set_sort_box(*sc, F);
         sc->geometry.release();
         sc->geometry = std::move(geometry);
         sc->nodes = F.nodes.size();
@@ -887,11 +928,15 @@ uint32_t rtg_render_progressive_noalloc(uint32_t handle, uint32_t film, uint32_t
         return RTG_STATUS_BAD_SCENE;
     }
     NoallocJob job{&sc->S, sc->d_lights, f->dev, sc->width, sc->height, first_sample, count, sc->stream, g_sms};
+    if (f->fuse_guides) {
+        job.guide_sum = f->albedo_sum();
+        job.guide_weight = f->albedo_weight();
+    }
     NoallocResult res;
     const char* why = "";
     uint32_t st = noalloc_render(job, res, &why);
     if (st) { g_error = why; return st; }
-    sc->launches += res.waves * (2 + 6 * (uint64_t)wave_rounds(sc->S));
+    sc->launches += res.waves * (2 + 6 * (uint64_t)wave_rounds(sc->S) + (job.guide_sum ? 2 : 0));
     sc->rays += res.extend_rays + res.shadow_rays;
     sc->extend_rays += res.extend_rays;
     sc->shadow_rays += res.shadow_rays;
@@ -1043,14 +1088,15 @@ uint32_t rtg_queue_run(uint32_t queue, uint32_t flags, uint64_t* rays) {
     // A job that fills waves on its own (at least PLAIN_JOB_PATHS paths, a whole sample in one
     // wave) gains nothing from sharing them and would pay the batched kernels' segment lookups and
     // the deepest job's bounce count: it runs as the plain path's waves, with its own scene
-    // constants and lights. Its film gets the same bits either way.
+    // constants and lights. Its film gets the same bits either way, and its waves are captured
+    // into the run's graph like the batched ones.
     const bool graph = (flags & RTG_QUEUE_GRAPH) != 0;
     std::vector<uint8_t> plain(q->jobs.size(), 0);
     uint64_t plain_need = 0;
     for (size_t j = 0; j < q->jobs.size(); ++j) {
         const QueueJob& J = *q->jobs[j];
         const uint64_t npix = (uint64_t)J.width * J.height;
-        if (!graph && npix * J.count >= PLAIN_JOB_PATHS && npix <= cap) {
+        if (npix * J.count >= PLAIN_JOB_PATHS && npix <= cap) {
             plain[j] = 1;
             plain_need = std::max(plain_need, npix * std::min<uint64_t>(J.count, cap / npix));
         }
@@ -1256,6 +1302,7 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     for (uint32_t j = 0; j < nl; ++j) grads[4 * nm + j] = 0.0f;
     for (uint32_t i = 0; i < na; ++i) {
         uint32_t j = sc->light_source[i];
+        if (j >= nl) continue;  // an emissive mesh: its emission is not a parameter
         float p = sc->light_power[j];
         if (p > 0.0f) grads[4 * nm + j] += g[4 * nm + i] / p;
     }
@@ -1410,6 +1457,39 @@ uint32_t rtg_set_path_capacity(uint32_t handle, uint32_t paths) {
     if (!sc) return RTG_STATUS_BAD_HANDLE;
     if (paths != 0 && paths < 1024) paths = 1024;
     sc->max_capacity = paths;
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_set_tuning(uint32_t handle, const uint32_t* values, uint32_t n) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (!values && n) return RTG_STATUS_NULL_POINTER;
+    RaySort o = sc->order;
+    uint32_t cap = sc->max_capacity;
+    if (n > 0) {
+        if (values[0] > RAY_SORT_MAX_BITS) { g_error = "rtg_set_tuning: ray-sort bits above 5"; return RTG_STATUS_BAD_SCENE; }
+        o.ray_bits = values[0];
+    }
+    if (n > 1) o.shadow_sort = values[1] != 0;
+    if (n > 2) o.material_sort = values[2] != 0;
+    if (n > 3) cap = values[3] != 0 && values[3] < 1024 ? 1024 : values[3];
+    // A wave leaves both histograms at zero, but the cursors of fewer bits lie inside the
+    // histogram of more: clear them when the key count changes.
+    if (o.ray_bits != sc->order.ray_bits && sc->P.rbins) RTG_CHECK(cudaMemsetAsync(sc->P.rbins, 0, SORT_BINS_BYTES, sc->stream));
+    sc->order = o;
+    sc->max_capacity = cap;
+    refresh_order(*sc);
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_get_tuning(uint32_t handle, uint32_t* values, uint32_t n) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (!values && n) return RTG_STATUS_NULL_POINTER;
+    const uint32_t v[4] = {sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity};
+    for (uint32_t k = 0; k < n && k < 4; ++k) values[k] = v[k];
     return RTG_STATUS_OK;
 }
 

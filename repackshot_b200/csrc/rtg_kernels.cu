@@ -125,11 +125,84 @@ __device__ __forceinline__ void warp_count(uint32_t* bins, uint32_t key) {
     if ((threadIdx.x & 31) == (uint32_t)(__ffs((int)mask) - 1)) atomicAdd(&bins[key], (uint32_t)__popc(mask));
 }
 
+// ---- ray order (RaySort): coherence keys, their prefix and the scatter ---------------------------------
+// Cell of coordinate v on a grid of n cells from lo with `scale` cells per unit (NaN and below: 0).
+__device__ __forceinline__ uint32_t sort_cell(float v, float lo, float scale, uint32_t n) {
+    const float f = (v - lo) * scale;
+    return f > 0.0f ? (uint32_t)fminf(f, (float)(n - 1u)) : 0u;
+}
+// The coherence key of a ray: the octant of d (3 bits) over the Morton code of o's cell.
+__device__ __forceinline__ uint32_t ray_key(const RaySort& R, V3 o, V3 d) {
+    const uint32_t n = 1u << R.ray_bits;
+    const uint32_t cx = sort_cell(o.x, R.lo[0], R.scale[0], n), cy = sort_cell(o.y, R.lo[1], R.scale[1], n),
+                   cz = sort_cell(o.z, R.lo[2], R.scale[2], n);
+    uint32_t m = 0;
+#pragma unroll
+    for (uint32_t b = 0; b < RAY_SORT_MAX_BITS; ++b)
+        m |= (((cx >> b) & 1u) << (3u * b)) | (((cy >> b) & 1u) << (3u * b + 1u)) | (((cz >> b) & 1u) << (3u * b + 2u));
+    const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    return (oct << (3u * R.ray_bits)) | m;
+}
+
+// bins[nk, 2 nk) = exclusive prefix of the histogram bins[0, nk), which is cleared. One block of
+// 1024 threads: each warp sums a contiguous chunk, the chunk sums are scanned, then each warp
+// scans its chunk row by row (coalesced).
+__global__ void __launch_bounds__(1024) k_key_scan(uint32_t* bins, uint32_t nk) {
+    __shared__ uint32_t chunk[32];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t per = ((nk + 31u) / 32u + 31u) & ~31u;
+    const uint32_t b0 = min(warp * per, nk), b1 = min(b0 + per, nk);
+    uint32_t s = 0;
+    for (uint32_t e = b0 + lane; e < b1; e += 32u) s += bins[e];
+    s = __reduce_add_sync(0xffffffffu, s);
+    if (lane == 0) chunk[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t v = chunk[lane];
+        uint32_t x = v;
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        chunk[lane] = x - v;
+    }
+    __syncthreads();
+    uint32_t off = chunk[warp];
+    for (uint32_t r = b0; r < b1; r += 32u) {
+        const uint32_t e = r + lane;
+        const uint32_t v = e < b1 ? bins[e] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (e < b1) {
+            bins[nk + e] = off + x - v;
+            bins[e] = 0u;
+        }
+        off += __shfl_sync(0xffffffffu, x, 31);
+    }
+}
+
+// out = the *count items of `list` (null: 0, 1, 2, ...) ordered by keys[item] (any order within a
+// key: every ray's result depends on its own item only).
+__global__ void k_key_scatter(const uint32_t* __restrict__ list, const uint32_t* __restrict__ keys, uint32_t* cursors,
+                              const uint32_t* count, uint32_t* out) {
+    const uint32_t n = *(volatile const uint32_t*)count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t item = list ? list[i] : i;
+        out[atomicAdd(&cursors[keys[item]], 1u)] = item;
+    }
+}
+
 // ---- extend: nearest hit of every active path ------------------------------------------------------------
 // Persistent warps over the active queue: a lane whose ray has finished takes the next queue entry
 // (one atomic per warp on counters[4]) while the rest of the warp keeps traversing, so no lane idles
 // until the slowest ray of its warp is done.
-__global__ void __launch_bounds__(TRACE_THREADS) k_extend(SceneDev S, PathBuffers P, int cur) {
+// `order`: the active queue in the order to trace it (P.queue[cur], or its ray-sorted copy).
+__global__ void __launch_bounds__(TRACE_THREADS) k_extend(SceneDev S, PathBuffers P, int cur, const uint32_t* __restrict__ order) {
     __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
     uint64_t deep[STACK_CAP - SHORT_STACK];
     SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
@@ -149,7 +222,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_extend(SceneDev S, PathBuffer
                 if (base + (uint32_t)__popc(idle) >= n) drained = true;
                 const uint32_t i = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
                 if (!busy && i < n) {
-                    slot = P.queue[cur][i];
+                    slot = order[i];
                     const float4 o = P.o[slot], d = P.d[slot];
                     const bool primary = (P.flags[slot] & PF_PRIMARY) != 0;
                     busy = trav_init(S, T, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, f_inf(), primary);
@@ -194,12 +267,12 @@ __global__ void k_scan(PathBuffers P) {
     }
 }
 
-// The active queue reordered by material key (the order inside a key does not matter: every
-// path's result depends on its own slot only).
-__global__ void k_scatter(PathBuffers P, int cur) {
+// The active queue `in` reordered by material key into `out` (the order inside a key does not
+// matter: every path's result depends on its own slot only).
+__global__ void k_scatter(PathBuffers P, int cur, const uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
     uint32_t n = *(volatile uint32_t*)&P.counters[cur];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t slot = P.queue[cur][i];
+        uint32_t slot = in[i];
         uint32_t key = P.key[slot];
         uint32_t mask = __match_any_sync(__activemask(), key);
         int leader = __ffs((int)mask) - 1;
@@ -207,16 +280,18 @@ __global__ void k_scatter(PathBuffers P, int cur) {
         if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&P.bins[256 + key], (uint32_t)__popc(mask));
         base = __shfl_sync(mask, base, leader);
         uint32_t rank = __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
-        P.sorted[base + rank] = slot;
+        out[base + rank] = slot;
     }
 }
 
 // ---- shade: one vertex of every active path ----------------------------------------------------------
 // One vertex of the path in `slot` with the scene constants S and lights L; xyi(x, y, index) gives
 // the path's pixel and sample index (the sampler's key).
+// With P.rbins set, each surviving path's next ray gets its coherence key (in P.key) and is counted
+// in the histogram; with P.sbins set, each shadow ray likewise (in P.sh_key).
 template <class XYI>
-__device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L, const PathBuffers& P, uint32_t slot, int cur, XYI xyi,
-                                           uint32_t& rays_local, uint32_t& shadow_local) {
+__device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L, const PathBuffers& P, const RaySort& R, uint32_t slot, int cur,
+                                           XYI xyi, uint32_t& rays_local, uint32_t& shadow_local) {
     float4 o4 = P.o[slot], d4 = P.d[slot], thr4 = P.thr[slot], sum = P.sum[slot];
     uint32_t flags = P.flags[slot];
     const uint32_t bounce = (flags & PF_BOUNCE_MASK) >> PF_BOUNCE_SHIFT;
@@ -295,8 +370,12 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
             s_outside = h.outside;
             mat = S.materials + I->material;
             if (mat->kind == MATERIAL_EMISSIVE) {
-                if (h.front || !(I->flags & 1u))
-                    add_clamped(sum, thr * rgb(mat->emission[0], mat->emission[1], mat->emission[2]) * 1.0f, bounce >= 2, S.clamp_indirect);
+                // A BSDF-sampled ray that finds a mesh light weighs it against the light's own
+                // sample (integrator/mod.rs:1556); other emitters and camera rays weigh 1.
+                if (h.front || !(I->flags & 1u)) {
+                    const float wgt = has_pdf ? emitter_weight(L, I->emitter, pdf, from, offset + t_geometry, dot(ng, rd)) : 1.0f;
+                    add_clamped(sum, thr * rgb(mat->emission[0], mat->emission[1], mat->emission[2]) * wgt, bounce >= 2, S.clamp_indirect);
+                }
                 break;
             }
             // A cut-out lets the ray through with probability 1 - opacity: no vertex, the same
@@ -373,6 +452,11 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
                         P.sh_o[k] = make_float4(from_p.x, from_p.y, from_p.z, tmax);
                         P.sh_d[k] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, bounce >= 1 ? 1.0f : 0.0f);  // w: indirect
                         P.sh_c[k] = make_float4(c.r, c.g, c.b, __uint_as_float(slot));
+                        if (P.sbins) {
+                            const uint32_t sk = ray_key(R, from_p, ls.wi);
+                            P.sh_key[k] = sk;
+                            atomicAdd(&P.sbins[sk], 1u);
+                        }
                     }
                 }
             }
@@ -424,6 +508,12 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
     if (alive) {
         uint32_t k = atomicAdd(&P.counters[cur ^ 1], 1u);
         P.queue[cur ^ 1][k] = slot;
+        if (P.rbins) {
+            const float4 no = P.o[slot], nd = P.d[slot];
+            const uint32_t rk = ray_key(R, v3(no.x, no.y, no.z), v3(nd.x, nd.y, nd.z));
+            P.key[slot] = rk;
+            atomicAdd(&P.rbins[rk], 1u);
+        }
     }
 }
 
@@ -431,20 +521,22 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
 // Eight blocks per SM (64 registers, with some spills) beat the 128 registers the compiler would
 // use on its own: the kernel waits on scattered hit-detail loads, and more warps hide them (1080p
 // frame: 369 -> 383 Mpaths/s; 5, 6 and 7 blocks measured 367, 379 and 372).
+// `order`: the active queue in the order to shade it (material-sorted, or as traced).
 template <bool BATCH>
-__global__ void __launch_bounds__(128, 8) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w) {
+__global__ void __launch_bounds__(128, 8) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w,
+                                                  const uint32_t* __restrict__ order, RaySort R) {
     uint32_t n = *(volatile uint32_t*)&P.counters[cur];
     uint32_t rays_local = 0, shadow_local = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = P.sorted[i];
+        const uint32_t slot = order[i];
         if constexpr (BATCH) {
             uint32_t job, x, y, index;
             batch_slot(w, slot, job, x, y, index);
             const JobDev& J = w.jobs[job];
-            shade_slot(J.S, *J.lights, P, slot, cur, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { xx = x; yy = y; ii = index; },
+            shade_slot(J.S, *J.lights, P, R, slot, cur, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { xx = x; yy = y; ii = index; },
                        rays_local, shadow_local);
         } else {
-            shade_slot(S, *Lg, P, slot, cur, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { wave_slot(w, slot, xx, yy, ii); },
+            shade_slot(S, *Lg, P, R, slot, cur, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { wave_slot(w, slot, xx, yy, ii); },
                        rays_local, shadow_local);
         }
     }
@@ -465,7 +557,8 @@ __device__ __forceinline__ void shadow_unblocked(const PathBuffers& P, uint32_t 
     P.sum[slot] = s;
 }
 
-__global__ void __launch_bounds__(TRACE_THREADS) k_shadow(SceneDev S, PathBuffers P) {
+// `perm` (may be null): the shadow queue in the order to trace it.
+__global__ void __launch_bounds__(TRACE_THREADS) k_shadow(SceneDev S, PathBuffers P, const uint32_t* __restrict__ perm) {
     __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
     uint64_t deep[STACK_CAP - SHORT_STACK];
     SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
@@ -485,10 +578,10 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow(SceneDev S, PathBuffer
                 if (base + (uint32_t)__popc(idle) >= n) drained = true;
                 const uint32_t i = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
                 if (!busy && i < n) {
-                    ray = i;
-                    const float4 o = P.sh_o[i], d = P.sh_d[i];
+                    ray = perm ? perm[i] : i;
+                    const float4 o = P.sh_o[ray], d = P.sh_d[ray];
                     busy = trav_init(S, T, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, o.w, false);
-                    if (!busy) shadow_unblocked(P, i);
+                    if (!busy) shadow_unblocked(P, ray);
                 }
             }
         }
@@ -513,13 +606,14 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow(SceneDev S, PathBuffer
 // behind it, up to 32 crossings; any other surface blocks it. One thread per ray: only scenes with
 // passable instances run it, instead of k_shadow. BATCH: each ray's job gives its materials.
 template <bool BATCH>
-__global__ void __launch_bounds__(TRACE_THREADS) k_shadow_walk(SceneDev S, PathBuffers P, WaveDesc w) {
+__global__ void __launch_bounds__(TRACE_THREADS) k_shadow_walk(SceneDev S, PathBuffers P, WaveDesc w, const uint32_t* __restrict__ perm) {
     __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
     uint64_t deep[STACK_CAP - SHORT_STACK];
     SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
     const uint32_t n = *(volatile uint32_t*)&P.counters[2];
     uint32_t err = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t i = perm ? perm[j] : j;
         const float4 o4 = P.sh_o[i], d4 = P.sh_d[i], c4 = P.sh_c[i];
         const uint32_t slot = __float_as_uint(c4.w);
         const SceneDev* Sp = &S;
@@ -1003,34 +1097,68 @@ static int resident_blocks(const void* kernel, int threads) {
     return sms * per_sm;
 }
 
+uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P) {
+    const uint32_t rounds = wave_rounds(S);
+    const bool rsort = order.ray_bits > 0 && P.rbins, ssort = rsort && order.shadow_sort && P.sbins;
+    uint32_t per_round = 5 + (order.material_sort ? 1u : 0u) + (ssort ? 2u : 0u);
+    return 2 + rounds * per_round + (rsort && rounds > 1 ? 2u * (rounds - 1u) : 0u);
+}
+
 void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const FilmDev* film, cudaStream_t st,
-                 int grid, WaveTiming* timing) {
+                 int grid, WaveTiming* timing, const RaySort& order) {
     static const int ext_resident = resident_blocks((const void*)k_extend, TRACE_THREADS);
     static const int sh_resident = resident_blocks((const void*)k_shadow, TRACE_THREADS);
     const int g = grid;
     const int g_ext = ext_resident > 0 && ext_resident < g ? ext_resident : g;
     const int g_sh = sh_resident > 0 && sh_resident < g ? sh_resident : g;
     const bool batch = w.segs != nullptr;
+    const bool rsort = order.ray_bits > 0 && order.ray_bits <= RAY_SORT_MAX_BITS && P.rbins;
+    const bool ssort = rsort && order.shadow_sort && P.sbins;
+    const uint32_t nk = ray_sort_keys(order.ray_bits);
     if (batch) k_camera<true><<<g, 256, 0, st>>>(S, w, P);
     else k_camera<false><<<g, 256, 0, st>>>(S, w, P);
     int cur = 0;
     const uint32_t rounds = wave_rounds(S);
     for (uint32_t round = 0; round < rounds; ++round) {
+        // The camera rays are traced in pixel order; later rounds' rays in coherence order.
+        const uint32_t* traced = P.queue[cur];
+        if (rsort && round > 0) {
+            k_key_scan<<<1, 1024, 0, st>>>(P.rbins, nk);
+            k_key_scatter<<<g, 256, 0, st>>>(P.queue[cur], P.key, P.rbins + nk, &P.counters[cur], P.sorted);
+            traced = P.sorted;
+        }
         if (timing && timing->ev_count + 2 <= WaveTiming::MAX_EVENTS) {
             cudaEventRecord(timing->ev[timing->ev_count++], st);
-            k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur);
+            k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur, traced);
             cudaEventRecord(timing->ev[timing->ev_count++], st);
         } else {
-            k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur);
+            k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur, traced);
         }
         if (round == 0 && w.alb && film && !batch) k_albedo_hits<<<g, 256, 0, st>>>(S, L, w, P);
         k_scan<<<1, 32, 0, st>>>(P);
-        k_scatter<<<g, 256, 0, st>>>(P, cur);
-        if (batch) k_shade<true><<<g, 128, 0, st>>>(S, L, P, cur, w);
-        else k_shade<false><<<g, 128, 0, st>>>(S, L, P, cur, w);
-        if (!S.any_passable) k_shadow<<<g_sh, TRACE_THREADS, 0, st>>>(S, P);
-        else if (batch) k_shadow_walk<true><<<g, TRACE_THREADS, 0, st>>>(S, P, w);
-        else k_shadow_walk<false><<<g, TRACE_THREADS, 0, st>>>(S, P, w);
+        // The material-sorted copy goes to whichever list the traversal did not read.
+        const uint32_t* shaded = traced;
+        if (order.material_sort) {
+            uint32_t* sorted = traced == P.sorted ? P.queue[cur] : P.sorted;
+            k_scatter<<<g, 256, 0, st>>>(P, cur, traced, sorted);
+            shaded = sorted;
+        }
+        // Keys for the next round's rays (none after the last round) and for this round's shadow rays.
+        PathBuffers Q = P;
+        Q.rbins = rsort && round + 1 < rounds ? P.rbins : nullptr;
+        Q.sbins = ssort ? P.sbins : nullptr;
+        if (batch) k_shade<true><<<g, 128, 0, st>>>(S, L, Q, cur, w, shaded, order);
+        else k_shade<false><<<g, 128, 0, st>>>(S, L, Q, cur, w, shaded, order);
+        // queue[cur] is free once shade has read its list: it holds the shadow rays' order.
+        const uint32_t* perm = nullptr;
+        if (ssort) {
+            k_key_scan<<<1, 1024, 0, st>>>(P.sbins, nk);
+            k_key_scatter<<<g, 256, 0, st>>>(nullptr, P.sh_key, P.sbins + nk, &P.counters[2], P.queue[cur]);
+            perm = P.queue[cur];
+        }
+        if (!S.any_passable) k_shadow<<<g_sh, TRACE_THREADS, 0, st>>>(S, P, perm);
+        else if (batch) k_shadow_walk<true><<<g, TRACE_THREADS, 0, st>>>(S, P, w, perm);
+        else k_shadow_walk<false><<<g, TRACE_THREADS, 0, st>>>(S, P, w, perm);
         k_next_round<<<1, 1, 0, st>>>(P, cur);
         cur ^= 1;
     }
@@ -1076,9 +1204,9 @@ void launch_adjoint_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& 
     k_adjoint_camera<<<g, 256, 0, st>>>(S, w, P, A);
     int cur = 0;
     for (uint32_t bounce = 0; bounce <= S.max_depth; ++bounce) {
-        k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur);
+        k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur, P.queue[cur]);
         k_scan<<<1, 32, 0, st>>>(P);
-        k_scatter<<<g, 256, 0, st>>>(P, cur);
+        k_scatter<<<g, 256, 0, st>>>(P, cur, P.queue[cur], P.sorted);
         k_shade_adjoint<<<g, 128, 0, st>>>(S, L, P, cur, bounce, w, A);
         k_shadow_adjoint<<<g_sh, TRACE_THREADS, 0, st>>>(S, P, w, A);
         k_next_round<<<1, 1, 0, st>>>(P, cur);

@@ -84,7 +84,24 @@ struct PathBuffers {
     float4* sh_c;    // contribution, w: slot
     uint32_t* counters;  // [0], [1] queue lengths, [2] shadow queue length, [3] error bits
     unsigned long long* rays;
+    // Coherence sort of the rays before each traversal (RaySort); all null: off.
+    uint32_t* rbins;   // extension rays: [0, nk) key histogram, [nk, 2 nk) cursors
+    uint32_t* sbins;   // shadow rays: the same
+    uint32_t* sh_key;  // per shadow ray: its coherence key
 };
+
+// How a wave orders its work (the tunable half of the pipeline; none of it changes a film's bits).
+// ray_bits > 0: before every traversal after the camera rays, the extension rays are ordered by a
+// key of their direction's octant (3 bits) over the Morton code of their origin's cell on a grid of
+// 2^ray_bits cells per axis over the scene's box (counting sort: histogram, prefix, scatter);
+// shadow_sort: the shadow rays too (by their own origin and direction); material_sort: shade
+// reads the paths ordered by the material they hit (otherwise in traversal order).
+struct RaySort {
+    uint32_t ray_bits = 0, shadow_sort = 0, material_sort = 1;
+    float lo[3] = {0, 0, 0}, scale[3] = {0, 0, 0};  // cell = (p - lo) * scale per axis
+};
+constexpr uint32_t RAY_SORT_MAX_BITS = 5;
+inline uint32_t ray_sort_keys(uint32_t bits) { return 8u << (3u * bits); }
 
 struct FilmDev {
     uint32_t ox, oy, w, h;
@@ -137,7 +154,9 @@ struct WaveTiming {
 
 void set_sobol(const SobolTable& t, cudaStream_t s);
 void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const FilmDev* film, cudaStream_t st,
-                 int grid, WaveTiming* timing);
+                 int grid, WaveTiming* timing, const RaySort& order = RaySort());
+// Kernel launches of one launch_wave with a film (camera and accumulate included, guides not).
+uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P);
 // The adjoint: loss and per-pixel path derivatives of a film against a target (w*h*3 floats on
 // the device), then the backward wave: the replay of the wave that rendered the film.
 void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, const PathBuffers& P, uint32_t count, cudaStream_t st,

@@ -9,9 +9,10 @@ namespace rtg {
 RTG_HD V3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
 
 // ---- area lights --------------------------------------------------------------------------------
-RTG_HD float orientation_bound(V3 v, float d2, V3 axis, float bound) {  // light.rs:260 with θo = 0
+// light.rs:212: the largest cosine between a normal in the cone (axis, half-angle θo) of a light
+// bounded by a sphere of radius `bound` and the direction towards a point at v from its centre.
+RTG_HD float orientation_bound_cone(V3 v, float d2, V3 axis, float cos_o, float sin_o, float bound) {
     if (d2 <= bound * bound) return 1.0f;
-    const float cos_o = 1.0f, sin_o = 0.0f;
     float inv_d = 1.0f / sqrt_(d2);
     float sin_u = bound * inv_d;
     float cos_u = sqrt_(rmax(1.0f - sin_u * sin_u, 0.0f));
@@ -23,10 +24,21 @@ RTG_HD float orientation_bound(V3 v, float d2, V3 axis, float bound) {  // light
     float sin_t = sqrt_(rmax(1.0f - cos_t * cos_t, 0.0f));
     return rmax(cos_t * cos_s + sin_t * sin_s, 0.0f);
 }
+RTG_HD float orientation_bound(V3 v, float d2, V3 axis, float bound) {  // θo = 0: a flat light
+    return orientation_bound_cone(v, d2, axis, 1.0f, 0.0f, bound);
+}
 RTG_HD float area_weight(const LightDev& a, V3 x) {
     V3 v = x - ld3(a.centre);
     float d2 = len2(v);
     float o = orientation_bound(v, d2, ld3(a.fz), a.bound);
+    if (o <= 0.0f) return 0.0f;
+    return a.base * o / (rmax(d2, a.area) * 1.0e-6f);
+}
+// light.rs:468 MeshEmitter::weight: lum(L) A cos' / max(d^2, A) from its centroid.
+RTG_HD float mesh_weight(const LightDev& a, V3 x) {
+    V3 v = x - ld3(a.centre);
+    float d2 = len2(v);
+    float o = a.cos_o <= -1.0f ? 1.0f : orientation_bound_cone(v, d2, ld3(a.fz), a.cos_o, a.sin_o, a.bound);
     if (o <= 0.0f) return 0.0f;
     return a.base * o / (rmax(d2, a.area) * 1.0e-6f);
 }

@@ -23,8 +23,9 @@ namespace rtg {
 namespace {
 
 // Bytes per path of the structure-of-arrays state (PathBuffers): o, d, thr, sum, sel, hit, sh_o,
-// sh_d, sh_c (16 each), flags, medium, queue[0], queue[1], sorted, key (4 each).
-constexpr size_t kBytesPerPath = 9 * 16 + 6 * 4;
+// sh_d, sh_c (16 each), flags, medium, queue[0], queue[1], sorted, key (4 each); then the
+// first-hit albedo of each path (16), which a film with fused guides adds to its guide sums.
+constexpr size_t kBytesPerPath = 10 * 16 + 6 * 4;
 constexpr size_t kPaths = RTG_NOALLOC_MAX_PATHS;
 constexpr size_t kBinsBytes = 512 * 4;
 constexpr size_t kCountersBytes = 64;  // [0], [1] queue lengths, [2] shadow queue, [3] error bits
@@ -38,8 +39,9 @@ static __device__ __align__(256) unsigned char g_path_scratch[RTG_NOALLOC_SCRATC
 constexpr int kMaxDevices = 64;
 void* g_scratch_ptr[kMaxDevices] = {};  // the array's address on each device, once looked up
 
-// Carves one wave's path buffers out of the array, in the order of PathBuffers.
-PathBuffers carve(void* base) {
+// Carves one wave's path buffers out of the array, in the order of PathBuffers; *albedo gets the
+// per-path albedo slice after them.
+PathBuffers carve(void* base, float4** albedo) {
     unsigned char* p = static_cast<unsigned char*>(base);
     auto take = [&](size_t each) { unsigned char* r = p; p += kPaths * each; return r; };
     PathBuffers P{};
@@ -63,6 +65,8 @@ PathBuffers carve(void* base) {
     P.counters = (uint32_t*)p;
     p += kCountersBytes;
     P.rays = (unsigned long long*)p;
+    p += kRaysBytes;
+    *albedo = (float4*)take(16);
     return P;
 }
 
@@ -81,6 +85,15 @@ uint32_t noalloc_scratch(void** out, const char** why) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { *why = cudaGetErrorString(e); return RTG_STATUS_CUDA_ERROR; }
     if (dev < 0 || dev >= kMaxDevices) { *why = "device index beyond the 64 this library tracks"; return RTG_STATUS_CUDA_ERROR; }
+    // A cached address is checked against the device's mappings: after cudaDeviceReset the array
+    // is loaded again, possibly elsewhere, and the lookup is redone.
+    if (g_scratch_ptr[dev]) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, g_scratch_ptr[dev]) != cudaSuccess || a.type != cudaMemoryTypeDevice || a.device != dev) {
+            cudaGetLastError();
+            g_scratch_ptr[dev] = nullptr;
+        }
+    }
     if (!g_scratch_ptr[dev]) {
         void* ptr = nullptr;
         e = cudaGetSymbolAddress((void**)&ptr, g_path_scratch);
@@ -104,7 +117,8 @@ uint32_t noalloc_render(const NoallocJob& job, NoallocResult& res, const char** 
     void* base = nullptr;
     uint32_t st = noalloc_scratch(&base, why);
     if (st) return st;
-    const PathBuffers P = carve(base);
+    float4* albedo = nullptr;
+    const PathBuffers P = carve(base, &albedo);
     // Rows per band so that one band of one sample fits the array, then samples per wave.
     const uint64_t npix = (uint64_t)cw * ch;
     const uint32_t band_rows = npix > kPaths ? (uint32_t)(kPaths / cw) : ch;
@@ -120,7 +134,12 @@ uint32_t noalloc_render(const NoallocJob& job, NoallocResult& res, const char** 
         if (e != cudaSuccess) { *why = cudaGetErrorString(e); return RTG_STATUS_CUDA_ERROR; }
         for (uint32_t s = 0; s < job.count; s += per_wave) {
             const uint32_t ns = per_wave < job.count - s ? per_wave : job.count - s;
-            const WaveDesc wd{job.film.ox, job.film.oy + by, cw, bh, job.first + s, (uint32_t)(bpix * ns), nullptr};
+            WaveDesc wd{job.film.ox, job.film.oy + by, cw, bh, job.first + s, (uint32_t)(bpix * ns), nullptr};
+            if (job.guide_sum) {  // fused guides: every wave's first hits add their albedo too
+                wd.alb = albedo;
+                wd.guide_sum = job.guide_sum;
+                wd.guide_weight = job.guide_weight;
+            }
             launch_wave(*job.S, job.lights, wd, P, &job.film, job.stream, grid_for(wd.n, 128, job.sms), nullptr);
             e = cudaGetLastError();
             if (e != cudaSuccess) { *why = cudaGetErrorString(e); return RTG_STATUS_CUDA_ERROR; }

@@ -17,6 +17,8 @@ struct NoallocJob {
     uint32_t first, count;   // samples first .. first + count - 1
     cudaStream_t stream;
     int sms;
+    float* guide_sum = nullptr;     // a film with fused guides: its albedo sums (3 a pixel) ...
+    float* guide_weight = nullptr;  // ... and weights, which every wave adds to; else null
 };
 
 struct NoallocResult {

@@ -183,7 +183,6 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
                   r.of32(s.backplate_rect[0], 0.0f) && r.of32(s.backplate_rect[1], 0.0f) && r.of32(s.backplate_rect[2], 1.0f) &&
                   r.of32(s.backplate_rect[3], 1.0f) && r.ou32(s.sky_model, 0)))
                 return false;
-            if (s.env_kind == 2 && s.sky_model != 1) { error = "unsupported: physical sky model"; return false; }
         } else if (is("IESP")) {  // rsb.rs:1018: an IES file
             uint32_t n;
             if (!r.u32(n)) return false;
@@ -270,7 +269,6 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
     }
     for (const HMaterial& m : s.materials) {
         bool emissive = m.kind == MATERIAL_EMISSIVE;
-        if (emissive && (m.flags & 1u)) { error = "unsupported: emissive mesh lights"; return false; }
         if (m.scatter_mm > 0.0f && m.transmission > 0.0f) { error = "unsupported: scattering media"; return false; }
         if (m.abbe > 0.0f && m.transmission > 0.0f) { error = "unsupported: dispersive glass"; return false; }
         if (m.bevel_mm > 0.0f) { error = "unsupported: edge bevel"; return false; }
@@ -735,21 +733,117 @@ static bool prepare_lights(const HScene& s, const Box& scene_box, LightsDev& L, 
         refs.push_back({a.kind, (uint32_t)kinds[a.kind].size()});
         kinds[a.kind].push_back(a);
     }
+    // Emissive meshes (light.rs:867-958): every instance whose material is an emitter flagged as a
+    // light, sampled by area over its world-space triangles; entries after the scene's lights.
+    std::vector<LightDev> meshes;
+    F.mesh_light_data.clear();
+    for (size_t i = 0; i < s.instances.size(); ++i) {
+        const HInstance& in = s.instances[i];
+        if (in.material_id >= s.materials.size()) continue;
+        const HMaterial& m = s.materials[in.material_id];
+        if (m.kind != MATERIAL_EMISSIVE || !(m.flags & 1u)) continue;
+        const Rgb radiance = rgb(rmax(m.emission[0] * m.emission_power, 0.0f), rmax(m.emission[1] * m.emission_power, 0.0f),
+                                 rmax(m.emission[2] * m.emission_power, 0.0f));
+        if (!(luminance(radiance) > 0.0f)) continue;
+        if (in.mesh >= s.meshes.size()) continue;
+        const HMesh& M = s.meshes[in.mesh];
+        const Xf xf = xf_of(in.rows);
+        Xf inv;
+        if (!xf_inverse(xf, inv)) continue;  // never hit, so never lit either
+        std::vector<std::array<V3, 3>> corners;
+        std::vector<V3> normals;
+        std::vector<float> tri_areas;
+        V3 centroid = v3(0, 0, 0);
+        for (size_t t = 0; t < M.triangles(); ++t) {
+            const uint32_t ia = M.indices[3 * t], ib = M.indices[3 * t + 1], ic = M.indices[3 * t + 2];
+            if (ia >= M.positions.size() || ib >= M.positions.size() || ic >= M.positions.size()) continue;
+            const std::array<V3, 3> w = {xf_point(xf, M.positions[ia]), xf_point(xf, M.positions[ib]), xf_point(xf, M.positions[ic])};
+            const V3 c = cross(w[1] - w[0], w[2] - w[0]);
+            const float a = 0.5f * len(c);
+            if (!(a > 0.0f && finitef(a))) continue;
+            centroid = centroid + (w[0] + w[1] + w[2]) * (a / 3.0f);
+            corners.push_back(w);
+            normals.push_back(normalize(c));
+            tri_areas.push_back(a);
+        }
+        float area = 0.0f, total = 0.0f;
+        for (float a : tri_areas) area += a;
+        total = area;
+        if (!(total > 0.0f && finitef(total))) continue;  // build_cdf (light.rs:652): no CDF, no light
+        LightDev e;
+        std::memset(&e, 0, sizeof(e));
+        e.kind = LIGHT_MESH;
+        e.glossy = 1;
+        e.shadow = 1;
+        e.source = 0xffffffffu;
+        e.entry = (uint32_t)(refs.size() + meshes.size());
+        e.two_sided = (in.flags & 1u) == 0;
+        const float sides = e.two_sided ? 2.0f : 1.0f;
+        const float flux = luminance(radiance) * PI * area * 1.0e-6f * sides;
+        centroid = centroid / area;
+        float bound = 0.0f;
+        for (const auto& w : corners)
+            for (const V3& q : w) bound = rmax(bound, len(q - centroid));
+        V3 mean = v3(0, 0, 0);
+        for (size_t k = 0; k < normals.size(); ++k) mean = mean + normals[k] * tri_areas[k];
+        const float length = len(mean);
+        V3 axis = v3(0, 0, 1);
+        if (e.two_sided || length <= 1.0e-3f * area) {
+            e.cos_o = -1.0f;
+            e.sin_o = 0.0f;
+        } else {
+            axis = mean / length;
+            float c = 1.0f;
+            for (const V3& n : normals) c = rmin(c, dot(n, axis));
+            e.cos_o = rclamp(c, -1.0f, 1.0f);
+            e.sin_o = sqrt_(rmax(1.0f - e.cos_o * e.cos_o, 0.0f));
+        }
+        weights.push_back(flux * reach(centroid, nullptr));
+        put3(e.centre, centroid);
+        put3(e.fz, axis);
+        e.bound = bound;
+        e.area = area;
+        e.radiance[0] = radiance.r; e.radiance[1] = radiance.g; e.radiance[2] = radiance.b;
+        e.base = luminance(radiance) * area * 1.0e-6f;
+        // The triangles: corners, the cumulative area fraction (light.rs:652 build_cdf) in a's w,
+        // the unit normal; their offset in the scene's mesh-light data until upload.
+        e.n_tris = (uint32_t)corners.size();
+        e.tris = reinterpret_cast<const float4*>(F.mesh_light_data.size());
+        float acc = 0.0f;
+        for (size_t k = 0; k < corners.size(); ++k) {
+            acc += tri_areas[k];
+            const float cdf = k + 1 == corners.size() ? 1.0f : acc / total;
+            const V3& a = corners[k][0];
+            const V3& b = corners[k][1];
+            const V3& c = corners[k][2];
+            const V3& n = normals[k];
+            const float rec[16] = {a.x, a.y, a.z, cdf, b.x, b.y, b.z, 0.0f, c.x, c.y, c.z, 0.0f, n.x, n.y, n.z, 0.0f};
+            F.mesh_light_data.insert(F.mesh_light_data.end(), rec, rec + 16);
+        }
+        F.instances[i].emitter = (uint32_t)meshes.size() + 1;  // made absolute below
+        meshes.push_back(e);
+        if (refs.size() + meshes.size() > (size_t)MAX_LIGHTS) { error = "unsupported: more than 63 lights"; return false; }
+    }
     uint32_t first[3] = {0, (uint32_t)kinds[0].size(), (uint32_t)(kinds[0].size() + kinds[1].size())};
     for (int k = 0; k < 3; ++k)
         for (size_t i = 0; i < kinds[k].size(); ++i) L.lights[first[k] + i] = kinds[k][i];
     L.n_areas = (int)kinds[0].size();
     L.n_suns = (uint32_t)kinds[1].size();
     L.n_spheres = (uint32_t)kinds[2].size();
-    L.n_lights = (uint32_t)refs.size();
+    const uint32_t first_mesh = (uint32_t)refs.size();
+    for (size_t i = 0; i < meshes.size(); ++i) L.lights[first_mesh + i] = meshes[i];
+    for (DevInstance& d : F.instances)
+        if (d.emitter) d.emitter += first_mesh;
+    L.n_lights = (uint32_t)(refs.size() + meshes.size());
     for (const auto& r : refs) L.entries[L.n_entries++] = (int)(first[r.first] + r.second);
+    for (size_t i = 0; i < meshes.size(); ++i) L.entries[L.n_entries++] = (int)(first_mesh + i);
     // EnvLight::new (environment.rs:335): an HDRI with its bitmap is a map (black when it has no
     // light), any other kind the ramp (flat: three equal stops; an HDRI without a bitmap: the dome).
     float strength = rmax(s.env_strength, 0.0f);
     float f0 = s.env_kind == 1 ? s.env_horizon : s.env_floor, h0 = s.env_horizon, z0 = s.env_kind == 1 ? s.env_horizon : s.env_zenith;
     F.env_image = nullptr;
     if (s.env_kind == 2) {  // the sky, tabulated; scale 1 and no rotation
-        F.sky = classic_sky_image(s);
+        F.sky = sky_image(s);
         if (build_env_map(F.sky, 1.0f, 0.0f, F.env_map)) {
             L.env_is_map = 1;
             F.env_image = &F.sky;
@@ -901,6 +995,22 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
         F.instances.push_back(d);
         if (live[i]) scene_box = scene_box.uni(instance_box(M, xf[i]));
         if (live[i]) F.instanced_triangles += M.triangles();
+    }
+    // The box the ray sort grids: the instances that hold at least 1% of the triangles (where
+    // most rays start; a large floor quad of two triangles would otherwise spread the grid thin),
+    // or the whole scene's.
+    {
+        uint64_t total = 0;
+        for (size_t i = 0; i < ni; ++i)
+            if (live[i]) total += s.meshes[s.instances[i].mesh].triangles();
+        Box bulk;
+        for (size_t i = 0; i < ni; ++i) {
+            const HMesh& M = s.meshes[s.instances[i].mesh];
+            if (live[i] && (uint64_t)M.triangles() * 100 >= total) bulk = bulk.uni(instance_box(M, xf[i]));
+        }
+        if (bulk.empty()) bulk = scene_box;
+        F.box_lo[0] = bulk.lo.x; F.box_lo[1] = bulk.lo.y; F.box_lo[2] = bulk.lo.z;
+        F.box_hi[0] = bulk.hi.x; F.box_hi[1] = bulk.hi.y; F.box_hi[2] = bulk.hi.z;
     }
     // Materials.
     for (const HMaterial& m : s.materials) {

@@ -73,10 +73,11 @@ bool decode_bitmap(uint32_t format, uint32_t width, uint32_t height, const uint8
                    bool& unsupported);
 // Map::new (environment.rs:60): false when the map has no light to sample.
 bool build_env_map(const HImage& img, float scale, float rotation_deg, HEnvMap& out);
-// sky_image (environment.rs:178) of the classic sky model (sky.rs:245, Preetham et al. 1999): the
-// sky tabulated into a 256 x 128 map, scaled to the dome's irradiance, the ground below.
+// sky_image (environment.rs:178): the scene's sky -- the physical model (sky.rs:96, the Hosek-Wilkie
+// form with the Repackshot fit) or the classic one (sky.rs:245, Preetham et al. 1999) --
+// tabulated into a 256 x 128 map, scaled to the dome's irradiance, the ground below.
 struct HScene;
-HImage classic_sky_image(const HScene& s);
+HImage sky_image(const HScene& s);
 struct HScene {
     V3 cam_position{0, -1000, 0}, cam_target{0, 0, 0}, cam_up{0, 0, 1};
     float focal_mm = 50, sensor_mm = 36, fstop = 0, focus_dist = 1000, ortho_width = 1000;
@@ -127,6 +128,7 @@ struct Flat {
     HEnvMap env_map;
     HImage sky;  // the tabulated sky of a sky environment
     std::vector<float> ies_data;  // per IES light: vertical angles, horizontal angles, candela
+    std::vector<float> mesh_light_data;  // per mesh light's triangle: 16 floats (LightDev::tris)
     const HImage* env_image = nullptr;
     const HImage* plate = nullptr;
     std::vector<QNode> nodes;
@@ -141,6 +143,7 @@ struct Flat {
     SceneDev scene;  // pointers left null
     uint32_t tlas_root = NODE_EMPTY;
     uint32_t stack_need = 0;
+    float box_lo[3] = {0, 0, 0}, box_hi[3] = {0, 0, 0};  // the ray sort's box (empty: lo > hi)
     uint64_t instanced_triangles = 0;
     double build_seconds = 0;
 };

@@ -171,6 +171,7 @@ RTG_D float entry_weight(const LightsDev& L, int e, V3 x) {  // light.rs:1014
     const LightDev& l = L.lights[a];
     if (l.kind == LIGHT_AREA) return area_weight(l, x);
     if (l.kind == LIGHT_SUN) return l.base;
+    if (l.kind == LIGHT_MESH) return mesh_weight(l, x);
     return sphere_weight(l, x);
 }
 RTG_D Sel select_at(const LightsDev& L, V3 x) {
@@ -194,6 +195,16 @@ RTG_D float power_heuristic(float pa, float pb) {
     return 1.0f / (1.0f + r * r);
 }
 
+// light.rs:1543 emitter_weight: for a BSDF-sampled ray (density pdf, selection `from`) that hit an
+// emissive instance at distance t with `cos` between the ray and the geometric normal, the MIS
+// weight of its emission against its mesh light's next-event sample (1 without a mesh light).
+RTG_D float emitter_weight(const LightsDev& L, uint32_t emitter, float pdf, const Sel& from, float t, float cos) {
+    if (emitter == 0) return 1.0f;
+    const LightDev& l = L.lights[emitter - 1];
+    const float light_pdf = pmf_of(L, l.entry, from) * t * t / (l.area * rmax(absf(cos), 1.0e-7f));
+    return power_heuristic(pdf, light_pdf);
+}
+
 // light: index into lights[], -1 the environment; delta: no other technique finds it
 struct LightSample { V3 wi; float distance; Rgb radiance; float pdf; bool glossy, shadow, delta; int light; };
 
@@ -201,23 +212,31 @@ RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, flo
     int n = L.n_entries;
     if (n == 0) return false;
     int index = 0;
-    float pmf = 0.0f;
-    if (s.by_flux) {
+    float pmf = 0.0f, rest = 0.0f;  // rest: where u_select falls within its bucket (a mesh light's triangle)
+    if (s.by_flux) {  // pick (light.rs:634)
         int k = 0;
         while (k < n && L.cdf[k] <= u_select) ++k;
         index = k < n - 1 ? k : n - 1;
         pmf = pmf_of(L, (uint32_t)index, s);
+        const float lo = index == 0 ? 0.0f : L.cdf[index - 1], width = L.cdf[index] - lo;
+        rest = width > 0.0f ? rclamp((u_select - lo) / width, 0.0f, 0.99999994f) : 0.0f;
     } else {
         if (!(s.total > 0.0f && finitef(s.total))) return false;
-        // pick_at (light.rs:1118): the first bucket whose end passes u_select (the point within
-        // it is not needed: every light kind here samples with its own two numbers)
-        float acc = 0.0f;
+        // pick_at (light.rs:1118): the first bucket whose end passes u_select
+        float acc = 0.0f, lo = 0.0f;
         int last = n - 1;
         for (int e = 0; e <= last; ++e) {
             float w = entry_weight(L, e, s.p);
             acc += w;
             float hi = e == last ? 1.0f : acc / s.total;
-            if (hi > u_select || e == last) { index = e; pmf = w / s.total; break; }
+            if (hi > u_select || e == last) {
+                index = e;
+                pmf = w / s.total;
+                const float width = hi - lo;
+                rest = width > 0.0f ? rclamp((u_select - lo) / width, 0.0f, 0.99999994f) : 0.0f;
+                break;
+            }
+            lo = hi;
         }
     }
     if (!(pmf > 0.0f)) return false;
@@ -268,6 +287,29 @@ RTG_D_NI bool sample_light(const LightsDev& L, const Sel& s, float u_select, flo
             out.radiance = rgb(l.radiance[0], l.radiance[1], l.radiance[2]) * m;
             out.pdf = pmf / (TAU * omc);
         }
+    } else if (a >= 0 && L.lights[a].kind == LIGHT_MESH) {  // light.rs:1270: a triangle by area, a point uniformly
+        const LightDev& l = L.lights[a];
+        uint32_t k = 0;
+        while (k < l.n_tris && __ldg(&l.tris[4 * k].w) <= rest) ++k;
+        const uint32_t t = k < l.n_tris - 1 ? k : l.n_tris - 1;
+        const float4 ca = __ldg(&l.tris[4 * t]), cb = __ldg(&l.tris[4 * t + 1]), cc = __ldg(&l.tris[4 * t + 2]), nn = __ldg(&l.tris[4 * t + 3]);
+        const float su = sqrt_(u0);  // warp.rs:57 uniform_triangle
+        const float b0 = 1.0f - su, b1 = u1 * su, b2 = 1.0f - b0 - b1;
+        const V3 p = v3(ca.x, ca.y, ca.z) * b0 + v3(cb.x, cb.y, cb.z) * b1 + v3(cc.x, cc.y, cc.z) * b2;
+        const V3 d = p - s.p;
+        const float dist2 = len2(d);
+        const float distance = sqrt_(dist2);
+        const V3 wi = d / distance;
+        const float facing = -dot(wi, v3(nn.x, nn.y, nn.z));
+        if (!(distance > 0.0f) || (!l.two_sided && facing <= 0.0f)) return false;
+        const float cos = absf(facing);
+        if (!(cos > 0.0f)) return false;
+        out.wi = wi;
+        out.distance = distance;
+        out.radiance = rgb(l.radiance[0], l.radiance[1], l.radiance[2]);
+        out.pdf = pmf * dist2 / (l.area * cos);
+        out.glossy = true;
+        out.shadow = true;
     } else if (a >= 0) {
         const LightDev& l = L.lights[a];
         float x, y;

@@ -101,9 +101,11 @@ def test_adjoint_on_a_crop_matches_finite_differences(rtg):
     s.update(scenes.to_rsb(base, meshes=False))
 
 
-def test_a_queue_job_that_fills_waves_alone_runs_plain_and_keeps_its_bits(rtg):
+@pytest.mark.parametrize("graph", [False, True])
+def test_a_queue_job_that_fills_waves_alone_runs_plain_and_keeps_its_bits(rtg, graph):
     """A queue job of at least 2^24 paths runs as the plain path's waves, with its own camera and
-    lights, beside small jobs batched as before: every film equals its plain render bit for bit."""
+    lights, beside small jobs batched as before, whether the run is captured into a CUDA graph or
+    not: every film equals its plain render bit for bit."""
     from repackshot_b200 import scenes
     base = scenes.cfg4_scene(width=64, height=36, spp=1)
     s = rtg.Scene(scenes.to_rsb(base))
@@ -112,7 +114,7 @@ def test_a_queue_job_that_fills_waves_alone_runs_plain_and_keeps_its_bits(rtg):
             for w, h, n, r in sizes]
     q = rtg.Queue(s)
     films = [q.add(b, 0, n, w, h) for b, w, h, n in jobs]
-    q.run()
+    q.run(graph=graph)
     for (b, w, h, n), qf in zip(jobs, films):
         s.update(b)
         f = s.film()

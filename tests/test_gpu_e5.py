@@ -61,6 +61,15 @@ def test_e5_under_the_classic_sky_has_the_pinned_hash(rtg, pins):
     assert rtg.fnv1a(f.resolve()) == pins["film_hashes"]["e5_sky_4spp"]
 
 
+def test_e5c_under_the_physical_sky_has_the_pinned_hash(rtg, pins):
+    # render.rs:1112-1128: the physical sky tabulated on the host, sampled and seen on the device.
+    from repackshot_b200 import scenes
+    f = rtg.Scene(scenes.to_rsb(scenes.e5c_scene())).film()
+    f.render(0, 2)
+    f.render(2, 2)
+    assert rtg.fnv1a(f.resolve()) == pins["film_hashes"]["e5c_physical_sky_4spp"]
+
+
 def sky(**changes):
     from repackshot_b200 import scenes
     s = scenes.e5_scene(sky=True)

@@ -71,3 +71,18 @@ def test_handles_and_empty_work(rtg, cfg0_rsb):
     g.render_noalloc(3, 2)
     ref.render(3, 2)
     assert_films_agree(g, ref)
+
+
+def test_fused_guides_match_the_progressive_render(rtg, example_rsb):
+    # A film with fused guides takes each render's first-hit albedo into its guide sums; the
+    # allocation-free render fills them from its own array. The denoised image reads those sums,
+    # so it agrees only when both renders added the same albedo.
+    s = rtg.Scene(example_rsb)
+    ref, fixed = s.film(), s.film()
+    ref.fuse_guides(True)
+    fixed.fuse_guides(True)
+    for first, count in ((0, 2), (2, 2)):
+        ref.render(first, count)
+        fixed.render_noalloc(first, count)
+        assert_films_agree(fixed, ref)
+    assert np.allclose(fixed.denoise(4), ref.denoise(4), rtol=RTOL, atol=ATOL)
