@@ -487,6 +487,9 @@ static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, ui
     }
     Ray ray = scene.camera.generate_ray(aspect, u, v, lx, ly);
     radiance(scene, prep, sampler, ray, rclamp(u, 0.0f, 1.0f), rclamp(v, 0.0f, 1.0f), c, alpha, st);
+    // A panoramic camera's sample where it sees nothing brings no light (scene/mod.rs:338: its
+    // weight is black; render.rs:465 multiplies the radiance by it).
+    if (scene.camera.panoramic() && !(ray.t_max > 0.0f)) c = c * BLACK;
 }
 
 // The exact passes of a centre ray (passes.rs:168) that the edge mask compares: part and
@@ -537,7 +540,8 @@ static Exact centre_exact(const Scene& scene, const Prepared& prep, uint32_t x, 
     }
     Vec3 forward, right, upv;
     scene.camera.basis(forward, right, upv);
-    e.depth = t * dot(ray.dir, forward) + dot(ray.origin - scene.camera.position, forward);
+    // passes.rs:191: along the view axis; a panorama has no axis for what it sees: the distance.
+    e.depth = scene.camera.panoramic() ? t * length(ray.dir) : t * dot(ray.dir, forward) + dot(ray.origin - scene.camera.position, forward);
     return e;
 }
 // EdgeMask::of (pixel_filter.rs:175) for the whole image (the same for any tile cut): a pixel is

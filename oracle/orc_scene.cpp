@@ -16,9 +16,42 @@ void Camera::basis(Vec3& forward, Vec3& right, Vec3& upv) const {
     }
     upv = cross(right, forward);
 }
+bool Camera::panorama_dir(float aspect, float u, float v, Vec3& dir) const {
+    Vec3 forward, right, upv;
+    basis(forward, right, upv);
+    if (projection == 1) {  // equirectangular: longitude across the width, latitude across the height
+        float lon = (u - 0.5f) * (fov_x_deg * DEG_TO_RAD);
+        float lat = (0.5f - v) * (fov_y_deg * DEG_TO_RAD);
+        float s_lat, c_lat, s_lon, c_lon;
+        sin_cos(lat, s_lat, c_lat);
+        sin_cos(lon, s_lon, c_lon);
+        dir = forward * (c_lat * c_lon) + right * (c_lat * s_lon) + upv * s_lat;
+        return true;
+    }
+    if (projection == 2) {  // equidistant fisheye: the angle from the axis grows with the distance from the centre
+        float k = fov_x_deg * DEG_TO_RAD;
+        float x = (u - 0.5f) * k;
+        float y = (0.5f - v) * k / rmax(aspect, 1.0e-6f);
+        float theta = std::sqrt(x * x + y * y);
+        if (theta != theta || theta > PI) return false;
+        if (theta == 0.0f) { dir = forward; return true; }
+        float s, c;
+        sin_cos(theta, s, c);
+        dir = forward * c + (right * x + upv * y) * (s / theta);
+        return true;
+    }
+    return false;
+}
 Ray Camera::generate_ray(float aspect, float u, float v, float lx, float ly) const {
     Vec3 forward, right, upv;
     basis(forward, right, upv);
+    if (panoramic()) {  // scene/mod.rs:227 panorama_ray
+        Vec3 dir;
+        if (panorama_dir(aspect, u, v, dir)) return Ray(position, dir);
+        Ray r(position, forward);
+        r.t_max = 0.0f;
+        return r;
+    }
     if (ortho) {
         float w = ortho_width;
         Vec3 origin = position + right * ((u - 0.5f) * w) + upv * ((0.5f - v) * w / aspect);
@@ -123,7 +156,6 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             auto field = [](float v) { return v > 0.0f && v <= 3600.0f; };
             if (!field(c.fov_x_deg) || !field(c.fov_y_deg)) return r.invalid("fov_x_deg and fov_y_deg must be positive and at most 3600");
             if (c.exterior < 0.0f) return r.invalid("exterior must not be negative");
-            if (c.projection == 1 || c.projection == 2) { error = "unsupported: panoramic camera projection"; return false; }
         } else if (is("MESH")) {
             uint32_t vc, ic;
             if (!(r.u32(vc) && r.u32(ic))) return false;

@@ -20,7 +20,12 @@ struct Camera {  // scene/mod.rs:91
     uint32_t projection = 0;
     float fov_x_deg = 360, fov_y_deg = 180, exterior = 1;
     void basis(Vec3& forward, Vec3& right, Vec3& upv) const;
-    float lens_radius() const { return (fstop > 0.0f && focus_dist > 0.0f && !ortho) ? focal_mm / fstop * 0.5f : 0.0f; }
+    bool panoramic() const { return projection == 1 || projection == 2; }  // K3 (scene/mod.rs:178)
+    // A panoramic camera takes no lens sample (scene/mod.rs:338 sample_ray is a pinhole for it).
+    float lens_radius() const { return (fstop > 0.0f && focus_dist > 0.0f && !ortho && !panoramic()) ? focal_mm / fstop * 0.5f : 0.0f; }
+    // scene/mod.rs:196 panorama_dir: false where a fisheye sees nothing (more than 180 degrees from its axis)
+    bool panorama_dir(float aspect, float u, float v, Vec3& dir) const;
+    // scene/mod.rs:294 generate_ray; a panoramic camera's ray where it sees nothing has t_max 0
     Ray generate_ray(float aspect, float u, float v, float lx, float ly) const;
 };
 enum class LightKind : uint32_t { Rect = 0, Disk = 1, Sun = 2, Point = 3, Spot = 4, Ies = 5 };

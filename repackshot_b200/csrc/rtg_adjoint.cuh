@@ -64,13 +64,16 @@ __global__ void k_adjoint_camera(SceneDev S, WaveDesc w, PathBuffers P, AdjointD
         uint32_t x, y, index;
         wave_slot(w, slot, x, y, index);
         V3 o, d;
-        camera_ray(S, c_sobol, x, y, index, o, d);
+        const bool sees = camera_ray(S, c_sobol, x, y, index, o, d);
         P.o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
         P.d[slot] = make_float4(d.x, d.y, d.z, 0.0f);
-        P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        P.flags[slot] = PF_PRIMARY;
+        // A panoramic camera's sample that sees nothing added nothing to the film: it replays with
+        // no throughput and no radiance to come, so it adds no gradient.
+        const float w0 = sees ? 1.0f : 0.0f;
+        P.thr[slot] = make_float4(w0, w0, w0, 1.0f);
+        P.flags[slot] = PF_PRIMARY | (sees ? 0u : PF_NOTHING);
         P.queue[0][slot] = slot;
-        float4 L = P.sum[slot];
+        float4 L = sees ? P.sum[slot] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         A.rem[slot] = L;
         A.pend[slot] = ADJ_NONE;
         all += absf(L.x) + absf(L.y) + absf(L.z);

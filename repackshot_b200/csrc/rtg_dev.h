@@ -126,6 +126,8 @@ struct SceneDev {
     float cam_pos[3], cam_fwd[3], cam_right[3], cam_up[3];
     float focal_mm, sensor_mm, focus_dist, lens_radius, ortho_width, exterior;
     uint32_t ortho;
+    uint32_t projection;        // K3 (scene/mod.rs:55): 0 the standard camera, 1 equirectangular, 2 fisheye
+    float fov_x_deg, fov_y_deg;  // a panoramic camera's fields across the width and the height
     // render settings
     uint32_t width, height, seed, max_depth, pixel_filter;
     float clamp_indirect;

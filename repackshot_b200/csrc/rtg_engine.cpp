@@ -1395,14 +1395,18 @@ uint32_t rtg_render_paths(uint32_t handle, const uint32_t* xys, uint32_t n, floa
     st = run_wave(*sc, wd, nullptr);
     if (st) return st;
     std::vector<float4> sum(n), thr(n);
+    std::vector<uint32_t> flags(n);
     RTG_CHECK(cudaMemcpyAsync(sum.data(), sc->P.sum, (size_t)n * 16, cudaMemcpyDeviceToHost, sc->stream));
     RTG_CHECK(cudaMemcpyAsync(thr.data(), sc->P.thr, (size_t)n * 16, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaMemcpyAsync(flags.data(), sc->P.flags, (size_t)n * 4, cudaMemcpyDeviceToHost, sc->stream));
     st = finish(*sc, nullptr);
     if (st) return st;
     for (uint32_t i = 0; i < n; ++i) {
-        out5[5 * i] = sum[i].x;
-        out5[5 * i + 1] = sum[i].y;
-        out5[5 * i + 2] = sum[i].z;
+        // a panoramic camera's sample that sees nothing weighs black (render.rs:465)
+        const float k = (flags[i] & 8u) ? 0.0f : 1.0f;
+        out5[5 * i] = k == 1.0f ? sum[i].x : sum[i].x * k;
+        out5[5 * i + 1] = k == 1.0f ? sum[i].y : sum[i].y * k;
+        out5[5 * i + 2] = k == 1.0f ? sum[i].z : sum[i].z * k;
         out5[5 * i + 3] = thr[i].w;
         out5[5 * i + 4] = 0.0f;
     }

@@ -18,6 +18,9 @@ constexpr int TRACE_THREADS = 128;
 
 // Flags of a path slot.
 constexpr uint32_t PF_HAS_PDF = 1, PF_PRIMARY = 2, PF_MEDIUM = 4;
+// A panoramic camera's sample that sees nothing (scene/mod.rs:227): its ray has an empty interval
+// (no hit, no floor) and its radiance is multiplied by its black weight when it reaches the film.
+constexpr uint32_t PF_NOTHING = 8;
 // The path's flags also hold the cut-outs it passed (bits 8-14, at most MAX_CUTOUTS) and its vertex
 // count (bits 16-26): a cut-out pass is no vertex, so a path's bounce can fall behind the round.
 constexpr uint32_t PF_CUT_SHIFT = 8, PF_CUT_MASK = 0x7fu << 8, PF_BOUNCE_SHIFT = 16, PF_BOUNCE_MASK = 0x7ffu << 16;
@@ -86,19 +89,20 @@ __global__ void k_camera(SceneDev S, WaveDesc w, PathBuffers P) {
     for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.n; slot += gridDim.x * blockDim.x) {
         uint32_t x, y, index;
         V3 o, d;
+        bool sees;
         if constexpr (BATCH) {
             uint32_t job;
             batch_slot(w, slot, job, x, y, index);
-            camera_ray(w.jobs[job].S, c_sobol, x, y, index, o, d);
+            sees = camera_ray(w.jobs[job].S, c_sobol, x, y, index, o, d);
         } else {
             wave_slot(w, slot, x, y, index);
-            camera_ray(S, c_sobol, x, y, index, o, d);
+            sees = camera_ray(S, c_sobol, x, y, index, o, d);
         }
         P.o[slot] = make_float4(o.x, o.y, o.z, 0.0f);  // w: distance since the last scattering vertex
         P.d[slot] = make_float4(d.x, d.y, d.z, 0.0f);  // w: density of the BSDF sample
         P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);  // w: alpha
         P.sum[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        P.flags[slot] = PF_PRIMARY;
+        P.flags[slot] = PF_PRIMARY | (sees ? 0u : PF_NOTHING);
         P.queue[0][slot] = slot;
     }
     if (blockIdx.x == 0) {
@@ -224,8 +228,8 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_extend(SceneDev S, PathBuffer
                 if (!busy && i < n) {
                     slot = order[i];
                     const float4 o = P.o[slot], d = P.d[slot];
-                    const bool primary = (P.flags[slot] & PF_PRIMARY) != 0;
-                    busy = trav_init(S, T, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, f_inf(), primary);
+                    const uint32_t pf = P.flags[slot];
+                    busy = !(pf & PF_NOTHING) && trav_init(S, T, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, f_inf(), (pf & PF_PRIMARY) != 0);
                     if (!busy) {
                         P.hit[slot] = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
                         const uint32_t key = material_key(S, false, 0);
@@ -305,7 +309,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
     float t_geometry = hit.w ? __uint_as_float(hit.z) : f_inf();
     // floor_t (integrator/mod.rs:493)
     float t_floor = f_inf();
-    if ((S.floor_mode == 1) && rd.z != 0.0f) {
+    if ((S.floor_mode == 1) && rd.z != 0.0f && !(flags & PF_NOTHING)) {
         float t = (S.floor_z - ro.z) / rd.z;
         if (t > 1.0e-3f && t < f_inf()) t_floor = t;
     }
@@ -671,6 +675,13 @@ __global__ void k_next_round(PathBuffers P, int cur) {
 }
 
 // ---- accumulate: film += each pixel's samples in sample-index order (image.rs:82) -------------------------
+// A sample's radiance times its camera weight (render.rs:465): white, or black for a panoramic
+// camera's sample that sees nothing.
+__device__ __forceinline__ float4 sample_sum(const PathBuffers& P, uint32_t slot) {
+    const float4 c = P.sum[slot];
+    if (!(P.flags[slot] & PF_NOTHING)) return c;
+    return make_float4(c.x * 0.0f, c.y * 0.0f, c.z * 0.0f, c.w);
+}
 // Film pixel (x, y) += the ns samples in slots slot0, slot0 + stride, ..., in that order
 // (Film::splat_alpha, image.rs:82).
 __device__ __forceinline__ void accumulate_pixel(const FilmDev& F, uint32_t x, uint32_t y, const PathBuffers& P, uint32_t slot0, uint32_t stride,
@@ -681,7 +692,7 @@ __device__ __forceinline__ void accumulate_pixel(const FilmDev& F, uint32_t x, u
     float wt = F.weight[fi], al = F.alpha[fi], l2 = F.lum2[fi];
     for (uint32_t s = 0; s < ns; ++s) {
         uint32_t slot = slot0 + s * stride;
-        float4 c = P.sum[slot];
+        float4 c = sample_sum(P, slot);
         r = r + c.x; g = g + c.y; b = b + c.z;
         wt = wt + 1.0f;
         al = al + P.thr[slot].w;
@@ -717,7 +728,7 @@ __global__ void k_accumulate_edges(WaveDesc w, PathBuffers P, FilmDev F) {
             float sr = 0.0f, sg = 0.0f, sb = 0.0f, cov = 0.0f;
             for (uint32_t j = 0; j < k; ++j) {
                 const uint32_t slot = (s * w.ne + e) * k + j;
-                const float4 c = P.sum[slot];
+                const float4 c = sample_sum(P, slot);
                 sr = sr + c.x; sg = sg + c.y; sb = sb + c.z;
                 cov = cov + P.thr[slot].w;
             }
@@ -747,12 +758,12 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_edge_exact(SceneDev S, const 
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         const uint32_t x = p % S.width, y = p / S.width;
         V3 o, d;
-        camera_ray_at(S, ((float)x + 0.5f) / (float)S.width, ((float)y + 0.5f) / (float)S.height, 0.0f, 0.0f, o, d);
+        const bool sees = camera_ray_at(S, ((float)x + 0.5f) / (float)S.width, ((float)y + 0.5f) / (float)S.height, 0.0f, 0.0f, o, d);
         TraceResult res;
-        const bool got = traverse<false>(S, o, d, 1.0e-3f, f_inf(), true, res, &err, stack);
+        const bool got = sees && traverse<false>(S, o, d, 1.0e-3f, f_inf(), true, res, &err, stack);
         const float t_geometry = got ? res.t : f_inf();
         float t_floor = f_inf();
-        if (S.floor_mode == 1 && d.z != 0.0f) {
+        if (S.floor_mode == 1 && d.z != 0.0f && sees) {
             const float t = (S.floor_z - o.z) / d.z;
             if (t > 1.0e-3f && t < f_inf()) t_floor = t;
         }
@@ -776,7 +787,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_edge_exact(SceneDev S, const 
             }
             if (ok) {
                 const V3 fwd = ld3(S.cam_fwd);
-                e.z = __float_as_uint(t * dot(d, fwd) + dot(o - ld3(S.cam_pos), fwd));
+                e.z = __float_as_uint(S.projection ? t * len(d) : t * dot(d, fwd) + dot(o - ld3(S.cam_pos), fwd));
             } else {
                 e = make_uint4(0u, 0u, __float_as_uint(f_inf()), 0u);
             }
@@ -790,13 +801,14 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_edge_exact(SceneDev S, const 
 // and depth bits as k_edge_exact writes them, the normal facing the ray (the floor's +-z), and the
 // albedo (passes.rs:209: the material's base colour, the default material's for an index out of
 // range, the floor's colour, black for the background).
-__device__ void first_hit_passes(const SceneDev& S, const LightsDev& L, V3 o, V3 d, SplitStack& stack, uint32_t* err, uint4& e, V3& normal,
-                                 Rgb& albedo) {
+// `sees`: false for a panoramic camera's ray that sees nothing (an empty interval: the background).
+__device__ void first_hit_passes(const SceneDev& S, const LightsDev& L, V3 o, V3 d, bool sees, SplitStack& stack, uint32_t* err, uint4& e,
+                                 V3& normal, Rgb& albedo) {
     TraceResult res;
-    const bool got = traverse<false>(S, o, d, 1.0e-3f, f_inf(), true, res, err, stack);
+    const bool got = sees && traverse<false>(S, o, d, 1.0e-3f, f_inf(), true, res, err, stack);
     const float t_geometry = got ? res.t : f_inf();
     float t_floor = f_inf();
-    if (S.floor_mode == 1 && d.z != 0.0f) {
+    if (S.floor_mode == 1 && d.z != 0.0f && sees) {
         const float t = (S.floor_z - o.z) / d.z;
         if (t > 1.0e-3f && t < f_inf()) t_floor = t;
     }
@@ -824,7 +836,7 @@ __device__ void first_hit_passes(const SceneDev& S, const LightsDev& L, V3 o, V3
         t = res.t;
     }
     const V3 fwd = ld3(S.cam_fwd);
-    e.z = __float_as_uint(t * dot(d, fwd) + dot(o - ld3(S.cam_pos), fwd));
+    e.z = __float_as_uint(S.projection ? t * len(d) : t * dot(d, fwd) + dot(o - ld3(S.cam_pos), fwd));  // passes.rs:191
 }
 
 // The exact passes of the centre rays of a rectangle (render.rs:529), background outside the image.
@@ -843,8 +855,8 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_exact_passes(SceneDev S, cons
         Rgb a;
         if (x < S.width && y < S.height) {
             V3 o, d;
-            camera_ray_at(S, ((float)x + 0.5f) / (float)S.width, ((float)y + 0.5f) / (float)S.height, 0.0f, 0.0f, o, d);
-            first_hit_passes(S, *Lg, o, d, stack, &err, e, nn, a);
+            const bool sees = camera_ray_at(S, ((float)x + 0.5f) / (float)S.width, ((float)y + 0.5f) / (float)S.height, 0.0f, 0.0f, o, d);
+            first_hit_passes(S, *Lg, o, d, sees, stack, &err, e, nn, a);
         }
         normal[3 * p] = nn.x;
         normal[3 * p + 1] = nn.y;
@@ -877,13 +889,13 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_albedo_pass(SceneDev S, const
             V3 nn, o, d;
             Rgb a;
             if (k <= 1) {
-                camera_ray(S, c_sobol, x, y, first + s, o, d);
-                first_hit_passes(S, *Lg, o, d, stack, &err, e, nn, a);
+                const bool sees = camera_ray(S, c_sobol, x, y, first + s, o, d);
+                first_hit_passes(S, *Lg, o, d, sees, stack, &err, e, nn, a);
             } else {
                 Rgb acc = rgb(0.0f, 0.0f, 0.0f);
                 for (uint32_t j = 0; j < k; ++j) {
-                    camera_ray(S, c_sobol, x, y, (first + s) * k + j, o, d);  // render.rs:376 sub_sample
-                    first_hit_passes(S, *Lg, o, d, stack, &err, e, nn, a);
+                    const bool sees = camera_ray(S, c_sobol, x, y, (first + s) * k + j, o, d);  // render.rs:376 sub_sample
+                    first_hit_passes(S, *Lg, o, d, sees, stack, &err, e, nn, a);
                     acc = rgb(acc.r + a.r, acc.g + a.g, acc.b + a.b);
                 }
                 const float inv = 1.0f / (float)k;
@@ -914,7 +926,7 @@ __global__ void k_albedo_hits(SceneDev S, const LightsDev* __restrict__ Lg, Wave
         const bool got = hit.w != 0u;
         const float t_geometry = got ? __uint_as_float(hit.z) : f_inf();
         float t_floor = f_inf();
-        if (S.floor_mode == 1 && d.z != 0.0f) {
+        if (S.floor_mode == 1 && d.z != 0.0f && !(P.flags[slot] & PF_NOTHING)) {
             const float t = (S.floor_z - o.z) / d.z;
             if (t > 1.0e-3f && t < f_inf()) t_floor = t;
         }

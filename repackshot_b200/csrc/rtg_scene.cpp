@@ -114,7 +114,6 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (!(s.fov_x > 0.0f && s.fov_x <= 3600.0f) || !(s.fov_y > 0.0f && s.fov_y <= 3600.0f))
                 return r.invalid("fov_x_deg and fov_y_deg must be positive and at most 3600");
             if (s.exterior < 0.0f) return r.invalid("exterior must not be negative");
-            if (s.projection == 1 || s.projection == 2) { error = "unsupported: panoramic camera projection"; return false; }
         } else if (is("MESH")) {
             seen_mesh = true;
             uint32_t vc, ic;
@@ -1193,8 +1192,11 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
     S.cam_right[0] = right.x; S.cam_right[1] = right.y; S.cam_right[2] = right.z;
     S.cam_up[0] = up.x; S.cam_up[1] = up.y; S.cam_up[2] = up.z;
     S.focal_mm = s.focal_mm; S.sensor_mm = s.sensor_mm; S.focus_dist = s.focus_dist;
-    S.lens_radius = (s.fstop > 0.0f && s.focus_dist > 0.0f && !s.ortho) ? s.focal_mm / s.fstop * 0.5f : 0.0f;
+    const bool panoramic = s.projection == 1 || s.projection == 2;  // K3: a pinhole, no lens sample
+    S.lens_radius = (s.fstop > 0.0f && s.focus_dist > 0.0f && !s.ortho && !panoramic) ? s.focal_mm / s.fstop * 0.5f : 0.0f;
     S.ortho_width = s.ortho_width; S.ortho = s.ortho; S.exterior = s.exterior;
+    S.projection = panoramic ? s.projection : 0;
+    S.fov_x_deg = s.fov_x; S.fov_y_deg = s.fov_y;
     S.width = s.width; S.height = s.height; S.seed = s.seed;
     S.max_depth = s.max_depth == 0 ? 8 : (s.max_depth < 1024 ? s.max_depth : 1024);
     S.pixel_filter = s.pixel_filter;

@@ -450,17 +450,43 @@ RTG_D void screen_of(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_
     su = rclamp(((float)x + du) / (float)width, 0.0f, 1.0f);
     sv = rclamp(((float)y + dv) / (float)height, 0.0f, 1.0f);
 }
-// Camera::generate_ray (scene/mod.rs:280) through the image point (u, v) and the lens point
-// (lx, ly) of the unit disc.
-RTG_D void camera_ray_at(const SceneDev& S, float u, float v, float lx, float ly, V3& o, V3& d) {
+// Camera::generate_ray (scene/mod.rs:294) through the image point (u, v) and the lens point
+// (lx, ly) of the unit disc. False where a panoramic camera sees nothing (a fisheye beyond 180
+// degrees from its axis: scene/mod.rs:227 gives a ray along the axis with an empty interval, whose
+// sample weighs black); the ray is then (position, axis).
+RTG_D bool camera_ray_at(const SceneDev& S, float u, float v, float lx, float ly, V3& o, V3& d) {
     uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
     float aspect = (float)width / (float)height;
     V3 pos = ld3(S.cam_pos), fwd = ld3(S.cam_fwd), right = ld3(S.cam_right), up = ld3(S.cam_up);
+    if (S.projection == 1) {  // scene/mod.rs:200: longitude across the width, latitude across the height
+        const float lon = (u - 0.5f) * (S.fov_x_deg * (PI / 180.0f));
+        const float lat = (0.5f - v) * (S.fov_y_deg * (PI / 180.0f));
+        float s_lat, c_lat, s_lon, c_lon;
+        sin_cos(lat, s_lat, c_lat);
+        sin_cos(lon, s_lon, c_lon);
+        o = pos;
+        d = fwd * (c_lat * c_lon) + right * (c_lat * s_lon) + up * s_lat;
+        return true;
+    }
+    if (S.projection == 2) {  // scene/mod.rs:207: the equidistant fisheye
+        const float k = S.fov_x_deg * (PI / 180.0f);
+        const float x = (u - 0.5f) * k;
+        const float y = (0.5f - v) * k / rmax(aspect, 1.0e-6f);
+        const float theta = sqrt_(x * x + y * y);
+        o = pos;
+        d = fwd;
+        if (theta != theta || theta > PI) return false;
+        if (theta == 0.0f) return true;
+        float s, c;
+        sin_cos(theta, s, c);
+        d = fwd * c + (right * x + up * y) * (s / theta);
+        return true;
+    }
     if (S.ortho) {
         float w = S.ortho_width;
         o = pos + right * ((u - 0.5f) * w) + up * ((0.5f - v) * w / aspect);
         d = fwd;
-        return;
+        return true;
     }
     float sw, sh;
     if (aspect >= 1.0f) { sw = S.sensor_mm; sh = S.sensor_mm / aspect; }
@@ -468,13 +494,15 @@ RTG_D void camera_ray_at(const SceneDev& S, float u, float v, float lx, float ly
     float px = (u - 0.5f) * sw;
     float py = (0.5f - v) * sh;
     V3 dir = normalize(fwd * S.focal_mm + right * px + up * py);
-    if (S.lens_radius == 0.0f) { o = pos; d = dir; return; }
+    if (S.lens_radius == 0.0f) { o = pos; d = dir; return true; }
     V3 focus = pos + dir * (S.focus_dist / dot(dir, fwd));
     o = pos + (right * lx + up * ly) * S.lens_radius;
     d = normalize(focus - o);
+    return true;
 }
-// The camera sample of (pixel, index): camera_sample_weighted (render.rs:79) with the plain thin lens.
-RTG_D void camera_ray(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, V3& o, V3& d) {
+// The camera sample of (pixel, index): camera_sample_weighted (render.rs:79) with the plain thin
+// lens; false for a panoramic camera's sample that sees nothing (its weight is black).
+RTG_D bool camera_ray(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, V3& o, V3& d) {
     uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
     uint64_t key = pixel_key(S.seed, x, y);
     float du = filter_offset(S, sample1(T, key, index, DIM_CAMERA));
@@ -484,7 +512,7 @@ RTG_D void camera_ray(const SceneDev& S, const SobolTable& T, uint32_t x, uint32
     float lx = 0.0f, ly = 0.0f;
     if (!S.ortho && S.lens_radius > 0.0f)
         concentric_disk(sample1(T, key, index, DIM_LENS), sample1(T, key, index, DIM_LENS + 1), lx, ly);
-    camera_ray_at(S, u, v, lx, ly, o, d);
+    return camera_ray_at(S, u, v, lx, ly, o, d);
 }
 
 }  // namespace rtg

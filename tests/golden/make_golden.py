@@ -17,6 +17,8 @@ its path tracer, read from the reference's own source tree (run where it is chec
   tests/golden/ies_profiles.json;
 * the hash of six adaptive-sampling decisions of the synthetic 45 x 37 image
   (engine/crates/rt-core/src/adaptive/tests.rs:497-534);
+* the three K3 interior views (tests/fixtures/k3-{plan,panorama,fisheye}.rsb, copied beside this
+  script as test inputs) and their pinned 4-spp film hashes (render/k3_tests.rs:17-22);
 * the hashes of the denoised example: the full filter at 4 spp and the viewport's at 2 and 4 spp
   (engine/crates/rt-post/src/denoise/tests.rs:392, 527-528).
 
@@ -85,6 +87,15 @@ def main():
     l5 = (REF / "tests" / "fixtures" / "l5.rsb").read_bytes()
     ies = {name: (REF / "tests" / "fixtures" / "ies" / (name + ".ies")).read_text() for name in ("downlight-symmetric", "wall-washer")}
     (OUT.parent / "ies_profiles.json").write_text(json.dumps(ies, indent=1) + "\n")
+    # The three interior views of K3 as the reference writes them (rt --write-k3-*-example), kept
+    # as test inputs: the room's split boxes, cylinder and sphere, the disk uplight, the physical
+    # sky through a thin pane, an orthographic plan with its ceiling hidden to the camera and the
+    # panoramic cameras; their films at 4 spp are pinned in render/k3_tests.rs.
+    k3 = (CORE / "render" / "k3_tests.rs").read_text()
+    for view in ("plan", "panorama", "fisheye"):
+        data = (REF / "tests" / "fixtures" / f"k3-{view}.rsb").read_bytes()
+        (OUT.parent / f"k3-{view}.rsb").write_bytes(data)
+        pins[f"k3_{view}_4spp"] = pinned(k3, f"PINNED_K3_{view.upper()}_4SPP")
     out = {
         "source": "Repackshot reference tree (engine crate rt-core), read by tests/golden/make_golden.py",
         "film_hashes": pins,
