@@ -59,6 +59,7 @@ def lib():
             "orc_ies": (u32, [ctypes.c_char_p, u32, v, u32, v, v, u32, v, v]),
             "orc_blackman_harris_table": (None, [v]),
             "orc_set_sky_table": (None, [v, u32]),
+            "orc_adjoint_reference": (u32, [u32, u32, u32, u32, u32, u32, u32, u32, v, u32, v, v]),
             "orc_edge_mask": (None, [u32, v]),
             "orc_adaptive_decide": (u32, [u32, u32, ctypes.c_float, ctypes.c_float, u32, v, v, v, v, v]),
             "orc_adaptive_film": (u32, [u32, u32, u32, u32, v, v, v, v, v, v]),
@@ -94,9 +95,10 @@ class OracleScene:
         self.handle = lib().orc_scene_load(rsb, len(rsb))
         if not self.handle:
             raise ValueError(error())
-        info = np.zeros(6, np.uint32)
+        info = np.zeros(8, np.uint32)
         lib().orc_scene_info(self.handle, _p(info))
-        self.width, self.height, self.seed, self.max_depth, self.instances, self.triangles = map(int, info)
+        (self.width, self.height, self.seed, self.max_depth, self.instances, self.triangles, self.n_materials,
+         self.n_lights) = map(int, info)
 
     def close(self):
         if self.handle:
@@ -141,6 +143,22 @@ class OracleScene:
         out = np.zeros((len(xys), 5), np.float32)
         lib().orc_paths(self.handle, _p(xys), len(xys), _p(out), int(threads))
         return out
+
+    def adjoint_reference(self, target, first, count, x=0, y=0, w=None, h=None, threads=0, correlated=False):
+        """The CPU reference of the device adjoint (orc_adjoint_reference): (loss, gradients as
+        float64: 4 per material -- base R, G, B, alpha -- then one per scene light's power);
+        decorrelated by sample halves unless `correlated`."""
+        w = self.width if w is None else w
+        h = self.height if h is None else h
+        t = np.ascontiguousarray(target, np.float32).reshape(-1)
+        assert t.size == 3 * w * h
+        n = 4 * self.n_materials + self.n_lights
+        grads = np.zeros(n, np.float64)
+        loss = np.zeros(1, np.float64)
+        if lib().orc_adjoint_reference(self.handle, x, y, w, h, first, count, int(correlated), _p(t), int(threads), _p(grads),
+                                       _p(loss)):
+            raise ValueError("orc_adjoint_reference: bad arguments")
+        return float(loss[0]), grads
 
     def trace(self, rays, camera=False, brute=False, threads=0):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)

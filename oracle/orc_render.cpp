@@ -220,12 +220,28 @@ bool Prepared::shadow(const Scene& s, const Ray& ray, Rgb& pass, PathStats& st) 
     return blocker == F_INF && peak(keep) > 0.0f;
 }
 
-// radiance_weighted (integrator/mod.rs:1140) for the scene features this subset reads.
+// One parameter perturbed for the adjoint's reference gradient, detached: sampling, light
+// selection, MIS weights and roulette are those of the unperturbed scene, while what a path
+// carries is evaluated with the perturbed value (the estimator the adjoint differentiates).
+struct Perturb {
+    int kind = 0;             // 1: a material's base colour (all channels at once), 2: its GGX alpha, 3: a light's power
+    uint32_t index = 0;       // the material (kinds 1, 2) or the scene light (kind 3)
+    Bsdf outside, inside;     // kinds 1, 2: the perturbed material's BSDFs
+    Rgb sigma;                // kind 1: its medium's absorption per mm (when it has one)
+    float light_ratio = 1.0f; // kind 3: perturbed power / power
+};
+
+// radiance_weighted (integrator/mod.rs:1140) for the scene features this subset reads. With
+// `pert`, *out_pert receives the same path's radiance under the detached perturbation.
 static void radiance(const Scene& scene, const Prepared& prep, const PixelSampler& sampler, Ray camera_ray, float su, float sv,
-                     Rgb& out, float& alpha_out, PathStats& st) {
+                     Rgb& out, float& alpha_out, PathStats& st, const Perturb* pert = nullptr, Rgb* out_pert = nullptr) {
     const Lights& lights = prep.lights;
     Ray ray = camera_ray;
     Rgb throughput = WHITE, sum = BLACK;
+    Rgb thr_p = WHITE, sum_p = BLACK;  // under the perturbation
+    const int only = pert && pert->kind == 3 ? (int)pert->index : -1;
+    const float ratio = pert && pert->kind == 3 ? pert->light_ratio : 1.0f;
+    uint32_t medium_material = 0;
     float alpha = 1.0f;
     bool has_pdf = false;
     float bsdf_pdf = 0.0f;
@@ -252,22 +268,35 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
         if (in_medium && finite(t_nearest)) {
             Rgb bl(fexp(-sigma.r * t_nearest), fexp(-sigma.g * t_nearest), fexp(-sigma.b * t_nearest));
             throughput = throughput * bl;
+            if (pert) {
+                const bool mine = pert->kind == 1 && medium_material == pert->index;
+                const Rgb& sg = mine ? pert->sigma : sigma;
+                thr_p = thr_p * (mine ? Rgb(fexp(-sg.r * t_nearest), fexp(-sg.g * t_nearest), fexp(-sg.b * t_nearest)) : bl);
+            }
         }
         const float* sp = has_pdf ? &bsdf_pdf : nullptr;
-        Rgb crossed = lights.crossed_from(ray, t_nearest, sp, &sampled_at, offset);
+        Rgb part;
+        Rgb crossed = lights.crossed_from(ray, t_nearest, sp, &sampled_at, offset, only, pert ? &part : nullptr);
         prep.add(sum, throughput * crossed, bounce >= 2);
+        if (pert) prep.add(sum_p, thr_p * (crossed + part * (ratio - 1.0f)), bounce >= 2);
         if (t_nearest == F_INF) {
             if (primary && prep.background == 0) {
-                Rgb seen = lights.escaped(ray.dir, nullptr, nullptr);
+                Rgb seen = lights.escaped(ray.dir, nullptr, nullptr, only, pert ? &part : nullptr);
                 float k = scene.camera.exterior;
                 sum = sum + throughput * (k == 1.0f ? seen : seen * k);
+                if (pert) {
+                    Rgb seen_p = seen + part * (ratio - 1.0f);
+                    sum_p = sum_p + thr_p * (k == 1.0f ? seen_p : seen_p * k);
+                }
             } else if (primary && (prep.background == 1 || prep.background == 3)) {
                 sum = sum + throughput * prep.backdrop(su, sv);
+                if (pert) sum_p = sum_p + thr_p * prep.backdrop(su, sv);
             } else if (primary && prep.background == 2) {
                 alpha = peak(crossed) > 0.0f ? 1.0f : 0.0f;
             } else {
-                Rgb sky = lights.escaped(ray.dir, sp, &sampled_at);
+                Rgb sky = lights.escaped(ray.dir, sp, &sampled_at, only, pert ? &part : nullptr);
                 prep.add(sum, throughput * sky, bounce >= 2);
+                if (pert) prep.add(sum_p, thr_p * (sky + part * (ratio - 1.0f)), bounce >= 2);
             }
             break;
         }
@@ -305,6 +334,7 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
                 // light.rs:1543).
                 float weight = has_pdf ? lights.emitter_weight(inst, bsdf_pdf, sampled_at, offset + t_geometry, dot(s_geometric, ray.dir)) : 1.0f;
                 prep.add(sum, throughput * material->radiance() * weight, bounce >= 2);
+                if (pert) prep.add(sum_p, thr_p * material->radiance() * weight, bounce >= 2);
             }
             break;
         }
@@ -321,6 +351,10 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
         }
         if (bounce >= prep.max_depth) break;
         Bsdf bsdf = material ? Bsdf::surface(*material, s_outside) : prep.floor_bsdf;
+        // the vertex's BSDF under the perturbation, when it is the perturbed material's
+        const bool perturbed = pert && (pert->kind == 1 || pert->kind == 2) && material && s_inst &&
+                               geo.instances[inst].material_id == pert->index;
+        const Bsdf* bsdf_p = perturbed ? (s_outside ? &pert->outside : &pert->inside) : nullptr;
         Frame frame = prep.frame(s_inst, inst, s_point, s_normal);
         Vec3 wo = frame.to_local(-ray.dir);
         Vec3 ng = s_geometric;
@@ -353,6 +387,13 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
                     Rgb c = throughput * f * ls.radiance * (std::fabs(wi.z) * weight / ls.pdf);
                     if (!(pass == WHITE)) c = c * pass;
                     prep.add(sum, c, bounce >= 1);
+                    if (pert) {
+                        Rgb fp = bsdf_p ? bsdf_p->eval(wo, wi, lobes) : f;
+                        Rgb lp = ls.source == only && only >= 0 ? ls.radiance * ratio : ls.radiance;
+                        Rgb cp = thr_p * fp * lp * (std::fabs(wi.z) * weight / ls.pdf);
+                        if (!(pass == WHITE)) cp = cp * pass;
+                        prep.add(sum_p, cp, bounce >= 1);
+                    }
                 }
             }
         }
@@ -369,10 +410,19 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
             break;
         }
         throughput = throughput * bs.weight;
+        if (pert) {
+            Rgb k = bs.weight;
+            if (bsdf_p && !bs.straight) {  // the sample's weight f / pdf with f perturbed, pdf held
+                Rgb f = bsdf.eval(wo, bs.wi, Lobes::All), fp = bsdf_p->eval(wo, bs.wi, Lobes::All);
+                k = Rgb(f.r > 0.0f ? k.r * (fp.r / f.r) : k.r, f.g > 0.0f ? k.g * (fp.g / f.g) : k.g, f.b > 0.0f ? k.b * (fp.b / f.b) : k.b);
+            }
+            thr_p = thr_p * k;
+        }
         if (bounce >= 2) {
             float survive = rclamp(peak(throughput), 0.05f, 1.0f);
             if (sampler.get1(dims + OFFSET_ROULETTE) >= survive) break;
             throughput = throughput / survive;
+            if (pert) thr_p = thr_p / survive;
         }
         float pk = peak(throughput);
         if (!(pk > 0.0f && finite(pk))) break;
@@ -390,6 +440,7 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
                     uint32_t mid = geo.instances[inst].material_id;
                     in_medium = mid < prep.has_medium.size() && prep.has_medium[mid];
                     if (in_medium) sigma = prep.media[mid];
+                    medium_material = mid;
                 } else {
                     in_medium = false;
                 }
@@ -400,6 +451,7 @@ static void radiance(const Scene& scene, const Prepared& prep, const PixelSample
     }
     out = sum;
     alpha_out = alpha;
+    if (out_pert) *out_pert = sum_p;
 }
 
 // The inverse CDF of the Blackman-Harris window (F. J. Harris, Proc. IEEE 66, 1978: a0 - a1 cos 2pi t
@@ -469,7 +521,7 @@ static Ray sample_ray(const Scene& scene, const PixelSampler& sampler, uint32_t 
 
 // camera_sample_weighted (render.rs:79) and the shade of render_tile_traced (render.rs:388).
 static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, uint32_t y, uint32_t index, Rgb& c,
-                        float& alpha, PathStats& st) {
+                        float& alpha, PathStats& st, const Perturb* pert = nullptr, Rgb* c_pert = nullptr) {
     uint32_t width = scene.render.width ? scene.render.width : 1, height = scene.render.height ? scene.render.height : 1;
     float aspect = (float)width / (float)height;
     PixelSampler sampler(scene.render.seed, x, y, index);
@@ -486,10 +538,13 @@ static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, ui
         concentric_disk(a, b, lx, ly);
     }
     Ray ray = scene.camera.generate_ray(aspect, u, v, lx, ly);
-    radiance(scene, prep, sampler, ray, rclamp(u, 0.0f, 1.0f), rclamp(v, 0.0f, 1.0f), c, alpha, st);
+    radiance(scene, prep, sampler, ray, rclamp(u, 0.0f, 1.0f), rclamp(v, 0.0f, 1.0f), c, alpha, st, pert, c_pert);
     // A panoramic camera's sample where it sees nothing brings no light (scene/mod.rs:338: its
     // weight is black; render.rs:465 multiplies the radiance by it).
-    if (scene.camera.panoramic() && !(ray.t_max > 0.0f)) c = c * BLACK;
+    if (scene.camera.panoramic() && !(ray.t_max > 0.0f)) {
+        c = c * BLACK;
+        if (c_pert) *c_pert = *c_pert * BLACK;
+    }
 }
 
 // The exact passes of a centre ray (passes.rs:168) that the edge mask compares: part and
@@ -709,9 +764,12 @@ uint32_t orc_scene_free(uint32_t h) {
     return 0;
 }
 // Scene facts: width, height, seed, max_depth, instance count, triangle count (instanced).
+// out8: width, height, seed, max depth, instances, triangles, materials, scene lights.
 uint32_t orc_scene_info(uint32_t h, uint32_t* out6) {
     Loaded* l = get(h);
     if (!l || !out6) return 1;
+    out6[6] = (uint32_t)l->scene.materials.size();
+    out6[7] = (uint32_t)l->scene.lights.size();
     out6[0] = l->scene.render.width;
     out6[1] = l->scene.render.height;
     out6[2] = l->scene.render.seed;
@@ -919,6 +977,129 @@ uint64_t orc_render_tile(uint32_t h, uint32_t x, uint32_t y, uint32_t w, uint32_
         if (out_alpha) out_alpha[i] = wt > 0.0f ? film.alpha[i] * inv : 0.0f;
     }
     return st.rays;
+}
+
+// The adjoint's reference gradient on the CPU: the loss of the film of samples [first, first +
+// count) of the rectangle (x0, y0, w, hgt) against `target` (w hgt 3 floats: mean over pixels and
+// channels of (film - target)^2, summed in double), and its gradient with respect to every
+// material's base colour (R, G, B) and GGX alpha and every scene light's power (grads: 4 per
+// material, then one per light), for the estimator the device adjoint differentiates: detached
+// sampling, and with two halves of the samples (count >= 2) each half's derivative weighted by
+// the other half's residual (the derivative of the mean over pixels and channels of
+// (mean_A - target)(mean_B - target)); with one sample or `correlated`, of the loss itself. Each parameter's
+// derivative is a central difference of the detached estimator (base colour and alpha +- 1e-3,
+// as the device's BSDF differences; a light's power +- 1e-3 of itself), every sum in double.
+// Returns 0, or 1 for a bad handle or argument.
+uint32_t orc_adjoint_reference(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint32_t hgt, uint32_t first, uint32_t count,
+                               uint32_t correlated, const float* target, uint32_t threads, double* grads, double* loss) {
+    Loaded* l = get(h);
+    if (!l || !target || !grads || !loss || w == 0 || hgt == 0 || count == 0) return 1;
+    const Scene& sc = l->scene;
+    const size_t npix = (size_t)w * hgt;
+    const uint32_t nm = (uint32_t)sc.materials.size(), nl = (uint32_t)sc.lights.size();
+    const uint32_t half = correlated ? 0 : count / 2;  // 0: one estimate from all samples
+    // Per pixel and channel: the sums of halves A (samples before first + half) and B.
+    auto render = [&](const Perturb* pert, std::vector<double>& sa, std::vector<double>& sb, std::vector<float>* film) {
+        sa.assign(3 * npix, 0.0);
+        sb.assign(3 * npix, 0.0);
+        if (film) film->assign(3 * npix, 0.0f);
+        parallel_chunks((uint32_t)npix, threads, [&](uint32_t b, uint32_t e, uint32_t) {
+            for (uint32_t p = b; p < e; ++p) {
+                const uint32_t px = x0 + p % w, py = y0 + p / w;
+                float fr = 0.0f, fg = 0.0f, fb = 0.0f;
+                for (uint32_t k = 0; k < count; ++k) {
+                    PathStats st;
+                    Rgb c, cp;
+                    float a;
+                    shade_pixel(sc, l->prep, px, py, first + k, c, a, st, pert, &cp);
+                    const Rgb& v = pert ? cp : c;
+                    double* acc = (half > 0 && k >= half) ? &sb[3 * p] : &sa[3 * p];
+                    acc[0] += v.r; acc[1] += v.g; acc[2] += v.b;
+                    fr = fr + c.r; fg = fg + c.g; fb = fb + c.b;
+                }
+                if (film) { (*film)[3 * p] = fr; (*film)[3 * p + 1] = fg; (*film)[3 * p + 2] = fb; }
+            }
+        });
+    };
+    std::vector<double> sa, sb, pa, pb, ma, mb;
+    std::vector<float> film;
+    render(nullptr, sa, sb, &film);
+    // the loss, and each half's weights: d loss / d (its mean) per pixel and channel
+    const double norm = 3.0 * (double)npix;
+    std::vector<double> wa(3 * npix), wb(3 * npix);
+    double lsum = 0.0;
+    const float inv = 1.0f / (float)count;
+    for (size_t i = 0; i < 3 * npix; ++i) {
+        const double t = target[i];
+        const double e = (double)(film[i] * inv) - t;
+        lsum += e * e;
+        if (half == 0) {
+            wa[i] = 2.0 * e / norm;
+            wb[i] = 0.0;
+        } else {
+            wa[i] = (sb[i] / (double)(count - half) - t) / norm;  // A's derivative takes B's residual
+            wb[i] = (sa[i] / (double)half - t) / norm;
+        }
+    }
+    *loss = lsum / norm;
+    const double na = half == 0 ? (double)count : (double)half, nb = (double)(count - half);
+    // sum over pixels of w . (mean_plus - mean_minus) per channel
+    auto delta = [&](int c) {
+        double g = 0.0;
+        for (size_t p = 0; p < npix; ++p) {
+            const size_t i = 3 * p + c;
+            g += wa[i] * (pa[i] - ma[i]) / na;
+            if (half > 0) g += wb[i] * (pb[i] - mb[i]) / nb;
+        }
+        return g;
+    };
+    const float hm = 1.0e-3f;
+    for (uint32_t m = 0; m < nm; ++m) {
+        for (int kind = 1; kind <= 2; ++kind) {
+            Perturb plus, minus;
+            for (int sgn = 0; sgn < 2; ++sgn) {
+                Perturb& q = sgn == 0 ? plus : minus;
+                Material mat = sc.materials[m];
+                const float d = sgn == 0 ? hm : -hm;
+                if (kind == 1) {
+                    mat.base_color = Rgb(mat.base_color.r + d, mat.base_color.g + d, mat.base_color.b + d);
+                } else {
+                    const float alpha = mat.roughness * mat.roughness;
+                    mat.roughness = std::sqrt(rmax(alpha + d, 0.0f));
+                }
+                q.kind = kind;
+                q.index = m;
+                q.outside = Bsdf::surface(mat, true);
+                q.inside = Bsdf::surface(mat, false);
+                if (kind == 1 && mat.absorption_mm > 0.0f) {
+                    auto f = [&](float c) { return -fln(rclamp(c, 1.0e-4f, 1.0f)) / mat.absorption_mm; };
+                    q.sigma = Rgb(f(mat.base_color.r), f(mat.base_color.g), f(mat.base_color.b));
+                }
+            }
+            render(&plus, pa, pb, nullptr);
+            render(&minus, ma, mb, nullptr);
+            if (kind == 1) {
+                for (int c = 0; c < 3; ++c) grads[4 * m + c] = delta(c) / (2.0 * (double)hm);
+            } else {
+                grads[4 * m + 3] = (delta(0) + delta(1) + delta(2)) / (2.0 * (double)hm);
+            }
+        }
+    }
+    for (uint32_t j = 0; j < nl; ++j) {
+        const float power = sc.lights[j].power;
+        grads[4 * nm + j] = 0.0;
+        if (!(power > 0.0f)) continue;
+        Perturb plus, minus;
+        plus.kind = minus.kind = 3;
+        plus.index = minus.index = j;
+        plus.light_ratio = 1.0f + hm;
+        minus.light_ratio = 1.0f - hm;
+        render(&plus, pa, pb, nullptr);
+        render(&minus, ma, mb, nullptr);
+        const double dp = (double)power * (double)(plus.light_ratio - minus.light_ratio);
+        grads[4 * nm + j] = (delta(0) + delta(1) + delta(2)) / dp;
+    }
+    return 0;
 }
 
 // Per-path radiance of explicit (pixel x, pixel y, sample) triples: out = r, g, b, alpha, rays.

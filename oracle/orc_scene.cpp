@@ -515,7 +515,8 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
         return facing / (d * d);
     };
     std::vector<float> weights;
-    for (const Light& light : scene.lights) {
+    for (size_t li = 0; li < scene.lights.size(); ++li) {
+        const Light& light = scene.lights[li];
         bool glossy = (light.flags & LIGHT_FLAG_GLOSSY) != 0;
         bool camera = (light.flags & LIGHT_FLAG_CAMERA) != 0;
         bool shadow = (light.flags & LIGHT_FLAG_NO_SHADOW) == 0;
@@ -544,6 +545,7 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
             sun.shadow = shadow;
             sun.entry = entry;
             sun.base = irradiance.luminance();
+            sun.source = (uint32_t)li;
             L.suns.push_back(sun);
             continue;
         }
@@ -583,6 +585,7 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
             sp.entry = entry;
             sp.base = sp.intensity.luminance();
             sp.near2 = rmax(r_m * r_m, 1.0e-6f);  // MIN_DISTANCE2_M2
+            sp.source = (uint32_t)li;
             // An IES light inside the sphere that bounds the scene sends it its whole flux.
             float toward = (sp.ies && length(light.position - centre) <= radius) ? sp.ies->efficiency() : 0.05f + 0.95f * sp.mask(centre);
             weights.push_back(flux * toward * reach(light.position, nullptr));
@@ -616,6 +619,7 @@ Lights Lights::make(const Scene& scene) {  // light.rs:673
         a.shadow = shadow;
         a.entry = entry;
         a.base = a.radiance.luminance() * a.area * 1.0e-6f;
+        a.source = (uint32_t)li;
         L.areas.push_back(a);
     }
     // light.rs:867-958: every emissive instance whose material is flagged as a light, sampled by
@@ -766,11 +770,11 @@ bool Lights::sample_selected(const Selection& from, float u_select, float u0, fl
     if (e.kind == LightRef::Sun) {  // light.rs:1197
         const SunLight& sun = suns[e.index];
         if (sun.delta) {
-            out = {sun.frame.z, F_INF, sun.radiance, pmf_v, true, sun.glossy, sun.glossy, sun.shadow};
+            out = {sun.frame.z, F_INF, sun.radiance, pmf_v, true, sun.glossy, sun.glossy, sun.shadow, (int)sun.source};
         } else {
             Vec3 local = uniform_cone(u0, u1, sun.one_minus_cos_max);
             out = {normalize(sun.frame.to_world(local)), F_INF, sun.radiance, pmf_v / sun.solid_angle, false, sun.glossy,
-                   sun.glossy, sun.shadow};
+                   sun.glossy, sun.shadow, (int)sun.source};
         }
     } else if (e.kind == LightRef::Sphere) {  // light.rs:1224
         const SphereLight& light = spheres[e.index];
@@ -783,14 +787,16 @@ bool Lights::sample_selected(const Selection& from, float u_select, float u0, fl
         float omc = 0.0f;
         if (light.radius > 0.0f && !light.cone(dist2, omc)) return false;
         if (omc == 0.0f) {
-            out = {towards, dist, light.intensity * (m / (dist2 * 1.0e-6f)), pmf_v, true, light.glossy, false, light.shadow};
+            out = {towards, dist, light.intensity * (m / (dist2 * 1.0e-6f)), pmf_v, true, light.glossy, false, light.shadow,
+                   (int)light.source};
         } else {
             Vec3 local = uniform_cone(u0, u1, omc);
             Vec3 wi = normalize(Frame::from_normal(towards).to_world(local));
             float b = dot(wi, d);
             float r2 = light.radius * light.radius;
             float near = b - std::sqrt(rmax(r2 - length_squared(d - wi * b), 0.0f));
-            out = {wi, rmax(near, 0.0f), light.radiance * m, pmf_v / (TAU * omc), false, light.glossy, false, light.shadow};
+            out = {wi, rmax(near, 0.0f), light.radiance * m, pmf_v / (TAU * omc), false, light.glossy, false, light.shadow,
+                   (int)light.source};
         }
     } else if (e.kind == LightRef::Area) {
         const AreaLight& light = areas[e.index];
@@ -802,7 +808,7 @@ bool Lights::sample_selected(const Selection& from, float u_select, float u0, fl
         float cos = -dot(wi, light.frame.z);
         if (!(cos > 0.0f && distance > 0.0f)) return false;
         out = {wi, distance, light.radiance_at(cos), pmf_v * dist2 / (light.area * cos), false, light.glossy, light.glossy,
-               light.shadow};
+               light.shadow, (int)light.source};
     } else if (e.kind == LightRef::Mesh) {  // light.rs:1270: a triangle by area, a point on it uniformly
         const MeshEmitter& em = meshes[e.index];
         size_t t;
@@ -829,8 +835,10 @@ bool Lights::sample_selected(const Selection& from, float u_select, float u0, fl
     }
     return out.pdf > 0.0f && finite(out.pdf) && out.radiance.luminance() > 0.0f;
 }
-Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, const Selection* from, float offset) const {
+Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, const Selection* from, float offset, int only,
+                         Rgb* part) const {
     Rgb sum = BLACK;  // light.rs:1354 crossed_areas, then light.rs:1387 crossed_spheres
+    if (part) *part = BLACK;
     for (const AreaLight& light : areas) {
         bool visible = bsdf_pdf ? light.glossy : light.camera;
         if (!visible) continue;
@@ -843,6 +851,7 @@ Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, con
             w = power_heuristic(*bsdf_pdf, light_pdf);
         }
         sum = sum + light.radiance_at(cos) * w;
+        if (part && (int)light.source == only) *part = *part + light.radiance_at(cos) * w;
     }
     for (const SphereLight& light : spheres) {
         bool visible = bsdf_pdf ? light.glossy : light.camera;
@@ -861,6 +870,7 @@ Rgb Lights::crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, con
                 w = 0.0f;
         }
         sum = sum + light.radiance * (m * w);
+        if (part && (int)light.source == only) *part = *part + light.radiance * (m * w);
     }
     return sum;
 }
@@ -881,14 +891,16 @@ bool Lights::camera_sees_panel(const Ray& ray, float t_max) const {
     }
     return false;
 }
-Rgb Lights::escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from) const {  // light.rs:1502
+Rgb Lights::escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from, int only, Rgb* part) const {  // light.rs:1502
     Rgb sum = env.radiance(dir);
+    if (part) *part = BLACK;
     if (bsdf_pdf && env_is_entry) sum = sum * power_heuristic(*bsdf_pdf, pmf(env_entry, *from) * env.pdf(dir));
     for (const SunLight& sun : suns) {
         bool visible = bsdf_pdf ? sun.glossy : sun.camera;
         if (!(visible && sun.contains(dir))) continue;
         float w = bsdf_pdf ? power_heuristic(*bsdf_pdf, pmf(sun.entry, *from) / sun.solid_angle) : 1.0f;
         sum = sum + sun.radiance * w;
+        if (part && (int)sun.source == only) *part = *part + sun.radiance * w;
     }
     return sum;
 }

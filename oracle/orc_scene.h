@@ -192,6 +192,7 @@ struct AreaLight {
     bool glossy, camera, shadow;
     uint32_t entry;
     float base, bound;
+    uint32_t source;  // the scene light it was built from
     Rgb radiance_at(float cos) const { return exponent == 0.0f ? radiance : radiance * powf_(cos, exponent); }
     Vec3 sample_point(float u0, float u1) const;
     bool intersect(const Ray& ray, float t_max, float& t, float& cos) const;
@@ -204,6 +205,7 @@ struct SunLight {  // light.rs:300
     bool delta, glossy, camera, shadow;
     uint32_t entry;
     float base;
+    uint32_t source;  // the scene light it was built from
     bool contains(Vec3 dir) const { return !delta && dot(dir, frame.z) >= cos_max; }
 };
 struct SphereLight {  // light.rs:330 (point lights, spots and IES lights)
@@ -217,6 +219,7 @@ struct SphereLight {  // light.rs:330 (point lights, spots and IES lights)
     bool glossy, camera, shadow;
     uint32_t entry;
     float base, near2;
+    uint32_t source;  // the scene light it was built from
     float mask(Vec3 x) const;
     bool cone(float dist2, float& omc) const;
     bool intersect(const Ray& ray, float t_max, float& t) const;
@@ -238,7 +241,8 @@ struct MeshEmitter {  // light.rs:440: an emissive instance sampled as an area l
     float weight(Vec3 x) const;
 };
 struct Selection { Vec3 point; float total = 0; bool by_flux = true; float weights[8] = {}; };
-struct LightSample { Vec3 wi; float distance; Rgb radiance; float pdf; bool delta, glossy, photon, shadow; };
+// source: the scene light the sample came from (-1: the environment or an emissive mesh)
+struct LightSample { Vec3 wi; float distance; Rgb radiance; float pdf; bool delta, glossy, photon, shadow; int source = -1; };
 struct LightRef {  // light.rs:488
     enum Kind : uint32_t { Area, Sun, Sphere, Mesh, Environment } kind;
     uint32_t index;
@@ -265,7 +269,9 @@ struct Lights {
     float pmf(uint32_t entry, const Selection& from) const;
     void pick_at(const Selection& s, float u, size_t& idx, float& rest, float& pmf_out) const;
     bool sample_selected(const Selection& s, float u_select, float u0, float u1, LightSample& out) const;
-    Rgb crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, const Selection* from, float offset) const;
+    // `only` >= 0: *part receives the share of scene light `only` in the result.
+    Rgb crossed_from(const Ray& ray, float t_max, const float* bsdf_pdf, const Selection* from, float offset, int only = -1,
+                     Rgb* part = nullptr) const;
     // light.rs:1536-1550: for a BSDF-sampled ray that hit emissive instance `instance` at
     // distance t with `cos` between the ray and the geometric normal, the MIS weight of the emission
     // found (1 when the instance is not a mesh light).
@@ -273,7 +279,7 @@ struct Lights {
     // light.rs:1490: a camera ray meets a light it sees (an area light flagged camera, or a sphere
     // flagged camera lit towards the ray's origin) before t_max.
     bool camera_sees_panel(const Ray& ray, float t_max) const;
-    Rgb escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from) const;
+    Rgb escaped(Vec3 dir, const float* bsdf_pdf, const Selection* from, int only = -1, Rgb* part = nullptr) const;
 };
 inline float power_heuristic(float pa, float pb) {  // light.rs:129
     if (!(pa > 0.0f)) return 0.0f;
