@@ -233,6 +233,20 @@ uint32_t rtg_set_path_capacity(uint32_t scene, uint32_t paths);
 uint32_t rtg_set_tuning(uint32_t scene, const uint32_t* values, uint32_t n);
 uint32_t rtg_get_tuning(uint32_t scene, uint32_t* values, uint32_t n);
 
+/* No counterpart in the reference: the autotuner. Chooses the scene's tuning (the four values of
+ * rtg_set_tuning) by rendering samples [first_sample, first_sample + count) of the rectangle
+ * (x, y, w, h) of the image (clipped to it; into a film of its own) under candidate settings, by
+ * coordinate descent: the ray sort's bits 0, 3, 4 and 5 (shadow rays sorted along), then shadow
+ * rays sorted or not, shading material-sorted or not, then waves of the whole call, a half or a
+ * quarter of its paths (at least 2^20). Each candidate renders once to warm up, then once timed
+ * with CUDA events on the scene's stream; the scene keeps the fastest. `report` (may be null)
+ * receives 5 doubles per candidate tried, at most max_report of them: its four values and its
+ * milliseconds; *n_tried (may be null) the number tried. Films are not touched; a render of the
+ * candidate is what a call with those samples would cost, so pick a count that is representative
+ * of the calls to come. RTG_STATUS_BAD_TILE for an empty rectangle or no samples. */
+uint32_t rtg_autotune(uint32_t scene, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t first_sample, uint32_t count,
+                      double* report, uint32_t max_report, uint32_t* n_tried);
+
 /* Extend-kernel timing: when enabled, every extend launch is bracketed by CUDA events on the
  * scene's stream. out5 = total extend milliseconds, extend launches, camera + extension rays,
  * shadow rays, kernels launched, accumulated since the last reset (read before this call's

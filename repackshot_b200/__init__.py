@@ -68,6 +68,7 @@ ABI = {
     "rtg_set_path_capacity": (_u32, [_u32, _u32]),
     "rtg_set_tuning": (_u32, [_u32, _f, _u32]),
     "rtg_get_tuning": (_u32, [_u32, _f, _u32]),
+    "rtg_autotune": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _u32, _f, _u32, ctypes.POINTER(_u32)]),
     "rtg_timing": (_u32, [_u32, _u32, _u32, _f]),
     "rtg_set_stream": (_u32, [_u32, ctypes.c_void_p]),
     "rtg_synchronize": (_u32, [_u32]),
@@ -245,6 +246,18 @@ class Scene:
                cur["capacity"] if capacity is None else int(capacity)]
         v = np.array(new, np.uint32)
         _check(lib().rtg_set_tuning(self.handle, _ptr(v), 4))
+
+    def autotune(self, first: int, count: int, x: int = 0, y: int = 0, w: int | None = None, h: int | None = None) -> dict:
+        """rtg_autotune: times candidate tunings on samples [first, first + count) of the rectangle
+        (default: the whole image) and keeps the fastest; returns it and every candidate's time."""
+        w = self.width if w is None else w
+        h = self.height if h is None else h
+        report = np.zeros((16, 5), np.float64)
+        n = _u32(0)
+        _check(lib().rtg_autotune(self.handle, x, y, w, h, first, count, _ptr(report), 16, ctypes.byref(n)))
+        tried = [{"ray_bits": int(r[0]), "shadow_sort": int(r[1]), "material_sort": int(r[2]), "capacity": int(r[3]), "ms": float(r[4])}
+                 for r in report[:int(n.value)]]
+        return {"chosen": self.tuning(), "tried": tried}
 
     def tuning(self) -> dict:
         """rtg_get_tuning: ray-sort bits, shadow sort, material sort, paths per wave (0: automatic)."""

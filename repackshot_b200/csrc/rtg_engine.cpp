@@ -1487,6 +1487,87 @@ uint32_t rtg_set_tuning(uint32_t handle, const uint32_t* values, uint32_t n) {
     return RTG_STATUS_OK;
 }
 
+// The autotuner: coordinate descent over the tuning, each candidate rendered once to warm up and
+// then timed with CUDA events on the scene's stream; the scene keeps the fastest.
+uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t first_sample, uint32_t count, double* report,
+                      uint32_t max_report, uint32_t* n_tried) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    if (n_tried) *n_tried = 0;
+    const uint64_t x_end = std::min<uint64_t>((uint64_t)x + w, sc->width), y_end = std::min<uint64_t>((uint64_t)y + h, sc->height);
+    if (x >= x_end || y >= y_end || count == 0) { g_error = "rtg_autotune: an empty rectangle or no samples"; return RTG_STATUS_BAD_TILE; }
+    Film tmp;
+    uint32_t st = make_film(x, y, (uint32_t)(x_end - x), (uint32_t)(y_end - y), tmp);
+    if (st) return st;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    RTG_CHECK(cudaEventCreate(&e0));
+    RTG_CHECK(cudaEventCreate(&e1));
+    std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> g0(e0, cudaEventDestroy), g1(e1, cudaEventDestroy);
+    const uint64_t paths = (x_end - x) * (y_end - y) * (uint64_t)count;
+    const bool timing = sc->timing;
+    sc->timing = false;
+    struct Cand { uint32_t bits, shadow, msort, cap; };
+    std::vector<std::pair<Cand, double>> tried;
+    auto measure = [&](const Cand& c, double& ms) -> uint32_t {
+        for (const auto& t : tried)
+            if (t.first.bits == c.bits && t.first.shadow == c.shadow && t.first.msort == c.msort && t.first.cap == c.cap) { ms = t.second; return 0; }
+        if (c.bits != sc->order.ray_bits && sc->P.rbins) RTG_CHECK(cudaMemsetAsync(sc->P.rbins, 0, SORT_BINS_BYTES, sc->stream));
+        sc->order.ray_bits = c.bits;
+        sc->order.shadow_sort = c.shadow;
+        sc->order.material_sort = c.msort;
+        sc->max_capacity = c.cap;
+        refresh_order(*sc);
+        uint32_t r = render_region(*sc, tmp.dev.ox, tmp.dev.oy, tmp.dev.w, tmp.dev.h, first_sample, count, tmp.dev, nullptr);  // warm-up
+        if (r) return r;
+        RTG_CHECK(cudaEventRecord(e0, sc->stream));
+        r = render_region(*sc, tmp.dev.ox, tmp.dev.oy, tmp.dev.w, tmp.dev.h, first_sample, count, tmp.dev, nullptr);
+        if (r) return r;
+        RTG_CHECK(cudaEventRecord(e1, sc->stream));
+        RTG_CHECK(cudaEventSynchronize(e1));
+        float f = 0.0f;
+        RTG_CHECK(cudaEventElapsedTime(&f, e0, e1));
+        ms = f;
+        tried.push_back({c, ms});
+        return 0;
+    };
+    Cand best{sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity};
+    double best_ms = 1e300;
+    auto consider = [&](const Cand& c) -> uint32_t {
+        double ms = 0.0;
+        uint32_t r = measure(c, ms);
+        if (r) return r;
+        if (ms < best_ms) { best_ms = ms; best = c; }
+        return 0;
+    };
+    // 1. the ray sort's grid (shadow rays sorted with it), 2. shadow rays, 3. material sort, 4. wave size
+    for (uint32_t bits : {0u, 3u, 4u, 5u})
+        if ((st = consider(Cand{bits, bits > 0 ? 1u : 0u, 1u, 0u}))) break;
+    if (!st && best.bits > 0) st = consider(Cand{best.bits, 1u - best.shadow, best.msort, best.cap});
+    if (!st) st = consider(Cand{best.bits, best.shadow, 1u - best.msort, best.cap});
+    for (uint64_t div : {2u, 4u}) {
+        if (st) break;
+        const uint64_t cap = paths / div;
+        if (cap >= (1u << 20)) st = consider(Cand{best.bits, best.shadow, best.msort, (uint32_t)std::min<uint64_t>(cap, MAX_WAVE_PATHS)});
+    }
+    // keep the fastest
+    if (best.bits != sc->order.ray_bits && sc->P.rbins) cudaMemsetAsync(sc->P.rbins, 0, SORT_BINS_BYTES, sc->stream);
+    sc->order.ray_bits = best.bits;
+    sc->order.shadow_sort = best.shadow;
+    sc->order.material_sort = best.msort;
+    sc->max_capacity = best.cap;
+    refresh_order(*sc);
+    sc->timing = timing;
+    if (n_tried) *n_tried = (uint32_t)tried.size();
+    for (size_t k = 0; report && k < tried.size() && k < max_report; ++k) {
+        const Cand& c = tried[k].first;
+        double* r = report + 5 * k;
+        r[0] = c.bits; r[1] = c.shadow; r[2] = c.msort; r[3] = c.cap; r[4] = tried[k].second;
+    }
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    return st;
+}
+
 uint32_t rtg_get_tuning(uint32_t handle, uint32_t* values, uint32_t n) {
     std::lock_guard<std::mutex> lk(g_mu);
     Scene* sc = scene_of(handle);
