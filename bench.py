@@ -325,11 +325,14 @@ def stress_comparison(rtg, spp, dist, world, stream):
             "adjoint_crop_1024_ms": adjoint_s * 1e3, "adjoint_params": 4 * nm + nl, "adjoint_loss": float(loss)}
 
 
-def batched_comparison(rtg, scene, spp_scale, dist, world):
+def batched_comparison(rtg, scene, spp_scale, dist, world, steady_mpaths_s):
     """The metric's plain-vs-batched half: the 64 camera x light-rig jobs of uneven resolution and
     spp on this scene's geometry, rendered back to back through the plain path (rtg_scene_update +
-    rtg_render_progressive per job) and as one batched queue (rtg_queue_*). Wall time around
-    synchronous calls, max over ranks; each rank renders the whole job set (replicas)."""
+    rtg_render_progressive per job) and as one batched queue (rtg_queue_*, run as one captured CUDA
+    graph), both with the autotuned tuning. Wall time around synchronous calls, max over ranks;
+    each rank renders the whole job set (replicas). `steady_mpaths_s` (the 1080p frame's device
+    throughput, one wave of 132.7 M paths) bounds what any schedule of the same paths can reach:
+    the ideal time is the jobs' paths at that rate."""
     from repackshot_b200 import scenes, shards
     jobs = scenes.product_jobs(spp_scale=spp_scale)
     rsbs = [scenes.to_rsb(j, meshes=False) for j in jobs]
@@ -358,10 +361,14 @@ def batched_comparison(rtg, scene, spp_scale, dist, world):
     q = rtg.Queue(scene)
     t0 = time.perf_counter()
     films = [q.add(b, 0, j.max_samples, j.width, j.height) for j, b in zip(jobs, rsbs)]
-    q.run()
+    q.run(graph=True)
     t_batched = shards.max_over_ranks(time.perf_counter() - t0, dist)
     same = bool(np.array_equal(films[-1].resolve(), plain_img))
+    ideal_s = paths / (steady_mpaths_s * 1e6)
     return {"jobs": len(jobs), "paths_per_gpu": paths, "spp_scale": spp_scale,
+            "ideal_s": ideal_s, "ideal_note": "the jobs' paths at the 1080p frame's steady device throughput (one wave of "
+                                              "132.7 M paths): no schedule of these paths beats it",
+            "batched_over_ideal": ideal_s / t_batched, "plain_over_ideal": ideal_s / t_plain,
             "workload": "64 jobs on the product geometry: 8 orbit cameras (0-315 deg, 35-135 mm) x 8 light rigs (1-4 "
                         "softboxes, radiance 1-20); per job a resolution from {256^2, 512^2, 1280x720, 1920x1080, "
                         "2048x1152} and spp from {4, 16, 64, 256} x spp_scale, drawn from PCG32 seeded with the job id",
@@ -444,6 +451,11 @@ def run_ours(args, world, rank, local, dist):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
+    # The autotuner picks the wave tuning on 4 samples of the frame (sample indices outside the
+    # timed ones), before the warm-up.
+    t0 = time.perf_counter()
+    tuned = scene.autotune(base + 90_000, 4) if args.autotune else {"chosen": scene.tuning(), "tried": []}
+    tune_s = time.perf_counter() - t0
     for i in range(args.warmup):
         film.clear()
         film.render(base + 10_000 * (i + 1), SPP)
@@ -485,7 +497,8 @@ def run_ours(args, world, rank, local, dist):
     stress = stress_comparison(rtg, args.stress_spp, dist, world, stream) if args.stress_spp > 0 else None
     adaptive = adaptive_comparison(rtg, scene, dist, world, args.adaptive_target, total_ms / args.steps) if args.adaptive_target > 0 else None
     # The metric's other halves (0 leaves a section out, e.g. for a profiler's launch list).
-    batched = batched_comparison(rtg, scene, args.batched_spp_scale, dist, world) if args.batched_spp_scale > 0 else None
+    batched = (batched_comparison(rtg, scene, args.batched_spp_scale, dist, world, value / world)
+               if args.batched_spp_scale > 0 else None)
     adjoint = adjoint_comparison(rtg, dist, world, args.fit_iterations) if args.fit_iterations > 0 else None
 
     if rank != 0:
@@ -522,7 +535,10 @@ def run_ours(args, world, rank, local, dist):
                    "l2": "flushed between steps (512 MiB write); the per-step working set (168 B of path state per path, "
                          "22 GB for the frame) exceeds L2",
                    "parallelism": f"replicas x{world}: each rank renders its own sample range of the frame",
-                   "scene_gen_s": round(gen_s, 3), "scene_load_s": round(load_s, 3), "bvh_build_s": round(scene.build_seconds, 3)},
+                   "scene_gen_s": round(gen_s, 3), "scene_load_s": round(load_s, 3), "bvh_build_s": round(scene.build_seconds, 3),
+                   "tuning": tuned["chosen"]},
+        "autotune": {"seconds": round(tune_s, 3), "workload": "the frame at 4 spp per candidate (a warm-up and a timed render)",
+                     "tried": tuned["tried"]},
         "mrays_per_s": world * rays / (total_ms / 1e3) / 1e6 if rank == 0 else None,
         "roofline": {"kernel": "k_extend (nearest-hit traversal)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_src,
@@ -569,10 +585,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--capacity", type=int, default=0, help="paths per wave (default: the library's automatic size)")
     ap.add_argument("--fit-iterations", type=int, default=200, help="adjoint fit iterations of the differentiable workload")
-    ap.add_argument("--batched-spp-scale", type=float, default=0.25,
+    ap.add_argument("--batched-spp-scale", type=float, default=1.0,
                     help="spp of the batched-queue comparison's 64 jobs, as a fraction of theirs (1: the full 6.5 G paths)")
     ap.add_argument("--stress-spp", type=int, default=8,
                     help="spp of the 10 M-triangle 4K stress section (plain, 8-rig queue, adjoint on a crop; 0 leaves it out)")
+    ap.add_argument("--autotune", type=int, default=1, help="choose the wave tuning with rtg_autotune before the warm-up (0: the default)")
     ap.add_argument("--denoise", type=int, default=1, help="time the guide passes and the denoiser on the frame (0 leaves it out)")
     ap.add_argument("--adaptive-target", type=float, default=0.02,
                     help="noise target of the adaptive-sampling comparison (0 leaves it out)")

@@ -391,7 +391,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
 
 // Eight blocks per SM (64 registers, with spills) rather than the compiler's 168 registers: as for
 // k_shade, more warps hide the scattered loads (512^2 adjoint iteration 51.4 -> 48.9 ms).
-__global__ void __launch_bounds__(128, 8) k_shade_adjoint(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, uint32_t bounce,
+__global__ void __launch_bounds__(128, RTG_SHADE_MIN_BLOCKS) k_shade_adjoint(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, uint32_t bounce,
                                                        WaveDesc w, AdjointDev A) {
     __shared__ float s_grad[MAX_ADJOINT_PARAMS];
     AdjBlock blk{s_grad};

@@ -15,6 +15,11 @@ __constant__ SobolTable c_sobol;
 
 // Threads per block of the traversal kernels (the stride of their shared stacks).
 constexpr int TRACE_THREADS = 128;
+// Blocks of 128 threads per SM that the shade kernels are compiled for (their register cap:
+// 65536 / (128 x this)); a build may set it (RTG_SHADE_MIN_BLOCKS) to compare occupancies.
+#ifndef RTG_SHADE_MIN_BLOCKS
+#define RTG_SHADE_MIN_BLOCKS 8
+#endif
 
 // Flags of a path slot.
 constexpr uint32_t PF_HAS_PDF = 1, PF_PRIMARY = 2, PF_MEDIUM = 4;
@@ -527,7 +532,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
 // frame: 369 -> 383 Mpaths/s; 5, 6 and 7 blocks measured 367, 379 and 372).
 // `order`: the active queue in the order to shade it (material-sorted, or as traced).
 template <bool BATCH>
-__global__ void __launch_bounds__(128, 8) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w,
+__global__ void __launch_bounds__(128, RTG_SHADE_MIN_BLOCKS) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w,
                                                   const uint32_t* __restrict__ order, RaySort R) {
     uint32_t n = *(volatile uint32_t*)&P.counters[cur];
     uint32_t rays_local = 0, shadow_local = 0;
