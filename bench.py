@@ -287,26 +287,31 @@ def stress_comparison(rtg, spp, dist, world, stream):
     rigs = [scenes.to_rsb(scenes.cfg4_scene(width=W4, height=H4, spp=spp, depth=D4, rig=scenes.light_rig(r), seed=1 + r), meshes=False)
             for r in range(8)]
     # the 8 rigs back to back through the plain path (rtg_scene_update + rtg_render_progressive),
-    # then as one batched queue: wall time around synchronous calls for both
-    s.synchronize()
-    t0 = time.perf_counter()
-    keep = []
-    for r in rigs:
-        s.update(r)
-        fr = s.film()
-        fr.render(0, spp)
-        keep.append(fr)
-    s.synchronize()
-    plain8_s = shards.max_over_ranks(time.perf_counter() - t0, dist)
-    del keep
-    q = rtg.Queue(s)
-    s.synchronize()
-    t0 = time.perf_counter()
-    films = [q.add(r, 0, spp, W4, H4) for r in rigs]
-    q.run()
-    queue_s = shards.max_over_ranks(time.perf_counter() - t0, dist)
-    del films
-    q.close()
+    # then as one batched queue (a captured graph): wall time around synchronous calls for both,
+    # alternated twice and the faster of each kept (a few seconds each at full power: the two
+    # should see the same clocks)
+    plain_times, queue_times = [], []
+    for _ in range(2):
+        s.synchronize()
+        t0 = time.perf_counter()
+        keep = []
+        for r in rigs:
+            s.update(r)
+            fr = s.film()
+            fr.render(0, spp)
+            keep.append(fr)
+        s.synchronize()
+        plain_times.append(shards.max_over_ranks(time.perf_counter() - t0, dist))
+        del keep
+        q = rtg.Queue(s)
+        s.synchronize()
+        t0 = time.perf_counter()
+        films = [q.add(r, 0, spp, W4, H4) for r in rigs]
+        q.run(graph=True)
+        queue_times.append(shards.max_over_ranks(time.perf_counter() - t0, dist))
+        del films
+        q.close()
+    plain8_s, queue_s = min(plain_times), min(queue_times)
     s.update(scenes.to_rsb(base, meshes=False))
     crop = ((W4 - 1024) // 2, (H4 - 1024) // 2, 1024, 1024)
     target = np.full((1024, 1024, 3), 0.5, np.float32)
@@ -322,6 +327,7 @@ def stress_comparison(rtg, spp, dist, world, stream):
             "plain_mpaths_s": world * paths / plain_s / 1e6, "plain_ms": plain_s * 1e3,
             "plain_8_rigs_back_to_back_mpaths_s": world * 8 * paths / plain8_s / 1e6, "plain_8_rigs_s": plain8_s,
             "queue_8_rigs_mpaths_s": world * 8 * paths / queue_s / 1e6, "queue_8_rigs_s": queue_s,
+            "plain_8_rigs_times_s": plain_times, "queue_8_rigs_times_s": queue_times,
             "adjoint_crop_1024_ms": adjoint_s * 1e3, "adjoint_params": 4 * nm + nl, "adjoint_loss": float(loss)}
 
 

@@ -26,9 +26,11 @@ CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 DEVICE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
                 "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v"]
-# RTG_SHADE_MIN_BLOCKS (environment): blocks per SM the shade kernels are compiled for (default 8).
-if os.environ.get("RTG_SHADE_MIN_BLOCKS", "").isdigit():
-    DEVICE_FLAGS.append("-DRTG_SHADE_MIN_BLOCKS=" + os.environ["RTG_SHADE_MIN_BLOCKS"])
+# RTG_SHADE_MIN_BLOCKS (environment): blocks per SM the shade kernels are compiled for (default 8);
+# RTG_SHORT_STACK (environment): traversal stack entries kept in shared memory (default 24).
+for _name in ("RTG_SHADE_MIN_BLOCKS", "RTG_SHORT_STACK"):
+    if os.environ.get(_name, "").isdigit():
+        DEVICE_FLAGS.append(f"-D{_name}={os.environ[_name]}")
 HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-pthread", f"-I{CUDA_HOME}/include"]
 
 HOST_SOURCES = ["rtg_scene.cpp", "rtg_bitmap.cpp", "rtg_ies.cpp", "rtg_tables.cpp", "rtg_energy.cpp", "rtg_adaptive.cpp", "rtg_engine.cpp"]

@@ -141,7 +141,12 @@ struct FlatStack {
 // A traversal stack whose first SHORT_STACK entries sit in shared memory, interleaved by thread
 // (entry k of thread i at sm[k * stride + i]), and the deeper ones in a per-thread array. Almost
 // every ray stays within the shared part.
-constexpr int SHORT_STACK = 24;
+// A build may set RTG_SHORT_STACK to trade shared memory (8 bytes x 128 threads per entry and
+// block) against spills to the deeper part.
+#ifndef RTG_SHORT_STACK
+#define RTG_SHORT_STACK 24
+#endif
+constexpr int SHORT_STACK = RTG_SHORT_STACK;
 struct SplitStack {
     uint64_t* sm;   // this thread's column of the shared block
     uint64_t* deep; // STACK_CAP - SHORT_STACK entries

@@ -3,7 +3,7 @@
 * Traversal: nearest-hit (instance, triangle, t bits) and any-hit flags on identical ray batches
   are bit-exact against the oracle's BVH and brute force.
 * Paths: per-path radiance of the CUDA wavefront equals the oracle's (tolerance 1e-4 relative,
-  the north star's bound; the path is built to be bit-exact and the tests report exactness).
+  the bound this path is held to; it is built to be bit-exact and the tests report exactness).
 * Films: the example at 4 spp through rtg_render_progressive and the pinned tiles through
   rtg_render_tile hash to the reference's pinned FNV-1a values; the benchmark's small scene at
   its full 16 spp is within rel-MSE 1e-3 of the oracle.
