@@ -237,33 +237,35 @@ class Scene:
         _check(lib().rtg_set_path_capacity(self.handle, paths))
 
     def set_tuning(self, ray_bits: int | None = None, shadow_sort: bool | None = None, material_sort: bool | None = None,
-                   capacity: int | None = None):
+                   capacity: int | None = None, l2_persist: bool | None = None):
         """rtg_set_tuning: how the scene's waves order their rays and paths (None keeps a value)."""
         cur = self.tuning()
         new = [cur["ray_bits"] if ray_bits is None else int(ray_bits),
                cur["shadow_sort"] if shadow_sort is None else int(bool(shadow_sort)),
                cur["material_sort"] if material_sort is None else int(bool(material_sort)),
-               cur["capacity"] if capacity is None else int(capacity)]
+               cur["capacity"] if capacity is None else int(capacity),
+               cur["l2_persist"] if l2_persist is None else int(bool(l2_persist))]
         v = np.array(new, np.uint32)
-        _check(lib().rtg_set_tuning(self.handle, _ptr(v), 4))
+        _check(lib().rtg_set_tuning(self.handle, _ptr(v), 5))
 
     def autotune(self, first: int, count: int, x: int = 0, y: int = 0, w: int | None = None, h: int | None = None) -> dict:
         """rtg_autotune: times candidate tunings on samples [first, first + count) of the rectangle
         (default: the whole image) and keeps the fastest; returns it and every candidate's time."""
         w = self.width if w is None else w
         h = self.height if h is None else h
-        report = np.zeros((16, 5), np.float64)
+        report = np.zeros((16, 6), np.float64)
         n = _u32(0)
         _check(lib().rtg_autotune(self.handle, x, y, w, h, first, count, _ptr(report), 16, ctypes.byref(n)))
-        tried = [{"ray_bits": int(r[0]), "shadow_sort": int(r[1]), "material_sort": int(r[2]), "capacity": int(r[3]), "ms": float(r[4])}
-                 for r in report[:int(n.value)]]
+        tried = [{"ray_bits": int(r[0]), "shadow_sort": int(r[1]), "material_sort": int(r[2]), "capacity": int(r[3]),
+                  "l2_persist": int(r[4]), "ms": float(r[5])} for r in report[:int(n.value)]]
         return {"chosen": self.tuning(), "tried": tried}
 
     def tuning(self) -> dict:
         """rtg_get_tuning: ray-sort bits, shadow sort, material sort, paths per wave (0: automatic)."""
-        v = np.zeros(4, np.uint32)
-        _check(lib().rtg_get_tuning(self.handle, _ptr(v), 4))
-        return {"ray_bits": int(v[0]), "shadow_sort": int(v[1]), "material_sort": int(v[2]), "capacity": int(v[3])}
+        v = np.zeros(5, np.uint32)
+        _check(lib().rtg_get_tuning(self.handle, _ptr(v), 5))
+        return {"ray_bits": int(v[0]), "shadow_sort": int(v[1]), "material_sort": int(v[2]), "capacity": int(v[3]),
+                "l2_persist": int(v[4])}
 
     def timing(self, enable: bool, reset: bool = False):
         """(extend ms, extend launches, camera+extension rays, shadow rays, kernels launched)

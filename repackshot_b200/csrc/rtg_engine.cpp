@@ -88,6 +88,7 @@ struct Scene {
     uint32_t capacity = 0;
     uint32_t max_capacity = 0;  // paths per wave; 0: automatic (wave_limit)
     RaySort order;              // how waves order their rays and paths (rtg_set_tuning)
+    size_t hot_bytes = 0;       // the traversal data at the start of the geometry allocation
     float sort_lo[3] = {0, 0, 0}, sort_hi[3] = {0, 0, 0};  // the box the ray sort grids
     // statistics
     uint64_t rays = 0;
@@ -218,15 +219,36 @@ uint32_t upload(BufSet& set, const std::vector<T>& v, const T*& out) {
 }
 
 // Uploads the trees, leaf triangles and hit-detail arrays of `F` into `set`, pointers into `S`.
-uint32_t upload_geometry(const Flat& F, BufSet& set, SceneDev& S) {
+// What traversal reads (nodes, leaf triangles, top-level leaves) lies first, in one allocation,
+// so that one L2 access-policy window can cover it (its size in *hot_bytes).
+uint32_t upload_geometry(const Flat& F, BufSet& set, SceneDev& S, size_t* hot_bytes = nullptr) {
     std::vector<float4> pos(F.positions.size() / 4), nrm(F.normals.size() / 4);
     std::memcpy(pos.data(), F.positions.data(), F.positions.size() * 4);
     std::memcpy(nrm.data(), F.normals.data(), F.normals.size() * 4);
     std::vector<uint4> ti(F.tri_index.size() / 4);
     std::memcpy(ti.data(), F.tri_index.data(), F.tri_index.size() * 4);
+    auto round = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t b_nodes = F.nodes.size() * sizeof(QNode), b_tris = F.tris.size() * sizeof(TriRec), b_blas = F.blas.size() * sizeof(BlasInst);
+    const size_t hot = round(b_nodes) + round(b_tris) + round(b_blas);
+    if (hot_bytes) *hot_bytes = hot;
+    S.nodes = nullptr;
+    S.tris = nullptr;
+    S.blas = nullptr;
+    if (hot) {
+        DevBuf b;
+        b.bytes = hot;
+        RTG_CHECK(cudaMalloc(&b.p, b.bytes));
+        set.bufs.push_back(b);
+        uint8_t* p = (uint8_t*)b.p;
+        if (b_nodes) RTG_CHECK(cudaMemcpy(p, F.nodes.data(), b_nodes, cudaMemcpyHostToDevice));
+        if (b_tris) RTG_CHECK(cudaMemcpy(p + round(b_nodes), F.tris.data(), b_tris, cudaMemcpyHostToDevice));
+        if (b_blas) RTG_CHECK(cudaMemcpy(p + round(b_nodes) + round(b_tris), F.blas.data(), b_blas, cudaMemcpyHostToDevice));
+        if (b_nodes) S.nodes = (const QNode*)p;
+        if (b_tris) S.tris = (const TriRec*)(p + round(b_nodes));
+        if (b_blas) S.blas = (const BlasInst*)(p + round(b_nodes) + round(b_tris));
+    }
     uint32_t st;
-    if ((st = upload(set, F.nodes, S.nodes)) || (st = upload(set, F.tris, S.tris)) || (st = upload(set, F.blas, S.blas)) ||
-        (st = upload(set, pos, S.positions)) || (st = upload(set, nrm, S.normals)) || (st = upload(set, ti, S.tri_index)))
+    if ((st = upload(set, pos, S.positions)) || (st = upload(set, nrm, S.normals)) || (st = upload(set, ti, S.tri_index)))
         return st;
     return RTG_STATUS_OK;
 }
@@ -307,8 +329,28 @@ constexpr uint64_t MAX_WAVE_PATHS = 0x7fffffffu;
 // own path buffers). Each wave ends with a tail of long paths that leaves the GPU part-idle, so
 // the fewer waves a call takes, the faster it runs: a 1080p frame at 64 spp is one wave of
 // 132.7 M paths (22 GB).
-// The ray sort's grid over the scene's sort box at the current bits per axis.
+// The L2 set-aside for persisting accesses this library asked for (0: none), per device.
+size_t g_l2_set_aside[64] = {};
+
+// The ray sort's grid over the scene's sort box at the current bits per axis, and the L2 window
+// over its traversal data: at most the device's largest window, persisting for the share of it
+// the set-aside holds. The set-aside is asked for when a scene first turns the window on; it is
+// a limit of this process's CUDA context and ends with it.
 void refresh_order(Scene& sc) {
+    int dev = 0, max_window = 0, max_persist = 0;
+    size_t aside = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev);
+        const size_t want = sc.order.l2_persist ? std::min<size_t>((size_t)std::max(max_persist, 0), sc.hot_bytes) : 0;
+        if (want > g_l2_set_aside[dev] && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess)
+            g_l2_set_aside[dev] = want;
+        cudaGetLastError();
+        aside = g_l2_set_aside[dev];
+    }
+    sc.order.l2_base = sc.S.nodes;
+    sc.order.l2_bytes = std::min<size_t>(sc.hot_bytes, (size_t)std::max(max_window, 0));
+    sc.order.l2_hit_ratio = sc.order.l2_bytes ? std::min(1.0f, (float)((double)aside / (double)sc.order.l2_bytes)) : 0.0f;
     const float cells = (float)(1u << sc.order.ray_bits);
     for (int k = 0; k < 3; ++k) {
         const float extent = sc.sort_hi[k] - sc.sort_lo[k];
@@ -776,7 +818,7 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     auto sc = std::make_unique<Scene>();
     if (cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking) != cudaSuccess) { g_error = "cudaStreamCreate failed"; return 0; }
     SceneDev geom = F.scene, shade = F.scene;
-    if (upload_geometry(F, sc->geometry, geom) || upload_shading(F, sc->shading, shade)) return 0;
+    if (upload_geometry(F, sc->geometry, geom, &sc->hot_bytes) || upload_shading(F, sc->shading, shade)) return 0;
     sc->S = compose(F.scene, geom, shade);
     sc->d_lights = sc->shading.lights;
     sc->geom_key = geometry_key(hs);
@@ -818,7 +860,8 @@ uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
     RTG_CHECK(cudaStreamSynchronize(sc->stream));
     BufSet geometry, shading;
     SceneDev geom = sc->S, shade = F.scene;
-    uint32_t st = same_geometry ? RTG_STATUS_OK : upload_geometry(F, geometry, geom);
+    size_t hot = sc->hot_bytes;
+    uint32_t st = same_geometry ? RTG_STATUS_OK : upload_geometry(F, geometry, geom, &hot);
     if (!st) st = upload_shading(F, shading, shade);
     if (st) {
         geometry.release();
@@ -832,6 +875,7 @@ uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
         geom.tlas_root = F.scene.tlas_root;
         geom.stack_need = F.scene.stack_need;
         set_sort_box(*sc, F);
+        sc->hot_bytes = hot;
         sc->geometry.release();
         sc->geometry = std::move(geometry);
         sc->nodes = F.nodes.size();
@@ -843,6 +887,7 @@ uint32_t rtg_scene_update(uint32_t handle, const uint8_t* bytes, uint32_t len) {
     sc->edges_ready = false;
     sc->S = compose(F.scene, geom, shade);
     sc->d_lights = sc->shading.lights;
+    refresh_order(*sc);  // the L2 window follows the geometry
     keep_shading(*sc, hs, F);
     if (!kept) sc->meshes = std::move(hs.meshes);
     sc->bitmaps = std::move(hs.bitmaps);
@@ -1478,6 +1523,7 @@ uint32_t rtg_set_tuning(uint32_t handle, const uint32_t* values, uint32_t n) {
     if (n > 1) o.shadow_sort = values[1] != 0;
     if (n > 2) o.material_sort = values[2] != 0;
     if (n > 3) cap = values[3] != 0 && values[3] < 1024 ? 1024 : values[3];
+    if (n > 4) o.l2_persist = values[4] != 0;
     // A wave leaves both histograms at zero, but the cursors of fewer bits lie inside the
     // histogram of more: clear them when the key count changes.
     if (o.ray_bits != sc->order.ray_bits && sc->P.rbins) RTG_CHECK(cudaMemsetAsync(sc->P.rbins, 0, SORT_BINS_BYTES, sc->stream));
@@ -1507,15 +1553,19 @@ uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint3
     const uint64_t paths = (x_end - x) * (y_end - y) * (uint64_t)count;
     const bool timing = sc->timing;
     sc->timing = false;
-    struct Cand { uint32_t bits, shadow, msort, cap; };
+    struct Cand { uint32_t bits, shadow, msort, cap, l2; };
     std::vector<std::pair<Cand, double>> tried;
     auto measure = [&](const Cand& c, double& ms) -> uint32_t {
         for (const auto& t : tried)
-            if (t.first.bits == c.bits && t.first.shadow == c.shadow && t.first.msort == c.msort && t.first.cap == c.cap) { ms = t.second; return 0; }
+            if (t.first.bits == c.bits && t.first.shadow == c.shadow && t.first.msort == c.msort && t.first.cap == c.cap && t.first.l2 == c.l2) {
+                ms = t.second;
+                return 0;
+            }
         if (c.bits != sc->order.ray_bits && sc->P.rbins) RTG_CHECK(cudaMemsetAsync(sc->P.rbins, 0, SORT_BINS_BYTES, sc->stream));
         sc->order.ray_bits = c.bits;
         sc->order.shadow_sort = c.shadow;
         sc->order.material_sort = c.msort;
+        sc->order.l2_persist = c.l2;
         sc->max_capacity = c.cap;
         refresh_order(*sc);
         uint32_t r = render_region(*sc, tmp.dev.ox, tmp.dev.oy, tmp.dev.w, tmp.dev.h, first_sample, count, tmp.dev, nullptr);  // warm-up
@@ -1531,7 +1581,7 @@ uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint3
         tried.push_back({c, ms});
         return 0;
     };
-    Cand best{sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity};
+    Cand best{sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity, sc->order.l2_persist};
     double best_ms = 1e300;
     auto consider = [&](const Cand& c) -> uint32_t {
         double ms = 0.0;
@@ -1540,29 +1590,33 @@ uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint3
         if (ms < best_ms) { best_ms = ms; best = c; }
         return 0;
     };
-    // 1. the ray sort's grid (shadow rays sorted with it), 2. shadow rays, 3. material sort, 4. wave size
+    // 1. the ray sort's grid (shadow rays sorted with it), 2. shadow rays, 3. material sort, 4. the
+    // L2 window over the traversal data, 5. wave size
     for (uint32_t bits : {0u, 3u, 4u, 5u})
-        if ((st = consider(Cand{bits, bits > 0 ? 1u : 0u, 1u, 0u}))) break;
-    if (!st && best.bits > 0) st = consider(Cand{best.bits, 1u - best.shadow, best.msort, best.cap});
-    if (!st) st = consider(Cand{best.bits, best.shadow, 1u - best.msort, best.cap});
+        if ((st = consider(Cand{bits, bits > 0 ? 1u : 0u, 1u, 0u, 0u}))) break;
+    if (!st && best.bits > 0) st = consider(Cand{best.bits, 1u - best.shadow, best.msort, best.cap, best.l2});
+    if (!st) st = consider(Cand{best.bits, best.shadow, 1u - best.msort, best.cap, best.l2});
+    if (!st) st = consider(Cand{best.bits, best.shadow, best.msort, best.cap, 1u - best.l2});
     for (uint64_t div : {2u, 4u}) {
         if (st) break;
         const uint64_t cap = paths / div;
-        if (cap >= (1u << 20)) st = consider(Cand{best.bits, best.shadow, best.msort, (uint32_t)std::min<uint64_t>(cap, MAX_WAVE_PATHS)});
+        if (cap >= (1u << 20))
+            st = consider(Cand{best.bits, best.shadow, best.msort, (uint32_t)std::min<uint64_t>(cap, MAX_WAVE_PATHS), best.l2});
     }
     // keep the fastest
     if (best.bits != sc->order.ray_bits && sc->P.rbins) cudaMemsetAsync(sc->P.rbins, 0, SORT_BINS_BYTES, sc->stream);
     sc->order.ray_bits = best.bits;
     sc->order.shadow_sort = best.shadow;
     sc->order.material_sort = best.msort;
+    sc->order.l2_persist = best.l2;
     sc->max_capacity = best.cap;
     refresh_order(*sc);
     sc->timing = timing;
     if (n_tried) *n_tried = (uint32_t)tried.size();
     for (size_t k = 0; report && k < tried.size() && k < max_report; ++k) {
         const Cand& c = tried[k].first;
-        double* r = report + 5 * k;
-        r[0] = c.bits; r[1] = c.shadow; r[2] = c.msort; r[3] = c.cap; r[4] = tried[k].second;
+        double* r = report + 6 * k;
+        r[0] = c.bits; r[1] = c.shadow; r[2] = c.msort; r[3] = c.cap; r[4] = c.l2; r[5] = tried[k].second;
     }
     RTG_CHECK(cudaStreamSynchronize(sc->stream));
     return st;
@@ -1573,8 +1627,8 @@ uint32_t rtg_get_tuning(uint32_t handle, uint32_t* values, uint32_t n) {
     Scene* sc = scene_of(handle);
     if (!sc) return RTG_STATUS_BAD_HANDLE;
     if (!values && n) return RTG_STATUS_NULL_POINTER;
-    const uint32_t v[4] = {sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity};
-    for (uint32_t k = 0; k < n && k < 4; ++k) values[k] = v[k];
+    const uint32_t v[5] = {sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity, sc->order.l2_persist};
+    for (uint32_t k = 0; k < n && k < 5; ++k) values[k] = v[k];
     return RTG_STATUS_OK;
 }
 

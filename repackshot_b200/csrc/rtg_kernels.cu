@@ -1114,6 +1114,30 @@ static int resident_blocks(const void* kernel, int threads) {
     return sms * per_sm;
 }
 
+// A traversal kernel's launch; with order.l2_persist, with an L2 access-policy window over the
+// scene's traversal data (persisting for its hit ratio, the rest streaming).
+template <class... KArgs, class... Args>
+static void launch_traversal(const RaySort& order, int grid, cudaStream_t st, void (*kernel)(KArgs...), Args... args) {
+    if (!(order.l2_persist && order.l2_base && order.l2_bytes)) {
+        kernel<<<grid, TRACE_THREADS, 0, st>>>(args...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(TRACE_THREADS);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(order.l2_base);
+    attr[0].val.accessPolicyWindow.num_bytes = order.l2_bytes;
+    attr[0].val.accessPolicyWindow.hitRatio = order.l2_hit_ratio;
+    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P) {
     const uint32_t rounds = wave_rounds(S);
     const bool rsort = order.ray_bits > 0 && P.rbins, ssort = rsort && order.shadow_sort && P.sbins;
@@ -1146,10 +1170,10 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
         }
         if (timing && timing->ev_count + 2 <= WaveTiming::MAX_EVENTS) {
             cudaEventRecord(timing->ev[timing->ev_count++], st);
-            k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur, traced);
+            launch_traversal(order, g_ext, st, k_extend, S, P, cur, traced);
             cudaEventRecord(timing->ev[timing->ev_count++], st);
         } else {
-            k_extend<<<g_ext, TRACE_THREADS, 0, st>>>(S, P, cur, traced);
+            launch_traversal(order, g_ext, st, k_extend, S, P, cur, traced);
         }
         if (round == 0 && w.alb && film && !batch) k_albedo_hits<<<g, 256, 0, st>>>(S, L, w, P);
         k_scan<<<1, 32, 0, st>>>(P);
@@ -1173,7 +1197,7 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
             k_key_scatter<<<g, 256, 0, st>>>(nullptr, P.sh_key, P.sbins + nk, &P.counters[2], P.queue[cur]);
             perm = P.queue[cur];
         }
-        if (!S.any_passable) k_shadow<<<g_sh, TRACE_THREADS, 0, st>>>(S, P, perm);
+        if (!S.any_passable) launch_traversal(order, g_sh, st, k_shadow, S, P, perm);
         else if (batch) k_shadow_walk<true><<<g, TRACE_THREADS, 0, st>>>(S, P, w, perm);
         else k_shadow_walk<false><<<g, TRACE_THREADS, 0, st>>>(S, P, w, perm);
         k_next_round<<<1, 1, 0, st>>>(P, cur);

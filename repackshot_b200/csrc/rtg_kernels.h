@@ -99,6 +99,13 @@ struct PathBuffers {
 struct RaySort {
     uint32_t ray_bits = 0, shadow_sort = 0, material_sort = 1;
     float lo[3] = {0, 0, 0}, scale[3] = {0, 0, 0};  // cell = (p - lo) * scale per axis
+    // l2_persist: the traversal kernels' launches mark the scene's traversal data (l2_base,
+    // l2_bytes: nodes, leaf triangles, top-level leaves) as persisting in L2 for the fraction
+    // l2_hit_ratio of it, so that the streamed path state does not evict it.
+    uint32_t l2_persist = 0;
+    const void* l2_base = nullptr;
+    size_t l2_bytes = 0;
+    float l2_hit_ratio = 0.0f;
 };
 constexpr uint32_t RAY_SORT_MAX_BITS = 5;
 inline uint32_t ray_sort_keys(uint32_t bits) { return 8u << (3u * bits); }

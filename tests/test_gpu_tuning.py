@@ -22,12 +22,13 @@ def bits(film):
 
 def test_every_tuning_gives_the_same_film(rtg, small_product_rsb):
     s = rtg.Scene(small_product_rsb)
-    assert s.tuning() == {"ray_bits": 4, "shadow_sort": 1, "material_sort": 1, "capacity": 0}
+    assert s.tuning() == {"ray_bits": 4, "shadow_sort": 1, "material_sort": 1, "capacity": 0, "l2_persist": 0}
     ref = None
-    for ray_bits, shadow, msort, cap in [(0, 0, 1, 0), (4, 1, 1, 0), (5, 1, 1, 0), (3, 0, 1, 0), (2, 1, 0, 0), (1, 1, 1, 4096),
-                                         (5, 0, 0, 20000), (4, 1, 1, 0)]:
-        s.set_tuning(ray_bits=ray_bits, shadow_sort=shadow, material_sort=msort, capacity=cap)
-        assert s.tuning() == {"ray_bits": ray_bits, "shadow_sort": shadow, "material_sort": msort, "capacity": max(cap, 1024) if cap else 0}
+    for ray_bits, shadow, msort, cap, l2 in [(0, 0, 1, 0, 0), (4, 1, 1, 0, 1), (5, 1, 1, 0, 0), (3, 0, 1, 0, 1), (2, 1, 0, 0, 0),
+                                             (1, 1, 1, 4096, 1), (5, 0, 0, 20000, 0), (4, 1, 1, 0, 0)]:
+        s.set_tuning(ray_bits=ray_bits, shadow_sort=shadow, material_sort=msort, capacity=cap, l2_persist=l2)
+        assert s.tuning() == {"ray_bits": ray_bits, "shadow_sort": shadow, "material_sort": msort,
+                              "capacity": max(cap, 1024) if cap else 0, "l2_persist": l2}
         f = s.film()
         f.render(0, 3)
         f.render(3, 5)
@@ -35,7 +36,7 @@ def test_every_tuning_gives_the_same_film(rtg, small_product_rsb):
         if ref is None:
             ref = got
         for a, b in zip(got, ref):
-            assert np.array_equal(a, b), (ray_bits, shadow, msort, cap)
+            assert np.array_equal(a, b), (ray_bits, shadow, msort, cap, l2)
 
 
 def test_out_of_range_bits_are_refused(rtg, cfg0_rsb):
@@ -55,7 +56,7 @@ def test_autotuner_keeps_the_fastest_and_the_bits(rtg, small_product_rsb):
     tried = out["tried"]
     assert len(tried) >= 5
     fastest = min(tried, key=lambda t: t["ms"])
-    assert out["chosen"] == {k: fastest[k] for k in ("ray_bits", "shadow_sort", "material_sort", "capacity")}
+    assert out["chosen"] == {k: fastest[k] for k in ("ray_bits", "shadow_sort", "material_sort", "capacity", "l2_persist")}
     f = s.film()
     f.render(0, 8)
     for a, b in zip(bits(f), bits(ref)):
