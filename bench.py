@@ -331,14 +331,35 @@ def stress_comparison(rtg, spp, dist, world, stream):
             "adjoint_crop_1024_ms": adjoint_s * 1e3, "adjoint_params": 4 * nm + nl, "adjoint_loss": float(loss)}
 
 
+def steady_rates(scene, jobs, rsbs, min_paths=64_000_000):
+    """Paths per second of each of the 8 cameras' path mixes at steady state: the first job with
+    that camera rendered with enough samples for one wave of at least `min_paths` paths, so that
+    its tail of long paths costs a few percent (device time around a synchronous call)."""
+    import math
+    rates = {}
+    for cam in range(8):
+        j = next(k for k in range(len(jobs)) if k % 8 == cam)
+        scene.update(rsbs[j])
+        npix = jobs[j].width * jobs[j].height
+        spp = max(1, math.ceil(min_paths / npix))
+        f = scene.film()
+        f.render(10_000, 1)  # warm-up
+        scene.synchronize()
+        t0 = time.perf_counter()
+        f.render(0, spp)
+        scene.synchronize()
+        rates[cam] = npix * spp / (time.perf_counter() - t0)
+    return rates
+
+
 def batched_comparison(rtg, scene, spp_scale, dist, world, steady_mpaths_s):
     """The metric's plain-vs-batched half: the 64 camera x light-rig jobs of uneven resolution and
     spp on this scene's geometry, rendered back to back through the plain path (rtg_scene_update +
     rtg_render_progressive per job) and as one batched queue (rtg_queue_*, run as one captured CUDA
     graph), both with the autotuned tuning. Wall time around synchronous calls, max over ranks;
-    each rank renders the whole job set (replicas). `steady_mpaths_s` (the 1080p frame's device
-    throughput, one wave of 132.7 M paths) bounds what any schedule of the same paths can reach:
-    the ideal time is the jobs' paths at that rate."""
+    each rank renders the whole job set (replicas). The ideal time, which no schedule of these
+    paths beats, is every job's paths at the steady rate of its camera's path mix (steady_rates);
+    `steady_mpaths_s` is the 1080p product frame's rate, for comparison."""
     from repackshot_b200 import scenes, shards
     jobs = scenes.product_jobs(spp_scale=spp_scale)
     rsbs = [scenes.to_rsb(j, meshes=False) for j in jobs]
@@ -370,10 +391,13 @@ def batched_comparison(rtg, scene, spp_scale, dist, world, steady_mpaths_s):
     q.run(graph=True)
     t_batched = shards.max_over_ranks(time.perf_counter() - t0, dist)
     same = bool(np.array_equal(films[-1].resolve(), plain_img))
-    ideal_s = paths / (steady_mpaths_s * 1e6)
+    del films
+    rates = steady_rates(scene, jobs, rsbs)
+    ideal_s = shards.max_over_ranks(sum(j.width * j.height * j.max_samples / rates[k % 8] for k, j in enumerate(jobs)), dist)
     return {"jobs": len(jobs), "paths_per_gpu": paths, "spp_scale": spp_scale,
-            "ideal_s": ideal_s, "ideal_note": "the jobs' paths at the 1080p frame's steady device throughput (one wave of "
-                                              "132.7 M paths): no schedule of these paths beats it",
+            "ideal_s": ideal_s, "ideal_note": "every job's paths at the steady rate of its camera's path mix (one wave of at "
+                                              "least 64 M paths per camera): no schedule of these paths beats it",
+            "steady_mpaths_s_per_camera": [rates[c] / 1e6 for c in range(8)], "frame_mpaths_s": steady_mpaths_s,
             "batched_over_ideal": ideal_s / t_batched, "plain_over_ideal": ideal_s / t_plain,
             "workload": "64 jobs on the product geometry: 8 orbit cameras (0-315 deg, 35-135 mm) x 8 light rigs (1-4 "
                         "softboxes, radiance 1-20); per job a resolution from {256^2, 512^2, 1280x720, 1920x1080, "

@@ -232,7 +232,7 @@ uint32_t rtg_set_path_capacity(uint32_t scene, uint32_t paths);
  *   context sets L2 aside for it the first time), so the streamed path state does not evict it.
  * rtg_set_tuning sets the first n values (n <= 5; later ones keep theirs); RTG_STATUS_BAD_SCENE for
  * ray-sort bits above 5. rtg_get_tuning writes the first n (n <= 5). A loaded scene starts at
- * 4, 1, 1, 0, 0. */
+ * 0, 0, 1, 0, 0. */
 uint32_t rtg_set_tuning(uint32_t scene, const uint32_t* values, uint32_t n);
 uint32_t rtg_get_tuning(uint32_t scene, uint32_t* values, uint32_t n);
 

@@ -31,11 +31,14 @@ class FitState:
 
 class Fit:
     def __init__(self, scene, desc: scenes.Scene, target: np.ndarray, spp: int, materials: Sequence[int] = range(16),
-                 lights: Sequence[int] = range(3), lr: float = 0.02):
-        """scene: a loaded repackshot_b200.Scene of `desc`; target: h x w x 3 linear RGB."""
+                 lights: Sequence[int] = range(3), lr: float = 0.02, decay: float = 1.0):
+        """scene: a loaded repackshot_b200.Scene of `desc`; target: h x w x 3 linear RGB. The step
+        size is lr at the first step and shrinks by `decay` at every step: with noisy gradients,
+        Adam's normalised steps let weakly constrained parameters wander by about lr per step, and
+        a decaying step lets them settle."""
         self.scene, self.desc = scene, copy.deepcopy(desc)
         self.target = np.ascontiguousarray(target, np.float32)
-        self.spp, self.lr = spp, lr
+        self.spp, self.lr, self.decay = spp, lr, decay
         self.materials, self.lights = list(materials), list(lights)
         self.film = scene.film()
         theta = np.concatenate([
@@ -78,7 +81,7 @@ class Fit:
         st.m = b1 * st.m + (1 - b1) * g
         st.v = b2 * st.v + (1 - b2) * g * g
         mh, vh = st.m / (1 - b1 ** st.step), st.v / (1 - b2 ** st.step)
-        st.theta = st.theta - self.lr * mh / (np.sqrt(vh) + eps)
+        st.theta = st.theta - self.lr * self.decay ** (st.step - 1) * mh / (np.sqrt(vh) + eps)
         k = len(self.materials)
         st.theta[:3 * k] = np.clip(st.theta[:3 * k], 0.0, 1.0)
         st.theta[3 * k:4 * k] = np.clip(st.theta[3 * k:4 * k], 0.01, 1.0)

@@ -69,9 +69,12 @@ def image(film):
 def test_adjoint_on_a_crop_matches_finite_differences(rtg):
     """The decorrelated adjoint's light-power gradients on a 64 x 40 crop at depth 16 against
     central finite differences (h = 1e-3 of each power, the same sample indices) of the loss it
-    differentiates: mean((mean_A - target)(mean_B - target)) over the two halves of the samples."""
+    differentiates, mean((mean_A - target)(mean_B - target)) over the two halves of the samples,
+    over 8 independent ranges of 4096 samples: their means agree within 1e-2 relative plus three
+    standard errors of their difference per range (the finite difference's light choices, which
+    follow the powers, flip under the step; the adjoint's are held)."""
     from repackshot_b200 import scenes
-    spp = 4096
+    spp, reps = 4096, 8
     base = scenes.cfg4_scene(width=W, height=H, spp=spp, depth=16)
     target_scene = copy.deepcopy(base)
     for light in target_scene.lights:
@@ -79,15 +82,17 @@ def test_adjoint_on_a_crop_matches_finite_differences(rtg):
     crop = (16, 8, 64, 40)
     ts = rtg.Scene(scenes.to_rsb(target_scene))
     tf = ts.film(*crop)
-    tf.render(10_000, 256)
+    tf.render(1_000_000, 256)
     target = image(tf).astype(np.float64)
     s = rtg.Scene(scenes.to_rsb(base))
-    f = s.film(*crop)
     nm, nl = s.adjoint_params()
     assert nl == len(base.lights) and nm == 17
-    loss, grads, _ = s.adjoint(f, target.astype(np.float32), 0, spp)
-    assert np.isfinite(loss) and np.all(np.isfinite(grads))
-    lg = grads[4 * nm:].astype(np.float64)
+    lg = []
+    for r in range(reps):
+        loss, grads, _ = s.adjoint(s.film(*crop), target.astype(np.float32), r * spp, spp)
+        assert np.isfinite(loss) and np.all(np.isfinite(grads))
+        lg.append(grads[4 * nm:].astype(np.float64))
+    lg = np.array(lg)
     half = spp // 2
     for j in range(len(base.lights)):
         h = 1.0e-3 * base.lights[j].power
@@ -96,13 +101,20 @@ def test_adjoint_on_a_crop_matches_finite_differences(rtg):
             v = copy.deepcopy(base)
             v.lights[j].power += sign * h
             s.update(scenes.to_rsb(v, meshes=False))
-            a, b = s.film(*crop), s.film(*crop)
-            a.render(0, half)
-            b.render(half, spp - half)
-            out.append(float(np.mean((image(a).astype(np.float64) - target) * (image(b).astype(np.float64) - target))))
+            per = []
+            for r in range(reps):
+                a, b = s.film(*crop), s.film(*crop)
+                a.render(r * spp, half)
+                b.render(r * spp + half, spp - half)
+                per.append(float(np.mean((image(a).astype(np.float64) - target) * (image(b).astype(np.float64) - target))))
+            out.append(np.array(per))
         fd = (out[0] - out[1]) / (2 * h)
-        print(f"cfg4 crop light {j}: adjoint {lg[j]:.6g} finite difference {fd:.6g}")
-        assert abs(lg[j] - fd) <= 1e-2 * abs(fd) + 1e-3 * np.abs(lg).max()
+        d = lg[:, j] - fd
+        sem = float(np.std(d, ddof=1) / np.sqrt(reps))
+        ma, mf = float(lg[:, j].mean()), float(fd.mean())
+        print(f"cfg4 crop light {j}: adjoint {ma:.6g} finite difference {mf:.6g} (relative {abs(ma - mf) / abs(mf):.3%}, "
+              f"noise {sem / abs(mf):.3%})")
+        assert abs(ma - mf) <= 1e-2 * abs(mf) + 3.0 * sem
     s.update(scenes.to_rsb(base, meshes=False))
 
 

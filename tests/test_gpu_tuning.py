@@ -22,7 +22,7 @@ def bits(film):
 
 def test_every_tuning_gives_the_same_film(rtg, small_product_rsb):
     s = rtg.Scene(small_product_rsb)
-    assert s.tuning() == {"ray_bits": 4, "shadow_sort": 1, "material_sort": 1, "capacity": 0, "l2_persist": 0}
+    assert s.tuning() == {"ray_bits": 0, "shadow_sort": 0, "material_sort": 1, "capacity": 0, "l2_persist": 0}
     ref = None
     for ray_bits, shadow, msort, cap, l2 in [(0, 0, 1, 0, 0), (4, 1, 1, 0, 1), (5, 1, 1, 0, 0), (3, 0, 1, 0, 1), (2, 1, 0, 0, 0),
                                              (1, 1, 1, 4096, 1), (5, 0, 0, 20000, 0), (4, 1, 1, 0, 0)]:
@@ -45,7 +45,7 @@ def test_out_of_range_bits_are_refused(rtg, cfg0_rsb):
     v = np.array([6, 1, 1, 0], np.uint32)
     assert L.rtg_set_tuning(s.handle, rtg._ptr(v), 4) == rtg.STATUS_BAD_SCENE
     assert L.rtg_set_tuning(0, rtg._ptr(v), 4) == rtg.STATUS_BAD_HANDLE
-    assert s.tuning()["ray_bits"] == 4
+    assert s.tuning()["ray_bits"] == 0
 
 
 def test_autotuner_keeps_the_fastest_and_the_bits(rtg, small_product_rsb):
