@@ -40,13 +40,25 @@ extern "C" {
 /* rt_version (ffi.rs): the ABI version. */
 uint32_t rtg_version(void);
 
+/* Bits of rtg_features (rt-core/src/lib.rs:76-150 FEATURE_*; the same values). */
+#define RTG_FEATURE_IES 8u      /* L5: IES lights (LGHT kind 5, IESP sections) */
+#define RTG_FEATURE_CAMERAS 16u /* K3: panoramic projections, the exterior factor, instances hidden to the camera */
+
+/* rt_features (ffi.rs:22, lib.rs:159 FEATURES): what this engine reads beyond the RSB every engine
+ * reads, as the reference's FEATURE_* bits: RTG_FEATURE_IES | RTG_FEATURE_CAMERAS. The other bits
+ * (textures, material programs, section views, pattern nodes, drops, front glass, weather, nested
+ * dielectrics) are clear: those sections are refused at load, so a host writes none of them. */
+uint32_t rtg_features(void);
+
 /* rt_scene_load (ffi.rs:56-66, lib.rs:145): parses an RSB scene (copied; the caller keeps its
  * bytes), builds its BVHs and uploads it. Returns a handle > 0, or 0 after recording the error
- * (rtg_scene_error_len / _copy). Lights of kinds 0-5 (rect, disk, sun, point, spot, IES), HDRI
- * environments and background images (BMAP sections: 8-bit sRGB, linear f32, Radiance files), the
- * classic sky, cut-outs and thin walls render; features outside the path tracer's core (textures,
- * lens optics, particles, the physical sky, OpenEXR bitmaps, emissive mesh lights, scattering
- * media, bevels, the shadow catcher) are refused with a message that starts with "unsupported:". */
+ * (rtg_scene_error_len / _copy). Lights of kinds 0-5 (rect, disk, sun, point, spot, IES) and
+ * emissive meshes, HDRI environments and background images (BMAP sections: 8-bit sRGB, linear f32,
+ * Radiance files), the classic and the physical sky, panoramic cameras, cut-outs and thin walls
+ * render; features outside the path tracer's core (textures, material programs, lens optics,
+ * particles, section views, front glass, weather, nested dielectrics, OpenEXR bitmaps, scattering
+ * media, dispersive glass, bevels, caustic photon maps, the shadow catcher) are refused with a
+ * message that starts with "unsupported:". */
 uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len);
 
 /* rt_scene_update (ffi.rs:68-88, rt-wasm/src/lib.rs:171-193, Scene::update_from_rsb
@@ -321,6 +333,11 @@ uint32_t rtg_render_tile_passes(uint32_t handle, uint32_t x, uint32_t y, uint32_
  * rectangle's pixels, w*h*3 floats: the base colour of what that sample's camera ray met first
  * (0 for the background and outside the image; an edge pixel's mean over its sub-samples). */
 uint32_t rtg_render_tile_albedo(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index, float* out);
+/* rt_render_tile_alpha (ffi.rs:379-418, lib.rs:537): the coverage (the alpha pass) of sample
+ * `sample_index` of the rectangle's pixels, w*h floats: 1 where that sample's camera ray met a
+ * surface of an instance first, 0 where it met the floor, a light panel or nothing (0 outside the
+ * image; an edge pixel's mean over its sub-samples). Status as rtg_render_tile. */
+uint32_t rtg_render_tile_alpha(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index, float* out);
 /* rt_denoise / rt_denoise_with (ffi.rs:599-683, lib.rs:420-475): the denoiser on a band of `rows`
  * image rows from `origin_y` of a width x height image of `samples` samples a pixel. `in` holds
  * width*rows*14 little-endian words: the planes sums (RGBA), lum2, albedo (3), normal (3), depth,

@@ -66,6 +66,7 @@ def lib():
             "orc_pixel_error": (ctypes.c_float, [ctypes.c_float] * 4 + [u32, ctypes.c_float]),
             "orc_render_passes": (u32, [u32, u32, u32, u32, u32, v, v, v, v]),
             "orc_render_albedo": (u32, [u32, u32, u32, u32, u32, u32, v]),
+            "orc_render_alpha": (u32, [u32, u32, u32, u32, u32, u32, v]),
             "orc_denoise": (u32, [u32, ctypes.c_float, u32, u32, u32, u32, u32, u32, u32, v, u32, v]),
             "orc_denoise_halo": (u32, [u32]),
         }
@@ -234,6 +235,14 @@ class OracleScene:
         h = self.height if h is None else h
         out = np.zeros((h, w, 3), np.float32)
         lib().orc_render_albedo(self.handle, x, y, w, h, sample, _p(out))
+        return out
+
+    def alpha(self, sample, x=0, y=0, w=None, h=None):
+        """The coverage of sample `sample` of the rectangle (rt_render_tile_alpha): (h, w)."""
+        w = self.width if w is None else w
+        h = self.height if h is None else h
+        out = np.zeros((h, w), np.float32)
+        lib().orc_render_alpha(self.handle, x, y, w, h, sample, _p(out))
         return out
 
     def guides(self, samples):

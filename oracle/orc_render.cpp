@@ -554,8 +554,10 @@ struct Exact { uint32_t part = 0, material = 0; float depth = F_INF; Vec3 normal
 constexpr uint32_t FLOOR_ID = 0xffffffffu;
 // first_hit (integrator/mod.rs:911) for the albedo pass (passes.rs:209 albedo_of): the base colour
 // of the material of what the ray met (the default material's for an index out of range), the
-// floor's colour, black for the background.
-static Rgb first_albedo(const Scene& scene, const Prepared& prep, const Ray& ray) {
+// floor's colour, black for the background. `covers` (may be null) gets passes.rs:221
+// coverage_of: 1 for FirstHit::Surface, 0 for the floor and the background (a light panel too).
+static Rgb first_albedo(const Scene& scene, const Prepared& prep, const Ray& ray, float* covers = nullptr) {
+    if (covers) *covers = 0.0f;
     RayHit hit;
     bool got = scene.geometry.trace(ray, true, hit, nullptr);
     float t_geometry = got ? hit.t : F_INF;
@@ -565,6 +567,7 @@ static Rgb first_albedo(const Scene& scene, const Prepared& prep, const Ray& ray
     if (t_floor < t_geometry) return scene.floor.color;
     Hit d;
     if (!scene.geometry.hit_details(ray, hit, d)) return BLACK;
+    if (covers) *covers = 1.0f;
     return prep.material(scene, d.instance).base_color;
 }
 // render.rs:503 centre_ray and integrator/mod.rs:911 first_hit, as Exact::of reads them.
@@ -865,6 +868,40 @@ uint32_t orc_render_passes(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uin
 // rt_render_tile_albedo (rt-wasm/src/lib.rs:510, render.rs:590): the albedo of sample `index` of
 // the rectangle's pixels, 3 floats a pixel (0 outside the image); an edge pixel gives the mean of
 // its k sub-samples.
+// render.rs:590 render_tile_albedo_traced, its alpha plane (rt-wasm lib.rs:537
+// render_tile_alpha_sample): the coverage of sample `index` of each pixel of the rectangle, an
+// edge pixel's the mean over its k sub-samples (summed in order, times 1/k), 0 outside the image.
+uint32_t orc_render_alpha(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint32_t hh, uint32_t index, float* out) {
+    Loaded* l = get(h);
+    if (!l || !out) return 1;
+    const Scene& sc = l->scene;
+    const uint32_t W = sc.render.width, H = sc.render.height;
+    const uint32_t k = sc.render.edge_supersample < 1 ? 1 : (sc.render.edge_supersample > 16 ? 16 : sc.render.edge_supersample);
+    for (uint32_t y = 0; y < hh; ++y)
+        for (uint32_t x = 0; x < w; ++x) {
+            const size_t i = (size_t)y * w + x;
+            float a = 0.0f;
+            const uint32_t px = x0 + x, py = y0 + y;
+            if ((uint64_t)x0 + x < W && (uint64_t)y0 + y < H) {
+                const bool edge = k > 1 && !l->edges.empty() && l->edges[(size_t)py * W + px];
+                float u, v;
+                if (!edge) {
+                    first_albedo(sc, l->prep, sample_ray(sc, PixelSampler(sc.render.seed, px, py, index), px, py, u, v), &a);
+                } else {
+                    float covered = 0.0f;
+                    for (uint32_t j = 0; j < k; ++j) {
+                        float c = 0.0f;
+                        first_albedo(sc, l->prep, sample_ray(sc, PixelSampler(sc.render.seed, px, py, index * k + j), px, py, u, v), &c);
+                        covered += c;
+                    }
+                    a = covered * (1.0f / (float)k);
+                }
+            }
+            out[i] = a;
+        }
+    return 0;
+}
+
 uint32_t orc_render_albedo(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w, uint32_t hh, uint32_t index, float* out) {
     Loaded* l = get(h);
     if (!l || !out) return 1;

@@ -39,6 +39,7 @@ _u32, _u64, _f = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
 # The ABI of include/repackshot_b200.h: name -> (restype, argtypes).
 ABI = {
     "rtg_version": (_u32, []),
+    "rtg_features": (_u32, []),
     "rtg_scene_load": (_u32, [ctypes.c_char_p, _u32]),
     "rtg_scene_update": (_u32, [_u32, ctypes.c_char_p, _u32]),
     "rtg_scene_error_len": (_u32, []),
@@ -81,6 +82,7 @@ ABI = {
     "rtg_adaptive_free": (_u32, [_u32]),
     "rtg_render_tile_passes": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _f]),
     "rtg_render_tile_albedo": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _f]),
+    "rtg_render_tile_alpha": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _f]),
     "rtg_denoise": (_u32, [_u32, _u32, _u32, _u32, _u32, _u32, _u32, _f, _f]),
     "rtg_denoise_with": (_u32, [_u32, ctypes.c_float, _u32, _u32, _u32, _u32, _u32, _u32, _u32, _f, _f]),
     "rtg_denoise_halo": (_u32, [_u32]),
@@ -418,6 +420,21 @@ def tile_albedo(handle: int, x: int, y: int, w: int, h: int, sample_index: int):
     out = np.zeros(max(w * h * 3, 1), np.float32)
     st = lib().rtg_render_tile_albedo(handle, x, y, w, h, sample_index, _ptr(out))
     return st, out[:w * h * 3]
+
+
+def tile_alpha(handle: int, x: int, y: int, w: int, h: int, sample_index: int):
+    """rt_render_tile_alpha: (status, w*h float32 coverage)."""
+    out = np.zeros(max(w * h, 1), np.float32)
+    st = lib().rtg_render_tile_alpha(handle, x, y, w, h, sample_index, _ptr(out))
+    return st, out[:w * h]
+
+
+FEATURE_IES, FEATURE_CAMERAS = 8, 16
+
+
+def features() -> int:
+    """rt_features: the reference's FEATURE_* bits this engine reads (IES lights, interior cameras)."""
+    return int(lib().rtg_features())
 
 
 class Adaptive:

@@ -806,6 +806,8 @@ extern "C" {
 
 uint32_t rtg_version(void) { return RTG_ABI_VERSION; }
 
+uint32_t rtg_features(void) { return RTG_FEATURE_IES | RTG_FEATURE_CAMERAS; }
+
 uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!bytes) { g_error = "null pointer"; return 0; }
@@ -1911,10 +1913,38 @@ uint32_t rtg_render_tile_albedo(uint32_t handle, uint32_t x, uint32_t y, uint32_
     RTG_CHECK(cudaMalloc(&m.p, m.bytes));
     RTG_CHECK(cudaMemsetAsync(m.p, 0, m.bytes, sc->stream));
     float* sum = (float*)m.p;
-    RTG_CHECK(launch_albedo_pass(sc->S, sc->d_lights, mask, x, y, w, h, sample_index, 1, sum, sum + 3 * px, sc->stream,
+    RTG_CHECK(launch_albedo_pass(sc->S, sc->d_lights, mask, x, y, w, h, sample_index, 1, sum, sum + 3 * px, nullptr, sc->stream,
                                  grid_for((uint32_t)px, 128)));
     sc->launches += 1;
     RTG_CHECK(cudaMemcpyAsync(out, sum, px * 12, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaStreamSynchronize(sc->stream));
+    return RTG_STATUS_OK;
+}
+
+uint32_t rtg_render_tile_alpha(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t sample_index, float* out) {
+    if (!out) return RTG_STATUS_NULL_POINTER;
+    std::lock_guard<std::mutex> lk(g_mu);
+    Scene* sc = scene_of(handle);
+    if (!sc) return RTG_STATUS_BAD_HANDLE;
+    const uint64_t px = (uint64_t)w * h;
+    if (px == 0 || px > RTG_MAX_TILE_PIXELS) return RTG_STATUS_BAD_TILE;
+    const uint8_t* mask = nullptr;
+    if (sc->S.edge_k > 1) {
+        uint32_t *l = nullptr, *c = nullptr;
+        const uint32_t st = edge_mask_of(*sc, mask, l, c);
+        if (st) return st;
+    }
+    DevBuf m;
+    struct Release { DevBuf& b; ~Release() { b.release(); } } release{m};
+    m.bytes = px * 20;
+    RTG_CHECK(cudaMalloc(&m.p, m.bytes));
+    RTG_CHECK(cudaMemsetAsync(m.p, 0, m.bytes, sc->stream));
+    float* sum = (float*)m.p;
+    float* alpha = sum + 4 * px;
+    RTG_CHECK(launch_albedo_pass(sc->S, sc->d_lights, mask, x, y, w, h, sample_index, 1, sum, sum + 3 * px, alpha, sc->stream,
+                                 grid_for((uint32_t)px, 128)));
+    sc->launches += 1;
+    RTG_CHECK(cudaMemcpyAsync(out, alpha, px * 4, cudaMemcpyDeviceToHost, sc->stream));
     RTG_CHECK(cudaStreamSynchronize(sc->stream));
     return RTG_STATUS_OK;
 }
@@ -1942,7 +1972,7 @@ uint32_t rtg_film_guides(uint32_t scene, uint32_t film, uint32_t first_sample, u
                                   grid_for((uint32_t)n, 128)));
     if (count)
         RTG_CHECK(launch_albedo_pass(sc->S, sc->d_lights, mask, d.ox, d.oy, d.w, d.h, first_sample, count, f->albedo_sum(), f->albedo_weight(),
-                                     sc->stream, grid_for((uint32_t)n, 128)));
+                                     nullptr, sc->stream, grid_for((uint32_t)n, 128)));
     sc->launches += count ? 2 : 1;
     RTG_CHECK(cudaStreamSynchronize(sc->stream));
     return RTG_STATUS_OK;

@@ -844,6 +844,10 @@ __device__ void first_hit_passes(const SceneDev& S, const LightsDev& L, V3 o, V3
     e.z = __float_as_uint(S.projection ? t * len(d) : t * dot(d, fwd) + dot(o - ld3(S.cam_pos), fwd));  // passes.rs:191
 }
 
+// passes.rs:221 coverage_of: whether first_hit_passes met a surface of an instance (its part id is
+// the instance + 1; the floor's is all ones, the background's and a light panel's 0).
+__device__ __forceinline__ bool first_hit_covers(uint4 e) { return e.x != 0u && e.x != 0xffffffffu; }
+
 // The exact passes of the centre rays of a rectangle (render.rs:529), background outside the image.
 __global__ void __launch_bounds__(TRACE_THREADS) k_exact_passes(SceneDev S, const LightsDev* __restrict__ Lg, uint32_t x0, uint32_t y0,
                                                                  uint32_t w, uint32_t h, float* normal, float* depth, uint32_t* part,
@@ -875,10 +879,12 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_exact_passes(SceneDev S, cons
 
 // The albedo of samples [first, first + count) of a rectangle's pixels inside the image, added in
 // sample order to `sum` (3 a pixel) with `weight` += 1 each (render.rs:590 render_tile_albedo_traced):
-// an edge pixel (`edge`, the image's mask, may be null) adds the mean of its k sub-samples.
+// an edge pixel (`edge`, the image's mask, may be null) adds the mean of its k sub-samples. With
+// `alpha` (may be null) the coverage of the same first hits is added likewise (passes.rs:221
+// coverage_of: 1 for a surface of an instance, 0 for the floor, a light panel or the background).
 __global__ void __launch_bounds__(TRACE_THREADS) k_albedo_pass(SceneDev S, const LightsDev* __restrict__ Lg, const uint8_t* __restrict__ edge,
                                                                 uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t first,
-                                                                uint32_t count, float* sum, float* weight) {
+                                                                uint32_t count, float* sum, float* weight, float* alpha) {
     __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
     uint64_t deep[STACK_CAP - SHORT_STACK];
     SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
@@ -888,33 +894,40 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_albedo_pass(SceneDev S, const
         const uint32_t x = x0 + p % w, y = y0 + p / w;
         if (x >= S.width || y >= S.height) continue;
         const uint32_t k = (edge && S.edge_k > 1 && edge[(size_t)y * S.width + x]) ? S.edge_k : 1u;
-        float r = sum[3 * p], g = sum[3 * p + 1], b = sum[3 * p + 2], wt = weight[p];
+        float r = sum[3 * p], g = sum[3 * p + 1], b = sum[3 * p + 2], wt = weight[p], cv = alpha ? alpha[p] : 0.0f;
         for (uint32_t s = 0; s < count; ++s) {
             uint4 e;
             V3 nn, o, d;
             Rgb a;
+            float c;
             if (k <= 1) {
                 const bool sees = camera_ray(S, c_sobol, x, y, first + s, o, d);
                 first_hit_passes(S, *Lg, o, d, sees, stack, &err, e, nn, a);
+                c = first_hit_covers(e) ? 1.0f : 0.0f;
             } else {
                 Rgb acc = rgb(0.0f, 0.0f, 0.0f);
+                float covered = 0.0f;
                 for (uint32_t j = 0; j < k; ++j) {
                     const bool sees = camera_ray(S, c_sobol, x, y, (first + s) * k + j, o, d);  // render.rs:376 sub_sample
                     first_hit_passes(S, *Lg, o, d, sees, stack, &err, e, nn, a);
                     acc = rgb(acc.r + a.r, acc.g + a.g, acc.b + a.b);
+                    covered = covered + (first_hit_covers(e) ? 1.0f : 0.0f);
                 }
                 const float inv = 1.0f / (float)k;
                 a = rgb(acc.r * inv, acc.g * inv, acc.b * inv);
+                c = covered * inv;
             }
             r = r + a.r;
             g = g + a.g;
             b = b + a.b;
             wt = wt + 1.0f;
+            cv = cv + c;
         }
         sum[3 * p] = r;
         sum[3 * p + 1] = g;
         sum[3 * p + 2] = b;
         weight[p] = wt;
+        if (alpha) alpha[p] = cv;
     }
     (void)err;
 }
@@ -1220,8 +1233,8 @@ cudaError_t launch_exact_passes(const SceneDev& S, const LightsDev* L, uint32_t 
     return cudaGetLastError();
 }
 cudaError_t launch_albedo_pass(const SceneDev& S, const LightsDev* L, const uint8_t* edge, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
-                               uint32_t first, uint32_t count, float* sum, float* weight, cudaStream_t st, int grid) {
-    k_albedo_pass<<<grid, TRACE_THREADS, 0, st>>>(S, L, edge, x0, y0, w, h, first, count, sum, weight);
+                               uint32_t first, uint32_t count, float* sum, float* weight, float* alpha, cudaStream_t st, int grid) {
+    k_albedo_pass<<<grid, TRACE_THREADS, 0, st>>>(S, L, edge, x0, y0, w, h, first, count, sum, weight, alpha);
     return cudaGetLastError();
 }
 cudaError_t launch_edge_list(const uint8_t* mask, uint32_t stride, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t* list,

@@ -23,7 +23,7 @@ cudaError_t launch_edge_mask(const SceneDev& S, const LightsDev* L, uint4* exact
 cudaError_t launch_exact_passes(const SceneDev& S, const LightsDev* L, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, float* normal,
                                 float* depth, uint32_t* part, uint32_t* material, cudaStream_t st, int grid);
 cudaError_t launch_albedo_pass(const SceneDev& S, const LightsDev* L, const uint8_t* edge, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
-                               uint32_t first, uint32_t count, float* sum, float* weight, cudaStream_t st, int grid);
+                               uint32_t first, uint32_t count, float* sum, float* weight, float* alpha, cudaStream_t st, int grid);
 cudaError_t launch_edge_list(const uint8_t* mask, uint32_t stride, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t* list,
                              uint32_t* count, cudaStream_t st, int grid);
 

@@ -60,6 +60,13 @@ def test_version_and_constants(rtg):
         assert getattr(rtg, "STATUS_" + name) == header_define("RTG_STATUS_" + name)
 
 
+def test_features_are_the_reference_bits_of_what_loads(rtg):
+    # rt_features (ffi.rs:22): FEATURE_IES = 8 (L5) and FEATURE_CAMERAS = 16 (K3), rt-core lib.rs:93,100;
+    # the texture, program, section, drop, glass, weather and nesting bits stay clear.
+    assert rtg.features() == header_define("RTG_FEATURE_IES") | header_define("RTG_FEATURE_CAMERAS") == 24
+    assert (rtg.FEATURE_IES, rtg.FEATURE_CAMERAS) == (8, 16)
+
+
 def test_bad_handles_and_null_pointers(rtg):
     L = rtg.lib()
     out = (ctypes.c_float * 12)()
@@ -67,6 +74,8 @@ def test_bad_handles_and_null_pointers(rtg):
     assert L.rtg_scene_free(4096) == rtg.STATUS_BAD_HANDLE
     assert L.rtg_render_tile(4096, 0, 0, 2, 2, 0, out) == rtg.STATUS_BAD_HANDLE
     assert L.rtg_render_tile_rgba(4096, 0, 0, 1, 1, 0, out) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_render_tile_alpha(4096, 0, 0, 4, 4, 0, out) == rtg.STATUS_BAD_HANDLE
+    assert L.rtg_render_tile_alpha(4096, 0, 0, 4, 4, 0, None) == rtg.STATUS_NULL_POINTER
     assert L.rtg_film_free(4096) == rtg.STATUS_BAD_FILM
     assert L.rtg_film_create(4096, 0, 0, 4, 4) == 0
     assert L.rtg_render_progressive(4096, 1, 0, 1, None) == rtg.STATUS_BAD_HANDLE
