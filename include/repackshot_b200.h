@@ -169,19 +169,23 @@ uint32_t rtg_queue_free(uint32_t queue);
  * light (1: its power).
  *
  * rtg_render_adjoint clears `film`, renders samples [first_sample, first_sample + count) into it
- * (the forward pass: the same bits as rtg_render_progressive), and returns
+ * (the forward pass: with RTG_ADJOINT_CORRELATED the same bits as rtg_render_progressive), and
+ * returns
  *   *loss = mean over the film's pixels and channels of (I - target)^2, I = rgb / weight, `target`
  *           w*h*3 floats of linear RGB over the film's rectangle (row major, host memory);
  *   grads[0 .. 4 n_materials): per material d loss / d (base R, base G, base B, alpha);
  *   grads[4 n_materials ..): per light d loss / d power  (n_grads = 4 n_materials + n_lights).
  * The backward pass replays every path from its pixel and sample index (nothing of the paths is
  * stored) and propagates the loss through them; sampling decisions are held fixed (detached).
- * By default the samples are split into two halves and each half's paths take the loss's
- * derivative from the other half's image, which makes the gradient an unbiased estimate of the
- * gradient of the loss of the noise-free image (a residual and a derivative from the same paths
- * carry correlated noise, a bias towards less noise, e.g. dimmer lights). With
- * RTG_ADJOINT_CORRELATED every path uses the residual of the whole film: the derivative of this
- * very estimate, as a same-seed finite difference measures it.
+ * By default the samples are split into two halves, A = [first_sample, first_sample + count/2)
+ * and B = the rest, and each half's paths take the loss's derivative from the other half's image.
+ * Half B is drawn with the scene's seed complemented (~seed): an independent scramble, since two
+ * ranges of one pixel's scrambled sequence are stratified together and so correlated. The
+ * gradient is then an unbiased estimate of the gradient of the loss of the noise-free image (a
+ * residual and a derivative from the same paths, or from correlated halves, carry a covariance
+ * term that shifts the minimum, e.g. towards dimmer lights). With RTG_ADJOINT_CORRELATED every
+ * path uses the residual of the whole film, all samples from the scene's seed: the derivative of
+ * this very estimate, as a same-seed finite difference measures it.
  * The film must lie inside the image; every path of the call is held in one wave (172 bytes each).
  * `residual` (may be null) receives the sum over replayed paths of |radiance left after the
  * replay| and of |radiance|: the first is 0 up to rounding when the replay retraced the forward

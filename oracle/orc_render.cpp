@@ -520,11 +520,14 @@ static Ray sample_ray(const Scene& scene, const PixelSampler& sampler, uint32_t 
 }
 
 // camera_sample_weighted (render.rs:79) and the shade of render_tile_traced (render.rs:388).
+// Sample indices from `split_b` on are scrambled with the seed's complement (the decorrelated
+// adjoint's second half); renders leave it at 0xffffffff.
 static void shade_pixel(const Scene& scene, const Prepared& prep, uint32_t x, uint32_t y, uint32_t index, Rgb& c,
-                        float& alpha, PathStats& st, const Perturb* pert = nullptr, Rgb* c_pert = nullptr) {
+                        float& alpha, PathStats& st, const Perturb* pert = nullptr, Rgb* c_pert = nullptr,
+                        uint32_t split_b = 0xffffffffu) {
     uint32_t width = scene.render.width ? scene.render.width : 1, height = scene.render.height ? scene.render.height : 1;
     float aspect = (float)width / (float)height;
-    PixelSampler sampler(scene.render.seed, x, y, index);
+    PixelSampler sampler(index >= split_b ? ~scene.render.seed : scene.render.seed, x, y, index);
     float du, dv;
     sampler.get2(DIM_CAMERA, du, dv);
     du = filter_offset(scene.render.pixel_filter, du);
@@ -1023,7 +1026,8 @@ uint64_t orc_render_tile(uint32_t h, uint32_t x, uint32_t y, uint32_t w, uint32_
 // material, then one per light), for the estimator the device adjoint differentiates: detached
 // sampling, and with two halves of the samples (count >= 2) each half's derivative weighted by
 // the other half's residual (the derivative of the mean over pixels and channels of
-// (mean_A - target)(mean_B - target)); with one sample or `correlated`, of the loss itself. Each parameter's
+// (mean_A - target)(mean_B - target)), half B drawn with the seed's complement as the device
+// draws it; with one sample or `correlated`, of the loss itself. Each parameter's
 // derivative is a central difference of the detached estimator (base colour and alpha +- 1e-3,
 // as the device's BSDF differences; a light's power +- 1e-3 of itself), every sum in double.
 // Returns 0, or 1 for a bad handle or argument.
@@ -1048,7 +1052,7 @@ uint32_t orc_adjoint_reference(uint32_t h, uint32_t x0, uint32_t y0, uint32_t w,
                     PathStats st;
                     Rgb c, cp;
                     float a;
-                    shade_pixel(sc, l->prep, px, py, first + k, c, a, st, pert, &cp);
+                    shade_pixel(sc, l->prep, px, py, first + k, c, a, st, pert, &cp, half > 0 ? first + half : 0xffffffffu);
                     const Rgb& v = pert ? cp : c;
                     double* acc = (half > 0 && k >= half) ? &sb[3 * p] : &sa[3 * p];
                     acc[0] += v.r; acc[1] += v.g; acc[2] += v.b;

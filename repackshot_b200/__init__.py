@@ -216,8 +216,9 @@ class Scene:
 
     def adjoint(self, film: "Film", target: np.ndarray, first: int, count: int, correlated: bool = False):
         """rtg_render_adjoint: (loss, gradients, residual). gradients: per material d/d base R, G,
-        B and d/d alpha, then per light d/d power. By default decorrelated by sample halves (an
-        unbiased gradient for fitting); `correlated` gives the derivative of this very estimate."""
+        B and d/d alpha, then per light d/d power. By default decorrelated by sample halves, the
+        second drawn with the seed adjoint_seed_b(seed) (an unbiased gradient for fitting);
+        `correlated` gives the derivative of this very estimate."""
         nm, nl = self.adjoint_params()
         target = np.ascontiguousarray(target, dtype=np.float32).reshape(-1)
         grads = np.zeros(4 * nm + nl, np.float32)
@@ -420,6 +421,12 @@ def tile_albedo(handle: int, x: int, y: int, w: int, h: int, sample_index: int):
     out = np.zeros(max(w * h * 3, 1), np.float32)
     st = lib().rtg_render_tile_albedo(handle, x, y, w, h, sample_index, _ptr(out))
     return st, out[:w * h * 3]
+
+
+def adjoint_seed_b(seed: int) -> int:
+    """The render seed the decorrelated adjoint draws its second half of samples with: the seed's
+    complement (32 bits)."""
+    return (~int(seed)) & 0xFFFFFFFF
 
 
 def tile_alpha(handle: int, x: int, y: int, w: int, h: int, sample_index: int):

@@ -264,7 +264,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
         V3 ng = s_geom;
         V3 origin = offset_origin(s_point, ng);
         uint32_t dims = bounce_dim(bounce);
-        uint64_t key = pixel_key(S.seed, x, y);
+        uint64_t key = sample_key(S, x, y, index);
         Sel selection = select_at(L, s_point);
         LightSample ls;
         if (sample_light(L, selection, sample1(c_sobol, key, index, dims + OFF_LIGHT_SELECT), sample1(c_sobol, key, index, dims + OFF_LIGHT),

@@ -130,6 +130,9 @@ struct SceneDev {
     float fov_x_deg, fov_y_deg;  // a panoramic camera's fields across the width and the height
     // render settings
     uint32_t width, height, seed, max_depth, pixel_filter;
+    // Sample indices from split_b on are scrambled with seed_b instead of seed (sample_key). A
+    // render keeps split_b = 0xffffffff; the decorrelated adjoint draws its second half with it.
+    uint32_t seed_b, split_b;
     float clamp_indirect;
     const float* filter_table;  // the Blackman-Harris inverse CDF, 256 points (pixel filter 3)
     uint32_t edge_k;            // samples per sample index of an edge pixel (1: no edge samples)

@@ -1316,6 +1316,18 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     RTG_CHECK(cudaMemcpyAsync(base + off_tab, tab.data(), tab.size() * sizeof(Bsdf), cudaMemcpyHostToDevice, s));
     RTG_CHECK(cudaMemcpyAsync(base + off_target, target, npix * 12, cudaMemcpyHostToDevice, s));
     RTG_CHECK(cudaMemsetAsync(base + off_grads, 0, off_loss + 8 - off_grads, s));
+    // With two halves, the second is drawn with the seed's complement: an independent scramble,
+    // so that E[(mean_A - T)(mean_B - T)] is the converged image's loss with no covariance term
+    // (two ranges of one Owen-scrambled sequence are stratified together, hence correlated). The
+    // launches of this call take the split; the scene's own renders never see it.
+    const bool halves = count >= 2 && !(flags & RTG_ADJOINT_CORRELATED);
+    struct SplitSeeds {
+        SceneDev& S;
+        SplitSeeds(SceneDev& s_, bool on, uint32_t split) : S(s_) {
+            if (on) { S.split_b = split; S.seed_b = ~S.seed; }
+        }
+        ~SplitSeeds() { S.split_b = 0xffffffffu; S.seed_b = S.seed; }
+    } split_seeds(sc->S, halves, first_sample + count / 2);
     // Forward: every path of the call in one wave, into the cleared film.
     RTG_CHECK(cudaMemsetAsync(f->mem.p, 0, f->mem.bytes, s));
     RTG_CHECK(cudaMemsetAsync(sc->P.counters, 0, 16, s));
@@ -1324,7 +1336,6 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     st = run_wave(*sc, wd, &F);
     if (st) return st;
     // Loss and path derivatives, then the replay.
-    const bool halves = count >= 2 && !(flags & RTG_ADJOINT_CORRELATED);
     launch_adjoint_delta(F, (const float*)(base + off_target), (float4*)(base + off_dpath), (double*)(base + off_loss), sc->P,
                          halves ? count : 1, s, grid_for((uint32_t)npix, 256));
     const Bsdf* t0 = (const Bsdf*)(base + off_tab);

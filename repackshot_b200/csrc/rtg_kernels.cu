@@ -394,7 +394,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
             if (S.any_cutout && mat->opacity < 1.0f && cut < MAX_CUTOUTS) {
                 uint32_t x, y, index;
                 xyi(x, y, index);
-                const float u = sample1(c_sobol, pixel_key(S.seed, x, y), index, cutout_dim(bounce, cut));
+                const float u = sample1(c_sobol, sample_key(S, x, y, index), index, cutout_dim(bounce, cut));
                 flags = (flags & ~PF_CUT_MASK) | ((cut + 1u) << PF_CUT_SHIFT);
                 if (u >= rmax(mat->opacity, 0.0f)) {
                     const V3 o2 = offset_origin(h.point, -ng);
@@ -427,7 +427,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
         uint32_t dims = bounce_dim(bounce);
         uint32_t x, y, index;
         xyi(x, y, index);
-        uint64_t key = pixel_key(S.seed, x, y);
+        uint64_t key = sample_key(S, x, y, index);
         // Next-event estimation: one light; the shadow ray goes to the shadow queue.
         Sel selection = select_at(L, s_point);
         LightSample ls;

@@ -1197,7 +1197,7 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
     S.ortho_width = s.ortho_width; S.ortho = s.ortho; S.exterior = s.exterior;
     S.projection = panoramic ? s.projection : 0;
     S.fov_x_deg = s.fov_x; S.fov_y_deg = s.fov_y;
-    S.width = s.width; S.height = s.height; S.seed = s.seed;
+    S.width = s.width; S.height = s.height; S.seed = s.seed; S.seed_b = s.seed; S.split_b = 0xffffffffu;
     S.max_depth = s.max_depth == 0 ? 8 : (s.max_depth < 1024 ? s.max_depth : 1024);
     S.pixel_filter = s.pixel_filter;
     S.edge_k = s.edge_supersample < 1 ? 1 : (s.edge_supersample > 16 ? 16 : s.edge_supersample);  // RenderSettings::edge_factor

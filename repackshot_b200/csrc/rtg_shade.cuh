@@ -441,10 +441,15 @@ RTG_D float filter_offset(const SceneDev& S, float u) {
     }
     return u;
 }
+// The scramble key of a pixel's sample (sampler.rs:339 with the render's seed): indices from
+// S.split_b on take S.seed_b. Every render has split_b = 0xffffffff, so its keys are the seed's.
+RTG_D uint64_t sample_key(const SceneDev& S, uint32_t x, uint32_t y, uint32_t index) {
+    return pixel_key(index >= S.split_b ? S.seed_b : S.seed, x, y);
+}
 // The screen position (u, v) in [0, 1]^2 of a camera sample (render.rs:96).
 RTG_D void screen_of(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, float& su, float& sv) {
     uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
-    uint64_t key = pixel_key(S.seed, x, y);
+    uint64_t key = sample_key(S, x, y, index);
     float du = filter_offset(S, sample1(T, key, index, DIM_CAMERA));
     float dv = filter_offset(S, sample1(T, key, index, DIM_CAMERA + 1));
     su = rclamp(((float)x + du) / (float)width, 0.0f, 1.0f);
@@ -504,7 +509,7 @@ RTG_D bool camera_ray_at(const SceneDev& S, float u, float v, float lx, float ly
 // lens; false for a panoramic camera's sample that sees nothing (its weight is black).
 RTG_D bool camera_ray(const SceneDev& S, const SobolTable& T, uint32_t x, uint32_t y, uint32_t index, V3& o, V3& d) {
     uint32_t width = S.width ? S.width : 1, height = S.height ? S.height : 1;
-    uint64_t key = pixel_key(S.seed, x, y);
+    uint64_t key = sample_key(S, x, y, index);
     float du = filter_offset(S, sample1(T, key, index, DIM_CAMERA));
     float dv = filter_offset(S, sample1(T, key, index, DIM_CAMERA + 1));
     float u = ((float)x + du) / (float)width;

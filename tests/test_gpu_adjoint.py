@@ -9,8 +9,8 @@
   relative, both the decorrelated gradient and the correlated one.
 - Against central finite differences at h = 1e-3 (base colour and alpha +- 1e-3, a light's power
   +- 1e-3 of itself) of the loss the decorrelated gradient differentiates, mean((mean_A - target)
-  (mean_B - target)) over two halves of the samples (whose expectation is the L2 loss of the
-  converged image), at the differentiable workload's depth 6 over 8 independent ranges of 4096
+  (mean_B - target)) over two halves of the samples, half B drawn with the complemented seed
+  (independent of A, so its expectation is the L2 loss of the converged image), at the differentiable workload's depth 6 over 8 independent ranges of 4096
   samples on 64 x 64 pixels: colour, alpha (alpha >= 0.1) and light power within 1e-2 relative
   plus three standard errors of the difference as the ranges measure it. The adjoint holds
   sampling fixed; the finite difference lets light choices, lobe choices and roulette move with
@@ -154,24 +154,36 @@ def fd_setup(rtg):
     s = rtg.Scene(scenes.to_rsb(base))
     grads = np.stack([s.adjoint(s.film(), target.astype(np.float32), r * spp, spp)[1] for r in range(REPS)]).astype(np.float64)
     half = spp // 2
+    # half B as the adjoint draws it: the same scene rendered with the complemented seed
+    s_b = rtg.Scene(scenes.to_rsb(with_seed(base, rtg.adjoint_seed_b(base.seed))))
 
     def split_loss(first):
-        a, b = s.film(), s.film()
+        a, b = s.film(), s_b.film()
         a.render(first, half)
         b.render(first + half, spp - half)
         return float(np.mean((image(a) - target) * (image(b) - target)))
+
+    def update(v):
+        s.update(scenes.to_rsb(v, meshes=False))
+        s_b.update(scenes.to_rsb(with_seed(v, rtg.adjoint_seed_b(v.seed)), meshes=False))
 
     def fd(kind, index, dh):
         out = []
         for sign in (1, -1):
             v = copy.deepcopy(base)
             set_param(v, kind, index, get_param(base, kind, index) + sign * dh)
-            s.update(scenes.to_rsb(v, meshes=False))
+            update(v)
             out.append(np.array([split_loss(r * spp) for r in range(REPS)]))
-        s.update(scenes.to_rsb(base, meshes=False))
+        update(base)
         return (out[0] - out[1]) / (2 * dh)
 
     return base, grads, fd
+
+
+def with_seed(desc, seed):
+    v = copy.deepcopy(desc)
+    v.seed = seed
+    return v
 
 
 def agree(name, adj, fd):

@@ -69,7 +69,8 @@ def image(film):
 def test_adjoint_on_a_crop_matches_finite_differences(rtg):
     """The decorrelated adjoint's light-power gradients on a 64 x 40 crop at depth 16 against
     central finite differences (h = 1e-3 of each power, the same sample indices) of the loss it
-    differentiates, mean((mean_A - target)(mean_B - target)) over the two halves of the samples,
+    differentiates, mean((mean_A - target)(mean_B - target)) over the two halves of the samples
+    (half B from the complemented seed, as the adjoint draws it),
     over 8 independent ranges of 4096 samples: their means agree within 1e-2 relative plus three
     standard errors of their difference per range (the finite difference's light choices, which
     follow the powers, flip under the step; the adjoint's are held)."""
@@ -85,6 +86,10 @@ def test_adjoint_on_a_crop_matches_finite_differences(rtg):
     tf.render(1_000_000, 256)
     target = image(tf).astype(np.float64)
     s = rtg.Scene(scenes.to_rsb(base))
+    seed_b = rtg.adjoint_seed_b(base.seed)  # half B as the adjoint draws it
+    b_desc = copy.deepcopy(base)
+    b_desc.seed = seed_b
+    s_b = rtg.Scene(scenes.to_rsb(b_desc))
     nm, nl = s.adjoint_params()
     assert nl == len(base.lights) and nm == 17
     lg = []
@@ -101,9 +106,11 @@ def test_adjoint_on_a_crop_matches_finite_differences(rtg):
             v = copy.deepcopy(base)
             v.lights[j].power += sign * h
             s.update(scenes.to_rsb(v, meshes=False))
+            v.seed = seed_b
+            s_b.update(scenes.to_rsb(v, meshes=False))
             per = []
             for r in range(reps):
-                a, b = s.film(*crop), s.film(*crop)
+                a, b = s.film(*crop), s_b.film(*crop)
                 a.render(r * spp, half)
                 b.render(r * spp + half, spp - half)
                 per.append(float(np.mean((image(a).astype(np.float64) - target) * (image(b).astype(np.float64) - target))))
