@@ -246,21 +246,26 @@ uint32_t rtg_set_path_capacity(uint32_t scene, uint32_t paths);
  * values[4]: 1 marks the scene's traversal data (tree nodes, leaf triangles) as persisting in L2
  *   for the traversal kernels (an access-policy window on their launches; the process's CUDA
  *   context sets L2 aside for it the first time), so the streamed path state does not evict it.
- * rtg_set_tuning sets the first n values (n <= 5; later ones keep theirs); RTG_STATUS_BAD_SCENE for
- * ray-sort bits above 5. rtg_get_tuning writes the first n (n <= 5). A loaded scene starts at
- * 0, 0, 1, 0, 0. */
+ * values[5]: the tail limit (0: off). From a wave's third round on, a round whose extension queue
+ *   holds at most this many paths runs them, and every later round of the wave, in one launch:
+ *   each thread carries its paths to the end alone (nearest hit, vertex, shadow ray, next ray).
+ *   Scenes with cut-outs or thin walls and batched queue waves keep the wavefront.
+ * rtg_set_tuning sets the first n values (n <= 6; later ones keep theirs); RTG_STATUS_BAD_SCENE for
+ * ray-sort bits above 5. rtg_get_tuning writes the first n (n <= 6). A loaded scene starts at
+ * 0, 0, 1, 0, 0, 0. */
 uint32_t rtg_set_tuning(uint32_t scene, const uint32_t* values, uint32_t n);
 uint32_t rtg_get_tuning(uint32_t scene, uint32_t* values, uint32_t n);
 
-/* No counterpart in the reference: the autotuner. Chooses the scene's tuning (the five values of
+/* No counterpart in the reference: the autotuner. Chooses the scene's tuning (the six values of
  * rtg_set_tuning) by rendering samples [first_sample, first_sample + count) of the rectangle
  * (x, y, w, h) of the image (clipped to it; into a film of its own) under candidate settings, by
  * coordinate descent: the ray sort's bits 0, 3, 4 and 5 (shadow rays sorted along), then shadow
- * rays sorted or not, shading material-sorted or not, the L2 window on or off, then waves of the
- * whole call, a half or a quarter of its paths (at least 2^20). Each candidate renders once to
- * warm up, then once timed with CUDA events on the scene's stream; the scene keeps the fastest.
- * `report` (may be null) receives 6 doubles per candidate tried, at most max_report of them: its
- * five values and its milliseconds; *n_tried (may be null) the number tried. Films are not touched; a render of the
+ * rays sorted or not, shading material-sorted or not, the L2 window on or off, the tail limit 0,
+ * 2^16, 2^18 or 2^20, then waves of the whole call, a half or a quarter of its paths (at least
+ * 2^20). Each candidate renders once to warm up, then once timed with CUDA events on the scene's
+ * stream; the scene keeps the fastest.
+ * `report` (may be null) receives 7 doubles per candidate tried, at most max_report of them: its
+ * six values and its milliseconds; *n_tried (may be null) the number tried. Films are not touched; a render of the
  * candidate is what a call with those samples would cost, so pick a count that is representative
  * of the calls to come. RTG_STATUS_BAD_TILE for an empty rectangle or no samples. */
 uint32_t rtg_autotune(uint32_t scene, uint32_t x, uint32_t y, uint32_t w, uint32_t h, uint32_t first_sample, uint32_t count,

@@ -240,35 +240,37 @@ class Scene:
         _check(lib().rtg_set_path_capacity(self.handle, paths))
 
     def set_tuning(self, ray_bits: int | None = None, shadow_sort: bool | None = None, material_sort: bool | None = None,
-                   capacity: int | None = None, l2_persist: bool | None = None):
+                   capacity: int | None = None, l2_persist: bool | None = None, tail_paths: int | None = None):
         """rtg_set_tuning: how the scene's waves order their rays and paths (None keeps a value)."""
         cur = self.tuning()
         new = [cur["ray_bits"] if ray_bits is None else int(ray_bits),
                cur["shadow_sort"] if shadow_sort is None else int(bool(shadow_sort)),
                cur["material_sort"] if material_sort is None else int(bool(material_sort)),
                cur["capacity"] if capacity is None else int(capacity),
-               cur["l2_persist"] if l2_persist is None else int(bool(l2_persist))]
+               cur["l2_persist"] if l2_persist is None else int(bool(l2_persist)),
+               cur["tail_paths"] if tail_paths is None else int(tail_paths)]
         v = np.array(new, np.uint32)
-        _check(lib().rtg_set_tuning(self.handle, _ptr(v), 5))
+        _check(lib().rtg_set_tuning(self.handle, _ptr(v), 6))
 
     def autotune(self, first: int, count: int, x: int = 0, y: int = 0, w: int | None = None, h: int | None = None) -> dict:
         """rtg_autotune: times candidate tunings on samples [first, first + count) of the rectangle
         (default: the whole image) and keeps the fastest; returns it and every candidate's time."""
         w = self.width if w is None else w
         h = self.height if h is None else h
-        report = np.zeros((16, 6), np.float64)
+        report = np.zeros((24, 7), np.float64)
         n = _u32(0)
-        _check(lib().rtg_autotune(self.handle, x, y, w, h, first, count, _ptr(report), 16, ctypes.byref(n)))
+        _check(lib().rtg_autotune(self.handle, x, y, w, h, first, count, _ptr(report), 24, ctypes.byref(n)))
         tried = [{"ray_bits": int(r[0]), "shadow_sort": int(r[1]), "material_sort": int(r[2]), "capacity": int(r[3]),
-                  "l2_persist": int(r[4]), "ms": float(r[5])} for r in report[:int(n.value)]]
+                  "l2_persist": int(r[4]), "tail_paths": int(r[5]), "ms": float(r[6])} for r in report[:int(n.value)]]
         return {"chosen": self.tuning(), "tried": tried}
 
     def tuning(self) -> dict:
-        """rtg_get_tuning: ray-sort bits, shadow sort, material sort, paths per wave (0: automatic)."""
-        v = np.zeros(5, np.uint32)
-        _check(lib().rtg_get_tuning(self.handle, _ptr(v), 5))
+        """rtg_get_tuning: ray-sort bits, shadow sort, material sort, paths per wave (0: automatic),
+        the L2 window, the tail limit (0: off)."""
+        v = np.zeros(6, np.uint32)
+        _check(lib().rtg_get_tuning(self.handle, _ptr(v), 6))
         return {"ray_bits": int(v[0]), "shadow_sort": int(v[1]), "material_sort": int(v[2]), "capacity": int(v[3]),
-                "l2_persist": int(v[4])}
+                "l2_persist": int(v[4]), "tail_paths": int(v[5])}
 
     def timing(self, enable: bool, reset: bool = False):
         """(extend ms, extend launches, camera+extension rays, shadow rays, kernels launched)

@@ -322,6 +322,8 @@ constexpr size_t SORT_BINS_BYTES = 2 * 2 * (size_t)(8u << (3u * RAY_SORT_MAX_BIT
 // made the extend kernel 4% faster and the frame 3-9% slower (its own passes); rtg_autotune
 // measures it per scene.
 constexpr uint32_t DEFAULT_RAY_BITS = 0, DEFAULT_SHADOW_SORT = 0, DEFAULT_MATERIAL_SORT = 1;
+// The default tail limit (RaySort::tail_paths): 0, the wavefront to the last round.
+constexpr uint32_t DEFAULT_TAIL_PATHS = 0;
 constexpr uint64_t AUTO_MIN_PATHS = 1u << 20;
 constexpr uint64_t PLAIN_JOB_PATHS = 1u << 24;  // a queue job this large runs as plain waves
 constexpr uint64_t MAX_WAVE_PATHS = 0x7fffffffu;
@@ -443,7 +445,7 @@ uint32_t run_wave(Scene& sc, const WaveDesc& w, const FilmDev* film, const Scene
     }
     launch_wave(Sw, lights ? lights : sc.d_lights, w, sc.P, film, sc.stream, grid_for(w.n, 128), t, sc.order);
     RTG_CHECK(cudaGetLastError());
-    sc.launches += wave_launches(Sw, sc.order, sc.P) - ((film || w.segs) ? 0 : 1) + ((w.alb && film && !w.segs) ? 2 : 0);
+    sc.launches += wave_launches(Sw, sc.order, sc.P, w.segs != nullptr) - ((film || w.segs) ? 0 : 1) + ((w.alb && film && !w.segs) ? 2 : 0);
     if (t) {
         RTG_CHECK(cudaStreamSynchronize(sc.stream));
         for (int i = 0; i + 1 < t->ev_count; i += 2) {
@@ -839,6 +841,7 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     sc->order.ray_bits = DEFAULT_RAY_BITS;
     sc->order.shadow_sort = DEFAULT_SHADOW_SORT;
     sc->order.material_sort = DEFAULT_MATERIAL_SORT;
+    sc->order.tail_paths = DEFAULT_TAIL_PATHS;
     set_sort_box(*sc, F);
     g_error.clear();
     for (size_t i = 0; i < g_scenes.size(); ++i)
@@ -1539,6 +1542,7 @@ uint32_t rtg_set_tuning(uint32_t handle, const uint32_t* values, uint32_t n) {
     if (n > 2) o.material_sort = values[2] != 0;
     if (n > 3) cap = values[3] != 0 && values[3] < 1024 ? 1024 : values[3];
     if (n > 4) o.l2_persist = values[4] != 0;
+    if (n > 5) o.tail_paths = values[5];
     // A wave leaves both histograms at zero, but the cursors of fewer bits lie inside the
     // histogram of more: clear them when the key count changes.
     if (o.ray_bits != sc->order.ray_bits && sc->P.rbins) RTG_CHECK(cudaMemsetAsync(sc->P.rbins, 0, SORT_BINS_BYTES, sc->stream));
@@ -1568,11 +1572,12 @@ uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint3
     const uint64_t paths = (x_end - x) * (y_end - y) * (uint64_t)count;
     const bool timing = sc->timing;
     sc->timing = false;
-    struct Cand { uint32_t bits, shadow, msort, cap, l2; };
+    struct Cand { uint32_t bits, shadow, msort, cap, l2, tail; };
     std::vector<std::pair<Cand, double>> tried;
     auto measure = [&](const Cand& c, double& ms) -> uint32_t {
         for (const auto& t : tried)
-            if (t.first.bits == c.bits && t.first.shadow == c.shadow && t.first.msort == c.msort && t.first.cap == c.cap && t.first.l2 == c.l2) {
+            if (t.first.bits == c.bits && t.first.shadow == c.shadow && t.first.msort == c.msort && t.first.cap == c.cap && t.first.l2 == c.l2 &&
+                t.first.tail == c.tail) {
                 ms = t.second;
                 return 0;
             }
@@ -1581,6 +1586,7 @@ uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint3
         sc->order.shadow_sort = c.shadow;
         sc->order.material_sort = c.msort;
         sc->order.l2_persist = c.l2;
+        sc->order.tail_paths = c.tail;
         sc->max_capacity = c.cap;
         refresh_order(*sc);
         uint32_t r = render_region(*sc, tmp.dev.ox, tmp.dev.oy, tmp.dev.w, tmp.dev.h, first_sample, count, tmp.dev, nullptr);  // warm-up
@@ -1596,7 +1602,7 @@ uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint3
         tried.push_back({c, ms});
         return 0;
     };
-    Cand best{sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity, sc->order.l2_persist};
+    Cand best{sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity, sc->order.l2_persist, sc->order.tail_paths};
     double best_ms = 1e300;
     auto consider = [&](const Cand& c) -> uint32_t {
         double ms = 0.0;
@@ -1606,17 +1612,22 @@ uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint3
         return 0;
     };
     // 1. the ray sort's grid (shadow rays sorted with it), 2. shadow rays, 3. material sort, 4. the
-    // L2 window over the traversal data, 5. wave size
+    // L2 window over the traversal data, 5. the tail limit, 6. wave size
+    const uint32_t tail0 = sc->order.tail_paths;
     for (uint32_t bits : {0u, 3u, 4u, 5u})
-        if ((st = consider(Cand{bits, bits > 0 ? 1u : 0u, 1u, 0u, 0u}))) break;
-    if (!st && best.bits > 0) st = consider(Cand{best.bits, 1u - best.shadow, best.msort, best.cap, best.l2});
-    if (!st) st = consider(Cand{best.bits, best.shadow, 1u - best.msort, best.cap, best.l2});
-    if (!st) st = consider(Cand{best.bits, best.shadow, best.msort, best.cap, 1u - best.l2});
+        if ((st = consider(Cand{bits, bits > 0 ? 1u : 0u, 1u, 0u, 0u, tail0}))) break;
+    if (!st && best.bits > 0) st = consider(Cand{best.bits, 1u - best.shadow, best.msort, best.cap, best.l2, best.tail});
+    if (!st) st = consider(Cand{best.bits, best.shadow, 1u - best.msort, best.cap, best.l2, best.tail});
+    if (!st) st = consider(Cand{best.bits, best.shadow, best.msort, best.cap, 1u - best.l2, best.tail});
+    for (uint32_t tail : {0u, 1u << 16, 1u << 18, 1u << 20}) {
+        if (st) break;
+        st = consider(Cand{best.bits, best.shadow, best.msort, best.cap, best.l2, tail});
+    }
     for (uint64_t div : {2u, 4u}) {
         if (st) break;
         const uint64_t cap = paths / div;
         if (cap >= (1u << 20))
-            st = consider(Cand{best.bits, best.shadow, best.msort, (uint32_t)std::min<uint64_t>(cap, MAX_WAVE_PATHS), best.l2});
+            st = consider(Cand{best.bits, best.shadow, best.msort, (uint32_t)std::min<uint64_t>(cap, MAX_WAVE_PATHS), best.l2, best.tail});
     }
     // keep the fastest
     if (best.bits != sc->order.ray_bits && sc->P.rbins) cudaMemsetAsync(sc->P.rbins, 0, SORT_BINS_BYTES, sc->stream);
@@ -1624,14 +1635,15 @@ uint32_t rtg_autotune(uint32_t handle, uint32_t x, uint32_t y, uint32_t w, uint3
     sc->order.shadow_sort = best.shadow;
     sc->order.material_sort = best.msort;
     sc->order.l2_persist = best.l2;
+    sc->order.tail_paths = best.tail;
     sc->max_capacity = best.cap;
     refresh_order(*sc);
     sc->timing = timing;
     if (n_tried) *n_tried = (uint32_t)tried.size();
     for (size_t k = 0; report && k < tried.size() && k < max_report; ++k) {
         const Cand& c = tried[k].first;
-        double* r = report + 6 * k;
-        r[0] = c.bits; r[1] = c.shadow; r[2] = c.msort; r[3] = c.cap; r[4] = c.l2; r[5] = tried[k].second;
+        double* r = report + 7 * k;
+        r[0] = c.bits; r[1] = c.shadow; r[2] = c.msort; r[3] = c.cap; r[4] = c.l2; r[5] = c.tail; r[6] = tried[k].second;
     }
     RTG_CHECK(cudaStreamSynchronize(sc->stream));
     return st;
@@ -1642,8 +1654,9 @@ uint32_t rtg_get_tuning(uint32_t handle, uint32_t* values, uint32_t n) {
     Scene* sc = scene_of(handle);
     if (!sc) return RTG_STATUS_BAD_HANDLE;
     if (!values && n) return RTG_STATUS_NULL_POINTER;
-    const uint32_t v[5] = {sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity, sc->order.l2_persist};
-    for (uint32_t k = 0; k < n && k < 5; ++k) values[k] = v[k];
+    const uint32_t v[6] = {sc->order.ray_bits, sc->order.shadow_sort, sc->order.material_sort, sc->max_capacity, sc->order.l2_persist,
+                           sc->order.tail_paths};
+    for (uint32_t k = 0; k < n && k < 6; ++k) values[k] = v[k];
     return RTG_STATUS_OK;
 }
 

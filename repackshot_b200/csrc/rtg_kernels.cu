@@ -15,6 +15,21 @@ __constant__ SobolTable c_sobol;
 
 // Threads per block of the traversal kernels (the stride of their shared stacks).
 constexpr int TRACE_THREADS = 128;
+// RTG_RAY_AHEAD (build setting): the traversal kernels fetch each lane's next ray one step ahead
+// (1) or when the lane needs it (0). The answers do not depend on it.
+#ifndef RTG_RAY_AHEAD
+#define RTG_RAY_AHEAD 0
+#endif
+// RTG_TRACE_MIN_BLOCKS (build setting): blocks per SM the traversal kernels are compiled for
+// (0: the compiler's choice of registers).
+#ifndef RTG_TRACE_MIN_BLOCKS
+#define RTG_TRACE_MIN_BLOCKS 0
+#endif
+#if RTG_TRACE_MIN_BLOCKS > 0
+#define RTG_TRACE_BOUNDS __launch_bounds__(TRACE_THREADS, RTG_TRACE_MIN_BLOCKS)
+#else
+#define RTG_TRACE_BOUNDS __launch_bounds__(TRACE_THREADS)
+#endif
 // Blocks of 128 threads per SM that the shade kernels are compiled for (their register cap:
 // 65536 / (128 x this)); a build may set it (RTG_SHADE_MIN_BLOCKS) to compare occupancies.
 #ifndef RTG_SHADE_MIN_BLOCKS
@@ -211,7 +226,75 @@ __global__ void k_key_scatter(const uint32_t* __restrict__ list, const uint32_t*
 // (one atomic per warp on counters[4]) while the rest of the warp keeps traversing, so no lane idles
 // until the slowest ray of its warp is done.
 // `order`: the active queue in the order to trace it (P.queue[cur], or its ray-sorted copy).
-__global__ void __launch_bounds__(TRACE_THREADS) k_extend(SceneDev S, PathBuffers P, int cur, const uint32_t* __restrict__ order) {
+#if RTG_RAY_AHEAD
+// The same with each lane's next ray fetched ahead: its list index is claimed and its slot read
+// one step, its ray read the next, and it is taken when the lane's current ray ends. The loads
+// then overlap the warp's traversal steps instead of stalling the warp at every refill.
+__global__ void RTG_TRACE_BOUNDS k_extend(SceneDev S, PathBuffers P, int cur, const uint32_t* __restrict__ order) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const uint32_t n = *(volatile uint32_t*)&P.counters[cur];
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t err = 0, slot = 0;
+    bool busy = false, drained = false;
+    uint32_t ahead = 0, a_slot = 0, a_flags = 0;  // ahead: 0 none, 1 slot being read, 2 ray being read
+    float4 a_o = make_float4(0.0f, 0.0f, 0.0f, 0.0f), a_d = a_o;
+    Trav T;
+    for (;;) {
+        if (!busy && ahead == 2) {
+            slot = a_slot;
+            ahead = 0;
+            busy = !(a_flags & PF_NOTHING) &&
+                   trav_init(S, T, v3(a_o.x, a_o.y, a_o.z), v3(a_d.x, a_d.y, a_d.z), 1.0e-3f, f_inf(), (a_flags & PF_PRIMARY) != 0);
+            if (!busy) {
+                P.hit[slot] = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+                const uint32_t key = material_key(S, false, 0);
+                P.key[slot] = key;
+                warp_count(P.bins, key);
+            }
+        }
+        if (ahead == 1) {
+            a_o = P.o[a_slot];
+            a_d = P.d[a_slot];
+            a_flags = P.flags[a_slot];
+            ahead = 2;
+        }
+        if (!drained) {
+            const uint32_t want = __ballot_sync(0xffffffffu, ahead == 0);
+            if (want) {
+                const int leader = __ffs((int)want) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(&P.counters[4], (uint32_t)__popc(want));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + (uint32_t)__popc(want) >= n) drained = true;
+                const uint32_t i = base + (uint32_t)__popc(want & ((1u << lane) - 1u));
+                if (ahead == 0 && i < n) {
+                    a_slot = order[i];
+                    ahead = 1;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy || ahead != 0)) {
+            if (drained) break;
+            continue;
+        }
+        if (busy) {
+            bool got = false;
+            if (trav_step<false>(S, T, stack, &err, got)) {
+                busy = false;
+                P.hit[slot] = got ? make_uint4(T.best_i, T.best_tri, __float_as_uint(T.best_t), 1u)
+                                  : make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+                const uint32_t key = material_key(S, got, T.best_i);
+                P.key[slot] = key;
+                warp_count(P.bins, key);
+            }
+        }
+    }
+    if (err) atomicOr(&P.counters[3], err);
+}
+#else
+__global__ void RTG_TRACE_BOUNDS k_extend(SceneDev S, PathBuffers P, int cur, const uint32_t* __restrict__ order) {
     __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
     uint64_t deep[STACK_CAP - SHORT_STACK];
     SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
@@ -262,6 +345,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_extend(SceneDev S, PathBuffer
     }
     if (err) atomicOr(&P.counters[3], err);
 }
+#endif
 
 // Exclusive prefix of the key histogram into the scatter cursors; clears the histogram.
 __global__ void k_scan(PathBuffers P) {
@@ -298,9 +382,15 @@ __global__ void k_scatter(PathBuffers P, int cur, const uint32_t* __restrict__ i
 // the path's pixel and sample index (the sampler's key).
 // With P.rbins set, each surviving path's next ray gets its coherence key (in P.key) and is counted
 // in the histogram; with P.sbins set, each shadow ray likewise (in P.sh_key).
+// With `tail` (the tail kernel), the shadow ray goes to *tail instead of the shadow queue and the
+// surviving path to no queue. Returns whether the path goes on.
+struct TailShadow {
+    bool on;
+    float4 o, d, c;
+};
 template <class XYI>
-__device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L, const PathBuffers& P, const RaySort& R, uint32_t slot, int cur,
-                                           XYI xyi, uint32_t& rays_local, uint32_t& shadow_local) {
+__device__ __forceinline__ bool shade_slot(const SceneDev& S, const LightsDev& L, const PathBuffers& P, const RaySort& R, uint32_t slot, int cur,
+                                           XYI xyi, uint32_t& rays_local, uint32_t& shadow_local, TailShadow* tail = nullptr) {
     float4 o4 = P.o[slot], d4 = P.d[slot], thr4 = P.thr[slot], sum = P.sum[slot];
     uint32_t flags = P.flags[slot];
     const uint32_t bounce = (flags & PF_BOUNCE_MASK) >> PF_BOUNCE_SHIFT;
@@ -457,14 +547,24 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
                         floor_blocks = t > 1.0e-3f && t < tmax;
                     }
                     if (finite_c && !floor_blocks) {
-                        uint32_t k = atomicAdd(&P.counters[2], 1u);
-                        P.sh_o[k] = make_float4(from_p.x, from_p.y, from_p.z, tmax);
-                        P.sh_d[k] = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, bounce >= 1 ? 1.0f : 0.0f);  // w: indirect
-                        P.sh_c[k] = make_float4(c.r, c.g, c.b, __uint_as_float(slot));
-                        if (P.sbins) {
-                            const uint32_t sk = ray_key(R, from_p, ls.wi);
-                            P.sh_key[k] = sk;
-                            atomicAdd(&P.sbins[sk], 1u);
+                        const float4 so = make_float4(from_p.x, from_p.y, from_p.z, tmax);
+                        const float4 sd = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, bounce >= 1 ? 1.0f : 0.0f);  // w: indirect
+                        const float4 sc = make_float4(c.r, c.g, c.b, __uint_as_float(slot));
+                        if (tail) {
+                            tail->on = true;
+                            tail->o = so;
+                            tail->d = sd;
+                            tail->c = sc;
+                        } else {
+                            uint32_t k = atomicAdd(&P.counters[2], 1u);
+                            P.sh_o[k] = so;
+                            P.sh_d[k] = sd;
+                            P.sh_c[k] = sc;
+                            if (P.sbins) {
+                                const uint32_t sk = ray_key(R, from_p, ls.wi);
+                                P.sh_key[k] = sk;
+                                atomicAdd(&P.sbins[sk], 1u);
+                            }
                         }
                     }
                 }
@@ -514,7 +614,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
     } while (false);
     P.thr[slot] = make_float4(thr.r, thr.g, thr.b, alpha);
     P.sum[slot] = sum;
-    if (alive) {
+    if (alive && !tail) {
         uint32_t k = atomicAdd(&P.counters[cur ^ 1], 1u);
         P.queue[cur ^ 1][k] = slot;
         if (P.rbins) {
@@ -524,6 +624,7 @@ __device__ __forceinline__ void shade_slot(const SceneDev& S, const LightsDev& L
             atomicAdd(&P.rbins[rk], 1u);
         }
     }
+    return alive;
 }
 
 // BATCH: the slots belong to the jobs of a batched wave, each with its own constants and lights.
@@ -567,7 +668,62 @@ __device__ __forceinline__ void shadow_unblocked(const PathBuffers& P, uint32_t 
 }
 
 // `perm` (may be null): the shadow queue in the order to trace it.
-__global__ void __launch_bounds__(TRACE_THREADS) k_shadow(SceneDev S, PathBuffers P, const uint32_t* __restrict__ perm) {
+#if RTG_RAY_AHEAD
+// With each lane's next shadow ray fetched ahead, as k_extend's.
+__global__ void RTG_TRACE_BOUNDS k_shadow(SceneDev S, PathBuffers P, const uint32_t* __restrict__ perm) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const uint32_t n = *(volatile uint32_t*)&P.counters[2];
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t err = 0, ray = 0;
+    bool busy = false, drained = false;
+    uint32_t ahead = 0, a_ray = 0;  // ahead: 0 none, 1 ray index being read, 2 ray being read
+    float4 a_o = make_float4(0.0f, 0.0f, 0.0f, 0.0f), a_d = a_o;
+    Trav T;
+    for (;;) {
+        if (!busy && ahead == 2) {
+            ray = a_ray;
+            ahead = 0;
+            busy = trav_init(S, T, v3(a_o.x, a_o.y, a_o.z), v3(a_d.x, a_d.y, a_d.z), 1.0e-3f, a_o.w, false);
+            if (!busy) shadow_unblocked(P, ray);
+        }
+        if (ahead == 1) {
+            a_o = P.sh_o[a_ray];
+            a_d = P.sh_d[a_ray];
+            ahead = 2;
+        }
+        if (!drained) {
+            const uint32_t want = __ballot_sync(0xffffffffu, ahead == 0);
+            if (want) {
+                const int leader = __ffs((int)want) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(&P.counters[5], (uint32_t)__popc(want));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + (uint32_t)__popc(want) >= n) drained = true;
+                const uint32_t i = base + (uint32_t)__popc(want & ((1u << lane) - 1u));
+                if (ahead == 0 && i < n) {
+                    a_ray = perm ? perm[i] : i;
+                    ahead = 1;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, busy || ahead != 0)) {
+            if (drained) break;
+            continue;
+        }
+        if (busy) {
+            bool blocked = false;
+            if (trav_step<true>(S, T, stack, &err, blocked)) {
+                busy = false;
+                if (!blocked) shadow_unblocked(P, ray);
+            }
+        }
+    }
+    if (err) atomicOr(&P.counters[3], err);
+}
+#else
+__global__ void RTG_TRACE_BOUNDS k_shadow(SceneDev S, PathBuffers P, const uint32_t* __restrict__ perm) {
     __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
     uint64_t deep[STACK_CAP - SHORT_STACK];
     SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
@@ -608,6 +764,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow(SceneDev S, PathBuffer
     }
     if (err) atomicOr(&P.counters[3], err);
 }
+#endif
 
 // ---- shadow walk: shadow rays through cut-outs and thin walls (integrator/mod.rs:629-690) ------------
 // Nearest hits along the ray: a passable surface multiplies what arrives by its straight
@@ -668,6 +825,64 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow_walk(SceneDev S, PathB
         P.sum[slot] = s4;
     }
     if (err) atomicOr(&P.counters[3], err);
+}
+
+// ---- tail: the last rounds of a wave, a path per thread -----------------------------------------------
+// When the round's extension queue holds at most `limit` paths, each thread carries its share of
+// them through the wave's remaining `rounds_left` rounds alone: the nearest hit (as k_extend), the
+// vertex (shade_slot), the any hit of its shadow ray and its contribution (as k_shadow), the next
+// ray; each path's arithmetic in the order the wavefront gives it, so its sum has the same bits.
+// A wave whose last rounds hold few paths then pays one launch as long as its slowest path instead
+// of a chain of launches, each as long as its slowest ray. k_tail_end then empties the queue, so
+// the later rounds' launches find no work. Scenes with passable surfaces (shadow walks) and
+// batched waves keep the wavefront.
+__global__ void RTG_TRACE_BOUNDS k_tail(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w, uint32_t rounds_left,
+                                        uint32_t limit) {
+    const uint32_t n = *(volatile uint32_t*)&P.counters[cur];
+    if (n == 0 || n > limit) return;
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const uint32_t* __restrict__ queue = P.queue[cur];
+    const RaySort R;  // no coherence keys
+    uint32_t err = 0, rays_local = 0, shadow_local = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = queue[i];
+        for (uint32_t r = 0; r < rounds_left; ++r) {
+            const float4 o = P.o[slot], d = P.d[slot];
+            const uint32_t pf = P.flags[slot];
+            TraceResult res;
+            const bool got = !(pf & PF_NOTHING) &&
+                             traverse<false>(S, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, f_inf(), (pf & PF_PRIMARY) != 0, res, &err, stack);
+            P.hit[slot] = got ? make_uint4(res.inst, res.tri, __float_as_uint(res.t), 1u) : make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+            TailShadow sh;
+            sh.on = false;
+            const bool alive = shade_slot(S, *Lg, P, R, slot, cur, [&](uint32_t& xx, uint32_t& yy, uint32_t& ii) { wave_slot(w, slot, xx, yy, ii); },
+                                          rays_local, shadow_local, &sh);
+            if (sh.on) {
+                TraceResult unused;
+                if (!traverse<true>(S, v3(sh.o.x, sh.o.y, sh.o.z), v3(sh.d.x, sh.d.y, sh.d.z), 1.0e-3f, sh.o.w, false, unused, &err, stack)) {
+                    float4 sum = P.sum[slot];  // shadow_unblocked's addition
+                    sum.x = sum.x + sh.c.x;
+                    sum.y = sum.y + sh.c.y;
+                    sum.z = sum.z + sh.c.z;
+                    P.sum[slot] = sum;
+                }
+            }
+            if (!alive) break;
+        }
+    }
+    uint32_t total = __reduce_add_sync(0xffffffffu, rays_local);
+    uint32_t shadows = __reduce_add_sync(0xffffffffu, shadow_local);
+    if ((threadIdx.x & 31) == 0 && total) atomicAdd(P.rays, (unsigned long long)total);
+    if ((threadIdx.x & 31) == 0 && shadows) atomicAdd(P.rays + 1, (unsigned long long)shadows);
+    if (err) atomicOr(&P.counters[3], err);
+}
+
+// After k_tail: a queue it carried to the end is empty for the rest of the wave.
+__global__ void k_tail_end(PathBuffers P, int cur, uint32_t limit) {
+    const uint32_t n = P.counters[cur];
+    if (n > 0 && n <= limit) P.counters[cur] = 0;
 }
 
 __global__ void k_next_round(PathBuffers P, int cur) {
@@ -1151,17 +1366,22 @@ static void launch_traversal(const RaySort& order, int grid, cudaStream_t st, vo
     cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P) {
+// Whether a wave's last rounds run in k_tail: a limit set, no shadow walks, not batched.
+static bool tail_on(const SceneDev& S, const RaySort& order, bool batch) { return order.tail_paths > 0 && !S.any_passable && !batch; }
+
+uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P, bool batch) {
     const uint32_t rounds = wave_rounds(S);
     const bool rsort = order.ray_bits > 0 && P.rbins, ssort = rsort && order.shadow_sort && P.sbins;
     uint32_t per_round = 5 + (order.material_sort ? 1u : 0u) + (ssort ? 2u : 0u);
-    return 2 + rounds * per_round + (rsort && rounds > 1 ? 2u * (rounds - 1u) : 0u);
+    const uint32_t tail = tail_on(S, order, batch) && rounds > TAIL_FIRST_ROUND ? 2u * (rounds - TAIL_FIRST_ROUND) : 0u;
+    return 2 + rounds * per_round + (rsort && rounds > 1 ? 2u * (rounds - 1u) : 0u) + tail;
 }
 
 void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const FilmDev* film, cudaStream_t st,
                  int grid, WaveTiming* timing, const RaySort& order) {
     static const int ext_resident = resident_blocks((const void*)k_extend, TRACE_THREADS);
     static const int sh_resident = resident_blocks((const void*)k_shadow, TRACE_THREADS);
+    static const int tail_resident = resident_blocks((const void*)k_tail, TRACE_THREADS);
     const int g = grid;
     const int g_ext = ext_resident > 0 && ext_resident < g ? ext_resident : g;
     const int g_sh = sh_resident > 0 && sh_resident < g ? sh_resident : g;
@@ -1173,7 +1393,12 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
     else k_camera<false><<<g, 256, 0, st>>>(S, w, P);
     int cur = 0;
     const uint32_t rounds = wave_rounds(S);
+    const bool tail = tail_on(S, order, batch);
     for (uint32_t round = 0; round < rounds; ++round) {
+        if (tail && round >= TAIL_FIRST_ROUND) {
+            k_tail<<<tail_resident > 0 ? tail_resident : g, TRACE_THREADS, 0, st>>>(S, L, P, cur, w, rounds - round, order.tail_paths);
+            k_tail_end<<<1, 1, 0, st>>>(P, cur, order.tail_paths);
+        }
         // The camera rays are traced in pixel order; later rounds' rays in coherence order.
         const uint32_t* traced = P.queue[cur];
         if (rsort && round > 0) {

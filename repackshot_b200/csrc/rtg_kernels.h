@@ -106,7 +106,11 @@ struct RaySort {
     const void* l2_base = nullptr;
     size_t l2_bytes = 0;
     float l2_hit_ratio = 0.0f;
+    // tail_paths > 0: from round TAIL_FIRST_ROUND on, a round whose extension queue holds at most
+    // tail_paths paths and every later round run in one launch, a path per thread (k_tail).
+    uint32_t tail_paths = 0;
 };
+constexpr uint32_t TAIL_FIRST_ROUND = 2;
 constexpr uint32_t RAY_SORT_MAX_BITS = 5;
 inline uint32_t ray_sort_keys(uint32_t bits) { return 8u << (3u * bits); }
 
@@ -163,7 +167,7 @@ void set_sobol(const SobolTable& t, cudaStream_t s);
 void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const PathBuffers& P, const FilmDev* film, cudaStream_t st,
                  int grid, WaveTiming* timing, const RaySort& order = RaySort());
 // Kernel launches of one launch_wave with a film (camera and accumulate included, guides not).
-uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P);
+uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P, bool batch);
 // The adjoint: loss and per-pixel path derivatives of a film against a target (w*h*3 floats on
 // the device), then the backward wave: the replay of the wave that rendered the film.
 void launch_adjoint_delta(const FilmDev& F, const float* target, float4* dpath, double* loss, const PathBuffers& P, uint32_t count, cudaStream_t st,

@@ -77,6 +77,14 @@ RTG_D bool watertight(const PRay& r, const float* v0, const float* v1, const flo
 RTG_D float smax_(float a, float b) { return a > b ? a : b; }
 RTG_D float smin_(float a, float b) { return a < b ? a : b; }
 
+// A plane of a quantised box: p + q s for the byte q (byte k of `word`) and the power of two s.
+// q s is exact, so the one rounding of the fused form is the sum's: the bits of p + q * s. The
+// byte becomes a float as 2^23 + q (a byte permute into 0x4b0000qq) minus 2^23, both exact.
+RTG_D float qplane(uint32_t word, int k, float s, float p) {
+    const float q = __uint_as_float(__byte_perm(word, 0x4b000000u, 0x7540u | (uint32_t)k)) - 8388608.0f;
+    return __fmaf_rn(q, s, p);
+}
+
 // Slab test of the eight children of a quantised node; returns the hit mask and entry distances.
 RTG_D uint32_t node_test(const QNode* __restrict__ node, const PRay& r, float tmax, float nr[8], uint32_t child[8]) {
     const float4* q = reinterpret_cast<const float4*>(node);
@@ -86,28 +94,34 @@ RTG_D uint32_t node_test(const QNode* __restrict__ node, const PRay& r, float tm
     float sx = __uint_as_float((meta & 0xffu) << 23);
     float sy = __uint_as_float(((meta >> 8) & 0xffu) << 23);
     float sz = __uint_as_float(((meta >> 16) & 0xffu) << 23);
-    // qlo x,y,z then qhi x,y,z: 8 bytes each = two words each.
-    uint32_t qw[12] = {__float_as_uint(w1.x), __float_as_uint(w1.y), __float_as_uint(w1.z), __float_as_uint(w1.w),
-                       __float_as_uint(w2.x), __float_as_uint(w2.y), __float_as_uint(w2.z), __float_as_uint(w2.w),
-                       __float_as_uint(w3.x), __float_as_uint(w3.y), __float_as_uint(w3.z), __float_as_uint(w3.w)};
+    // qlo x,y,z then qhi x,y,z: 8 bytes each = two words each. The near and far planes of each
+    // axis are the low and high ones, swapped where the ray runs towards -axis: chosen here once
+    // per node, word by word.
+    const uint32_t lo[6] = {__float_as_uint(w1.x), __float_as_uint(w1.y), __float_as_uint(w1.z), __float_as_uint(w1.w),
+                            __float_as_uint(w2.x), __float_as_uint(w2.y)};
+    const uint32_t hi[6] = {__float_as_uint(w2.z), __float_as_uint(w2.w), __float_as_uint(w3.x), __float_as_uint(w3.y),
+                            __float_as_uint(w3.z), __float_as_uint(w3.w)};
+    uint32_t nw[6], fw[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const bool neg = r.neg[a];
+        nw[2 * a] = neg ? hi[2 * a] : lo[2 * a];
+        nw[2 * a + 1] = neg ? hi[2 * a + 1] : lo[2 * a + 1];
+        fw[2 * a] = neg ? lo[2 * a] : hi[2 * a];
+        fw[2 * a + 1] = neg ? lo[2 * a + 1] : hi[2 * a + 1];
+    }
     child[0] = __float_as_uint(w4.x); child[1] = __float_as_uint(w4.y); child[2] = __float_as_uint(w4.z); child[3] = __float_as_uint(w4.w);
     child[4] = __float_as_uint(w5.x); child[5] = __float_as_uint(w5.y); child[6] = __float_as_uint(w5.z); child[7] = __float_as_uint(w5.w);
     uint32_t bits = 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        int word = c >> 2, sh = (c & 3) * 8;
-        float lx = px + (float)((qw[0 + word] >> sh) & 0xffu) * sx;
-        float ly = py + (float)((qw[2 + word] >> sh) & 0xffu) * sy;
-        float lz = pz + (float)((qw[4 + word] >> sh) & 0xffu) * sz;
-        float hx = px + (float)((qw[6 + word] >> sh) & 0xffu) * sx;
-        float hy = py + (float)((qw[8 + word] >> sh) & 0xffu) * sy;
-        float hz = pz + (float)((qw[10 + word] >> sh) & 0xffu) * sz;
-        float tx0 = ((r.neg[0] ? hx : lx) - r.org[0]) * r.inv[0];
-        float ty0 = ((r.neg[1] ? hy : ly) - r.org[1]) * r.inv[1];
-        float tz0 = ((r.neg[2] ? hz : lz) - r.org[2]) * r.inv[2];
-        float tx1 = ((r.neg[0] ? lx : hx) - r.org[0]) * r.inv[0];
-        float ty1 = ((r.neg[1] ? ly : hy) - r.org[1]) * r.inv[1];
-        float tz1 = ((r.neg[2] ? lz : hz) - r.org[2]) * r.inv[2];
+        const int word = c >> 2, k = c & 3;
+        float tx0 = (qplane(nw[0 + word], k, sx, px) - r.org[0]) * r.inv[0];
+        float ty0 = (qplane(nw[2 + word], k, sy, py) - r.org[1]) * r.inv[1];
+        float tz0 = (qplane(nw[4 + word], k, sz, pz) - r.org[2]) * r.inv[2];
+        float tx1 = (qplane(fw[0 + word], k, sx, px) - r.org[0]) * r.inv[0];
+        float ty1 = (qplane(fw[2 + word], k, sy, py) - r.org[1]) * r.inv[1];
+        float tz1 = (qplane(fw[4 + word], k, sz, pz) - r.org[2]) * r.inv[2];
         float n = smax_(tz0, smax_(ty0, smax_(tx0, r.tmin)));
         float f = smin_(tz1, smin_(ty1, smin_(tx1, tmax))) * RTG_ROBUST;
         nr[c] = n;
