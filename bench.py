@@ -434,7 +434,7 @@ def adjoint_comparison(rtg, dist, world, iterations):
         f.render(i * SPP, SPP)
         s.synchronize()
         fwd.append(time.perf_counter() - t0)
-    F = fit.Fit(s, base, target, SPP, lr=0.02)
+    F = fit.Fit(s, base, target, SPP, lr=0.02, decay=0.985)
     F.step()  # warm-up (allocations)
     t0 = time.perf_counter()
     for _ in range(iterations):
@@ -443,6 +443,9 @@ def adjoint_comparison(rtg, dist, world, iterations):
     t_fit = shards.max_over_ranks(time.perf_counter() - t0, dist)
     t_fwd = shards.max_over_ranks(statistics.median(fwd), dist)
     want = np.array([l.power for l in tgt.lights])
+    want_c = np.array([m.base_color for m in tgt.materials[:16]])
+    want_a = np.array([m.roughness ** 2 for m in tgt.materials[:16]])
+    cols, alphas, powers = F.params()
     return {"workload": "differentiable render: small-scene icosphere split into 16 instances with the product "
                         "material table (16 base colours, 16 GGX alphas in 0.05-0.8), 3 rect lights, 512x512, 32 spp, "
                         "depth 6; target at parameters perturbed by U(0.8, 1.2) (PCG32 seed 3), 512 spp",
@@ -450,7 +453,13 @@ def adjoint_comparison(rtg, dist, world, iterations):
             "adjoint_over_forward": (t_fit / iterations) / t_fwd, "iterations": iterations,
             "loss_first": F.state.losses[0], "loss_last": F.state.losses[-1],
             "light_power_error_first": float(np.abs(np.array([l.power for l in base.lights]) - want).sum()),
-            "light_power_error_last": float(np.abs(F.params()[2] - want).sum()),
+            "light_power_error_last": float(np.abs(powers - want).sum()),
+            "colour_error_first": float(np.abs(np.array([m.base_color for m in base.materials[:16]]) - want_c).mean()),
+            "colour_error_last": float(np.abs(cols - want_c).mean()),
+            "alpha_error_first": float(np.abs(np.array([m.roughness ** 2 for m in base.materials[:16]]) - want_a).mean()),
+            "alpha_error_last": float(np.abs(alphas - want_a).mean()),
+            "errors": "light power: sum over the 3 lights of |power - target power| (W); colour and alpha: mean over the "
+                      "16 materials (and channels) of |value - target value|",
             "iteration": "rtg_scene_update (parameters) + rtg_render_adjoint (forward wave, loss, backward wave) + Adam step"}
 
 

@@ -252,7 +252,7 @@ uint32_t rtg_set_path_capacity(uint32_t scene, uint32_t paths);
  *   Scenes with cut-outs or thin walls and batched queue waves keep the wavefront.
  * rtg_set_tuning sets the first n values (n <= 6; later ones keep theirs); RTG_STATUS_BAD_SCENE for
  * ray-sort bits above 5. rtg_get_tuning writes the first n (n <= 6). A loaded scene starts at
- * 0, 0, 1, 0, 0, 0. */
+ * 0, 0, 1, 0, 0, 16384. */
 uint32_t rtg_set_tuning(uint32_t scene, const uint32_t* values, uint32_t n);
 uint32_t rtg_get_tuning(uint32_t scene, uint32_t* values, uint32_t n);
 

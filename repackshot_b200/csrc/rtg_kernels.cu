@@ -15,11 +15,6 @@ __constant__ SobolTable c_sobol;
 
 // Threads per block of the traversal kernels (the stride of their shared stacks).
 constexpr int TRACE_THREADS = 128;
-// RTG_RAY_AHEAD (build setting): the traversal kernels fetch each lane's next ray one step ahead
-// (1) or when the lane needs it (0). The answers do not depend on it.
-#ifndef RTG_RAY_AHEAD
-#define RTG_RAY_AHEAD 0
-#endif
 // RTG_TRACE_MIN_BLOCKS (build setting): blocks per SM the traversal kernels are compiled for
 // (0: the compiler's choice of registers).
 #ifndef RTG_TRACE_MIN_BLOCKS
@@ -226,74 +221,6 @@ __global__ void k_key_scatter(const uint32_t* __restrict__ list, const uint32_t*
 // (one atomic per warp on counters[4]) while the rest of the warp keeps traversing, so no lane idles
 // until the slowest ray of its warp is done.
 // `order`: the active queue in the order to trace it (P.queue[cur], or its ray-sorted copy).
-#if RTG_RAY_AHEAD
-// The same with each lane's next ray fetched ahead: its list index is claimed and its slot read
-// one step, its ray read the next, and it is taken when the lane's current ray ends. The loads
-// then overlap the warp's traversal steps instead of stalling the warp at every refill.
-__global__ void RTG_TRACE_BOUNDS k_extend(SceneDev S, PathBuffers P, int cur, const uint32_t* __restrict__ order) {
-    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
-    uint64_t deep[STACK_CAP - SHORT_STACK];
-    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
-    const uint32_t n = *(volatile uint32_t*)&P.counters[cur];
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t err = 0, slot = 0;
-    bool busy = false, drained = false;
-    uint32_t ahead = 0, a_slot = 0, a_flags = 0;  // ahead: 0 none, 1 slot being read, 2 ray being read
-    float4 a_o = make_float4(0.0f, 0.0f, 0.0f, 0.0f), a_d = a_o;
-    Trav T;
-    for (;;) {
-        if (!busy && ahead == 2) {
-            slot = a_slot;
-            ahead = 0;
-            busy = !(a_flags & PF_NOTHING) &&
-                   trav_init(S, T, v3(a_o.x, a_o.y, a_o.z), v3(a_d.x, a_d.y, a_d.z), 1.0e-3f, f_inf(), (a_flags & PF_PRIMARY) != 0);
-            if (!busy) {
-                P.hit[slot] = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
-                const uint32_t key = material_key(S, false, 0);
-                P.key[slot] = key;
-                warp_count(P.bins, key);
-            }
-        }
-        if (ahead == 1) {
-            a_o = P.o[a_slot];
-            a_d = P.d[a_slot];
-            a_flags = P.flags[a_slot];
-            ahead = 2;
-        }
-        if (!drained) {
-            const uint32_t want = __ballot_sync(0xffffffffu, ahead == 0);
-            if (want) {
-                const int leader = __ffs((int)want) - 1;
-                uint32_t base = 0;
-                if ((int)lane == leader) base = atomicAdd(&P.counters[4], (uint32_t)__popc(want));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (base + (uint32_t)__popc(want) >= n) drained = true;
-                const uint32_t i = base + (uint32_t)__popc(want & ((1u << lane) - 1u));
-                if (ahead == 0 && i < n) {
-                    a_slot = order[i];
-                    ahead = 1;
-                }
-            }
-        }
-        if (!__any_sync(0xffffffffu, busy || ahead != 0)) {
-            if (drained) break;
-            continue;
-        }
-        if (busy) {
-            bool got = false;
-            if (trav_step<false>(S, T, stack, &err, got)) {
-                busy = false;
-                P.hit[slot] = got ? make_uint4(T.best_i, T.best_tri, __float_as_uint(T.best_t), 1u)
-                                  : make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
-                const uint32_t key = material_key(S, got, T.best_i);
-                P.key[slot] = key;
-                warp_count(P.bins, key);
-            }
-        }
-    }
-    if (err) atomicOr(&P.counters[3], err);
-}
-#else
 __global__ void RTG_TRACE_BOUNDS k_extend(SceneDev S, PathBuffers P, int cur, const uint32_t* __restrict__ order) {
     __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
     uint64_t deep[STACK_CAP - SHORT_STACK];
@@ -345,7 +272,6 @@ __global__ void RTG_TRACE_BOUNDS k_extend(SceneDev S, PathBuffers P, int cur, co
     }
     if (err) atomicOr(&P.counters[3], err);
 }
-#endif
 
 // Exclusive prefix of the key histogram into the scatter cursors; clears the histogram.
 __global__ void k_scan(PathBuffers P) {
@@ -668,61 +594,6 @@ __device__ __forceinline__ void shadow_unblocked(const PathBuffers& P, uint32_t 
 }
 
 // `perm` (may be null): the shadow queue in the order to trace it.
-#if RTG_RAY_AHEAD
-// With each lane's next shadow ray fetched ahead, as k_extend's.
-__global__ void RTG_TRACE_BOUNDS k_shadow(SceneDev S, PathBuffers P, const uint32_t* __restrict__ perm) {
-    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
-    uint64_t deep[STACK_CAP - SHORT_STACK];
-    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
-    const uint32_t n = *(volatile uint32_t*)&P.counters[2];
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t err = 0, ray = 0;
-    bool busy = false, drained = false;
-    uint32_t ahead = 0, a_ray = 0;  // ahead: 0 none, 1 ray index being read, 2 ray being read
-    float4 a_o = make_float4(0.0f, 0.0f, 0.0f, 0.0f), a_d = a_o;
-    Trav T;
-    for (;;) {
-        if (!busy && ahead == 2) {
-            ray = a_ray;
-            ahead = 0;
-            busy = trav_init(S, T, v3(a_o.x, a_o.y, a_o.z), v3(a_d.x, a_d.y, a_d.z), 1.0e-3f, a_o.w, false);
-            if (!busy) shadow_unblocked(P, ray);
-        }
-        if (ahead == 1) {
-            a_o = P.sh_o[a_ray];
-            a_d = P.sh_d[a_ray];
-            ahead = 2;
-        }
-        if (!drained) {
-            const uint32_t want = __ballot_sync(0xffffffffu, ahead == 0);
-            if (want) {
-                const int leader = __ffs((int)want) - 1;
-                uint32_t base = 0;
-                if ((int)lane == leader) base = atomicAdd(&P.counters[5], (uint32_t)__popc(want));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (base + (uint32_t)__popc(want) >= n) drained = true;
-                const uint32_t i = base + (uint32_t)__popc(want & ((1u << lane) - 1u));
-                if (ahead == 0 && i < n) {
-                    a_ray = perm ? perm[i] : i;
-                    ahead = 1;
-                }
-            }
-        }
-        if (!__any_sync(0xffffffffu, busy || ahead != 0)) {
-            if (drained) break;
-            continue;
-        }
-        if (busy) {
-            bool blocked = false;
-            if (trav_step<true>(S, T, stack, &err, blocked)) {
-                busy = false;
-                if (!blocked) shadow_unblocked(P, ray);
-            }
-        }
-    }
-    if (err) atomicOr(&P.counters[3], err);
-}
-#else
 __global__ void RTG_TRACE_BOUNDS k_shadow(SceneDev S, PathBuffers P, const uint32_t* __restrict__ perm) {
     __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
     uint64_t deep[STACK_CAP - SHORT_STACK];
@@ -764,7 +635,6 @@ __global__ void RTG_TRACE_BOUNDS k_shadow(SceneDev S, PathBuffers P, const uint3
     }
     if (err) atomicOr(&P.counters[3], err);
 }
-#endif
 
 // ---- shadow walk: shadow rays through cut-outs and thin walls (integrator/mod.rs:629-690) ------------
 // Nearest hits along the ray: a passable surface multiplies what arrives by its straight
@@ -836,7 +706,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow_walk(SceneDev S, PathB
 // of a chain of launches, each as long as its slowest ray. k_tail_end then empties the queue, so
 // the later rounds' launches find no work. Scenes with passable surfaces (shadow walks) and
 // batched waves keep the wavefront.
-__global__ void RTG_TRACE_BOUNDS k_tail(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w, uint32_t rounds_left,
+__global__ void __launch_bounds__(TRACE_THREADS) k_tail(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w, uint32_t rounds_left,
                                         uint32_t limit) {
     const uint32_t n = *(volatile uint32_t*)&P.counters[cur];
     if (n == 0 || n > limit) return;
