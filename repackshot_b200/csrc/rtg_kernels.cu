@@ -15,10 +15,13 @@ __constant__ SobolTable c_sobol;
 
 // Threads per block of the traversal kernels (the stride of their shared stacks).
 constexpr int TRACE_THREADS = 128;
-// RTG_TRACE_MIN_BLOCKS (build setting): blocks per SM the traversal kernels are compiled for
-// (0: the compiler's choice of registers).
+// RTG_TRACE_MIN_BLOCKS (build setting): blocks per SM the traversal kernels (k_extend, k_shadow)
+// are compiled for (0: the compiler's choice of registers, 76). At 8 (64 registers, no spills in
+// k_extend, 40 bytes in k_shadow) the 1080p product frame's extend time fell from 163 to 145 ms
+// and the frame from 349 to 327 ms: more warps hide the node fetches. 7 and 9 blocks measured
+// 337-338 ms, 10 blocks 350 ms.
 #ifndef RTG_TRACE_MIN_BLOCKS
-#define RTG_TRACE_MIN_BLOCKS 0
+#define RTG_TRACE_MIN_BLOCKS 8
 #endif
 #if RTG_TRACE_MIN_BLOCKS > 0
 #define RTG_TRACE_BOUNDS __launch_bounds__(TRACE_THREADS, RTG_TRACE_MIN_BLOCKS)

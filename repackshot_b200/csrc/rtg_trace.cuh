@@ -156,9 +156,11 @@ struct FlatStack {
 // (entry k of thread i at sm[k * stride + i]), and the deeper ones in a per-thread array. Almost
 // every ray stays within the shared part.
 // A build may set RTG_SHORT_STACK to trade shared memory (8 bytes x 128 threads per entry and
-// block) against spills to the deeper part.
+// block) against spills to the deeper part. 16 entries (16 KB a block) leave 128 KB of the SM's
+// shared memory to L1 at 8 blocks per SM, where the node fetches hit; on the 1080p product frame
+// 12, 16 and 20 entries measured within 1% of each other, 24 entries 3% slower.
 #ifndef RTG_SHORT_STACK
-#define RTG_SHORT_STACK 24
+#define RTG_SHORT_STACK 16
 #endif
 constexpr int SHORT_STACK = RTG_SHORT_STACK;
 struct SplitStack {
