@@ -259,11 +259,12 @@ uint32_t rtg_get_tuning(uint32_t scene, uint32_t* values, uint32_t n);
 /* No counterpart in the reference: the autotuner. Chooses the scene's tuning (the six values of
  * rtg_set_tuning) by rendering samples [first_sample, first_sample + count) of the rectangle
  * (x, y, w, h) of the image (clipped to it; into a film of its own) under candidate settings, by
- * coordinate descent: the ray sort's bits 0, 3, 4 and 5 (shadow rays sorted along), then shadow
- * rays sorted or not, shading material-sorted or not, the L2 window on or off, the tail limit 0,
- * 2^16, 2^18 or 2^20, then waves of the whole call, a half or a quarter of its paths (at least
- * 2^20). Each candidate renders once to warm up, then once timed with CUDA events on the scene's
- * stream; the scene keeps the fastest.
+ * coordinate descent from the scene's own tuning: the ray sort's bits 0, 3, 4 and 5 (shadow rays
+ * sorted along), then shadow rays sorted or not, shading material-sorted or not, the L2 window on
+ * or off, the tail limit 0, 2^16, 2^18 or 2^20, then waves of the whole call, a half or a quarter
+ * of its paths (at least 2^20). Each candidate renders once to warm up, then three times timed
+ * with CUDA events on the scene's stream; its median counts, and a candidate replaces the fastest
+ * so far only when it is more than 1% faster. The scene keeps the fastest.
  * `report` (may be null) receives 7 doubles per candidate tried, at most max_report of them: its
  * six values and its milliseconds; *n_tried (may be null) the number tried. Films are not touched; a render of the
  * candidate is what a call with those samples would cost, so pick a count that is representative

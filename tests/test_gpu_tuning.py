@@ -59,8 +59,12 @@ def test_autotuner_keeps_the_fastest_and_the_bits(rtg, small_product_rsb):
     out = s.autotune(0, 4)
     tried = out["tried"]
     assert len(tried) >= 7
-    fastest = min(tried, key=lambda t: t["ms"])
-    assert out["chosen"] == {k: fastest[k] for k in ("ray_bits", "shadow_sort", "material_sort", "capacity", "l2_persist", "tail_paths")}
+    # The chosen tuning was tried, and no candidate was more than 1% faster (a candidate must beat
+    # the best so far by more than 1% to replace it).
+    keys = ("ray_bits", "shadow_sort", "material_sort", "capacity", "l2_persist", "tail_paths")
+    chosen = [t for t in tried if {k: t[k] for k in keys} == out["chosen"]]
+    assert len(chosen) == 1
+    assert chosen[0]["ms"] <= min(t["ms"] for t in tried) / 0.99 + 1e-9
     f = s.film()
     f.render(0, 8)
     for a, b in zip(bits(f), bits(ref)):
