@@ -82,6 +82,7 @@ struct Scene {
     DevBuf alb_mem;  // one float4 a path slot: the albedo of renders that fill a film's guides
     uint64_t edge_builds = 0;  // masks built so far: what depends on the mask checks it
     cudaStream_t stream = nullptr;
+    int device = -1;  // the CUDA device the scene was loaded on
     // path buffers
     PathBuffers P{};
     DevBuf path_mem;
@@ -338,10 +339,29 @@ constexpr uint64_t MAX_WAVE_PATHS = 0x7fffffffu;
 // The L2 set-aside for persisting accesses this library asked for (0: none), per device.
 size_t g_l2_set_aside[64] = {};
 
+// Whether a scene on device `dev` other than `self` has the L2 window on.
+bool other_window_on(int dev, const Scene* self) {
+    for (const auto& s : g_scenes)
+        if (s && s.get() != self && s->device == dev && s->order.l2_persist) return true;
+    return false;
+}
+// Gives the set-aside back when no scene on `dev` has the window on any longer: L2 set aside for
+// persisting lines is not all normal accesses' again until the limit returns to 0 (the 1080p frame
+// ran 9% slower after the window had been on once).
+void release_set_aside(int dev, const Scene* self) {
+    if (dev < 0 || dev >= 64 || g_l2_set_aside[dev] == 0 || other_window_on(dev, self)) return;
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != dev) return;
+    cudaCtxResetPersistingL2Cache();
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0) == cudaSuccess) g_l2_set_aside[dev] = 0;
+    cudaGetLastError();
+}
+
 // The ray sort's grid over the scene's sort box at the current bits per axis, and the L2 window
 // over its traversal data: at most the device's largest window, persisting for the share of it
-// the set-aside holds. The set-aside is asked for when a scene first turns the window on; it is
-// a limit of this process's CUDA context and ends with it.
+// the set-aside holds. The set-aside is asked for when a scene turns the window on, and given back
+// when the last scene on the device turns it off or is freed; it is a limit of this process's
+// CUDA context.
 void refresh_order(Scene& sc) {
     int dev = 0, max_window = 0, max_persist = 0;
     size_t aside = 0;
@@ -352,6 +372,7 @@ void refresh_order(Scene& sc) {
         if (want > g_l2_set_aside[dev] && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess)
             g_l2_set_aside[dev] = want;
         cudaGetLastError();
+        if (!sc.order.l2_persist) release_set_aside(dev, &sc);
         aside = g_l2_set_aside[dev];
     }
     sc.order.l2_base = sc.S.nodes;
@@ -825,6 +846,7 @@ uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     if (device_init() != RTG_STATUS_OK) return 0;
     auto sc = std::make_unique<Scene>();
     if (cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking) != cudaSuccess) { g_error = "cudaStreamCreate failed"; return 0; }
+    if (cudaGetDevice(&sc->device) != cudaSuccess) sc->device = -1;
     SceneDev geom = F.scene, shade = F.scene;
     if (upload_geometry(F, sc->geometry, geom, &sc->hot_bytes) || upload_shading(F, sc->shading, shade)) return 0;
     sc->S = compose(F.scene, geom, shade);
@@ -921,8 +943,12 @@ void rtg_scene_error_copy(uint8_t* out) {
 uint32_t rtg_scene_free(uint32_t handle) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!scene_of(handle)) return RTG_STATUS_BAD_HANDLE;
-    cudaStreamSynchronize(g_scenes[handle - 1]->stream);
+    Scene* sc = g_scenes[handle - 1].get();
+    cudaStreamSynchronize(sc->stream);
+    const int dev = sc->device;
+    const bool window = sc->order.l2_persist != 0;
     g_scenes[handle - 1].reset();
+    if (window) release_set_aside(dev, nullptr);
     return RTG_STATUS_OK;
 }
 
