@@ -85,12 +85,6 @@ RTG_D float qplane(uint32_t word, int k, float s, float p) {
     return __fmaf_rn(q, s, p);
 }
 
-// RTG_NODE_NMAX (build setting): 1 tests a node's children only up to the most any active lane's
-// node has (a warp-uniform bound: the slots past a node's own children are empty and never hit).
-#ifndef RTG_NODE_NMAX
-#define RTG_NODE_NMAX 0
-#endif
-
 // Slab test of the eight children of a quantised node; returns the hit mask and entry distances.
 RTG_D uint32_t node_test(const QNode* __restrict__ node, const PRay& r, float tmax, float nr[8], uint32_t child[8]) {
     const float4* q = reinterpret_cast<const float4*>(node);
@@ -119,16 +113,8 @@ RTG_D uint32_t node_test(const QNode* __restrict__ node, const PRay& r, float tm
     child[0] = __float_as_uint(w4.x); child[1] = __float_as_uint(w4.y); child[2] = __float_as_uint(w4.z); child[3] = __float_as_uint(w4.w);
     child[4] = __float_as_uint(w5.x); child[5] = __float_as_uint(w5.y); child[6] = __float_as_uint(w5.z); child[7] = __float_as_uint(w5.w);
     uint32_t bits = 0;
-#if RTG_NODE_NMAX
-    const uint32_t nmax = __reduce_max_sync(__activemask(), meta >> 24);
-#pragma unroll
-    for (int c = 0; c < 8; ++c) nr[c] = 0.0f;
-#endif
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-#if RTG_NODE_NMAX
-        if ((uint32_t)c >= nmax) break;
-#endif
         const int word = c >> 2, k = c & 3;
         float tx0 = (qplane(nw[0 + word], k, sx, px) - r.org[0]) * r.inv[0];
         float ty0 = (qplane(nw[2 + word], k, sy, py) - r.org[1]) * r.inv[1];
