@@ -219,12 +219,6 @@ RTG_D bool trav_init(const SceneDev& S, Trav& T, V3 o, V3 d, float tmin, float t
     return true;
 }
 
-// RTG_ANY_NEAREST (build setting): 1 visits an any-hit query's children nearest first, as the
-// nearest-hit query does (0: in slot order). The answer does not depend on it.
-#ifndef RTG_ANY_NEAREST
-#define RTG_ANY_NEAREST 0
-#endif
-
 // One step of the two-level traversal: the slab test of one node, or the triangles of one leaf,
 // then the next node (a child, or the nearest entry of the stack that is still in range).
 // `ANY`: stop at the first hit in [t_min, t_max] (shadow rays; children in slot order). Otherwise
@@ -250,7 +244,7 @@ RTG_D bool trav_step(const SceneDev& S, Trav& T, Stack& stack, uint32_t* err, bo
                 return false;
             }
             if (T.sp + 8 > STACK_CAP) { *err |= 1u; hit = false; return true; }
-            if (ANY && !RTG_ANY_NEAREST) {
+            if (ANY) {
                 // Slot order: the lowest slot next, the others pushed lowest first.
                 const uint32_t first = bits & (0u - bits);
 #pragma unroll
