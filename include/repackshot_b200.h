@@ -110,7 +110,7 @@ uint32_t rtg_render_progressive(uint32_t scene, uint32_t film, uint32_t first_sa
  * error in the middle of a frame. (The scene and the film are allocated when they are created,
  * as before; only the per-wave path state differs.)
  *
- * The path state lives in one fixed array of RTG_NOALLOC_SCRATCH_BYTES (14 MiB) in the
+ * The path state lives in one fixed array of RTG_NOALLOC_SCRATCH_BYTES (12 MiB) in the
  * library's device code. Every GPU that loads the library holds that array until the process
  * exits, whether or not this function is called. A wave holds at most RTG_NOALLOC_MAX_PATHS
  * paths, so the film is rendered in bands of rows and waves of samples that fit; any film of a
@@ -134,7 +134,7 @@ uint32_t rtg_render_progressive(uint32_t scene, uint32_t film, uint32_t first_sa
  * are the same, and so are its guide sums when the film has fused guides
  * (rtg_film_guides_fused): the first hits' albedo goes through a slice of the same array. Extend-kernel timing (rtg_timing) counts its rays and launches but brackets no
  * launch with events. */
-#define RTG_NOALLOC_SCRATCH_BYTES (14ull << 20)
+#define RTG_NOALLOC_SCRATCH_BYTES (12ull << 20)
 #define RTG_NOALLOC_MAX_PATHS 65536u
 uint32_t rtg_render_progressive_noalloc(uint32_t scene, uint32_t film, uint32_t first_sample, uint32_t count,
                                         uint64_t* rays);
@@ -186,7 +186,7 @@ uint32_t rtg_queue_free(uint32_t queue);
  * term that shifts the minimum, e.g. towards dimmer lights). With RTG_ADJOINT_CORRELATED every
  * path uses the residual of the whole film, all samples from the scene's seed: the derivative of
  * this very estimate, as a same-seed finite difference measures it.
- * The film must lie inside the image; every path of the call is held in one wave (196 bytes each).
+ * The film must lie inside the image; every path of the call is held in one wave (172 bytes each).
  * `residual` (may be null) receives the sum over replayed paths of |radiance left after the
  * replay| and of |radiance|: the first is 0 up to rounding when the replay retraced the forward
  * paths. A scene with cut-outs or thin walls is refused (RTG_STATUS_BAD_SCENE): the replay does not
@@ -229,7 +229,7 @@ uint32_t rtg_trace_rays(uint32_t scene, const float* rays, uint32_t n, uint32_t 
  * triangles, BVH build seconds, rays cast so far. */
 uint32_t rtg_scene_stats(uint32_t scene, double* out8);
 
-/* Largest number of paths one wave holds (196 bytes of device memory per path, kept until the
+/* Largest number of paths one wave holds (172 bytes of device memory per path, kept until the
  * scene is freed). 0, the default, sizes each wave to every path of the call, bounded by half of
  * the device memory then free: a call then runs as few waves as memory allows, and each wave's
  * tail of long paths is paid once. */

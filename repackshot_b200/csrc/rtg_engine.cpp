@@ -314,9 +314,9 @@ SceneDev compose(const SceneDev& constants, const SceneDev& geom, const SceneDev
     return S;
 }
 
-// Device bytes of one path slot: its record (PATH_RECORD: o, d, hit, flags, medium, thr, sum,
-// sel), sh_o, sh_d, sh_c (16 each), queue[0], queue[1], sorted, key, sh_key (4 each).
-constexpr size_t PATH_BYTES = PATH_RECORD + 3 * 16 + 5 * 4;
+// Device bytes of one path slot: o, d, thr, sum, sel, hit, sh_o, sh_d, sh_c (16 each), flags,
+// medium, queue[0], queue[1], sorted, key, sh_key (4 each).
+constexpr size_t PATH_BYTES = 9 * 16 + 7 * 4;
 // The ray sort's two key histograms with their cursors, at the largest key count.
 constexpr size_t SORT_BINS_BYTES = 2 * 2 * (size_t)(8u << (3u * RAY_SORT_MAX_BITS)) * 4;
 // The default tuning: no ray sort, material-sorted shading. On the 1080p product frame the sort
@@ -413,8 +413,15 @@ uint32_t ensure_capacity(Scene& sc, uint32_t paths) {
     sc.path_mem.bytes = bytes;
     uint8_t* p = (uint8_t*)sc.path_mem.p;
     auto take = [&](size_t each) { uint8_t* r = p; p += ((n * each + 255) / 256) * 256; return r; };
-    // (sizes rounded to 256 bytes; `bytes` above leaves room for the rounding of 9 arrays)
-    set_path_records(sc.P, take(PATH_RECORD));
+    // (sizes rounded to 256 bytes; `bytes` above leaves room for the rounding of 14 arrays)
+    sc.P.o = (float4*)take(16);
+    sc.P.d = (float4*)take(16);
+    sc.P.thr = (float4*)take(16);
+    sc.P.sum = (float4*)take(16);
+    sc.P.sel = (float4*)take(16);
+    sc.P.flags = (uint32_t*)take(4);
+    sc.P.medium = (uint32_t*)take(4);
+    sc.P.hit = (uint4*)take(16);
     sc.P.queue[0] = (uint32_t*)take(4);
     sc.P.queue[1] = (uint32_t*)take(4);
     sc.P.sorted = (uint32_t*)take(4);
@@ -1480,10 +1487,9 @@ uint32_t rtg_render_paths(uint32_t handle, const uint32_t* xys, uint32_t n, floa
     if (st) return st;
     std::vector<float4> sum(n), thr(n);
     std::vector<uint32_t> flags(n);
-    // each a field of the path records: one row of the field's bytes per record
-    RTG_CHECK(cudaMemcpy2DAsync(sum.data(), 16, sc->P.sum.base, PATH_RECORD, 16, n, cudaMemcpyDeviceToHost, sc->stream));
-    RTG_CHECK(cudaMemcpy2DAsync(thr.data(), 16, sc->P.thr.base, PATH_RECORD, 16, n, cudaMemcpyDeviceToHost, sc->stream));
-    RTG_CHECK(cudaMemcpy2DAsync(flags.data(), 4, sc->P.flags.base, PATH_RECORD, 4, n, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaMemcpyAsync(sum.data(), sc->P.sum, (size_t)n * 16, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaMemcpyAsync(thr.data(), sc->P.thr, (size_t)n * 16, cudaMemcpyDeviceToHost, sc->stream));
+    RTG_CHECK(cudaMemcpyAsync(flags.data(), sc->P.flags, (size_t)n * 4, cudaMemcpyDeviceToHost, sc->stream));
     st = finish(*sc, nullptr);
     if (st) return st;
     for (uint32_t i = 0; i < n; ++i) {

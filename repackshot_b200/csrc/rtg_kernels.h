@@ -65,30 +65,16 @@ struct WaveDesc {
     float* guide_weight;
 };
 
-// The path state of a wave is an array of 128-byte records, one per path slot, each on its own
-// cache line: a kernel that visits paths out of slot order (shade reads them in material order)
-// moves one line per path instead of a 32-byte sector per field in separate arrays. The record:
-// bytes 0-31 origin and direction (what the traversal reads), 32-63 hit, flags and medium, 64-127
-// throughput, radiance and the light selection's point. A PathField is one field of it.
-constexpr size_t PATH_RECORD = 128;
-constexpr size_t PATH_O = 0, PATH_D = 16, PATH_HIT = 32, PATH_FLAGS = 48, PATH_MEDIUM = 52, PATH_THR = 64, PATH_SUM = 80,
-                 PATH_SEL = 96;
-template <class T>
-struct PathField {
-    unsigned char* base = nullptr;  // the field in slot 0's record
-    __host__ __device__ __forceinline__ T& operator[](size_t slot) const { return *reinterpret_cast<T*>(base + slot * PATH_RECORD); }
-};
-
-// The path state of one wave (device memory).
+// Structure-of-arrays path state of one wave (device pointers).
 struct PathBuffers {
-    PathField<float4> o;       // origin, w: distance since the last scattering vertex (straight events)
-    PathField<float4> d;       // direction, w: density of the BSDF sample that produced it
-    PathField<float4> thr;     // throughput, w: alpha
-    PathField<float4> sum;     // radiance
-    PathField<float4> sel;     // point of the light selection the MIS weights use
-    PathField<uint32_t> flags;
-    PathField<uint32_t> medium;
-    PathField<uint4> hit;
+    float4* o;       // origin, w: distance since the last scattering vertex (straight events)
+    float4* d;       // direction, w: density of the BSDF sample that produced it
+    float4* thr;     // throughput, w: alpha
+    float4* sum;     // radiance
+    float4* sel;     // point of the light selection the MIS weights use
+    uint32_t* flags;
+    uint32_t* medium;
+    uint4* hit;
     uint32_t* queue[2];
     uint32_t* sorted;    // the active queue ordered by material key (shade reads it)
     uint32_t* key;       // per slot: material of the hit (n_materials: floor or miss)
@@ -125,19 +111,6 @@ struct RaySort {
     uint32_t tail_paths = 0;
 };
 constexpr uint32_t TAIL_FIRST_ROUND = 2;
-// Points the path state's fields into `records` (PATH_RECORD bytes a slot, 128-byte aligned).
-inline void set_path_records(PathBuffers& P, void* records) {
-    unsigned char* r = static_cast<unsigned char*>(records);
-    P.o.base = r + PATH_O;
-    P.d.base = r + PATH_D;
-    P.hit.base = r + PATH_HIT;
-    P.flags.base = r + PATH_FLAGS;
-    P.medium.base = r + PATH_MEDIUM;
-    P.thr.base = r + PATH_THR;
-    P.sum.base = r + PATH_SUM;
-    P.sel.base = r + PATH_SEL;
-}
-
 constexpr uint32_t RAY_SORT_MAX_BITS = 5;
 inline uint32_t ray_sort_keys(uint32_t bits) { return 8u << (3u * bits); }
 

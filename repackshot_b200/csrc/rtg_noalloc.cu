@@ -7,7 +7,7 @@
 // meet an out-of-memory error in the middle of a frame -- use this variant instead. It runs the
 // same kernels in the same order; only the path buffers differ, so the film receives the same bits.
 //
-// The array is RTG_NOALLOC_SCRATCH_BYTES (14 MiB) of device memory in this file's module. Every
+// The array is RTG_NOALLOC_SCRATCH_BYTES (12 MiB) of device memory in this file's module. Every
 // GPU that loads the module holds it until the process exits, whether or not this variant is
 // called. It holds one wave of at most RTG_NOALLOC_MAX_PATHS (65,536) paths.
 #include <cuda_runtime.h>
@@ -22,10 +22,10 @@
 namespace rtg {
 namespace {
 
-// Bytes per path of the state (PathBuffers): its record (PATH_RECORD), sh_o, sh_d, sh_c (16
-// each), queue[0], queue[1], sorted, key (4 each); then the first-hit albedo of each path (16),
-// which a film with fused guides adds to its guide sums.
-constexpr size_t kBytesPerPath = PATH_RECORD + 4 * 16 + 4 * 4;
+// Bytes per path of the structure-of-arrays state (PathBuffers): o, d, thr, sum, sel, hit, sh_o,
+// sh_d, sh_c (16 each), flags, medium, queue[0], queue[1], sorted, key (4 each); then the
+// first-hit albedo of each path (16), which a film with fused guides adds to its guide sums.
+constexpr size_t kBytesPerPath = 10 * 16 + 6 * 4;
 constexpr size_t kPaths = RTG_NOALLOC_MAX_PATHS;
 constexpr size_t kBinsBytes = 512 * 4;
 constexpr size_t kCountersBytes = 64;  // [0], [1] queue lengths, [2] shadow queue, [3] error bits
@@ -45,7 +45,14 @@ PathBuffers carve(void* base, float4** albedo) {
     unsigned char* p = static_cast<unsigned char*>(base);
     auto take = [&](size_t each) { unsigned char* r = p; p += kPaths * each; return r; };
     PathBuffers P{};
-    set_path_records(P, take(PATH_RECORD));
+    P.o = (float4*)take(16);
+    P.d = (float4*)take(16);
+    P.thr = (float4*)take(16);
+    P.sum = (float4*)take(16);
+    P.sel = (float4*)take(16);
+    P.flags = (uint32_t*)take(4);
+    P.medium = (uint32_t*)take(4);
+    P.hit = (uint4*)take(16);
     P.queue[0] = (uint32_t*)take(4);
     P.queue[1] = (uint32_t*)take(4);
     P.sorted = (uint32_t*)take(4);
