@@ -561,14 +561,6 @@ __device__ __forceinline__ bool shade_slot(const SceneDev& S, const LightsDev& L
 // use on its own: the kernel waits on scattered hit-detail loads, and more warps hide them (1080p
 // frame: 369 -> 383 Mpaths/s; 5, 6 and 7 blocks measured 367, 379 and 372).
 // `order`: the active queue in the order to shade it (material-sorted, or as traced).
-// RTG_SHADE_PREFETCH (build setting): 1 has each thread ask L2 for the path state of the path it
-// shades next while it shades this one (the state's reads are scattered: shade visits paths in
-// material order).
-#ifndef RTG_SHADE_PREFETCH
-#define RTG_SHADE_PREFETCH 0
-#endif
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
 template <bool BATCH>
 __global__ void __launch_bounds__(128, RTG_SHADE_MIN_BLOCKS) k_shade(SceneDev S, const LightsDev* __restrict__ Lg, PathBuffers P, int cur, WaveDesc w,
                                                   const uint32_t* __restrict__ order, RaySort R) {
@@ -576,19 +568,6 @@ __global__ void __launch_bounds__(128, RTG_SHADE_MIN_BLOCKS) k_shade(SceneDev S,
     uint32_t rays_local = 0, shadow_local = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t slot = order[i];
-#if RTG_SHADE_PREFETCH
-        const uint32_t i2 = i + gridDim.x * blockDim.x;
-        if (i2 < n) {
-            const uint32_t s2 = order[i2];
-            prefetch_l2(&P.o[s2]);
-            prefetch_l2(&P.d[s2]);
-            prefetch_l2(&P.thr[s2]);
-            prefetch_l2(&P.sum[s2]);
-            prefetch_l2(&P.hit[s2]);
-            prefetch_l2(&P.sel[s2]);
-            prefetch_l2(&P.flags[s2]);
-        }
-#endif
         if constexpr (BATCH) {
             uint32_t job, x, y, index;
             batch_slot(w, slot, job, x, y, index);
