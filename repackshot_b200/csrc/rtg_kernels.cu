@@ -15,6 +15,11 @@ __constant__ SobolTable c_sobol;
 
 // Threads per block of the traversal kernels (the stride of their shared stacks).
 constexpr int TRACE_THREADS = 128;
+// RTG_REFILL_MIN (build setting): idle lanes a k_extend warp waits for before it takes new rays
+// (1: every step with an idle lane).
+#ifndef RTG_REFILL_MIN
+#define RTG_REFILL_MIN 1
+#endif
 // RTG_TRACE_MIN_BLOCKS (build setting): blocks per SM the traversal kernels (k_extend, k_shadow)
 // are compiled for (0: the compiler's choice of registers, 76). At 8 (64 registers, no spills in
 // k_extend, 40 bytes in k_shadow) the 1080p product frame's extend time fell from 163 to 145 ms
@@ -236,7 +241,7 @@ __global__ void RTG_TRACE_BOUNDS k_extend(SceneDev S, PathBuffers P, int cur, co
     for (;;) {
         if (!drained) {
             const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
-            if (idle) {
+            if (idle && (RTG_REFILL_MIN <= 1 || __popc(idle) >= RTG_REFILL_MIN || idle == 0xffffffffu)) {
                 const int leader = __ffs((int)idle) - 1;
                 uint32_t base = 0;
                 if ((int)lane == leader) base = atomicAdd(&P.counters[4], (uint32_t)__popc(idle));
