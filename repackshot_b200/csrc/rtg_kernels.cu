@@ -20,6 +20,10 @@ constexpr int TRACE_THREADS = 128;
 #ifndef RTG_REFILL_MIN
 #define RTG_REFILL_MIN 1
 #endif
+// RTG_SHADOW_REFILL_MIN (build setting): the same for k_shadow.
+#ifndef RTG_SHADOW_REFILL_MIN
+#define RTG_SHADOW_REFILL_MIN 1
+#endif
 // RTG_TRACE_MIN_BLOCKS (build setting): blocks per SM the traversal kernels (k_extend, k_shadow)
 // are compiled for (0: the compiler's choice of registers, 76). At 8 (64 registers, no spills in
 // k_extend, 40 bytes in k_shadow) the 1080p product frame's extend time fell from 163 to 145 ms
@@ -614,7 +618,7 @@ __global__ void RTG_TRACE_BOUNDS k_shadow(SceneDev S, PathBuffers P, const uint3
     for (;;) {
         if (!drained) {
             const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
-            if (idle) {
+            if (idle && (RTG_SHADOW_REFILL_MIN <= 1 || __popc(idle) >= RTG_SHADOW_REFILL_MIN || idle == 0xffffffffu)) {
                 const int leader = __ffs((int)idle) - 1;
                 uint32_t base = 0;
                 if ((int)lane == leader) base = atomicAdd(&P.counters[5], (uint32_t)__popc(idle));
