@@ -29,9 +29,9 @@ struct PRay {
 RTG_D PRay prepare_ray(V3 o, V3 d, float tmin, float tmax) {  // triangle.rs:60
     PRay r;
     float dd[3] = {d.x, d.y, d.z};
-    r.inv[0] = 1.0f / d.x;
-    r.inv[1] = 1.0f / d.y;
-    r.inv[2] = 1.0f / d.z;
+    r.inv[0] = __frcp_rn(d.x);  // 1 / d, correctly rounded (the division's IEEE result)
+    r.inv[1] = __frcp_rn(d.y);
+    r.inv[2] = __frcp_rn(d.z);
     float a0 = absf(d.x), a1 = absf(d.y), a2 = absf(d.z);
     int kz = (a0 >= a1 && a0 >= a2) ? 0 : (a1 >= a2 ? 1 : 2);
     int kx = (kz + 1) % 3, ky = (kz + 2) % 3;
@@ -185,6 +185,7 @@ struct Trav {
     uint32_t leaf_k, leaf_end;  // a leaf being tested a few triangles a step: the next one, the end (0: none)
     int sp, level;
     bool camera;
+    bool moved;  // R is in a transformed instance's object space (else it is the world ray)
 };
 
 // Triangles of a leaf tested per traversal step (0: the whole leaf in one step). With a bound,
@@ -216,6 +217,7 @@ RTG_D bool trav_init(const SceneDev& S, Trav& T, V3 o, V3 d, float tmin, float t
     T.camera = camera;
     T.leaf_k = 0;
     T.leaf_end = 0;
+    T.moved = false;
     return true;
 }
 
@@ -290,6 +292,7 @@ RTG_D bool trav_step(const SceneDev& S, Trav& T, Stack& stack, uint32_t* err, bo
 #pragma unroll
                     for (int k = 0; k < 12; ++k) m[k] = __ldg(&bi->to_local[k]);
                     T.R = prepare_ray(xf_point(m, T.o), xf_vector(m, T.d), T.tmin, T.tmax);
+                    T.moved = true;
                 }
                 T.b_inst = __ldg(&bi->instance);
                 T.b_flags = flags;
@@ -335,7 +338,10 @@ RTG_D bool trav_step(const SceneDev& S, Trav& T, Stack& stack, uint32_t* err, bo
         uint32_t ref = (uint32_t)e;
         if (ref == STACK_RETURN) {
             T.level = 0;
-            T.R = prepare_ray(T.o, T.d, T.tmin, T.tmax);
+            if (T.moved) {  // an identity instance's tree was walked with the world ray itself
+                T.R = prepare_ray(T.o, T.d, T.tmin, T.tmax);
+                T.moved = false;
+            }
             continue;
         }
         float t = __uint_as_float((uint32_t)(e >> 32));
