@@ -42,8 +42,8 @@ DATA = "synthetic (seeded procedural scene; no dataset)"
 FALLBACK_HBM_GBS = 6650.0
 BYTES_RAY_IO = 32 + 12  # ray in, hit out
 # DRAM bytes (read + write) per extend ray, from one ncu capture of k_extend on this scene (round 0
-# of a 4 Mi-path wave: 372 MB for 4,147,200 rays). Scaled to a launch by the rays it traces.
-DRAM_BYTES_PER_EXTEND_RAY = 90.0
+# of a 4 Mi-path wave: 341 MB for 4,147,200 rays). Scaled to a launch by the rays it traces.
+DRAM_BYTES_PER_EXTEND_RAY = 82.0
 
 
 def peaks():
