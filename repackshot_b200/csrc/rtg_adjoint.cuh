@@ -442,7 +442,8 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow_adjoint(SceneDev S, Pa
     for (;;) {
         if (!drained) {
             const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
-            if (idle) {
+            // k_shadow's refill threshold (RTG_SHADOW_REFILL_MIN idle lanes, or all of them)
+            if (idle && (RTG_SHADOW_REFILL_MIN <= 1 || __popc(idle) >= RTG_SHADOW_REFILL_MIN || idle == 0xffffffffu)) {
                 const int leader = __ffs((int)idle) - 1;
                 uint32_t base = 0;
                 if ((int)lane == leader) base = atomicAdd(&P.counters[5], (uint32_t)__popc(idle));

@@ -213,6 +213,18 @@ def test_material_gradients_match_finite_differences(fd_setup, name, materials, 
     agree(f"{name} material {m} column {c}", grads[:, 4 * m + c], fd(kind, (m, c if c < 3 else 0), 1.0e-3))
 
 
+def test_alpha_gradient_matches_a_wider_finite_difference(fd_setup):
+    """The alpha check at h = 1e-3 is dominated by its finite difference's noise: a step in alpha
+    moves the sampled GGX directions, so a few paths change entirely. At h = 1e-2 that noise is
+    ten times smaller against the step, and the central difference's own error (of order h^2 times
+    the third derivative) stays far below 1e-2 of the gradient: within 1e-2 relative plus three
+    standard errors, as the other checks."""
+    base, grads, fd = fd_setup
+    materials = [m for m in range(16) if base.materials[m].roughness ** 2 >= 0.1 and base.materials[m].ior != 1.0]
+    (m, c), _ = pick(grads.mean(axis=0), materials, 3)
+    agree(f"alpha material {m} at h = 1e-2", grads[:, 4 * m + 3], fd("alpha", (m, 0), 1.0e-2))
+
+
 def test_light_power_gradients_match_finite_differences(fd_setup):
     base, grads, fd = fd_setup
     for j in range(3):
