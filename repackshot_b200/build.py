@@ -32,9 +32,8 @@ DEVICE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true
 # RTG_TRACE_MIN_BLOCKS (environment): blocks per SM the traversal kernels are compiled for (default 8).
 # RTG_REFILL_MIN, RTG_SHADOW_REFILL_MIN (environment): idle lanes a k_extend / k_shadow warp waits
 # for before it refills (default 8).
-# RTG_COMPACT (environment): 1 builds each round's extension queue in slot order (default 0).
 for _name in ("RTG_SHADE_MIN_BLOCKS", "RTG_SHORT_STACK", "RTG_LEAF_STEP", "RTG_TRACE_MIN_BLOCKS", "RTG_REFILL_MIN",
-              "RTG_SHADOW_REFILL_MIN", "RTG_COMPACT"):
+              "RTG_SHADOW_REFILL_MIN"):
     if os.environ.get(_name, "").isdigit():
         DEVICE_FLAGS.append(f"-D{_name}={os.environ[_name]}")
 HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-pthread", f"-I{CUDA_HOME}/include"]

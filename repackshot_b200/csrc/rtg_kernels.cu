@@ -52,15 +52,6 @@ constexpr uint32_t PF_HAS_PDF = 1, PF_PRIMARY = 2, PF_MEDIUM = 4;
 // A panoramic camera's sample that sees nothing (scene/mod.rs:227): its ray has an empty interval
 // (no hit, no floor) and its radiance is multiplied by its black weight when it reaches the film.
 constexpr uint32_t PF_NOTHING = 8;
-// RTG_COMPACT (build setting): 1 builds each round's extension queue in slot order (k_compact
-// over the wave's slots, from PF_ALIVE, which shade sets on the paths that go on) instead of
-// shade appending them in the order it shades them. The order of a queue changes no path's bits;
-// slot order keeps neighbouring pixels' paths together, so the kernels that read their state
-// share more of each sector and DRAM page.
-#ifndef RTG_COMPACT
-#define RTG_COMPACT 0
-#endif
-constexpr uint32_t PF_ALIVE = 16;
 // The path's flags also hold the cut-outs it passed (bits 8-14, at most MAX_CUTOUTS) and its vertex
 // count (bits 16-26): a cut-out pass is no vertex, so a path's bounce can fall behind the round.
 constexpr uint32_t PF_CUT_SHIFT = 8, PF_CUT_MASK = 0x7fu << 8, PF_BOUNCE_SHIFT = 16, PF_BOUNCE_MASK = 0x7ffu << 16;
@@ -441,7 +432,7 @@ __device__ __forceinline__ bool shade_slot(const SceneDev& S, const LightsDev& L
                     const V3 o2 = offset_origin(h.point, -ng);
                     offset += dot(o2 - ro, rd);
                     P.o[slot] = make_float4(o2.x, o2.y, o2.z, offset);
-                    P.flags[slot] = flags | (RTG_COMPACT && !tail ? PF_ALIVE : 0u);
+                    P.flags[slot] = flags;
                     alive = true;
                     break;
                 }
@@ -560,16 +551,14 @@ __device__ __forceinline__ bool shade_slot(const SceneDev& S, const LightsDev& L
         }
         P.o[slot] = make_float4(next_origin.x, next_origin.y, next_origin.z, offset);
         P.d[slot] = make_float4(wi.x, wi.y, wi.z, pdf);
-        P.flags[slot] = (flags & ~PF_BOUNCE_MASK) | ((bounce + 1u) << PF_BOUNCE_SHIFT) | (RTG_COMPACT && !tail ? PF_ALIVE : 0u);
+        P.flags[slot] = (flags & ~PF_BOUNCE_MASK) | ((bounce + 1u) << PF_BOUNCE_SHIFT);
         alive = true;
     } while (false);
     P.thr[slot] = make_float4(thr.r, thr.g, thr.b, alpha);
     P.sum[slot] = sum;
     if (alive && !tail) {
-        if (!RTG_COMPACT) {
-            uint32_t k = atomicAdd(&P.counters[cur ^ 1], 1u);
-            P.queue[cur ^ 1][k] = slot;
-        }
+        uint32_t k = atomicAdd(&P.counters[cur ^ 1], 1u);
+        P.queue[cur ^ 1][k] = slot;
         if (P.rbins) {
             const float4 no = P.o[slot], nd = P.d[slot];
             const uint32_t rk = ray_key(R, v3(no.x, no.y, no.z), v3(nd.x, nd.y, nd.z));
@@ -774,27 +763,6 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_tail(SceneDev S, const Lights
     if ((threadIdx.x & 31) == 0 && total) atomicAdd(P.rays, (unsigned long long)total);
     if ((threadIdx.x & 31) == 0 && shadows) atomicAdd(P.rays + 1, (unsigned long long)shadows);
     if (err) atomicOr(&P.counters[3], err);
-}
-
-// The next round's extension queue in slot order: every slot of the wave whose path shade marked
-// PF_ALIVE, a warp's 32 slots at a time (one atomic a warp), the mark cleared.
-__global__ void k_compact(PathBuffers P, int next, uint32_t n) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += stride) {
-        const uint32_t slot = base + lane;
-        const uint32_t f = slot < n ? P.flags[slot] : 0u;
-        const bool alive = (f & PF_ALIVE) != 0u;
-        const uint32_t mask = __ballot_sync(0xffffffffu, alive);
-        if (mask == 0u) continue;
-        uint32_t pos = 0;
-        if (lane == 0) pos = atomicAdd(&P.counters[next], (uint32_t)__popc(mask));
-        pos = __shfl_sync(0xffffffffu, pos, 0);
-        if (alive) {
-            P.queue[next][pos + (uint32_t)__popc(mask & ((1u << lane) - 1u))] = slot;
-            P.flags[slot] = f & ~PF_ALIVE;
-        }
-    }
 }
 
 // After k_tail: a queue it carried to the end is empty for the rest of the wave.
@@ -1284,24 +1252,13 @@ static void launch_traversal(const RaySort& order, int grid, cudaStream_t st, vo
     cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-// Blocks of 256 threads for k_compact over n slots: a warp per 32 slots up to 16 blocks per SM.
-static int grid_compact(uint32_t n) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
-    }
-    const long g = std::min<long>(((long)n + 255) / 256, (long)sms * 16);
-    return (int)std::max<long>(g, 1);
-}
-
 // Whether a wave's last rounds run in k_tail: a limit set, no shadow walks, not batched.
 static bool tail_on(const SceneDev& S, const RaySort& order, bool batch) { return order.tail_paths > 0 && !S.any_passable && !batch; }
 
 uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P, bool batch) {
     const uint32_t rounds = wave_rounds(S);
     const bool rsort = order.ray_bits > 0 && P.rbins, ssort = rsort && order.shadow_sort && P.sbins;
-    uint32_t per_round = 5 + (order.material_sort ? 1u : 0u) + (ssort ? 2u : 0u) + (RTG_COMPACT ? 1u : 0u);
+    uint32_t per_round = 5 + (order.material_sort ? 1u : 0u) + (ssort ? 2u : 0u);
     const uint32_t tail = tail_on(S, order, batch) && rounds > TAIL_FIRST_ROUND ? 2u * (rounds - TAIL_FIRST_ROUND) : 0u;
     return 2 + rounds * per_round + (rsort && rounds > 1 ? 2u * (rounds - 1u) : 0u) + tail;
 }
@@ -1367,7 +1324,6 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
         if (!S.any_passable) launch_traversal(order, g_sh, st, k_shadow, S, P, perm);
         else if (batch) k_shadow_walk<true><<<g, TRACE_THREADS, 0, st>>>(S, P, w, perm);
         else k_shadow_walk<false><<<g, TRACE_THREADS, 0, st>>>(S, P, w, perm);
-        if (RTG_COMPACT) k_compact<<<grid_compact(w.n), 256, 0, st>>>(P, cur ^ 1, w.n);
         k_next_round<<<1, 1, 0, st>>>(P, cur);
         cur ^= 1;
     }
