@@ -28,10 +28,11 @@ DEVICE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true
                 "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v"]
 # RTG_SHADE_MIN_BLOCKS (environment): blocks per SM the shade kernels are compiled for (default 8);
 # RTG_SHORT_STACK (environment): traversal stack entries kept in shared memory (default 16).
+# RTG_LEAF_STEP (environment): triangles of a leaf tested per traversal step (default 0: all).
 # RTG_TRACE_MIN_BLOCKS (environment): blocks per SM the traversal kernels are compiled for (default 8).
 # RTG_REFILL_MIN, RTG_SHADOW_REFILL_MIN (environment): idle lanes a k_extend / k_shadow warp waits
 # for before it refills (default 8).
-for _name in ("RTG_SHADE_MIN_BLOCKS", "RTG_SHORT_STACK", "RTG_TRACE_MIN_BLOCKS", "RTG_REFILL_MIN",
+for _name in ("RTG_SHADE_MIN_BLOCKS", "RTG_SHORT_STACK", "RTG_LEAF_STEP", "RTG_TRACE_MIN_BLOCKS", "RTG_REFILL_MIN",
               "RTG_SHADOW_REFILL_MIN"):
     if os.environ.get(_name, "").isdigit():
         DEVICE_FLAGS.append(f"-D{_name}={os.environ[_name]}")

@@ -182,10 +182,19 @@ struct Trav {
     float tmin, tmax;
     float best_t;
     uint32_t best_i, best_tri, cur, b_inst, b_flags;
+    uint32_t leaf_k, leaf_end;  // a leaf being tested a few triangles a step: the next one, the end (0: none)
     int sp, level;
     bool camera;
     bool moved;  // R is in a transformed instance's object space (else it is the world ray)
 };
+
+// Triangles of a leaf tested per traversal step (0: the whole leaf in one step). With a bound,
+// a lane in a long leaf takes as many steps as its triangles need while the rest of its warp
+// walks inner nodes, instead of holding them at one step until its leaf is done. A build may set
+// RTG_LEAF_STEP; the answer does not depend on it.
+#ifndef RTG_LEAF_STEP
+#define RTG_LEAF_STEP 0
+#endif
 
 // Sets up a query. False when the ray can meet nothing (non-finite or zero direction, empty
 // interval): a miss.
@@ -206,6 +215,8 @@ RTG_D bool trav_init(const SceneDev& S, Trav& T, V3 o, V3 d, float tmin, float t
     T.sp = 0;
     T.level = 0;
     T.camera = camera;
+    T.leaf_k = 0;
+    T.leaf_end = 0;
     T.moved = false;
     return true;
 }
@@ -290,7 +301,10 @@ RTG_D bool trav_step(const SceneDev& S, Trav& T, Stack& stack, uint32_t* err, bo
                 return false;
             }
         } else {
-            for (uint32_t k = first; k < first + count; ++k) {
+            uint32_t k = T.leaf_end ? T.leaf_k : first;
+            const uint32_t end = T.leaf_end ? T.leaf_end : first + count;
+            const uint32_t stop = (RTG_LEAF_STEP > 0 && end - k > (uint32_t)RTG_LEAF_STEP) ? k + (uint32_t)RTG_LEAF_STEP : end;
+            for (; k < stop; ++k) {
                 const float4* tr = reinterpret_cast<const float4*>(S.tris + k);
                 float4 a = __ldg(tr), b = __ldg(tr + 1), c = __ldg(tr + 2);
                 uint32_t flags = __float_as_uint(c.w) | T.b_flags;
@@ -298,7 +312,7 @@ RTG_D bool trav_step(const SceneDev& S, Trav& T, Stack& stack, uint32_t* err, bo
                 float v0[3] = {a.x, a.y, a.z}, v1[3] = {b.x, b.y, b.z}, v2[3] = {c.x, c.y, c.z};
                 float t, uu, vv, ww, det;
                 if (watertight(T.R, v0, v1, v2, ANY ? T.R.tmax : T.best_t, (flags & 1u) != 0, t, uu, vv, ww, det)) {
-                    if (ANY) { hit = true; return true; }
+                    if (ANY) { T.leaf_end = 0; hit = true; return true; }
                     uint32_t inst = __float_as_uint(b.w);
                     if (inst == 0xffffffffu) inst = T.b_inst;
                     uint32_t tri = __float_as_uint(a.w);
@@ -307,6 +321,12 @@ RTG_D bool trav_step(const SceneDev& S, Trav& T, Stack& stack, uint32_t* err, bo
                     }
                 }
             }
+            if (k < end) {  // more of this leaf next step
+                T.leaf_k = k;
+                T.leaf_end = end;
+                return false;
+            }
+            T.leaf_end = 0;
         }
     }
     for (;;) {
