@@ -573,8 +573,8 @@ def run_ours(args, world, rank, local, dist):
         "dtype": "f32", "data": DATA,
         "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": DEPTH,
                    "triangles": scene.triangles, "paths_per_step_per_gpu": paths_step,
-                   "l2": "flushed between steps (512 MiB write); the per-step working set (168 B of path state per path, "
-                         "22 GB for the frame) exceeds L2",
+                   "l2": "flushed between steps (512 MiB write); the per-step working set (172 B of path state per path, "
+                         "23 GB for the frame) exceeds L2",
                    "parallelism": f"replicas x{world}: each rank renders its own sample range of the frame",
                    "scene_gen_s": round(gen_s, 3), "scene_load_s": round(load_s, 3), "bvh_build_s": round(scene.build_seconds, 3),
                    "tuning": tuned["chosen"]},
