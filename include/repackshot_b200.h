@@ -208,6 +208,11 @@ uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, f
 uint32_t rtg_film_srgb8(uint32_t film, float ev, uint32_t tonemap, uint8_t* out);
 uint32_t rtg_film_srgb16(uint32_t film, float ev, uint32_t tonemap, uint16_t* out);
 
+/* Film::to_linear_exposed (rt-core/src/image.rs:218-221): the film resolved as above and
+ * multiplied by 2^ev, scene-linear light with no tone curve and no clamp: `out` w*h*3 floats, row
+ * major. The samples of the reference's 32-bit float TIFF and of its DNG (rt-cli/src/lib.rs:740-760). */
+uint32_t rtg_film_linear(uint32_t film, float ev, float* out);
+
 /* The scene's output settings from its RNDR section: exposure in stops, tone curve, samples per
  * pixel (any pointer may be null). */
 uint32_t rtg_scene_output(uint32_t scene, float* exposure_ev, uint32_t* tonemap, uint32_t* max_samples);

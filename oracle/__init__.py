@@ -46,6 +46,7 @@ def lib():
             "orc_sampler_get1": (ctypes.c_float, [u32, u32, u32, u32, u32]),
             "orc_fmath": (None, [u32, v, u32, v]),
             "orc_film_encode": (None, [v, v, u32, ctypes.c_float, u32, v, v]),
+            "orc_film_linear": (None, [v, v, u32, ctypes.c_float, v]),
             "orc_color": (None, [u32, v, u32, v]),
             "orc_agx_identity": (None, [v]),
             "orc_light_count": (u32, [u32]),
@@ -393,6 +394,16 @@ def film_encode(rgb, weight, ev, tonemap):
     out16 = np.zeros(3 * n, np.uint16)
     lib().orc_film_encode(_p(rgb), _p(weight), n, ev, tonemap, _p(out8), _p(out16))
     return out8.reshape(n, 3), out16.reshape(n, 3)
+
+
+def film_linear(rgb, weight, ev):
+    """image.rs to_linear_exposed of film sums: float32 (n, 3), the resolved film times 2^ev."""
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1)
+    weight = np.ascontiguousarray(weight, np.float32).reshape(-1)
+    n = weight.size
+    out = np.zeros(3 * n, np.float32)
+    lib().orc_film_linear(_p(rgb), _p(weight), n, ev, _p(out))
+    return out.reshape(n, 3)
 
 
 def color(which, xs):

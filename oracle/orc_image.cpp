@@ -119,6 +119,16 @@ void orc_film_encode(const float* rgb, const float* weight, uint32_t n, float ev
     }
 }
 
+// Film::to_linear_exposed (image.rs:218-221): the resolved film times exposure(ev), no curve, no clamp.
+void orc_film_linear(const float* rgb, const float* weight, uint32_t n, float ev, float* out) {
+    float gain = exp2(ev);
+    for (uint32_t i = 0; i < n; ++i) {
+        float w = weight[i];
+        float inv = w > 0.0f ? 1.0f / w : 0.0f;
+        for (int c = 0; c < 3; ++c) out[3 * i + c] = (w > 0.0f ? rgb[3 * i + c] * inv : 0.0f) * gain;
+    }
+}
+
 // The single-value functions for the reference's known answers: which 0 exposure, 1 ACES (one
 // channel), 2 sRGB encode; 3..7 Tonemap::apply with kind which - 3 on the grey (x, x, x), giving
 // its green channel.

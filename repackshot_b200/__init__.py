@@ -60,6 +60,7 @@ ABI = {
     "rtg_render_adjoint": (_u32, [_u32, _u32, _f, _u32, _u32, _u32, ctypes.POINTER(ctypes.c_float), _f, _u32, _f]),
     "rtg_film_srgb8": (_u32, [_u32, ctypes.c_float, _u32, _f]),
     "rtg_film_srgb16": (_u32, [_u32, ctypes.c_float, _u32, _f]),
+    "rtg_film_linear": (_u32, [_u32, ctypes.c_float, _f]),
     "rtg_scene_output": (_u32, [_u32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
@@ -327,6 +328,14 @@ class Film:
         out = np.zeros((self.h, self.w, 3), np.uint8 if bits == 8 else np.uint16)
         fn = lib().rtg_film_srgb8 if bits == 8 else lib().rtg_film_srgb16
         _check(fn(self.handle, ev, tonemap, _ptr(out)))
+        return out
+
+    def linear(self, ev: float | None = None) -> np.ndarray:
+        """Film::to_linear_exposed (image.rs:218): (h, w, 3) float32, the resolved film times 2^ev,
+        no tone curve and no clamp. Exposure defaults to the scene's RNDR setting."""
+        ev = self.scene.output()[0] if ev is None else ev
+        out = np.zeros((self.h, self.w, 3), np.float32)
+        _check(lib().rtg_film_linear(self.handle, ev, _ptr(out)))
         return out
 
     def resolve(self) -> np.ndarray:

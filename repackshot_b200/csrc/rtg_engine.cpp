@@ -1416,7 +1416,7 @@ namespace {
 uint32_t film_encode(uint32_t film, float ev, uint32_t tonemap, uint32_t bits, void* out) {
     Film* f = film_of(film);
     if (!f) return RTG_STATUS_BAD_FILM;
-    if (!out) { g_error = "rtg_film_srgb: null pointer"; return RTG_STATUS_NULL_POINTER; }
+    if (!out) { g_error = bits == 32 ? "rtg_film_linear: null pointer" : "rtg_film_srgb: null pointer"; return RTG_STATUS_NULL_POINTER; }
     Scene* sc = scene_of(f->scene);
     cudaStream_t s = sc ? sc->stream : 0;
     size_t bytes = (size_t)f->dev.w * f->dev.h * 3 * (bits / 8);
@@ -1441,6 +1441,10 @@ uint32_t rtg_film_srgb8(uint32_t film, float ev, uint32_t tonemap, uint8_t* out)
 uint32_t rtg_film_srgb16(uint32_t film, float ev, uint32_t tonemap, uint16_t* out) {
     std::lock_guard<std::mutex> lk(g_mu);
     return film_encode(film, ev, tonemap, 16, out);
+}
+uint32_t rtg_film_linear(uint32_t film, float ev, float* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return film_encode(film, ev, 0, 32, out);
 }
 
 uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2) {

@@ -1167,7 +1167,8 @@ __global__ void k_accumulate_jobs(WaveDesc w, PathBuffers P) {
     }
 }
 
-// ---- film output (image.rs:186-214): resolve, exposure, tone curve, sRGB, 8 or 16 bits ----------------
+// ---- film output (image.rs:186-221): resolve, exposure, then either the tone curve and sRGB at 8 or 16
+// bits, or (bits 32) the exposed linear light as floats with no curve and no clamp (to_linear_exposed) ----
 __global__ void k_film_encode(FilmDev F, float gain, uint32_t kind, AgxMatrices agx, uint32_t bits, void* out) {
     const uint32_t n = F.w * F.h;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -1176,6 +1177,13 @@ __global__ void k_film_encode(FilmDev F, float gain, uint32_t kind, AgxMatrices 
         if (w > 0.0f) {
             float inv = 1.0f / w;
             px = rgb(F.rgb[3 * p] * inv, F.rgb[3 * p + 1] * inv, F.rgb[3 * p + 2] * inv);
+        }
+        if (bits == 32) {
+            float* o = static_cast<float*>(out) + 3 * p;
+            o[0] = px.r * gain;
+            o[1] = px.g * gain;
+            o[2] = px.b * gain;
+            continue;
         }
         Rgb m = tonemap_apply(kind, px * gain, agx);
         float v[3] = {srgb_encode(m.r), srgb_encode(m.g), srgb_encode(m.b)};

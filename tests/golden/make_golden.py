@@ -21,6 +21,9 @@ its path tracer, read from the reference's own source tree (run where it is chec
   script as test inputs) and their pinned 4-spp film hashes (render/k3_tests.rs:17-22);
 * the hashes of the denoised example: the full filter at 4 spp and the viewport's at 2 and 4 spp
   (engine/crates/rt-post/src/denoise/tests.rs:392, 527-528).
+* the golden TIFF and DNG files the reference's writers must reproduce byte for byte
+  (tests/fixtures/tiff/*, made by engine/crates/rt-cli/tests/tiff_golden.rs:48-80 from 4 x 4 and
+  50 x 60 images of closed-form samples), copied to tests/golden/tiff/.
 
 Usage: python tests/golden/make_golden.py /path/to/reference
 """
@@ -38,6 +41,8 @@ if len(sys.argv) != 2:
 REF = Path(sys.argv[1])
 CORE = REF / "engine" / "crates" / "rt-core" / "src"
 OUT = Path(__file__).resolve().parent / "reference_pins.json"
+TIFF_GOLDEN = ("rgb8.tif", "rgba8.tif", "rgb16.tif", "rgba16-300dpi.tif", "rgb32.tif", "rgba32.tif", "strips.tif",
+               "linear.dng")
 
 
 def pinned(src: str, name: str) -> int:
@@ -96,6 +101,10 @@ def main():
         data = (REF / "tests" / "fixtures" / f"k3-{view}.rsb").read_bytes()
         (OUT.parent / f"k3-{view}.rsb").write_bytes(data)
         pins[f"k3_{view}_4spp"] = pinned(k3, f"PINNED_K3_{view.upper()}_4SPP")
+    # The TIFF and DNG files rt-cli/tests/tiff_golden.rs compares rt_core::tiff and rt_core::dng with.
+    (OUT.parent / "tiff").mkdir(exist_ok=True)
+    for name in TIFF_GOLDEN:
+        (OUT.parent / "tiff" / name).write_bytes((REF / "tests" / "fixtures" / "tiff" / name).read_bytes())
     out = {
         "source": "Repackshot reference tree (engine crate rt-core), read by tests/golden/make_golden.py",
         "film_hashes": pins,

@@ -55,6 +55,16 @@ def test_encode_quantises_as_the_reference(oracle_lib):
     assert list(b8[1]) == [0, 0, 0] and list(b16[1]) == [0, 0, 0]
 
 
+def test_linear_film_is_the_resolve_times_the_exposure(oracle_lib):
+    # Film::to_linear_exposed (image.rs:218): rgb * (1 / weight) * 2^ev, black where no sample, no
+    # clamp: a pixel of 3 over weight 2 at +2 stops is 6.
+    rgb = np.float32([2.0, 1.0, 0.5, 0, 0, 0, 3.0, 0.25, 7.0])
+    wt = np.float32([2.0, 0.0, 2.0])
+    for ev in (0.0, 2.0, -3.0):
+        want = (rgb.reshape(3, 3) * np.float32([0.5, 0.0, 0.5])[:, None] * np.float32(2.0 ** ev)).astype(np.float32)
+        assert np.array_equal(oracle_lib.film_linear(rgb, wt, ev), want)
+
+
 @pytest.mark.parametrize("dtype", [np.uint8, np.uint16])
 def test_png_round_trip(dtype):
     from repackshot_b200.image import png_bytes, read_png
