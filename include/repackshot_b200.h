@@ -213,6 +213,14 @@ uint32_t rtg_film_srgb16(uint32_t film, float ev, uint32_t tonemap, uint16_t* ou
  * major. The samples of the reference's 32-bit float TIFF and of its DNG (rt-cli/src/lib.rs:740-760). */
 uint32_t rtg_film_linear(uint32_t film, float ev, float* out);
 
+/* The same encodings of film planes given in host memory: `rgb` w*h*3 sums and `weight` w*h
+ * sample weights (a Film's rgb and weight, rt-core/src/image.rs), `bits` 8 or 16 (tone curve and
+ * sRGB, as rtg_film_srgb8/16) or 32 (linear exposed floats, as rtg_film_linear; `tonemap` unused);
+ * `out` w*h*3 bytes, 16-bit words or floats. For images that are no render's film: the
+ * denoised film of the command line (rt-cli/src/cli.rs:1886-1900) is encoded through it. */
+uint32_t rtg_encode_planes(const float* rgb, const float* weight, uint32_t width, uint32_t height, float ev, uint32_t tonemap,
+                           uint32_t bits, void* out);
+
 /* The scene's output settings from its RNDR section: exposure in stops, tone curve, samples per
  * pixel (any pointer may be null). */
 uint32_t rtg_scene_output(uint32_t scene, float* exposure_ev, uint32_t* tonemap, uint32_t* max_samples);

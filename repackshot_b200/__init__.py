@@ -61,6 +61,7 @@ ABI = {
     "rtg_film_srgb8": (_u32, [_u32, ctypes.c_float, _u32, _f]),
     "rtg_film_srgb16": (_u32, [_u32, ctypes.c_float, _u32, _f]),
     "rtg_film_linear": (_u32, [_u32, ctypes.c_float, _f]),
+    "rtg_encode_planes": (_u32, [_f, _f, _u32, _u32, ctypes.c_float, _u32, _u32, _f]),
     "rtg_scene_output": (_u32, [_u32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
@@ -448,6 +449,22 @@ def tile_alpha(handle: int, x: int, y: int, w: int, h: int, sample_index: int):
 
 
 FEATURE_IES, FEATURE_CAMERAS = 8, 16
+
+
+def encode_planes(rgb: np.ndarray, weight: np.ndarray, ev: float, tonemap: int, bits: int) -> np.ndarray:
+    """rtg_encode_planes: film planes in host memory ((h, w, 3) sums and (h, w) weights) encoded on
+    the device as Film.srgb (bits 8 or 16) or Film.linear (bits 32) encode a render's film."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    weight = np.ascontiguousarray(weight, np.float32)
+    h, w = weight.shape
+    if rgb.shape != (h, w, 3):
+        raise ValueError("rgb must be (h, w, 3) and weight (h, w)")
+    dtype = {8: np.uint8, 16: np.uint16, 32: np.float32}.get(bits)
+    if dtype is None:
+        raise ValueError("bits must be 8, 16 or 32")
+    out = np.zeros((h, w, 3), dtype)
+    _check(lib().rtg_encode_planes(_ptr(rgb), _ptr(weight), w, h, ev, tonemap, bits, _ptr(out)))
+    return out
 
 
 def features() -> int:

@@ -1447,6 +1447,32 @@ uint32_t rtg_film_linear(uint32_t film, float ev, float* out) {
     return film_encode(film, ev, 0, 32, out);
 }
 
+uint32_t rtg_encode_planes(const float* rgb, const float* weight, uint32_t width, uint32_t height, float ev, uint32_t tonemap,
+                           uint32_t bits, void* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!rgb || !weight || !out) return RTG_STATUS_NULL_POINTER;
+    if (width == 0 || height == 0 || width > 16384 || height > 16384) return RTG_STATUS_BAD_TILE;
+    if (bits != 8 && bits != 16 && bits != 32) { g_error = "rtg_encode_planes: bits must be 8, 16 or 32"; return RTG_STATUS_BAD_ARGUMENT; }
+    uint32_t st = device_init();
+    if (st) return st;
+    const size_t npix = (size_t)width * height;
+    const size_t rgb_bytes = (npix * 12 + 255) & ~(size_t)255, weight_bytes = (npix * 4 + 255) & ~(size_t)255;
+    const size_t out_bytes = npix * 3 * (bits / 8);
+    DevBuf m;
+    struct Release { DevBuf& b; ~Release() { b.release(); } } release{m};
+    m.bytes = rgb_bytes + weight_bytes + out_bytes;
+    RTG_CHECK(cudaMalloc(&m.p, m.bytes));
+    uint8_t* base = (uint8_t*)m.p;
+    FilmDev F{0, 0, width, height, (float*)base, (float*)(base + rgb_bytes), nullptr, nullptr};
+    void* d_out = base + rgb_bytes + weight_bytes;
+    RTG_CHECK(cudaMemcpy(F.rgb, rgb, npix * 12, cudaMemcpyHostToDevice));
+    RTG_CHECK(cudaMemcpy(F.weight, weight, npix * 4, cudaMemcpyHostToDevice));
+    launch_film_encode(F, ev, tonemap, bits, d_out, 0, grid_for((uint32_t)npix, 256));
+    RTG_CHECK(cudaGetLastError());
+    RTG_CHECK(cudaMemcpy(out, d_out, out_bytes, cudaMemcpyDeviceToHost));
+    return RTG_STATUS_OK;
+}
+
 uint32_t rtg_film_read(uint32_t film, float* rgb, float* weight, float* alpha, float* lum2) {
     std::lock_guard<std::mutex> lk(g_mu);
     Film* f = film_of(film);

@@ -78,6 +78,9 @@ def test_bad_handles_and_null_pointers(rtg):
     assert L.rtg_render_tile_alpha(4096, 0, 0, 4, 4, 0, None) == rtg.STATUS_NULL_POINTER
     assert L.rtg_film_free(4096) == rtg.STATUS_BAD_FILM
     assert L.rtg_film_linear(4096, 0.0, out) == rtg.STATUS_BAD_FILM
+    assert L.rtg_encode_planes(None, out, 2, 2, 0.0, 0, 8, out) == rtg.STATUS_NULL_POINTER
+    assert L.rtg_encode_planes(out, out, 0, 2, 0.0, 0, 8, out) == rtg.STATUS_BAD_TILE
+    assert L.rtg_encode_planes(out, out, 2, 2, 0.0, 0, 12, out) == rtg.STATUS_BAD_ARGUMENT
     assert L.rtg_film_create(4096, 0, 0, 4, 4) == 0
     assert L.rtg_render_progressive(4096, 1, 0, 1, None) == rtg.STATUS_BAD_HANDLE
     assert L.rtg_scene_update(4096, b"RSB1", 4) == rtg.STATUS_BAD_HANDLE
