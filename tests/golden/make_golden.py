@@ -21,6 +21,8 @@ its path tracer, read from the reference's own source tree (run where it is chec
   script as test inputs) and their pinned 4-spp film hashes (render/k3_tests.rs:17-22);
 * the hashes of the denoised example: the full filter at 4 spp and the viewport's at 2 and 4 spp
   (engine/crates/rt-post/src/denoise/tests.rs:392, 527-528).
+* the hashes of the exact passes and the 4-sample albedo and alpha of the example and the E5 example
+  (engine/crates/rt-core/src/render/passes_tests.rs:365-398, 865-868);
 * the golden TIFF and DNG files the reference's writers must reproduce byte for byte
   (tests/fixtures/tiff/*, made by engine/crates/rt-cli/tests/tiff_golden.rs:48-80 from 4 x 4 and
   50 x 60 images of closed-form samples), copied to tests/golden/tiff/.
@@ -105,6 +107,14 @@ def main():
     (OUT.parent / "tiff").mkdir(exist_ok=True)
     for name in TIFF_GOLDEN:
         (OUT.parent / "tiff" / name).write_bytes((REF / "tests" / "fixtures" / "tiff" / name).read_bytes())
+    passes_src = (CORE / "render" / "passes_tests.rs").read_text()
+    pass_keys = ("albedo", "normal", "depth", "part_id", "material_id", "coc")
+    passes = {
+        "example": {k: pinned(passes_src, "PINNED_PASS_" + k.upper()) for k in pass_keys},
+        "e5_hdri": {k: pinned(passes_src, "PINNED_E5_PASS_" + k.upper()) for k in pass_keys},
+    }
+    passes["example"]["alpha"] = pinned(passes_src, "PINNED_PASS_ALPHA")
+    passes["e5_hdri"]["alpha"] = pinned(passes_src, "PINNED_E5_PASS_ALPHA")
     out = {
         "source": "Repackshot reference tree (engine crate rt-core), read by tests/golden/make_golden.py",
         "film_hashes": pins,
@@ -117,6 +127,7 @@ def main():
         "l5_rsb": {"bytes": len(l5), "sha256": hashlib.sha256(l5).hexdigest()},
         "blackman_harris_inv_cdf": {"count": len(bh), "sha256": hashlib.sha256(bh_raw).hexdigest()},
         "e10_synthetic_decisions": pinned((CORE / "adaptive" / "tests.rs").read_text(), "PINNED_E10_DECISIONS"),
+        "passes_4spp": passes,
         "denoised": {k: pinned(denoise, "PINNED_DENOISED_" + k.upper()) for k in
                      ("example_4spp", "viewport_example_2spp", "viewport_example_4spp")},
     }

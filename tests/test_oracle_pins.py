@@ -1,10 +1,12 @@
 """The oracle against the reference's own known answers (tests/golden/reference_pins.json, read
 from the reference tree by tests/golden/make_golden.py): the pinned film hashes of the example
-scene, the PCG32 and mix64 values, the first Sobol points and the six energy tables."""
+scene, the PCG32 and mix64 values, the first Sobol points, the six energy tables, and the exact
+passes with the 4-sample albedo and alpha of the example and the E5 example."""
 import hashlib
 import struct
 
 import numpy as np
+import pytest
 
 
 def test_pcg32_and_mix64(oracle_lib, pins):
@@ -49,3 +51,34 @@ def test_whole_example_at_four_samples_has_the_pinned_hash(oracle_lib, example_r
     s = oracle_lib.OracleScene(example_rsb)
     rgb, w, _, _, _ = s.render_film(0, 4, tile=32, threads=4)
     assert oracle_lib.fnv1a(oracle_lib.resolve(rgb, w)) == pins["film_hashes"]["example_4spp"]
+
+
+def pass_hashes(fnv1a, normal, depth, part, material, albedo_sum, alpha_sum, samples):
+    """FNV-1a of each plane as the reference hashes them (passes.rs:529, Plane::fnv1a over the
+    little-endian words): the albedo and alpha sums scaled by the f32 reciprocal of the count."""
+    inv = np.float32(1.0) / np.float32(samples)
+    return {
+        "albedo": fnv1a((albedo_sum * inv).astype(np.float32)),
+        "normal": fnv1a(normal),
+        "depth": fnv1a(depth),
+        "part_id": fnv1a(np.ascontiguousarray(part, np.uint32).view(np.float32)),
+        "material_id": fnv1a(np.ascontiguousarray(material, np.uint32).view(np.float32)),
+        "alpha": fnv1a((alpha_sum * inv).astype(np.float32)),
+    }
+
+
+@pytest.mark.parametrize("name", ["example", "e5_hdri"])
+def test_passes_of_the_example_and_e5_have_the_pinned_hashes(oracle_lib, pins, name):
+    """render/passes_tests.rs:155-194, 197-230, 840-862: the exact passes and 4 samples of albedo and
+    alpha, added in sample order, of the example (512 x 384) and the E5 example with its HDRI."""
+    from repackshot_b200 import scenes
+    desc = scenes.example_scene() if name == "example" else scenes.e5_scene()
+    o = oracle_lib.OracleScene(scenes.to_rsb(desc))
+    normal, depth, part, material = o.passes()
+    albedo, alpha = np.zeros_like(o.albedo(0)), np.zeros_like(o.alpha(0))
+    for s in range(4):
+        albedo = (albedo + o.albedo(s)).astype(np.float32)
+        alpha = (alpha + o.alpha(s)).astype(np.float32)
+    got = pass_hashes(oracle_lib.fnv1a, normal, depth, part, material, albedo, alpha, 4)
+    want = {k: v for k, v in pins["passes_4spp"][name].items() if k != "coc"}
+    assert got == want
