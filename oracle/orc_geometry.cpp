@@ -368,7 +368,7 @@ const char* Mesh::make(Mesh& m, const std::vector<Vec3>& positions, const std::v
 }
 
 // ---- geometry/mod.rs:294-384 -----------------------------------------------------------------
-static Aabb instance_bounds(const Mesh& mesh, const Transform& t) {
+Aabb instance_bounds(const Mesh& mesh, const Transform& t) {
     if (t.is_identity()) return mesh.bounds;
     Aabb b = t.aabb(mesh.bounds);
     float scale = max_component(vmax(vabs(b.min), vabs(b.max)));
@@ -634,7 +634,7 @@ struct AnyInstance {
 inline bool usable(const Ray& r) { return vfinite(r.origin) && vfinite(r.dir) && !(r.dir == Vec3(0, 0, 0)); }
 }  // namespace
 
-bool Geometry::trace(const Ray& ray, bool camera, RayHit& out, TraceStats* st) const {
+bool Geometry::trace_raw(const Ray& ray, bool camera, RayHit& out, TraceStats* st) const {
     if (!usable(ray)) return false;
     PreparedRay r = PreparedRay::make(ray);
     if (!r.has_interval()) return false;
@@ -646,7 +646,7 @@ bool Geometry::trace(const Ray& ray, bool camera, RayHit& out, TraceStats* st) c
     return true;
 }
 
-bool Geometry::occluded(const Ray& ray, bool camera, TraceStats* st) const {
+bool Geometry::occluded_raw(const Ray& ray, bool camera, TraceStats* st) const {
     if (!usable(ray)) return false;
     PreparedRay r = PreparedRay::make(ray);
     if (!r.has_interval()) return false;
@@ -681,6 +681,7 @@ bool Geometry::trace_brute(const Ray& ray, bool camera, RayHit& out) const {
 // hit_details (geometry/mod.rs:731)
 bool Geometry::hit_details(const Ray& ray, const RayHit& hit, Hit& out) const {
     if (hit.instance >= instances.size()) return false;
+    if (hit.triangle == CAP_TRIANGLE) return cap_details(ray, hit, out);
     const PreparedInstance& p = prepared[hit.instance];
     if (!p.active) return false;
     const Instance& inst = instances[hit.instance];

@@ -116,7 +116,7 @@ struct Mesh {
 };
 
 // ---- geometry/mod.rs ------------------------------------------------------------------------
-constexpr uint32_t INSTANCE_ONE_SIDED = 1, INSTANCE_NO_CAMERA = 4;
+constexpr uint32_t INSTANCE_ONE_SIDED = 1, INSTANCE_NO_SECTION = 2, INSTANCE_NO_CAMERA = 4;
 struct Instance { uint32_t mesh = 0; Transform transform; uint32_t material_id = 0; uint32_t flags = 0; };
 struct PreparedInstance { Transform to_local; bool identity = true; Cull cull = Cull::None; bool active = false; bool camera_hidden = false; };
 struct RayHit { uint32_t instance, triangle; float t; };
@@ -130,6 +130,37 @@ struct Hit {
 // Per-query traversal statistics (reference BVH8 layout): inner-node visits and packet tests.
 struct TraceStats { uint64_t nodes = 0, packets = 0; };
 
+// ---- geometry/solid.rs, geometry/section.rs ---------------------------------------------------
+// What a mesh is as a solid: open (no inside), or closed and wound outward (the back of a triangle
+// is the inside) or inward.
+enum class Solid : uint8_t { Open, Outward, Inward };
+// geometry/mod.rs:284: a mesh's box in the world, padded for a transformed one.
+Aabb instance_bounds(const Mesh& mesh, const Transform& t);
+Solid analyse_solid(const Mesh& mesh);
+inline bool inside_before(Solid s, bool front) { return s == Solid::Outward ? !front : s == Solid::Inward ? front : false; }
+
+// The `triangle` of a hit on the cap of a cut solid.
+constexpr uint32_t CAP_TRIANGLE = 0xffffffffu;
+
+// The plane normal . p = distance; the kept side is normal . p <= distance.
+struct SectionPlane {
+    Vec3 normal;
+    float distance = 0.0f;
+    bool cap = false;
+    // SectionPlane::new: false for a zero or non-finite normal or distance; the normal normalised
+    // unless it is unit already to 1e-6.
+    static bool make(Vec3 normal, float distance, bool cap, SectionPlane& out);
+    float side(Vec3 p) const { return dot(normal, p) - distance; }
+};
+
+struct Section {
+    SectionPlane plane;
+    std::vector<Solid> caps;           // per instance
+    Aabb cap_bounds;                   // the capped instances' world boxes, grown
+    std::vector<uint8_t> exempt;       // per instance (empty: none is exempt)
+    std::vector<Aabb> exempt_boxes;    // the exempt instances' world boxes, grown
+};
+
 struct Geometry {
     std::vector<Mesh> meshes;
     std::vector<Instance> instances;
@@ -139,10 +170,21 @@ struct Geometry {
     Aabb bounds;
     static const char* make(Geometry& g, std::vector<Mesh> meshes, std::vector<Instance> instances);
 
+    bool has_section = false;
+    Section section;
+    // Geometry::set_section: `capped[i]` false for an instance the plane may not cap (a thin wall).
+    void set_section(const SectionPlane* plane, const std::vector<bool>& capped);
+
+    // The queries, through the section when there is one (geometry/section.rs:224-324).
     bool trace(const Ray& ray, bool camera, RayHit& out, TraceStats* st = nullptr) const;
     bool occluded(const Ray& ray, bool camera, TraceStats* st = nullptr) const;
+    // The queries against the whole model.
+    bool trace_raw(const Ray& ray, bool camera, RayHit& out, TraceStats* st = nullptr) const;
+    bool occluded_raw(const Ray& ray, bool camera, TraceStats* st = nullptr) const;
     bool trace_brute(const Ray& ray, bool camera, RayHit& out) const;
     bool hit_details(const Ray& ray, const RayHit& hit, Hit& out) const;
+    // Section::cap_details (section.rs:424-448): on the plane, facing the side the ray came from.
+    bool cap_details(const Ray& ray, const RayHit& hit, Hit& out) const;
     Vec3 terminator_point(const Hit& hit) const;
 };
 

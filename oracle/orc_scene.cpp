@@ -121,7 +121,8 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
     std::memcpy(&header_len, bytes + 4, 4);
     size_t pos = 8 + (size_t)header_len;
     if (pos > len) { error = "RSB file is truncated in header"; return false; }
-    bool have_cam = false, have_env = false, have_floor = false, have_render = false;
+    bool have_cam = false, have_env = false, have_floor = false, have_render = false, have_section = false;
+    SectionPlane section;
     std::vector<Mesh> meshes;
     std::vector<Instance> instances;
     scene = Scene();
@@ -255,6 +256,13 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             }
             r.pos += n;
             scene.bitmaps.push_back(std::move(img));
+        } else if (is("SECT")) {  // rsb.rs:1070 parse_section
+            if (dup(have_section)) return false;
+            uint32_t flags;
+            Vec3 normal;
+            float distance;
+            if (!(r.u32(flags) && r.vec3(normal) && r.f32(distance))) return false;
+            if (!SectionPlane::make(normal, distance, (flags & 1u) != 0, section)) return r.invalid("section normal is zero");
         } else if (is("FLOR")) {
             if (dup(have_floor)) return false;
             Floor& f = scene.floor;
@@ -281,7 +289,7 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
             if (s.max_seconds < 0.0f || s.clamp_indirect < 0.0f) return r.invalid("max_seconds and clamp_indirect must not be negative");
 
         } else {
-            static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "SECT", "GLAS",
+            static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "GLAS",
                                                  "WETP", "WETF", "WTP2", "WETG", "NEST"};
             for (const char* t : feature_tags)
                 if (is(t)) { error = std::string("unsupported: RSB section ") + t; return false; }
@@ -319,6 +327,12 @@ bool read_rsb(const uint8_t* bytes, size_t len, Scene& scene, std::string& error
     }
     const char* e = Geometry::make(scene.geometry, std::move(meshes), std::move(instances));
     if (*e) { error = e; return false; }
+    if (have_section) {  // Scene::apply_section (scene/mod.rs:1092-1111): a thin wall has no inside to cap
+        std::vector<bool> capped;
+        for (const Instance& in : scene.geometry.instances)
+            capped.push_back((scene.materials[in.material_id].flags & MATERIAL_FLAG_THIN) == 0);
+        scene.geometry.set_section(&section, capped);
+    }
     return true;
 }
 

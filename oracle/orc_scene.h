@@ -113,7 +113,8 @@ struct Scene {
 };
 // Parses the RSB subset (CAMR, MESH, MATL, LGHT, ENVR, FLOR, RNDR, INST; unknown tags skipped).
 // Sections of features outside the path tracer's core (LENS, BMAP, PATN, IMGS, PROG, FXAM,
-// SECT, GLAS, WET*, NEST, IESP) and scene values that need them are refused with a message.
+// GLAS, WET*, NEST) and scene values that need them are refused with a message; SECT (the section
+// view) and IESP (IES profiles) are read.
 bool read_rsb(const uint8_t* bytes, size_t len, Scene& out, std::string& error);
 
 // ---- environment.rs: the dome / flat ramp ------------------------------------------------------

@@ -21,6 +21,8 @@ its path tracer, read from the reference's own source tree (run where it is chec
   script as test inputs) and their pinned 4-spp film hashes (render/k3_tests.rs:17-22);
 * the hashes of the denoised example: the full filter at 4 spp and the viewport's at 2 and 4 spp
   (engine/crates/rt-post/src/denoise/tests.rs:392, 527-528).
+* the Q1 section view (tests/fixtures/q1.rsb, copied beside this script as a test input) and its
+  pinned 4-spp film hash (render/section_tests.rs:11);
 * the hashes of the exact passes and the 4-sample albedo and alpha of the example and the E5 example
   (engine/crates/rt-core/src/render/passes_tests.rs:365-398, 865-868);
 * the golden TIFF and DNG files the reference's writers must reproduce byte for byte
@@ -107,6 +109,9 @@ def main():
     (OUT.parent / "tiff").mkdir(exist_ok=True)
     for name in TIFF_GOLDEN:
         (OUT.parent / "tiff" / name).write_bytes((REF / "tests" / "fixtures" / "tiff" / name).read_bytes())
+    # The Q1 parity scene: E5 cut in two by a capped section, the floor exempt from it.
+    (OUT.parent / "q1.rsb").write_bytes((REF / "tests" / "fixtures" / "q1.rsb").read_bytes())
+    pins["q1_section_4spp"] = pinned((CORE / "render" / "section_tests.rs").read_text(), "PINNED_Q1_SECTION_4SPP")
     passes_src = (CORE / "render" / "passes_tests.rs").read_text()
     pass_keys = ("albedo", "normal", "depth", "part_id", "material_id", "coc")
     passes = {
