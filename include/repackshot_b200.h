@@ -41,12 +41,13 @@ extern "C" {
 uint32_t rtg_version(void);
 
 /* Bits of rtg_features (rt-core/src/lib.rs:76-150 FEATURE_*; the same values). */
+#define RTG_FEATURE_SECTION 4u  /* Q1: the section view (SECT), caps of the cut solids */
 #define RTG_FEATURE_IES 8u      /* L5: IES lights (LGHT kind 5, IESP sections) */
 #define RTG_FEATURE_CAMERAS 16u /* K3: panoramic projections, the exterior factor, instances hidden to the camera */
 
 /* rt_features (ffi.rs:22, lib.rs:159 FEATURES): what this engine reads beyond the RSB every engine
- * reads, as the reference's FEATURE_* bits: RTG_FEATURE_IES | RTG_FEATURE_CAMERAS. The other bits
- * (textures, material programs, section views, pattern nodes, drops, front glass, weather, nested
+ * reads, as the reference's FEATURE_* bits: RTG_FEATURE_SECTION | RTG_FEATURE_IES | RTG_FEATURE_CAMERAS.
+ * The other bits (textures, material programs, pattern nodes, drops, front glass, weather, nested
  * dielectrics) are clear: those sections are refused at load, so a host writes none of them. */
 uint32_t rtg_features(void);
 
@@ -54,9 +55,10 @@ uint32_t rtg_features(void);
  * bytes), builds its BVHs and uploads it. Returns a handle > 0, or 0 after recording the error
  * (rtg_scene_error_len / _copy). Lights of kinds 0-5 (rect, disk, sun, point, spot, IES) and
  * emissive meshes, HDRI environments and background images (BMAP sections: 8-bit sRGB, linear f32,
- * Radiance files), the classic and the physical sky, panoramic cameras, cut-outs and thin walls
- * render; features outside the path tracer's core (textures, material programs, lens optics,
- * particles, section views, front glass, weather, nested dielectrics, OpenEXR bitmaps, scattering
+ * Radiance files), the classic and the physical sky, panoramic cameras, cut-outs, thin walls and
+ * section views (SECT: the model cut by a plane, closed solids capped, the studio exempt) render;
+ * features outside the path tracer's core (textures, material programs, lens optics,
+ * particles, front glass, weather, nested dielectrics, OpenEXR bitmaps, scattering
  * media, dispersive glass, bevels, caustic photon maps, the shadow catcher) are refused with a
  * message that starts with "unsupported:". */
 uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len);

@@ -448,7 +448,7 @@ def tile_alpha(handle: int, x: int, y: int, w: int, h: int, sample_index: int):
     return st, out[:w * h]
 
 
-FEATURE_IES, FEATURE_CAMERAS = 8, 16
+FEATURE_SECTION, FEATURE_IES, FEATURE_CAMERAS = 4, 8, 16
 
 
 def encode_planes(rgb: np.ndarray, weight: np.ndarray, ev: float, tonemap: int, bits: int) -> np.ndarray:
@@ -468,7 +468,8 @@ def encode_planes(rgb: np.ndarray, weight: np.ndarray, ev: float, tonemap: int, 
 
 
 def features() -> int:
-    """rt_features: the reference's FEATURE_* bits this engine reads (IES lights, interior cameras)."""
+    """rt_features: the reference's FEATURE_* bits this engine reads (section views, IES lights, interior
+    cameras)."""
     return int(lib().rtg_features())
 
 

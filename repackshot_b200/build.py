@@ -38,7 +38,7 @@ for _name in ("RTG_SHADE_MIN_BLOCKS", "RTG_SHORT_STACK", "RTG_LEAF_STEP", "RTG_T
         DEVICE_FLAGS.append(f"-D{_name}={os.environ[_name]}")
 HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-pthread", f"-I{CUDA_HOME}/include"]
 
-HOST_SOURCES = ["rtg_scene.cpp", "rtg_bitmap.cpp", "rtg_ies.cpp", "rtg_tables.cpp", "rtg_energy.cpp", "rtg_adaptive.cpp", "rtg_engine.cpp"]
+HOST_SOURCES = ["rtg_scene.cpp", "rtg_section.cpp", "rtg_bitmap.cpp", "rtg_ies.cpp", "rtg_tables.cpp", "rtg_energy.cpp", "rtg_adaptive.cpp", "rtg_engine.cpp"]
 DEVICE_SOURCES = ["rtg_kernels.cu", "rtg_noalloc.cu", "rtg_adaptive.cu", "rtg_denoise.cu"]
 
 

@@ -224,7 +224,7 @@ __device__ __forceinline__ void shade_adjoint_slot(const SceneDev& S, const Ligh
         } else {
             HitInfo h;
             uint4 idx;
-            if (!hit_details(S, ro, rd, 1.0e-3f, f_inf(), hit.x, hit.y, h, I, idx)) break;
+            if (!hit_details(S, ro, rd, 1.0e-3f, f_inf(), hit.x, hit.y, __uint_as_float(hit.z), h, I, idx)) break;
             V3 ng = h.geometric, nrm = h.normal;
             if (dot(nrm, ng) < 0.0f) nrm = -nrm;
             if (dot(nrm, rd) >= -1.0e-4f) nrm = ng;

@@ -54,10 +54,12 @@ struct alignas(16) DevInstance {
     float to_world[12];
     uint32_t identity, active, material, mesh;
     uint32_t flags, inside_out, has_normals, tri_base;  // tri_base: first global triangle of its mesh
-    uint32_t tangent_on, passable, emitter, pad2;  // passable: shadow rays cross it (cut-out or thin wall);
-                                                   // emitter: its mesh light's index in lights[] + 1, or 0
+    uint32_t tangent_on, passable, emitter, solid;  // passable: shadow rays cross it (cut-out or thin wall);
+                                                    // emitter: its mesh light's index in lights[] + 1, or 0;
+                                                    // solid: the section caps it, 1 wound outward, 2 inward (0 not)
     float tan_centre[3], tan_axis[3], tan_x[3];
-    float pad3[3];
+    uint32_t exempt;  // the section neither cuts nor caps it (INST flag 2, the studio)
+    float pad3[2];
 };
 
 // One light of the selection (light.rs:300-495): an area light (rect or disk), a sun, a sphere
@@ -162,6 +164,14 @@ struct SceneDev {
     const Bsdf* bsdfs;
     uint32_t tlas_root, n_instances, n_materials, stack_need;
     EnergyTables energy;
+    // The section view (geometry/section.rs): the plane n . p = d removes the side n points to from
+    // every query; with section_cap the closed solids it cuts are capped (their instances' `solid`),
+    // and a point can only be on a cap inside cap_lo..cap_hi (cap_any: some instance is capped). The
+    // exempt instances' world boxes, grown, are 6 floats each (lo, hi).
+    uint32_t section_on, section_cap, cap_any, n_exempt;
+    float section_n[3], section_d;
+    float cap_lo[3], cap_hi[3];
+    const float* exempt_boxes;
 };
 
 }  // namespace rtg

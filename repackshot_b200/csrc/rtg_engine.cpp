@@ -282,6 +282,8 @@ uint32_t upload_shading(const Flat& F, BufSet& set, SceneDev& S) {
     }
     S.plate = nullptr;
     if (F.plate && (st = upload(set, F.plate->texels, S.plate))) return st;
+    S.exempt_boxes = nullptr;
+    if (!F.exempt_boxes.empty() && (st = upload(set, F.exempt_boxes, S.exempt_boxes))) return st;
     RTG_CHECK(cudaMalloc(&set.lights, sizeof(LightsDev)));
     RTG_CHECK(cudaMemcpy(set.lights, &L, sizeof(LightsDev), cudaMemcpyHostToDevice));
     return RTG_STATUS_OK;
@@ -309,6 +311,7 @@ SceneDev compose(const SceneDev& constants, const SceneDev& geom, const SceneDev
     S.positions = geom.positions; S.normals = geom.normals; S.tri_index = geom.tri_index;
     S.tlas_root = geom.tlas_root; S.stack_need = geom.stack_need;
     S.instances = shade.instances; S.materials = shade.materials; S.bsdfs = shade.bsdfs; S.plate = shade.plate;
+    S.exempt_boxes = shade.exempt_boxes;
     S.energy = g_energy;
     S.filter_table = g_filter_table;
     return S;
@@ -831,7 +834,7 @@ extern "C" {
 
 uint32_t rtg_version(void) { return RTG_ABI_VERSION; }
 
-uint32_t rtg_features(void) { return RTG_FEATURE_IES | RTG_FEATURE_CAMERAS; }
+uint32_t rtg_features(void) { return RTG_FEATURE_SECTION | RTG_FEATURE_IES | RTG_FEATURE_CAMERAS; }
 
 uint32_t rtg_scene_load(const uint8_t* bytes, uint32_t len) {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -1062,6 +1065,8 @@ uint32_t rtg_queue_add(uint32_t queue, const uint8_t* bytes, uint32_t len, uint3
     Flat F;
     if (!flatten_scene(hs, F, err, false)) { g_error = err; return RTG_STATUS_BAD_SCENE; }
     if (F.scene.edge_k > 1) { g_error = "unsupported in the batched queue: edge samples"; return RTG_STATUS_BAD_SCENE; }
+    // The queue's traversal reads the shared scene's constants, so a job cannot bring a section.
+    if (F.scene.section_on || sc->S.section_on) { g_error = "unsupported in the batched queue: a section view"; return RTG_STATUS_BAD_SCENE; }
     auto job = std::make_unique<QueueJob>();
     job->constants = F.scene;
     job->shade = F.scene;
@@ -1282,6 +1287,10 @@ uint32_t rtg_render_adjoint(uint32_t scene, uint32_t film, const float* target, 
     }
     if (sc->S.edge_k > 1) {
         g_error = "rtg_render_adjoint: unsupported: edge samples (the replay takes one sample per index)";
+        return RTG_STATUS_BAD_SCENE;
+    }
+    if (sc->S.section_on) {
+        g_error = "rtg_render_adjoint: unsupported: a section view (the replay traces without it)";
         return RTG_STATUS_BAD_SCENE;
     }
     const FilmDev& F = f->dev;

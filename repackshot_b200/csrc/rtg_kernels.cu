@@ -397,7 +397,7 @@ __device__ __forceinline__ bool shade_slot(const SceneDev& S, const LightsDev& L
         } else {
             HitInfo h;
             uint4 idx;
-            if (!hit_details(S, ro, rd, 1.0e-3f, f_inf(), hit.x, hit.y, h, I, idx)) break;
+            if (!hit_details(S, ro, rd, 1.0e-3f, f_inf(), hit.x, hit.y, __uint_as_float(hit.z), h, I, idx)) break;
             // bevel.rs:232 shading_point without a bevel
             V3 ng = h.geometric, nrm = h.normal;
             if (dot(nrm, ng) < 0.0f) nrm = -nrm;
@@ -652,6 +652,47 @@ __global__ void RTG_TRACE_BOUNDS k_shadow(SceneDev S, PathBuffers P, const uint3
     if (err) atomicOr(&P.counters[3], err);
 }
 
+// ---- the section view: k_extend and k_shadow through the section's queries (geometry/section.rs) -------
+// One ray per thread: a query may be several traversals (the kept part, the cap's probe beyond the
+// plane, the studio on the removed side), so the lane refill of the plain kernels does not apply.
+// Launched instead of them for a scene with a section; they write the same records (a cap is a hit
+// with triangle CAP_TRIANGLE).
+__global__ void __launch_bounds__(TRACE_THREADS) k_extend_section(SceneDev S, PathBuffers P, int cur, const uint32_t* __restrict__ order) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const uint32_t n = *(volatile uint32_t*)&P.counters[cur];
+    uint32_t err = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = order[i];
+        const float4 o = P.o[slot], d = P.d[slot];
+        const uint32_t pf = P.flags[slot];
+        TraceResult res;
+        const bool got = !(pf & PF_NOTHING) &&
+                         trace_q<false>(S, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, f_inf(), (pf & PF_PRIMARY) != 0, res, &err, stack);
+        P.hit[slot] = got ? make_uint4(res.inst, res.tri, __float_as_uint(res.t), 1u) : make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+        const uint32_t key = material_key(S, got, got ? res.inst : 0u);
+        P.key[slot] = key;
+        warp_count(P.bins, key);
+    }
+    if (err) atomicOr(&P.counters[3], err);
+}
+
+__global__ void __launch_bounds__(TRACE_THREADS) k_shadow_section(SceneDev S, PathBuffers P, const uint32_t* __restrict__ perm) {
+    __shared__ uint64_t s_stack[SHORT_STACK * TRACE_THREADS];
+    uint64_t deep[STACK_CAP - SHORT_STACK];
+    SplitStack stack{s_stack + threadIdx.x, deep, TRACE_THREADS};
+    const uint32_t n = *(volatile uint32_t*)&P.counters[2];
+    uint32_t err = 0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t ray = perm ? perm[j] : j;
+        const float4 o = P.sh_o[ray], d = P.sh_d[ray];
+        TraceResult unused;
+        if (!trace_q<true>(S, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), 1.0e-3f, o.w, false, unused, &err, stack)) shadow_unblocked(P, ray);
+    }
+    if (err) atomicOr(&P.counters[3], err);
+}
+
 // ---- shadow walk: shadow rays through cut-outs and thin walls (integrator/mod.rs:629-690) ------------
 // Nearest hits along the ray: a passable surface multiplies what arrives by its straight
 // transmittance (a thin wall's) times its opacity plus 1 - opacity, and the ray goes on from just
@@ -683,12 +724,12 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_shadow_walk(SceneDev S, PathB
         bool arrives = false;
         for (uint32_t k = 0; k < 32; ++k) {  // MAX_SHADOW_CROSSINGS
             TraceResult res;
-            if (!traverse<false>(J, o, d, 1.0e-3f, tmax, false, res, &err, stack)) { arrives = true; break; }
+            if (!trace_q<false>(J, o, d, 1.0e-3f, tmax, false, res, &err, stack)) { arrives = true; break; }
             if (res.inst >= J.n_instances || !J.instances[res.inst].passable) break;
             HitInfo h;
             uint4 idx;
             const DevInstance* I = nullptr;
-            if (!hit_details(J, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, h, I, idx)) break;
+            if (!hit_details(J, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, res.t, h, I, idx)) break;
             const uint32_t m = I->material;
             const float opacity = rclamp(J.materials[m].opacity, 0.0f, 1.0f);
             keep = keep * (straight_transmittance(J.bsdfs[2 * m], dot(h.geometric, d)) * opacity + splat(1.0f - opacity));
@@ -866,7 +907,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_edge_exact(SceneDev S, const 
         V3 o, d;
         const bool sees = camera_ray_at(S, ((float)x + 0.5f) / (float)S.width, ((float)y + 0.5f) / (float)S.height, 0.0f, 0.0f, o, d);
         TraceResult res;
-        const bool got = sees && traverse<false>(S, o, d, 1.0e-3f, f_inf(), true, res, &err, stack);
+        const bool got = sees && trace_q<false>(S, o, d, 1.0e-3f, f_inf(), true, res, &err, stack);
         const float t_geometry = got ? res.t : f_inf();
         float t_floor = f_inf();
         if (S.floor_mode == 1 && d.z != 0.0f && sees) {
@@ -884,7 +925,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_edge_exact(SceneDev S, const 
                 HitInfo h;
                 uint4 idx;
                 const DevInstance* I = nullptr;
-                ok = hit_details(S, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, h, I, idx) && I != nullptr;
+                ok = hit_details(S, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, res.t, h, I, idx) && I != nullptr;
                 if (ok) {
                     e.x = res.inst + 1u;
                     e.y = I->material < S.n_materials ? I->material + 1u : 0u;
@@ -911,7 +952,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_edge_exact(SceneDev S, const 
 __device__ void first_hit_passes(const SceneDev& S, const LightsDev& L, V3 o, V3 d, bool sees, SplitStack& stack, uint32_t* err, uint4& e,
                                  V3& normal, Rgb& albedo) {
     TraceResult res;
-    const bool got = sees && traverse<false>(S, o, d, 1.0e-3f, f_inf(), true, res, err, stack);
+    const bool got = sees && trace_q<false>(S, o, d, 1.0e-3f, f_inf(), true, res, err, stack);
     const float t_geometry = got ? res.t : f_inf();
     float t_floor = f_inf();
     if (S.floor_mode == 1 && d.z != 0.0f && sees) {
@@ -932,7 +973,7 @@ __device__ void first_hit_passes(const SceneDev& S, const LightsDev& L, V3 o, V3
         HitInfo h;
         uint4 idx;
         const DevInstance* I = nullptr;
-        if (!(hit_details(S, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, h, I, idx) && I != nullptr)) return;
+        if (!(hit_details(S, o, d, 1.0e-3f, f_inf(), res.inst, res.tri, res.t, h, I, idx) && I != nullptr)) return;
         e.x = res.inst + 1u;
         const bool known = I->material < S.n_materials;
         e.y = known ? I->material + 1u : 0u;
@@ -1058,7 +1099,7 @@ __global__ void k_albedo_hits(SceneDev S, const LightsDev* __restrict__ Lg, Wave
                 HitInfo h;
                 uint4 idx;
                 const DevInstance* I = nullptr;
-                if (hit_details(S, o, d, 1.0e-3f, f_inf(), hit.x, hit.y, h, I, idx) && I != nullptr) {
+                if (hit_details(S, o, d, 1.0e-3f, f_inf(), hit.x, hit.y, __uint_as_float(hit.z), h, I, idx) && I != nullptr) {
                     if (I->material < S.n_materials) {
                         const float* b = S.materials[I->material].base;
                         a = make_float4(b[0], b[1], b[2], 0.0f);
@@ -1206,9 +1247,9 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_batch(SceneDev S, const
         TraceResult res;
         V3 o = v3(r[0], r[1], r[2]), d = v3(r[3], r[4], r[5]);
         if (mode & 2u) {
-            out[i] = traverse<true>(S, o, d, r[6], r[7], (mode & 1u) != 0, res, &err, stack) ? 1u : 0u;
+            out[i] = trace_q<true>(S, o, d, r[6], r[7], (mode & 1u) != 0, res, &err, stack) ? 1u : 0u;
         } else {
-            bool got = traverse<false>(S, o, d, r[6], r[7], (mode & 1u) != 0, res, &err, stack);
+            bool got = trace_q<false>(S, o, d, r[6], r[7], (mode & 1u) != 0, res, &err, stack);
             out[3 * i] = got ? res.inst : 0xffffffffu;
             out[3 * i + 1] = got ? res.tri : 0xffffffffu;
             out[3 * i + 2] = got ? __float_as_uint(res.t) : 0u;
@@ -1261,7 +1302,10 @@ static void launch_traversal(const RaySort& order, int grid, cudaStream_t st, vo
 }
 
 // Whether a wave's last rounds run in k_tail: a limit set, no shadow walks, not batched.
-static bool tail_on(const SceneDev& S, const RaySort& order, bool batch) { return order.tail_paths > 0 && !S.any_passable && !batch; }
+// The tail traces with the plain traversal: scenes with passable surfaces or a section keep the wavefront.
+static bool tail_on(const SceneDev& S, const RaySort& order, bool batch) {
+    return order.tail_paths > 0 && !S.any_passable && !S.section_on && !batch;
+}
 
 uint32_t wave_launches(const SceneDev& S, const RaySort& order, const PathBuffers& P, bool batch) {
     const uint32_t rounds = wave_rounds(S);
@@ -1302,10 +1346,10 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
         }
         if (timing && timing->ev_count + 2 <= WaveTiming::MAX_EVENTS) {
             cudaEventRecord(timing->ev[timing->ev_count++], st);
-            launch_traversal(order, g_ext, st, k_extend, S, P, cur, traced);
+            launch_traversal(order, g_ext, st, S.section_on ? k_extend_section : k_extend, S, P, cur, traced);
             cudaEventRecord(timing->ev[timing->ev_count++], st);
         } else {
-            launch_traversal(order, g_ext, st, k_extend, S, P, cur, traced);
+            launch_traversal(order, g_ext, st, S.section_on ? k_extend_section : k_extend, S, P, cur, traced);
         }
         if (round == 0 && w.alb && film && !batch) k_albedo_hits<<<g, 256, 0, st>>>(S, L, w, P);
         k_scan<<<1, 32, 0, st>>>(P);
@@ -1329,7 +1373,7 @@ void launch_wave(const SceneDev& S, const LightsDev* L, const WaveDesc& w, const
             k_key_scatter<<<g, 256, 0, st>>>(nullptr, P.sh_key, P.sbins + nk, &P.counters[2], P.queue[cur]);
             perm = P.queue[cur];
         }
-        if (!S.any_passable) launch_traversal(order, g_sh, st, k_shadow, S, P, perm);
+        if (!S.any_passable) launch_traversal(order, g_sh, st, S.section_on ? k_shadow_section : k_shadow, S, P, perm);
         else if (batch) k_shadow_walk<true><<<g, TRACE_THREADS, 0, st>>>(S, P, w, perm);
         else k_shadow_walk<false><<<g, TRACE_THREADS, 0, st>>>(S, P, w, perm);
         k_next_round<<<1, 1, 0, st>>>(P, cur);

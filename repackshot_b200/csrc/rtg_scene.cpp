@@ -86,7 +86,7 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
     std::memcpy(&header_len, bytes + 4, 4);
     size_t pos = 8 + (size_t)header_len;
     if (pos > len) { error = "RSB file is truncated in header"; return false; }
-    bool seen_cam = false, seen_env = false, seen_floor = false, seen_render = false;
+    bool seen_cam = false, seen_env = false, seen_floor = false, seen_render = false, seen_section = false;
     while (pos < len) {
         if (len - pos < 8) { error = "RSB file is truncated in section header"; return false; }
         const uint8_t* tag = bytes + pos;
@@ -204,6 +204,18 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             }
             r.pos += n;
             s.bitmaps.push_back(std::move(img));
+        } else if (is("SECT")) {  // rsb.rs:1070 parse_section, geometry/section.rs:69 SectionPlane::new
+            if (!once(seen_section)) return false;
+            uint32_t flags;
+            V3 n;
+            float d;
+            if (!(r.u32(flags) && r.vec3(n) && r.f32(d))) return false;
+            const float length = std::sqrt(len2(n));
+            if (!(std::isfinite(length) && length > 0.0f)) return r.invalid("section normal is zero");
+            s.section_on = 1;
+            s.section_cap = (flags & 1u) != 0;
+            s.section_n = absf(length - 1.0f) <= 1.0e-6f ? n : n * (1.0f / length);
+            s.section_d = d;
         } else if (is("FLOR")) {
             if (!once(seen_floor)) return false;
             if (!(r.u32(s.floor_mode) && r.f32(s.floor_z) && r.f3(s.floor_color))) return false;
@@ -231,7 +243,7 @@ bool parse_rsb(const uint8_t* bytes, size_t len, HScene& s, std::string& error, 
             if (s.max_seconds < 0.0f || s.clamp_indirect < 0.0f) return r.invalid("max_seconds and clamp_indirect must not be negative");
 
         } else {
-            static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM", "SECT",
+            static const char* feature_tags[] = {"LENS", "PATN", "IMGS", "PROG", "FXAM",
                                                  "GLAS", "WETP", "WETF", "WTP2", "WETG", "NEST"};
             for (const char* t : feature_tags)
                 if (is(t)) { error = std::string("unsupported: RSB section ") + t; return false; }
@@ -1219,6 +1231,45 @@ bool flatten_scene(const HScene& s, Flat& F, std::string& error, bool geometry) 
     S.background = s.background_mode == 1 ? 1 : s.background_mode == 2 ? 2 : s.background_mode == 3 ? (F.plate ? 3 : 1) : 0;
     for (int c = 0; c < 3; ++c) S.background_color[c] = rmax(s.background_color[c], 0.0f);
     for (const DevInstance& d : F.instances) S.any_passable |= d.passable;
+    // The section view (geometry/section.rs:180-222, scene/mod.rs:1092-1111): per instance whether
+    // the plane caps it (a closed solid that is live, not exempt and not a thin wall) or leaves it
+    // alone (the studio), the grown box where caps can be, and the exempt instances' grown boxes.
+    F.exempt_boxes.clear();
+    if (s.section_on) {
+        S.section_on = 1;
+        S.section_cap = s.section_cap;
+        S.section_n[0] = s.section_n.x; S.section_n[1] = s.section_n.y; S.section_n[2] = s.section_n.z;
+        S.section_d = s.section_d;
+        auto grown = [](Box b) {
+            const V3 d = b.hi - b.lo;
+            const float pad = rmax(rmax(d.x, d.y), d.z) * 1.0e-5f + 1.0e-4f;
+            b.lo = b.lo - v3(pad, pad, pad);
+            b.hi = b.hi + v3(pad, pad, pad);
+            return b;
+        };
+        std::vector<int> solid(s.meshes.size(), -1);  // per mesh, analysed on first use
+        Box caps;
+        for (size_t i = 0; i < ni; ++i) {
+            const HInstance& in = s.instances[i];
+            const HMesh& M = s.meshes[in.mesh];
+            DevInstance& d = F.instances[i];
+            const bool exempt = (in.flags & 2u) != 0;
+            if (exempt && d.active) {
+                d.exempt = 1;
+                const Box b = grown(instance_box(M, xf_of(in.rows)));
+                F.exempt_boxes.insert(F.exempt_boxes.end(), {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z});
+            }
+            const bool thin = (s.materials[in.material_id].flags & MATERIAL_FLAG_THIN) != 0;
+            if (!(s.section_cap && !exempt && !thin && d.active)) continue;
+            if (solid[in.mesh] < 0) solid[in.mesh] = (int)solid_of(M);
+            d.solid = (uint32_t)solid[in.mesh];
+            if (d.solid) caps = caps.uni(grown(instance_box(M, xf_of(in.rows))));
+        }
+        S.cap_any = !caps.empty();
+        S.cap_lo[0] = caps.lo.x; S.cap_lo[1] = caps.lo.y; S.cap_lo[2] = caps.lo.z;
+        S.cap_hi[0] = caps.hi.x; S.cap_hi[1] = caps.hi.y; S.cap_hi[2] = caps.hi.z;
+        S.n_exempt = (uint32_t)(F.exempt_boxes.size() / 6);
+    }
     for (const HInstance& in : s.instances) {
         const HMaterial& m = s.materials[in.material_id];
         if (m.kind != MATERIAL_EMISSIVE && m.opacity < 1.0f) S.any_cutout = 1;

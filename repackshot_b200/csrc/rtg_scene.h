@@ -38,6 +38,9 @@ struct HMesh {
     bool empty_bounds = true, inside_out = false;
     size_t triangles() const { return indices.size() / 3; }
 };
+// geometry/solid.rs: what a mesh is as a solid, 0 open, 1 closed and wound outward, 2 inward.
+uint32_t solid_of(const HMesh& m);
+
 struct HInstance {
     uint32_t mesh = 0;
     float rows[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
@@ -80,6 +83,10 @@ struct HScene;
 HImage sky_image(const HScene& s);
 struct HScene {
     V3 cam_position{0, -1000, 0}, cam_target{0, 0, 0}, cam_up{0, 0, 1};
+    // SECT (Q1): the section plane section_n . p = section_d, normalised as SectionPlane::new does.
+    uint32_t section_on = 0, section_cap = 0;
+    V3 section_n{0, 0, 1};
+    float section_d = 0;
     float focal_mm = 50, sensor_mm = 36, fstop = 0, focus_dist = 1000, ortho_width = 1000;
     uint32_t ortho = 0, projection = 0;
     float fov_x = 360, fov_y = 180, exterior = 1;
@@ -129,6 +136,7 @@ struct Flat {
     HImage sky;  // the tabulated sky of a sky environment
     std::vector<float> ies_data;  // per IES light: vertical angles, horizontal angles, candela
     std::vector<float> mesh_light_data;  // per mesh light's triangle: 16 floats (LightDev::tris)
+    std::vector<float> exempt_boxes;     // the section's exempt instances: grown world box lo, hi
     const HImage* env_image = nullptr;
     const HImage* plate = nullptr;
     std::vector<QNode> nodes;

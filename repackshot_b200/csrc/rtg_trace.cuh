@@ -362,19 +362,192 @@ RTG_D bool traverse(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, bool 
     return hit;
 }
 
+// ---- the section view (geometry/section.rs:127-448) --------------------------------------------------
+// A query of a scene with a section sees the model as if the side of the plane its normal points to
+// were empty: the ray is clipped to the interval where it is on the kept side; where it crosses the
+// plane inside a closed solid (the next surface along it is met from behind) it hits the solid's cap
+// on the plane; and the studio instances (exempt from the section) are found on the removed side by
+// stepping over the cut model's surfaces, at most 48 deep.
+constexpr uint32_t CAP_TRIANGLE = 0xffffffffu;  // the `tri` of a hit on a cap
+constexpr int SECTION_MAX_SKIPS = 48;
+enum : int { SPAN_REMOVED = 0, SPAN_WHOLE = 1, SPAN_ENTERS = 2, SPAN_LEAVES = 3 };
+
+RTG_D int section_span(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, float& t) {
+    const V3 n = v3(S.section_n[0], S.section_n[1], S.section_n[2]);
+    const float from_plane = dot(n, o) - S.section_d;
+    const float towards = dot(n, d);
+    if (towards == 0.0f) return from_plane <= 0.0f ? SPAN_WHOLE : SPAN_REMOVED;
+    t = -from_plane / towards;
+    if (towards > 0.0f) return t < tmin ? SPAN_REMOVED : (t >= tmax ? SPAN_WHOLE : SPAN_LEAVES);
+    return t <= tmin ? SPAN_WHOLE : (t > tmax ? SPAN_REMOVED : SPAN_ENTERS);
+}
+
+RTG_D bool section_may_cap(const SceneDev& S, V3 p) {
+    return S.cap_any && p.x >= S.cap_lo[0] && p.x <= S.cap_hi[0] && p.y >= S.cap_lo[1] && p.y <= S.cap_hi[1] &&
+           p.z >= S.cap_lo[2] && p.z <= S.cap_hi[2];
+}
+
+RTG_D bool section_hidden(const SceneDev& S, bool camera, uint32_t inst) {
+    return camera && inst < S.n_instances && (S.instances[inst].flags & 4u) != 0;  // INSTANCE_NO_CAMERA
+}
+
+// True when triangle `tri` of capped instance `inst` is met by direction d from inside its solid.
+RTG_D bool section_met_from_inside(const SceneDev& S, V3 d, uint32_t inst, uint32_t tri) {
+    if (inst >= S.n_instances) return false;
+    const DevInstance* I = S.instances + inst;
+    if (!I->active || I->solid == 0u) return false;
+    const uint4 idx = __ldg(S.tri_index + I->tri_base + tri);
+    const float4 q0 = __ldg(S.positions + idx.x), q1 = __ldg(S.positions + idx.y), q2 = __ldg(S.positions + idx.z);
+    const V3 p0 = v3(q0.x, q0.y, q0.z), p1 = v3(q1.x, q1.y, q1.z), p2 = v3(q2.x, q2.y, q2.z);
+    V3 w = cross(p1 - p0, p2 - p0);
+    if (!I->identity) w = xf_transpose(I->to_local, w);
+    const bool front = dot(w, d) < 0.0f;
+    return I->solid == 1u ? !front : front;
+}
+
+// The first exempt instance within [near, far], stepping over the others' surfaces.
+template <class Stack>
+RTG_D bool section_first_exempt(const SceneDev& S, V3 o, V3 d, float near, float far, bool camera, TraceResult& res,
+                                uint32_t* err, Stack& stack) {
+    float t = near;
+    for (int k = 0; k < SECTION_MAX_SKIPS; ++k) {
+        TraceResult h;
+        if (!traverse<false>(S, o, d, t, far, camera, h, err, stack)) return false;
+        if (h.inst < S.n_instances && S.instances[h.inst].exempt) { res = h; return true; }
+        t = __uint_as_float(__float_as_uint(fmaxf(h.t, 0.0f)) + 1u);  // strictly past the surface
+        if (t > far) return false;
+    }
+    return false;
+}
+
+// The nearest exempt hit within [from, to] (a removed part of the ray's range), looked for inside
+// each exempt instance's box only (Aabb::intersect, math.rs:388).
+template <class Stack>
+RTG_D bool section_exempt_in(const SceneDev& S, V3 o, V3 d, float from, float to, bool camera, TraceResult& res, uint32_t* err,
+                             Stack& stack) {
+    if (S.n_exempt == 0u || from != from || to != to || from > to) return false;
+    const float inv[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z}, org[3] = {o.x, o.y, o.z};
+    bool found = false;
+    for (uint32_t b = 0; b < S.n_exempt; ++b) {
+        const float* box = S.exempt_boxes + 6 * b;
+        const float end = found ? fminf(res.t, to) : to;
+        float near = from, far = end;
+        for (int a = 0; a < 3; ++a) {
+            const float x = (__ldg(box + a) - org[a]) * inv[a], y = (__ldg(box + 3 + a) - org[a]) * inv[a];
+            if (x != x || y != y) continue;  // parallel to the slab, on its boundary
+            near = fmaxf(near, fminf(x, y));
+            far = fminf(far, fmaxf(x, y));
+        }
+        if (!(near <= far && near < f_inf())) continue;
+        TraceResult h;
+        if (section_first_exempt(S, o, d, near, fminf(far, end), camera, h, err, stack) && (!found || h.t < res.t)) {
+            res = h;
+            found = true;
+        }
+    }
+    return found;
+}
+
+// The cap at t where the ray leaves the kept side having hit nothing: there when the next surface of
+// the whole model beyond the plane is met from inside its solid.
+template <class Stack>
+RTG_D bool section_cap_beyond(const SceneDev& S, V3 o, V3 d, float t, TraceResult& res, uint32_t* err, Stack& stack) {
+    if (!S.section_cap || !section_may_cap(S, o + d * t)) return false;
+    TraceResult h;
+    if (!traverse<false>(S, o, d, t, f_inf(), false, h, err, stack)) return false;
+    if (!section_met_from_inside(S, d, h.inst, h.tri)) return false;
+    res.inst = h.inst;
+    res.tri = CAP_TRIANGLE;
+    res.t = t;
+    return true;
+}
+
+// Geometry::trace_sectioned / occluded_sectioned (section.rs:224-324). Out of line: scenes without
+// a section never call it, and the kernels that can keep their registers for the plain traversal.
+template <bool ANY, class Stack>
+RTG_D_NI bool section_query(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, bool camera, TraceResult& res,
+                            uint32_t* err, Stack& stack) {
+    float t = 0.0f;
+    const int span = section_span(S, o, d, tmin, tmax, t);
+    TraceResult other;
+    if (ANY) {
+        switch (span) {
+            case SPAN_REMOVED: return section_exempt_in(S, o, d, tmin, tmax, camera, other, err, stack);
+            case SPAN_WHOLE: return traverse<true>(S, o, d, tmin, tmax, camera, res, err, stack);
+            case SPAN_LEAVES:
+                return traverse<true>(S, o, d, tmin, t, camera, res, err, stack) || section_cap_beyond(S, o, d, t, other, err, stack) ||
+                       section_exempt_in(S, o, d, t, tmax, camera, other, err, stack);
+            default:  // the cap of a ray that enters is at the start of what it can hit anyway
+                return traverse<true>(S, o, d, t, tmax, camera, res, err, stack) ||
+                       section_exempt_in(S, o, d, tmin, t, camera, other, err, stack);
+        }
+    }
+    switch (span) {
+        case SPAN_REMOVED: return section_exempt_in(S, o, d, tmin, tmax, camera, res, err, stack);
+        case SPAN_WHOLE: return traverse<false>(S, o, d, tmin, tmax, camera, res, err, stack);
+        case SPAN_LEAVES:
+            // The kept part; else a cap looked for beyond the plane; else the studio beyond it.
+            if (traverse<false>(S, o, d, tmin, t, camera, res, err, stack)) return true;
+            if (section_cap_beyond(S, o, d, t, other, err, stack) && !section_hidden(S, camera, other.inst)) {
+                res = other;
+                return true;
+            }
+            return section_exempt_in(S, o, d, t, tmax, camera, res, err, stack);
+        default: {
+            // The studio on the removed side is nearer than anything on the kept one; then the
+            // nearest surface beyond the plane, whose side tells whether the crossing is a cap.
+            if (section_exempt_in(S, o, d, tmin, t, camera, res, err, stack)) return true;
+            const bool got = traverse<false>(S, o, d, t, tmax, camera, other, err, stack);
+            if (got && S.section_cap && section_may_cap(S, o + d * t) && section_met_from_inside(S, d, other.inst, other.tri) &&
+                !section_hidden(S, camera, other.inst)) {
+                res.inst = other.inst;
+                res.tri = CAP_TRIANGLE;
+                res.t = t;
+                return true;
+            }
+            if (got) res = other;
+            return got;
+        }
+    }
+}
+
+// A whole query through the scene's section when it has one.
+template <bool ANY, class Stack>
+RTG_D bool trace_q(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, bool camera, TraceResult& res, uint32_t* err,
+                   Stack& stack) {
+    if (!S.section_on) return traverse<ANY>(S, o, d, tmin, tmax, camera, res, err, stack);
+    return section_query<ANY>(S, o, d, tmin, tmax, camera, res, err, stack);
+}
+
 struct HitInfo {
     V3 point, normal, geometric;
     float bary[3];
     bool front, outside;
+    bool cap;  // on a section's cap: no triangle, the plane's normal
 };
 
 // geometry/mod.rs:731 hit_details for an instance hit.
-RTG_D_NI bool hit_details(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, uint32_t inst, uint32_t tri, HitInfo& h,
-                       const DevInstance*& I_out, uint4& idx_out) {
+RTG_D_NI bool hit_details(const SceneDev& S, V3 o, V3 d, float tmin, float tmax, uint32_t inst, uint32_t tri, float t_hit,
+                       HitInfo& h, const DevInstance*& I_out, uint4& idx_out) {
     if (inst >= S.n_instances) return false;
     const DevInstance* I = S.instances + inst;
     I_out = I;
     if (!I->active) return false;
+    h.cap = tri == CAP_TRIANGLE;
+    if (h.cap) {  // Section::cap_details (section.rs:424-448): on the plane, facing where the ray came from
+        if (!S.section_on) return false;
+        const V3 n = v3(S.section_n[0], S.section_n[1], S.section_n[2]);
+        const V3 at = o + d * t_hit;
+        h.point = at - n * (dot(n, at) - S.section_d);
+        h.front = dot(n, d) < 0.0f;
+        h.normal = h.front ? n : -n;
+        h.geometric = h.normal;
+        h.bary[0] = 1.0f;
+        h.bary[1] = h.bary[2] = 0.0f;
+        h.outside = h.front;
+        idx_out = make_uint4(0u, 0u, 0u, 0u);
+        return true;
+    }
     uint4 idx = __ldg(S.tri_index + I->tri_base + tri);
     idx_out = idx;
     float4 q0 = __ldg(S.positions + idx.x), q1 = __ldg(S.positions + idx.y), q2 = __ldg(S.positions + idx.z);
@@ -410,7 +583,7 @@ RTG_D_NI bool hit_details(const SceneDev& S, V3 o, V3 d, float tmin, float tmax,
 
 // geometry/mod.rs:682 terminator_point (Hanika 2021).
 RTG_D_NI V3 terminator_point(const SceneDev& S, const DevInstance* I, uint4 idx, const HitInfo& h) {
-    if (!I->has_normals) return h.point;
+    if (h.cap || !I->has_normals) return h.point;
     float4 q[3] = {__ldg(S.positions + idx.x), __ldg(S.positions + idx.y), __ldg(S.positions + idx.z)};
     float4 m[3] = {__ldg(S.normals + idx.x), __ldg(S.normals + idx.y), __ldg(S.normals + idx.z)};
     V3 c[3], n[3];

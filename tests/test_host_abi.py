@@ -61,10 +61,11 @@ def test_version_and_constants(rtg):
 
 
 def test_features_are_the_reference_bits_of_what_loads(rtg):
-    # rt_features (ffi.rs:22): FEATURE_IES = 8 (L5) and FEATURE_CAMERAS = 16 (K3), rt-core lib.rs:93,100;
-    # the texture, program, section, drop, glass, weather and nesting bits stay clear.
-    assert rtg.features() == header_define("RTG_FEATURE_IES") | header_define("RTG_FEATURE_CAMERAS") == 24
-    assert (rtg.FEATURE_IES, rtg.FEATURE_CAMERAS) == (8, 16)
+    # rt_features (ffi.rs:22): FEATURE_SECTION = 4 (Q1), FEATURE_IES = 8 (L5) and FEATURE_CAMERAS = 16
+    # (K3), rt-core lib.rs:88,93,100; the texture, program, drop, glass, weather and nesting bits stay clear.
+    bits = header_define("RTG_FEATURE_SECTION") | header_define("RTG_FEATURE_IES") | header_define("RTG_FEATURE_CAMERAS")
+    assert rtg.features() == bits == 28
+    assert (rtg.FEATURE_SECTION, rtg.FEATURE_IES, rtg.FEATURE_CAMERAS) == (4, 8, 16)
 
 
 def test_bad_handles_and_null_pointers(rtg):
