@@ -74,10 +74,13 @@ def test_the_passes_see_the_cap_as_the_cut_solid(rtg, oracle_lib):
     assert np.array_equal(words[:3 * n], np.ascontiguousarray(normal, np.float32).view(np.uint32).reshape(-1))
     assert np.array_equal(words[3 * n:4 * n], np.ascontiguousarray(depth, np.float32).view(np.uint32).reshape(-1))
     assert np.array_equal(words[4 * n:5 * n], part.reshape(-1))
-    # Pixels of the cap face the camera with the plane's normal (+x: the camera is on the removed side).
+    assert np.array_equal(words[5 * n:6 * n], material.reshape(-1))
+    # section_tests.rs:45-92: the glass sphere (instance 0, id 1 in the pass; 0 is the background) is
+    # seen cut, its cap facing the camera on the removed side with the plane's normal +x, material 1.
     nx = normal.reshape(-1, 3)
-    on_cap = (part.reshape(-1) == 0) & (nx[:, 0] == np.float32(1.0))
-    assert on_cap.sum() > 50
+    on_cap = (part.reshape(-1) == 1) & (np.abs(nx[:, 0] - 1.0) < 1e-5) & (np.abs(nx[:, 1]) < 1e-5) & (np.abs(nx[:, 2]) < 1e-5)
+    assert on_cap.sum() > 500
+    assert (material.reshape(-1)[on_cap] == 1).all()
     for sample in (0, 3):
         st, alb = rtg.tile_albedo(g.handle, 0, 0, w, h, sample)
         assert st == rtg.STATUS_OK
