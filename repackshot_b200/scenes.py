@@ -14,7 +14,7 @@ from __future__ import annotations
 import math
 import struct
 from dataclasses import dataclass, field
-from typing import List, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -138,6 +138,8 @@ class Scene:
     caustic_photons: int = 0  # photons of the caustic maps a sample index (0: none)
     adaptive: int = 0  # bit 0: the host samples adaptively (E10)
     noise_threshold: float = 0.0  # relative error a block stops at (0: none)
+    # SECT (Q1): (flags, normal x, y, z, distance); flags bit 0 caps the cut solids. None: no section.
+    section: Optional[Tuple[int, float, float, float, float]] = None
 
 
 def _sec(tag: bytes, payload: bytes) -> bytes:
@@ -188,6 +190,8 @@ def to_rsb(s: Scene, meshes: bool = True) -> bytes:
                     _u(s.tonemap, s.max_depth) + _f(s.clamp_indirect) + _u(0, 0, s.caustic_photons) + _f(0.0, 1.0) +
                     _u(s.pixel_filter, s.edge_supersample) +
                     (_u(s.adaptive) + _f(s.noise_threshold) if s.adaptive or s.noise_threshold else b"")))
+    if s.section is not None:  # rsb.rs:1884, written only when the scene has one
+        out.append(_sec(b"SECT", _u(s.section[0]) + _f(*s.section[1:])))
     return b"".join(out)
 
 
@@ -493,6 +497,83 @@ def emissive_scene(width: int = 96, height: int = 96, spp: int = 8) -> Scene:
     s.meshes.append(Mesh(q, np.zeros((4, 3), np.float32), np.array([0, 2, 1, 0, 3, 2], np.uint32), 3))
     s.instances += [Instance(2, material_id=2), Instance(3, material_id=3, flags=INSTANCE_ONE_SIDED)]
     return s
+
+
+def box_mesh(lo, hi, material_id: int = 0, inward: bool = False, skip_faces=()) -> Mesh:
+    """An axis-aligned box of 24 vertices (4 per face, each with its face's normal), the faces wound
+    counter-clockwise seen from outside, or from inside with `inward`. `skip_faces` leaves out faces
+    by (axis, side) with side 0 the low face: an open box."""
+    lo, hi = np.asarray(lo, np.float32), np.asarray(hi, np.float32)
+    pos, nrm, idx = [], [], []
+    for axis in range(3):
+        for side in (0, 1):
+            if (axis, side) in skip_faces:
+                continue
+            u, v = (axis + 1) % 3, (axis + 2) % 3
+            corners = []
+            for cu, cv in ((0, 0), (1, 0), (1, 1), (0, 1)):
+                c = np.zeros(3, np.float32)
+                c[axis] = hi[axis] if side else lo[axis]
+                c[u] = hi[u] if cu else lo[u]
+                c[v] = hi[v] if cv else lo[v]
+                corners.append(c)
+            out = np.zeros(3, np.float32)
+            out[axis] = 1.0 if side else -1.0
+            if (np.dot(np.cross(corners[1] - corners[0], corners[2] - corners[0]), out) < 0) != inward:
+                corners.reverse()
+            base = len(pos)
+            pos += corners
+            nrm += [-out if inward else out] * 4
+            idx += [base, base + 1, base + 2, base, base + 2, base + 3]
+    return Mesh(np.array(pos, np.float32), np.array(nrm, np.float32), np.array(idx, np.uint32), material_id)
+
+
+def section_scene(width: int = 96, height: int = 64, spp: int = 4) -> Scene:
+    """A section view that takes every rule of geometry/section.rs: a plane of normal (1, 0.2, 0)
+    (normalised on load) at 10 mm cutting
+    * a closed cube of 24 vertices (closed once welded), rotated 30 degrees and scaled (1.5, 0.8, 1.2):
+      capped;
+    * a cube wound inward: capped, its inside the front of its triangles;
+    * an open box (no top) and a cube of a thin-walled material: cut but never capped;
+    * a cube hidden to the camera: capped for every ray but camera rays;
+    and, exempt from the section (the studio), the floor and a hollow box on the removed side that
+    holds 60 parallel slices of the cut model: a ray looking for the box's wall from behind more
+    than 48 of them gives up."""
+    ang = math.radians(30.0)
+    c, sn = math.cos(ang), math.sin(ang)
+    def placed(scale, t):
+        sx, sy, sz = scale
+        return (c * sx, -sn * sy, 0.0, t[0], sn * sx, c * sy, 0.0, t[1], 0.0, 0.0, sz, t[2])
+    slices_p, slices_i = [], []
+    for k in range(60):  # quads perpendicular to x at x = 210 + 1.5 k
+        x = 210.0 + 1.5 * k
+        b = len(slices_p)
+        slices_p += [(x, -80.0, 10.0), (x, 80.0, 10.0), (x, 80.0, 140.0), (x, -80.0, 140.0)]
+        slices_i += [b, b + 1, b + 2, b, b + 2, b + 3]
+    slices = Mesh(np.array(slices_p, np.float32), np.zeros((len(slices_p), 3), np.float32), np.array(slices_i, np.uint32), 0)
+    return Scene(
+        camera_position=(700.0, -500.0, 420.0), camera_target=(40.0, 0.0, 60.0), focal_mm=35.0, focus_dist=900.0,
+        materials=[Material(base_color=(0.9, 0.45, 0.2), roughness=0.4),
+                   Material(kind=MATERIAL_GLASS, base_color=(0.9, 0.95, 1.0), transmission=1.0, roughness=0.05, ior=1.5),
+                   Material(kind=MATERIAL_GLASS, base_color=(0.9, 0.95, 1.0), transmission=1.0, roughness=0.05, flags=MATERIAL_FLAG_THIN),
+                   Material(base_color=(0.5, 0.5, 0.52), roughness=0.8),
+                   Material(base_color=(0.3, 0.6, 0.3), roughness=0.6)],
+        meshes=[box_mesh((-50, -50, -50), (50, 50, 50)), box_mesh((-50, -50, -50), (50, 50, 50), inward=True),
+                box_mesh((-50, -50, -50), (50, 50, 50), skip_faces=((2, 1),)), floor_quad(0.0, 900.0, 3),
+                box_mesh((200, -100, 0), (320, 100, 150)), slices],
+        instances=[Instance(0, rows=placed((1.5, 0.8, 1.2), (0.0, -140.0, 70.0)), material_id=0),
+                   Instance(1, rows=(0.8, 0, 0, 0.0, 0, 0.8, 0, 0.0, 0, 0, 0.8, 60.0), material_id=1),
+                   Instance(2, rows=(1, 0, 0, 0.0, 0, 1, 0, 140.0, 0, 0, 1, 60.0), material_id=0),
+                   Instance(0, rows=(1, 0, 0, 0.0, 0, 1, 0, 280.0, 0, 0, 1, 60.0), material_id=2),
+                   Instance(0, rows=(1, 0, 0, 60.0, 0, 1, 0, -290.0, 0, 0, 1, 60.0), material_id=4, flags=4),
+                   Instance(3, material_id=3, flags=2),
+                   Instance(4, material_id=4, flags=2),
+                   Instance(5, material_id=0)],
+        lights=[Light(kind=0, position=(200.0, -300.0, 700.0), direction=(-0.2, 0.3, -0.93), up=(0.0, 1.0, 0.0), size_x=300.0,
+                      size_y=300.0, power=6.0)],
+        env_kind=0, env_floor=0.05, env_horizon=0.12, env_zenith=0.3,
+        width=width, height=height, max_samples=spp, seed=3, max_depth=8,
+        section=(1, 1.0, 0.2, 0.0, 10.0))
 
 
 def _value_noise3(p: np.ndarray, seed: int) -> np.ndarray:

@@ -105,3 +105,33 @@ def strip_meshes(rsb: bytes) -> bytes:
         if tag != b"MESH":
             out += rsb[start:at + n]
     return out
+
+
+# ---- the synthetic scene of every rule (repackshot_b200.scenes.section_scene) ---------------------
+
+def test_every_rule_is_the_oracles(rtg, oracle_lib):
+    """Welded, rotated and scaled, inward, open, thin and camera-hidden solids, the studio floor and
+    the studio box behind 60 slices: nearest hits, any-hit answers, the exact passes and a 4-spp film
+    are the oracle's bit for bit."""
+    from repackshot_b200 import scenes
+    rsb = scenes.to_rsb(scenes.section_scene())
+    g, o = rtg.Scene(rsb), oracle_lib.OracleScene(rsb)
+    rays = np.concatenate([random_rays(60000, (-250, -400, 5), (250, 400, 150), seed=41),
+                           random_rays(20000, (200, -100, 0), (320, 100, 150), seed=42)])
+    rays[::5, 7] = np.float32(120.0)
+    for camera in (False, True):
+        want, _ = o.trace(rays, camera=camera)
+        assert np.array_equal(g.trace(rays, camera=camera), want)
+    assert (want[:, 1] == CAP).sum() > 500
+    assert np.array_equal(g.trace(rays, any_hit=True).astype(np.uint8), o.occluded(rays))
+    w, h = g.width, g.height
+    st, words = rtg.tile_passes(g.handle, 0, 0, w, h, 0x3E)
+    assert st == rtg.STATUS_OK
+    normal, depth, part, material = o.passes()
+    n = w * h
+    assert np.array_equal(words[:3 * n], np.ascontiguousarray(normal, np.float32).view(np.uint32).reshape(-1))
+    assert np.array_equal(words[4 * n:5 * n], part.reshape(-1))
+    f = g.film()
+    f.render(0, 4)
+    rgb, wt, _, _, _ = o.render_film(0, 4, threads=16)
+    assert rtg.fnv1a(f.resolve()) == oracle_lib.fnv1a(oracle_lib.resolve(rgb, wt))
