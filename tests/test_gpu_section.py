@@ -135,3 +135,23 @@ def test_every_rule_is_the_oracles(rtg, oracle_lib):
     f.render(0, 4)
     rgb, wt, _, _, _ = o.render_film(0, 4, threads=16)
     assert rtg.fnv1a(f.resolve()) == oracle_lib.fnv1a(oracle_lib.resolve(rgb, wt))
+
+
+def test_an_update_brings_and_takes_the_section(rtg, pins):
+    """rt_scene_update (ffi.rs:68-88, rsb.rs: an update replaces the section; a file without SECT has
+    none): E5 updated with Q1's file without its meshes renders Q1, and back to E5."""
+    from repackshot_b200 import scenes
+    s = rtg.Scene(scenes.to_rsb(scenes.e5_scene()))
+
+    def film():
+        f = s.film()
+        f.render(0, 4)
+        return rtg.fnv1a(f.resolve())
+
+    assert film() == pins["film_hashes"]["e5_hdri_4spp"]
+    s.update(strip_meshes(q1()))
+    assert film() == pins["film_hashes"]["q1_section_4spp"]
+    s.update(strip_meshes(scenes.to_rsb(scenes.e5_scene())))
+    assert film() == pins["film_hashes"]["e5_hdri_4spp"]
+    s.update(strip_meshes(with_section(q1(), None)))
+    assert film() == pins["film_hashes"]["e5_hdri_4spp"]
