@@ -240,6 +240,12 @@ uint32_t rtg_render_paths(uint32_t scene, const uint32_t* xys, uint32_t n, float
  * t bits (instance 0xffffffff: miss). Any: out n u32 = 1 when blocked. */
 uint32_t rtg_trace_rays(uint32_t scene, const float* rays, uint32_t n, uint32_t mode, uint32_t* out);
 
+/* What a mesh is as a solid for the caps of a section view (rt-core/src/geometry/solid.rs analyse):
+ * `positions` 3*n_vertices floats, `indices` n_indices (a multiple of 3) vertex indices. `solid`
+ * gets 0 (open: not capped), 1 (closed, wound counter-clockwise seen from outside) or 2 (closed,
+ * wound inward). The host computation a scene load runs for every capped instance's mesh; no GPU. */
+uint32_t rtg_mesh_solid(const float* positions, uint32_t n_vertices, const uint32_t* indices, uint32_t n_indices, uint32_t* solid);
+
 /* Facts of a loaded scene: width, height, max depth, instanced triangles, BVH nodes, leaf
  * triangles, BVH build seconds, rays cast so far. */
 uint32_t rtg_scene_stats(uint32_t scene, double* out8);

@@ -47,6 +47,7 @@ def lib():
             "orc_fmath": (None, [u32, v, u32, v]),
             "orc_film_encode": (None, [v, v, u32, ctypes.c_float, u32, v, v]),
             "orc_film_linear": (None, [v, v, u32, ctypes.c_float, v]),
+            "orc_mesh_solid": (u32, [v, u32, v, u32]),
             "orc_color": (None, [u32, v, u32, v]),
             "orc_agx_identity": (None, [v]),
             "orc_light_count": (u32, [u32]),
@@ -404,6 +405,13 @@ def film_linear(rgb, weight, ev):
     out = np.zeros(3 * n, np.float32)
     lib().orc_film_linear(_p(rgb), _p(weight), n, ev, _p(out))
     return out.reshape(n, 3)
+
+
+def mesh_solid(positions, indices):
+    """solid.rs analyse of a mesh: 0 open, 1 closed and wound outward, 2 inward."""
+    p = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    return int(lib().orc_mesh_solid(_p(p), len(p), _p(i), len(i)))
 
 
 def color(which, xs):

@@ -375,3 +375,16 @@ bool Geometry::occluded(const Ray& ray, bool camera, TraceStats* st) const {
 }
 
 }  // namespace orc
+
+// analyse_solid of a mesh given as arrays: 0 open, 1 outward, 2 inward; 0xffffffff when the mesh is
+// invalid (an index out of range, a non-finite position).
+extern "C" uint32_t orc_mesh_solid(const float* positions, uint32_t n_vertices, const uint32_t* indices, uint32_t n_indices) {
+    using namespace orc;
+    std::vector<Vec3> p(n_vertices), n(n_vertices, Vec3(0, 0, 0));
+    for (uint32_t v = 0; v < n_vertices; ++v) p[v] = Vec3(positions[3 * v], positions[3 * v + 1], positions[3 * v + 2]);
+    std::vector<uint32_t> idx(indices, indices + n_indices);
+    Mesh m;
+    if (*Mesh::make(m, p, n, idx, 0)) return 0xffffffffu;
+    const Solid s = analyse_solid(m);
+    return s == Solid::Open ? 0u : s == Solid::Outward ? 1u : 2u;
+}

@@ -62,6 +62,7 @@ ABI = {
     "rtg_film_srgb16": (_u32, [_u32, ctypes.c_float, _u32, _f]),
     "rtg_film_linear": (_u32, [_u32, ctypes.c_float, _f]),
     "rtg_encode_planes": (_u32, [_f, _f, _u32, _u32, ctypes.c_float, _u32, _u32, _f]),
+    "rtg_mesh_solid": (_u32, [_f, _u32, _f, _u32, _f]),
     "rtg_scene_output": (_u32, [_u32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "rtg_film_read": (_u32, [_u32, _f, _f, _f, _f]),
     "rtg_film_device": (_u32, [_u32, _f, _f, _f, _f]),
@@ -465,6 +466,15 @@ def encode_planes(rgb: np.ndarray, weight: np.ndarray, ev: float, tonemap: int, 
     out = np.zeros((h, w, 3), dtype)
     _check(lib().rtg_encode_planes(_ptr(rgb), _ptr(weight), w, h, ev, tonemap, bits, _ptr(out)))
     return out
+
+
+def mesh_solid(positions: np.ndarray, indices: np.ndarray) -> int:
+    """rtg_mesh_solid: 0 open, 1 closed and wound outward, 2 closed and wound inward (solid.rs)."""
+    p = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    out = _u32(0)
+    _check(lib().rtg_mesh_solid(_ptr(p), len(p), _ptr(i), len(i), ctypes.byref(out)))
+    return int(out.value)
 
 
 def features() -> int:

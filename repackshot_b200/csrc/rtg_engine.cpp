@@ -1543,6 +1543,30 @@ uint32_t rtg_render_paths(uint32_t handle, const uint32_t* xys, uint32_t n, floa
     return RTG_STATUS_OK;
 }
 
+uint32_t rtg_mesh_solid(const float* positions, uint32_t n_vertices, const uint32_t* indices, uint32_t n_indices, uint32_t* solid) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!positions || !solid || (n_indices && !indices)) { g_error = "rtg_mesh_solid: null pointer"; return RTG_STATUS_NULL_POINTER; }
+    if (n_indices % 3) { g_error = "rtg_mesh_solid: index count is not a multiple of 3"; return RTG_STATUS_BAD_ARGUMENT; }
+    HMesh m;
+    m.positions.resize(n_vertices);
+    V3 lo = v3(f_inf(), f_inf(), f_inf()), hi = v3(-f_inf(), -f_inf(), -f_inf());
+    for (uint32_t v = 0; v < n_vertices; ++v) {
+        const V3 p = v3(positions[3 * v], positions[3 * v + 1], positions[3 * v + 2]);
+        if (!vfinite(p)) { g_error = "rtg_mesh_solid: non-finite vertex position"; return RTG_STATUS_BAD_ARGUMENT; }
+        m.positions[v] = p;
+        lo = v3(rmin(lo.x, p.x), rmin(lo.y, p.y), rmin(lo.z, p.z));
+        hi = v3(rmax(hi.x, p.x), rmax(hi.y, p.y), rmax(hi.z, p.z));
+    }
+    m.indices.assign(indices, indices + n_indices);
+    for (uint32_t i : m.indices)
+        if (i >= n_vertices) { g_error = "rtg_mesh_solid: vertex index out of range"; return RTG_STATUS_BAD_ARGUMENT; }
+    m.bmin = lo;
+    m.bmax = hi;
+    m.empty_bounds = m.positions.empty();
+    *solid = solid_of(m);
+    return RTG_STATUS_OK;
+}
+
 uint32_t rtg_trace_rays(uint32_t handle, const float* rays, uint32_t n, uint32_t mode, uint32_t* out) {
     std::lock_guard<std::mutex> lk(g_mu);
     Scene* sc = scene_of(handle);
