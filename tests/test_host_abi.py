@@ -128,3 +128,19 @@ def test_without_a_gpu_a_valid_scene_fails_loudly(rtg, cfg0_rsb):
         pytest.skip("a GPU is present")
     assert rtg.scene_load(cfg0_rsb) == 0
     assert "CUDA" in rtg.error_message()
+
+
+@pytest.mark.parametrize("section, copies, words", [
+    ((1, 0.0, 0.0, 0.0, 5.0), 1, "RSB section SECT is invalid: section normal is zero"),
+    ((1, 1.0, 0.0, 0.0, 0.0), 2, "RSB section SECT appears more than once"),
+])
+def test_bad_sections_are_refused_as_the_reference_refuses_them(rtg, section, copies, words):
+    # rsb.rs:1070 parse_section and set_once: the load stops before any device work.
+    from repackshot_b200 import scenes
+    s = scenes.example_scene()
+    s.section = section
+    rsb = scenes.to_rsb(s)
+    if copies == 2:
+        rsb += rsb[rsb.index(b"SECT"):]
+    assert rtg.scene_load(rsb) == 0
+    assert rtg.error_message() == words
