@@ -1,8 +1,9 @@
 """ORACLE (test infrastructure only): ctypes binding of the C++ restatement of the Repackshot
 engine's path tracer (oracle/*.cpp, built by oracle/Makefile into oracle/_build/liborc.so).
 
-Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use it, as the checker
-and the timed CPU reference; the product (repackshot_b200) never imports it.
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use it, as the CPU results
+the device's are compared with and as the timed CPU reference; the product (repackshot_b200) never
+imports it.
 """
 from __future__ import annotations
 
