@@ -19,7 +19,6 @@ from __future__ import annotations
 import struct
 import zlib
 from fractions import Fraction
-from pathlib import Path
 
 import numpy as np
 
